@@ -1,0 +1,226 @@
+"""Host-side mirror of HPRMAT's R-matrix interface on the B200 solver.
+
+Names and argument meanings follow the reference:
+  * ``rmat_ini(nr, ns, rmax) -> zrma``                     (src/rmatrix_hp.F90:61)
+  * ``rmatrix(nch, lval, qk, eta, rmax, nr, ns, cpot) -> (cu, nopen)``
+                                                            (src/rmatrix_hp.F90:175-176)
+  * ``solve_rmatrix(cmat, B_vector, nch, nlag, normfac, solver_type=7) -> Rmat``
+                                                            (src/rmat_solvers.F90:49)
+  * ``RMatrixSolver(nr, ns, rmax).solve(lval, qk, eta, cpot) -> (cu, nopen)``
+                                                            (bindings/python/hprmat.py:79-163)
+``solver_type`` 7 is this backend; precision "mixed" (default) or "fp64" selects the
+factorisation arithmetic.  Errors raise ``HprmatError``; a collision matrix whose
+refinement stopped above the tolerance raises as well unless ``allow_unconverged``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native as nat
+from ._native import HprmatError, Stats
+
+SOLVER_B200 = nat.SOLVER_B200
+
+_PREC = {"mixed": nat.PREC_MIXED, "fp64": nat.PREC_FP64}
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+class Context:
+    """One device context (stream + device buffers) of the C library."""
+
+    def __init__(self, device: int = 0, precision: str = "mixed", max_refine: int = 3, tol: float = 1e-13,
+                 panel_nb: int = 0):
+        self._lib = nat.load()
+        self._h = ctypes.c_void_p()
+        self.opts = nat.Opts()
+        self._lib.hprmat_b200_default_opts(ctypes.byref(self.opts))
+        self.opts.precision = _PREC[precision]
+        self.opts.max_refine = int(max_refine)
+        self.opts.tol = float(tol)
+        self.opts.panel_nb = int(panel_nb)
+        nat.check(self._lib.hprmat_b200_create(int(device), ctypes.byref(self.opts), ctypes.byref(self._h)))
+        self.device = device
+        self.mesh = None
+        self._mesh_key = None
+        self.last_stats = None
+
+    def close(self):
+        if self._h:
+            self._lib.hprmat_b200_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_precision(self, precision: str, max_refine: int | None = None, tol: float | None = None):
+        self.opts.precision = _PREC[precision]
+        if max_refine is not None:
+            self.opts.max_refine = int(max_refine)
+        if tol is not None:
+            self.opts.tol = float(tol)
+        nat.check(self._lib.hprmat_b200_set_opts(self._h, ctypes.byref(self.opts)))
+
+    def set_stream(self, stream_handle: int | None):
+        nat.check(self._lib.hprmat_b200_set_stream(self._h, ctypes.c_void_p(stream_handle or 0)))
+
+    # -- rmat_ini ---------------------------------------------------------------
+    def rmat_ini(self, nr: int, ns: int, rmax: float) -> np.ndarray:
+        zrma = np.zeros(nr * ns, dtype=np.float64)
+        nat.check(self._lib.hprmat_b200_rmat_ini(self._h, int(nr), int(ns), float(rmax), _dptr(zrma)))
+        self.mesh = zrma
+        self._mesh_key = (int(nr), int(ns), float(rmax))
+        return zrma
+
+    def _ensure_mesh(self, nr, ns, rmax):
+        if self._mesh_key != (int(nr), int(ns), float(rmax)):
+            self.rmat_ini(nr, ns, rmax)
+
+    # -- rmatrix ----------------------------------------------------------------
+    def rmatrix(self, nch, lval, qk, eta, rmax, nr, ns, cpot, ndim=None, allow_unconverged=False):
+        """Collision matrix ``cu`` (ndim x ndim, U in cu[:nopen, :nopen]) and ``nopen``."""
+        self._ensure_mesh(nr, ns, rmax)
+        lval = np.ascontiguousarray(lval, dtype=np.int32)
+        qk = np.ascontiguousarray(qk, dtype=np.float64)
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        cpot = np.asfortranarray(cpot, dtype=np.complex128)
+        ncp1 = cpot.shape[0]
+        ndim = int(ndim or cpot.shape[1])
+        cu = np.zeros((ndim, ndim), dtype=np.complex128, order="F")
+        nopen = ctypes.c_int(0)
+        st = Stats()
+        s = self._lib.hprmat_b200_rmatrix(self._h, int(nch), _iptr(lval), _dptr(qk), _dptr(eta), float(rmax),
+                                          int(nr), int(ns), _dptr(cpot), int(ncp1), ndim,
+                                          _dptr(cu), ctypes.byref(nopen), ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
+        return cu, nopen.value
+
+    def rmatrix_device(self, nch, lval, qk, eta, rmax, nr, ns, d_cpot, ncp1, ndim, d_cu, allow_unconverged=False):
+        """Device-resident variant: ``d_cpot``/``d_cu`` are device addresses (ints)."""
+        self._ensure_mesh(nr, ns, rmax)
+        lval = np.ascontiguousarray(lval, dtype=np.int32)
+        qk = np.ascontiguousarray(qk, dtype=np.float64)
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        nopen = ctypes.c_int(0)
+        st = Stats()
+        s = self._lib.hprmat_b200_rmatrix_device(self._h, int(nch), _iptr(lval), _dptr(qk), _dptr(eta), float(rmax),
+                                                 int(nr), int(ns), ctypes.c_void_p(d_cpot), int(ncp1), int(ndim),
+                                                 ctypes.c_void_p(d_cu), ctypes.byref(nopen), ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
+        return nopen.value
+
+    # -- dense solves -------------------------------------------------------------
+    def solve_linear(self, A, B, allow_unconverged=False):
+        """X with A X = B (A: n x n, B: n x nrhs complex)."""
+        A = np.asfortranarray(A, dtype=np.complex128)
+        X = np.array(B, dtype=np.complex128, order="F", copy=True)
+        if X.ndim == 1:
+            X = X.reshape(-1, 1, order="F")
+        n, nrhs = X.shape
+        st = Stats()
+        s = self._lib.hprmat_b200_solve_linear(self._h, _dptr(A), _dptr(X), n,
+                                               nrhs, ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
+        return X
+
+    def solve_linear_device(self, d_A, d_B, n, nrhs, allow_unconverged=False):
+        st = Stats()
+        s = self._lib.hprmat_b200_solve_linear_device(self._h, ctypes.c_void_p(d_A), ctypes.c_void_p(d_B), int(n),
+                                                      int(nrhs), ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
+
+    def solve_rmatrix(self, cmat, B_vector, nch, nlag, normfac=1.0, allow_unconverged=False):
+        cmat = np.asfortranarray(cmat, dtype=np.complex128)
+        b = np.ascontiguousarray(B_vector, dtype=np.complex128)
+        rm = np.zeros((nch, nch), dtype=np.complex128, order="F")
+        st = Stats()
+        s = self._lib.hprmat_b200_solve_rmatrix(self._h, _dptr(cmat), _dptr(b),
+                                                int(nch), int(nlag), float(normfac), _dptr(rm),
+                                                ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
+        return rm
+
+
+def boundary_values(lval, qk, eta, rmax):
+    """Per-channel (co, cop, xc1, xc2, nopen) at the channel radius (host computation)."""
+    lib = nat.load()
+    lval = np.ascontiguousarray(lval, dtype=np.int32)
+    qk = np.ascontiguousarray(qk, dtype=np.float64)
+    eta = np.ascontiguousarray(eta, dtype=np.float64)
+    n = len(lval)
+    co = np.zeros(n, np.complex128)
+    cop = np.zeros(n, np.complex128)
+    xc1 = np.zeros(n)
+    xc2 = np.zeros(n)
+    nopen = ctypes.c_int(0)
+    nat.check(lib.hprmat_b200_boundary(n, _iptr(lval), _dptr(qk), _dptr(eta), float(rmax), _dptr(co),
+                                       _dptr(cop), _dptr(xc1), _dptr(xc2), ctypes.byref(nopen)))
+    return co, cop, xc1, xc2, nopen.value
+
+
+_default: Context | None = None
+
+
+def default_context() -> Context:
+    global _default
+    if _default is None:
+        _default = Context()
+    return _default
+
+
+def rmat_ini(nr: int, ns: int, rmax: float) -> np.ndarray:
+    return default_context().rmat_ini(nr, ns, rmax)
+
+
+def rmatrix(nch, lval, qk, eta, rmax, nr, ns, cpot, precision: str | None = None):
+    ctx = default_context()
+    if precision is not None:
+        ctx.set_precision(precision)
+    return ctx.rmatrix(nch, lval, qk, eta, rmax, nr, ns, cpot)
+
+
+def solve_rmatrix(cmat, B_vector, nch, nlag, normfac=1.0, solver_type=SOLVER_B200, precision: str | None = None):
+    if solver_type != SOLVER_B200:
+        raise ValueError(f"this backend is solver_type {SOLVER_B200}")
+    ctx = default_context()
+    if precision is not None:
+        ctx.set_precision(precision)
+    return ctx.solve_rmatrix(cmat, B_vector, nch, nlag, normfac)
+
+
+class RMatrixSolver:
+    """Mirror of the reference Python binding's ``RMatrixSolver`` for solver type 7."""
+
+    def __init__(self, nr, ns, rmax, solver=SOLVER_B200, device=0, precision="mixed"):
+        if solver != SOLVER_B200:
+            raise ValueError(f"this backend is solver type {SOLVER_B200}")
+        self.nr, self.ns, self.rmax, self.solver = int(nr), int(ns), float(rmax), int(solver)
+        self.ctx = Context(device=device, precision=precision)
+        self.mesh = self.ctx.rmat_ini(self.nr, self.ns, self.rmax)
+
+    def solve(self, lval, qk, eta, cpot, solver=None):
+        lval = np.asarray(lval, dtype=np.int32)
+        cu, nopen = self.ctx.rmatrix(len(lval), lval, qk, eta, self.rmax, self.nr, self.ns, cpot)
+        return cu, nopen

@@ -1,0 +1,128 @@
+// Shared helpers of the B200 R-matrix solver: complex arithmetic on interleaved pairs,
+// error plumbing, the bounded grid barrier used by cooperative kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+namespace hprmat {
+
+// ---------------------------------------------------------------- complex arithmetic
+template <typename R> struct Cplx;
+template <> struct Cplx<double> { using T = double2; };
+template <> struct Cplx<float> { using T = float2; };
+
+template <typename T> struct RealOf;
+template <> struct RealOf<double2> { using R = double; };
+template <> struct RealOf<float2> { using R = float; };
+
+__host__ __device__ inline double2 mk(double a, double b) { return make_double2(a, b); }
+__host__ __device__ inline float2 mk(float a, float b) { return make_float2(a, b); }
+template <typename T> __host__ __device__ inline T czero() { T z; z.x = 0; z.y = 0; return z; }
+
+template <typename T> __host__ __device__ inline T cadd(T a, T b) { T r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
+template <typename T> __host__ __device__ inline T csub(T a, T b) { T r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+template <typename T> __host__ __device__ inline T cmul(T a, T b) {
+  T r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+// acc -= a*b with fused multiply-adds
+template <typename T> __host__ __device__ inline void cfms(T& acc, T a, T b) {
+  acc.x = fma(-a.x, b.x, acc.x);
+  acc.x = fma(a.y, b.y, acc.x);
+  acc.y = fma(-a.x, b.y, acc.y);
+  acc.y = fma(-a.y, b.x, acc.y);
+}
+// acc += a*b
+template <typename T> __host__ __device__ inline void cfma(T& acc, T a, T b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+}
+// |re| + |im|: the modulus izamax/icamax use to choose pivots (LAPACK dcabs1)
+template <typename T> __host__ __device__ inline typename RealOf<T>::R cabs1(T a) {
+  return fabs(a.x) + fabs(a.y);
+}
+// 1/a with scaling (Smith's method) so that neither tiny nor huge pivots overflow
+template <typename T> __host__ __device__ inline T crecip(T a) {
+  using R = typename RealOf<T>::R;
+  T r;
+  if (fabs(a.x) >= fabs(a.y)) {
+    R t = a.y / a.x;
+    R d = a.x + a.y * t;
+    r.x = R(1) / d;
+    r.y = -t / d;
+  } else {
+    R t = a.x / a.y;
+    R d = a.x * t + a.y;
+    r.x = t / d;
+    r.y = R(-1) / d;
+  }
+  return r;
+}
+// a/b (Smith)
+template <typename T> __host__ __device__ inline T cdiv(T a, T b) { return cmul(a, crecip(b)); }
+
+__host__ __device__ inline float2 to_f(double2 a) { return make_float2((float)a.x, (float)a.y); }
+__host__ __device__ inline double2 to_d(float2 a) { return make_double2((double)a.x, (double)a.y); }
+
+// ---------------------------------------------------------------- device status words
+// Layout of the per-context device status block (int32 each).
+enum StatusWord {
+  SW_INFO = 0,       // first zero pivot, 1-based (LAPACK info), 0 if none
+  SW_TIMEOUT = 1,    // nonzero if a bounded wait gave up (value = site id)
+  SW_BARRIER = 2,    // grid barrier arrival counter (reset per cooperative launch)
+  SW_COUNT = 8
+};
+
+// Bounded grid-wide barrier for cooperative launches.  `target` = number of CTAs times
+// the barrier's ordinal (1-based) since the counter was zeroed.  Returns false when the
+// wait exceeded its limit; the caller must then stop touching shared data and return.
+__device__ inline bool grid_barrier(int* counter, int* timeout_flag, unsigned target, int site) {
+  __syncthreads();
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(counter, 1);
+    int ok = 1;
+    unsigned spins = 0;
+    for (;;) {
+      unsigned v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(counter) : "memory");
+      if (v >= target) break;
+      int tf;
+      asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(tf) : "l"(timeout_flag) : "memory");
+      if (tf != 0) { ok = 0; break; }
+      if (++spins > (1u << 24)) {  // ~ seconds with the back-off below
+        atomicExch(timeout_flag, site);
+        ok = 0;
+        break;
+      }
+      if (spins > 64) __nanosleep(64);
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+}  // namespace hprmat
+
+// ---------------------------------------------------------------- host error plumbing
+#define HPR_CUDA_TRY(expr)                                                           \
+  do {                                                                               \
+    cudaError_t _e = (expr);                                                         \
+    if (_e != cudaSuccess) {                                                         \
+      hprmat::set_last_error(_e, #expr, __FILE__, __LINE__);                         \
+      return (_e == cudaErrorMemoryAllocation) ? -3 : -2;                            \
+    }                                                                                \
+  } while (0)
+
+namespace hprmat {
+void set_last_error(cudaError_t e, const char* what, const char* file, int line);
+void set_last_error_msg(const char* msg);
+}  // namespace hprmat

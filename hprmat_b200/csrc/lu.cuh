@@ -1,0 +1,576 @@
+// Blocked right-looking complex LU with partial pivoting, and the triangular solves that
+// use its factors.  Templates over the complex element type T (double2 = FP64 path,
+// float2 = panels/solves of the mixed path).
+//
+// Storage: the matrix W is column-major with leading dimension ld (complex elements).
+// Block step s factors columns [k0, k0+ncols) with k0 = s*nb:
+//   1. panel_kernel      -- cooperative launch, the panel rows spread over all SMs and held
+//                           in shared memory; one grid barrier per column: every CTA posts
+//                           its local |re|+|im| maximum (the modulus LAPACK's izamax uses)
+//                           and that row, then all CTAs pick the same pivot, swap and
+//                           eliminate their rows.  Writes ipiv and the step's row-interchange
+//                           list.
+//   2. trsm_lower_kernel -- applies the step's row interchanges to the columns right of the
+//                           panel (or to right-hand sides) and solves with the unit lower
+//                           diagonal block: U12 = L11^-1 P A12.
+//   3. trailing update   -- A22 -= L21 U12 (cgemm_update_kernel here; the mixed path uses
+//                           the tcgen05 kernel of tc_gemm.cu).
+// Row interchanges are applied only to columns at or right of the current panel; the
+// forward solve applies each step's interchanges to the right-hand side just before that
+// step's block column, which is consistent with the factors stored that way.
+#pragma once
+#include "common.cuh"
+
+namespace hprmat {
+
+constexpr int kMaxNB = 128;
+
+// Row-interchange list of one block step (global row indices).
+struct StepSwaps {
+  int* top_src;    // [nbmax]  source row of final row k0+j, j < ncols
+  int* extra_dst;  // [nbmax]  rows >= k0+ncols that receive a displaced row
+  int* extra_src;  // [nbmax]
+  int* n_extra;    // [1]
+};
+
+template <typename T>
+struct PanelArgs {
+  T* W;
+  long ld;
+  int N, k0, ncols, rpc, G;
+  int* ipiv;                      // [N] global pivot rows (0-based)
+  T* cand_rows;                   // [2][G][NB]
+  typename RealOf<T>::R* cand_val;  // [2][G]
+  int* cand_idx;                  // [2][G]
+  T* rowj;                        // [2][NB]
+  int* status;                    // device status block
+  StepSwaps sw;
+  unsigned* growth_bits;          // running max |u_ij| (as float bits, non-negative)
+  // Optional: A-operand planes of the mixed path (hi/lo splits of Re/Im of L21, K-major).
+  float* aop;
+  long aop_plane;                 // elements between planes
+};
+
+// -------------------------------------------------------------------------------------
+// Split x into an exactly-representable TF32 head and the FP32 remainder.  hi = x rounded
+// to 10 explicit mantissa bits (round-to-nearest-even on the raw bits), lo = x - hi is
+// exact in FP32 and |lo| <= 2^-11 |x|.
+__device__ __forceinline__ void tf32_split(float x, float& hi, float& lo) {
+  unsigned u = __float_as_uint(x);
+  unsigned r = u + 0x0FFFu + ((u >> 13) & 1u);
+  r &= 0xFFFFE000u;
+  // keep inf/nan as they are
+  if ((u & 0x7F800000u) == 0x7F800000u) r = u;
+  hi = __uint_as_float(r);
+  lo = x - hi;
+}
+
+template <typename T, int NB, int NT>
+__global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
+  using R = typename RealOf<T>::R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int m = a.N - a.k0;
+  const int b = blockIdx.x;
+  const int r0 = b * a.rpc;
+  const int r1 = min(r0 + a.rpc, m);
+  const int nloc = max(r1 - r0, 0);
+  const int rpcp = a.rpc | 1;  // odd column stride: conflict-free row gathers
+  T* P = reinterpret_cast<T*>(smem_raw);                 // [NB][rpcp] column-major
+  T* urow = P + (size_t)NB * rpcp;                       // [NB]
+  __shared__ R red_v[NT / 32];
+  __shared__ int red_i[NT / 32];
+  __shared__ int s_piv, s_win, s_loc_ipiv[NB];
+  __shared__ R s_growth;
+  const int tid = threadIdx.x;
+  const int ncols = a.ncols;
+
+  // load rows [r0, r1) of the panel
+  for (int idx = tid; idx < nloc * ncols; idx += NT) {
+    int lr = idx % nloc, c = idx / nloc;
+    P[(size_t)c * rpcp + lr] = a.W[(size_t)(a.k0 + r0 + lr) + (size_t)(a.k0 + c) * a.ld];
+  }
+  if (tid == 0) s_growth = R(0);
+  __syncthreads();
+
+  for (int j = 0; j < ncols; ++j) {
+    const int buf = j & 1;
+    // (1) local pivot candidate: max |re|+|im| over rows >= j, lowest row on ties
+    R bv = R(-1);
+    int bi = 0x7fffffff;
+    for (int lr = max(j - r0, 0) + tid; lr < nloc; lr += NT) {
+      R v = cabs1(P[(size_t)j * rpcp + lr]);
+      if (v > bv) { bv = v; bi = r0 + lr; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      R ov = __shfl_down_sync(0xffffffffu, bv, o);
+      int oi = __shfl_down_sync(0xffffffffu, bi, o);
+      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    }
+    if ((tid & 31) == 0) { red_v[tid >> 5] = bv; red_i[tid >> 5] = bi; }
+    __syncthreads();
+    if (tid < 32) {
+      bv = (tid < NT / 32) ? red_v[tid] : R(-1);
+      bi = (tid < NT / 32) ? red_i[tid] : 0x7fffffff;
+      for (int o = 16; o > 0; o >>= 1) {
+        R ov = __shfl_down_sync(0xffffffffu, bv, o);
+        int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+      }
+      if (tid == 0) {
+        a.cand_val[buf * a.G + b] = bv;
+        a.cand_idx[buf * a.G + b] = bi;
+        s_piv = bi;
+      }
+    }
+    __syncthreads();
+    // (2) post the candidate row and, from its owner, the current row j
+    {
+      const int ci = s_piv;
+      const bool have = ci != 0x7fffffff;
+      for (int c = tid; c < ncols; c += NT) {
+        if (have) a.cand_rows[((size_t)buf * a.G + b) * NB + c] = P[(size_t)c * rpcp + (ci - r0)];
+        if (j >= r0 && j < r1) a.rowj[(size_t)buf * NB + c] = P[(size_t)c * rpcp + (j - r0)];
+      }
+    }
+    // (3) every CTA has posted
+    if (!grid_barrier(a.status + SW_BARRIER, a.status + SW_TIMEOUT, (unsigned)a.G * (j + 1), 1))
+      return;
+    // (4) global pivot: same reduction order in every CTA, so all agree
+    if (tid < 32) {
+      R v = R(-1);
+      int i = 0x7fffffff, w = 0;
+      for (int g = tid; g < a.G; g += 32) {
+        R gv = __ldcg(a.cand_val + buf * a.G + g);
+        int gi = __ldcg(a.cand_idx + buf * a.G + g);
+        if (gv > v || (gv == v && gi < i)) { v = gv; i = gi; w = g; }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        R ov = __shfl_down_sync(0xffffffffu, v, o);
+        int oi = __shfl_down_sync(0xffffffffu, i, o);
+        int ow = __shfl_down_sync(0xffffffffu, w, o);
+        if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; w = ow; }
+      }
+      if (tid == 0) { s_piv = i; s_win = w; }
+    }
+    __syncthreads();
+    const int p = s_piv;
+    for (int c = tid; c < ncols; c += NT) {
+      T u = __ldcg(reinterpret_cast<const T*>(a.cand_rows) + ((size_t)buf * a.G + s_win) * NB + c);
+      urow[c] = u;
+    }
+    __syncthreads();
+    if (p != j) {
+      for (int c = tid; c < ncols; c += NT) {
+        if (p >= r0 && p < r1)
+          P[(size_t)c * rpcp + (p - r0)] = __ldcg(reinterpret_cast<const T*>(a.rowj) + (size_t)buf * NB + c);
+        if (j >= r0 && j < r1) P[(size_t)c * rpcp + (j - r0)] = urow[c];
+      }
+    }
+    if (tid == 0) {
+      s_loc_ipiv[j] = p;
+      R gmax = s_growth;
+      for (int c = j; c < ncols; ++c) gmax = fmax(gmax, cabs1(urow[c]));
+      s_growth = gmax;
+    }
+    __syncthreads();
+    // (5) scale column j below the diagonal, then rank-1 update of the remaining columns
+    T piv = urow[j];
+    T inv;
+    const bool zero = (piv.x == R(0) && piv.y == R(0));
+    if (zero) {
+      inv = czero<T>();
+      if (b == 0 && tid == 0) atomicCAS(a.status + SW_INFO, 0, a.k0 + j + 1);
+    } else {
+      inv = crecip(piv);
+    }
+    const int lo = max(j + 1 - r0, 0);
+    const int nact = nloc - lo;
+    if (!zero) {
+      for (int lr = lo + tid; lr < nloc; lr += NT)
+        P[(size_t)j * rpcp + lr] = cmul(P[(size_t)j * rpcp + lr], inv);
+    }
+    __syncthreads();
+    const int nc = ncols - j - 1;
+    if (nact > 0 && nc > 0) {
+      for (int idx = tid; idx < nact * nc; idx += NT) {
+        int lr = lo + idx % nact;
+        int c = j + 1 + idx / nact;
+        T l = P[(size_t)j * rpcp + lr];
+        T v = P[(size_t)c * rpcp + lr];
+        cfms(v, l, urow[c]);
+        P[(size_t)c * rpcp + lr] = v;
+      }
+    }
+    __syncthreads();
+  }
+
+  // write the factored rows back
+  for (int idx = tid; idx < nloc * ncols; idx += NT) {
+    int lr = idx % nloc, c = idx / nloc;
+    a.W[(size_t)(a.k0 + r0 + lr) + (size_t)(a.k0 + c) * a.ld] = P[(size_t)c * rpcp + lr];
+  }
+  // A-operand planes (mixed path): rows below the diagonal block, K-major, zero padded
+  if (a.aop != nullptr) {
+    const int lr0 = max(ncols - r0, 0);
+    const int nl = nloc - lr0;
+    for (int idx = tid; idx < nl * NB; idx += NT) {
+      int c = idx % NB;
+      int lr = lr0 + idx / NB;
+      size_t row = (size_t)(r0 + lr - ncols);
+      float hr = 0.f, lrr = 0.f, hi_ = 0.f, li = 0.f;
+      if (c < ncols) {
+        T v = P[(size_t)c * rpcp + lr];
+        tf32_split((float)v.x, hr, lrr);
+        tf32_split((float)v.y, hi_, li);
+      }
+      a.aop[0 * a.aop_plane + row * NB + c] = hr;
+      a.aop[1 * a.aop_plane + row * NB + c] = lrr;
+      a.aop[2 * a.aop_plane + row * NB + c] = hi_;
+      a.aop[3 * a.aop_plane + row * NB + c] = li;
+    }
+  }
+  if (b == 0) {
+    __syncthreads();
+    if (tid < ncols) a.ipiv[a.k0 + tid] = a.k0 + s_loc_ipiv[tid];
+    if (tid == 0 && a.growth_bits) atomicMax(a.growth_bits, __float_as_uint((float)s_growth));
+    // Row-interchange list of this step: simulate the swaps on the touched positions.
+    if (tid < 32) {
+      __shared__ int pos[2 * NB], src[2 * NB];
+      __shared__ int cnt;
+      for (int j = tid; j < ncols; j += 32) { pos[j] = a.k0 + j; src[j] = a.k0 + j; }
+      if (tid == 0) cnt = ncols;
+      __syncwarp();
+      for (int j = 0; j < ncols; ++j) {
+        int bp = a.k0 + s_loc_ipiv[j];
+        if (bp == a.k0 + j) continue;
+        int slot;
+        if (bp < a.k0 + ncols) {
+          slot = bp - a.k0;
+        } else {
+          int found = -1;
+          for (int base = ncols; base < cnt; base += 32) {
+            int s = base + tid;
+            unsigned m_ = __ballot_sync(0xffffffffu, s < cnt && pos[s] == bp);
+            if (m_) { found = base + __ffs(m_) - 1; break; }
+          }
+          if (found < 0) {
+            if (tid == 0) { pos[cnt] = bp; src[cnt] = bp; cnt = cnt + 1; }
+            __syncwarp();
+            found = cnt - 1;
+          }
+          slot = found;
+        }
+        if (tid == 0) { int t = src[j]; src[j] = src[slot]; src[slot] = t; }
+        __syncwarp();
+      }
+      for (int j = tid; j < ncols; j += 32) a.sw.top_src[j] = src[j];
+      if (tid == 0) {
+        int ne = 0;
+        for (int s = ncols; s < cnt; ++s)
+          if (src[s] != pos[s]) { a.sw.extra_dst[ne] = pos[s]; a.sw.extra_src[ne] = src[s]; ++ne; }
+        *a.sw.n_extra = ne;
+      }
+    }
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// Apply the step's row interchanges to columns [c_begin, c_end) of X and solve with the
+// unit lower triangle L11 = W[k0:k0+ncols, k0:k0+ncols].  Optionally emit the result as the
+// B-operand planes of the mixed path (per column, NB consecutive K values).
+template <typename T>
+struct TrsmArgs {
+  const T* W;
+  long ld;
+  int k0, ncols;
+  const int* top_src;
+  const int* extra_dst;
+  const int* extra_src;
+  const int* n_extra;
+  T* X;
+  long ldx;
+  int c_begin, c_end;
+  float* bop;        // optional B-operand planes
+  long bop_plane;
+  int bop_col0;      // column of X that maps to B-operand column 0
+  unsigned* growth_bits;
+};
+
+template <typename T, int NB, int CW, int NT>
+__global__ void __launch_bounds__(NT) trsm_lower_kernel(TrsmArgs<T> a) {
+  using R = typename RealOf<T>::R;
+  constexpr int NBP = NB + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* A = reinterpret_cast<T*>(smem_raw);  // [CW][NBP]
+  T* E = A + CW * NBP;                    // [CW][NB]
+  const int tid = threadIdx.x;
+  const int cb = a.c_begin + blockIdx.x * CW;
+  const int ncw = min(CW, a.c_end - cb);
+  if (ncw <= 0) return;
+  const int ncols = a.ncols;
+  const int ne = *a.n_extra;
+  for (int idx = tid; idx < ncw * ncols; idx += NT) {
+    int j = idx % ncols, cc = idx / ncols;
+    A[cc * NBP + j] = a.X[(size_t)a.top_src[j] + (size_t)(cb + cc) * a.ldx];
+  }
+  for (int idx = tid; idx < ncw * ne; idx += NT) {
+    int e = idx % ne, cc = idx / ne;
+    E[cc * NB + e] = a.X[(size_t)a.extra_src[e] + (size_t)(cb + cc) * a.ldx];
+  }
+  __syncthreads();
+  for (int idx = tid; idx < ncw * ne; idx += NT) {
+    int e = idx % ne, cc = idx / ne;
+    a.X[(size_t)a.extra_dst[e] + (size_t)(cb + cc) * a.ldx] = E[cc * NB + e];
+  }
+  for (int j = 0; j < ncols - 1; ++j) {
+    __syncthreads();
+    const int nr = ncols - j - 1;
+    const T* Lcol = a.W + (size_t)(a.k0 + j) * a.ld + a.k0;
+    for (int idx = tid; idx < nr * ncw; idx += NT) {
+      int i = j + 1 + idx % nr, cc = idx / nr;
+      T l = Lcol[i];
+      T v = A[cc * NBP + i];
+      cfms(v, l, A[cc * NBP + j]);
+      A[cc * NBP + i] = v;
+    }
+  }
+  __syncthreads();
+  R gmax = R(0);
+  for (int idx = tid; idx < ncw * ncols; idx += NT) {
+    int j = idx % ncols, cc = idx / ncols;
+    T v = A[cc * NBP + j];
+    a.X[(size_t)(a.k0 + j) + (size_t)(cb + cc) * a.ldx] = v;
+    gmax = fmax(gmax, cabs1(v));
+  }
+  if (a.growth_bits) {
+    for (int o = 16; o > 0; o >>= 1) gmax = fmax(gmax, __shfl_down_sync(0xffffffffu, gmax, o));
+    if ((tid & 31) == 0) atomicMax(a.growth_bits, __float_as_uint((float)gmax));
+  }
+  if (a.bop != nullptr) {
+    for (int idx = tid; idx < ncw * NB; idx += NT) {
+      int j = idx % NB, cc = idx / NB;
+      float hr = 0.f, lr = 0.f, hi_ = 0.f, li = 0.f;
+      if (j < ncols) {
+        T v = A[cc * NBP + j];
+        tf32_split((float)v.x, hr, lr);
+        tf32_split((float)v.y, hi_, li);
+      }
+      size_t off = (size_t)(cb + cc - a.bop_col0) * NB + j;
+      a.bop[0 * a.bop_plane + off] = hr;
+      a.bop[1 * a.bop_plane + off] = lr;
+      a.bop[2 * a.bop_plane + off] = hi_;
+      a.bop[3 * a.bop_plane + off] = li;
+    }
+  }
+}
+
+// Solve with the upper triangle U11 = W[k0:k0+ncols, k0:k0+ncols] (non-unit diagonal) for
+// rows k0..k0+ncols of columns [c_begin, c_end) of X.
+template <typename T, int NB, int CW, int NT>
+__global__ void __launch_bounds__(NT) trsm_upper_kernel(const T* __restrict__ W, long ld, int k0,
+                                                        int ncols, T* X, long ldx, int c_begin,
+                                                        int c_end) {
+  constexpr int NBP = NB + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* A = reinterpret_cast<T*>(smem_raw);  // [CW][NBP]
+  T* rd = A + CW * NBP;                   // [NB]
+  const int tid = threadIdx.x;
+  const int cb = c_begin + blockIdx.x * CW;
+  const int ncw = min(CW, c_end - cb);
+  if (ncw <= 0) return;
+  for (int j = tid; j < ncols; j += NT) {
+    T d = W[(size_t)(k0 + j) + (size_t)(k0 + j) * ld];
+    rd[j] = (d.x == 0 && d.y == 0) ? czero<T>() : crecip(d);
+  }
+  for (int idx = tid; idx < ncw * ncols; idx += NT) {
+    int j = idx % ncols, cc = idx / ncols;
+    A[cc * NBP + j] = X[(size_t)(k0 + j) + (size_t)(cb + cc) * ldx];
+  }
+  for (int j = ncols - 1; j >= 0; --j) {
+    __syncthreads();
+    for (int cc = tid; cc < ncw; cc += NT) A[cc * NBP + j] = cmul(A[cc * NBP + j], rd[j]);
+    __syncthreads();
+    if (j == 0) break;
+    const T* Ucol = W + (size_t)(k0 + j) * ld + k0;
+    for (int idx = tid; idx < j * ncw; idx += NT) {
+      int i = idx % j, cc = idx / j;
+      T v = A[cc * NBP + i];
+      cfms(v, Ucol[i], A[cc * NBP + j]);
+      A[cc * NBP + i] = v;
+    }
+  }
+  __syncthreads();
+  for (int idx = tid; idx < ncw * ncols; idx += NT) {
+    int j = idx % ncols, cc = idx / ncols;
+    X[(size_t)(k0 + j) + (size_t)(cb + cc) * ldx] = A[cc * NBP + j];
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// C[M x N] -= A[M x K] * B[K x N], all column-major complex (SIMT, FMA units).  Used for
+// the FP64 LU's trailing update, the block updates of the triangular solves and the dense
+// FP64 residual.  64 x 64 output tile per 256-thread CTA, 4 x 4 outputs per thread,
+// K staged through shared memory 16 at a time.
+template <typename T>
+__global__ void __launch_bounds__(256) cgemm_update_kernel(int M, int N, int K, const T* __restrict__ A,
+                                                           long lda, const T* __restrict__ B, long ldb,
+                                                           T* C, long ldc) {
+  constexpr int BM = 64, BN = 64, BK = 16;
+  __shared__ T As[BK][BM];
+  __shared__ T Bs[BK][BN + 1];
+  const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  T acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = czero<T>();
+  for (int kb = 0; kb < K; kb += BK) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int e = tid + 256 * q;
+      int r = e & 63, k = e >> 6;
+      int gm = m0 + r, gk = kb + k;
+      As[k][r] = (gm < M && gk < K) ? A[(size_t)gm + (size_t)gk * lda] : czero<T>();
+      int kk = e & 15, cc = e >> 4;
+      int gn = n0 + cc, gk2 = kb + kk;
+      Bs[kk][cc] = (gn < N && gk2 < K) ? B[(size_t)gk2 + (size_t)gn * ldb] : czero<T>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < BK; ++k) {
+      T av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = As[k][tx + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = Bs[k][ty + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) cfma(acc[i][j], av[i], bv[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    int gm = m0 + tx + 16 * i;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int gn = n0 + ty + 16 * j;
+      if (gn >= N) continue;
+      T* p = C + (size_t)gm + (size_t)gn * ldc;
+      T v = *p;
+      v.x -= acc[i][j].x;
+      v.y -= acc[i][j].y;
+      *p = v;
+    }
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// Explicit inverses of the diagonal blocks, used by the triangular solves with many
+// right-hand sides (each block solve becomes a small dense product instead of a chain of
+// nb dependent steps).  blockIdx.x = step, blockIdx.y = 0: unit lower L11, 1: upper U11.
+// Output per step: inv[(2*s + y) * NB * NB], column-major NB x NB, zero outside the
+// triangle, explicit unit diagonal for L11^-1.  In-place column sweeps as LAPACK's
+// xTRTI2: lower from the last column backwards, upper from the first column onwards.
+template <typename T, int NB, int NT>
+__global__ void __launch_bounds__(NT) tri_inverse_kernel(const T* __restrict__ W, long ld, int N, int nb,
+                                                         T* inv) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* S = reinterpret_cast<T*>(smem_raw);  // [NB][NB] column-major
+  T* tmp = S + NB * NB;                   // [NB]
+  const int s = blockIdx.x;
+  const bool upper = blockIdx.y == 1;
+  const int k0 = s * nb;
+  const int nc = min(nb, N - k0);
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < NB * NB; idx += NT) {
+    int i = idx % NB, j = idx / NB;
+    T v = czero<T>();
+    if (i < nc && j < nc) {
+      if ((!upper && i > j) || (upper && i <= j)) v = W[(size_t)(k0 + i) + (size_t)(k0 + j) * ld];
+      if (!upper && i == j) v.x = 1;
+    }
+    if (i >= nc && i == j) v.x = 1;  // identity padding keeps the padded block invertible
+    S[idx] = v;
+  }
+  __syncthreads();
+  if (!upper) {
+    for (int j = nc - 2; j >= 0; --j) {
+      for (int i = j + 1 + tid; i < nc; i += NT) tmp[i] = S[i + j * NB];
+      __syncthreads();
+      for (int i = j + 1 + tid; i < nc; i += NT) {
+        T acc = czero<T>();
+        for (int k = j + 1; k <= i; ++k) cfma(acc, S[i + k * NB], tmp[k]);  // S[i][i] = 1
+        acc.x = -acc.x;
+        acc.y = -acc.y;
+        S[i + j * NB] = acc;
+      }
+      __syncthreads();
+    }
+  } else {
+    for (int j = 0; j < nc; ++j) {
+      for (int i = tid; i <= j; i += NT) tmp[i] = S[i + j * NB];
+      __syncthreads();
+      T d = tmp[j];
+      T dinv = (d.x == 0 && d.y == 0) ? czero<T>() : crecip(d);
+      for (int i = tid; i < j; i += NT) {
+        T acc = czero<T>();
+        for (int k = i; k < j; ++k) cfma(acc, S[i + k * NB], tmp[k]);
+        acc = cmul(acc, dinv);
+        acc.x = -acc.x;
+        acc.y = -acc.y;
+        S[i + j * NB] = acc;
+      }
+      if (tid == 0) S[j + j * NB] = dinv;
+      __syncthreads();
+    }
+  }
+  T* out = inv + ((size_t)2 * s + (upper ? 1 : 0)) * NB * NB;
+  for (int idx = tid; idx < NB * NB; idx += NT) out[idx] = S[idx];
+}
+
+// One diagonal block of a triangular solve with many right-hand sides:
+//   X[k0:k0+ncols, cols] = Tinv * (P X)[k0:k0+ncols, cols]
+// where P is the step's row-interchange list (forward solve; pass top_src = nullptr for
+// the backward solve).  Each CTA owns CW right-hand-side columns.
+template <typename T, int NB, int CW, int NT>
+__global__ void __launch_bounds__(NT) diag_apply_kernel(const T* __restrict__ Tinv, int ncols, int k0,
+                                                        const int* top_src, const int* extra_dst,
+                                                        const int* extra_src, const int* n_extra,
+                                                        T* X, long ldx, int nrhs) {
+  constexpr int NBP = NB + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Bv = reinterpret_cast<T*>(smem_raw);  // [CW][NBP]
+  T* E = Bv + CW * NBP;                    // [CW][NB]
+  const int tid = threadIdx.x;
+  const int cb = blockIdx.x * CW;
+  const int ncw = min(CW, nrhs - cb);
+  if (ncw <= 0) return;
+  const int ne = top_src ? *n_extra : 0;
+  for (int idx = tid; idx < ncw * ncols; idx += NT) {
+    int j = idx % ncols, cc = idx / ncols;
+    int src = top_src ? top_src[j] : k0 + j;
+    Bv[cc * NBP + j] = X[(size_t)src + (size_t)(cb + cc) * ldx];
+  }
+  for (int idx = tid; idx < ncw * ne; idx += NT) {
+    int e = idx % ne, cc = idx / ne;
+    E[cc * NB + e] = X[(size_t)extra_src[e] + (size_t)(cb + cc) * ldx];
+  }
+  __syncthreads();
+  for (int idx = tid; idx < ncw * ne; idx += NT) {
+    int e = idx % ne, cc = idx / ne;
+    X[(size_t)extra_dst[e] + (size_t)(cb + cc) * ldx] = E[cc * NB + e];
+  }
+  for (int idx = tid; idx < ncw * ncols; idx += NT) {
+    int i = idx % ncols, cc = idx / ncols;
+    T acc = czero<T>();
+    for (int j = 0; j < ncols; ++j) cfma(acc, Tinv[i + (size_t)j * NB], Bv[cc * NBP + j]);
+    X[(size_t)(k0 + i) + (size_t)(cb + cc) * ldx] = acc;
+  }
+}
+
+}  // namespace hprmat

@@ -1,0 +1,510 @@
+// Device kernels of the R-matrix path around the LU: assembly of C(E), the FP64
+// residual r = B - C X evaluated from C's generators, R-matrix extraction and the
+// collision-matrix (U) step, and the per-column FGMRES kernels of the refinement.
+#pragma once
+#include "common.cuh"
+
+namespace hprmat {
+
+// Per-channel data of one (J, pi, E), device resident.
+struct ChannelData {
+  const double* fac;     // [nch] l(l+1)
+  const double* kk;      // [nch] -k^2 (open) or +k^2 (closed): diagonal energy term
+  const double* bloch;   // [nch] xc(c,1) / a for closed channels, 0 for open ones
+};
+
+struct MeshDev {
+  const double* tc;      // [nr*nr] kinetic + Bloch matrix / a^2 (column-major)
+  const double* blo0;    // [nr*nr] Bloch matrix / a
+  const double* r;       // [nr] mesh radii
+  const double* q2;      // [nr] surface values
+  int nr;
+};
+
+// C(E) of src/rmatrix_hp.F90:246-293 (one interval, local potentials):
+//   channel block (c,c): tc + diag(l(l+1)/r^2 -+ k^2) - (xc/a) blo0 (closed channels)
+//   every block (c,c'):  + diag(cpot(r_i, c, c'))
+// One thread per element, threads along rows (column-major, coalesced stores).  Writes T
+// (double2 or float2).
+template <typename T>
+__global__ void assemble_kernel(MeshDev mesh, ChannelData ch, int nch, const double2* __restrict__ cpot,
+                                long ncp1, long ndim, T* W, long ld, int N) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  const int col = blockIdx.y;
+  if (row >= N) return;
+  const int nr = mesh.nr;
+  const int c = row / nr, i = row - c * nr;
+  const int cp = col / nr, j = col - cp * nr;
+  double re = 0.0, im = 0.0;
+  if (c == cp) {
+    re = mesh.tc[i + (size_t)j * nr] - ch.bloch[c] * mesh.blo0[i + (size_t)j * nr];
+    if (i == j) {
+      double rr = mesh.r[i];
+      re += ch.fac[c] / (rr * rr) + ch.kk[c];
+    }
+  }
+  if (i == j) {
+    double2 v = cpot[(size_t)i + ncp1 * ((size_t)c + ndim * (size_t)cp)];
+    re += v.x;
+    im += v.y;
+  }
+  T out;
+  out.x = (typename RealOf<T>::R)re;
+  out.y = (typename RealOf<T>::R)im;
+  W[(size_t)row + (size_t)col * ld] = out;
+}
+
+// Channel-surface right-hand sides X = blockdiag(q2) (src/rmatrix_hp.F90:456-461), scaled.
+template <typename T>
+__global__ void surface_rhs_kernel(const double* __restrict__ q2, int nr, int nch, T* X, long ldx,
+                                   int N, double scale) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  const int col = blockIdx.y;
+  if (row >= N) return;
+  const int c = row / nr, i = row - c * nr;
+  T v = czero<T>();
+  if (c == col) v.x = (typename RealOf<T>::R)(q2[i] * scale);
+  X[(size_t)row + (size_t)col * ldx] = v;
+}
+
+// out = beta*B - C X for the channel-diagonal part of C (kinetic, centrifugal, threshold,
+// closed-channel Bloch).  grid (ceil(nr/32), nch, ceil(ncol/8)), block (32, 8).
+// B is blockdiag(q2) (only when with_b != 0).
+__global__ void resid_kinetic_kernel(MeshDev mesh, ChannelData ch, const double2* __restrict__ X,
+                                     long ldx, int ncol, double2* out, long ldo, int with_b) {
+  const int nr = mesh.nr;
+  const int i = blockIdx.x * 32 + threadIdx.x;
+  const int c = blockIdx.y;
+  const int col = blockIdx.z * 8 + threadIdx.y;
+  if (i >= nr || col >= ncol) return;
+  const double bl = ch.bloch[c];
+  const double2* xc = X + (size_t)col * ldx + (size_t)c * nr;
+  double ar = 0.0, ai = 0.0;
+  for (int j = 0; j < nr; ++j) {
+    double k = mesh.tc[i + (size_t)j * nr] - bl * mesh.blo0[i + (size_t)j * nr];
+    double2 x = __ldg(xc + j);
+    ar = fma(k, x.x, ar);
+    ai = fma(k, x.y, ai);
+  }
+  const double rr = mesh.r[i];
+  const double d = ch.fac[c] / (rr * rr) + ch.kk[c];
+  double2 xi = xc[i];
+  ar = fma(d, xi.x, ar);
+  ai = fma(d, xi.y, ai);
+  double br = (with_b && c == col) ? mesh.q2[i] : 0.0;
+  out[(size_t)(c * nr + i) + (size_t)col * ldo] = make_double2(br - ar, -ai);
+}
+
+// out -= V X for the coupling part: (V X)[(c,i), col] = sum_c' cpot(r_i, c, c') X[(c',i), col].
+// grid (nr, ceil(ncol/CT)), block 256: thread -> (channel c, column).
+__global__ void resid_coupling_kernel(int nr, int nch, const double2* __restrict__ cpot, long ncp1,
+                                      long ndim, const double2* __restrict__ X, long ldx, int ncol,
+                                      double2* out, long ldo) {
+  extern __shared__ double2 xs[];  // [ncol_tile][nch] X values at radial point i
+  const int i = blockIdx.x;
+  const int ct = 32;
+  const int col0 = blockIdx.y * ct;
+  const int ncl = min(ct, ncol - col0);
+  for (int idx = threadIdx.x; idx < ncl * nch; idx += blockDim.x) {
+    int cp = idx % nch, cc = idx / nch;
+    xs[cc * nch + cp] = X[(size_t)(cp * nr + i) + (size_t)(col0 + cc) * ldx];
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < ncl * nch; idx += blockDim.x) {
+    int c = idx % nch, cc = idx / nch;
+    double ar = 0.0, ai = 0.0;
+    for (int cp = 0; cp < nch; ++cp) {
+      double2 v = __ldg(cpot + (size_t)i + ncp1 * ((size_t)c + ndim * (size_t)cp));
+      double2 x = xs[cc * nch + cp];
+      ar = fma(v.x, x.x, ar);
+      ar = fma(-v.y, x.y, ar);
+      ai = fma(v.x, x.y, ai);
+      ai = fma(v.y, x.x, ai);
+    }
+    double2* p = out + (size_t)(c * nr + i) + (size_t)(col0 + cc) * ldo;
+    double2 o = *p;
+    o.x -= ar;
+    o.y -= ai;
+    *p = o;
+  }
+}
+
+// Per-column sums of |x|^2 of an N x ncol block; one CTA per column (deterministic).
+__global__ void colnorm2_kernel(const double2* __restrict__ X, long ldx, int N, double* out) {
+  const int col = blockIdx.x;
+  const double2* x = X + (size_t)col * ldx;
+  double s = 0.0;
+  for (int r = threadIdx.x; r < N; r += blockDim.x) {
+    double2 v = x[r];
+    s = fma(v.x, v.x, fma(v.y, v.y, s));
+  }
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) out[col] = s;
+  }
+}
+
+// Conversions between the FP64 refinement vectors and the LU's element type.
+__global__ void d2f_kernel(const double2* __restrict__ src, long lds, float2* dst, long ldd, int N,
+                           const double* __restrict__ colscale) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int col = blockIdx.y;
+  if (r >= N) return;
+  double s = colscale ? colscale[col] : 1.0;
+  double2 v = src[(size_t)r + (size_t)col * lds];
+  dst[(size_t)r + (size_t)col * ldd] = make_float2((float)(v.x * s), (float)(v.y * s));
+}
+__global__ void f2d_kernel(const float2* __restrict__ src, long lds, double2* dst, long ldd, int N,
+                           const double* __restrict__ colscale) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int col = blockIdx.y;
+  if (r >= N) return;
+  double s = colscale ? colscale[col] : 1.0;
+  float2 v = src[(size_t)r + (size_t)col * lds];
+  dst[(size_t)r + (size_t)col * ldd] = make_double2((double)v.x * s, (double)v.y * s);
+}
+__global__ void copy_d_kernel(const double2* __restrict__ src, long lds, double2* dst, long ldd, int N) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int col = blockIdx.y;
+  if (r >= N) return;
+  dst[(size_t)r + (size_t)col * ldd] = src[(size_t)r + (size_t)col * lds];
+}
+__global__ void d2f_matrix_kernel(const double2* __restrict__ src, long lds, float2* dst, long ldd, int N) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int col = blockIdx.y;
+  if (r >= N) return;
+  double2 v = src[(size_t)r + (size_t)col * lds];
+  dst[(size_t)r + (size_t)col * ldd] = make_float2((float)v.x, (float)v.y);
+}
+
+// ---------------------------------------------------------------- FGMRES (per column)
+// Arnoldi step j of right-preconditioned (flexible) GMRES, one CTA per right-hand side:
+//   H[0..j, j] = V_i^H w (classical Gram-Schmidt, applied twice), w -= sum_i H[i,j] V_i,
+//   H[j+1, j] = |w|, V_{j+1} = w / |w|; then the Givens rotations of the column's
+//   least-squares problem are updated.  V: (m+1) blocks of N x ncol, w is V_{j+1}'s slot.
+// Per-column state (double): hess[(m+1) x m complex], cs[m] (real), sn[m] (complex),
+// g[m+1] (complex).
+struct GmresState {
+  double2* V;     // [(m+1)][ldv * ncol]
+  long ldv;
+  long vstride;   // elements between V blocks
+  double2* H;     // [ncol][(m+1)*m]
+  double* cs;     // [ncol][m]
+  double2* sn;    // [ncol][m]
+  double2* g;     // [ncol][m+1]
+  int m, N, ncol;
+};
+
+template <int NT>
+__device__ inline double2 block_sum2(double2 v, double2* red) {
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = (threadIdx.x < NT / 32) ? red[threadIdx.x] : make_double2(0, 0);
+    for (int o = 16; o > 0; o >>= 1) {
+      v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+      v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+    }
+    if (threadIdx.x == 0) red[32] = v;
+  }
+  __syncthreads();
+  return red[32];
+}
+
+// V_0 = r / |r|, g = (|r|, 0, ...).  r is V block 0 on entry.
+template <int NT>
+__global__ void __launch_bounds__(NT) gmres_start_kernel(GmresState s) {
+  __shared__ double2 red[33];
+  const int col = blockIdx.x;
+  double2* v = s.V + (size_t)col * s.ldv;
+  double2 acc = make_double2(0, 0);
+  for (int r = threadIdx.x; r < s.N; r += NT) {
+    double2 x = v[r];
+    acc.x = fma(x.x, x.x, fma(x.y, x.y, acc.x));
+  }
+  double beta = sqrt(block_sum2<NT>(acc, red).x);
+  double inv = beta > 0 ? 1.0 / beta : 0.0;
+  for (int r = threadIdx.x; r < s.N; r += NT) {
+    double2 x = v[r];
+    v[r] = make_double2(x.x * inv, x.y * inv);
+  }
+  if (threadIdx.x <= s.m) s.g[(size_t)col * (s.m + 1) + threadIdx.x] = make_double2(threadIdx.x == 0 ? beta : 0.0, 0.0);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) gmres_arnoldi_kernel(GmresState s, int j) {
+  __shared__ double2 red[33];
+  __shared__ double2 h[16];
+  const int col = blockIdx.x;
+  const int m = s.m;
+  double2* w = s.V + (size_t)(j + 1) * s.vstride + (size_t)col * s.ldv;
+  for (int i = threadIdx.x; i <= j; i += NT) h[i] = make_double2(0, 0);
+  __syncthreads();
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int i = 0; i <= j; ++i) {
+      const double2* vi = s.V + (size_t)i * s.vstride + (size_t)col * s.ldv;
+      double2 acc = make_double2(0, 0);
+      for (int r = threadIdx.x; r < s.N; r += NT) {
+        double2 a = vi[r], b = w[r];
+        acc.x = fma(a.x, b.x, fma(a.y, b.y, acc.x));   // conj(a) * b
+        acc.y = fma(a.x, b.y, fma(-a.y, b.x, acc.y));
+      }
+      double2 hi = block_sum2<NT>(acc, red);
+      for (int r = threadIdx.x; r < s.N; r += NT) {
+        double2 a = vi[r], b = w[r];
+        b.x -= hi.x * a.x - hi.y * a.y;
+        b.y -= hi.x * a.y + hi.y * a.x;
+        w[r] = b;
+      }
+      if (threadIdx.x == 0) { h[i].x += hi.x; h[i].y += hi.y; }
+      __syncthreads();
+    }
+  }
+  double2 acc = make_double2(0, 0);
+  for (int r = threadIdx.x; r < s.N; r += NT) {
+    double2 b = w[r];
+    acc.x = fma(b.x, b.x, fma(b.y, b.y, acc.x));
+  }
+  double hn = sqrt(block_sum2<NT>(acc, red).x);
+  const bool breakdown = !(hn > 1e-300);
+  double inv = breakdown ? 0.0 : 1.0 / hn;
+  for (int r = threadIdx.x; r < s.N; r += NT) {
+    double2 b = w[r];
+    w[r] = make_double2(b.x * inv, b.y * inv);
+  }
+  if (threadIdx.x == 0) {
+    double2* H = s.H + (size_t)col * (m + 1) * m;
+    double* cs = s.cs + (size_t)col * m;
+    double2* sn = s.sn + (size_t)col * m;
+    double2* g = s.g + (size_t)col * (m + 1);
+    double2 hc[17];
+    for (int i = 0; i <= j; ++i) hc[i] = h[i];
+    hc[j + 1] = make_double2(breakdown ? 0.0 : hn, 0.0);
+    // apply previous rotations: [c s; -conj(s) c]
+    for (int i = 0; i < j; ++i) {
+      double c = cs[i];
+      double2 sv = sn[i];
+      double2 a = hc[i], b = hc[i + 1];
+      double2 t0 = make_double2(c * a.x + (sv.x * b.x - sv.y * b.y), c * a.y + (sv.x * b.y + sv.y * b.x));
+      double2 t1 = make_double2(-(sv.x * a.x + sv.y * a.y) + c * b.x, -(sv.x * a.y - sv.y * a.x) + c * b.y);
+      hc[i] = t0;
+      hc[i + 1] = t1;
+    }
+    // new rotation zeroing hc[j+1]
+    double2 a = hc[j], b = hc[j + 1];
+    double na = hypot(a.x, a.y), nb = hypot(b.x, b.y);
+    double c;
+    double2 sv;
+    if (nb == 0.0) {
+      c = 1.0;
+      sv = make_double2(0, 0);
+    } else if (na == 0.0) {
+      c = 0.0;
+      sv = make_double2(b.x / nb, -b.y / nb);  // conj(b)/|b|
+    } else {
+      double nrm = hypot(na, nb);
+      c = na / nrm;
+      // s = (a/|a|) * conj(b) / nrm
+      double2 ph = make_double2(a.x / na, a.y / na);
+      sv = make_double2((ph.x * b.x + ph.y * b.y) / nrm, (ph.y * b.x - ph.x * b.y) / nrm);
+    }
+    cs[j] = c;
+    sn[j] = sv;
+    double2 r0 = make_double2(c * a.x + (sv.x * b.x - sv.y * b.y), c * a.y + (sv.x * b.y + sv.y * b.x));
+    hc[j] = r0;
+    hc[j + 1] = make_double2(0, 0);
+    double2 gj = g[j];
+    g[j] = make_double2(c * gj.x, c * gj.y);
+    g[j + 1] = make_double2(-(sv.x * gj.x + sv.y * gj.y), -(sv.x * gj.y - sv.y * gj.x));
+    for (int i = 0; i <= j + 1; ++i) H[(size_t)j * (m + 1) + i] = hc[i];
+  }
+}
+
+// Solve the rotated (upper triangular) least-squares system for y and apply
+// X += sum_i y_i Z_i (flexible GMRES: Z_i = M^-1 V_i).  One CTA per column.
+template <int NT>
+__global__ void __launch_bounds__(NT) gmres_update_kernel(GmresState s, int jdone, const double2* Z, long zstride,
+                                                          long ldz, double2* X, long ldx, double sign) {
+  __shared__ double2 y[16];
+  const int col = blockIdx.x;
+  const int m = s.m;
+  if (threadIdx.x == 0) {
+    const double2* H = s.H + (size_t)col * (m + 1) * m;
+    const double2* g = s.g + (size_t)col * (m + 1);
+    for (int i = jdone - 1; i >= 0; --i) {
+      double2 acc = g[i];
+      for (int k = i + 1; k < jdone; ++k) {
+        double2 hk = H[(size_t)k * (m + 1) + i];
+        acc.x -= hk.x * y[k].x - hk.y * y[k].y;
+        acc.y -= hk.x * y[k].y + hk.y * y[k].x;
+      }
+      double2 d = H[(size_t)i * (m + 1) + i];
+      double dn = d.x * d.x + d.y * d.y;
+      if (dn == 0.0) {
+        y[i] = make_double2(0, 0);
+      } else {
+        y[i] = make_double2((acc.x * d.x + acc.y * d.y) / dn, (acc.y * d.x - acc.x * d.y) / dn);
+      }
+    }
+  }
+  __syncthreads();
+  double2* x = X + (size_t)col * ldx;
+  for (int r = threadIdx.x; r < s.N; r += NT) {
+    double2 acc = x[r];
+    for (int i = 0; i < jdone; ++i) {
+      double2 z = Z[(size_t)i * zstride + (size_t)col * ldz + r];
+      acc.x += sign * (y[i].x * z.x - y[i].y * z.y);
+      acc.y += sign * (y[i].x * z.y + y[i].y * z.x);
+    }
+    x[r] = acc;
+  }
+}
+
+// ---------------------------------------------------------------- R and U
+// R(i, j) = sum_r q2(r) X((i-1) nr + r, j) / a  (src/rmatrix_hp.F90:466-474 and :337).
+__global__ void rmat_extract_kernel(const double2* __restrict__ X, long ldx, const double* __restrict__ q2,
+                                    int nr, int nch, double inv_a, double2* R) {
+  const int i = blockIdx.x;
+  const int jc = threadIdx.x + blockIdx.y * blockDim.x;
+  if (jc >= nch) return;
+  const double2* x = X + (size_t)jc * ldx + (size_t)i * nr;
+  double ar = 0.0, ai = 0.0;
+  for (int r = 0; r < nr; ++r) {
+    double2 v = x[r];
+    ar = fma(q2[r], v.x, ar);
+    ai = fma(q2[r], v.y, ai);
+  }
+  R[i + (size_t)jc * nch] = make_double2(ar * inv_a, ai * inv_a);
+}
+
+// Collision matrix (src/rmatrix_hp.F90:348-368): Z_O U = Z_I with
+//   Z_O = diag(co) - Rt diag(cop), Z_I = diag(conj co) - Rt diag(conj cop),
+//   Rt(m1,m2) = R(i1,i2) sqrt(k_i1/k_i2) over open channels; solved by Gaussian
+// elimination with partial pivoting (|re|+|im|) in one CTA.  cu (ndim x ndim) is zeroed
+// and receives U in its leading nopen x nopen block.  Work arrays: zo, zi (nopen^2).
+__global__ void __launch_bounds__(1024) umatrix_kernel(const double2* __restrict__ R, int nch,
+                                                       const int* __restrict__ open_idx,
+                                                       const double* __restrict__ qk,
+                                                       const double2* __restrict__ co,
+                                                       const double2* __restrict__ cop, int no,
+                                                       double2* zo, double2* zi, double2* cu,
+                                                       int ndim, int* info) {
+  const int tid = threadIdx.x, NT = blockDim.x;
+  for (int idx = tid; idx < ndim * ndim; idx += NT) cu[idx] = make_double2(0, 0);
+  for (int idx = tid; idx < no * no; idx += NT) {
+    int m1 = idx % no, m2 = idx / no;
+    int i1 = open_idx[m1], i2 = open_idx[m2];
+    double2 r = R[i1 + (size_t)i2 * nch];
+    double s = sqrt(qk[i1] / qk[i2]);
+    r.x *= s;
+    r.y *= s;
+    double2 p = cop[m2];
+    // zo = -r * cop ; zi = -r * conj(cop)
+    double2 a = make_double2(-(r.x * p.x - r.y * p.y), -(r.x * p.y + r.y * p.x));
+    double2 b = make_double2(-(r.x * p.x + r.y * p.y), -(-r.x * p.y + r.y * p.x));
+    if (m1 == m2) {
+      a.x += co[m1].x;
+      a.y += co[m1].y;
+      b.x += co[m1].x;
+      b.y -= co[m1].y;
+    }
+    zo[idx] = a;
+    zi[idx] = b;
+  }
+  __syncthreads();
+  __shared__ int s_p;
+  __shared__ double s_v[32];
+  __shared__ int s_i[32];
+  for (int k = 0; k < no; ++k) {
+    double bv = -1.0;
+    int bi = 0x7fffffff;
+    for (int r = k + tid; r < no; r += NT) {
+      double v = fabs(zo[r + (size_t)k * no].x) + fabs(zo[r + (size_t)k * no].y);
+      if (v > bv) { bv = v; bi = r; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      double ov = __shfl_down_sync(0xffffffffu, bv, o);
+      int oi = __shfl_down_sync(0xffffffffu, bi, o);
+      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    }
+    if ((tid & 31) == 0) { s_v[tid >> 5] = bv; s_i[tid >> 5] = bi; }
+    __syncthreads();
+    if (tid < 32) {
+      bv = (tid < NT / 32) ? s_v[tid] : -1.0;
+      bi = (tid < NT / 32) ? s_i[tid] : 0x7fffffff;
+      for (int o = 16; o > 0; o >>= 1) {
+        double ov = __shfl_down_sync(0xffffffffu, bv, o);
+        int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+      }
+      if (tid == 0) {
+        s_p = bi;
+        if (bv == 0.0 && *info == 0) *info = k + 1;
+      }
+    }
+    __syncthreads();
+    const int p = s_p;
+    if (p != k) {
+      for (int c = tid; c < no; c += NT) {
+        double2 t = zo[k + (size_t)c * no];
+        zo[k + (size_t)c * no] = zo[p + (size_t)c * no];
+        zo[p + (size_t)c * no] = t;
+        t = zi[k + (size_t)c * no];
+        zi[k + (size_t)c * no] = zi[p + (size_t)c * no];
+        zi[p + (size_t)c * no] = t;
+      }
+    }
+    __syncthreads();
+    double2 piv = zo[k + (size_t)k * no];
+    double2 inv = (piv.x == 0 && piv.y == 0) ? make_double2(0, 0) : crecip(piv);
+    for (int r = k + 1 + tid; r < no; r += NT) zo[r + (size_t)k * no] = cmul(zo[r + (size_t)k * no], inv);
+    __syncthreads();
+    const int nrow = no - k - 1;
+    const int ncz = no - k - 1;  // columns k+1.. of zo
+    const int total = nrow * (ncz + no);
+    for (int idx = tid; idx < total; idx += NT) {
+      int r = k + 1 + idx % nrow;
+      int c = idx / nrow;
+      double2 l = zo[r + (size_t)k * no];
+      if (c < ncz) {
+        int cc = k + 1 + c;
+        double2 v = zo[r + (size_t)cc * no];
+        cfms(v, l, zo[k + (size_t)cc * no]);
+        zo[r + (size_t)cc * no] = v;
+      } else {
+        int cc = c - ncz;
+        double2 v = zi[r + (size_t)cc * no];
+        cfms(v, l, zi[k + (size_t)cc * no]);
+        zi[r + (size_t)cc * no] = v;
+      }
+    }
+    __syncthreads();
+  }
+  // back substitution, columns of zi in parallel
+  for (int c = tid; c < no; c += NT) {
+    for (int k = no - 1; k >= 0; --k) {
+      double2 v = zi[k + (size_t)c * no];
+      for (int q = k + 1; q < no; ++q) cfms(v, zo[k + (size_t)q * no], zi[q + (size_t)c * no]);
+      double2 d = zo[k + (size_t)k * no];
+      v = (d.x == 0 && d.y == 0) ? make_double2(0, 0) : cdiv(v, d);
+      zi[k + (size_t)c * no] = v;
+    }
+  }
+  __syncthreads();
+  for (int idx = tid; idx < no * no; idx += NT) {
+    int m1 = idx % no, m2 = idx / no;
+    cu[m1 + (size_t)m2 * ndim] = zi[idx];
+  }
+}
+
+}  // namespace hprmat

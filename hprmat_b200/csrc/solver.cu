@@ -1,0 +1,1203 @@
+// Host runtime of the B200 R-matrix solver: context, mesh, LU / solve drivers, FP64
+// refinement and the C ABI declared in include/hprmat_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/hprmat_b200.h"
+#include "../../include/hprmat_b200_dev.h"
+#include "common.cuh"
+#include "coulomb.cuh"
+#include "lu.cuh"
+#include "rmat_kernels.cuh"
+#include "tc_gemm.cuh"
+
+using namespace hprmat;
+
+// ------------------------------------------------------------------ error reporting
+static thread_local std::string g_last_error;
+
+void hprmat::set_last_error(cudaError_t e, const char* what, const char* file, int line) {
+  char buf[512];
+  snprintf(buf, sizeof(buf), "%s: %s (%s:%d)", cudaGetErrorString(e), what, file, line);
+  g_last_error = buf;
+}
+void hprmat::set_last_error_msg(const char* msg) { g_last_error = msg; }
+
+static int fail(int status, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return status;
+}
+
+#define TRY(expr)                  \
+  do {                             \
+    int _s = (expr);               \
+    if (_s != HPRMAT_B200_OK) return _s; \
+  } while (0)
+
+#define LAUNCH_CHECK() HPR_CUDA_TRY(cudaGetLastError())
+
+// ------------------------------------------------------------------ device buffers
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t b) {
+    if (b <= bytes && p) return HPRMAT_B200_OK;
+    release();
+    if (b == 0) b = 16;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      bytes = 0;
+      cudaGetLastError();
+      return fail(HPRMAT_B200_ERR_OOM, "cudaMalloc(%zu bytes) failed: %s", b, cudaGetErrorString(e));
+    }
+    bytes = b;
+    return HPRMAT_B200_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+static constexpr int kSwapStride = 3 * kMaxNB + 4;  // ints per step in the swap store
+static constexpr int kGmresM = 3;                    // inner FGMRES iterations per outer step
+
+struct hprmat_b200_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  hprmat_b200_opts opts{};
+  int nsm = 0;
+  int smem_optin = 0;
+  // mesh (rmat_ini)
+  int nr = 0, ns = 0;
+  double rmax = 0.0;
+  std::vector<double> xle, wle, tc, blo0, q2, zrma;
+  DevBuf mesh;  // tc | blo0 | r | q2
+  // work buffers
+  DevBuf W, A64, X, X64, R64, B64, V, Z, gm, swaps, ipiv, stage, status, ops, inv, chan, rmat,
+      zwork, cpot, cu, norms;
+  int* h_status = nullptr;  // pinned
+  double* h_norms = nullptr;  // pinned
+  TcGemmPlan tcplan;
+};
+
+// ------------------------------------------------------------------ mesh (rmat_ini)
+// Gauss-Legendre nodes and weights on (0,1): LEGZO, src/rmatrix_hp.F90:741-783.
+static void legzo(int n, std::vector<double>& x, std::vector<double>& w) {
+  const double pi = 3.1415926535898, one = 1.0;
+  std::vector<double> X(n + 1, 0.0), Wt(n + 1, 0.0);
+  int n0 = (n + 1) / 2;
+  for (int nr = 1; nr <= n0; ++nr) {
+    double z = cos(pi * (nr - 0.25) / (n + 0.5));
+    double pd = 0.0, pf = 0.0;
+    for (;;) {
+      double z0 = z, p = 1.0;
+      for (int i = 1; i <= nr - 1; ++i) p = p * (z - X[i]);
+      double f0 = 1.0;
+      if (nr == n0 && n != 2 * (n / 2)) z = 0.0;
+      double f1 = z;
+      for (int k = 2; k <= n; ++k) {
+        pf = (2 - one / k) * z * f1 - (1 - one / k) * f0;
+        pd = k * (f1 - z * pf) / (1 - z * z);
+        f0 = f1;
+        f1 = pf;
+      }
+      if (z == 0.0) break;
+      double fd = pf / p, q = 0.0;
+      for (int i = 1; i <= nr - 1; ++i) {
+        double wp = 1.0;
+        for (int j = 1; j <= nr - 1; ++j)
+          if (j != i) wp = wp * (z - X[j]);
+        q = q + wp;
+      }
+      double gd = (pd - q * fd) / p;
+      z = z - fd / gd;
+      if (!(fabs(z - z0) > fabs(z) * 1.0e-15)) break;
+    }
+    X[nr] = z;
+    X[n + 1 - nr] = -z;
+    Wt[nr] = 2 / ((1 - z * z) * pd * pd);
+    Wt[n + 1 - nr] = Wt[nr];
+  }
+  x.resize(n);
+  w.resize(n);
+  for (int i = 0; i < n; ++i) {
+    x[i] = (1 + X[n - i]) / 2;
+    w[i] = Wt[n - i] / 2;
+  }
+}
+
+// Kinetic + Bloch matrix, Bloch matrix and surface values of the first interval:
+// src/rmatrix_hp.F90:85-151 (is = 1), scaled as at :146-151.
+static void build_mesh(hprmat_b200_ctx* c, int nr, int ns, double rmax) {
+  c->nr = nr;
+  c->ns = ns;
+  c->rmax = rmax;
+  legzo(nr, c->xle, c->wle);
+  const double rmax0 = rmax / ns;
+  c->tc.assign((size_t)nr * nr, 0.0);
+  c->blo0.assign((size_t)nr * nr, 0.0);
+  c->q2.assign(nr, 0.0);
+  for (int i1 = 1; i1 <= nr; ++i1) {
+    double xi = c->xle[i1 - 1], xi2 = xi * (1 - xi);
+    double xx = 4.0 * nr * (nr + 1) + 3 + (1 - 6 * xi) / xi2;
+    c->tc[(i1 - 1) + (size_t)(i1 - 1) * nr] = xx / (3 * xi2);
+    c->blo0[(i1 - 1) + (size_t)(i1 - 1) * nr] = 1 / xi2;
+    for (int i2 = 1; i2 <= i1 - 1; ++i2) {
+      double xj = c->xle[i2 - 1], xj2 = xj * (1 - xj);
+      double d = xi - xj;
+      double t = (double)nr * (nr + 1) + 1 + (xi + xj - 2 * xi * xj) / (d * d) - 1 / (1 - xi) - 1 / (1 - xj);
+      t = t / sqrt(xi2 * xj2);
+      double b = 1 / sqrt(xi2 * xj2);
+      if ((i1 + i2) % 2 == 1) {
+        t = -t;
+        b = -b;
+      }
+      c->tc[(i1 - 1) + (size_t)(i2 - 1) * nr] = t;
+      c->tc[(i2 - 1) + (size_t)(i1 - 1) * nr] = t;
+      c->blo0[(i1 - 1) + (size_t)(i2 - 1) * nr] = b;
+      c->blo0[(i2 - 1) + (size_t)(i1 - 1) * nr] = b;
+    }
+  }
+  for (int i = 0; i < nr; ++i) {
+    double q = 1 / sqrt(c->xle[i] * (1 - c->xle[i]));
+    if (nr % 2 == 1) q = -q;
+    if (i % 2 == 0) q = -q;  // q2(1:nr:2) = -q2(1:nr:2)
+    c->q2[i] = q / sqrt(rmax0);
+  }
+  for (auto& v : c->tc) v = v / (rmax0 * rmax0);
+  for (auto& v : c->blo0) v = v / rmax0;
+  c->zrma.resize((size_t)nr * ns);
+  for (int is = 0; is < ns; ++is)
+    for (int i = 0; i < nr; ++i) c->zrma[(size_t)is * nr + i] = (is + c->xle[i]) * rmax0;
+}
+
+static int upload_mesh(hprmat_b200_ctx* c) {
+  const int nr = c->nr;
+  size_t n = (size_t)2 * nr * nr + 2 * nr;
+  TRY(c->mesh.ensure(n * sizeof(double)));
+  std::vector<double> h(n);
+  std::copy(c->tc.begin(), c->tc.end(), h.begin());
+  std::copy(c->blo0.begin(), c->blo0.end(), h.begin() + (size_t)nr * nr);
+  for (int i = 0; i < nr; ++i) h[(size_t)2 * nr * nr + i] = c->zrma[i];
+  for (int i = 0; i < nr; ++i) h[(size_t)2 * nr * nr + nr + i] = c->q2[i];
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->mesh.p, h.data(), n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return HPRMAT_B200_OK;
+}
+
+static MeshDev mesh_dev(const hprmat_b200_ctx* c) {
+  const double* base = c->mesh.as<double>();
+  MeshDev m;
+  m.nr = c->nr;
+  m.tc = base;
+  m.blo0 = base + (size_t)c->nr * c->nr;
+  m.r = base + (size_t)2 * c->nr * c->nr;
+  m.q2 = base + (size_t)2 * c->nr * c->nr + c->nr;
+  return m;
+}
+
+// ------------------------------------------------------------------ launch helpers
+template <typename K>
+static int set_smem(K kernel, size_t bytes) {
+  if (bytes > 48 * 1024)
+    HPR_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return HPRMAT_B200_OK;
+}
+
+static inline unsigned cdiv_u(long a, long b) { return (unsigned)((a + b - 1) / b); }
+
+// ------------------------------------------------------------------ LU driver
+struct LUState {
+  int N = 0;
+  long ld = 0;
+  int nb = 0;
+  int nsteps = 0;
+};
+
+static int pick_nb(const hprmat_b200_ctx* c, int N, size_t elem, int preferred) {
+  if (c->opts.panel_nb > 0) preferred = c->opts.panel_nb;
+  for (int nb = preferred; nb >= 16; nb /= 2) {
+    int G = std::min(c->nsm, std::max(1, (N + 31) / 32));
+    int rpc = (N + G - 1) / G;
+    size_t smem = ((size_t)nb * (rpc | 1) + nb) * elem;
+    if (smem + 8192 <= (size_t)c->smem_optin) return nb;
+  }
+  return 0;
+}
+
+template <typename T, int NB>
+static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUState& st) {
+  constexpr int NT = 256;
+  const int nsteps = (N + NB - 1) / NB;
+  st.N = N;
+  st.ld = ld;
+  st.nb = NB;
+  st.nsteps = nsteps;
+  int* status = c->status.as<int>();
+  HPR_CUDA_TRY(cudaMemsetAsync(status, 0, SW_COUNT * sizeof(int), c->stream));
+  const int G0 = std::min(c->nsm, std::max(1, (N + 31) / 32));
+  TRY(c->stage.ensure((size_t)2 * G0 * NB * sizeof(T) + (size_t)4 * G0 * sizeof(double) +
+                      (size_t)2 * NB * sizeof(T) + 256));
+  TRY(c->swaps.ensure((size_t)nsteps * kSwapStride * sizeof(int)));
+  TRY(c->ipiv.ensure((size_t)N * sizeof(int) + 64));
+  unsigned char* sp = c->stage.as<unsigned char>();
+  T* cand_rows = reinterpret_cast<T*>(sp);
+  sp += (size_t)2 * G0 * NB * sizeof(T);
+  typename RealOf<T>::R* cand_val = reinterpret_cast<typename RealOf<T>::R*>(sp);
+  sp += (size_t)2 * G0 * sizeof(double);
+  int* cand_idx = reinterpret_cast<int*>(sp);
+  sp += (size_t)2 * G0 * sizeof(double);
+  T* rowj = reinterpret_cast<T*>(sp);
+  unsigned* growth = reinterpret_cast<unsigned*>(status + SW_COUNT - 1);
+
+  float* aop = nullptr;
+  float* bop = nullptr;
+  long plane = 0;
+  if (mixed) {
+    plane = (long)(N + 256) * NB;
+    TRY(c->ops.ensure((size_t)8 * plane * sizeof(float)));
+    aop = c->ops.as<float>();
+    bop = aop + 4 * plane;
+  }
+
+  auto pk = panel_kernel<T, NB, NT>;
+  for (int s = 0; s < nsteps; ++s) {
+    const int k0 = s * NB;
+    const int ncols = std::min(NB, N - k0);
+    const int m = N - k0;
+    const int G = std::min(G0, std::max(1, (m + 31) / 32));
+    const int rpc = (m + G - 1) / G;
+    const size_t smem = ((size_t)NB * (rpc | 1) + NB) * sizeof(T);
+    TRY(set_smem(pk, smem));
+    HPR_CUDA_TRY(cudaMemsetAsync(status + SW_BARRIER, 0, sizeof(int), c->stream));
+    PanelArgs<T> pa;
+    pa.W = W;
+    pa.ld = ld;
+    pa.N = N;
+    pa.k0 = k0;
+    pa.ncols = ncols;
+    pa.rpc = rpc;
+    pa.G = G;
+    pa.ipiv = c->ipiv.as<int>();
+    pa.cand_rows = cand_rows;
+    pa.cand_val = cand_val;
+    pa.cand_idx = cand_idx;
+    pa.rowj = rowj;
+    pa.status = status;
+    int* swb = c->swaps.as<int>() + (size_t)s * kSwapStride;
+    pa.sw.top_src = swb;
+    pa.sw.extra_dst = swb + kMaxNB;
+    pa.sw.extra_src = swb + 2 * kMaxNB;
+    pa.sw.n_extra = swb + 3 * kMaxNB;
+    pa.growth_bits = growth;
+    pa.aop = (mixed && k0 + ncols < N) ? aop : nullptr;
+    pa.aop_plane = plane;
+    void* args[] = {&pa};
+    HPR_CUDA_TRY(cudaLaunchCooperativeKernel((void*)pk, dim3(G), dim3(NT), args, smem, c->stream));
+    if (k0 + ncols >= N) break;
+    // row interchanges + U12 = L11^-1 A12
+    {
+      constexpr int CW = 32;
+      auto tk = trsm_lower_kernel<T, NB, CW, NT>;
+      size_t tsm = (size_t)CW * (NB + 1) * sizeof(T) + (size_t)CW * NB * sizeof(T);
+      TRY(set_smem(tk, tsm));
+      TrsmArgs<T> ta;
+      ta.W = W;
+      ta.ld = ld;
+      ta.k0 = k0;
+      ta.ncols = ncols;
+      ta.top_src = pa.sw.top_src;
+      ta.extra_dst = pa.sw.extra_dst;
+      ta.extra_src = pa.sw.extra_src;
+      ta.n_extra = pa.sw.n_extra;
+      ta.X = W;
+      ta.ldx = ld;
+      ta.c_begin = k0 + ncols;
+      ta.c_end = N;
+      ta.bop = mixed ? bop : nullptr;
+      ta.bop_plane = plane;
+      ta.bop_col0 = k0 + ncols;
+      ta.growth_bits = growth;
+      tk<<<cdiv_u(N - k0 - ncols, CW), NT, tsm, c->stream>>>(ta);
+      LAUNCH_CHECK();
+    }
+    // trailing update A22 -= L21 U12
+    const int M2 = N - k0 - ncols;
+    if (mixed) {
+      TRY(tc_trailing_update(c->tcplan, aop, bop, plane, NB, ncols, reinterpret_cast<float2*>(W) + (k0 + ncols) + (size_t)(k0 + ncols) * ld,
+                             ld, M2, M2, c->stream));
+    } else {
+      dim3 grid(cdiv_u(M2, 64), cdiv_u(M2, 64));
+      cgemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(M2, M2, ncols, W + (k0 + ncols) + (size_t)k0 * ld, ld,
+                                                         W + k0 + (size_t)(k0 + ncols) * ld, ld,
+                                                         W + (k0 + ncols) + (size_t)(k0 + ncols) * ld, ld);
+      LAUNCH_CHECK();
+    }
+  }
+  // explicit inverses of the diagonal blocks for the solves
+  {
+    TRY(c->inv.ensure((size_t)2 * nsteps * NB * NB * sizeof(T)));
+    auto ik = tri_inverse_kernel<T, NB, NT>;
+    size_t ism = ((size_t)NB * NB + NB) * sizeof(T);
+    TRY(set_smem(ik, ism));
+    ik<<<dim3(nsteps, 2), NT, ism, c->stream>>>(W, ld, N, NB, c->inv.as<T>());
+    LAUNCH_CHECK();
+  }
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->h_status, status, SW_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (c->h_status[SW_TIMEOUT] != 0)
+    return fail(HPRMAT_B200_ERR_TIMEOUT, "panel factorisation: grid barrier wait limit exceeded (site %d)",
+                c->h_status[SW_TIMEOUT]);
+  if (mixed) {
+    int err = 0;
+    TRY(tc_gemm_check(c->tcplan, c->stream, &err));
+    if (err) return fail(HPRMAT_B200_ERR_TIMEOUT, "tensor-core update: wait limit exceeded at site %d", err);
+  }
+  return HPRMAT_B200_OK;
+}
+
+template <typename T>
+static int factor(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, int nb, LUState& st) {
+  switch (nb) {
+    case 128: return factor_impl<T, 128>(c, W, ld, N, mixed, st);
+    case 64: return factor_impl<T, 64>(c, W, ld, N, mixed, st);
+    case 32: return factor_impl<T, 32>(c, W, ld, N, mixed, st);
+    case 16: return factor_impl<T, 16>(c, W, ld, N, mixed, st);
+  }
+  return fail(HPRMAT_B200_ERR_UNSUPPORTED, "unsupported block size %d", nb);
+}
+
+// Forward and backward substitution with the stored factors, in place on X (N x nrhs).
+template <typename T, int NB>
+static int lu_solve_impl(hprmat_b200_ctx* c, const T* W, const LUState& st, T* X, long ldx, int nrhs) {
+  constexpr int NT = 256, CW = 8;
+  const int N = st.N;
+  const long ld = st.ld;
+  const T* inv = c->inv.as<T>();
+  auto dk = diag_apply_kernel<T, NB, CW, NT>;
+  size_t dsm = (size_t)CW * (NB + 1) * sizeof(T) + (size_t)CW * NB * sizeof(T);
+  TRY(set_smem(dk, dsm));
+  const int* swb = c->swaps.as<int>();
+  for (int s = 0; s < st.nsteps; ++s) {
+    const int k0 = s * NB, ncols = std::min(NB, N - k0);
+    const int* sw = swb + (size_t)s * kSwapStride;
+    dk<<<cdiv_u(nrhs, CW), NT, dsm, c->stream>>>(inv + (size_t)2 * s * NB * NB, ncols, k0, sw, sw + kMaxNB,
+                                                 sw + 2 * kMaxNB, sw + 3 * kMaxNB, X, ldx, nrhs);
+    LAUNCH_CHECK();
+    const int M2 = N - k0 - ncols;
+    if (M2 > 0) {
+      dim3 grid(cdiv_u(M2, 64), cdiv_u(nrhs, 64));
+      cgemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(M2, nrhs, ncols, W + (k0 + ncols) + (size_t)k0 * ld, ld,
+                                                         X + k0, ldx, X + k0 + ncols, ldx);
+      LAUNCH_CHECK();
+    }
+  }
+  for (int s = st.nsteps - 1; s >= 0; --s) {
+    const int k0 = s * NB, ncols = std::min(NB, N - k0);
+    dk<<<cdiv_u(nrhs, CW), NT, dsm, c->stream>>>(inv + ((size_t)2 * s + 1) * NB * NB, ncols, k0, nullptr,
+                                                 nullptr, nullptr, nullptr, X, ldx, nrhs);
+    LAUNCH_CHECK();
+    if (k0 > 0) {
+      dim3 grid(cdiv_u(k0, 64), cdiv_u(nrhs, 64));
+      cgemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(k0, nrhs, ncols, W + (size_t)k0 * ld, ld, X + k0, ldx,
+                                                         X, ldx);
+      LAUNCH_CHECK();
+    }
+  }
+  return HPRMAT_B200_OK;
+}
+
+template <typename T>
+static int lu_solve(hprmat_b200_ctx* c, const T* W, const LUState& st, T* X, long ldx, int nrhs) {
+  switch (st.nb) {
+    case 128: return lu_solve_impl<T, 128>(c, W, st, X, ldx, nrhs);
+    case 64: return lu_solve_impl<T, 64>(c, W, st, X, ldx, nrhs);
+    case 32: return lu_solve_impl<T, 32>(c, W, st, X, ldx, nrhs);
+    case 16: return lu_solve_impl<T, 16>(c, W, st, X, ldx, nrhs);
+  }
+  return fail(HPRMAT_B200_ERR_UNSUPPORTED, "unsupported block size %d", st.nb);
+}
+
+// ------------------------------------------------------------------ operators for refinement
+// out = with_b * B - C X (FP64).  Either the structured C(E) of the R-matrix problem or a
+// dense FP64 matrix.
+struct Operator {
+  bool structured = false;
+  // structured
+  MeshDev mesh;
+  ChannelData ch;
+  int nch = 0;
+  const double2* cpot = nullptr;
+  long ncp1 = 0, ndim = 0;
+  // dense
+  const double2* A = nullptr;
+  long lda = 0;
+  const double2* B = nullptr;  // dense right-hand side (N x nrhs, ld = ldb)
+  long ldb = 0;
+  int N = 0;
+};
+
+static int apply_residual(hprmat_b200_ctx* c, const Operator& op, const double2* X, long ldx, int ncol,
+                          double2* out, long ldo, bool with_b) {
+  const int N = op.N;
+  if (op.structured) {
+    const int nr = op.mesh.nr;
+    dim3 g1(cdiv_u(nr, 32), op.nch, cdiv_u(ncol, 8));
+    resid_kinetic_kernel<<<g1, dim3(32, 8), 0, c->stream>>>(op.mesh, op.ch, X, ldx, ncol, out, ldo, with_b ? 1 : 0);
+    LAUNCH_CHECK();
+    size_t sm = (size_t)32 * op.nch * sizeof(double2);
+    TRY(set_smem(resid_coupling_kernel, sm));
+    dim3 g2(nr, cdiv_u(ncol, 32));
+    resid_coupling_kernel<<<g2, 256, sm, c->stream>>>(nr, op.nch, op.cpot, op.ncp1, op.ndim, X, ldx, ncol, out, ldo);
+    LAUNCH_CHECK();
+  } else {
+    dim3 g0(cdiv_u(N, 256), ncol);
+    if (with_b) {
+      copy_d_kernel<<<g0, 256, 0, c->stream>>>(op.B, op.ldb, out, ldo, N);
+    } else {
+      HPR_CUDA_TRY(cudaMemset2DAsync(out, ldo * sizeof(double2), 0, (size_t)N * sizeof(double2), ncol, c->stream));
+    }
+    LAUNCH_CHECK();
+    dim3 grid(cdiv_u(N, 64), cdiv_u(ncol, 64));
+    cgemm_update_kernel<double2><<<grid, 256, 0, c->stream>>>(N, ncol, N, op.A, op.lda, X, ldx, out, ldo);
+    LAUNCH_CHECK();
+  }
+  return HPRMAT_B200_OK;
+}
+
+static int frob_norm(hprmat_b200_ctx* c, const double2* X, long ldx, int N, int ncol, double* result) {
+  TRY(c->norms.ensure((size_t)ncol * sizeof(double)));
+  colnorm2_kernel<<<ncol, 256, 0, c->stream>>>(X, ldx, N, c->norms.as<double>());
+  LAUNCH_CHECK();
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->h_norms, c->norms.p, (size_t)ncol * sizeof(double), cudaMemcpyDeviceToHost,
+                               c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  double s = 0.0;
+  for (int i = 0; i < ncol; ++i) s += c->h_norms[i];
+  *result = sqrt(s);
+  return HPRMAT_B200_OK;
+}
+
+// Mixed path: X64 (N x nrhs, FP64) from the FP32 factors, refined with FGMRES on the FP64
+// operator.  Each outer step: r = B - C X; stop when |r|_F/|B|_F < tol; otherwise run
+// kGmresM flexible-GMRES iterations on C d = r, preconditioned by the FP32 LU solve, and
+// X += d.  Returns NOT_CONVERGED if max_refine outer corrections did not reach tol.
+static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W32, const LUState& st,
+                        double2* X64, long ldx, int nrhs, double bnorm, hprmat_b200_stats* stats) {
+  const int N = op.N;
+  const int m = kGmresM;
+  const long ldv = st.ld;
+  const long vstride = ldv * nrhs;
+  TRY(c->V.ensure((size_t)(m + 1) * vstride * sizeof(double2)));
+  TRY(c->Z.ensure((size_t)m * vstride * sizeof(double2)));
+  TRY(c->gm.ensure((size_t)nrhs * ((m + 1) * m * sizeof(double2) + m * sizeof(double) + m * sizeof(double2) +
+                                   (m + 1) * sizeof(double2)) + 256));
+  TRY(c->X.ensure((size_t)ldv * nrhs * sizeof(float2)));
+  double2* V = c->V.as<double2>();
+  double2* Z = c->Z.as<double2>();
+  float2* X32 = c->X.as<float2>();
+  GmresState gs;
+  gs.V = V;
+  gs.ldv = ldv;
+  gs.vstride = vstride;
+  unsigned char* gp = c->gm.as<unsigned char>();
+  gs.H = reinterpret_cast<double2*>(gp);
+  gp += (size_t)nrhs * (m + 1) * m * sizeof(double2);
+  gs.sn = reinterpret_cast<double2*>(gp);
+  gp += (size_t)nrhs * m * sizeof(double2);
+  gs.g = reinterpret_cast<double2*>(gp);
+  gp += (size_t)nrhs * (m + 1) * sizeof(double2);
+  gs.cs = reinterpret_cast<double*>(gp);
+  gs.m = m;
+  gs.N = N;
+  gs.ncol = nrhs;
+  dim3 gconv(cdiv_u(N, 256), nrhs);
+  int steps = 0;
+  int status = HPRMAT_B200_OK;
+  for (int outer = 0;; ++outer) {
+    TRY(apply_residual(c, op, X64, ldx, nrhs, V, ldv, true));
+    double rn;
+    TRY(frob_norm(c, V, ldv, N, nrhs, &rn));
+    double rel = rn / bnorm;
+    if (stats && outer < 9) stats->residual_history[outer] = rel;
+    if (stats) stats->rel_residual = rel;
+    if (!(rel >= c->opts.tol)) break;  // converged (also stops on rel == 0)
+    if (outer >= c->opts.max_refine) {
+      status = HPRMAT_B200_NOT_CONVERGED;
+      break;
+    }
+    gmres_start_kernel<256><<<nrhs, 256, 0, c->stream>>>(gs);
+    LAUNCH_CHECK();
+    for (int j = 0; j < m; ++j) {
+      d2f_kernel<<<gconv, 256, 0, c->stream>>>(V + (size_t)j * vstride, ldv, X32, ldv, N, nullptr);
+      LAUNCH_CHECK();
+      TRY(lu_solve<float2>(c, W32, st, X32, ldv, nrhs));
+      f2d_kernel<<<gconv, 256, 0, c->stream>>>(X32, ldv, Z + (size_t)j * vstride, ldv, N, nullptr);
+      LAUNCH_CHECK();
+      // V_{j+1} = -C Z_j: FGMRES runs on the operator -C, so the correction is subtracted
+      TRY(apply_residual(c, op, Z + (size_t)j * vstride, ldv, nrhs, V + (size_t)(j + 1) * vstride, ldv, false));
+      gmres_arnoldi_kernel<256><<<nrhs, 256, 0, c->stream>>>(gs, j);
+      LAUNCH_CHECK();
+    }
+    gmres_update_kernel<256><<<nrhs, 256, 0, c->stream>>>(gs, m, Z, vstride, ldv, X64, ldx, -1.0);
+    LAUNCH_CHECK();
+    ++steps;
+  }
+  if (stats) stats->refine_steps = steps;
+  return status;
+}
+
+// ------------------------------------------------------------------ boundary values
+struct Boundary {
+  int nopen = 0;
+  std::vector<int> open_idx;
+  std::vector<double> fac, kk, bloch, qk;
+  std::vector<double2> co, cop;
+};
+
+// src/rmatrix_hp.F90:224-244 and the per-channel diagonal terms of :259-276.
+static int boundary_values(int nch, const int* lval, const double* qk, const double* eta, double rmax, double rmax2,
+                           Boundary& b) {
+  b = Boundary();
+  b.fac.resize(nch);
+  b.kk.resize(nch);
+  b.bloch.resize(nch);
+  b.qk.assign(qk, qk + nch);
+  for (int c = 0; c < nch; ++c) {
+    const int l = lval[c];
+    if (l < 0) return fail(HPRMAT_B200_ERR_ARG, "lval(%d) = %d < 0", c + 1, l);
+    b.fac[c] = (double)l * (l + 1);
+    b.kk[c] = 0.0;
+    b.bloch[c] = 0.0;
+    if (qk[c] > 0) {
+      b.kk[c] = -qk[c] * qk[c];
+      CoulombFG f = coulfg_single(qk[c] * rmax, eta[c], (double)l);
+      if (f.ifail != 0) return fail(HPRMAT_B200_ERR_ARG, "COULFG failed (ifail=%d) for channel %d", f.ifail, c + 1);
+      b.open_idx.push_back(c);
+      b.co.push_back(make_double2(f.g, f.f));
+      b.cop.push_back(make_double2(f.gp * qk[c] * rmax, f.fp * qk[c] * rmax));
+    } else {
+      if (qk[c] < 0) b.kk[c] = qk[c] * qk[c];
+      double qk2 = -qk[c];
+      WhitOut w = whit_l(eta[c], rmax, qk2, l);
+      double xc1 = rmax * w.wd / w.w;
+      b.bloch[c] = xc1 / rmax2;
+    }
+  }
+  b.nopen = (int)b.open_idx.size();
+  return HPRMAT_B200_OK;
+}
+
+// ------------------------------------------------------------------ public API helpers
+static int check_ctx(hprmat_b200_ctx* c) {
+  if (!c) return fail(HPRMAT_B200_ERR_ARG, "null context");
+  HPR_CUDA_TRY(cudaSetDevice(c->device));
+  return HPRMAT_B200_OK;
+}
+
+using Clock = std::chrono::steady_clock;
+static double ms_since(Clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+}
+
+static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const double* qk, const double* eta,
+                        double rmax, int nr, int ns, const double2* d_cpot, int ncp1, int ndim, double2* d_cu,
+                        int* nopen, hprmat_b200_stats* stats) {
+  auto t_all = Clock::now();
+  if (nch <= 0 || nr <= 0 || !lval || !qk || !eta || !d_cpot || !d_cu || !nopen)
+    return fail(HPRMAT_B200_ERR_ARG, "rmatrix: invalid arguments");
+  if (ns != 1) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "rmatrix: only ns = 1 (one interval) is supported");
+  if (ndim < nch || ncp1 < nr * ns) return fail(HPRMAT_B200_ERR_ARG, "rmatrix: ndim < nch or ncp1 < nr*ns");
+  if (c->nr != nr || c->ns != ns || c->rmax != rmax)
+    return fail(HPRMAT_B200_ERR_ARG, "rmatrix: call rmat_ini(nr=%d, ns=%d, rmax=%g) first", nr, ns, rmax);
+  const long Nl = (long)nch * nr;
+  if (Nl > 200000) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "rmatrix: N = %ld too large", Nl);
+  const int N = (int)Nl;
+  Boundary bnd;
+  TRY(boundary_values(nch, lval, qk, eta, rmax, rmax / ns, bnd));
+  *nopen = bnd.nopen;
+  // channel data: fac | kk | bloch | qk (doubles), then co | cop (double2), then open_idx
+  const size_t nd = 4 * (size_t)nch;
+  const size_t bytes = nd * sizeof(double) + 2 * (size_t)std::max(1, bnd.nopen) * sizeof(double2) +
+                       (size_t)std::max(1, bnd.nopen) * sizeof(int) + 64;
+  TRY(c->chan.ensure(bytes));
+  std::vector<unsigned char> h(bytes, 0);
+  double* hd = reinterpret_cast<double*>(h.data());
+  std::copy(bnd.fac.begin(), bnd.fac.end(), hd);
+  std::copy(bnd.kk.begin(), bnd.kk.end(), hd + nch);
+  std::copy(bnd.bloch.begin(), bnd.bloch.end(), hd + 2 * nch);
+  std::copy(bnd.qk.begin(), bnd.qk.end(), hd + 3 * nch);
+  double2* hz = reinterpret_cast<double2*>(hd + nd);
+  std::copy(bnd.co.begin(), bnd.co.end(), hz);
+  std::copy(bnd.cop.begin(), bnd.cop.end(), hz + std::max(1, bnd.nopen));
+  int* hi = reinterpret_cast<int*>(hz + 2 * std::max(1, bnd.nopen));
+  std::copy(bnd.open_idx.begin(), bnd.open_idx.end(), hi);
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->chan.p, h.data(), bytes, cudaMemcpyHostToDevice, c->stream));
+  const double* dd = c->chan.as<double>();
+  ChannelData chd{dd, dd + nch, dd + 2 * nch};
+  const double* d_qk = dd + 3 * nch;
+  const double2* d_co = reinterpret_cast<const double2*>(dd + nd);
+  const double2* d_cop = d_co + std::max(1, bnd.nopen);
+  const int* d_open = reinterpret_cast<const int*>(d_cop + std::max(1, bnd.nopen));
+
+  const MeshDev md = mesh_dev(c);
+  const long ld = (N + 3) / 4 * 4;
+  const bool mixed = c->opts.precision == HPRMAT_B200_PREC_MIXED;
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->n = N;
+    stats->nrhs = nch;
+    stats->rel_residual = -1.0;
+  }
+  TRY(c->X64.ensure((size_t)ld * nch * sizeof(double2)));
+  double2* X64 = c->X64.as<double2>();
+  Operator op;
+  op.structured = true;
+  op.mesh = md;
+  op.ch = chd;
+  op.nch = nch;
+  op.cpot = d_cpot;
+  op.ncp1 = ncp1;
+  op.ndim = ndim;
+  op.N = N;
+  // |B|_F of blockdiag(q2)
+  double q2n = 0.0;
+  for (int i = 0; i < nr; ++i) q2n += c->q2[i] * c->q2[i];
+  const double bnorm = sqrt(q2n * nch);
+  LUState st;
+  int status = HPRMAT_B200_OK;
+  dim3 ga(cdiv_u(N, 256), N);
+  dim3 gr(cdiv_u(N, 256), nch);
+  auto t0 = Clock::now();
+  if (!mixed) {
+    TRY(c->W.ensure((size_t)ld * N * sizeof(double2)));
+    double2* W = c->W.as<double2>();
+    assemble_kernel<double2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N);
+    LAUNCH_CHECK();
+    surface_rhs_kernel<double2><<<gr, 256, 0, c->stream>>>(md.q2, nr, nch, X64, ld, N, 1.0);
+    LAUNCH_CHECK();
+    int nb = pick_nb(c, N, sizeof(double2), 64);
+    if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
+    auto t1 = Clock::now();
+    TRY(factor<double2>(c, W, ld, N, false, nb, st));
+    if (stats) stats->ms_factor = ms_since(t1);
+    auto t2 = Clock::now();
+    TRY(lu_solve<double2>(c, W, st, X64, ld, nch));
+    TRY(c->R64.ensure((size_t)ld * nch * sizeof(double2)));
+    TRY(apply_residual(c, op, X64, ld, nch, c->R64.as<double2>(), ld, true));
+    double rn;
+    TRY(frob_norm(c, c->R64.as<double2>(), ld, N, nch, &rn));
+    if (stats) {
+      stats->rel_residual = rn / bnorm;
+      stats->residual_history[0] = rn / bnorm;
+      stats->ms_solve = ms_since(t2);
+    }
+  } else {
+    TRY(c->W.ensure((size_t)ld * N * sizeof(float2)));
+    float2* W = c->W.as<float2>();
+    assemble_kernel<float2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N);
+    LAUNCH_CHECK();
+    int nb = pick_nb(c, N, sizeof(float2), 128);
+    if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
+    auto t1 = Clock::now();
+    TRY(factor<float2>(c, W, ld, N, true, nb, st));
+    if (stats) stats->ms_factor = ms_since(t1);
+    auto t2 = Clock::now();
+    TRY(c->X.ensure((size_t)ld * nch * sizeof(float2)));
+    float2* X32 = c->X.as<float2>();
+    surface_rhs_kernel<float2><<<gr, 256, 0, c->stream>>>(md.q2, nr, nch, X32, ld, N, 1.0);
+    LAUNCH_CHECK();
+    TRY(lu_solve<float2>(c, W, st, X32, ld, nch));
+    f2d_kernel<<<gr, 256, 0, c->stream>>>(X32, ld, X64, ld, N, nullptr);
+    LAUNCH_CHECK();
+    if (stats) stats->ms_solve = ms_since(t2);
+    auto t3 = Clock::now();
+    status = refine_mixed(c, op, W, st, X64, ld, nch, bnorm, stats);
+    if (status != HPRMAT_B200_OK && status != HPRMAT_B200_NOT_CONVERGED) return status;
+    if (stats) stats->ms_refine = ms_since(t3);
+  }
+  if (stats) stats->nb = st.nb;
+  if (c->h_status[SW_INFO] != 0) {
+    if (stats) stats->info = c->h_status[SW_INFO];
+    return fail(HPRMAT_B200_SINGULAR, "C(E) is singular: zero pivot in column %d", c->h_status[SW_INFO]);
+  }
+  // R and U
+  auto t4 = Clock::now();
+  const int no = bnd.nopen;
+  TRY(c->rmat.ensure((size_t)nch * nch * sizeof(double2) + 64));
+  TRY(c->zwork.ensure((size_t)2 * std::max(1, no * no) * sizeof(double2) + 64));
+  double2* R = c->rmat.as<double2>();
+  rmat_extract_kernel<<<dim3(nch, cdiv_u(nch, 128)), 128, 0, c->stream>>>(X64, ld, md.q2, nr, nch, 1.0 / (rmax / ns), R);
+  LAUNCH_CHECK();
+  int* d_info = c->status.as<int>() + SW_INFO;
+  HPR_CUDA_TRY(cudaMemsetAsync(d_info, 0, sizeof(int), c->stream));
+  double2* zo = c->zwork.as<double2>();
+  umatrix_kernel<<<1, 1024, 0, c->stream>>>(R, nch, d_open, d_qk, d_co, d_cop, no, zo, zo + std::max(1, no * no), d_cu,
+                                            ndim, d_info);
+  LAUNCH_CHECK();
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->h_status, c->status.p, SW_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (c->h_status[SW_INFO] != 0) return fail(HPRMAT_B200_SINGULAR, "singular Z_O in the collision-matrix step");
+  if (stats) {
+    stats->ms_umatrix = ms_since(t4);
+    stats->ms_total = ms_since(t_all);
+    stats->status = status;
+  }
+  (void)t0;
+  return status;
+}
+
+// Dense solve A X = B with device operands (A read only, B overwritten with X).
+static int solve_dense_core(hprmat_b200_ctx* c, const double2* dA, double2* dB, int n, int nrhs,
+                            hprmat_b200_stats* stats) {
+  auto t_all = Clock::now();
+  if (n <= 0 || nrhs <= 0 || !dA || !dB) return fail(HPRMAT_B200_ERR_ARG, "solve_linear: invalid arguments");
+  const int N = n;
+  const long ld = (N + 3) / 4 * 4;
+  const bool mixed = c->opts.precision == HPRMAT_B200_PREC_MIXED;
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->n = N;
+    stats->nrhs = nrhs;
+    stats->rel_residual = -1.0;
+  }
+  LUState st;
+  int status = HPRMAT_B200_OK;
+  dim3 ga(cdiv_u(N, 256), N);
+  dim3 gr(cdiv_u(N, 256), nrhs);
+  if (!mixed) {
+    TRY(c->W.ensure((size_t)ld * N * sizeof(double2)));
+    double2* W = c->W.as<double2>();
+    HPR_CUDA_TRY(cudaMemcpy2DAsync(W, ld * sizeof(double2), dA, (size_t)N * sizeof(double2),
+                                   (size_t)N * sizeof(double2), N, cudaMemcpyDeviceToDevice, c->stream));
+    int nb = pick_nb(c, N, sizeof(double2), 64);
+    if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
+    auto t1 = Clock::now();
+    TRY(factor<double2>(c, W, ld, N, false, nb, st));
+    if (stats) stats->ms_factor = ms_since(t1);
+    if (c->h_status[SW_INFO] != 0) {
+      if (stats) stats->info = c->h_status[SW_INFO];
+      return fail(HPRMAT_B200_SINGULAR, "matrix is singular: zero pivot in column %d", c->h_status[SW_INFO]);
+    }
+    auto t2 = Clock::now();
+    TRY(c->X64.ensure((size_t)ld * nrhs * sizeof(double2)));
+    double2* X = c->X64.as<double2>();
+    copy_d_kernel<<<gr, 256, 0, c->stream>>>(dB, N, X, ld, N);
+    LAUNCH_CHECK();
+    TRY(lu_solve<double2>(c, W, st, X, ld, nrhs));
+    copy_d_kernel<<<gr, 256, 0, c->stream>>>(X, ld, dB, N, N);
+    LAUNCH_CHECK();
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (stats) stats->ms_solve = ms_since(t2);
+  } else {
+    TRY(c->W.ensure((size_t)ld * N * sizeof(float2)));
+    float2* W = c->W.as<float2>();
+    d2f_matrix_kernel<<<ga, 256, 0, c->stream>>>(dA, N, W, ld, N);
+    LAUNCH_CHECK();
+    int nb = pick_nb(c, N, sizeof(float2), 128);
+    if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
+    auto t1 = Clock::now();
+    TRY(factor<float2>(c, W, ld, N, true, nb, st));
+    if (stats) stats->ms_factor = ms_since(t1);
+    if (c->h_status[SW_INFO] != 0) {
+      if (stats) stats->info = c->h_status[SW_INFO];
+      return fail(HPRMAT_B200_SINGULAR, "matrix is singular: zero pivot in column %d", c->h_status[SW_INFO]);
+    }
+    auto t2 = Clock::now();
+    TRY(c->X.ensure((size_t)ld * nrhs * sizeof(float2)));
+    TRY(c->X64.ensure((size_t)ld * nrhs * sizeof(double2)));
+    float2* X32 = c->X.as<float2>();
+    double2* X64 = c->X64.as<double2>();
+    d2f_kernel<<<gr, 256, 0, c->stream>>>(dB, N, X32, ld, N, nullptr);
+    LAUNCH_CHECK();
+    TRY(lu_solve<float2>(c, W, st, X32, ld, nrhs));
+    f2d_kernel<<<gr, 256, 0, c->stream>>>(X32, ld, X64, ld, N, nullptr);
+    LAUNCH_CHECK();
+    if (stats) stats->ms_solve = ms_since(t2);
+    Operator op;
+    op.structured = false;
+    op.A = dA;
+    op.lda = N;
+    op.B = dB;
+    op.ldb = N;
+    op.N = N;
+    double bn;
+    TRY(frob_norm(c, dB, N, N, nrhs, &bn));
+    if (bn == 0.0) bn = 1.0;
+    auto t3 = Clock::now();
+    status = refine_mixed(c, op, W, st, X64, ld, nrhs, bn, stats);
+    if (status != HPRMAT_B200_OK && status != HPRMAT_B200_NOT_CONVERGED) return status;
+    copy_d_kernel<<<gr, 256, 0, c->stream>>>(X64, ld, dB, N, N);
+    LAUNCH_CHECK();
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (stats) stats->ms_refine = ms_since(t3);
+  }
+  if (stats) {
+    stats->nb = st.nb;
+    stats->ms_total = ms_since(t_all);
+    stats->status = status;
+  }
+  return status;
+}
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+void hprmat_b200_default_opts(hprmat_b200_opts* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->precision = HPRMAT_B200_PREC_MIXED;
+  o->max_refine = 3;
+  o->tol = 1.0e-13;
+  o->panel_nb = 0;
+}
+
+static int validate_opts(const hprmat_b200_opts* o) {
+  if (o->precision != HPRMAT_B200_PREC_FP64 && o->precision != HPRMAT_B200_PREC_MIXED)
+    return fail(HPRMAT_B200_ERR_ARG, "opts.precision must be 0 (FP64) or 1 (mixed)");
+  if (o->max_refine < 0 || o->max_refine > 8) return fail(HPRMAT_B200_ERR_ARG, "opts.max_refine must be in 0..8");
+  if (!(o->tol >= 0.0)) return fail(HPRMAT_B200_ERR_ARG, "opts.tol must be >= 0");
+  if (o->panel_nb != 0 && o->panel_nb != 16 && o->panel_nb != 32 && o->panel_nb != 64 && o->panel_nb != 128)
+    return fail(HPRMAT_B200_ERR_ARG, "opts.panel_nb must be 0, 16, 32, 64 or 128");
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_create(int device, const hprmat_b200_opts* opts, hprmat_b200_ctx** out) {
+  if (!out) return fail(HPRMAT_B200_ERR_ARG, "null output pointer");
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(HPRMAT_B200_ERR_NODEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+  }
+  if (device < 0 || device >= ndev) return fail(HPRMAT_B200_ERR_ARG, "device %d out of range", device);
+  cudaDeviceProp prop;
+  HPR_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10)
+    return fail(HPRMAT_B200_ERR_NODEVICE, "device %d is sm_%d%d; this library is built for sm_100a", device,
+                prop.major, prop.minor);
+  hprmat_b200_opts o;
+  hprmat_b200_default_opts(&o);
+  if (opts) o = *opts;
+  TRY(validate_opts(&o));
+  auto* c = new hprmat_b200_ctx();
+  c->device = device;
+  c->opts = o;
+  c->nsm = prop.multiProcessorCount;
+  c->smem_optin = (int)prop.sharedMemPerBlockOptin;
+  HPR_CUDA_TRY(cudaSetDevice(device));
+  HPR_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  c->own_stream = true;
+  HPR_CUDA_TRY(cudaMallocHost(&c->h_status, 64 * sizeof(int)));
+  HPR_CUDA_TRY(cudaMallocHost(&c->h_norms, 4096 * sizeof(double)));
+  int s = c->status.ensure(64 * sizeof(int));
+  if (s != HPRMAT_B200_OK) {
+    delete c;
+    return s;
+  }
+  HPR_CUDA_TRY(cudaMemset(c->status.p, 0, 64 * sizeof(int)));
+  s = tc_gemm_init(c->tcplan, device);
+  if (s != HPRMAT_B200_OK) {
+    delete c;
+    return s;
+  }
+  *out = c;
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_destroy(hprmat_b200_ctx* c) {
+  if (!c) return HPRMAT_B200_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  DevBuf* bufs[] = {&c->mesh, &c->W, &c->A64, &c->X, &c->X64, &c->R64, &c->B64, &c->V, &c->Z, &c->gm,
+                    &c->swaps, &c->ipiv, &c->stage, &c->status, &c->ops, &c->inv, &c->chan, &c->rmat,
+                    &c->zwork, &c->cpot, &c->cu, &c->norms};
+  for (DevBuf* b : bufs) b->release();
+  if (c->h_status) cudaFreeHost(c->h_status);
+  if (c->h_norms) cudaFreeHost(c->h_norms);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_set_opts(hprmat_b200_ctx* c, const hprmat_b200_opts* o) {
+  if (!c || !o) return fail(HPRMAT_B200_ERR_ARG, "null argument");
+  TRY(validate_opts(o));
+  c->opts = *o;
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_set_stream(hprmat_b200_ctx* c, void* stream) {
+  TRY(check_ctx(c));
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  if (stream) {
+    c->stream = (cudaStream_t)stream;
+    c->own_stream = false;
+  } else {
+    HPR_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->own_stream = true;
+  }
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_rmat_ini(hprmat_b200_ctx* c, int nr, int ns, double rmax, double* zrma) {
+  TRY(check_ctx(c));
+  if (nr < 2 || ns < 1 || !(rmax > 0)) return fail(HPRMAT_B200_ERR_ARG, "rmat_ini: need nr >= 2, ns >= 1, rmax > 0");
+  build_mesh(c, nr, ns, rmax);
+  TRY(upload_mesh(c));
+  if (zrma) std::copy(c->zrma.begin(), c->zrma.end(), zrma);
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_rmatrix_device(hprmat_b200_ctx* c, int nch, const int* lval, const double* qk, const double* eta,
+                               double rmax, int nr, int ns, const void* d_cpot, int ncp1, int ndim, void* d_cu,
+                               int* nopen, hprmat_b200_stats* stats) {
+  TRY(check_ctx(c));
+  int s = rmatrix_core(c, nch, lval, qk, eta, rmax, nr, ns, (const double2*)d_cpot, ncp1, ndim, (double2*)d_cu, nopen,
+                       stats);
+  if (stats) stats->status = s;
+  return s;
+}
+
+int hprmat_b200_rmatrix(hprmat_b200_ctx* c, int nch, const int* lval, const double* qk, const double* eta,
+                        double rmax, int nr, int ns, const double* cpot, int ncp1, int ndim, double* cu, int* nopen,
+                        hprmat_b200_stats* stats) {
+  TRY(check_ctx(c));
+  if (!cpot || !cu || ndim <= 0 || ncp1 <= 0) return fail(HPRMAT_B200_ERR_ARG, "rmatrix: invalid arguments");
+  const size_t pbytes = (size_t)ncp1 * ndim * ndim * sizeof(double2);
+  const size_t ubytes = (size_t)ndim * ndim * sizeof(double2);
+  TRY(c->cpot.ensure(pbytes));
+  TRY(c->cu.ensure(ubytes));
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->cpot.p, cpot, pbytes, cudaMemcpyHostToDevice, c->stream));
+  int s = rmatrix_core(c, nch, lval, qk, eta, rmax, nr, ns, c->cpot.as<double2>(), ncp1, ndim, c->cu.as<double2>(),
+                       nopen, stats);
+  if (s == HPRMAT_B200_OK || s == HPRMAT_B200_NOT_CONVERGED) {
+    HPR_CUDA_TRY(cudaMemcpyAsync(cu, c->cu.p, ubytes, cudaMemcpyDeviceToHost, c->stream));
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
+  if (stats) stats->status = s;
+  return s;
+}
+
+int hprmat_b200_solve_linear_device(hprmat_b200_ctx* c, const void* d_A, void* d_B, int n, int nrhs,
+                                    hprmat_b200_stats* stats) {
+  TRY(check_ctx(c));
+  int s = solve_dense_core(c, (const double2*)d_A, (double2*)d_B, n, nrhs, stats);
+  if (stats) stats->status = s;
+  return s;
+}
+
+int hprmat_b200_solve_linear(hprmat_b200_ctx* c, const double* A, double* B, int n, int nrhs,
+                             hprmat_b200_stats* stats) {
+  TRY(check_ctx(c));
+  if (!A || !B || n <= 0 || nrhs <= 0) return fail(HPRMAT_B200_ERR_ARG, "solve_linear: invalid arguments");
+  const size_t abytes = (size_t)n * n * sizeof(double2);
+  const size_t bbytes = (size_t)n * nrhs * sizeof(double2);
+  TRY(c->A64.ensure(abytes));
+  TRY(c->B64.ensure(bbytes));
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->A64.p, A, abytes, cudaMemcpyHostToDevice, c->stream));
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->B64.p, B, bbytes, cudaMemcpyHostToDevice, c->stream));
+  int s = solve_dense_core(c, c->A64.as<double2>(), c->B64.as<double2>(), n, nrhs, stats);
+  if (s == HPRMAT_B200_OK || s == HPRMAT_B200_NOT_CONVERGED) {
+    HPR_CUDA_TRY(cudaMemcpyAsync(B, c->B64.p, bbytes, cudaMemcpyDeviceToHost, c->stream));
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
+  if (stats) stats->status = s;
+  return s;
+}
+
+int hprmat_b200_solve_rmatrix(hprmat_b200_ctx* c, const double* cmat, const double* bvec, int nch, int nlag,
+                              double normfac, double* rmat, hprmat_b200_stats* stats) {
+  TRY(check_ctx(c));
+  if (!cmat || !bvec || !rmat || nch <= 0 || nlag <= 0) return fail(HPRMAT_B200_ERR_ARG, "solve_rmatrix: invalid arguments");
+  const int N = nch * nlag;
+  std::vector<double> X((size_t)2 * N * nch, 0.0);
+  for (int ich = 0; ich < nch; ++ich)
+    for (int r = 0; r < nlag; ++r) {
+      size_t idx = (size_t)(ich * nlag + r) + (size_t)ich * N;
+      X[2 * idx] = bvec[2 * r];
+      X[2 * idx + 1] = bvec[2 * r + 1];
+    }
+  int s = hprmat_b200_solve_linear(c, cmat, X.data(), N, nch, stats);
+  if (s != HPRMAT_B200_OK && s != HPRMAT_B200_NOT_CONVERGED) return s;
+  // Rmat(ich, ichp) = normfac * sum_r B(r) X(r + (ich-1) nlag, ichp): complex products
+  for (int jp = 0; jp < nch; ++jp)
+    for (int i = 0; i < nch; ++i) {
+      double ar = 0.0, ai = 0.0;
+      for (int r = 0; r < nlag; ++r) {
+        size_t idx = (size_t)(i * nlag + r) + (size_t)jp * N;
+        double br = bvec[2 * r], bi = bvec[2 * r + 1];
+        double xr = X[2 * idx], xi = X[2 * idx + 1];
+        ar += br * xr - bi * xi;
+        ai += br * xi + bi * xr;
+      }
+      rmat[2 * (i + (size_t)jp * nch)] = ar * normfac;
+      rmat[2 * (i + (size_t)jp * nch) + 1] = ai * normfac;
+    }
+  return s;
+}
+
+// ---- Fortran-convention drop-ins on a lazily created device-0 context
+static std::mutex g_default_mu;
+static hprmat_b200_ctx* g_default = nullptr;
+
+static int default_ctx(hprmat_b200_ctx** out) {
+  if (!g_default) TRY(hprmat_b200_create(0, nullptr, &g_default));
+  *out = g_default;
+  return HPRMAT_B200_OK;
+}
+
+static int fortran_info(int s, const hprmat_b200_stats& st) {
+  switch (s) {
+    case HPRMAT_B200_OK: return 0;
+    case HPRMAT_B200_SINGULAR: return st.info > 0 ? st.info : 1;
+    case HPRMAT_B200_NOT_CONVERGED: return 99;
+    case HPRMAT_B200_ERR_OOM: return -2;
+    case HPRMAT_B200_ERR_NODEVICE: return -1;
+    default: return -1;
+  }
+}
+
+int gpu_b200_solve_mixed_(double* A, double* B, int* n, int* nrhs, int* max_refine, double* tol, int* info) {
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  hprmat_b200_ctx* c = nullptr;
+  int s = default_ctx(&c);
+  hprmat_b200_stats st{};
+  if (s == HPRMAT_B200_OK) {
+    hprmat_b200_opts o = c->opts;
+    o.precision = HPRMAT_B200_PREC_MIXED;
+    o.max_refine = max_refine ? std::max(0, std::min(8, *max_refine)) : 3;
+    o.tol = (tol && *tol > 0) ? *tol : 1.0e-13;
+    s = hprmat_b200_set_opts(c, &o);
+    if (s == HPRMAT_B200_OK) s = hprmat_b200_solve_linear(c, A, B, *n, *nrhs, &st);
+  }
+  if (info) *info = fortran_info(s, st);
+  return (s == HPRMAT_B200_OK) ? 0 : -1;
+}
+
+int gpu_b200_solve_double_(double* A, double* B, int* n, int* nrhs, int* info) {
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  hprmat_b200_ctx* c = nullptr;
+  int s = default_ctx(&c);
+  hprmat_b200_stats st{};
+  if (s == HPRMAT_B200_OK) {
+    hprmat_b200_opts o = c->opts;
+    o.precision = HPRMAT_B200_PREC_FP64;
+    s = hprmat_b200_set_opts(c, &o);
+    if (s == HPRMAT_B200_OK) s = hprmat_b200_solve_linear(c, A, B, *n, *nrhs, &st);
+  }
+  if (info) *info = fortran_info(s, st);
+  return (s == HPRMAT_B200_OK) ? 0 : -1;
+}
+
+int gpu_b200_finalize_(void) {
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  int s = hprmat_b200_destroy(g_default);
+  g_default = nullptr;
+  return s;
+}
+
+// ---- kernel-level hooks (include/hprmat_b200_dev.h)
+__global__ void split_planes_kernel(const float2* __restrict__ src, int rows, int nb, float* dst, long plane) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)rows * nb) return;
+  float2 v = src[idx];
+  float hr, lr, hi, li;
+  tf32_split(v.x, hr, lr);
+  tf32_split(v.y, hi, li);
+  dst[idx] = hr;
+  dst[plane + idx] = lr;
+  dst[2 * plane + idx] = hi;
+  dst[3 * plane + idx] = li;
+}
+
+int hprmat_b200_dev_split_planes(hprmat_b200_ctx* c, const void* src, int rows, int nb, float* dst, long plane) {
+  TRY(check_ctx(c));
+  if (!src || !dst || rows <= 0 || nb <= 0 || plane < (long)rows * nb) return fail(HPRMAT_B200_ERR_ARG, "split_planes: invalid arguments");
+  long n = (long)rows * nb;
+  split_planes_kernel<<<cdiv_u(n, 256), 256, 0, c->stream>>>((const float2*)src, rows, nb, dst, plane);
+  LAUNCH_CHECK();
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_dev_tc_update(hprmat_b200_ctx* c, const float* aop, const float* bop, long plane, int nb, void* C,
+                              long ldc, int M, int Nc) {
+  TRY(check_ctx(c));
+  if (!aop || !bop || !C || M < 0 || Nc < 0 || ldc < M || (nb != 16 && nb != 32 && nb != 64 && nb != 128) ||
+      plane < (long)std::max(M, Nc) * nb || ((uintptr_t)aop & 15) || ((uintptr_t)bop & 15) || (plane % 4))
+    return fail(HPRMAT_B200_ERR_ARG, "dev_tc_update: invalid arguments");
+  TRY(tc_trailing_update(c->tcplan, aop, bop, plane, nb, nb, (float2*)C, ldc, M, Nc, c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  int err = 0;
+  TRY(tc_gemm_check(c->tcplan, c->stream, &err));
+  if (err) return fail(HPRMAT_B200_ERR_TIMEOUT, "tensor-core update: wait limit exceeded at site %d", err);
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_boundary(int nch, const int* lval, const double* qk, const double* eta, double rmax, double* co,
+                         double* cop, double* xc1, double* xc2, int* nopen) {
+  if (nch <= 0 || !lval || !qk || !eta || !(rmax > 0)) return fail(HPRMAT_B200_ERR_ARG, "boundary: invalid arguments");
+  int no = 0;
+  for (int c = 0; c < nch; ++c) {
+    if (co) co[2 * c] = co[2 * c + 1] = 0.0;
+    if (cop) cop[2 * c] = cop[2 * c + 1] = 0.0;
+    if (xc1) xc1[c] = 0.0;
+    if (xc2) xc2[c] = 0.0;
+    if (lval[c] < 0) return fail(HPRMAT_B200_ERR_ARG, "lval(%d) < 0", c + 1);
+    if (qk[c] > 0) {
+      CoulombFG f = coulfg_single(qk[c] * rmax, eta[c], (double)lval[c]);
+      if (f.ifail != 0) return fail(HPRMAT_B200_ERR_ARG, "COULFG failed (ifail=%d) for channel %d", f.ifail, c + 1);
+      if (co) { co[2 * c] = f.g; co[2 * c + 1] = f.f; }
+      if (cop) { cop[2 * c] = f.gp * qk[c] * rmax; cop[2 * c + 1] = f.fp * qk[c] * rmax; }
+      ++no;
+    } else {
+      WhitOut w = whit_l(eta[c], rmax, -qk[c], lval[c]);
+      if (xc1) xc1[c] = rmax * w.wd / w.w;
+      if (xc2) xc2[c] = w.w;
+    }
+  }
+  if (nopen) *nopen = no;
+  return HPRMAT_B200_OK;
+}
+
+const char* hprmat_b200_status_string(int s) {
+  switch (s) {
+    case HPRMAT_B200_OK: return "ok";
+    case HPRMAT_B200_ERR_ARG: return "invalid argument";
+    case HPRMAT_B200_ERR_CUDA: return "CUDA error";
+    case HPRMAT_B200_ERR_OOM: return "device out of memory";
+    case HPRMAT_B200_ERR_TIMEOUT: return "device wait limit exceeded";
+    case HPRMAT_B200_ERR_UNSUPPORTED: return "unsupported input";
+    case HPRMAT_B200_ERR_NODEVICE: return "no usable sm_100 device";
+    case HPRMAT_B200_SINGULAR: return "singular matrix";
+    case HPRMAT_B200_NOT_CONVERGED: return "refinement did not converge";
+  }
+  return "unknown status";
+}
+
+const char* hprmat_b200_last_error(void) { return g_last_error.c_str(); }
+
+int hprmat_b200_version(void) { return 100; }
+
+}  // extern "C"

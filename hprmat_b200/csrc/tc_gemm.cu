@@ -1,0 +1,396 @@
+// Complex trailing update of the mixed-precision LU on sm_100a tensor cores.
+//
+//   C[M x Nc] -= A[M x K] * B[K x Nc]       (complex, C interleaved float2, column-major)
+//
+// Each complex product is formed as 4 real products (4M), and each real product X*Y as
+// the 3-term TF32 split hi(X)hi(Y) + hi(X)lo(Y) + lo(X)hi(Y) (3xTF32), so the bulk of the
+// LU runs on tcgen05 kind::tf32 with FP32 accumulation at close to FP32 accuracy:
+//   Re += Ar*Br - Ai*Bi,   Im += Ar*Bi + Ai*Br      -> 12 MMAs per K-step of 8.
+// The minus sign comes from the A-negate bit of the instruction descriptor.
+//
+// Tile 128 (rows) x 256 (columns); Re and Im accumulate in TMEM columns [0,256) and
+// [256,512) of a 512-column allocation.  One persistent CTA per SM, 6 warps:
+//   warp 0     TMA producer: per K-chunk of 16 one 3-D box for the 4 A planes
+//              (16 x 128 x 4 floats) and one for the 4 B planes (16 x 256 x 4), 64-byte
+//              swizzle, into a 2-stage ring; also prefetches the next C tile into L2;
+//   warp 1     TMEM allocator and single-thread MMA issuer;
+//   warps 2-5  epilogue: tcgen05.ld of Re/Im, C -= acc, coalesced along rows.
+// Every mbarrier wait is bounded; on expiry the kernel records the site in *err, stops
+// issuing work, waits (bounded) for its own TMA copies and frees its TMEM.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+#include "tc_gemm.cuh"
+
+namespace hprmat {
+
+namespace {
+
+constexpr int kBM = 128;
+constexpr int kBN = 256;
+constexpr int kKC = 16;                                 // K values per stage (64 bytes)
+constexpr int kStages = 2;
+constexpr int kABytes = 4 * kBM * kKC * 4;             // 32 KB
+constexpr int kBBytes = 4 * kBN * kKC * 4;             // 64 KB
+constexpr int kStageBytes = kABytes + kBBytes;          // 96 KB
+constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*barriers*/ + 1024 /*align*/;
+constexpr int kThreads = 192;
+constexpr unsigned kWaitLimit = 1u << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: false if the limit was reached or another role already gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err,
+                                          int site) {
+  for (unsigned it = 0; it < kWaitLimit; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 1023u) == 1023u && *abort_flag) return false;
+  }
+  *abort_flag = 1;
+  atomicCAS(err, 0, site);
+  return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Shared-memory matrix descriptor, K-major, 64-byte swizzle: rows of 64 bytes, 8-row
+// groups 512 bytes apart (stride byte offset), leading byte offset unused (1), version 1.
+__device__ __forceinline__ uint64_t sdesc_k_sw64(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)1 << 16;                 // LBO (ignored for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;        // SBO
+  d |= (uint64_t)1 << 46;                 // descriptor version (sm_100)
+  d |= (uint64_t)4 << 61;                 // SWIZZLE_64B
+  return d;
+}
+
+// Instruction descriptor: kind::tf32, D = F32, A = B = TF32, both K-major, M = 128, N = 256.
+__host__ __device__ constexpr uint32_t idesc_tf32(bool neg_a) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(kBN >> 3) << 17) |
+         ((uint32_t)(kBM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+template <int NB>
+__global__ void __launch_bounds__(kThreads, 1)
+    tc_update_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, float2* C,
+                     long ldc, int M, int Nc, int* err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
+  uint64_t* empty = full + kStages;
+  uint64_t* acc_full = empty + kStages;
+  uint64_t* acc_empty = acc_full + 1;
+  uint64_t* drain = acc_empty + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int mt = (M + kBM - 1) / kBM;
+  const int nt = (Nc + kBN - 1) / kBN;
+  const int ntiles = mt * nt;
+  constexpr int kChunks = NB / kKC;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, 128);
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0;
+      int inflight = 0;  // stages issued whose completion this thread has not observed
+      bool ok = true;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        const int m0 = (t % mt) * kBM;
+        const int n0 = (t / mt) * kBN;
+        // warm L2 with this tile of C for the epilogue
+        const int rows = min(kBM, M - m0);
+        const uint32_t cbytes = (uint32_t)((rows * 8) & ~15);
+        if (cbytes > 0) {
+          for (int c = 0; c < kBN && n0 + c < Nc; ++c) {
+            const float2* pc = C + m0 + (size_t)(n0 + c) * ldc;
+            if ((reinterpret_cast<uintptr_t>(pc) & 15u) == 0) prefetch_l2(pc, cbytes);
+          }
+        }
+        for (int kc = 0; kc < kChunks; ++kc) {
+          if (!mbar_wait(&empty[stage], phase ^ 1u, abort_flag, err, 11)) { ok = false; break; }
+          unsigned char* sa = smem + stage * kStageBytes;
+          mbar_expect_tx(&full[stage], kStageBytes);
+          tma_load_3d(sa, &tmA, &full[stage], kc * kKC, m0, 0);
+          tma_load_3d(sa + kABytes, &tmB, &full[stage], kc * kKC, n0, 0);
+          inflight = min(inflight + 1, kStages);
+          if (++stage == kStages) { stage = 0; phase ^= 1u; }
+        }
+      }
+      if (!ok) {
+        // let our own copies land before the CTA can exit: wait (bounded) on the fill
+        // barriers of the stages issued last
+        int s = stage, ph = phase;
+        for (int i = 0; i < inflight; ++i) {
+          if (--s < 0) { s = kStages - 1; ph ^= 1; }
+          for (unsigned it = 0; it < kWaitLimit && !mbar_try_wait(&full[s], ph); ++it) {}
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int stage = 0;
+      uint32_t phase = 0, acc_phase = 0;
+      bool ok = true;
+      const uint32_t id_pos = idesc_tf32(false), id_neg = idesc_tf32(true);
+      const uint32_t t_re = tmem, t_im = tmem + kBN;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        if (!mbar_wait(acc_empty, acc_phase ^ 1u, abort_flag, err, 21)) break;
+        tc_fence_after();
+        for (int kc = 0; kc < kChunks; ++kc) {
+          if (!mbar_wait(&full[stage], phase, abort_flag, err, 22)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t sa = smem_u32(smem + stage * kStageBytes);
+          const uint32_t sb = sa + kABytes;
+#pragma unroll
+          for (int kk = 0; kk < kKC / 8; ++kk) {
+            const uint32_t off = kk * 32;
+            const uint64_t a_rh = sdesc_k_sw64(sa + 0 * (kBM * 64) + off);
+            const uint64_t a_rl = sdesc_k_sw64(sa + 1 * (kBM * 64) + off);
+            const uint64_t a_ih = sdesc_k_sw64(sa + 2 * (kBM * 64) + off);
+            const uint64_t a_il = sdesc_k_sw64(sa + 3 * (kBM * 64) + off);
+            const uint64_t b_rh = sdesc_k_sw64(sb + 0 * (kBN * 64) + off);
+            const uint64_t b_rl = sdesc_k_sw64(sb + 1 * (kBN * 64) + off);
+            const uint64_t b_ih = sdesc_k_sw64(sb + 2 * (kBN * 64) + off);
+            const uint64_t b_il = sdesc_k_sw64(sb + 3 * (kBN * 64) + off);
+            const uint32_t first = (kc == 0 && kk == 0) ? 0u : 1u;
+            // small terms first, then the hi*hi product
+            mma_tf32(t_re, a_rh, b_rl, id_pos, first);
+            mma_tf32(t_re, a_rl, b_rh, id_pos, 1u);
+            mma_tf32(t_re, a_ih, b_il, id_neg, 1u);
+            mma_tf32(t_re, a_il, b_ih, id_neg, 1u);
+            mma_tf32(t_re, a_rh, b_rh, id_pos, 1u);
+            mma_tf32(t_re, a_ih, b_ih, id_neg, 1u);
+            mma_tf32(t_im, a_rh, b_il, id_pos, first);
+            mma_tf32(t_im, a_rl, b_ih, id_pos, 1u);
+            mma_tf32(t_im, a_ih, b_rl, id_pos, 1u);
+            mma_tf32(t_im, a_il, b_rh, id_pos, 1u);
+            mma_tf32(t_im, a_rh, b_ih, id_pos, 1u);
+            mma_tf32(t_im, a_ih, b_rh, id_pos, 1u);
+          }
+          mma_commit(&empty[stage]);
+          if (++stage == kStages) { stage = 0; phase ^= 1u; }
+        }
+        if (!ok) break;
+        mma_commit(acc_full);
+        acc_phase ^= 1u;
+      }
+      if (!ok || *abort_flag) {
+        // make sure no MMA of ours is still reading shared memory or writing TMEM
+        mma_commit(drain);
+        for (unsigned it = 0; it < kWaitLimit && !mbar_try_wait(drain, 0); ++it) {}
+      }
+    }
+  } else {
+    // epilogue warps 2..5: TMEM lane quarter q = warp % 4
+    const int q = warp & 3;
+    uint32_t acc_phase = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      const int m0 = (t % mt) * kBM;
+      const int n0 = (t / mt) * kBN;
+      bool ok = true;
+      if (lane == 0) ok = mbar_wait(acc_full, acc_phase, abort_flag, err, 31);
+      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+      if (!ok) break;
+      __syncwarp();
+      tc_fence_after();
+      const int row = m0 + q * 32 + lane;
+      const bool rv = row < M;
+      const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16);
+      for (int c0 = 0; c0 < kBN; c0 += 16) {
+        if (n0 + c0 >= Nc) break;  // warp-uniform
+        float2 cv[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = n0 + c0 + j;
+          cv[j] = (rv && col < Nc) ? C[row + (size_t)col * ldc] : make_float2(0.f, 0.f);
+        }
+        float re[16], im[16];
+        tmem_ld16(tl + c0, re);
+        tmem_ld16(tl + kBN + c0, im);
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = n0 + c0 + j;
+          if (rv && col < Nc) C[row + (size_t)col * ldc] = make_float2(cv[j].x - re[j], cv[j].y - im[j]);
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(acc_empty);
+      acc_phase ^= 1u;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+  }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int make_map(EncodeTiledFn enc, CUtensorMap* map, const float* base, int NB, long rows, long plane, int box_rows) {
+  cuuint64_t dims[3] = {(cuuint64_t)NB, (cuuint64_t)rows, 4};
+  cuuint64_t strides[2] = {(cuuint64_t)NB * 4, (cuuint64_t)plane * 4};
+  cuuint32_t box[3] = {(cuuint32_t)kKC, (cuuint32_t)box_rows, 4};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_last_error_msg("cuTensorMapEncodeTiled failed for a tensor-core operand");
+    return -2;
+  }
+  return 0;
+}
+
+}  // namespace
+
+int tc_gemm_init(TcGemmPlan& p, int device) {
+  p.device = device;
+  int nsm = 0;
+  HPR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  p.nsm = nsm;
+  cudaDriverEntryPointQueryResult q;
+  void* fn = nullptr;
+  HPR_CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+  if (q != cudaDriverEntryPointSuccess || fn == nullptr) {
+    set_last_error_msg("cuTensorMapEncodeTiled is not available from the driver");
+    return -2;
+  }
+  p.encode = fn;
+  if (!p.d_err) {
+    HPR_CUDA_TRY(cudaMalloc(&p.d_err, sizeof(int)));
+    HPR_CUDA_TRY(cudaMemset(p.d_err, 0, sizeof(int)));
+  }
+  HPR_CUDA_TRY(cudaFuncSetAttribute(tc_update_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+  HPR_CUDA_TRY(cudaFuncSetAttribute(tc_update_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+  HPR_CUDA_TRY(cudaFuncSetAttribute(tc_update_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+  HPR_CUDA_TRY(cudaFuncSetAttribute(tc_update_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+  return 0;
+}
+
+int tc_trailing_update(TcGemmPlan& p, const float* aop, const float* bop, long plane, int NB, int K, float2* C,
+                       long ldc, int M, int Nc, cudaStream_t s) {
+  (void)K;
+  if (M <= 0 || Nc <= 0) return 0;
+  EncodeTiledFn enc = reinterpret_cast<EncodeTiledFn>(p.encode);
+  CUtensorMap ma, mb;
+  if (make_map(enc, &ma, aop, NB, M, plane, kBM)) return -2;
+  if (make_map(enc, &mb, bop, NB, Nc, plane, kBN)) return -2;
+  const int ntiles = ((M + kBM - 1) / kBM) * ((Nc + kBN - 1) / kBN);
+  const int grid = ntiles < p.nsm ? ntiles : p.nsm;
+  switch (NB) {
+    case 128: tc_update_kernel<128><<<grid, kThreads, kSmemBytes, s>>>(ma, mb, C, ldc, M, Nc, p.d_err); break;
+    case 64: tc_update_kernel<64><<<grid, kThreads, kSmemBytes, s>>>(ma, mb, C, ldc, M, Nc, p.d_err); break;
+    case 32: tc_update_kernel<32><<<grid, kThreads, kSmemBytes, s>>>(ma, mb, C, ldc, M, Nc, p.d_err); break;
+    case 16: tc_update_kernel<16><<<grid, kThreads, kSmemBytes, s>>>(ma, mb, C, ldc, M, Nc, p.d_err); break;
+    default: set_last_error_msg("tensor-core update: unsupported block size"); return -5;
+  }
+  HPR_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int tc_gemm_check(TcGemmPlan& p, cudaStream_t s, int* err_out) {
+  int h = 0;
+  HPR_CUDA_TRY(cudaMemcpyAsync(&h, p.d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  HPR_CUDA_TRY(cudaStreamSynchronize(s));
+  if (h) HPR_CUDA_TRY(cudaMemsetAsync(p.d_err, 0, sizeof(int), s));
+  *err_out = h;
+  return 0;
+}
+
+}  // namespace hprmat

@@ -1,0 +1,148 @@
+/*
+ * hprmat_b200.h -- C ABI of the B200 (sm_100a) dense complex R-matrix solver.
+ *
+ * The library is a new solver type behind HPRMAT's `rmatrix` entry and its `solver_type`
+ * dispatch.  Every entry point takes plain pointers and sizes.  Complex arrays are
+ * interleaved (re, im) double pairs in Fortran column-major order, i.e. the memory of
+ * `complex*16` / `complex(c_double_complex)` arrays, passed as `double*`.
+ *
+ * Reference interfaces (paths relative to the HPRMAT project root) that each entry point
+ * replaces are cited next to it.  Errors are reported by the integer return value (see
+ * HPRMAT_B200_* below).  Nothing falls back to a CPU solver: a missing or failing GPU is an
+ * error.
+ *
+ * Threading: one context per host thread; calls on one context are ordered on the
+ * context's CUDA stream and return after their results are complete.
+ */
+#ifndef HPRMAT_B200_H
+#define HPRMAT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (return values). */
+#define HPRMAT_B200_OK               0
+#define HPRMAT_B200_ERR_ARG         -1   /* invalid argument (sizes, null pointers) */
+#define HPRMAT_B200_ERR_CUDA        -2   /* CUDA runtime error (message: hprmat_b200_last_error) */
+#define HPRMAT_B200_ERR_OOM         -3   /* device allocation failed */
+#define HPRMAT_B200_ERR_TIMEOUT     -4   /* a bounded device-side wait gave up */
+#define HPRMAT_B200_ERR_UNSUPPORTED -5   /* input outside what this build handles */
+#define HPRMAT_B200_ERR_NODEVICE    -6   /* no usable sm_100 device */
+#define HPRMAT_B200_SINGULAR         1   /* exactly zero pivot; stats.info = its 1-based column */
+#define HPRMAT_B200_NOT_CONVERGED   99   /* refinement stopped above tol (as info=99 in
+                                            src/cusolver_interface.cu:1577-1589) */
+
+/* Arithmetic of the LU factorisation. */
+#define HPRMAT_B200_PREC_FP64   0  /* plain FP64 complex LU (the "plain FP64 device LU") */
+#define HPRMAT_B200_PREC_MIXED  1  /* complex LU with 3xTF32 tcgen05 trailing updates, FP32
+                                      panels, FP64 residual refinement */
+
+/* solver_type id of this backend in HPRMAT's dispatch (next free id after 1..6,
+   src/rmatrix_hp.F90:299-322, src/rmat_solvers.F90:69-88). */
+#define HPRMAT_SOLVER_B200      7
+
+typedef struct hprmat_b200_ctx hprmat_b200_ctx;
+
+typedef struct {
+  int precision;   /* HPRMAT_B200_PREC_* (default MIXED) */
+  int max_refine;  /* FP64 refinement steps, 0..8 (default 3) */
+  double tol;      /* stop when ||B - C X||_F / ||B||_F < tol (default 1e-13); the same
+                      relative Frobenius rule as src/rmat_solvers.F90:253-262 */
+  int panel_nb;    /* LU block size; 0 = automatic */
+  int reserved[4];
+} hprmat_b200_opts;
+
+typedef struct {
+  int status;               /* return value of the call */
+  int info;                 /* LAPACK-style info: >0 = first zero pivot (1-based) */
+  int refine_steps;         /* refinement corrections applied */
+  int nb;                   /* LU block size used */
+  int n;                    /* order of the solved system */
+  int nrhs;
+  double rel_residual;      /* final ||B - C X||_F / ||B||_F, evaluated in FP64 */
+  double residual_history[9];
+  double ms_assemble, ms_factor, ms_solve, ms_refine, ms_umatrix, ms_total;
+} hprmat_b200_stats;
+
+/* Defaults for hprmat_b200_opts. */
+void hprmat_b200_default_opts(hprmat_b200_opts* opts);
+
+/* Create a context on CUDA device `device` (the reference auto-initialises device 0 in
+   gpu_solver_init_, src/cusolver_interface.cu:193-220).  opts may be NULL. */
+int hprmat_b200_create(int device, const hprmat_b200_opts* opts, hprmat_b200_ctx** out);
+/* Release every device buffer of the context (gpu_solver_finalize_,
+   src/cusolver_interface.cu:222-258). */
+int hprmat_b200_destroy(hprmat_b200_ctx* ctx);
+int hprmat_b200_set_opts(hprmat_b200_ctx* ctx, const hprmat_b200_opts* opts);
+/* Order the context's work on an existing cudaStream_t (passed as void*); NULL = the
+   context's own stream. */
+int hprmat_b200_set_stream(hprmat_b200_ctx* ctx, void* stream);
+
+/* Lagrange-Legendre mesh, kinetic and Bloch matrices: rmat_ini(nr, ns, rmax, zrma),
+   src/rmatrix_hp.F90:61-159.  zrma (nr*ns doubles) may be NULL. */
+int hprmat_b200_rmat_ini(hprmat_b200_ctx* ctx, int nr, int ns, double rmax, double* zrma);
+
+/* Collision matrix for one (J, pi, E): rmatrix(nch, lval, qk, eta, rmax, nr, ns, cpot, cu,
+   ncp1, ndim, nopen, ...) of src/rmatrix_hp.F90:175-368, for local potentials (ncp2 = 0) and
+   one interval (ns = 1).  Host buffers: cpot is complex (ncp1, ndim, ndim), cu is complex
+   (ndim, ndim) and receives U in cu(1:nopen, 1:nopen); the rest of cu is zeroed as in the
+   reference (:221).  The mesh must have been set by hprmat_b200_rmat_ini with the same
+   nr, ns and rmax.  stats may be NULL. */
+int hprmat_b200_rmatrix(hprmat_b200_ctx* ctx, int nch, const int* lval, const double* qk,
+                        const double* eta, double rmax, int nr, int ns, const double* cpot,
+                        int ncp1, int ndim, double* cu, int* nopen, hprmat_b200_stats* stats);
+
+/* Same as hprmat_b200_rmatrix with cpot and cu in device memory (cu: ndim x ndim complex,
+   column-major).  lval/qk/eta stay host arrays (O(nch)). */
+int hprmat_b200_rmatrix_device(hprmat_b200_ctx* ctx, int nch, const int* lval,
+                               const double* qk, const double* eta, double rmax, int nr,
+                               int ns, const void* d_cpot, int ncp1, int ndim, void* d_cu,
+                               int* nopen, hprmat_b200_stats* stats);
+
+/* Dense solve C X = B: the solve inside solve_rmatrix (src/rmat_solvers.F90:49-90), same
+   layout as gpu_solve_mixed_ (src/cusolver_interface.cu:321-443).  A (n x n complex,
+   column-major) is read only; B (n x nrhs complex) is overwritten with X.  Host buffers. */
+int hprmat_b200_solve_linear(hprmat_b200_ctx* ctx, const double* A, double* B, int n,
+                             int nrhs, hprmat_b200_stats* stats);
+/* Same with A and B in device memory. */
+int hprmat_b200_solve_linear_device(hprmat_b200_ctx* ctx, const void* d_A, void* d_B, int n,
+                                    int nrhs, hprmat_b200_stats* stats);
+
+/* solve_rmatrix(cmat, B_vector, nch, nlag, normfac, Rmat, solver_type=7)
+   (src/rmat_solvers.F90:49-90 and the R extraction of :135-144): solves with the nch
+   channel-surface right-hand sides blockdiag(B_vector) and returns
+   Rmat(i, j) = normfac * sum_r B(r) X((i-1)*nlag + r, j) (bilinear, no conjugate).
+   Host buffers: cmat (N x N), bvec (nlag), rmat (nch x nch), all complex. */
+int hprmat_b200_solve_rmatrix(hprmat_b200_ctx* ctx, const double* cmat, const double* bvec,
+                              int nch, int nlag, double normfac, double* rmat,
+                              hprmat_b200_stats* stats);
+
+/* Fortran-convention drop-ins (arguments by reference, trailing underscore) for the
+   reference's C ABI, bound in src/gpu_solver_interface.F90:61-99.  They use a context on
+   device 0 created on first use.  Return 0 on success, -1 on error; *info as in the
+   reference (0 ok, -1 init, -2 alloc, >0 singular pivot, 99 refinement not converged). */
+int gpu_b200_solve_mixed_(double* A, double* B, int* n, int* nrhs, int* max_refine,
+                          double* tol, int* info);  /* cf. gpu_solve_mixed_  :321-329 */
+int gpu_b200_solve_double_(double* A, double* B, int* n, int* nrhs,
+                           int* info);              /* cf. gpu_solve_double_ :737-795 */
+int gpu_b200_finalize_(void);                       /* cf. gpu_solver_finalize_ :222 */
+
+/* Boundary values of the R-matrix -> collision-matrix step at the channel radius a = rmax,
+   per channel, as computed in rmatrix (src/rmatrix_hp.F90:224-244).  Host only, needs no
+   GPU.  Open channels (qk > 0): co = G + iF and cop = (G' + iF') k a from COULFG
+   (src/special_functions.f:1-275).  Closed channels: xc1 = a W'/W and xc2 = W from WHIT
+   (src/special_functions.f:309-416).  co/cop are complex (nch entries each), xc1/xc2 real;
+   entries that do not apply to a channel are zero.  Any output may be NULL. */
+int hprmat_b200_boundary(int nch, const int* lval, const double* qk, const double* eta, double rmax,
+                         double* co, double* cop, double* xc1, double* xc2, int* nopen);
+
+/* Human-readable status and the last CUDA error message of this thread's calls. */
+const char* hprmat_b200_status_string(int status);
+const char* hprmat_b200_last_error(void);
+int hprmat_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HPRMAT_B200_H */

@@ -1,0 +1,29 @@
+/*
+ * hprmat_b200_dev.h -- kernel-level entry points of libhprmat_b200.so for tests and
+ * benchmarks.  They run one device kernel of the solver on caller-provided device buffers,
+ * ordered on the context's stream, and return after it completes.  They are not part of
+ * the HPRMAT interface and have no counterpart in the reference.
+ */
+#ifndef HPRMAT_B200_DEV_H
+#define HPRMAT_B200_DEV_H
+#include "hprmat_b200.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* C[M x Nc] -= A * B on the tensor cores: C complex float (interleaved, column-major, ldc),
+   A and B as 4 planes (Re hi, Re lo, Im hi, Im lo of the TF32 split), K-major with nb
+   floats per row / column, planes `plane` floats apart (the LU's operand buffers).
+   nb in {16, 32, 64, 128}. */
+int hprmat_b200_dev_tc_update(hprmat_b200_ctx* ctx, const float* aop, const float* bop, long plane, int nb,
+                              void* C, long ldc, int M, int Nc);
+
+/* Split complex float values into the 4 TF32 planes used by hprmat_b200_dev_tc_update:
+   src is rows x nb (row-major complex float, i.e. K contiguous), dst gets 4 planes of
+   rows x nb floats, `plane` floats apart. */
+int hprmat_b200_dev_split_planes(hprmat_b200_ctx* ctx, const void* src, int rows, int nb, float* dst, long plane);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,380 @@
+"""Oracle (test infrastructure only): FP64 CPU restatement of HPRMAT's R-matrix path.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg may use
+this module, and only as the checker or as the timed CPU baseline -- never as the product.
+
+This is the reference's "Type 1" path (dense LAPACK ZGESV), restated in NumPy with the
+same LAPACK routine (``scipy.linalg.lapack.zgesv``, OpenBLAS) and the same argument
+pattern.  Reference paths are relative to the HPRMAT project root:
+
+* ``legzo``                  -- ``src/rmatrix_hp.F90:741-783``
+* ``rmat_ini``               -- ``src/rmatrix_hp.F90:61-159``
+* ``boundary_values``        -- ``src/rmatrix_hp.F90:224-244``
+* ``assemble``               -- ``src/rmatrix_hp.F90:246-293``
+* ``solve_rmatrix_dense``    -- ``src/rmatrix_hp.F90:441-477`` (= ``src/rmat_solvers.F90:98-148``)
+* ``solve_rmatrix_4``        -- ``src/rmatrix_hp.F90:590-632``
+* ``rmatrix``                -- ``src/rmatrix_hp.F90:175-368`` (propagation for ns > 1 at
+  ``:326-345``, collision matrix at ``:348-368``)
+* ``solve_rmatrix_mixed``    -- ``src/rmat_solvers.F90:157-296`` (CGETRF + FP64 refinement)
+
+Arrays follow the Fortran layout: C(E) is column-major with row index
+``(channel-1)*nr + i``; ``cpot`` has shape ``(ncp1, ndim, ndim)`` (Fortran order,
+``cpot[ir, c, c']``).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+import scipy.linalg.lapack as lapack
+
+from .special_functions import coulfg, whit
+
+
+def legzo(n: int):
+    """Gauss-Legendre nodes/weights on (0, 1) (src/rmatrix_hp.F90:741-783)."""
+    pi = 3.1415926535898
+    one = 1.0
+    x = np.zeros(n + 1)  # 1-based
+    w = np.zeros(n + 1)
+    n0 = (n + 1) // 2
+    for nr in range(1, n0 + 1):
+        z = math.cos(pi * (nr - 0.25) / (n + 0.5))
+        while True:
+            z0 = z
+            p = 1.0
+            for i in range(1, nr):
+                p = p * (z - x[i])
+            f0 = 1.0
+            if nr == n0 and n != 2 * (n // 2):
+                z = 0.0
+            f1 = z
+            pf = pd = 0.0
+            for k in range(2, n + 1):
+                pf = (2 - one / k) * z * f1 - (1 - one / k) * f0
+                pd = k * (f1 - z * pf) / (1 - z * z)
+                f0 = f1
+                f1 = pf
+            if z == 0:
+                break
+            fd = pf / p
+            q = 0.0
+            for i in range(1, nr):
+                wp = 1.0
+                for j in range(1, nr):
+                    if j != i:
+                        wp = wp * (z - x[j])
+                q = q + wp
+            gd = (pd - q * fd) / p
+            z = z - fd / gd
+            if not (abs(z - z0) > abs(z) * 1.0e-15):
+                break
+        x[nr] = z
+        x[n + 1 - nr] = -z
+        w[nr] = 2 / ((1 - z * z) * pd * pd)
+        w[n + 1 - nr] = w[nr]
+    xs = (1 + x[n:0:-1]) / 2
+    ws = w[n:0:-1] / 2
+    return xs.copy(), ws.copy()
+
+
+@dataclass
+class Mesh:
+    nr: int
+    ns: int
+    rmax: float
+    rmax0: float
+    xle: np.ndarray
+    wle: np.ndarray
+    tc: np.ndarray     # (nr, nr, ns)
+    blo0: np.ndarray   # (nr, nr)
+    blo1: np.ndarray
+    blo2: np.ndarray
+    q1: np.ndarray     # (nr, ns)
+    q2: np.ndarray     # (nr, ns)
+    zrma: np.ndarray   # (nr*ns,)
+
+
+def rmat_ini(nr: int, ns: int, rmax: float) -> Mesh:
+    """Lagrange-Legendre mesh, kinetic + Bloch matrices (src/rmatrix_hp.F90:61-159)."""
+    tc = np.zeros((nr, nr, ns))
+    blo0 = np.zeros((nr, nr))
+    blo1 = np.zeros((nr, nr))
+    blo2 = np.zeros((nr, nr))
+    q1 = np.zeros((nr, ns))
+    q2 = np.zeros((nr, ns))
+    rmax0 = rmax / ns
+    xle, wle = legzo(nr)
+    for is_ in range(1, ns + 1):
+        s = is_ - 1
+        for i1 in range(1, nr + 1):
+            xi = xle[i1 - 1]
+            xi2 = xi * (1 - xi)
+            if is_ == 1:
+                xx = 4 * nr * (nr + 1) + 3 + (1 - 6 * xi) / xi2
+                tc[i1 - 1, i1 - 1, 0] = xx / (3 * xi2)
+                blo0[i1 - 1, i1 - 1] = 1 / xi2
+            else:
+                xlb = xi / (1 - xi) * (nr * (nr + 1) - 1 / (1 - xi))
+                xla = (1 - xi) / xi * (-nr * (nr + 1) + 1 / xi)
+                tc[i1 - 1, i1 - 1, s] = (nr * nr + nr + 6 - 2 / xi2) / (3 * xi2) + xlb - xla
+                blo1[i1 - 1, i1 - 1] = (1 - xi) / xi
+                blo2[i1 - 1, i1 - 1] = xi / (1 - xi)
+            for i2 in range(1, i1):
+                xj = xle[i2 - 1]
+                xj2 = xj * (1 - xj)
+                if is_ == 1:
+                    xx = (nr * (nr + 1) + 1 + (xi + xj - 2 * xi * xj) / ((xi - xj) * (xi - xj))
+                          - 1 / (1 - xi) - 1 / (1 - xj))
+                    tc[i1 - 1, i2 - 1, 0] = xx / math.sqrt(xi2 * xj2)
+                    blo0[i1 - 1, i2 - 1] = 1 / math.sqrt(xi2 * xj2)
+                else:
+                    yy = (math.sqrt(xj2 / (xi2 * xi2 * xi2)) * (2 * xi * xj + 3 * xi - xj - 4 * xi * xi)
+                          / ((xj - xi) * (xj - xi)))
+                    xlb = math.sqrt(xi * xj / (1 - xi) / (1 - xj)) * (nr * (nr + 1) - 1 / (1 - xj))
+                    xla = math.sqrt((1 - xi) * (1 - xj) / xi / xj) * (-nr * (nr + 1) + 1 / xj)
+                    tc[i1 - 1, i2 - 1, s] = yy + xlb - xla
+                    blo1[i1 - 1, i2 - 1] = math.sqrt((1 - xi) * (1 - xj) / xi / xj)
+                    blo2[i1 - 1, i2 - 1] = math.sqrt(xi * xj / (1 - xi) / (1 - xj))
+                if (i1 + i2) % 2 == 1:
+                    tc[i1 - 1, i2 - 1, s] = -tc[i1 - 1, i2 - 1, s]
+                    blo0[i1 - 1, i2 - 1] = -blo0[i1 - 1, i2 - 1]
+                    blo1[i1 - 1, i2 - 1] = -blo1[i1 - 1, i2 - 1]
+                    blo2[i1 - 1, i2 - 1] = -blo2[i1 - 1, i2 - 1]
+                tc[i2 - 1, i1 - 1, s] = tc[i1 - 1, i2 - 1, s]
+                blo0[i2 - 1, i1 - 1] = blo0[i1 - 1, i2 - 1]
+                blo1[i2 - 1, i1 - 1] = blo1[i1 - 1, i2 - 1]
+                blo2[i2 - 1, i1 - 1] = blo2[i1 - 1, i2 - 1]
+            if is_ == 1:
+                q2[:, 0] = 1 / np.sqrt(xle * (1 - xle))
+                q1[:, 0] = 0
+            else:
+                q2[:, s] = np.sqrt(xle / (1 - xle))
+                q1[:, s] = -1 / q2[:, s]
+            if nr % 2 == 1:
+                q2[:, s] = -q2[:, s]
+            q1[0::2, s] = -q1[0::2, s]
+            q2[0::2, s] = -q2[0::2, s]
+    tc = tc / (rmax0 * rmax0)
+    blo0 = blo0 / rmax0
+    blo1 = blo1 / rmax0
+    blo2 = blo2 / rmax0
+    q1 = q1 / math.sqrt(rmax0)
+    q2 = q2 / math.sqrt(rmax0)
+    zrma = np.concatenate([((is_ - 1) + xle) * rmax0 for is_ in range(1, ns + 1)])
+    return Mesh(nr, ns, rmax, rmax0, xle, wle, tc, blo0, blo1, blo2, q1, q2, zrma)
+
+
+@dataclass
+class Boundary:
+    """Open-channel Coulomb values and closed-channel Whittaker values (rmatrix_hp.F90:224-244)."""
+    nopen: int
+    npo_open: list      # 0-based channel indices of open channels, in order
+    npo_closed: list
+    co: np.ndarray      # (nopen,) G + iF
+    cop: np.ndarray     # (nopen,) (G' + iF') * k * a
+    xc: np.ndarray      # (nch, 2): a*W'/W and W for closed channels
+
+
+def boundary_values(nch, lval, qk, eta, rmax) -> Boundary:
+    co, cop = [], []
+    xc = np.zeros((nch, 2))
+    npo_open, npo_closed = [], []
+    for i1 in range(nch):
+        l = int(lval[i1])
+        if qk[i1] > 0:
+            npo_open.append(i1)
+            fc, gc, dfc, dgc, ifail = coulfg(qk[i1] * rmax, eta[i1], float(l))
+            co.append(complex(gc, fc))
+            cop.append(complex(dgc, dfc) * qk[i1] * rmax)
+        else:
+            npo_closed.append(i1)
+            qk2 = -qk[i1]
+            f, fd, _ = whit(eta[i1], rmax, qk2, -qk2 * qk2, l, 0)
+            xc[i1, 0] = rmax * fd[l] / f[l]
+            xc[i1, 1] = f[l]
+    return Boundary(len(npo_open), npo_open, npo_closed, np.array(co, dtype=np.complex128),
+                    np.array(cop, dtype=np.complex128), xc)
+
+
+def assemble(mesh: Mesh, is_: int, nch, lval, qk, xc, cpot) -> np.ndarray:
+    """C(E) of interval ``is_`` (1-based), src/rmatrix_hp.F90:246-293 (local potentials)."""
+    nr = mesh.nr
+    rmax0 = mesh.rmax0
+    rmax1 = (is_ - 1) * rmax0
+    rmax2 = is_ * rmax0
+    ms = (is_ - 1) * nr
+    ntot = nch * nr
+    ch = np.zeros((ntot, ntot), dtype=np.complex128, order="F")
+    s = is_ - 1
+    rr = rmax1 + mesh.xle * rmax0
+    for i1 in range(nch):
+        m1 = i1 * nr
+        blk = mesh.tc[:, :, s].astype(np.complex128)
+        fac = float(lval[i1] * (lval[i1] + 1))
+        d = fac / (rr * rr)
+        if qk[i1] > 0:
+            d = d - qk[i1] * qk[i1]
+        if qk[i1] < 0:
+            d = d + qk[i1] * qk[i1]
+        blk[np.arange(nr), np.arange(nr)] += d
+        if qk[i1] < 0:
+            if is_ == 1:
+                blk = blk - xc[i1, 0] * mesh.blo0 / rmax2
+            else:
+                blk = blk - xc[i1, 0] * (mesh.blo2 / rmax2 - mesh.blo1 / rmax1)
+        ch[m1:m1 + nr, m1:m1 + nr] = blk
+        for i2 in range(nch):
+            m2 = i2 * nr
+            idx = np.arange(nr)
+            ch[m1 + idx, m2 + idx] += cpot[ms + idx, i1, i2]
+    return ch
+
+
+def _zgesv(a, b):
+    lu, piv, x, info = lapack.zgesv(np.asfortranarray(a), np.asfortranarray(b),
+                                    overwrite_a=True, overwrite_b=True)
+    return x, info
+
+
+def surface_rhs(q2col: np.ndarray, nch: int) -> np.ndarray:
+    """X = blockdiag(q2) RHS, one column per channel (src/rmatrix_hp.F90:456-461)."""
+    nr = q2col.shape[0]
+    x = np.zeros((nch * nr, nch), dtype=np.complex128, order="F")
+    for ich in range(nch):
+        x[ich * nr:(ich + 1) * nr, ich] = q2col
+    return x
+
+
+def extract_r(x: np.ndarray, bvec: np.ndarray, nch: int, normfac: float = 1.0) -> np.ndarray:
+    """R(i, j) = sum_r B(r) X((i-1)*nr + r, j) -- bilinear, no conjugate (rmatrix_hp.F90:466-474)."""
+    nr = bvec.shape[0]
+    rm = np.zeros((nch, nch), dtype=np.complex128)
+    for ich in range(nch):
+        rm[ich, :] = bvec @ x[ich * nr:(ich + 1) * nr, :]
+    return rm * normfac
+
+
+def solve_rmatrix_dense(cmat, bvec, nch, nlag, normfac=1.0):
+    """Type 1 solver (src/rmatrix_hp.F90:441-477): copy, ZGESV(N, nch), R extraction."""
+    a_work = np.array(cmat, dtype=np.complex128, order="F", copy=True)
+    xv = surface_rhs(np.asarray(bvec, dtype=np.complex128), nch)
+    x, info = _zgesv(a_work, xv)
+    if info != 0:
+        raise RuntimeError(f"Error in solve_rmatrix_hp ZGESV (info={info})")
+    return extract_r(x, np.asarray(bvec, dtype=np.complex128), nch, normfac), x
+
+
+def solve_rmatrix_mixed(cmat, bvec, nch, nlag, normfac=1.0, max_iter=2, tol=1.0e-10):
+    """Type 2 solver (src/rmat_solvers.F90:157-296): CGETRF + FP64 residual refinement."""
+    n = nch * nlag
+    a_sp = np.asfortranarray(cmat.astype(np.complex64))
+    b_dp = surface_rhs(np.asarray(bvec, dtype=np.complex128), nch)
+    b_norm = np.linalg.norm(b_dp)
+    if b_norm == 0.0:
+        b_norm = 1.0
+    lu, piv, info = lapack.cgetrf(a_sp)
+    if info != 0:
+        return solve_rmatrix_dense(cmat, bvec, nch, nlag, normfac)
+    w, info = lapack.cgetrs(lu, piv, b_dp.astype(np.complex64))
+    x = w.astype(np.complex128)
+    steps = 0
+    for _ in range(max_iter):
+        r = b_dp - cmat @ x
+        rel = np.linalg.norm(r) / b_norm
+        if rel < tol:
+            break
+        w, info = lapack.cgetrs(lu, piv, r.astype(np.complex64))
+        x = x + w.astype(np.complex128)
+        steps += 1
+    return extract_r(x, np.asarray(bvec, dtype=np.complex128), nch, normfac), x
+
+
+def solve_rmatrix_4(cmat, b0, b1, nch, nlag, normfac=1.0):
+    """R00, R01, R11 from one ZGESV with 2*nch RHS (src/rmatrix_hp.F90:590-632)."""
+    n = nch * nlag
+    xv = np.zeros((n, 2 * nch), dtype=np.complex128, order="F")
+    for ich in range(nch):
+        xv[ich * nlag:(ich + 1) * nlag, ich] = b0
+        xv[ich * nlag:(ich + 1) * nlag, ich + nch] = b1
+    x, info = _zgesv(np.array(cmat, order="F", copy=True), xv)
+    if info != 0:
+        raise RuntimeError("Error in solve_rmatrix_hp_4")
+    r00 = np.zeros((nch, nch), dtype=np.complex128)
+    r01 = np.zeros((nch, nch), dtype=np.complex128)
+    r11 = np.zeros((nch, nch), dtype=np.complex128)
+    for ich in range(nch):
+        blk = x[ich * nlag:(ich + 1) * nlag, :]
+        r00[ich, :] = (b0 @ blk[:, :nch]) * normfac
+        r01[ich, :] = (b0 @ blk[:, nch:]) * normfac
+        r11[ich, :] = (b1 @ blk[:, nch:]) * normfac
+    return r00, r01, r11
+
+
+def collision_matrix(rma: np.ndarray, bnd: Boundary, qk) -> np.ndarray:
+    """U from the R-matrix at the channel radius (src/rmatrix_hp.F90:348-368).
+
+    ``rma`` is R/a (crma0 at the last interval), shape (nch, nch).
+    """
+    no = bnd.nopen
+    idx = bnd.npo_open
+    crma2 = np.zeros((no, no), dtype=np.complex128)
+    for m1, i1 in enumerate(idx):
+        for m2, i2 in enumerate(idx):
+            crma2[m1, m2] = rma[i1, i2] * math.sqrt(qk[i1] / qk[i2])
+    cz = np.zeros((no, no), dtype=np.complex128)
+    cu = np.zeros((no, no), dtype=np.complex128)
+    for m1 in range(no):
+        cz[:, m1] = -crma2[:, m1] * bnd.cop[m1]
+        cu[:, m1] = -crma2[:, m1] * np.conj(bnd.cop[m1])
+        cz[m1, m1] += bnd.co[m1]
+        cu[m1, m1] += np.conj(bnd.co[m1])
+    if no == 0:
+        return cu
+    u, info = _zgesv(cz, cu)
+    if info != 0:
+        raise RuntimeError("Error in ZGESV for collision matrix")
+    return u
+
+
+@dataclass
+class RMatrixResult:
+    cu: np.ndarray        # (nopen, nopen) collision matrix
+    nopen: int
+    rma: np.ndarray       # R/a at the channel radius, (nch, nch)
+    boundary: Boundary
+    x: np.ndarray | None  # solution of the ns = 1 solve, (N, nch)
+
+
+def rmatrix(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, solver: str = "dense") -> RMatrixResult:
+    """Collision matrix for one (J, pi, E), src/rmatrix_hp.F90:175-368 (local potentials)."""
+    lval = np.asarray(lval)
+    qk = np.asarray(qk, dtype=np.float64)
+    eta = np.asarray(eta, dtype=np.float64)
+    nr, ns = mesh.nr, mesh.ns
+    bnd = boundary_values(nch, lval, qk, eta, rmax)
+    crma0_prev = None
+    x_last = None
+    for is_ in range(1, ns + 1):
+        rmax1 = (is_ - 1) * mesh.rmax0
+        rmax2 = is_ * mesh.rmax0
+        ch = assemble(mesh, is_, nch, lval, qk, bnd.xc, cpot)
+        bvec = mesh.q2[:, is_ - 1].astype(np.complex128)
+        if solver == "dense":
+            r11, x_last = solve_rmatrix_dense(ch, bvec, nch, nr)
+        elif solver == "mixed":
+            r11, x_last = solve_rmatrix_mixed(ch, bvec, nch, nr)
+        else:
+            raise ValueError(solver)
+        if ns > 1:
+            r00, r01, r11 = solve_rmatrix_4(ch, mesh.q1[:, is_ - 1], mesh.q2[:, is_ - 1], nch, nr)
+        if is_ == 1:
+            crma0 = r11 / rmax2
+        else:
+            cz = r00 + crma0_prev * rmax1
+            czi = np.linalg.solve(cz, np.eye(nch, dtype=np.complex128))
+            crma0 = (r11 - r01.T @ czi @ r01) / rmax2
+        crma0_prev = crma0
+    cu = collision_matrix(crma0_prev, bnd, qk)
+    return RMatrixResult(cu, bnd.nopen, crma0_prev, bnd, x_last if ns == 1 else None)

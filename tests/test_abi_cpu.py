@@ -1,0 +1,99 @@
+"""C ABI checks that need no GPU: the library loads, exports every declared symbol, and
+its host-side pieces agree with the oracle."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from hprmat_b200 import _native as nat
+from hprmat_b200 import api, workloads
+from oracle import rmatrix_oracle as orc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    names = []
+    for h in ("hprmat_b200.h", "hprmat_b200_dev.h"):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names += re.findall(r"\b((?:hprmat_b200|gpu_b200)_\w+)\s*\(", src)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = nat.load()
+    declared = _declared()
+    assert len(declared) >= 15
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert set(declared) == set(nat.EXPORTED)
+    out = subprocess.run(["nm", "-D", "--defined-only", nat.LIB_PATH], capture_output=True, text=True).stdout
+    for name in declared:
+        assert re.search(r"\bT " + re.escape(name) + r"$", out, re.M), name
+
+
+def test_library_is_built_for_sm100a():
+    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", nat.LIB_PATH], capture_output=True,
+                         text=True).stdout
+    assert "sm_100a" in out
+
+
+def test_default_opts_and_status_strings():
+    lib = nat.load()
+    o = nat.Opts()
+    lib.hprmat_b200_default_opts(ctypes.byref(o))
+    assert o.precision == nat.PREC_MIXED and o.max_refine == 3 and o.tol == 1e-13 and o.panel_nb == 0
+    assert lib.hprmat_b200_status_string(nat.SINGULAR) == b"singular matrix"
+    assert lib.hprmat_b200_status_string(nat.NOT_CONVERGED) == b"refinement did not converge"
+
+
+def test_create_without_device_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(nat.HprmatError) as e:
+        api.Context()
+    assert e.value.status == nat.ERR_NODEVICE
+
+
+@pytest.mark.parametrize("wl", ["small", "production", "sweep"])
+def test_boundary_values_match_oracle(wl):
+    w = {"small": workloads.small(), "production": workloads.production(nch=40),
+         "sweep": workloads.sweep(20)}[wl]
+    co, cop, xc1, xc2, nopen = api.boundary_values(w.lval, w.qk, w.eta, w.rmax)
+    ref = orc.boundary_values(w.nch, w.lval, w.qk, w.eta, w.rmax)
+    assert nopen == ref.nopen
+    for m, c in enumerate(ref.npo_open):
+        assert abs(co[c] - ref.co[m]) <= 1e-13 * abs(ref.co[m])
+        assert abs(cop[c] - ref.cop[m]) <= 1e-13 * abs(ref.cop[m])
+    for c in ref.npo_closed:
+        assert abs(xc1[c] - ref.xc[c, 0]) <= 1e-13 * abs(ref.xc[c, 0])
+        assert abs(xc2[c] - ref.xc[c, 1]) <= 1e-13 * abs(ref.xc[c, 1])
+
+
+def test_boundary_values_ex1_jwkb_branch():
+    """Ex1 at 10 MeV (l = 20, eta = 16) runs COULFG's JWKB branch; product == oracle."""
+    from tests.example_inputs import ex1_setup
+    mesh = orc.rmat_ini(60, 1, 14.0)
+    _, kin = ex1_setup(mesh.zrma)
+    for e in (10.0, 20.0, 50.0):
+        lval, qk, eta = kin(e, 20)
+        co, cop, _, _, _ = api.boundary_values(lval, qk, eta, 14.0)
+        ref = orc.boundary_values(1, lval, qk, eta, 14.0)
+        assert abs(co[0] - ref.co[0]) <= 1e-13 * abs(ref.co[0])
+        assert abs(cop[0] - ref.cop[0]) <= 1e-13 * abs(ref.cop[0])
+
+
+def test_boundary_rejects_bad_arguments():
+    lib = nat.load()
+    z = np.zeros(1)
+    assert lib.hprmat_b200_boundary(0, None, None, None, 1.0, None, None, None, None, None) == nat.ERR_ARG
+    lval = np.array([-1], np.int32)
+    assert lib.hprmat_b200_boundary(1, lval.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                    z.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                    z.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 1.0,
+                                    None, None, None, None, None) == nat.ERR_ARG

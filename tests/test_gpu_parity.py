@@ -1,0 +1,249 @@
+"""GPU parity of the CUDA path (through the C ABI) against the oracle.
+
+Tolerances: collision matrices agree with the FP64 LAPACK oracle to a relative Frobenius
+error of 1e-10 (the target of the solver), for both the plain FP64 LU and the mixed
+(3xTF32 tensor-core LU + FP64 refinement) path.  The tensor-core trailing-update kernel is
+checked on its own against an FP64 torch product to 3xTF32 accuracy (2e-6 relative).
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from hprmat_b200 import _native as nat
+from hprmat_b200 import api, workloads
+from oracle import rmatrix_oracle as orc
+from tests.example_inputs import ex1_setup, ex2_setup, ex4_setup
+
+pytestmark = pytest.mark.gpu
+
+U_TOL = 1e-10
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def _oracle_u(w):
+    mesh = orc.rmat_ini(w.nr, 1, w.rmax)
+    return orc.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, mesh, w.cpot)
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = api.Context(precision="mixed")
+    yield c
+    c.close()
+
+
+# ---------------------------------------------------------------- tensor-core kernel
+@pytest.mark.parametrize("M,Nc,nb", [(128, 256, 128), (300, 520, 128), (1000, 700, 64), (77, 33, 32)])
+def test_tc_update_kernel_matches_fp64(ctx, M, Nc, nb):
+    lib = nat.load()
+    g = torch.Generator(device="cpu").manual_seed(M + Nc)
+    A = torch.randn(M, nb, 2, generator=g, dtype=torch.float32)
+    B = torch.randn(Nc, nb, 2, generator=g, dtype=torch.float32)
+    C = torch.randn(Nc, M, 2, generator=g, dtype=torch.float32)   # column-major complex (M x Nc)
+    plane = max(M, Nc) * nb + 64
+    dA = A.cuda().contiguous()
+    dB = B.cuda().contiguous()
+    dC = C.cuda().contiguous()
+    aop = torch.zeros(4 * plane, dtype=torch.float32, device="cuda")
+    bop = torch.zeros(4 * plane, dtype=torch.float32, device="cuda")
+    h = ctx._h
+    nat.check(lib.hprmat_b200_dev_split_planes(h, dA.data_ptr(), M, nb, aop.data_ptr(), plane))
+    nat.check(lib.hprmat_b200_dev_split_planes(h, dB.data_ptr(), Nc, nb, bop.data_ptr(), plane))
+    nat.check(lib.hprmat_b200_dev_tc_update(h, aop.data_ptr(), bop.data_ptr(), plane, nb, dC.data_ptr(), M, M, Nc))
+    torch.cuda.synchronize()
+    Az = torch.complex(A[..., 0].double(), A[..., 1].double())          # M x nb
+    Bz = torch.complex(B[..., 0].double(), B[..., 1].double())          # Nc x nb (column j = row j)
+    Cz = torch.complex(C[..., 0].double(), C[..., 1].double()).T        # M x Nc
+    ref = Cz - Az @ Bz.T
+    got = dC.cpu().double()
+    got = torch.complex(got[..., 0], got[..., 1]).T
+    err = (got - ref).abs().max().item()
+    scale = (Az.abs() @ Bz.abs().T).max().item()
+    assert err <= 2e-6 * scale, (err, scale)
+
+
+# ---------------------------------------------------------------- R-matrix path
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_small_workload_u_matches_oracle(ctx, precision):
+    w = workloads.small()
+    ref = _oracle_u(w)
+    ctx.set_precision(precision)
+    cu, nopen = ctx.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+    assert nopen == ref.nopen == w.nch
+    assert _rel(cu[:nopen, :nopen], ref.cu) <= U_TOL, ctx.last_stats
+    st = ctx.last_stats
+    assert st["rel_residual"] < 1e-12
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_ex1_and_ex2_through_the_abi(ctx, precision):
+    """Reference examples 1 and 2 (ns = 1 cards): product == oracle, and the printed golden
+    values of the reference are reproduced."""
+    ctx.set_precision(precision)
+    mesh = orc.rmat_ini(60, 1, 14.0)
+    cpot, kin = ex1_setup(mesh.zrma)
+    for e in (10.0, 20.0, 30.0, 40.0, 50.0):
+        lval, qk, eta = kin(e, 20)
+        cu, nopen = ctx.rmatrix(1, lval, qk, eta, 14.0, 60, 1, cpot)
+        ref = orc.rmatrix(1, lval, qk, eta, 14.0, mesh, cpot).cu
+        assert abs(cu[0, 0] - ref[0, 0]) <= U_TOL * abs(ref[0, 0])
+    mesh = orc.rmat_ini(60, 1, 7.0)
+    cpot, kin = ex2_setup(mesh.zrma, 1)
+    for e in (12.0, 24.0, 36.0, 48.0):
+        lval, qk, eta = kin(e)
+        cu, nopen = ctx.rmatrix(2, lval, qk, eta, 7.0, 60, 1, cpot)
+        ref = orc.rmatrix(2, lval, qk, eta, 7.0, mesh, cpot).cu
+        assert _rel(cu[:2, :2], ref) <= U_TOL
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_ex4_closed_channels_single_interval(ctx, precision):
+    """Ex4's 12C + alpha couplings with closed channels, one interval (nr = 100, a = 10)."""
+    ctx.set_precision(precision)
+    mesh = orc.rmat_ini(100, 1, 10.0)
+    cpot, kin, nv = ex4_setup(mesh.zrma, 3)
+    for e in (4.0, 8.0, 16.0):
+        lval, qk, eta = kin(e)
+        cu, nopen = ctx.rmatrix(nv, lval, qk, eta, 10.0, 100, 1, cpot)
+        ref = orc.rmatrix(nv, lval, qk, eta, 10.0, mesh, cpot)
+        assert nopen == ref.nopen
+        assert _rel(cu[:nopen, :nopen], ref.cu) <= U_TOL
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_medium_production_generator(ctx, precision):
+    """Production-generator physics at N = 4000 (20 channels x 200 points): open and closed
+    channels, Coulomb, complex couplings."""
+    w = workloads.production(nch=20)
+    ref = _oracle_u(w)
+    ctx.set_precision(precision)
+    cu, nopen = ctx.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+    assert nopen == ref.nopen
+    assert _rel(cu[:nopen, :nopen], ref.cu) <= U_TOL, ctx.last_stats
+
+
+def test_sweep_generator_closed_at_40mev(ctx):
+    w = workloads.sweep(20)
+    ref = _oracle_u(w)
+    ctx.set_precision("mixed")
+    cu, nopen = ctx.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+    assert _rel(cu[:nopen, :nopen], ref.cu) <= U_TOL, ctx.last_stats
+
+
+# ---------------------------------------------------------------- dense solves
+def _diag_dominant(n, nrhs, seed):
+    """The reference's solver cross-check matrix (examples/Ex0/test_solver.f90:35-84):
+    uniform random entries, A_ii += 2N, B_r = 1/sqrt(r)."""
+    rng = np.random.default_rng(seed)
+    A = rng.random((n, n)) + 1j * rng.random((n, n))
+    A[np.arange(n), np.arange(n)] += 2 * n
+    B = np.zeros((n, nrhs), np.complex128)
+    for c in range(nrhs):
+        B[:, c] = 1.0 / np.sqrt(np.arange(1, n + 1)) * (c + 1)
+    return np.asfortranarray(A), np.asfortranarray(B)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("n,nrhs", [(500, 8), (1000, 1), (2053, 37)])
+def test_solve_linear_dense(ctx, precision, n, nrhs):
+    A, B = _diag_dominant(n, nrhs, n)
+    ctx.set_precision(precision)
+    X = ctx.solve_linear(A, B)
+    Xr = np.linalg.solve(A, B)
+    assert _rel(X, Xr) <= 1e-12
+
+
+@pytest.mark.parametrize("kappa", [1e2, 1e5, 1e8])
+def test_solve_linear_exact_condition_number(ctx, kappa):
+    """Householder A = H D H with geometric D (exact kappa), manufactured X = 1, as in
+    examples/Ex0/benchmark_mgpu_illcond.f90:41-95."""
+    n, nrhs = 1024, 4
+    rng = np.random.default_rng(7)
+    v = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    v /= np.linalg.norm(v)
+    H = np.eye(n) - 2 * np.outer(v, v.conj())
+    d = kappa ** (-np.arange(n) / (n - 1))
+    A = np.asfortranarray((H * d[None, :]) @ H)
+    Xt = np.ones((n, nrhs), np.complex128)
+    B = np.asfortranarray(A @ Xt)
+    ctx.set_precision("mixed", max_refine=3, tol=1e-13)
+    X = ctx.solve_linear(A, B, allow_unconverged=True)
+    st = ctx.last_stats
+    Xr = np.linalg.solve(A, B)
+    err_ref = _rel(Xr, Xt)
+    assert _rel(X, Xt) <= max(10 * err_ref, 1e-12), (st, err_ref)
+
+
+def test_fortran_dropins(ctx):
+    lib = nat.load()
+    n, nrhs = 700, 5
+    A, B = _diag_dominant(n, nrhs, 3)
+    Xr = np.linalg.solve(A, B)
+    import ctypes
+    for fn in ("mixed", "double"):
+        Bw = np.array(B, order="F", copy=True)
+        Ac = np.array(A, order="F", copy=True)
+        info = ctypes.c_int(-7)
+        nn, nr = ctypes.c_int(n), ctypes.c_int(nrhs)
+        dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        if fn == "mixed":
+            mr, tol = ctypes.c_int(3), ctypes.c_double(1e-13)
+            r = lib.gpu_b200_solve_mixed_(dp(Ac), dp(Bw), ctypes.byref(nn), ctypes.byref(nr), ctypes.byref(mr),
+                                          ctypes.byref(tol), ctypes.byref(info))
+        else:
+            r = lib.gpu_b200_solve_double_(dp(Ac), dp(Bw), ctypes.byref(nn), ctypes.byref(nr), ctypes.byref(info))
+        assert r == 0 and info.value == 0
+        assert np.array_equal(Ac, A)  # A is read only
+        assert _rel(Bw, Xr) <= 1e-12
+    assert lib.gpu_b200_finalize_() == 0
+
+
+def test_solve_rmatrix_matches_oracle(ctx):
+    w = workloads.small()
+    mesh = orc.rmat_ini(w.nr, 1, w.rmax)
+    bnd = orc.boundary_values(w.nch, w.lval, w.qk, w.eta, w.rmax)
+    C = orc.assemble(mesh, 1, w.nch, w.lval, w.qk, bnd.xc, w.cpot)
+    bvec = mesh.q2[:, 0].astype(np.complex128)
+    ref, _ = orc.solve_rmatrix_dense(C, bvec, w.nch, w.nr, 1.0)
+    ctx.set_precision("mixed")
+    rm = ctx.solve_rmatrix(C, bvec, w.nch, w.nr, 1.0)
+    assert _rel(rm, ref) <= 1e-10
+
+
+# ---------------------------------------------------------------- failures
+def test_singular_matrix_reports_status(ctx):
+    n = 300
+    A, B = _diag_dominant(n, 2, 11)
+    A[:, 17] = 0.0
+    for prec in ("fp64", "mixed"):
+        ctx.set_precision(prec)
+        with pytest.raises(nat.HprmatError) as e:
+            ctx.solve_linear(A, B)
+        assert e.value.status == nat.SINGULAR
+        assert ctx.last_stats["info"] == 18
+
+
+def test_refinement_cap_reports_not_converged(ctx):
+    """max_refine = 0 with a tolerance the FP32-accurate factors cannot reach."""
+    w = workloads.production(nch=20)
+    ctx.set_precision("mixed", max_refine=0, tol=1e-13)
+    with pytest.raises(nat.HprmatError) as e:
+        ctx.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+    assert e.value.status == nat.NOT_CONVERGED
+    cu, nopen = ctx.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot, allow_unconverged=True)
+    assert ctx.last_stats["rel_residual"] > 1e-13
+    ctx.set_precision("mixed", max_refine=3, tol=1e-13)
+
+
+def test_bad_arguments(ctx):
+    lib = nat.load()
+    assert lib.hprmat_b200_solve_linear(ctx._h, None, None, 0, 1, None) == nat.ERR_ARG
+    w = workloads.small()
+    with pytest.raises(nat.HprmatError) as e:
+        ctx.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 2, w.cpot)
+    assert e.value.status in (nat.ERR_UNSUPPORTED, nat.ERR_ARG)
