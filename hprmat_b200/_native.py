@@ -33,24 +33,28 @@ EXPORTED = (
     "gpu_b200_solve_mixed_", "gpu_b200_solve_double_", "gpu_b200_finalize_", "hprmat_b200_status_string",
     "hprmat_b200_last_error", "hprmat_b200_version", "hprmat_b200_boundary",
     # include/hprmat_b200_dev.h
-    "hprmat_b200_dev_tc_update", "hprmat_b200_dev_split_planes",
+    "hprmat_b200_dev_tc_update", "hprmat_b200_dev_split_planes", "hprmat_b200_dev_set_profile",
+    "hprmat_b200_dev_counters",
 )
 
 
 class Opts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("max_refine", ctypes.c_int), ("tol", ctypes.c_double),
-                ("panel_nb", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
+                ("surface_tol", ctypes.c_double), ("panel_nb", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
 
 
 class Stats(ctypes.Structure):
-    _fields_ = [("status", ctypes.c_int), ("info", ctypes.c_int), ("refine_steps", ctypes.c_int),
+    _fields_ = [("status", ctypes.c_int), ("info", ctypes.c_int), ("refine_steps", ctypes.c_int), ("inner_iterations", ctypes.c_int),
                 ("nb", ctypes.c_int), ("n", ctypes.c_int), ("nrhs", ctypes.c_int),
-                ("rel_residual", ctypes.c_double), ("residual_history", ctypes.c_double * 9),
+                ("rel_residual", ctypes.c_double), ("surface_change", ctypes.c_double),
+                ("residual_floor", ctypes.c_double), ("floor_history", ctypes.c_double * 9),
+                ("residual_history", ctypes.c_double * 9),
                 ("ms_assemble", ctypes.c_double), ("ms_factor", ctypes.c_double), ("ms_solve", ctypes.c_double),
                 ("ms_refine", ctypes.c_double), ("ms_umatrix", ctypes.c_double), ("ms_total", ctypes.c_double)]
 
     def as_dict(self):
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "residual_history"}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("residual_history", "floor_history")}
+        d["floor_history"] = [self.floor_history[i] for i in range(9) if self.floor_history[i] != 0.0]
         d["residual_history"] = [self.residual_history[i] for i in range(9) if self.residual_history[i] != 0.0]
         return d
 
@@ -94,8 +98,10 @@ def load():
         "hprmat_b200_last_error": (ctypes.c_char_p, []),
         "hprmat_b200_version": (I, []),
         "hprmat_b200_boundary": (I, [I, IP, DP, DP, D, DP, DP, DP, DP, IP]),
-        "hprmat_b200_dev_tc_update": (I, [P, P, P, ctypes.c_long, I, P, ctypes.c_long, I, I]),
+        "hprmat_b200_dev_tc_update": (I, [P, P, P, ctypes.c_long, I, P, ctypes.c_long, I, I, I]),
         "hprmat_b200_dev_split_planes": (I, [P, P, I, I, P, ctypes.c_long]),
+        "hprmat_b200_dev_set_profile": (I, [P, I]),
+        "hprmat_b200_dev_counters": (I, [P, ctypes.POINTER(ctypes.c_ulonglong), DP, DP, IP, I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -37,8 +37,8 @@ def _iptr(a: np.ndarray):
 class Context:
     """One device context (stream + device buffers) of the C library."""
 
-    def __init__(self, device: int = 0, precision: str = "mixed", max_refine: int = 3, tol: float = 1e-13,
-                 panel_nb: int = 0):
+    def __init__(self, device: int = 0, precision: str = "mixed", max_refine: int = 3, tol: float = 1e-12,
+                 panel_nb: int = 0, surface_tol: float = 1e-11):
         self._lib = nat.load()
         self._h = ctypes.c_void_p()
         self.opts = nat.Opts()
@@ -46,6 +46,7 @@ class Context:
         self.opts.precision = _PREC[precision]
         self.opts.max_refine = int(max_refine)
         self.opts.tol = float(tol)
+        self.opts.surface_tol = float(surface_tol)
         self.opts.panel_nb = int(panel_nb)
         nat.check(self._lib.hprmat_b200_create(int(device), ctypes.byref(self.opts), ctypes.byref(self._h)))
         self.device = device
@@ -70,8 +71,11 @@ class Context:
     def __exit__(self, *exc):
         self.close()
 
-    def set_precision(self, precision: str, max_refine: int | None = None, tol: float | None = None):
+    def set_precision(self, precision: str, max_refine: int | None = None, tol: float | None = None,
+                      surface_tol: float | None = None):
         self.opts.precision = _PREC[precision]
+        if surface_tol is not None:
+            self.opts.surface_tol = float(surface_tol)
         if max_refine is not None:
             self.opts.max_refine = int(max_refine)
         if tol is not None:

@@ -46,9 +46,12 @@ struct PanelArgs {
   int* status;                    // device status block
   StepSwaps sw;
   unsigned* growth_bits;          // running max |u_ij| (as float bits, non-negative)
-  // Optional: A-operand planes of the mixed path (hi/lo splits of Re/Im of L21, K-major).
-  float* aop;
-  long aop_plane;                 // elements between planes
+  // Optional (mixed path): the "LU planes", hi/lo TF32 splits of Re/Im of the factors,
+  // row-major (row stride lup_ld floats, planes lup_plane floats apart).  The panel writes
+  // its L21 rows there; they are the K-major A operand of the tensor-core updates.
+  float* lup;
+  long lup_ld;
+  long lup_plane;
 };
 
 // -------------------------------------------------------------------------------------
@@ -209,24 +212,22 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
     int lr = idx % nloc, c = idx / nloc;
     a.W[(size_t)(a.k0 + r0 + lr) + (size_t)(a.k0 + c) * a.ld] = P[(size_t)c * rpcp + lr];
   }
-  // A-operand planes (mixed path): rows below the diagonal block, K-major, zero padded
-  if (a.aop != nullptr) {
+  // L21 rows into the LU planes (mixed path): global row k0 + g, columns k0 .. k0+ncols
+  if (a.lup != nullptr) {
     const int lr0 = max(ncols - r0, 0);
     const int nl = nloc - lr0;
-    for (int idx = tid; idx < nl * NB; idx += NT) {
-      int c = idx % NB;
-      int lr = lr0 + idx / NB;
-      size_t row = (size_t)(r0 + lr - ncols);
-      float hr = 0.f, lrr = 0.f, hi_ = 0.f, li = 0.f;
-      if (c < ncols) {
-        T v = P[(size_t)c * rpcp + lr];
-        tf32_split((float)v.x, hr, lrr);
-        tf32_split((float)v.y, hi_, li);
-      }
-      a.aop[0 * a.aop_plane + row * NB + c] = hr;
-      a.aop[1 * a.aop_plane + row * NB + c] = lrr;
-      a.aop[2 * a.aop_plane + row * NB + c] = hi_;
-      a.aop[3 * a.aop_plane + row * NB + c] = li;
+    for (int idx = tid; idx < nl * ncols; idx += NT) {
+      int c = idx % ncols;
+      int lr = lr0 + idx / ncols;
+      size_t off = (size_t)(a.k0 + r0 + lr) * a.lup_ld + (size_t)(a.k0 + c);
+      float hr, lrr, hi_, li;
+      T v = P[(size_t)c * rpcp + lr];
+      tf32_split((float)v.x, hr, lrr);
+      tf32_split((float)v.y, hi_, li);
+      a.lup[off] = hr;
+      a.lup[a.lup_plane + off] = lrr;
+      a.lup[2 * a.lup_plane + off] = hi_;
+      a.lup[3 * a.lup_plane + off] = li;
     }
   }
   if (b == 0) {
@@ -294,6 +295,9 @@ struct TrsmArgs {
   long bop_plane;
   int bop_col0;      // column of X that maps to B-operand column 0
   unsigned* growth_bits;
+  float* lup;        // optional LU planes: U12 rows k0.. (row-major, see PanelArgs)
+  long lup_ld;
+  long lup_plane;
 };
 
 template <typename T, int NB, int CW, int NT>
@@ -345,6 +349,20 @@ __global__ void __launch_bounds__(NT) trsm_lower_kernel(TrsmArgs<T> a) {
   if (a.growth_bits) {
     for (int o = 16; o > 0; o >>= 1) gmax = fmax(gmax, __shfl_down_sync(0xffffffffu, gmax, o));
     if ((tid & 31) == 0) atomicMax(a.growth_bits, __float_as_uint((float)gmax));
+  }
+  if (a.lup != nullptr) {
+    for (int idx = tid; idx < ncw * ncols; idx += NT) {
+      int cc = idx % ncw, j = idx / ncw;
+      float hr, lr, hi_, li;
+      T v = A[cc * NBP + j];
+      tf32_split((float)v.x, hr, lr);
+      tf32_split((float)v.y, hi_, li);
+      size_t off = (size_t)(a.k0 + j) * a.lup_ld + (size_t)(cb + cc);
+      a.lup[off] = hr;
+      a.lup[a.lup_plane + off] = lr;
+      a.lup[2 * a.lup_plane + off] = hi_;
+      a.lup[3 * a.lup_plane + off] = li;
+    }
   }
   if (a.bop != nullptr) {
     for (int idx = tid; idx < ncw * NB; idx += NT) {
@@ -534,42 +552,50 @@ __global__ void __launch_bounds__(NT) tri_inverse_kernel(const T* __restrict__ W
 }
 
 // One diagonal block of a triangular solve with many right-hand sides:
-//   X[k0:k0+ncols, cols] = Tinv * (P X)[k0:k0+ncols, cols]
+//   X[k0:k0+ncols, col] = Tinv * (P X)[k0:k0+ncols, col]
 // where P is the step's row-interchange list (forward solve; pass top_src = nullptr for
-// the backward solve).  Each CTA owns CW right-hand-side columns.
-template <typename T, int NB, int CW, int NT>
-__global__ void __launch_bounds__(NT) diag_apply_kernel(const T* __restrict__ Tinv, int ncols, int k0,
+// the backward solve).  One CTA of NB threads per right-hand side: thread i forms row i
+// from Tinv (read along rows i, coalesced) and the gathered column in shared memory.
+// With rop != nullptr the result is also written as B-operand planes of the tensor-core
+// update (per right-hand side NB consecutive values, zero padded; planes rop_plane apart).
+template <typename T, int NB>
+__global__ void __launch_bounds__(NB) diag_apply_kernel(const T* __restrict__ Tinv, int ncols, int k0,
                                                         const int* top_src, const int* extra_dst,
                                                         const int* extra_src, const int* n_extra,
-                                                        T* X, long ldx, int nrhs) {
-  constexpr int NBP = NB + 1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* Bv = reinterpret_cast<T*>(smem_raw);  // [CW][NBP]
-  T* E = Bv + CW * NBP;                    // [CW][NB]
-  const int tid = threadIdx.x;
-  const int cb = blockIdx.x * CW;
-  const int ncw = min(CW, nrhs - cb);
-  if (ncw <= 0) return;
+                                                        T* X, long ldx, int nrhs, float* rop, long rop_plane) {
+  __shared__ T bv[NB];
+  __shared__ T ev[NB];
+  const int i = threadIdx.x;
+  const int col = blockIdx.x;
+  if (col >= nrhs) return;
+  T* x = X + (size_t)col * ldx;
   const int ne = top_src ? *n_extra : 0;
-  for (int idx = tid; idx < ncw * ncols; idx += NT) {
-    int j = idx % ncols, cc = idx / ncols;
-    int src = top_src ? top_src[j] : k0 + j;
-    Bv[cc * NBP + j] = X[(size_t)src + (size_t)(cb + cc) * ldx];
-  }
-  for (int idx = tid; idx < ncw * ne; idx += NT) {
-    int e = idx % ne, cc = idx / ne;
-    E[cc * NB + e] = X[(size_t)extra_src[e] + (size_t)(cb + cc) * ldx];
-  }
+  if (i < ncols) bv[i] = x[top_src ? top_src[i] : k0 + i];
+  if (i < ne) ev[i] = x[extra_src[i]];
   __syncthreads();
-  for (int idx = tid; idx < ncw * ne; idx += NT) {
-    int e = idx % ne, cc = idx / ne;
-    X[(size_t)extra_dst[e] + (size_t)(cb + cc) * ldx] = E[cc * NB + e];
+  if (i < ne) x[extra_dst[i]] = ev[i];
+  T acc0 = czero<T>(), acc1 = czero<T>();
+  if (i < ncols) {
+    const T* tr = Tinv + i;
+    int j = 0;
+#pragma unroll 4
+    for (; j + 1 < ncols; j += 2) {
+      cfma(acc0, __ldg(tr + (size_t)j * NB), bv[j]);
+      cfma(acc1, __ldg(tr + (size_t)(j + 1) * NB), bv[j + 1]);
+    }
+    if (j < ncols) cfma(acc0, __ldg(tr + (size_t)j * NB), bv[j]);
+    acc0 = cadd(acc0, acc1);
+    x[k0 + i] = acc0;
   }
-  for (int idx = tid; idx < ncw * ncols; idx += NT) {
-    int i = idx % ncols, cc = idx / ncols;
-    T acc = czero<T>();
-    for (int j = 0; j < ncols; ++j) cfma(acc, Tinv[i + (size_t)j * NB], Bv[cc * NBP + j]);
-    X[(size_t)(k0 + i) + (size_t)(cb + cc) * ldx] = acc;
+  if (rop != nullptr) {
+    float hr, lr, hi_, li;
+    tf32_split((float)acc0.x, hr, lr);
+    tf32_split((float)acc0.y, hi_, li);
+    size_t off = (size_t)col * NB + i;
+    rop[off] = hr;
+    rop[rop_plane + off] = lr;
+    rop[2 * rop_plane + off] = hi_;
+    rop[3 * rop_plane + off] = li;
   }
 }
 

@@ -21,17 +21,43 @@ struct MeshDev {
   int nr;
 };
 
+// Compensated accumulation (Ogita-Rump-Oishi Dot2): sum += a*b with the rounding errors of
+// the product (FMA) and of the sum (TwoSum) kept in a second word.  Gives the residual of
+// the outer refinement steps about twice the working precision, so that refinement
+// converges to the solution rather than to the rounding noise of u |C| |X|.
+struct Acc2 {
+  double hi = 0.0, lo = 0.0;
+  __device__ __forceinline__ void add_prod(double a, double b) {
+    double p = a * b;
+    double pe = fma(a, b, -p);
+    double s = hi + p;
+    double bb = s - hi;
+    double e = (hi - (s - bb)) + (p - bb);
+    hi = s;
+    lo += e + pe;
+  }
+  __device__ __forceinline__ void add(double p) {
+    double s = hi + p;
+    double bb = s - hi;
+    lo += (hi - (s - bb)) + (p - bb);
+    hi = s;
+  }
+  __device__ __forceinline__ double value() const { return hi + lo; }
+};
+
 // C(E) of src/rmatrix_hp.F90:246-293 (one interval, local potentials):
 //   channel block (c,c): tc + diag(l(l+1)/r^2 -+ k^2) - (xc/a) blo0 (closed channels)
 //   every block (c,c'):  + diag(cpot(r_i, c, c'))
 // One thread per element, threads along rows (column-major, coalesced stores).  Writes T
 // (double2 or float2).
+// Also accumulates ||C||_F^2 (FP64) into *fro2 for the refinement's backward error.
 template <typename T>
 __global__ void assemble_kernel(MeshDev mesh, ChannelData ch, int nch, const double2* __restrict__ cpot,
-                                long ncp1, long ndim, T* W, long ld, int N) {
+                                long ncp1, long ndim, T* W, long ld, int N, double* fro2) {
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   const int col = blockIdx.y;
-  if (row >= N) return;
+  double sq = 0.0;
+  if (row < N) {
   const int nr = mesh.nr;
   const int c = row / nr, i = row - c * nr;
   const int cp = col / nr, j = col - cp * nr;
@@ -52,6 +78,17 @@ __global__ void assemble_kernel(MeshDev mesh, ChannelData ch, int nch, const dou
   out.x = (typename RealOf<T>::R)re;
   out.y = (typename RealOf<T>::R)im;
   W[(size_t)row + (size_t)col * ld] = out;
+  sq = re * re + im * im;
+  }
+  for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    sq = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+    if (threadIdx.x == 0 && sq != 0.0) atomicAdd(fro2, sq);
+  }
 }
 
 // Channel-surface right-hand sides X = blockdiag(q2) (src/rmatrix_hp.F90:456-461), scaled.
@@ -70,8 +107,13 @@ __global__ void surface_rhs_kernel(const double* __restrict__ q2, int nr, int nc
 // out = beta*B - C X for the channel-diagonal part of C (kinetic, centrifugal, threshold,
 // closed-channel Bloch).  grid (ceil(nr/32), nch, ceil(ncol/8)), block (32, 8).
 // B is blockdiag(q2) (only when with_b != 0).
+// absmode != 0 instead forms |B| + |C_diag| |X| (moduli, real part only): the scale of the
+// rounding error of the residual.
+// With with_b the sums are compensated (Acc2); their low words go to lo_out (same layout as
+// out) when it is given, for resid_coupling_kernel to finish the compensated residual.
 __global__ void resid_kinetic_kernel(MeshDev mesh, ChannelData ch, const double2* __restrict__ X,
-                                     long ldx, int ncol, double2* out, long ldo, int with_b) {
+                                     long ldx, int ncol, double2* out, long ldo, int with_b, int absmode,
+                                     double2* lo_out) {
   const int nr = mesh.nr;
   const int i = blockIdx.x * 32 + threadIdx.x;
   const int c = blockIdx.y;
@@ -80,26 +122,71 @@ __global__ void resid_kinetic_kernel(MeshDev mesh, ChannelData ch, const double2
   const double bl = ch.bloch[c];
   const double2* xc = X + (size_t)col * ldx + (size_t)c * nr;
   double ar = 0.0, ai = 0.0;
+  const double rr = mesh.r[i];
+  const double d = ch.fac[c] / (rr * rr) + ch.kk[c];
+  const double br = (with_b && c == col) ? mesh.q2[i] : 0.0;
+  if (absmode) {
+    for (int j = 0; j < nr; ++j) {
+      double k = mesh.tc[i + (size_t)j * nr] - bl * mesh.blo0[i + (size_t)j * nr];
+      if (j == i) k += d;
+      double2 x = __ldg(xc + j);
+      ar = fma(fabs(k), hypot(x.x, x.y), ar);
+    }
+    out[(size_t)(c * nr + i) + (size_t)col * ldo] = make_double2(fabs(br) + ar, 0.0);
+    return;
+  }
+  if (with_b) {
+    // outer residual: compensated sums, B - sum starting from B
+    Acc2 sr, si;
+    sr.add(br);
+    for (int j = 0; j < nr; ++j) {
+      double k = mesh.tc[i + (size_t)j * nr] - bl * mesh.blo0[i + (size_t)j * nr];
+      double2 x = __ldg(xc + j);
+      sr.add_prod(-k, x.x);
+      si.add_prod(-k, x.y);
+    }
+    double2 xi = xc[i];
+    sr.add_prod(-d, xi.x);
+    si.add_prod(-d, xi.y);
+    // the low words ride along in a second output slot: (value, low part) packed by the caller
+    out[(size_t)(c * nr + i) + (size_t)col * ldo] = make_double2(sr.hi, si.hi);
+    if (lo_out) lo_out[(size_t)(c * nr + i) + (size_t)col * ldo] = make_double2(sr.lo, si.lo);
+    return;
+  }
   for (int j = 0; j < nr; ++j) {
     double k = mesh.tc[i + (size_t)j * nr] - bl * mesh.blo0[i + (size_t)j * nr];
     double2 x = __ldg(xc + j);
     ar = fma(k, x.x, ar);
     ai = fma(k, x.y, ai);
   }
-  const double rr = mesh.r[i];
-  const double d = ch.fac[c] / (rr * rr) + ch.kk[c];
   double2 xi = xc[i];
   ar = fma(d, xi.x, ar);
   ai = fma(d, xi.y, ai);
-  double br = (with_b && c == col) ? mesh.q2[i] : 0.0;
   out[(size_t)(c * nr + i) + (size_t)col * ldo] = make_double2(br - ar, -ai);
 }
 
-// out -= V X for the coupling part: (V X)[(c,i), col] = sum_c' cpot(r_i, c, c') X[(c',i), col].
-// grid (nr, ceil(ncol/CT)), block 256: thread -> (channel c, column).
-__global__ void resid_coupling_kernel(int nr, int nch, const double2* __restrict__ cpot, long ncp1,
-                                      long ndim, const double2* __restrict__ X, long ldx, int ncol,
-                                      double2* out, long ldo) {
+// Potential re-laid out per mesh point: vt[(i*nch + c')*nch + c] = cpot(r_i, c, c'), so the
+// coupling residual reads it with consecutive channels in consecutive threads.
+__global__ void cpot_transpose_kernel(const double2* __restrict__ cpot, long ncp1, long ndim, int nr, int nch,
+                                      double2* vt) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long total = (long)nr * nch * nch;
+  if (idx >= total) return;
+  const int c = (int)(idx % nch);
+  const int cp = (int)((idx / nch) % nch);
+  const int i = (int)(idx / ((long)nch * nch));
+  vt[idx] = cpot[(size_t)i + ncp1 * ((size_t)c + ndim * (size_t)cp)];
+}
+
+// out -= V X for the coupling part: (V X)[(c,i), col] = sum_c' cpot(r_i, c, c') X[(c',i), col]
+// with V read from the per-point layout of cpot_transpose_kernel.  absmode != 0 adds
+// |V| |X| to the real part instead.  grid (nr, ceil(ncol/32)), block 256: thread ->
+// (channel c, column).
+// With lo (low words from resid_kinetic_kernel) the coupling sums are compensated too and
+// the result is rounded once: out = hi + lo.
+__global__ void resid_coupling_kernel(int nr, int nch, const double2* __restrict__ vt, const double2* __restrict__ X,
+                                      long ldx, int ncol, double2* out, long ldo, int absmode,
+                                      const double2* __restrict__ lo) {
   extern __shared__ double2 xs[];  // [ncol_tile][nch] X values at radial point i
   const int i = blockIdx.x;
   const int ct = 32;
@@ -110,18 +197,48 @@ __global__ void resid_coupling_kernel(int nr, int nch, const double2* __restrict
     xs[cc * nch + cp] = X[(size_t)(cp * nr + i) + (size_t)(col0 + cc) * ldx];
   }
   __syncthreads();
+  const double2* vi = vt + (size_t)i * nch * nch;
   for (int idx = threadIdx.x; idx < ncl * nch; idx += blockDim.x) {
     int c = idx % nch, cc = idx / nch;
     double ar = 0.0, ai = 0.0;
+    if (absmode) {
+      for (int cp = 0; cp < nch; ++cp) {
+        double2 v = __ldg(vi + (size_t)cp * nch + c);
+        double2 x = xs[cc * nch + cp];
+        ar = fma(hypot(v.x, v.y), hypot(x.x, x.y), ar);
+      }
+      double2* p = out + (size_t)(c * nr + i) + (size_t)(col0 + cc) * ldo;
+      p->x += ar;
+      continue;
+    }
+    double2* p = out + (size_t)(c * nr + i) + (size_t)(col0 + cc) * ldo;
+    if (lo) {
+      const double2 l = lo[(size_t)(c * nr + i) + (size_t)(col0 + cc) * ldo];
+      Acc2 sr, si;
+      double2 o = *p;
+      sr.hi = o.x;
+      sr.lo = l.x;
+      si.hi = o.y;
+      si.lo = l.y;
+      for (int cp = 0; cp < nch; ++cp) {
+        double2 v = __ldg(vi + (size_t)cp * nch + c);
+        double2 x = xs[cc * nch + cp];
+        sr.add_prod(-v.x, x.x);
+        sr.add_prod(v.y, x.y);
+        si.add_prod(-v.x, x.y);
+        si.add_prod(-v.y, x.x);
+      }
+      *p = make_double2(sr.value(), si.value());
+      continue;
+    }
     for (int cp = 0; cp < nch; ++cp) {
-      double2 v = __ldg(cpot + (size_t)i + ncp1 * ((size_t)c + ndim * (size_t)cp));
+      double2 v = __ldg(vi + (size_t)cp * nch + c);
       double2 x = xs[cc * nch + cp];
       ar = fma(v.x, x.x, ar);
       ar = fma(-v.y, x.y, ar);
       ai = fma(v.x, x.y, ai);
       ai = fma(v.y, x.x, ai);
     }
-    double2* p = out + (size_t)(c * nr + i) + (size_t)(col0 + cc) * ldo;
     double2 o = *p;
     o.x -= ar;
     o.y -= ai;
@@ -174,6 +291,26 @@ __global__ void copy_d_kernel(const double2* __restrict__ src, long lds, double2
   if (r >= N) return;
   dst[(size_t)r + (size_t)col * ldd] = src[(size_t)r + (size_t)col * lds];
 }
+// ||A||_F^2 of a dense FP64 complex matrix (column-major), accumulated into *fro2.
+__global__ void fro2_kernel(const double2* __restrict__ A, long lda, int N, double* fro2) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int col = blockIdx.y;
+  double sq = 0.0;
+  if (r < N) {
+    double2 v = A[(size_t)r + (size_t)col * lda];
+    sq = v.x * v.x + v.y * v.y;
+  }
+  for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    sq = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+    if (threadIdx.x == 0 && sq != 0.0) atomicAdd(fro2, sq);
+  }
+}
+
 __global__ void d2f_matrix_kernel(const double2* __restrict__ src, long lds, float2* dst, long ldd, int N) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   const int col = blockIdx.y;
@@ -189,6 +326,19 @@ __global__ void d2f_matrix_kernel(const double2* __restrict__ src, long lds, flo
 //   least-squares problem are updated.  V: (m+1) blocks of N x ncol, w is V_{j+1}'s slot.
 // Per-column state (double): hess[(m+1) x m complex], cs[m] (real), sn[m] (complex),
 // g[m+1] (complex).
+constexpr int kGmresMaxM = 16;  // longest FGMRES cycle
+
+// Per column |g_{j+1}| / beta: the cycle's residual reduction so far (for the host's
+// stopping test).  One thread per column.
+__global__ void gmres_estimate_kernel(const double2* __restrict__ g, const double* __restrict__ beta, int m, int j,
+                                      int ncol, double* out) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncol) return;
+  double2 v = g[(size_t)col * (m + 1) + j + 1];
+  double b = beta[col];
+  out[col] = b > 0 ? hypot(v.x, v.y) / b : 0.0;
+}
+
 struct GmresState {
   double2* V;     // [(m+1)][ldv * ncol]
   long ldv;
@@ -197,6 +347,7 @@ struct GmresState {
   double* cs;     // [ncol][m]
   double2* sn;    // [ncol][m]
   double2* g;     // [ncol][m+1]
+  double* beta;   // [ncol] initial residual norm of each column
   int m, N, ncol;
 };
 
@@ -238,13 +389,14 @@ __global__ void __launch_bounds__(NT) gmres_start_kernel(GmresState s) {
     double2 x = v[r];
     v[r] = make_double2(x.x * inv, x.y * inv);
   }
-  if (threadIdx.x <= s.m) s.g[(size_t)col * (s.m + 1) + threadIdx.x] = make_double2(threadIdx.x == 0 ? beta : 0.0, 0.0);
+  for (int i = threadIdx.x; i <= s.m; i += NT) s.g[(size_t)col * (s.m + 1) + i] = make_double2(i == 0 ? beta : 0.0, 0.0);
+  if (threadIdx.x == 0) s.beta[col] = beta;
 }
 
 template <int NT>
 __global__ void __launch_bounds__(NT) gmres_arnoldi_kernel(GmresState s, int j) {
   __shared__ double2 red[33];
-  __shared__ double2 h[16];
+  __shared__ double2 h[kGmresMaxM + 1];
   const int col = blockIdx.x;
   const int m = s.m;
   double2* w = s.V + (size_t)(j + 1) * s.vstride + (size_t)col * s.ldv;
@@ -287,7 +439,7 @@ __global__ void __launch_bounds__(NT) gmres_arnoldi_kernel(GmresState s, int j) 
     double* cs = s.cs + (size_t)col * m;
     double2* sn = s.sn + (size_t)col * m;
     double2* g = s.g + (size_t)col * (m + 1);
-    double2 hc[17];
+    double2 hc[kGmresMaxM + 1];
     for (int i = 0; i <= j; ++i) hc[i] = h[i];
     hc[j + 1] = make_double2(breakdown ? 0.0 : hn, 0.0);
     // apply previous rotations: [c s; -conj(s) c]
@@ -335,7 +487,7 @@ __global__ void __launch_bounds__(NT) gmres_arnoldi_kernel(GmresState s, int j) 
 template <int NT>
 __global__ void __launch_bounds__(NT) gmres_update_kernel(GmresState s, int jdone, const double2* Z, long zstride,
                                                           long ldz, double2* X, long ldx, double sign) {
-  __shared__ double2 y[16];
+  __shared__ double2 y[kGmresMaxM];
   const int col = blockIdx.x;
   const int m = s.m;
   if (threadIdx.x == 0) {
@@ -367,6 +519,31 @@ __global__ void __launch_bounds__(NT) gmres_update_kernel(GmresState s, int jdon
       acc.y += sign * (y[i].x * z.y + y[i].y * z.x);
     }
     x[r] = acc;
+  }
+}
+
+// |a - b|^2 and |a|^2 of two complex vectors (one CTA): out[0], out[1].
+__global__ void rel_change_kernel(const double2* __restrict__ a, const double2* __restrict__ b, int n, double* out) {
+  double d = 0.0, s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double2 x = a[i], y = b[i];
+    double dx = x.x - y.x, dy = x.y - y.y;
+    d = fma(dx, dx, fma(dy, dy, d));
+    s = fma(x.x, x.x, fma(x.y, x.y, s));
+  }
+  __shared__ double rd[32], rs[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    d += __shfl_down_sync(0xffffffffu, d, o);
+    s += __shfl_down_sync(0xffffffffu, s, o);
+  }
+  if ((threadIdx.x & 31) == 0) { rd[threadIdx.x >> 5] = d; rs[threadIdx.x >> 5] = s; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    d = 0.0;
+    s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { d += rd[w]; s += rs[w]; }
+    out[0] = d;
+    out[1] = s;
   }
 }
 

@@ -48,7 +48,11 @@ static int fail(int status, const char* fmt, ...) {
     if (_s != HPRMAT_B200_OK) return _s; \
   } while (0)
 
-#define LAUNCH_CHECK() HPR_CUDA_TRY(cudaGetLastError())
+#define LAUNCH_CHECK()        \
+  do {                        \
+    ++c->launches;            \
+    HPR_CUDA_TRY(cudaGetLastError()); \
+  } while (0)
 
 // ------------------------------------------------------------------ device buffers
 struct DevBuf {
@@ -77,7 +81,8 @@ struct DevBuf {
 };
 
 static constexpr int kSwapStride = 3 * kMaxNB + 4;  // ints per step in the swap store
-static constexpr int kGmresM = 3;                    // inner FGMRES iterations per outer step
+static constexpr int kGmresM = 12;                   // longest FGMRES cycle per outer step
+static constexpr double kInnerTol = 1e-7;            // cycle stops once the residual fell this much
 
 struct hprmat_b200_ctx {
   int device = 0;
@@ -93,10 +98,23 @@ struct hprmat_b200_ctx {
   DevBuf mesh;  // tc | blo0 | r | q2
   // work buffers
   DevBuf W, A64, X, X64, R64, B64, V, Z, gm, swaps, ipiv, stage, status, ops, inv, chan, rmat,
-      zwork, cpot, cu, norms;
+      zwork, cpot, cu, norms, lup, rop, rsurf, vt, rlo;
+  // tensor-core operand views of the current factorisation (mixed path)
+  TcOperand op_lu, op_bop, op_rhs;
+  long lup_ld = 0, lup_plane = 0, rop_plane = 0;
+  int rop_nrhs = 0;
   int* h_status = nullptr;  // pinned
   double* h_norms = nullptr;  // pinned
   TcGemmPlan tcplan;
+  // counters for benchmarks: kernel launches issued, and (when profiling) CUDA-event
+  // time and algorithmic flops of the tensor-core trailing updates
+  unsigned long long launches = 0;
+  bool profile = false;
+  std::vector<cudaEvent_t> ev;
+  int ev_used = 0;
+  std::vector<double> ev_flops;
+  double tc_ms = 0.0, tc_flops = 0.0;
+  int tc_launches = 0;
 };
 
 // ------------------------------------------------------------------ mesh (rmat_ini)
@@ -269,14 +287,22 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
   T* rowj = reinterpret_cast<T*>(sp);
   unsigned* growth = reinterpret_cast<unsigned*>(status + SW_COUNT - 1);
 
-  float* aop = nullptr;
   float* bop = nullptr;
   long plane = 0;
   if (mixed) {
+    // B operand of the trailing update (U12, K-major per column) and the LU planes
     plane = (long)(N + 256) * NB;
-    TRY(c->ops.ensure((size_t)8 * plane * sizeof(float)));
-    aop = c->ops.as<float>();
-    bop = aop + 4 * plane;
+    TRY(c->ops.ensure((size_t)4 * plane * sizeof(float)));
+    bop = c->ops.as<float>();
+    c->lup_ld = (N + 3) / 4 * 4;
+    c->lup_plane = c->lup_ld * (long)N;
+    TRY(c->lup.ensure((size_t)4 * c->lup_plane * sizeof(float)));
+    if (N > NB) {  // views are used only when there is more than one block step
+      if (tc_make_operand(c->tcplan, c->op_lu, c->lup.as<float>(), N, N, c->lup_ld, c->lup_plane, 128))
+        return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+      if (tc_make_operand(c->tcplan, c->op_bop, bop, NB, N, NB, plane, 256))
+        return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+    }
   }
 
   auto pk = panel_kernel<T, NB, NT>;
@@ -309,10 +335,12 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
     pa.sw.extra_src = swb + 2 * kMaxNB;
     pa.sw.n_extra = swb + 3 * kMaxNB;
     pa.growth_bits = growth;
-    pa.aop = (mixed && k0 + ncols < N) ? aop : nullptr;
-    pa.aop_plane = plane;
+    pa.lup = (mixed && k0 + ncols < N) ? c->lup.as<float>() : nullptr;
+    pa.lup_ld = c->lup_ld;
+    pa.lup_plane = c->lup_plane;
     void* args[] = {&pa};
     HPR_CUDA_TRY(cudaLaunchCooperativeKernel((void*)pk, dim3(G), dim3(NT), args, smem, c->stream));
+    ++c->launches;
     if (k0 + ncols >= N) break;
     // row interchanges + U12 = L11^-1 A12
     {
@@ -337,14 +365,27 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
       ta.bop_plane = plane;
       ta.bop_col0 = k0 + ncols;
       ta.growth_bits = growth;
+      ta.lup = mixed ? c->lup.as<float>() : nullptr;
+      ta.lup_ld = c->lup_ld;
+      ta.lup_plane = c->lup_plane;
       tk<<<cdiv_u(N - k0 - ncols, CW), NT, tsm, c->stream>>>(ta);
       LAUNCH_CHECK();
     }
     // trailing update A22 -= L21 U12
     const int M2 = N - k0 - ncols;
     if (mixed) {
-      TRY(tc_trailing_update(c->tcplan, aop, bop, plane, NB, ncols, reinterpret_cast<float2*>(W) + (k0 + ncols) + (size_t)(k0 + ncols) * ld,
-                             ld, M2, M2, c->stream));
+      const bool prof = c->profile && c->ev_used + 2 <= (int)c->ev.size();
+      if (prof) HPR_CUDA_TRY(cudaEventRecord(c->ev[c->ev_used], c->stream));
+      if (tc_update(c->tcplan, c->op_lu, k0, k0 + ncols, c->op_bop, 0, 0, NB,
+                    reinterpret_cast<float2*>(W) + (k0 + ncols) + (size_t)(k0 + ncols) * ld, ld, M2, M2, 256,
+                    c->stream))
+        return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+      ++c->launches;
+      if (prof) {
+        HPR_CUDA_TRY(cudaEventRecord(c->ev[c->ev_used + 1], c->stream));
+        c->ev_flops.push_back(8.0 * (double)M2 * (double)M2 * (double)NB);
+        c->ev_used += 2;
+      }
     } else {
       dim3 grid(cdiv_u(M2, 64), cdiv_u(M2, 64));
       cgemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(M2, M2, ncols, W + (k0 + ncols) + (size_t)k0 * ld, ld,
@@ -367,6 +408,17 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
   if (c->h_status[SW_TIMEOUT] != 0)
     return fail(HPRMAT_B200_ERR_TIMEOUT, "panel factorisation: grid barrier wait limit exceeded (site %d)",
                 c->h_status[SW_TIMEOUT]);
+  if (c->profile) {
+    for (int i = 0; i + 1 < c->ev_used; i += 2) {
+      float ms = 0.f;
+      HPR_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev[i], c->ev[i + 1]));
+      c->tc_ms += ms;
+      c->tc_flops += c->ev_flops[i / 2];
+      ++c->tc_launches;
+    }
+    c->ev_used = 0;
+    c->ev_flops.clear();
+  }
   if (mixed) {
     int err = 0;
     TRY(tc_gemm_check(c->tcplan, c->stream, &err));
@@ -389,19 +441,16 @@ static int factor(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, int nb, 
 // Forward and backward substitution with the stored factors, in place on X (N x nrhs).
 template <typename T, int NB>
 static int lu_solve_impl(hprmat_b200_ctx* c, const T* W, const LUState& st, T* X, long ldx, int nrhs) {
-  constexpr int NT = 256, CW = 8;
   const int N = st.N;
   const long ld = st.ld;
   const T* inv = c->inv.as<T>();
-  auto dk = diag_apply_kernel<T, NB, CW, NT>;
-  size_t dsm = (size_t)CW * (NB + 1) * sizeof(T) + (size_t)CW * NB * sizeof(T);
-  TRY(set_smem(dk, dsm));
+  auto dk = diag_apply_kernel<T, NB>;
   const int* swb = c->swaps.as<int>();
   for (int s = 0; s < st.nsteps; ++s) {
     const int k0 = s * NB, ncols = std::min(NB, N - k0);
     const int* sw = swb + (size_t)s * kSwapStride;
-    dk<<<cdiv_u(nrhs, CW), NT, dsm, c->stream>>>(inv + (size_t)2 * s * NB * NB, ncols, k0, sw, sw + kMaxNB,
-                                                 sw + 2 * kMaxNB, sw + 3 * kMaxNB, X, ldx, nrhs);
+    dk<<<nrhs, NB, 0, c->stream>>>(inv + (size_t)2 * s * NB * NB, ncols, k0, sw, sw + kMaxNB, sw + 2 * kMaxNB,
+                                   sw + 3 * kMaxNB, X, ldx, nrhs, nullptr, 0);
     LAUNCH_CHECK();
     const int M2 = N - k0 - ncols;
     if (M2 > 0) {
@@ -413,8 +462,8 @@ static int lu_solve_impl(hprmat_b200_ctx* c, const T* W, const LUState& st, T* X
   }
   for (int s = st.nsteps - 1; s >= 0; --s) {
     const int k0 = s * NB, ncols = std::min(NB, N - k0);
-    dk<<<cdiv_u(nrhs, CW), NT, dsm, c->stream>>>(inv + ((size_t)2 * s + 1) * NB * NB, ncols, k0, nullptr,
-                                                 nullptr, nullptr, nullptr, X, ldx, nrhs);
+    dk<<<nrhs, NB, 0, c->stream>>>(inv + ((size_t)2 * s + 1) * NB * NB, ncols, k0, nullptr, nullptr, nullptr,
+                                   nullptr, X, ldx, nrhs, nullptr, 0);
     LAUNCH_CHECK();
     if (k0 > 0) {
       dim3 grid(cdiv_u(k0, 64), cdiv_u(nrhs, 64));
@@ -424,6 +473,64 @@ static int lu_solve_impl(hprmat_b200_ctx* c, const T* W, const LUState& st, T* X
     }
   }
   return HPRMAT_B200_OK;
+}
+
+// Mixed path: the same blocked substitution with the block updates on the tensor cores.
+// Each diagonal block (explicit inverse) also emits its result as the B operand; the update
+// reads L21 / U12 from the LU planes.
+template <int NB>
+static int lu_solve_tc_impl(hprmat_b200_ctx* c, const LUState& st, float2* X, long ldx, int nrhs) {
+  const int N = st.N;
+  const float2* inv = c->inv.as<float2>();
+  auto dk = diag_apply_kernel<float2, NB>;
+  const int npad = (nrhs + 127) / 128 * 128;
+  if (c->rop_nrhs != npad || !c->rop.p) {
+    c->rop_plane = (long)npad * NB;
+    TRY(c->rop.ensure((size_t)4 * c->rop_plane * sizeof(float)));
+    HPR_CUDA_TRY(cudaMemsetAsync(c->rop.p, 0, (size_t)4 * c->rop_plane * sizeof(float), c->stream));
+    if (tc_make_operand(c->tcplan, c->op_rhs, c->rop.as<float>(), NB, npad, NB, c->rop_plane, 128))
+      return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+    c->rop_nrhs = npad;
+  }
+  float* rop = c->rop.as<float>();
+  const int* swb = c->swaps.as<int>();
+  for (int s = 0; s < st.nsteps; ++s) {
+    const int k0 = s * NB, ncols = std::min(NB, N - k0);
+    const int* sw = swb + (size_t)s * kSwapStride;
+    const int M2 = N - k0 - ncols;
+    dk<<<nrhs, NB, 0, c->stream>>>(inv + (size_t)2 * s * NB * NB, ncols, k0, sw, sw + kMaxNB, sw + 2 * kMaxNB,
+                                   sw + 3 * kMaxNB, X, ldx, nrhs, M2 > 0 ? rop : nullptr, c->rop_plane);
+    LAUNCH_CHECK();
+    if (M2 > 0) {
+      if (tc_update(c->tcplan, c->op_lu, k0, k0 + ncols, c->op_rhs, 0, 0, (ncols + 15) / 16 * 16, X + k0 + ncols,
+                    ldx, M2, nrhs, 128, c->stream))
+        return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+      ++c->launches;
+    }
+  }
+  for (int s = st.nsteps - 1; s >= 0; --s) {
+    const int k0 = s * NB, ncols = std::min(NB, N - k0);
+    dk<<<nrhs, NB, 0, c->stream>>>(inv + ((size_t)2 * s + 1) * NB * NB, ncols, k0, nullptr, nullptr, nullptr,
+                                   nullptr, X, ldx, nrhs, k0 > 0 ? rop : nullptr, c->rop_plane);
+    LAUNCH_CHECK();
+    if (k0 > 0) {
+      if (tc_update(c->tcplan, c->op_lu, k0, 0, c->op_rhs, 0, 0, (ncols + 15) / 16 * 16, X, ldx, k0, nrhs, 128,
+                    c->stream))
+        return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+      ++c->launches;
+    }
+  }
+  return HPRMAT_B200_OK;
+}
+
+static int lu_solve_tc(hprmat_b200_ctx* c, const LUState& st, float2* X, long ldx, int nrhs) {
+  switch (st.nb) {
+    case 128: return lu_solve_tc_impl<128>(c, st, X, ldx, nrhs);
+    case 64: return lu_solve_tc_impl<64>(c, st, X, ldx, nrhs);
+    case 32: return lu_solve_tc_impl<32>(c, st, X, ldx, nrhs);
+    case 16: return lu_solve_tc_impl<16>(c, st, X, ldx, nrhs);
+  }
+  return fail(HPRMAT_B200_ERR_UNSUPPORTED, "unsupported block size %d", st.nb);
 }
 
 template <typename T>
@@ -446,28 +553,38 @@ struct Operator {
   MeshDev mesh;
   ChannelData ch;
   int nch = 0;
-  const double2* cpot = nullptr;
-  long ncp1 = 0, ndim = 0;
+  const double2* vt = nullptr;  // potential per mesh point (cpot_transpose_kernel layout)
   // dense
   const double2* A = nullptr;
   long lda = 0;
   const double2* B = nullptr;  // dense right-hand side (N x nrhs, ld = ldb)
   long ldb = 0;
   int N = 0;
+  // R-matrix problems: surface projection R = q2^T X per channel block, for the stopping rule
+  const double* q2 = nullptr;
+  int nr = 0;
 };
 
+// absmode: out = |B| + |C| |X| instead (structured operator only).
 static int apply_residual(hprmat_b200_ctx* c, const Operator& op, const double2* X, long ldx, int ncol,
-                          double2* out, long ldo, bool with_b) {
+                          double2* out, long ldo, bool with_b, bool absmode = false) {
   const int N = op.N;
   if (op.structured) {
     const int nr = op.mesh.nr;
+    // the outer residual (with B) is formed with compensated sums; low words in R64
+    double2* lo = nullptr;
+    if (with_b && !absmode) {
+      TRY(c->rlo.ensure((size_t)ldo * ncol * sizeof(double2)));
+      lo = c->rlo.as<double2>();
+    }
     dim3 g1(cdiv_u(nr, 32), op.nch, cdiv_u(ncol, 8));
-    resid_kinetic_kernel<<<g1, dim3(32, 8), 0, c->stream>>>(op.mesh, op.ch, X, ldx, ncol, out, ldo, with_b ? 1 : 0);
+    resid_kinetic_kernel<<<g1, dim3(32, 8), 0, c->stream>>>(op.mesh, op.ch, X, ldx, ncol, out, ldo, with_b ? 1 : 0,
+                                                            absmode ? 1 : 0, lo);
     LAUNCH_CHECK();
     size_t sm = (size_t)32 * op.nch * sizeof(double2);
     TRY(set_smem(resid_coupling_kernel, sm));
     dim3 g2(nr, cdiv_u(ncol, 32));
-    resid_coupling_kernel<<<g2, 256, sm, c->stream>>>(nr, op.nch, op.cpot, op.ncp1, op.ndim, X, ldx, ncol, out, ldo);
+    resid_coupling_kernel<<<g2, 256, sm, c->stream>>>(nr, op.nch, op.vt, X, ldx, ncol, out, ldo, absmode ? 1 : 0, lo);
     LAUNCH_CHECK();
   } else {
     dim3 g0(cdiv_u(N, 256), ncol);
@@ -502,7 +619,7 @@ static int frob_norm(hprmat_b200_ctx* c, const double2* X, long ldx, int N, int 
 // kGmresM flexible-GMRES iterations on C d = r, preconditioned by the FP32 LU solve, and
 // X += d.  Returns NOT_CONVERGED if max_refine outer corrections did not reach tol.
 static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W32, const LUState& st,
-                        double2* X64, long ldx, int nrhs, double bnorm, hprmat_b200_stats* stats) {
+                        double2* X64, long ldx, int nrhs, double bnorm, double cnorm, hprmat_b200_stats* stats) {
   const int N = op.N;
   const int m = kGmresM;
   const long ldv = st.ld;
@@ -510,7 +627,7 @@ static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W3
   TRY(c->V.ensure((size_t)(m + 1) * vstride * sizeof(double2)));
   TRY(c->Z.ensure((size_t)m * vstride * sizeof(double2)));
   TRY(c->gm.ensure((size_t)nrhs * ((m + 1) * m * sizeof(double2) + m * sizeof(double) + m * sizeof(double2) +
-                                   (m + 1) * sizeof(double2)) + 256));
+                                   (m + 1) * sizeof(double2) + 2 * sizeof(double)) + 256));
   TRY(c->X.ensure((size_t)ldv * nrhs * sizeof(float2)));
   double2* V = c->V.as<double2>();
   double2* Z = c->Z.as<double2>();
@@ -527,42 +644,116 @@ static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W3
   gs.g = reinterpret_cast<double2*>(gp);
   gp += (size_t)nrhs * (m + 1) * sizeof(double2);
   gs.cs = reinterpret_cast<double*>(gp);
+  gp += (size_t)nrhs * m * sizeof(double);
+  gs.beta = reinterpret_cast<double*>(gp);
+  gp += (size_t)nrhs * sizeof(double);
+  double* d_est = reinterpret_cast<double*>(gp);
   gs.m = m;
   gs.N = N;
   gs.ncol = nrhs;
   dim3 gconv(cdiv_u(N, 256), nrhs);
   int steps = 0;
   int status = HPRMAT_B200_OK;
+  double prev_rel = 0.0, prev_change = 0.0, floor_rel = 0.0, last_est = 1.0;
+  int inner_total = 0;
+  const bool surf = op.q2 != nullptr;
+  const int nchs = surf ? N / op.nr : 0;
+  if (surf) TRY(c->rsurf.ensure((size_t)2 * nchs * nchs * sizeof(double2) + 64));
+  (void)cnorm;
+  if (stats) stats->surface_change = -1.0;
   for (int outer = 0;; ++outer) {
     TRY(apply_residual(c, op, X64, ldx, nrhs, V, ldv, true));
     double rn;
     TRY(frob_norm(c, V, ldv, N, nrhs, &rn));
-    double rel = rn / bnorm;
+    const double rel = rn / bnorm;
+    double change = -1.0;
+    if (surf) {
+      // R of the current iterate into slot (outer & 1); compare with the previous one
+      double2* Rn = c->rsurf.as<double2>() + (size_t)(outer & 1) * nchs * nchs;
+      rmat_extract_kernel<<<dim3(nchs, cdiv_u(nchs, 128)), 128, 0, c->stream>>>(X64, ldx, op.q2, op.nr, nchs, 1.0, Rn);
+      LAUNCH_CHECK();
+      if (outer > 0) {
+        const double2* Ro = c->rsurf.as<double2>() + (size_t)((outer - 1) & 1) * nchs * nchs;
+        TRY(c->norms.ensure(2 * sizeof(double) * 2));
+        rel_change_kernel<<<1, 256, 0, c->stream>>>(Rn, Ro, nchs * nchs, c->norms.as<double>());
+        LAUNCH_CHECK();
+        HPR_CUDA_TRY(cudaMemcpyAsync(c->h_norms, c->norms.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        change = c->h_norms[1] > 0 ? sqrt(c->h_norms[0] / c->h_norms[1]) : 0.0;
+      }
+    }
+    if (op.structured) {
+      // rounding scale of the residual at the current iterate: u || |B| + |C||X| ||_F / ||B||_F
+      TRY(apply_residual(c, op, X64, ldx, nrhs, V + vstride, ldv, true, true));
+      double fn;
+      TRY(frob_norm(c, V + vstride, ldv, N, nrhs, &fn));
+      floor_rel = 1.1102230246251565e-16 * fn / bnorm;
+      if (stats && outer < 9) stats->floor_history[outer] = floor_rel;
+    }
     if (stats && outer < 9) stats->residual_history[outer] = rel;
-    if (stats) stats->rel_residual = rel;
-    if (!(rel >= c->opts.tol)) break;  // converged (also stops on rel == 0)
+    if (stats) {
+      stats->rel_residual = rel;
+      stats->surface_change = change;
+      stats->residual_floor = floor_rel;
+    }
+    if (!(rel >= c->opts.tol)) break;  // converged (also on rel == 0)
+    if (surf && outer > 0) {
+      // change = size of the last correction in R, i.e. the error of the previous iterate;
+      // the last cycle reduced that error by about last_est, which predicts the error left.
+      // (the GMRES estimate bounds the residual, not the error in R: keep a wide margin)
+      const double predicted = change * std::max(last_est, 1e-16);
+      if (!(change >= c->opts.surface_tol) || 1e3 * predicted < c->opts.surface_tol) break;
+      if (outer >= 2 && change > 0.5 * prev_change) {  // no longer improving
+        if (predicted > 1e-8) status = HPRMAT_B200_NOT_CONVERGED;
+        break;
+      }
+    } else if (!surf && outer >= 1 && rel > 0.5 * prev_rel) {  // dense operator: residual stalled
+      if (rel > 1e-8) status = HPRMAT_B200_NOT_CONVERGED;
+      break;
+    }
     if (outer >= c->opts.max_refine) {
       status = HPRMAT_B200_NOT_CONVERGED;
       break;
     }
+    prev_rel = rel;
+    prev_change = change;
     gmres_start_kernel<256><<<nrhs, 256, 0, c->stream>>>(gs);
     LAUNCH_CHECK();
+    // the first cycle starts from the FP32 solution; later cycles only polish
+    const double inner_tol = outer == 0 ? kInnerTol : 1e-2;
+    int jdone = 0;
+    double est = 1.0;
     for (int j = 0; j < m; ++j) {
       d2f_kernel<<<gconv, 256, 0, c->stream>>>(V + (size_t)j * vstride, ldv, X32, ldv, N, nullptr);
       LAUNCH_CHECK();
-      TRY(lu_solve<float2>(c, W32, st, X32, ldv, nrhs));
+      TRY(lu_solve_tc(c, st, X32, ldv, nrhs));
       f2d_kernel<<<gconv, 256, 0, c->stream>>>(X32, ldv, Z + (size_t)j * vstride, ldv, N, nullptr);
       LAUNCH_CHECK();
       // V_{j+1} = -C Z_j: FGMRES runs on the operator -C, so the correction is subtracted
       TRY(apply_residual(c, op, Z + (size_t)j * vstride, ldv, nrhs, V + (size_t)(j + 1) * vstride, ldv, false));
       gmres_arnoldi_kernel<256><<<nrhs, 256, 0, c->stream>>>(gs, j);
       LAUNCH_CHECK();
+      jdone = j + 1;
+      // residual estimate of the cycle (worst column) from the Givens-rotated right side
+      gmres_estimate_kernel<<<cdiv_u(nrhs, 128), 128, 0, c->stream>>>(gs.g, gs.beta, m, j, nrhs, d_est);
+      LAUNCH_CHECK();
+      HPR_CUDA_TRY(cudaMemcpyAsync(c->h_norms, d_est, (size_t)nrhs * sizeof(double), cudaMemcpyDeviceToHost,
+                                   c->stream));
+      HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+      est = 0.0;
+      for (int q = 0; q < nrhs; ++q) est = std::max(est, c->h_norms[q]);
+      if (est < inner_tol) break;
     }
-    gmres_update_kernel<256><<<nrhs, 256, 0, c->stream>>>(gs, m, Z, vstride, ldv, X64, ldx, -1.0);
+    last_est = est;
+    gmres_update_kernel<256><<<nrhs, 256, 0, c->stream>>>(gs, jdone, Z, vstride, ldv, X64, ldx, -1.0);
     LAUNCH_CHECK();
+    inner_total += jdone;
     ++steps;
   }
-  if (stats) stats->refine_steps = steps;
+  if (stats) {
+    stats->refine_steps = steps;
+    stats->inner_iterations = inner_total;
+  }
   return status;
 }
 
@@ -675,10 +866,16 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
   op.mesh = md;
   op.ch = chd;
   op.nch = nch;
-  op.cpot = d_cpot;
-  op.ncp1 = ncp1;
-  op.ndim = ndim;
   op.N = N;
+  TRY(c->vt.ensure((size_t)nr * nch * nch * sizeof(double2)));
+  {
+    const long tot = (long)nr * nch * nch;
+    cpot_transpose_kernel<<<cdiv_u(tot, 256), 256, 0, c->stream>>>(d_cpot, ncp1, ndim, nr, nch, c->vt.as<double2>());
+    LAUNCH_CHECK();
+  }
+  op.vt = c->vt.as<double2>();
+  op.q2 = md.q2;
+  op.nr = nr;
   // |B|_F of blockdiag(q2)
   double q2n = 0.0;
   for (int i = 0; i < nr; ++i) q2n += c->q2[i] * c->q2[i];
@@ -687,11 +884,13 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
   int status = HPRMAT_B200_OK;
   dim3 ga(cdiv_u(N, 256), N);
   dim3 gr(cdiv_u(N, 256), nch);
+  double* d_fro2 = reinterpret_cast<double*>(c->status.as<int>() + 32);
+  HPR_CUDA_TRY(cudaMemsetAsync(d_fro2, 0, sizeof(double), c->stream));
   auto t0 = Clock::now();
   if (!mixed) {
     TRY(c->W.ensure((size_t)ld * N * sizeof(double2)));
     double2* W = c->W.as<double2>();
-    assemble_kernel<double2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N);
+    assemble_kernel<double2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2);
     LAUNCH_CHECK();
     surface_rhs_kernel<double2><<<gr, 256, 0, c->stream>>>(md.q2, nr, nch, X64, ld, N, 1.0);
     LAUNCH_CHECK();
@@ -707,6 +906,7 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
     double rn;
     TRY(frob_norm(c, c->R64.as<double2>(), ld, N, nch, &rn));
     if (stats) {
+      stats->surface_change = -1.0;
       stats->rel_residual = rn / bnorm;
       stats->residual_history[0] = rn / bnorm;
       stats->ms_solve = ms_since(t2);
@@ -714,7 +914,7 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
   } else {
     TRY(c->W.ensure((size_t)ld * N * sizeof(float2)));
     float2* W = c->W.as<float2>();
-    assemble_kernel<float2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N);
+    assemble_kernel<float2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2);
     LAUNCH_CHECK();
     int nb = pick_nb(c, N, sizeof(float2), 128);
     if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
@@ -726,12 +926,15 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
     float2* X32 = c->X.as<float2>();
     surface_rhs_kernel<float2><<<gr, 256, 0, c->stream>>>(md.q2, nr, nch, X32, ld, N, 1.0);
     LAUNCH_CHECK();
-    TRY(lu_solve<float2>(c, W, st, X32, ld, nch));
+    TRY(lu_solve_tc(c, st, X32, ld, nch));
     f2d_kernel<<<gr, 256, 0, c->stream>>>(X32, ld, X64, ld, N, nullptr);
     LAUNCH_CHECK();
     if (stats) stats->ms_solve = ms_since(t2);
     auto t3 = Clock::now();
-    status = refine_mixed(c, op, W, st, X64, ld, nch, bnorm, stats);
+    double cn2;
+    HPR_CUDA_TRY(cudaMemcpyAsync(&cn2, d_fro2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    status = refine_mixed(c, op, W, st, X64, ld, nch, bnorm, sqrt(cn2), stats);
     if (status != HPRMAT_B200_OK && status != HPRMAT_B200_NOT_CONVERGED) return status;
     if (stats) stats->ms_refine = ms_since(t3);
   }
@@ -767,8 +970,10 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
 }
 
 // Dense solve A X = B with device operands (A read only, B overwritten with X).
+// surf_q2 (device, nlag doubles) enables the surface-projection stopping rule when the
+// right-hand sides are the channel-surface vectors blockdiag(q2) of an R-matrix problem.
 static int solve_dense_core(hprmat_b200_ctx* c, const double2* dA, double2* dB, int n, int nrhs,
-                            hprmat_b200_stats* stats) {
+                            hprmat_b200_stats* stats, const double* surf_q2 = nullptr, int nlag = 0) {
   auto t_all = Clock::now();
   if (n <= 0 || nrhs <= 0 || !dA || !dB) return fail(HPRMAT_B200_ERR_ARG, "solve_linear: invalid arguments");
   const int N = n;
@@ -829,7 +1034,7 @@ static int solve_dense_core(hprmat_b200_ctx* c, const double2* dA, double2* dB, 
     double2* X64 = c->X64.as<double2>();
     d2f_kernel<<<gr, 256, 0, c->stream>>>(dB, N, X32, ld, N, nullptr);
     LAUNCH_CHECK();
-    TRY(lu_solve<float2>(c, W, st, X32, ld, nrhs));
+    TRY(lu_solve_tc(c, st, X32, ld, nrhs));
     f2d_kernel<<<gr, 256, 0, c->stream>>>(X32, ld, X64, ld, N, nullptr);
     LAUNCH_CHECK();
     if (stats) stats->ms_solve = ms_since(t2);
@@ -840,11 +1045,20 @@ static int solve_dense_core(hprmat_b200_ctx* c, const double2* dA, double2* dB, 
     op.B = dB;
     op.ldb = N;
     op.N = N;
+    op.q2 = surf_q2;
+    op.nr = nlag;
     double bn;
     TRY(frob_norm(c, dB, N, N, nrhs, &bn));
     if (bn == 0.0) bn = 1.0;
+    double* d_fro2 = reinterpret_cast<double*>(c->status.as<int>() + 32);
+    HPR_CUDA_TRY(cudaMemsetAsync(d_fro2, 0, sizeof(double), c->stream));
+    fro2_kernel<<<ga, 256, 0, c->stream>>>(dA, N, N, d_fro2);
+    LAUNCH_CHECK();
+    double cn2;
+    HPR_CUDA_TRY(cudaMemcpyAsync(&cn2, d_fro2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
     auto t3 = Clock::now();
-    status = refine_mixed(c, op, W, st, X64, ld, nrhs, bn, stats);
+    status = refine_mixed(c, op, W, st, X64, ld, nrhs, bn, sqrt(cn2), stats);
     if (status != HPRMAT_B200_OK && status != HPRMAT_B200_NOT_CONVERGED) return status;
     copy_d_kernel<<<gr, 256, 0, c->stream>>>(X64, ld, dB, N, N);
     LAUNCH_CHECK();
@@ -867,7 +1081,8 @@ void hprmat_b200_default_opts(hprmat_b200_opts* o) {
   memset(o, 0, sizeof(*o));
   o->precision = HPRMAT_B200_PREC_MIXED;
   o->max_refine = 3;
-  o->tol = 1.0e-13;
+  o->tol = 1.0e-12;
+  o->surface_tol = 1.0e-11;
   o->panel_nb = 0;
 }
 
@@ -876,6 +1091,7 @@ static int validate_opts(const hprmat_b200_opts* o) {
     return fail(HPRMAT_B200_ERR_ARG, "opts.precision must be 0 (FP64) or 1 (mixed)");
   if (o->max_refine < 0 || o->max_refine > 8) return fail(HPRMAT_B200_ERR_ARG, "opts.max_refine must be in 0..8");
   if (!(o->tol >= 0.0)) return fail(HPRMAT_B200_ERR_ARG, "opts.tol must be >= 0");
+  if (!(o->surface_tol >= 0.0)) return fail(HPRMAT_B200_ERR_ARG, "opts.surface_tol must be >= 0");
   if (o->panel_nb != 0 && o->panel_nb != 16 && o->panel_nb != 32 && o->panel_nb != 64 && o->panel_nb != 128)
     return fail(HPRMAT_B200_ERR_ARG, "opts.panel_nb must be 0, 16, 32, 64 or 128");
   return HPRMAT_B200_OK;
@@ -931,8 +1147,9 @@ int hprmat_b200_destroy(hprmat_b200_ctx* c) {
   cudaStreamSynchronize(c->stream);
   DevBuf* bufs[] = {&c->mesh, &c->W, &c->A64, &c->X, &c->X64, &c->R64, &c->B64, &c->V, &c->Z, &c->gm,
                     &c->swaps, &c->ipiv, &c->stage, &c->status, &c->ops, &c->inv, &c->chan, &c->rmat,
-                    &c->zwork, &c->cpot, &c->cu, &c->norms};
+                    &c->zwork, &c->cpot, &c->cu, &c->norms, &c->lup, &c->rop, &c->rsurf, &c->vt, &c->rlo};
   for (DevBuf* b : bufs) b->release();
+  for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->h_norms) cudaFreeHost(c->h_norms);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -1038,8 +1255,28 @@ int hprmat_b200_solve_rmatrix(hprmat_b200_ctx* c, const double* cmat, const doub
       X[2 * idx] = bvec[2 * r];
       X[2 * idx + 1] = bvec[2 * r + 1];
     }
-  int s = hprmat_b200_solve_linear(c, cmat, X.data(), N, nch, stats);
+  // Real surface vectors (the R-matrix case) enable the surface stopping rule.
+  bool real_b = true;
+  for (int r = 0; r < nlag; ++r) real_b = real_b && bvec[2 * r + 1] == 0.0;
+  const double* d_q2 = nullptr;
+  if (real_b) {
+    std::vector<double> q(nlag);
+    for (int r = 0; r < nlag; ++r) q[r] = bvec[2 * r];
+    TRY(c->rmat.ensure(std::max(c->rmat.bytes, (size_t)nlag * sizeof(double) + 64)));
+    HPR_CUDA_TRY(cudaMemcpy(c->rmat.p, q.data(), (size_t)nlag * sizeof(double), cudaMemcpyHostToDevice));
+    d_q2 = c->rmat.as<double>();
+  }
+  const size_t abytes = (size_t)N * N * sizeof(double2);
+  const size_t bbytes = (size_t)N * nch * sizeof(double2);
+  TRY(c->A64.ensure(abytes));
+  TRY(c->B64.ensure(bbytes));
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->A64.p, cmat, abytes, cudaMemcpyHostToDevice, c->stream));
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->B64.p, X.data(), bbytes, cudaMemcpyHostToDevice, c->stream));
+  int s = solve_dense_core(c, c->A64.as<double2>(), c->B64.as<double2>(), N, nch, stats, d_q2, nlag);
+  if (stats) stats->status = s;
   if (s != HPRMAT_B200_OK && s != HPRMAT_B200_NOT_CONVERGED) return s;
+  HPR_CUDA_TRY(cudaMemcpyAsync(X.data(), c->B64.p, bbytes, cudaMemcpyDeviceToHost, c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
   // Rmat(ich, ichp) = normfac * sum_r B(r) X(r + (ich-1) nlag, ichp): complex products
   for (int jp = 0; jp < nch; ++jp)
     for (int i = 0; i < nch; ++i) {
@@ -1118,6 +1355,33 @@ int gpu_b200_finalize_(void) {
 }
 
 // ---- kernel-level hooks (include/hprmat_b200_dev.h)
+int hprmat_b200_dev_set_profile(hprmat_b200_ctx* c, int enable) {
+  TRY(check_ctx(c));
+  c->profile = enable != 0;
+  if (c->profile && c->ev.empty()) {
+    c->ev.resize(2 * 2048);
+    for (auto& e : c->ev) HPR_CUDA_TRY(cudaEventCreate(&e));
+  }
+  c->ev_used = 0;
+  c->ev_flops.clear();
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_dev_counters(hprmat_b200_ctx* c, unsigned long long* launches, double* tc_ms, double* tc_flops,
+                             int* tc_launches, int reset) {
+  if (!c) return fail(HPRMAT_B200_ERR_ARG, "null context");
+  if (launches) *launches = c->launches;
+  if (tc_ms) *tc_ms = c->tc_ms;
+  if (tc_flops) *tc_flops = c->tc_flops;
+  if (tc_launches) *tc_launches = c->tc_launches;
+  if (reset) {
+    c->launches = 0;
+    c->tc_ms = c->tc_flops = 0.0;
+    c->tc_launches = 0;
+  }
+  return HPRMAT_B200_OK;
+}
+
 __global__ void split_planes_kernel(const float2* __restrict__ src, int rows, int nb, float* dst, long plane) {
   const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long)rows * nb) return;
@@ -1142,12 +1406,17 @@ int hprmat_b200_dev_split_planes(hprmat_b200_ctx* c, const void* src, int rows, 
 }
 
 int hprmat_b200_dev_tc_update(hprmat_b200_ctx* c, const float* aop, const float* bop, long plane, int nb, void* C,
-                              long ldc, int M, int Nc) {
+                              long ldc, int M, int Nc, int bn) {
   TRY(check_ctx(c));
-  if (!aop || !bop || !C || M < 0 || Nc < 0 || ldc < M || (nb != 16 && nb != 32 && nb != 64 && nb != 128) ||
+  if (!aop || !bop || !C || M <= 0 || Nc <= 0 || ldc < M || nb < 16 || (nb % 16) || (bn != 128 && bn != 256) ||
       plane < (long)std::max(M, Nc) * nb || ((uintptr_t)aop & 15) || ((uintptr_t)bop & 15) || (plane % 4))
     return fail(HPRMAT_B200_ERR_ARG, "dev_tc_update: invalid arguments");
-  TRY(tc_trailing_update(c->tcplan, aop, bop, plane, nb, nb, (float2*)C, ldc, M, Nc, c->stream));
+  TcOperand A, B;
+  if (tc_make_operand(c->tcplan, A, aop, nb, plane / nb, nb, plane, 128) ||
+      tc_make_operand(c->tcplan, B, bop, nb, plane / nb, nb, plane, bn))
+    return fail(HPRMAT_B200_ERR_ARG, "%s", hprmat_b200_last_error());
+  if (tc_update(c->tcplan, A, 0, 0, B, 0, 0, nb, (float2*)C, ldc, M, Nc, bn, c->stream))
+    return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
   HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
   int err = 0;
   TRY(tc_gemm_check(c->tcplan, c->stream, &err));

@@ -1,4 +1,5 @@
-// Complex trailing update of the mixed-precision LU on sm_100a tensor cores.
+// Complex GEMM update of the mixed-precision LU (trailing update) and of its blocked
+// triangular solves, on sm_100a tensor cores.
 //
 //   C[M x Nc] -= A[M x K] * B[K x Nc]       (complex, C interleaved float2, column-major)
 //
@@ -8,11 +9,12 @@
 //   Re += Ar*Br - Ai*Bi,   Im += Ar*Bi + Ai*Br      -> 12 MMAs per K-step of 8.
 // The minus sign comes from the A-negate bit of the instruction descriptor.
 //
-// Tile 128 (rows) x 256 (columns); Re and Im accumulate in TMEM columns [0,256) and
-// [256,512) of a 512-column allocation.  One persistent CTA per SM, 6 warps:
+// Tile 128 (rows) x BN (columns, 256 for the trailing update, 128 for right-hand sides);
+// Re and Im accumulate in TMEM columns [0,BN) and [BN,2BN).  One persistent CTA per SM,
+// 6 warps:
 //   warp 0     TMA producer: per K-chunk of 16 one 3-D box for the 4 A planes
-//              (16 x 128 x 4 floats) and one for the 4 B planes (16 x 256 x 4), 64-byte
-//              swizzle, into a 2-stage ring; also prefetches the next C tile into L2;
+//              (16 x 128 x 4 floats) and one for the 4 B planes (16 x BN x 4), 64-byte
+//              swizzle, into a multi-stage ring; also prefetches the next C tile into L2;
 //   warp 1     TMEM allocator and single-thread MMA issuer;
 //   warps 2-5  epilogue: tcgen05.ld of Re/Im, C -= acc, coalesced along rows.
 // Every mbarrier wait is bounded; on expiry the kernel records the site in *err, stops
@@ -29,13 +31,15 @@ namespace hprmat {
 namespace {
 
 constexpr int kBM = 128;
-constexpr int kBN = 256;
 constexpr int kKC = 16;                                 // K values per stage (64 bytes)
-constexpr int kStages = 2;
 constexpr int kABytes = 4 * kBM * kKC * 4;             // 32 KB
-constexpr int kBBytes = 4 * kBN * kKC * 4;             // 64 KB
-constexpr int kStageBytes = kABytes + kBBytes;          // 96 KB
-constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*barriers*/ + 1024 /*align*/;
+template <int BN> struct TileCfg {
+  static constexpr int kBBytes = 4 * BN * kKC * 4;     // 64 KB (BN=256) / 32 KB (BN=128)
+  static constexpr int kStageBytes = kABytes + kBBytes;
+  static constexpr int kStages = (200 * 1024) / kStageBytes;   // 2 (BN=256) / 3 (BN=128)
+  static constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*barriers*/ + 1024 /*align*/;
+  static constexpr int kTmemCols = 2 * BN;
+};
 constexpr int kThreads = 192;
 constexpr unsigned kWaitLimit = 1u << 26;
 
@@ -100,9 +104,10 @@ __device__ __forceinline__ uint64_t sdesc_k_sw64(uint32_t saddr) {
   return d;
 }
 
-// Instruction descriptor: kind::tf32, D = F32, A = B = TF32, both K-major, M = 128, N = 256.
+// Instruction descriptor: kind::tf32, D = F32, A = B = TF32, both K-major, M = 128, N = BN.
+template <int BN>
 __host__ __device__ constexpr uint32_t idesc_tf32(bool neg_a) {
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(kBN >> 3) << 17) |
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(BN >> 3) << 17) |
          ((uint32_t)(kBM >> 4) << 24);
 }
 
@@ -136,10 +141,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-template <int NB>
+struct TcArgs {
+  int a_k0, a_row0, b_k0, b_row0, kchunks;
+  float2* C;
+  long ldc;
+  int M, Nc;
+  int* err;
+};
+
+template <int BN>
 __global__ void __launch_bounds__(kThreads, 1)
-    tc_update_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, float2* C,
-                     long ldc, int M, int Nc, int* err) {
+    tc_update_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcArgs p) {
+  using Cfg = TileCfg<BN>;
+  constexpr int kBN = BN;
+  constexpr int kStages = Cfg::kStages;
+  constexpr int kStageBytes = Cfg::kStageBytes;
+  float2* C = p.C;
+  const long ldc = p.ldc;
+  const int M = p.M, Nc = p.Nc;
+  int* err = p.err;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
@@ -155,7 +175,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int mt = (M + kBM - 1) / kBM;
   const int nt = (Nc + kBN - 1) / kBN;
   const int ntiles = mt * nt;
-  constexpr int kChunks = NB / kKC;
+  const int kChunks = p.kchunks;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
@@ -170,7 +190,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(512)
+                 "r"(Cfg::kTmemCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -201,8 +221,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (!mbar_wait(&empty[stage], phase ^ 1u, abort_flag, err, 11)) { ok = false; break; }
           unsigned char* sa = smem + stage * kStageBytes;
           mbar_expect_tx(&full[stage], kStageBytes);
-          tma_load_3d(sa, &tmA, &full[stage], kc * kKC, m0, 0);
-          tma_load_3d(sa + kABytes, &tmB, &full[stage], kc * kKC, n0, 0);
+          tma_load_3d(sa, &tmA, &full[stage], p.a_k0 + kc * kKC, p.a_row0 + m0, 0);
+          tma_load_3d(sa + kABytes, &tmB, &full[stage], p.b_k0 + kc * kKC, p.b_row0 + n0, 0);
           inflight = min(inflight + 1, kStages);
           if (++stage == kStages) { stage = 0; phase ^= 1u; }
         }
@@ -222,7 +242,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       int stage = 0;
       uint32_t phase = 0, acc_phase = 0;
       bool ok = true;
-      const uint32_t id_pos = idesc_tf32(false), id_neg = idesc_tf32(true);
+      const uint32_t id_pos = idesc_tf32<BN>(false), id_neg = idesc_tf32<BN>(true);
       const uint32_t t_re = tmem, t_im = tmem + kBN;
       for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         if (!mbar_wait(acc_empty, acc_phase ^ 1u, abort_flag, err, 21)) break;
@@ -314,28 +334,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::kTmemCols)
+                 : "memory");
   }
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-int make_map(EncodeTiledFn enc, CUtensorMap* map, const float* base, int NB, long rows, long plane, int box_rows) {
-  cuuint64_t dims[3] = {(cuuint64_t)NB, (cuuint64_t)rows, 4};
-  cuuint64_t strides[2] = {(cuuint64_t)NB * 4, (cuuint64_t)plane * 4};
-  cuuint32_t box[3] = {(cuuint32_t)kKC, (cuuint32_t)box_rows, 4};
-  cuuint32_t es[3] = {1, 1, 1};
-  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, es,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) {
-    set_last_error_msg("cuTensorMapEncodeTiled failed for a tensor-core operand");
-    return -2;
-  }
-  return 0;
-}
 
 }  // namespace
 
@@ -356,29 +362,57 @@ int tc_gemm_init(TcGemmPlan& p, int device) {
     HPR_CUDA_TRY(cudaMalloc(&p.d_err, sizeof(int)));
     HPR_CUDA_TRY(cudaMemset(p.d_err, 0, sizeof(int)));
   }
-  HPR_CUDA_TRY(cudaFuncSetAttribute(tc_update_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-  HPR_CUDA_TRY(cudaFuncSetAttribute(tc_update_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-  HPR_CUDA_TRY(cudaFuncSetAttribute(tc_update_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-  HPR_CUDA_TRY(cudaFuncSetAttribute(tc_update_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+  HPR_CUDA_TRY(cudaFuncSetAttribute(tc_update_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    TileCfg<256>::kSmemBytes));
+  HPR_CUDA_TRY(cudaFuncSetAttribute(tc_update_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    TileCfg<128>::kSmemBytes));
   return 0;
 }
 
-int tc_trailing_update(TcGemmPlan& p, const float* aop, const float* bop, long plane, int NB, int K, float2* C,
-                       long ldc, int M, int Nc, cudaStream_t s) {
-  (void)K;
-  if (M <= 0 || Nc <= 0) return 0;
+int tc_make_operand(TcGemmPlan& p, TcOperand& op, const float* base, long kext, long rows, long ld, long plane,
+                    int box_rows) {
+  if (((uintptr_t)base & 15) || (ld % 4) || (plane % 4) || kext < 16 || rows < 1 || ld < kext ||
+      (box_rows != 128 && box_rows != 256)) {
+    set_last_error_msg("tensor-core operand: misaligned or invalid view");
+    return -1;
+  }
   EncodeTiledFn enc = reinterpret_cast<EncodeTiledFn>(p.encode);
-  CUtensorMap ma, mb;
-  if (make_map(enc, &ma, aop, NB, M, plane, kBM)) return -2;
-  if (make_map(enc, &mb, bop, NB, Nc, plane, kBN)) return -2;
-  const int ntiles = ((M + kBM - 1) / kBM) * ((Nc + kBN - 1) / kBN);
-  const int grid = ntiles < p.nsm ? ntiles : p.nsm;
-  switch (NB) {
-    case 128: tc_update_kernel<128><<<grid, kThreads, kSmemBytes, s>>>(ma, mb, C, ldc, M, Nc, p.d_err); break;
-    case 64: tc_update_kernel<64><<<grid, kThreads, kSmemBytes, s>>>(ma, mb, C, ldc, M, Nc, p.d_err); break;
-    case 32: tc_update_kernel<32><<<grid, kThreads, kSmemBytes, s>>>(ma, mb, C, ldc, M, Nc, p.d_err); break;
-    case 16: tc_update_kernel<16><<<grid, kThreads, kSmemBytes, s>>>(ma, mb, C, ldc, M, Nc, p.d_err); break;
-    default: set_last_error_msg("tensor-core update: unsupported block size"); return -5;
+  cuuint64_t dims[3] = {(cuuint64_t)kext, (cuuint64_t)rows, 4};
+  cuuint64_t strides[2] = {(cuuint64_t)ld * 4, (cuuint64_t)plane * 4};
+  cuuint32_t box[3] = {(cuuint32_t)kKC, (cuuint32_t)box_rows, 4};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = enc(&op.map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_last_error_msg("cuTensorMapEncodeTiled failed for a tensor-core operand");
+    return -2;
+  }
+  op.kext = kext;
+  op.rows = rows;
+  return 0;
+}
+
+int tc_update(TcGemmPlan& p, const TcOperand& A, int a_k0, int a_row0, const TcOperand& B, int b_k0, int b_row0,
+              int K, float2* C, long ldc, int M, int Nc, int bn, cudaStream_t s) {
+  if (M <= 0 || Nc <= 0 || K <= 0) return 0;
+  // The K coordinate of every box is a multiple of 16 floats (64 bytes): TMA's 16-byte rule.
+  if ((K % kKC) || (a_k0 % 4) || (b_k0 % 4) || a_k0 < 0 || b_k0 < 0 || a_row0 < 0 || b_row0 < 0) {
+    set_last_error_msg("tensor-core update: K offsets must be multiples of 4 floats and K of 16");
+    return -1;
+  }
+  TcArgs args{a_k0, a_row0, b_k0, b_row0, K / kKC, C, ldc, M, Nc, p.d_err};
+  if (bn == 256) {
+    const int ntiles = ((M + kBM - 1) / kBM) * ((Nc + 255) / 256);
+    const int grid = ntiles < p.nsm ? ntiles : p.nsm;
+    tc_update_kernel<256><<<grid, kThreads, TileCfg<256>::kSmemBytes, s>>>(A.map, B.map, args);
+  } else if (bn == 128) {
+    const int ntiles = ((M + kBM - 1) / kBM) * ((Nc + 127) / 128);
+    const int grid = ntiles < p.nsm ? ntiles : p.nsm;
+    tc_update_kernel<128><<<grid, kThreads, TileCfg<128>::kSmemBytes, s>>>(A.map, B.map, args);
+  } else {
+    set_last_error_msg("tensor-core update: bn must be 128 or 256");
+    return -5;
   }
   HPR_CUDA_TRY(cudaGetLastError());
   return 0;

@@ -47,8 +47,11 @@ typedef struct hprmat_b200_ctx hprmat_b200_ctx;
 typedef struct {
   int precision;   /* HPRMAT_B200_PREC_* (default MIXED) */
   int max_refine;  /* FP64 refinement steps, 0..8 (default 3) */
-  double tol;      /* stop when ||B - C X||_F / ||B||_F < tol (default 1e-13); the same
+  double tol;      /* stop when ||B - C X||_F / ||B||_F < tol (default 1e-12); the same
                       relative Frobenius rule as src/rmat_solvers.F90:253-262 */
+  double surface_tol; /* R-matrix path: or when a refinement step changes the surface
+                         projection R = q2^T X (what the collision matrix depends on) by less
+                         than surface_tol relative (Frobenius; default 1e-11) */
   int panel_nb;    /* LU block size; 0 = automatic */
   int reserved[4];
 } hprmat_b200_opts;
@@ -56,11 +59,15 @@ typedef struct {
 typedef struct {
   int status;               /* return value of the call */
   int info;                 /* LAPACK-style info: >0 = first zero pivot (1-based) */
-  int refine_steps;         /* refinement corrections applied */
+  int refine_steps;         /* refinement corrections (outer steps) applied */
+  int inner_iterations;     /* preconditioned FGMRES iterations (LU solves) over all steps */
   int nb;                   /* LU block size used */
   int n;                    /* order of the solved system */
   int nrhs;
   double rel_residual;      /* final ||B - C X||_F / ||B||_F, evaluated in FP64 */
+  double surface_change;    /* relative change of R in the last refinement step (-1: n/a) */
+  double residual_floor;    /* estimated rounding floor of the relative FP64 residual (0: n/a) */
+  double floor_history[9];  /* the floor estimate at each outer step */
   double residual_history[9];
   double ms_assemble, ms_factor, ms_solve, ms_refine, ms_umatrix, ms_total;
 } hprmat_b200_stats;

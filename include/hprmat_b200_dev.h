@@ -14,14 +14,23 @@ extern "C" {
 /* C[M x Nc] -= A * B on the tensor cores: C complex float (interleaved, column-major, ldc),
    A and B as 4 planes (Re hi, Re lo, Im hi, Im lo of the TF32 split), K-major with nb
    floats per row / column, planes `plane` floats apart (the LU's operand buffers).
-   nb in {16, 32, 64, 128}. */
+   nb a multiple of 16; bn = 128 or 256 columns per tile. */
 int hprmat_b200_dev_tc_update(hprmat_b200_ctx* ctx, const float* aop, const float* bop, long plane, int nb,
-                              void* C, long ldc, int M, int Nc);
+                              void* C, long ldc, int M, int Nc, int bn);
 
 /* Split complex float values into the 4 TF32 planes used by hprmat_b200_dev_tc_update:
    src is rows x nb (row-major complex float, i.e. K contiguous), dst gets 4 planes of
    rows x nb floats, `plane` floats apart. */
 int hprmat_b200_dev_split_planes(hprmat_b200_ctx* ctx, const void* src, int rows, int nb, float* dst, long plane);
+
+/* Benchmark counters.  With profiling enabled, every tensor-core trailing update of a
+   factorisation is bracketed by CUDA events on the context's stream; the counters
+   accumulate their elapsed time (ms), their algorithmic flops (8 M^2 nb per launch, the
+   complex-LU convention) and their number.  `launches` counts every kernel the library
+   launched on the context.  reset != 0 clears them after reading. */
+int hprmat_b200_dev_set_profile(hprmat_b200_ctx* ctx, int enable);
+int hprmat_b200_dev_counters(hprmat_b200_ctx* ctx, unsigned long long* launches, double* tc_ms, double* tc_flops,
+                             int* tc_launches, int reset);
 
 #ifdef __cplusplus
 }

@@ -46,7 +46,8 @@ def test_default_opts_and_status_strings():
     lib = nat.load()
     o = nat.Opts()
     lib.hprmat_b200_default_opts(ctypes.byref(o))
-    assert o.precision == nat.PREC_MIXED and o.max_refine == 3 and o.tol == 1e-13 and o.panel_nb == 0
+    assert o.precision == nat.PREC_MIXED and o.max_refine == 3 and o.tol == 1e-12 and o.surface_tol == 1e-11
+    assert o.panel_nb == 0
     assert lib.hprmat_b200_status_string(nat.SINGULAR) == b"singular matrix"
     assert lib.hprmat_b200_status_string(nat.NOT_CONVERGED) == b"refinement did not converge"
 
