@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-comparators", action="store_true", help="skip the FP64 device-LU comparators")
+    ap.add_argument("--solves-only", action="store_true",
+                    help="only the device-resident timed solves (for profiler launch lists)")
+    ap.add_argument("--nch", type=int, default=128, help="channels of the production generator (N = 200 nch)")
     return ap.parse_args()
 
 
@@ -175,7 +178,8 @@ def main():
     from hprmat_b200 import _native as nat
     from hprmat_b200 import api, workloads
 
-    w = workloads.production()
+    w = workloads.production(nch=args.nch)
+    n_full = w.n
     ctx = api.Context(device=local, precision="mixed", max_refine=3, tol=1e-12)
     stream = torch.cuda.Stream(device=dev)
     ctx.set_stream(stream.cuda_stream)
@@ -196,7 +200,7 @@ def main():
 
     for _ in range(args.warmup):
         step_device()
-    st_warm = dict(ctx.last_stats)
+    st_warm = dict(ctx.last_stats or {})
     # ---- timed region (device-resident inputs)
     lib.hprmat_b200_dev_counters(ctx._h, None, None, None, None, 1)
     clocks = ClockSampler(local)
@@ -226,10 +230,20 @@ def main():
     cu = d_cu.cpu().numpy().view(np.complex128).reshape(ndim, ndim, order="F")
     nopen = int((w.qk > 0).sum())
     u_err = None
-    fx = os.path.join(ROOT, "tests", "golden", "production_u_nch128.npz")
+    fx = os.path.join(ROOT, "tests", "golden", f"production_u_nch{args.nch}.npz")
     if os.path.exists(fx):
         ref = np.load(fx)["u"]
         u_err = float(np.linalg.norm(cu[:nopen, :nopen] - ref) / np.linalg.norm(ref))
+
+    if args.solves_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                              "warmup": args.warmup, "ms_per_step": ms_per_step, "N": n_full, "u_rel_err": u_err,
+                              "gpu_launches": int(launches.value), "clocks": clk}))
+        ctx.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
 
     # ---- end to end through the host C ABI: pinned host cpot in, U out, every step
     h_cpot = torch.from_numpy(np.asfortranarray(w.cpot).ravel(order="F").view(np.float64)).pin_memory()
