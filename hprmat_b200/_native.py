@@ -32,6 +32,7 @@ EXPORTED = (
     "hprmat_b200_solve_linear", "hprmat_b200_solve_linear_device", "hprmat_b200_solve_rmatrix",
     "gpu_b200_solve_mixed_", "gpu_b200_solve_double_", "gpu_b200_finalize_", "hprmat_b200_status_string",
     "hprmat_b200_last_error", "hprmat_b200_version", "hprmat_b200_boundary",
+    "hprmat_b200_solve_linear_noalloc",
     # include/hprmat_b200_dev.h
     "hprmat_b200_dev_tc_update", "hprmat_b200_dev_split_planes", "hprmat_b200_dev_set_profile",
     "hprmat_b200_dev_counters",
@@ -98,6 +99,7 @@ def load():
         "hprmat_b200_last_error": (ctypes.c_char_p, []),
         "hprmat_b200_version": (I, []),
         "hprmat_b200_boundary": (I, [I, IP, DP, DP, D, DP, DP, DP, DP, IP]),
+        "hprmat_b200_solve_linear_noalloc": (I, [P, P, I, I, P, IP]),
         "hprmat_b200_dev_tc_update": (I, [P, P, P, ctypes.c_long, I, P, ctypes.c_long, I, I, I]),
         "hprmat_b200_dev_split_planes": (I, [P, P, I, I, P, ctypes.c_long]),
         "hprmat_b200_dev_set_profile": (I, [P, I]),

@@ -135,6 +135,25 @@ int gpu_b200_solve_double_(double* A, double* B, int* n, int* nrhs,
                            int* info);              /* cf. gpu_solve_double_ :737-795 */
 int gpu_b200_finalize_(void);                       /* cf. gpu_solver_finalize_ :222 */
 
+/* Dense FP64 solve A X = B of small systems that allocates no device memory.  No
+   counterpart in the reference: it is for callers that must not call cudaMalloc -- code that
+   runs the solver inside another framework's device memory pool (where a cudaMalloc fails
+   once the pool has reserved the memory) or in a latency-critical loop (where cudaFree
+   stalls the whole device).  Same algorithm and kernels as the FP64 path of
+   hprmat_b200_solve_linear_device; its working memory is a fixed array of about 5.8 MB
+   inside the library that every GPU loading the library holds until the process exits.
+   Limits: n <= 512, nrhs <= 64 (larger sizes return HPRMAT_B200_ERR_UNSUPPORTED).
+   d_A (n x n complex double, column-major, read only) and d_B (n x nrhs, overwritten with
+   X) are device pointers; the work is ordered on `stream` (a cudaStream_t, NULL = default
+   stream) and complete when the call returns.  *info (may be NULL) receives the first zero
+   pivot (1-based) when the status is HPRMAT_B200_SINGULAR.
+   The first call on a device looks up the array's device address (cudaGetSymbolAddress);
+   make that first call before any stream capture.  All calls share the one array: calls
+   whose GPU work overlaps (other threads or streams) race and must be serialised by the
+   caller. */
+int hprmat_b200_solve_linear_noalloc(const void* d_A, void* d_B, int n, int nrhs, void* stream,
+                                     int* info);
+
 /* Boundary values of the R-matrix -> collision-matrix step at the channel radius a = rmax,
    per channel, as computed in rmatrix (src/rmatrix_hp.F90:224-244).  Host only, needs no
    GPU.  Open channels (qk > 0): co = G + iF and cop = (G' + iF') k a from COULFG
