@@ -79,31 +79,32 @@ enum StatusWord {
 };
 
 // Bounded grid-wide barrier for cooperative launches.  `target` = number of CTAs times
-// the barrier's ordinal (1-based) since the counter was zeroed.  Returns false when the
-// wait exceeded its limit; the caller must then stop touching shared data and return.
+// the barrier's ordinal (1-based) since the counter was zeroed.  Thread 0 arrives with a
+// release-ordered add (publishing the CTA's earlier writes, ordered by __syncthreads) and
+// polls with acquire loads; the error flag is looked at only every 4096 polls.  Returns
+// false when the wait exceeded its limit; the caller must then stop touching shared data
+// and return.
 __device__ inline bool grid_barrier(int* counter, int* timeout_flag, unsigned target, int site) {
   __syncthreads();
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(counter, 1);
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(counter) : "memory");
     int ok = 1;
-    unsigned spins = 0;
-    for (;;) {
+    for (unsigned spins = 1;; ++spins) {
       unsigned v;
       asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(counter) : "memory");
       if (v >= target) break;
-      int tf;
-      asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(tf) : "l"(timeout_flag) : "memory");
-      if (tf != 0) { ok = 0; break; }
-      if (++spins > (1u << 24)) {  // ~ seconds with the back-off below
-        atomicExch(timeout_flag, site);
-        ok = 0;
-        break;
+      if ((spins & 4095u) == 0) {
+        int tf;
+        asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(tf) : "l"(timeout_flag) : "memory");
+        if (tf != 0) { ok = 0; break; }
+        if (spins >= (1u << 26)) {  // seconds: something is wrong
+          atomicExch(timeout_flag, site);
+          ok = 0;
+          break;
+        }
       }
-      if (spins > 64) __nanosleep(64);
     }
-    __threadfence();
     s_ok = ok;
   }
   __syncthreads();

@@ -40,8 +40,7 @@ struct PanelArgs {
   int N, k0, ncols, rpc, G;
   int* ipiv;                      // [N] global pivot rows (0-based)
   T* cand_rows;                   // [2][G][NB]
-  typename RealOf<T>::R* cand_val;  // [2][G]
-  int* cand_idx;                  // [2][G]
+  unsigned long long* keys;       // [NB] winning pivot key per panel column (zeroed per launch)
   T* rowj;                        // [2][NB]
   int* status;                    // device status block
   StepSwaps sw;
@@ -68,6 +67,15 @@ __device__ __forceinline__ void tf32_split(float x, float& hi, float& lo) {
   lo = x - hi;
 }
 
+// Pivot key of a candidate: |re|+|im| (as float bits, monotone for non-negative values) in
+// the high word, the complement of the panel row in the low word, so that one 64-bit
+// atomicMax picks the largest modulus and, among equal ones, the lowest row.  (On the FP64
+// path the modulus is compared after rounding to float; candidates within a relative 6e-8
+// of each other are equally good pivots.)
+__device__ __forceinline__ unsigned long long pivot_key(float v, int row) {
+  return ((unsigned long long)__float_as_uint(v) << 32) | (unsigned long long)(0xFFFFFFFFu - (unsigned)row);
+}
+
 template <typename T, int NB, int NT>
 __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
   using R = typename RealOf<T>::R;
@@ -80,49 +88,47 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
   const int rpcp = a.rpc | 1;  // odd column stride: conflict-free row gathers
   T* P = reinterpret_cast<T*>(smem_raw);                 // [NB][rpcp] column-major
   T* urow = P + (size_t)NB * rpcp;                       // [NB]
-  __shared__ R red_v[NT / 32];
+  __shared__ float red_v[NT / 32];
   __shared__ int red_i[NT / 32];
-  __shared__ int s_piv, s_win, s_loc_ipiv[NB];
-  __shared__ R s_growth;
+  __shared__ int s_piv, s_loc_ipiv[NB];
+  __shared__ unsigned s_growth;
   const int tid = threadIdx.x;
   const int ncols = a.ncols;
 
   // load rows [r0, r1) of the panel
-  for (int idx = tid; idx < nloc * ncols; idx += NT) {
-    int lr = idx % nloc, c = idx / nloc;
-    P[(size_t)c * rpcp + lr] = a.W[(size_t)(a.k0 + r0 + lr) + (size_t)(a.k0 + c) * a.ld];
-  }
-  if (tid == 0) s_growth = R(0);
+  for (int c = 0; c < ncols; ++c)
+    for (int lr = tid; lr < nloc; lr += NT)
+      P[(size_t)c * rpcp + lr] = a.W[(size_t)(a.k0 + r0 + lr) + (size_t)(a.k0 + c) * a.ld];
+  if (tid == 0) s_growth = 0u;
   __syncthreads();
 
   for (int j = 0; j < ncols; ++j) {
     const int buf = j & 1;
-    // (1) local pivot candidate: max |re|+|im| over rows >= j, lowest row on ties
-    R bv = R(-1);
+    // (1) local pivot candidate of column j: max |re|+|im| over rows >= j, lowest row on ties
+    float bv = -1.f;
     int bi = 0x7fffffff;
     for (int lr = max(j - r0, 0) + tid; lr < nloc; lr += NT) {
-      R v = cabs1(P[(size_t)j * rpcp + lr]);
+      float v = (float)cabs1(P[(size_t)j * rpcp + lr]);
       if (v > bv) { bv = v; bi = r0 + lr; }
     }
     for (int o = 16; o > 0; o >>= 1) {
-      R ov = __shfl_down_sync(0xffffffffu, bv, o);
+      float ov = __shfl_down_sync(0xffffffffu, bv, o);
       int oi = __shfl_down_sync(0xffffffffu, bi, o);
       if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
     }
     if ((tid & 31) == 0) { red_v[tid >> 5] = bv; red_i[tid >> 5] = bi; }
     __syncthreads();
     if (tid < 32) {
-      bv = (tid < NT / 32) ? red_v[tid] : R(-1);
+      bv = (tid < NT / 32) ? red_v[tid] : -1.f;
       bi = (tid < NT / 32) ? red_i[tid] : 0x7fffffff;
       for (int o = 16; o > 0; o >>= 1) {
-        R ov = __shfl_down_sync(0xffffffffu, bv, o);
+        float ov = __shfl_down_sync(0xffffffffu, bv, o);
         int oi = __shfl_down_sync(0xffffffffu, bi, o);
         if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
       }
       if (tid == 0) {
-        a.cand_val[buf * a.G + b] = bv;
-        a.cand_idx[buf * a.G + b] = bi;
         s_piv = bi;
+        if (bi != 0x7fffffff) atomicMax(a.keys + j, pivot_key(bv, bi));
       }
     }
     __syncthreads();
@@ -138,67 +144,42 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
     // (3) every CTA has posted
     if (!grid_barrier(a.status + SW_BARRIER, a.status + SW_TIMEOUT, (unsigned)a.G * (j + 1), 1))
       return;
-    // (4) global pivot: same reduction order in every CTA, so all agree
-    if (tid < 32) {
-      R v = R(-1);
-      int i = 0x7fffffff, w = 0;
-      for (int g = tid; g < a.G; g += 32) {
-        R gv = __ldcg(a.cand_val + buf * a.G + g);
-        int gi = __ldcg(a.cand_idx + buf * a.G + g);
-        if (gv > v || (gv == v && gi < i)) { v = gv; i = gi; w = g; }
-      }
-      for (int o = 16; o > 0; o >>= 1) {
-        R ov = __shfl_down_sync(0xffffffffu, v, o);
-        int oi = __shfl_down_sync(0xffffffffu, i, o);
-        int ow = __shfl_down_sync(0xffffffffu, w, o);
-        if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; w = ow; }
-      }
-      if (tid == 0) { s_piv = i; s_win = w; }
+    // (4) the winning key names the pivot row; its owner CTA is row / rpc
+    if (tid == 0) {
+      unsigned long long key = __ldcg(a.keys + j);
+      s_piv = (int)(0xFFFFFFFFu - (unsigned)(key & 0xFFFFFFFFull));
     }
     __syncthreads();
     const int p = s_piv;
+    const int win = p / a.rpc;
+    float g = 0.f;  // pivot growth: largest |re|+|im| in the U part of the pivot row
     for (int c = tid; c < ncols; c += NT) {
-      T u = __ldcg(reinterpret_cast<const T*>(a.cand_rows) + ((size_t)buf * a.G + s_win) * NB + c);
+      T u = __ldcg(reinterpret_cast<const T*>(a.cand_rows) + ((size_t)buf * a.G + win) * NB + c);
       urow[c] = u;
+      if (p != j && p >= r0 && p < r1)
+        P[(size_t)c * rpcp + (p - r0)] = __ldcg(reinterpret_cast<const T*>(a.rowj) + (size_t)buf * NB + c);
+      if (p != j && j >= r0 && j < r1) P[(size_t)c * rpcp + (j - r0)] = u;
+      if (c >= j) g = fmaxf(g, (float)cabs1(u));
     }
-    __syncthreads();
-    if (p != j) {
-      for (int c = tid; c < ncols; c += NT) {
-        if (p >= r0 && p < r1)
-          P[(size_t)c * rpcp + (p - r0)] = __ldcg(reinterpret_cast<const T*>(a.rowj) + (size_t)buf * NB + c);
-        if (j >= r0 && j < r1) P[(size_t)c * rpcp + (j - r0)] = urow[c];
-      }
+    if (tid < ((ncols + 31) & ~31)) {  // whole warps that may hold entries
+      for (int o = 16; o > 0; o >>= 1) g = fmaxf(g, __shfl_down_sync(0xffffffffu, g, o));
+      if ((tid & 31) == 0 && g > 0.f) atomicMax(&s_growth, __float_as_uint(g));
     }
-    if (tid == 0) {
-      s_loc_ipiv[j] = p;
-      R gmax = s_growth;
-      for (int c = j; c < ncols; ++c) gmax = fmax(gmax, cabs1(urow[c]));
-      s_growth = gmax;
-    }
+    if (tid == 0) s_loc_ipiv[j] = p;
     __syncthreads();
     // (5) scale column j below the diagonal, then rank-1 update of the remaining columns
-    T piv = urow[j];
-    T inv;
+    const T piv = urow[j];
     const bool zero = (piv.x == R(0) && piv.y == R(0));
-    if (zero) {
-      inv = czero<T>();
-      if (b == 0 && tid == 0) atomicCAS(a.status + SW_INFO, 0, a.k0 + j + 1);
-    } else {
-      inv = crecip(piv);
-    }
+    if (zero && b == 0 && tid == 0) atomicCAS(a.status + SW_INFO, 0, a.k0 + j + 1);
+    const T inv = zero ? czero<T>() : crecip(piv);
     const int lo = max(j + 1 - r0, 0);
-    const int nact = nloc - lo;
-    if (!zero) {
-      for (int lr = lo + tid; lr < nloc; lr += NT)
-        P[(size_t)j * rpcp + lr] = cmul(P[(size_t)j * rpcp + lr], inv);
-    }
-    __syncthreads();
-    const int nc = ncols - j - 1;
-    if (nact > 0 && nc > 0) {
-      for (int idx = tid; idx < nact * nc; idx += NT) {
-        int lr = lo + idx % nact;
-        int c = j + 1 + idx / nact;
-        T l = P[(size_t)j * rpcp + lr];
+    for (int lr = lo + tid; lr < nloc; lr += NT) {
+      T l = P[(size_t)j * rpcp + lr];
+      if (!zero) {
+        l = cmul(l, inv);
+        P[(size_t)j * rpcp + lr] = l;
+      }
+      for (int c = j + 1; c < ncols; ++c) {
         T v = P[(size_t)c * rpcp + lr];
         cfms(v, l, urow[c]);
         P[(size_t)c * rpcp + lr] = v;
@@ -208,10 +189,9 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
   }
 
   // write the factored rows back
-  for (int idx = tid; idx < nloc * ncols; idx += NT) {
-    int lr = idx % nloc, c = idx / nloc;
-    a.W[(size_t)(a.k0 + r0 + lr) + (size_t)(a.k0 + c) * a.ld] = P[(size_t)c * rpcp + lr];
-  }
+  for (int c = 0; c < ncols; ++c)
+    for (int lr = tid; lr < nloc; lr += NT)
+      a.W[(size_t)(a.k0 + r0 + lr) + (size_t)(a.k0 + c) * a.ld] = P[(size_t)c * rpcp + lr];
   // L21 rows into the LU planes (mixed path): global row k0 + g, columns k0 .. k0+ncols
   if (a.lup != nullptr) {
     const int lr0 = max(ncols - r0, 0);
@@ -233,7 +213,7 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
   if (b == 0) {
     __syncthreads();
     if (tid < ncols) a.ipiv[a.k0 + tid] = a.k0 + s_loc_ipiv[tid];
-    if (tid == 0 && a.growth_bits) atomicMax(a.growth_bits, __float_as_uint((float)s_growth));
+    if (tid == 0 && a.growth_bits) atomicMax(a.growth_bits, s_growth);
     // Row-interchange list of this step: simulate the swaps on the touched positions.
     if (tid < 32) {
       __shared__ int pos[2 * NB], src[2 * NB];
@@ -554,40 +534,53 @@ __global__ void __launch_bounds__(NT) tri_inverse_kernel(const T* __restrict__ W
 // One diagonal block of a triangular solve with many right-hand sides:
 //   X[k0:k0+ncols, col] = Tinv * (P X)[k0:k0+ncols, col]
 // where P is the step's row-interchange list (forward solve; pass top_src = nullptr for
-// the backward solve).  One CTA of NB threads per right-hand side: thread i forms row i
-// from Tinv (read along rows i, coalesced) and the gathered column in shared memory.
-// With rop != nullptr the result is also written as B-operand planes of the tensor-core
-// update (per right-hand side NB consecutive values, zero padded; planes rop_plane apart).
-template <typename T, int NB>
-__global__ void __launch_bounds__(NB) diag_apply_kernel(const T* __restrict__ Tinv, int ncols, int k0,
-                                                        const int* top_src, const int* extra_dst,
-                                                        const int* extra_src, const int* n_extra,
-                                                        T* X, long ldx, int nrhs, float* rop, long rop_plane) {
-  __shared__ T bv[NB];
-  __shared__ T ev[NB];
-  const int i = threadIdx.x;
-  const int col = blockIdx.x;
-  if (col >= nrhs) return;
-  T* x = X + (size_t)col * ldx;
+// the backward solve).  Each CTA stages the NB x NB inverse in shared memory with wide
+// independent loads, then handles CW right-hand sides: thread (i, cc) forms row i of
+// column cc.  With rop != nullptr the result is also written as B-operand planes of the
+// tensor-core update (per right-hand side NB consecutive values, zero padded; planes
+// rop_plane apart).  Dynamic shared memory: NB*NB + 2*CW*NB elements of T.
+template <typename T, int NB, int CW>
+__global__ void __launch_bounds__(NB * CW) diag_apply_kernel(const T* __restrict__ Tinv, int ncols, int k0,
+                                                             const int* top_src, const int* extra_dst,
+                                                             const int* extra_src, const int* n_extra,
+                                                             T* X, long ldx, int nrhs, float* rop, long rop_plane) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* ts = reinterpret_cast<T*>(smem_raw);  // [NB * NB] column-major
+  T* bv = ts + NB * NB;                     // [CW][NB]
+  T* ev = bv + CW * NB;                     // [CW][NB]
+  constexpr int NT = NB * CW;
+  const int tid = threadIdx.x;
+  const int i = tid % NB, cc = tid / NB;
+  const int col = blockIdx.x * CW + cc;
+  const bool active = col < nrhs;
+  T* x = X + (size_t)(active ? col : 0) * ldx;
   const int ne = top_src ? *n_extra : 0;
-  if (i < ncols) bv[i] = x[top_src ? top_src[i] : k0 + i];
-  if (i < ne) ev[i] = x[extra_src[i]];
+  // stage the inverse: 16-byte loads, all independent
+  {
+    const float4* src = reinterpret_cast<const float4*>(Tinv);
+    float4* dst = reinterpret_cast<float4*>(ts);
+    constexpr int n16 = NB * NB * (int)sizeof(T) / 16;
+#pragma unroll 8
+    for (int q = tid; q < n16; q += NT) dst[q] = __ldg(src + q);
+  }
+  if (active && i < ncols) bv[cc * NB + i] = x[top_src ? top_src[i] : k0 + i];
+  if (active && i < ne) ev[cc * NB + i] = x[extra_src[i]];
   __syncthreads();
-  if (i < ne) x[extra_dst[i]] = ev[i];
+  if (active && i < ne) x[extra_dst[i]] = ev[cc * NB + i];
   T acc0 = czero<T>(), acc1 = czero<T>();
-  if (i < ncols) {
-    const T* tr = Tinv + i;
+  if (active && i < ncols) {
+    const T* b = bv + cc * NB;
     int j = 0;
 #pragma unroll 4
     for (; j + 1 < ncols; j += 2) {
-      cfma(acc0, __ldg(tr + (size_t)j * NB), bv[j]);
-      cfma(acc1, __ldg(tr + (size_t)(j + 1) * NB), bv[j + 1]);
+      cfma(acc0, ts[i + j * NB], b[j]);
+      cfma(acc1, ts[i + (j + 1) * NB], b[j + 1]);
     }
-    if (j < ncols) cfma(acc0, __ldg(tr + (size_t)j * NB), bv[j]);
+    if (j < ncols) cfma(acc0, ts[i + j * NB], b[j]);
     acc0 = cadd(acc0, acc1);
     x[k0 + i] = acc0;
   }
-  if (rop != nullptr) {
+  if (active && rop != nullptr) {
     float hr, lr, hi_, li;
     tf32_split((float)acc0.x, hr, lr);
     tf32_split((float)acc0.y, hi_, li);

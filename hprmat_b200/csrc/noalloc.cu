@@ -38,9 +38,8 @@ constexpr size_t kOffSwaps =
     align256(kOffInv + (size_t)2 * kNoAllocSteps * kNoAllocNB * kNoAllocNB * sizeof(double2));
 constexpr size_t kOffIpiv = align256(kOffSwaps + (size_t)kNoAllocSteps * kSwapStrideNA * sizeof(int));
 constexpr size_t kOffCandRows = align256(kOffIpiv + (size_t)kNoAllocMaxN * sizeof(int));
-constexpr size_t kOffCandVal = align256(kOffCandRows + (size_t)2 * kNoAllocMaxG * kNoAllocNB * sizeof(double2));
-constexpr size_t kOffCandIdx = align256(kOffCandVal + (size_t)2 * kNoAllocMaxG * sizeof(double));
-constexpr size_t kOffRowj = align256(kOffCandIdx + (size_t)2 * kNoAllocMaxG * sizeof(int));
+constexpr size_t kOffKeys = align256(kOffCandRows + (size_t)2 * kNoAllocMaxG * kNoAllocNB * sizeof(double2));
+constexpr size_t kOffRowj = align256(kOffKeys + (size_t)kNoAllocNB * sizeof(unsigned long long));
 constexpr size_t kOffStatus = align256(kOffRowj + (size_t)2 * kNoAllocNB * sizeof(double2));
 constexpr size_t kScratchBytes = align256(kOffStatus + 64 * sizeof(int));  // about 5.8 MB
 
@@ -127,6 +126,7 @@ extern "C" int hprmat_b200_solve_linear_noalloc(const void* d_A, void* d_B, int 
     const size_t smem = ((size_t)NB * (rpc | 1) + NB) * sizeof(T);
     if (smem > 48 * 1024) HPR_CUDA_TRY(cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     HPR_CUDA_TRY(cudaMemsetAsync(status + SW_BARRIER, 0, sizeof(int), st));
+    HPR_CUDA_TRY(cudaMemsetAsync(base + kOffKeys, 0, (size_t)NB * sizeof(unsigned long long), st));
     PanelArgs<T> pa;
     pa.W = W;
     pa.ld = ld;
@@ -137,8 +137,7 @@ extern "C" int hprmat_b200_solve_linear_noalloc(const void* d_A, void* d_B, int 
     pa.G = G;
     pa.ipiv = ipiv;
     pa.cand_rows = reinterpret_cast<T*>(base + kOffCandRows);
-    pa.cand_val = reinterpret_cast<double*>(base + kOffCandVal);
-    pa.cand_idx = reinterpret_cast<int*>(base + kOffCandIdx);
+    pa.keys = reinterpret_cast<unsigned long long*>(base + kOffKeys);
     pa.rowj = reinterpret_cast<T*>(base + kOffRowj);
     pa.status = status;
     int* swb = swaps + (size_t)sidx * kSwapStrideNA;
@@ -185,11 +184,14 @@ extern "C" int hprmat_b200_solve_linear_noalloc(const void* d_A, void* d_B, int 
   ik<<<dim3(nsteps, 2), NT, ism, st>>>(W, ld, N, NB, inv);
   HPR_CUDA_TRY(cudaGetLastError());
   // forward and backward substitution
-  auto dk = diag_apply_kernel<T, NB>;
+  constexpr int DCW = 2;
+  auto dk = diag_apply_kernel<T, NB, DCW>;
+  const size_t dsm = ((size_t)NB * NB + 2 * DCW * NB) * sizeof(T);
+  if (dsm > 48 * 1024) HPR_CUDA_TRY(cudaFuncSetAttribute(dk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
   for (int sidx = 0; sidx < nsteps; ++sidx) {
     const int k0 = sidx * NB, ncols = std::min(NB, N - k0);
     const int* sw = swaps + (size_t)sidx * kSwapStrideNA;
-    dk<<<nrhs, NB, 0, st>>>(inv + (size_t)2 * sidx * NB * NB, ncols, k0, sw, sw + kMaxNB, sw + 2 * kMaxNB,
+    dk<<<(nrhs + DCW - 1) / DCW, NB * DCW, dsm, st>>>(inv + (size_t)2 * sidx * NB * NB, ncols, k0, sw, sw + kMaxNB, sw + 2 * kMaxNB,
                             sw + 3 * kMaxNB, X, ld, nrhs, nullptr, 0);
     HPR_CUDA_TRY(cudaGetLastError());
     const int M2 = N - k0 - ncols;
@@ -202,7 +204,7 @@ extern "C" int hprmat_b200_solve_linear_noalloc(const void* d_A, void* d_B, int 
   }
   for (int sidx = nsteps - 1; sidx >= 0; --sidx) {
     const int k0 = sidx * NB, ncols = std::min(NB, N - k0);
-    dk<<<nrhs, NB, 0, st>>>(inv + ((size_t)2 * sidx + 1) * NB * NB, ncols, k0, nullptr, nullptr, nullptr, nullptr, X,
+    dk<<<(nrhs + DCW - 1) / DCW, NB * DCW, dsm, st>>>(inv + ((size_t)2 * sidx + 1) * NB * NB, ncols, k0, nullptr, nullptr, nullptr, nullptr, X,
                             ld, nrhs, nullptr, 0);
     HPR_CUDA_TRY(cudaGetLastError());
     if (k0 > 0) {

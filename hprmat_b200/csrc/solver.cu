@@ -273,17 +273,15 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
   int* status = c->status.as<int>();
   HPR_CUDA_TRY(cudaMemsetAsync(status, 0, SW_COUNT * sizeof(int), c->stream));
   const int G0 = std::min(c->nsm, std::max(1, (N + 31) / 32));
-  TRY(c->stage.ensure((size_t)2 * G0 * NB * sizeof(T) + (size_t)4 * G0 * sizeof(double) +
+  TRY(c->stage.ensure((size_t)2 * G0 * NB * sizeof(T) + (size_t)NB * sizeof(unsigned long long) +
                       (size_t)2 * NB * sizeof(T) + 256));
   TRY(c->swaps.ensure((size_t)nsteps * kSwapStride * sizeof(int)));
   TRY(c->ipiv.ensure((size_t)N * sizeof(int) + 64));
   unsigned char* sp = c->stage.as<unsigned char>();
   T* cand_rows = reinterpret_cast<T*>(sp);
   sp += (size_t)2 * G0 * NB * sizeof(T);
-  typename RealOf<T>::R* cand_val = reinterpret_cast<typename RealOf<T>::R*>(sp);
-  sp += (size_t)2 * G0 * sizeof(double);
-  int* cand_idx = reinterpret_cast<int*>(sp);
-  sp += (size_t)2 * G0 * sizeof(double);
+  unsigned long long* keys = reinterpret_cast<unsigned long long*>(sp);
+  sp += (size_t)NB * sizeof(unsigned long long);
   T* rowj = reinterpret_cast<T*>(sp);
   unsigned* growth = reinterpret_cast<unsigned*>(status + SW_COUNT - 1);
 
@@ -300,7 +298,7 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
     if (N > NB) {  // views are used only when there is more than one block step
       if (tc_make_operand(c->tcplan, c->op_lu, c->lup.as<float>(), N, N, c->lup_ld, c->lup_plane, 128))
         return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
-      if (tc_make_operand(c->tcplan, c->op_bop, bop, NB, N, NB, plane, 256))
+      if (tc_make_operand(c->tcplan, c->op_bop, bop, NB, N, NB, plane, 128))
         return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
     }
   }
@@ -315,6 +313,7 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
     const size_t smem = ((size_t)NB * (rpc | 1) + NB) * sizeof(T);
     TRY(set_smem(pk, smem));
     HPR_CUDA_TRY(cudaMemsetAsync(status + SW_BARRIER, 0, sizeof(int), c->stream));
+    HPR_CUDA_TRY(cudaMemsetAsync(keys, 0, (size_t)NB * sizeof(unsigned long long), c->stream));
     PanelArgs<T> pa;
     pa.W = W;
     pa.ld = ld;
@@ -325,8 +324,7 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
     pa.G = G;
     pa.ipiv = c->ipiv.as<int>();
     pa.cand_rows = cand_rows;
-    pa.cand_val = cand_val;
-    pa.cand_idx = cand_idx;
+    pa.keys = keys;
     pa.rowj = rowj;
     pa.status = status;
     int* swb = c->swaps.as<int>() + (size_t)s * kSwapStride;
@@ -377,7 +375,7 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
       const bool prof = c->profile && c->ev_used + 2 <= (int)c->ev.size();
       if (prof) HPR_CUDA_TRY(cudaEventRecord(c->ev[c->ev_used], c->stream));
       if (tc_update(c->tcplan, c->op_lu, k0, k0 + ncols, c->op_bop, 0, 0, NB,
-                    reinterpret_cast<float2*>(W) + (k0 + ncols) + (size_t)(k0 + ncols) * ld, ld, M2, M2, 256,
+                    reinterpret_cast<float2*>(W) + (k0 + ncols) + (size_t)(k0 + ncols) * ld, ld, M2, M2, 128,
                     c->stream))
         return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
       ++c->launches;
@@ -444,12 +442,15 @@ static int lu_solve_impl(hprmat_b200_ctx* c, const T* W, const LUState& st, T* X
   const int N = st.N;
   const long ld = st.ld;
   const T* inv = c->inv.as<T>();
-  auto dk = diag_apply_kernel<T, NB>;
+  constexpr int DCW = 2;
+  auto dk = diag_apply_kernel<T, NB, DCW>;
+  const size_t dsm = ((size_t)NB * NB + 2 * DCW * NB) * sizeof(T);
+  TRY(set_smem(dk, dsm));
   const int* swb = c->swaps.as<int>();
   for (int s = 0; s < st.nsteps; ++s) {
     const int k0 = s * NB, ncols = std::min(NB, N - k0);
     const int* sw = swb + (size_t)s * kSwapStride;
-    dk<<<nrhs, NB, 0, c->stream>>>(inv + (size_t)2 * s * NB * NB, ncols, k0, sw, sw + kMaxNB, sw + 2 * kMaxNB,
+    dk<<<cdiv_u(nrhs, DCW), NB * DCW, dsm, c->stream>>>(inv + (size_t)2 * s * NB * NB, ncols, k0, sw, sw + kMaxNB, sw + 2 * kMaxNB,
                                    sw + 3 * kMaxNB, X, ldx, nrhs, nullptr, 0);
     LAUNCH_CHECK();
     const int M2 = N - k0 - ncols;
@@ -462,7 +463,7 @@ static int lu_solve_impl(hprmat_b200_ctx* c, const T* W, const LUState& st, T* X
   }
   for (int s = st.nsteps - 1; s >= 0; --s) {
     const int k0 = s * NB, ncols = std::min(NB, N - k0);
-    dk<<<nrhs, NB, 0, c->stream>>>(inv + ((size_t)2 * s + 1) * NB * NB, ncols, k0, nullptr, nullptr, nullptr,
+    dk<<<cdiv_u(nrhs, DCW), NB * DCW, dsm, c->stream>>>(inv + ((size_t)2 * s + 1) * NB * NB, ncols, k0, nullptr, nullptr, nullptr,
                                    nullptr, X, ldx, nrhs, nullptr, 0);
     LAUNCH_CHECK();
     if (k0 > 0) {
@@ -482,7 +483,10 @@ template <int NB>
 static int lu_solve_tc_impl(hprmat_b200_ctx* c, const LUState& st, float2* X, long ldx, int nrhs) {
   const int N = st.N;
   const float2* inv = c->inv.as<float2>();
-  auto dk = diag_apply_kernel<float2, NB>;
+  constexpr int DCW = 2;
+  auto dk = diag_apply_kernel<float2, NB, DCW>;
+  const size_t dsm = ((size_t)NB * NB + 2 * DCW * NB) * sizeof(float2);
+  TRY(set_smem(dk, dsm));
   const int npad = (nrhs + 127) / 128 * 128;
   if (c->rop_nrhs != npad || !c->rop.p) {
     c->rop_plane = (long)npad * NB;
@@ -498,7 +502,7 @@ static int lu_solve_tc_impl(hprmat_b200_ctx* c, const LUState& st, float2* X, lo
     const int k0 = s * NB, ncols = std::min(NB, N - k0);
     const int* sw = swb + (size_t)s * kSwapStride;
     const int M2 = N - k0 - ncols;
-    dk<<<nrhs, NB, 0, c->stream>>>(inv + (size_t)2 * s * NB * NB, ncols, k0, sw, sw + kMaxNB, sw + 2 * kMaxNB,
+    dk<<<cdiv_u(nrhs, DCW), NB * DCW, dsm, c->stream>>>(inv + (size_t)2 * s * NB * NB, ncols, k0, sw, sw + kMaxNB, sw + 2 * kMaxNB,
                                    sw + 3 * kMaxNB, X, ldx, nrhs, M2 > 0 ? rop : nullptr, c->rop_plane);
     LAUNCH_CHECK();
     if (M2 > 0) {
@@ -510,7 +514,7 @@ static int lu_solve_tc_impl(hprmat_b200_ctx* c, const LUState& st, float2* X, lo
   }
   for (int s = st.nsteps - 1; s >= 0; --s) {
     const int k0 = s * NB, ncols = std::min(NB, N - k0);
-    dk<<<nrhs, NB, 0, c->stream>>>(inv + ((size_t)2 * s + 1) * NB * NB, ncols, k0, nullptr, nullptr, nullptr,
+    dk<<<cdiv_u(nrhs, DCW), NB * DCW, dsm, c->stream>>>(inv + ((size_t)2 * s + 1) * NB * NB, ncols, k0, nullptr, nullptr, nullptr,
                                    nullptr, X, ldx, nrhs, k0 > 0 ? rop : nullptr, c->rop_plane);
     LAUNCH_CHECK();
     if (k0 > 0) {
@@ -682,13 +686,13 @@ static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W3
         change = c->h_norms[1] > 0 ? sqrt(c->h_norms[0] / c->h_norms[1]) : 0.0;
       }
     }
-    if (op.structured) {
-      // rounding scale of the residual at the current iterate: u || |B| + |C||X| ||_F / ||B||_F
+    if (op.structured && outer == 0) {
+      // rounding scale of the residual: u || |B| + |C||X| ||_F / ||B||_F (reported only)
       TRY(apply_residual(c, op, X64, ldx, nrhs, V + vstride, ldv, true, true));
       double fn;
       TRY(frob_norm(c, V + vstride, ldv, N, nrhs, &fn));
       floor_rel = 1.1102230246251565e-16 * fn / bnorm;
-      if (stats && outer < 9) stats->floor_history[outer] = floor_rel;
+      if (stats) stats->floor_history[0] = floor_rel;
     }
     if (stats && outer < 9) stats->residual_history[outer] = rel;
     if (stats) {

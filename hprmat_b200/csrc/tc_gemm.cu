@@ -9,14 +9,16 @@
 //   Re += Ar*Br - Ai*Bi,   Im += Ar*Bi + Ai*Br      -> 12 MMAs per K-step of 8.
 // The minus sign comes from the A-negate bit of the instruction descriptor.
 //
-// Tile 128 (rows) x BN (columns, 256 for the trailing update, 128 for right-hand sides);
-// Re and Im accumulate in TMEM columns [0,BN) and [BN,2BN).  One persistent CTA per SM,
-// 6 warps:
+// Tile 128 (rows) x BN columns (BN = 128 for the LU and the solves; 256 kept for
+// comparison).  Re and Im accumulate in 2 BN TMEM columns; with BN = 128 two such sets are
+// used alternately so the epilogue of one tile overlaps the MMAs of the next.  One
+// persistent CTA per SM, 10 warps:
 //   warp 0     TMA producer: per K-chunk of 16 one 3-D box for the 4 A planes
 //              (16 x 128 x 4 floats) and one for the 4 B planes (16 x BN x 4), 64-byte
-//              swizzle, into a multi-stage ring; also prefetches the next C tile into L2;
+//              swizzle, into a 3-stage ring (2 for BN = 256);
 //   warp 1     TMEM allocator and single-thread MMA issuer;
-//   warps 2-5  epilogue: tcgen05.ld of Re/Im, C -= acc, coalesced along rows.
+//   warps 2-9  epilogue: tcgen05.ld of Re/Im, C -= acc, coalesced along rows (two warps per
+//              TMEM lane quarter, each half of the tile's columns).
 // Every mbarrier wait is bounded; on expiry the kernel records the site in *err, stops
 // issuing work, waits (bounded) for its own TMA copies and frees its TMEM.
 #include <cuda.h>
@@ -38,9 +40,13 @@ template <int BN> struct TileCfg {
   static constexpr int kStageBytes = kABytes + kBBytes;
   static constexpr int kStages = (200 * 1024) / kStageBytes;   // 2 (BN=256) / 3 (BN=128)
   static constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*barriers*/ + 1024 /*align*/;
-  static constexpr int kTmemCols = 2 * BN;
+  // accumulator sets (Re + Im, 2 BN columns each) in the 512 TMEM columns: with two, the
+  // epilogue of one tile overlaps the MMAs of the next
+  static constexpr int kBufs = (4 * BN <= 512) ? 2 : 1;
+  static constexpr int kTmemCols = 512;
 };
-constexpr int kThreads = 192;
+constexpr int kEpiWarps = 8;                         // 2 per TMEM lane quarter
+constexpr int kThreads = 32 * (2 + kEpiWarps);
 constexpr unsigned kWaitLimit = 1u << 26;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -88,9 +94,6 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
-__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
 
 // Shared-memory matrix descriptor, K-major, 64-byte swizzle: rows of 64 bytes, 8-row
 // groups 512 bytes apart (stride byte offset), leading byte offset unused (1), version 1.
@@ -164,9 +167,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* acc_full = empty + kStages;
-  uint64_t* acc_empty = acc_full + 1;
-  uint64_t* drain = acc_empty + 1;
+  constexpr int kBufs = Cfg::kBufs;
+  uint64_t* acc_full = empty + kStages;       // [kBufs]
+  uint64_t* acc_empty = acc_full + kBufs;     // [kBufs]
+  uint64_t* drain = acc_empty + kBufs;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
@@ -182,8 +186,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(acc_full, 1);
-    mbar_init(acc_empty, 128);
+    for (int b = 0; b < kBufs; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 32 * kEpiWarps);
+    }
     mbar_init(drain, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -208,15 +214,6 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         const int m0 = (t % mt) * kBM;
         const int n0 = (t / mt) * kBN;
-        // warm L2 with this tile of C for the epilogue
-        const int rows = min(kBM, M - m0);
-        const uint32_t cbytes = (uint32_t)((rows * 8) & ~15);
-        if (cbytes > 0) {
-          for (int c = 0; c < kBN && n0 + c < Nc; ++c) {
-            const float2* pc = C + m0 + (size_t)(n0 + c) * ldc;
-            if ((reinterpret_cast<uintptr_t>(pc) & 15u) == 0) prefetch_l2(pc, cbytes);
-          }
-        }
         for (int kc = 0; kc < kChunks; ++kc) {
           if (!mbar_wait(&empty[stage], phase ^ 1u, abort_flag, err, 11)) { ok = false; break; }
           unsigned char* sa = smem + stage * kStageBytes;
@@ -240,12 +237,15 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp == 1) {
     if (lane == 0) {
       int stage = 0;
-      uint32_t phase = 0, acc_phase = 0;
+      uint32_t phase = 0;
       bool ok = true;
       const uint32_t id_pos = idesc_tf32<BN>(false), id_neg = idesc_tf32<BN>(true);
-      const uint32_t t_re = tmem, t_im = tmem + kBN;
-      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-        if (!mbar_wait(acc_empty, acc_phase ^ 1u, abort_flag, err, 21)) break;
+      int local = 0;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++local) {
+        const int buf = local % kBufs;
+        const uint32_t use = (uint32_t)(local / kBufs);
+        const uint32_t t_re = tmem + (uint32_t)(buf * 2 * kBN), t_im = t_re + kBN;
+        if (!mbar_wait(&acc_empty[buf], (use & 1u) ^ 1u, abort_flag, err, 21)) break;
         tc_fence_after();
         for (int kc = 0; kc < kChunks; ++kc) {
           if (!mbar_wait(&full[stage], phase, abort_flag, err, 22)) { ok = false; break; }
@@ -282,8 +282,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (++stage == kStages) { stage = 0; phase ^= 1u; }
         }
         if (!ok) break;
-        mma_commit(acc_full);
-        acc_phase ^= 1u;
+        mma_commit(&acc_full[buf]);
       }
       if (!ok || *abort_flag) {
         // make sure no MMA of ours is still reading shared memory or writing TMEM
@@ -292,22 +291,25 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
   } else {
-    // epilogue warps 2..5: TMEM lane quarter q = warp % 4
+    // epilogue warps 2..9: TMEM lane quarter q = warp % 4, column half (warp - 2) / 4
     const int q = warp & 3;
-    uint32_t acc_phase = 0;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int c_begin = ((warp - 2) >> 2) * (kBN / 2);
+    int local = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++local) {
       const int m0 = (t % mt) * kBM;
       const int n0 = (t / mt) * kBN;
+      const int buf = local % kBufs;
+      const uint32_t use = (uint32_t)(local / kBufs);
       bool ok = true;
-      if (lane == 0) ok = mbar_wait(acc_full, acc_phase, abort_flag, err, 31);
+      if (lane == 0) ok = mbar_wait(&acc_full[buf], use & 1u, abort_flag, err, 31);
       ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
       if (!ok) break;
       __syncwarp();
       tc_fence_after();
       const int row = m0 + q * 32 + lane;
       const bool rv = row < M;
-      const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16);
-      for (int c0 = 0; c0 < kBN; c0 += 16) {
+      const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 2 * kBN);
+      for (int c0 = c_begin; c0 < c_begin + kBN / 2; c0 += 16) {
         if (n0 + c0 >= Nc) break;  // warp-uniform
         float2 cv[16];
 #pragma unroll
@@ -326,8 +328,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
       }
       tc_fence_before();
-      mbar_arrive(acc_empty);
-      acc_phase ^= 1u;
+      mbar_arrive(&acc_empty[buf]);
     }
   }
   tc_fence_before();

@@ -39,7 +39,8 @@ def ctx():
 
 # ---------------------------------------------------------------- tensor-core kernel
 @pytest.mark.parametrize("M,Nc,nb,bn", [(128, 256, 128, 256), (300, 520, 128, 256), (1000, 700, 64, 256),
-                                        (77, 33, 32, 256), (640, 128, 128, 128), (129, 200, 64, 128)])
+                                        (77, 33, 32, 256), (640, 128, 128, 128), (129, 200, 64, 128),
+                                        (4096, 1100, 128, 128), (2500, 2100, 64, 256)])
 def test_tc_update_kernel_matches_fp64(ctx, M, Nc, nb, bn):
     lib = nat.load()
     g = torch.Generator(device="cpu").manual_seed(M + Nc)
