@@ -592,4 +592,184 @@ __global__ void __launch_bounds__(NB * CW) diag_apply_kernel(const T* __restrict
   }
 }
 
+// -------------------------------------------------------------------------------------
+// Tensor-core TRSM of the mixed path (U12 = L11^-1 P A12), in three steps per block step:
+//   l11_inverse_planes_kernel: Linv = L11^-1 (unit lower, one CTA, column sweeps as xTRTI2)
+//       written as the A-operand planes of (I - Linv), K-major rows;
+//   swap_gather_kernel: applies the step's row interchanges to the columns right of the
+//       panel, leaving P A12 in rows k0.. of W and as B-operand planes (per column K-major);
+//   tc_update: C -= (I - Linv) (P A12) with C = those rows of W, i.e. C = Linv P A12 = U12;
+//   u12_split_kernel: U12 -> B-operand planes of the trailing update and the LU planes.
+// Inverse of the unit lower triangle L11 in shared memory by recursive blocking: the
+// diagonal blocks of (up to) 32 x 32 are inverted by one warp each, all at once (column
+// sweeps, as xTRTI2), then pairs of blocks are joined with
+//   [A 0; B C]^-1 = [A^-1 0; -C^-1 B A^-1  C^-1]
+// until the whole NB x NB block is done.  Dynamic shared memory: (NB*NB + (NB/2)^2) float2.
+template <int NB, int NT>
+__global__ void __launch_bounds__(NT) l11_inverse_planes_kernel(const float2* __restrict__ W, long ld, int k0,
+                                                                 int ncols, float* planes, long plane) {
+  constexpr int B0 = NB < 32 ? NB : 32;
+  static_assert(NT >= 32 * (NB / B0), "one warp per diagonal block");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* S = reinterpret_cast<float2*>(smem_raw);  // [NB][NB] column-major, L11 -> L11^-1 in place
+  float2* T = S + NB * NB;                          // [NB/2][NB/2] scratch
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  for (int idx = tid; idx < NB * NB; idx += NT) {
+    int i = idx % NB, j = idx / NB;
+    float2 v = make_float2(0.f, 0.f);
+    if (i < ncols && j < ncols && i > j) v = W[(size_t)(k0 + i) + (size_t)(k0 + j) * ld];
+    if (i == j) v.x = 1.f;
+    S[idx] = v;
+  }
+  __syncthreads();
+  // level 0: warp w inverts the diagonal block [B0 w, B0 w + B0)
+  if (warp < NB / B0) {
+    const int b = B0 * warp;
+    const bool in = lane < B0;
+    for (int j = B0 - 2; j >= 0; --j) {
+      const float2 l = in ? S[(b + lane) + (b + j) * NB] : make_float2(0.f, 0.f);  // lane k: L[k][j]
+      float2 acc = make_float2(0.f, 0.f);
+      for (int k = j + 1; k < B0; ++k) {
+        float2 lk;
+        lk.x = __shfl_sync(0xffffffffu, l.x, k);
+        lk.y = __shfl_sync(0xffffffffu, l.y, k);
+        if (in && k <= lane) cfma(acc, S[(b + lane) + (b + k) * NB], lk);  // Linv[i][k], Linv[i][i] = 1
+      }
+      __syncwarp();
+      if (in && lane > j) S[(b + lane) + (b + j) * NB] = make_float2(-acc.x, -acc.y);
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  // join blocks of size h into blocks of size 2h
+  for (int h = B0; h < NB; h *= 2) {
+    const int npair = NB / (2 * h);
+    // T = B * Ainv for every pair (B: rows [a+h, a+2h), cols [a, a+h))
+    for (int idx = tid; idx < npair * h * h; idx += NT) {
+      int pr = idx / (h * h), r = idx % (h * h);
+      int i = r % h, j = r / h;
+      int a = pr * 2 * h;
+      float2 acc = make_float2(0.f, 0.f);
+      for (int k = j; k < h; ++k) cfma(acc, S[(a + h + i) + (a + k) * NB], S[(a + k) + (a + j) * NB]);
+      T[pr * h * h + i + j * h] = acc;
+    }
+    __syncthreads();
+    // B := -Cinv * T  (Cinv: rows/cols [a+h, a+2h), lower)
+    for (int idx = tid; idx < npair * h * h; idx += NT) {
+      int pr = idx / (h * h), r = idx % (h * h);
+      int i = r % h, j = r / h;
+      int a = pr * 2 * h;
+      float2 acc = make_float2(0.f, 0.f);
+      for (int k = 0; k <= i; ++k) cfma(acc, S[(a + h + i) + (a + h + k) * NB], T[pr * h * h + k + j * h]);
+      S[(a + h + i) + (a + j) * NB] = make_float2(-acc.x, -acc.y);
+    }
+    __syncthreads();
+  }
+  // (I - Linv) as A-operand planes: row i, K index j contiguous
+  for (int idx = tid; idx < NB * NB; idx += NT) {
+    int j = idx % NB, i = idx / NB;
+    float2 v = S[i + j * NB];
+    float2 d = make_float2((i == j ? 1.f : 0.f) - v.x, -v.y);
+    if (i >= ncols || j >= ncols) d = make_float2(0.f, 0.f);
+    float hr, lr, hi_, li;
+    tf32_split(d.x, hr, lr);
+    tf32_split(d.y, hi_, li);
+    planes[idx] = hr;
+    planes[plane + idx] = lr;
+    planes[2 * plane + idx] = hi_;
+    planes[3 * plane + idx] = li;
+  }
+}
+
+// Row interchanges of one step on columns [c_begin, c_end) of W, leaving P A12 in rows
+// k0 .. k0+ncols and as B-operand planes bg[(col - c_begin) * NB + j] (zero padded).
+template <int NB, int CW, int NT>
+__global__ void __launch_bounds__(NT) swap_gather_kernel(float2* W, long ld, int k0, int ncols,
+                                                         const int* __restrict__ top_src,
+                                                         const int* __restrict__ extra_dst,
+                                                         const int* __restrict__ extra_src,
+                                                         const int* __restrict__ n_extra, int c_begin, int c_end,
+                                                         float* bg, long plane) {
+  constexpr int NBP = NB + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* A = reinterpret_cast<float2*>(smem_raw);  // [CW][NBP]
+  float2* E = A + CW * NBP;                         // [CW][NB]
+  const int tid = threadIdx.x;
+  const int cb = c_begin + blockIdx.x * CW;
+  const int ncw = min(CW, c_end - cb);
+  if (ncw <= 0) return;
+  const int ne = *n_extra;
+  for (int idx = tid; idx < ncw * ncols; idx += NT) {
+    int j = idx % ncols, cc = idx / ncols;
+    A[cc * NBP + j] = W[(size_t)top_src[j] + (size_t)(cb + cc) * ld];
+  }
+  for (int idx = tid; idx < ncw * ne; idx += NT) {
+    int e = idx % ne, cc = idx / ne;
+    E[cc * NB + e] = W[(size_t)extra_src[e] + (size_t)(cb + cc) * ld];
+  }
+  __syncthreads();
+  for (int idx = tid; idx < ncw * ne; idx += NT) {
+    int e = idx % ne, cc = idx / ne;
+    W[(size_t)extra_dst[e] + (size_t)(cb + cc) * ld] = E[cc * NB + e];
+  }
+  for (int idx = tid; idx < ncw * NB; idx += NT) {
+    int j = idx % NB, cc = idx / NB;
+    float2 v = j < ncols ? A[cc * NBP + j] : make_float2(0.f, 0.f);
+    if (j < ncols) W[(size_t)(k0 + j) + (size_t)(cb + cc) * ld] = v;
+    float hr, lr, hi_, li;
+    tf32_split(v.x, hr, lr);
+    tf32_split(v.y, hi_, li);
+    size_t off = (size_t)(cb + cc - c_begin) * NB + j;
+    bg[off] = hr;
+    bg[plane + off] = lr;
+    bg[2 * plane + off] = hi_;
+    bg[3 * plane + off] = li;
+  }
+}
+
+// U12 (rows k0 .. k0+ncols of W, columns [c_begin, c_end)) -> B-operand planes of the
+// trailing update (per column K-major) and the row-major LU planes; tracks max |u_ij|.
+template <int NB, int CW, int NT>
+__global__ void __launch_bounds__(NT) u12_split_kernel(const float2* __restrict__ W, long ld, int k0, int ncols,
+                                                       int c_begin, int c_end, float* bop, long bplane, float* lup,
+                                                       long lup_ld, long lup_plane, unsigned* growth_bits) {
+  const int tid = threadIdx.x;
+  const int cb = c_begin + blockIdx.x * CW;
+  const int ncw = min(CW, c_end - cb);
+  if (ncw <= 0) return;
+  float gmax = 0.f;
+  // per column K-major operand: consecutive threads -> consecutive rows of one column
+  for (int idx = tid; idx < ncw * NB; idx += NT) {
+    int j = idx % NB, cc = idx / NB;
+    float2 v = j < ncols ? W[(size_t)(k0 + j) + (size_t)(cb + cc) * ld] : make_float2(0.f, 0.f);
+    gmax = fmaxf(gmax, fabsf(v.x) + fabsf(v.y));
+    float hr, lr, hi_, li;
+    tf32_split(v.x, hr, lr);
+    tf32_split(v.y, hi_, li);
+    size_t off = (size_t)(cb + cc - c_begin) * NB + j;
+    bop[off] = hr;
+    bop[bplane + off] = lr;
+    bop[2 * bplane + off] = hi_;
+    bop[3 * bplane + off] = li;
+  }
+  // row-major LU planes: consecutive threads -> consecutive columns of one row
+  for (int idx = tid; idx < ncw * ncols; idx += NT) {
+    int cc = idx % ncw, j = idx / ncw;
+    float2 v = W[(size_t)(k0 + j) + (size_t)(cb + cc) * ld];
+    float hr, lr, hi_, li;
+    tf32_split(v.x, hr, lr);
+    tf32_split(v.y, hi_, li);
+    size_t off = (size_t)(k0 + j) * lup_ld + (size_t)(cb + cc);
+    lup[off] = hr;
+    lup[lup_plane + off] = lr;
+    lup[2 * lup_plane + off] = hi_;
+    lup[3 * lup_plane + off] = li;
+  }
+  if (growth_bits) {
+    for (int o = 16; o > 0; o >>= 1) gmax = fmaxf(gmax, __shfl_down_sync(0xffffffffu, gmax, o));
+    if ((tid & 31) == 0 && gmax > 0.f) atomicMax(growth_bits, __float_as_uint(gmax));
+  }
+}
+
 }  // namespace hprmat

@@ -98,9 +98,9 @@ struct hprmat_b200_ctx {
   DevBuf mesh;  // tc | blo0 | r | q2
   // work buffers
   DevBuf W, A64, X, X64, R64, B64, V, Z, gm, swaps, ipiv, stage, status, ops, inv, chan, rmat,
-      zwork, cpot, cu, norms, lup, rop, rsurf, vt, rlo;
+      zwork, cpot, cu, norms, lup, rop, rsurf, vt, rlo, linv;
   // tensor-core operand views of the current factorisation (mixed path)
-  TcOperand op_lu, op_bop, op_rhs;
+  TcOperand op_lu, op_bop, op_rhs, op_linv;
   long lup_ld = 0, lup_plane = 0, rop_plane = 0;
   int rop_nrhs = 0;
   int* h_status = nullptr;  // pinned
@@ -295,7 +295,10 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
     c->lup_ld = (N + 3) / 4 * 4;
     c->lup_plane = c->lup_ld * (long)N;
     TRY(c->lup.ensure((size_t)4 * c->lup_plane * sizeof(float)));
+    TRY(c->linv.ensure((size_t)4 * NB * NB * sizeof(float)));
     if (N > NB) {  // views are used only when there is more than one block step
+      if (tc_make_operand(c->tcplan, c->op_linv, c->linv.as<float>(), NB, NB, NB, (long)NB * NB, 128))
+        return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
       if (tc_make_operand(c->tcplan, c->op_lu, c->lup.as<float>(), N, N, c->lup_ld, c->lup_plane, 128))
         return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
       if (tc_make_operand(c->tcplan, c->op_bop, bop, NB, N, NB, plane, 128))
@@ -341,12 +344,38 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
     ++c->launches;
     if (k0 + ncols >= N) break;
     // row interchanges + U12 = L11^-1 A12
-    {
+    if (mixed) {
+      // L11^-1 (as I - L11^-1 operand planes), P A12 gathered, U12 by one tensor-core GEMM
+      constexpr int CW = 32;
+      const size_t ism = ((size_t)NB * NB + (size_t)(NB / 2) * (NB / 2)) * sizeof(float2);
+      auto ik = l11_inverse_planes_kernel<NB, NT>;
+      TRY(set_smem(ik, ism));
+      ik<<<1, NT, ism, c->stream>>>(reinterpret_cast<const float2*>(W), ld, k0, ncols, c->linv.as<float>(),
+                                     (long)NB * NB);
+      LAUNCH_CHECK();
+      auto gk = swap_gather_kernel<NB, CW, NT>;
+      const size_t gsm = (size_t)CW * (NB + 1) * sizeof(float2) + (size_t)CW * NB * sizeof(float2);
+      TRY(set_smem(gk, gsm));
+      gk<<<cdiv_u(N - k0 - ncols, CW), NT, gsm, c->stream>>>(reinterpret_cast<float2*>(W), ld, k0, ncols,
+                                                              pa.sw.top_src, pa.sw.extra_dst, pa.sw.extra_src,
+                                                              pa.sw.n_extra, k0 + ncols, N, bop, plane);
+      LAUNCH_CHECK();
+      if (tc_update(c->tcplan, c->op_linv, 0, 0, c->op_bop, 0, 0, NB,
+                    reinterpret_cast<float2*>(W) + k0 + (size_t)(k0 + ncols) * ld, ld, ncols, N - k0 - ncols, 128,
+                    c->stream))
+        return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+      ++c->launches;
+      auto uk = u12_split_kernel<NB, CW, NT>;
+      uk<<<cdiv_u(N - k0 - ncols, CW), NT, 0, c->stream>>>(reinterpret_cast<const float2*>(W), ld, k0, ncols,
+                                                             k0 + ncols, N, bop, plane, c->lup.as<float>(),
+                                                             c->lup_ld, c->lup_plane, growth);
+      LAUNCH_CHECK();
+    } else {
       constexpr int CW = 32;
       auto tk = trsm_lower_kernel<T, NB, CW, NT>;
       size_t tsm = (size_t)CW * (NB + 1) * sizeof(T) + (size_t)CW * NB * sizeof(T);
       TRY(set_smem(tk, tsm));
-      TrsmArgs<T> ta;
+      TrsmArgs<T> ta{};
       ta.W = W;
       ta.ld = ld;
       ta.k0 = k0;
@@ -359,13 +388,7 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
       ta.ldx = ld;
       ta.c_begin = k0 + ncols;
       ta.c_end = N;
-      ta.bop = mixed ? bop : nullptr;
-      ta.bop_plane = plane;
-      ta.bop_col0 = k0 + ncols;
       ta.growth_bits = growth;
-      ta.lup = mixed ? c->lup.as<float>() : nullptr;
-      ta.lup_ld = c->lup_ld;
-      ta.lup_plane = c->lup_plane;
       tk<<<cdiv_u(N - k0 - ncols, CW), NT, tsm, c->stream>>>(ta);
       LAUNCH_CHECK();
     }
@@ -1151,7 +1174,7 @@ int hprmat_b200_destroy(hprmat_b200_ctx* c) {
   cudaStreamSynchronize(c->stream);
   DevBuf* bufs[] = {&c->mesh, &c->W, &c->A64, &c->X, &c->X64, &c->R64, &c->B64, &c->V, &c->Z, &c->gm,
                     &c->swaps, &c->ipiv, &c->stage, &c->status, &c->ops, &c->inv, &c->chan, &c->rmat,
-                    &c->zwork, &c->cpot, &c->cu, &c->norms, &c->lup, &c->rop, &c->rsurf, &c->vt, &c->rlo};
+                    &c->zwork, &c->cpot, &c->cu, &c->norms, &c->lup, &c->rop, &c->rsurf, &c->vt, &c->rlo, &c->linv};
   for (DevBuf* b : bufs) b->release();
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
   if (c->h_status) cudaFreeHost(c->h_status);
