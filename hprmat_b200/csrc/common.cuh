@@ -69,6 +69,20 @@ template <typename T> __host__ __device__ inline T cdiv(T a, T b) { return cmul(
 __host__ __device__ inline float2 to_f(double2 a) { return make_float2((float)a.x, (float)a.y); }
 __host__ __device__ inline double2 to_d(float2 a) { return make_double2((double)a.x, (double)a.y); }
 
+// ---------------------------------------------------------------- TF32 split
+// Split x into an exactly-representable TF32 head and the FP32 remainder.  hi = x rounded
+// to 10 explicit mantissa bits (round-to-nearest-even on the raw bits), lo = x - hi is
+// exact in FP32 and |lo| <= 2^-11 |x|.
+__device__ __forceinline__ void tf32_split(float x, float& hi, float& lo) {
+  unsigned u = __float_as_uint(x);
+  unsigned r = u + 0x0FFFu + ((u >> 13) & 1u);
+  r &= 0xFFFFE000u;
+  // keep inf/nan as they are
+  if ((u & 0x7F800000u) == 0x7F800000u) r = u;
+  hi = __uint_as_float(r);
+  lo = x - hi;
+}
+
 // ---------------------------------------------------------------- device status words
 // Layout of the per-context device status block (int32 each).
 enum StatusWord {

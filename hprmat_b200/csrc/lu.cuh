@@ -53,20 +53,6 @@ struct PanelArgs {
   long lup_plane;
 };
 
-// -------------------------------------------------------------------------------------
-// Split x into an exactly-representable TF32 head and the FP32 remainder.  hi = x rounded
-// to 10 explicit mantissa bits (round-to-nearest-even on the raw bits), lo = x - hi is
-// exact in FP32 and |lo| <= 2^-11 |x|.
-__device__ __forceinline__ void tf32_split(float x, float& hi, float& lo) {
-  unsigned u = __float_as_uint(x);
-  unsigned r = u + 0x0FFFu + ((u >> 13) & 1u);
-  r &= 0xFFFFE000u;
-  // keep inf/nan as they are
-  if ((u & 0x7F800000u) == 0x7F800000u) r = u;
-  hi = __uint_as_float(r);
-  lo = x - hi;
-}
-
 // Pivot key of a candidate: |re|+|im| (as float bits, monotone for non-negative values) in
 // the high word, the complement of the panel row in the low word, so that one 64-bit
 // atomicMax picks the largest modulus and, among equal ones, the lowest row.  (On the FP64

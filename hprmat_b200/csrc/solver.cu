@@ -10,6 +10,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/hprmat_b200.h"
@@ -19,6 +20,7 @@
 #include "lu.cuh"
 #include "rmat_kernels.cuh"
 #include "tc_gemm.cuh"
+#include "tc_solve.cuh"
 
 using namespace hprmat;
 
@@ -103,6 +105,17 @@ struct hprmat_b200_ctx {
   TcOperand op_lu, op_bop, op_rhs, op_linv;
   long lup_ld = 0, lup_plane = 0, rop_plane = 0;
   int rop_nrhs = 0;
+  // wavefront solves (mixed path, nb = 128): sigma maps and permutation, transposed
+  // off-diagonal blocks, diagonal-inverse planes, right-side / solution planes, flags
+  DevBuf wsig, wperm, wT, wdi, wbp, wyp, wxp, wflags;
+  TcOperand op_wT, op_wdi, op_wbp, op_wyp, op_wxp;
+  bool wave_ready = false;
+  int wave_un = 64;
+  int w_N = 0, w_npad = 0;
+  long w_xld = 0, w_xplane = 0;
+  bool wave_trace = false;
+  DevBuf wtrace;
+  int wtrace_units = 0;
   int* h_status = nullptr;  // pinned
   double* h_norms = nullptr;  // pinned
   TcGemmPlan tcplan;
@@ -260,6 +273,94 @@ static int pick_nb(const hprmat_b200_ctx* c, int N, size_t elem, int preferred) 
     if (smem + 8192 <= (size_t)c->smem_optin) return nb;
   }
   return 0;
+}
+
+// ------------------------------------------------------------------ wavefront solves
+// One-time preparation after a mixed nb = 128 factorisation (tc_solve.cuh): L rows in their
+// final order, off-diagonal blocks scaled by the inverse diagonal blocks of their block row,
+// diagonal inverses as planes.  Overwrites the off-diagonal part of the LU planes.
+static int wave_prepare(hprmat_b200_ctx* c, const LUState& st) {
+  const int N = st.N, ns = st.nsteps;
+  c->wave_ready = false;
+  const long sig_ld = (N + 3) / 4 * 4;
+  TRY(c->wsig.ensure((size_t)ns * sig_ld * sizeof(int)));
+  TRY(c->wperm.ensure((size_t)3 * N * sizeof(int) + 64));
+  int* work = c->wperm.as<int>();
+  int* perm0 = work + 2 * (size_t)N;
+  const long ldt = (N + 3) / 4 * 4;
+  const long tplane = ldt * (long)N;
+  TRY(c->wT.ensure((size_t)4 * tplane * sizeof(float)));
+  const long di_plane = (long)2 * ns * 128 * 128;
+  TRY(c->wdi.ensure((size_t)4 * di_plane * sizeof(float)));
+  if (wave_perm_chain(c->swaps.as<int>(), kSwapStride, N, ns, work, c->wsig.as<int>(), sig_ld, perm0, c->stream) ||
+      wave_transpose_offdiag(c->lup.as<float>(), c->lup_ld, c->lup_plane, c->wsig.as<int>(), sig_ld, N, ns,
+                             c->wT.as<float>(), ldt, tplane, c->stream) ||
+      wave_dinv_planes(c->inv.as<float2>(), ns, c->wdi.as<float>(), di_plane, c->stream) ||
+      tc_make_operand(c->tcplan, c->op_wdi, c->wdi.as<float>(), 128, (long)2 * ns * 128, 128, di_plane, 128) ||
+      tc_make_operand(c->tcplan, c->op_wT, c->wT.as<float>(), N, N, ldt, tplane, 128) ||
+      wave_scale_offdiag(c->tcplan, c->op_wdi, c->op_wT, N, ns, c->lup.as<float>(), c->lup_ld, c->lup_plane,
+                         c->stream))
+    return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+  c->launches += 4;
+  c->wave_ready = true;
+  return HPRMAT_B200_OK;
+}
+
+// X (N x nrhs, FP32 complex, ldx) <- (LU)^-1 P X with the prepared factors: right-hand side
+// planes of P X, forward sweep into the Y planes, backward sweep into X.
+static int lu_solve_wave(hprmat_b200_ctx* c, const LUState& st, float2* X, long ldx, int nrhs) {
+  const int N = st.N, ns = st.nsteps;
+  const int un = c->wave_un;
+  const int G = (nrhs + un - 1) / un;
+  const int npad = G * un;
+  const long xld = (N + 3) / 4 * 4;
+  const long xplane = xld * (long)npad;
+  if (c->w_N != N || c->w_npad != npad || c->w_xld != xld || !c->wbp.p) {
+    c->w_N = 0;
+    const size_t bytes = (size_t)4 * xplane * sizeof(float);
+    TRY(c->wbp.ensure(bytes));
+    TRY(c->wyp.ensure(bytes));
+    TRY(c->wxp.ensure(bytes));
+    HPR_CUDA_TRY(cudaMemsetAsync(c->wbp.p, 0, bytes, c->stream));
+    HPR_CUDA_TRY(cudaMemsetAsync(c->wyp.p, 0, bytes, c->stream));
+    HPR_CUDA_TRY(cudaMemsetAsync(c->wxp.p, 0, bytes, c->stream));
+    if (tc_make_operand(c->tcplan, c->op_wbp, c->wbp.as<float>(), N, npad, xld, xplane, un) ||
+        tc_make_operand(c->tcplan, c->op_wyp, c->wyp.as<float>(), N, npad, xld, xplane, un) ||
+        tc_make_operand(c->tcplan, c->op_wxp, c->wxp.as<float>(), N, npad, xld, xplane, un))
+      return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+    c->w_N = N;
+    c->w_npad = npad;
+    c->w_xld = xld;
+    c->w_xplane = xplane;
+  }
+  TRY(c->wflags.ensure((size_t)2 * ns * G * sizeof(int)));
+  const int* perm0 = c->wperm.as<int>() + 2 * (size_t)N;
+  WaveSolve ws;
+  ws.N = N;
+  ws.nsteps = ns;
+  ws.nrhs = nrhs;
+  ws.un = un;
+  ws.xp = c->wyp.as<float>();
+  ws.xp_ld = xld;
+  ws.xp_plane = xplane;
+  ws.flags = c->wflags.as<int>();
+  if (c->wave_trace) {
+    TRY(c->wtrace.ensure((size_t)2 * ns * G * 4 * sizeof(long long)));
+    c->wtrace_units = ns * G;
+    ws.trace = c->wtrace.as<long long>();
+  }
+  if (wave_rhs_planes(X, ldx, perm0, N, nrhs, c->wbp.as<float>(), xld, xplane, c->stream) ||
+      wave_sweep(c->tcplan, true, c->op_lu, c->op_wdi, c->op_wbp, c->op_wyp, ws, c->stream))
+    return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+  ws.xp = c->wxp.as<float>();
+  ws.xout = X;
+  ws.ldx = ldx;
+  ws.flags = c->wflags.as<int>() + (size_t)ns * G;
+  if (ws.trace) ws.trace += (size_t)ns * G * 4;
+  if (wave_sweep(c->tcplan, false, c->op_lu, c->op_wdi, c->op_wyp, c->op_wxp, ws, c->stream))
+    return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+  c->launches += 3;
+  return HPRMAT_B200_OK;
 }
 
 template <typename T, int NB>
@@ -424,6 +525,10 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
     ik<<<dim3(nsteps, 2), NT, ism, c->stream>>>(W, ld, N, NB, c->inv.as<T>());
     LAUNCH_CHECK();
   }
+  c->wave_ready = false;
+  if constexpr (NB == 128 && std::is_same<T, float2>::value) {
+    if (mixed && nsteps >= 2) TRY(wave_prepare(c, st));
+  }
   HPR_CUDA_TRY(cudaMemcpyAsync(c->h_status, status, SW_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
   if (c->h_status[SW_TIMEOUT] != 0)
@@ -504,6 +609,7 @@ static int lu_solve_impl(hprmat_b200_ctx* c, const T* W, const LUState& st, T* X
 // reads L21 / U12 from the LU planes.
 template <int NB>
 static int lu_solve_tc_impl(hprmat_b200_ctx* c, const LUState& st, float2* X, long ldx, int nrhs) {
+  if (NB == 128 && c->wave_ready) return lu_solve_wave(c, st, X, ldx, nrhs);
   const int N = st.N;
   const float2* inv = c->inv.as<float2>();
   constexpr int DCW = 2;
@@ -780,6 +886,12 @@ static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W3
   if (stats) {
     stats->refine_steps = steps;
     stats->inner_iterations = inner_total;
+  }
+  {
+    // a bounded wait that gave up inside a tensor-core solve invalidates the result
+    int err = 0;
+    TRY(tc_gemm_check(c->tcplan, c->stream, &err));
+    if (err) return fail(HPRMAT_B200_ERR_TIMEOUT, "tensor-core solve: wait limit exceeded at site %d", err);
   }
   return status;
 }
@@ -1391,6 +1503,24 @@ int hprmat_b200_dev_set_profile(hprmat_b200_ctx* c, int enable) {
   }
   c->ev_used = 0;
   c->ev_flops.clear();
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_dev_wave_trace(hprmat_b200_ctx* c, int enable) {
+  TRY(check_ctx(c));
+  c->wave_trace = enable != 0;
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_dev_wave_trace_read(hprmat_b200_ctx* c, long long* out, int cap, int* units) {
+  TRY(check_ctx(c));
+  if (!out || !units || cap < 0) return fail(HPRMAT_B200_ERR_ARG, "null output");
+  *units = c->wtrace_units;
+  const size_t n = std::min((size_t)cap, (size_t)c->wtrace_units * 8);
+  if (n && c->wtrace.p) {
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    HPR_CUDA_TRY(cudaMemcpy(out, c->wtrace.p, n * sizeof(long long), cudaMemcpyDeviceToHost));
+  }
   return HPRMAT_B200_OK;
 }
 

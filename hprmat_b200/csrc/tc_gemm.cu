@@ -26,12 +26,14 @@
 #include <stdint.h>
 
 #include "common.cuh"
+#include "tc_common.cuh"
 #include "tc_gemm.cuh"
 
 namespace hprmat {
 
 namespace {
 
+using namespace tc;
 constexpr int kBM = 128;
 constexpr int kKC = 16;                                 // K values per stage (64 bytes)
 constexpr int kABytes = 4 * kBM * kKC * 4;             // 32 KB
@@ -47,103 +49,6 @@ template <int BN> struct TileCfg {
 };
 constexpr int kEpiWarps = 8;                         // 2 per TMEM lane quarter
 constexpr int kThreads = 32 * (2 + kEpiWarps);
-constexpr unsigned kWaitLimit = 1u << 26;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait: false if the limit was reached or another role already gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err,
-                                          int site) {
-  for (unsigned it = 0; it < kWaitLimit; ++it) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 1023u) == 1023u && *abort_flag) return false;
-  }
-  *abort_flag = 1;
-  atomicCAS(err, 0, site);
-  return false;
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
-      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
-      : "memory");
-}
-
-
-// Shared-memory matrix descriptor, K-major, 64-byte swizzle: rows of 64 bytes, 8-row
-// groups 512 bytes apart (stride byte offset), leading byte offset unused (1), version 1.
-__device__ __forceinline__ uint64_t sdesc_k_sw64(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
-  d |= (uint64_t)1 << 16;                 // LBO (ignored for swizzled K-major)
-  d |= (uint64_t)(512 >> 4) << 32;        // SBO
-  d |= (uint64_t)1 << 46;                 // descriptor version (sm_100)
-  d |= (uint64_t)4 << 61;                 // SWIZZLE_64B
-  return d;
-}
-
-// Instruction descriptor: kind::tf32, D = F32, A = B = TF32, both K-major, M = 128, N = BN.
-template <int BN>
-__host__ __device__ constexpr uint32_t idesc_tf32(bool neg_a) {
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(BN >> 3) << 17) |
-         ((uint32_t)(kBM >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
-      "l"(a), "l"(b), "r"(idesc), "r"(acc)
-      : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr)
-      : "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
 struct TcArgs {
   int a_k0, a_row0, b_k0, b_row0, kchunks;
   float2* C;
@@ -300,23 +205,33 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int n0 = (t / mt) * kBN;
       const int buf = local % kBufs;
       const uint32_t use = (uint32_t)(local / kBufs);
+      const int row = m0 + q * 32 + lane;
+      const bool rv = row < M;
+      const int ncw = min(kBN / 2, Nc - (n0 + c_begin));  // columns of this warp (warp-uniform)
+      // C does not depend on the accumulator: the first chunk's loads go out before the
+      // wait, and each later chunk's loads before the previous chunk is consumed (two
+      // chunks of 16 columns in flight per lane).
+      float2 cv[2][16];
+      auto load_chunk = [&](float2* dst, int c0) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = n0 + c0 + j;
+          dst[j] = (rv && col < Nc) ? C[row + (size_t)col * ldc] : make_float2(0.f, 0.f);
+        }
+      };
+      if (ncw > 0) load_chunk(cv[0], c_begin);
       bool ok = true;
       if (lane == 0) ok = mbar_wait(&acc_full[buf], use & 1u, abort_flag, err, 31);
       ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
       if (!ok) break;
       __syncwarp();
       tc_fence_after();
-      const int row = m0 + q * 32 + lane;
-      const bool rv = row < M;
       const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 2 * kBN);
-      for (int c0 = c_begin; c0 < c_begin + kBN / 2; c0 += 16) {
-        if (n0 + c0 >= Nc) break;  // warp-uniform
-        float2 cv[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int col = n0 + c0 + j;
-          cv[j] = (rv && col < Nc) ? C[row + (size_t)col * ldc] : make_float2(0.f, 0.f);
-        }
+      for (int i = 0; i < kBN / 32; ++i) {
+        const int c0 = c_begin + 16 * i;
+        if (16 * i >= ncw) break;  // warp-uniform
+        if (i + 1 < kBN / 32 && 16 * (i + 1) < ncw) load_chunk(cv[(i + 1) & 1], c0 + 16);
         float re[16], im[16];
         tmem_ld16(tl + c0, re);
         tmem_ld16(tl + kBN + c0, im);
@@ -324,7 +239,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int col = n0 + c0 + j;
-          if (rv && col < Nc) C[row + (size_t)col * ldc] = make_float2(cv[j].x - re[j], cv[j].y - im[j]);
+          if (rv && col < Nc) C[row + (size_t)col * ldc] = make_float2(cv[i & 1][j].x - re[j], cv[i & 1][j].y - im[j]);
         }
       }
       tc_fence_before();
@@ -373,7 +288,7 @@ int tc_gemm_init(TcGemmPlan& p, int device) {
 int tc_make_operand(TcGemmPlan& p, TcOperand& op, const float* base, long kext, long rows, long ld, long plane,
                     int box_rows) {
   if (((uintptr_t)base & 15) || (ld % 4) || (plane % 4) || kext < 16 || rows < 1 || ld < kext ||
-      (box_rows != 128 && box_rows != 256)) {
+      (box_rows != 64 && box_rows != 128 && box_rows != 256)) {
     set_last_error_msg("tensor-core operand: misaligned or invalid view");
     return -1;
   }

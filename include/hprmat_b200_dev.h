@@ -32,6 +32,15 @@ int hprmat_b200_dev_set_profile(hprmat_b200_ctx* ctx, int enable);
 int hprmat_b200_dev_counters(hprmat_b200_ctx* ctx, unsigned long long* launches, double* tc_ms, double* tc_flops,
                              int* tc_launches, int reset);
 
+/* Tracing of the wavefront triangular solves of the mixed path.  With enable != 0 every
+   later sweep records, per unit (block row x right-hand-side group, in dependency order),
+   four device-clock stamps in ns: the producer starts the unit, the last dependency flag
+   was seen, the accumulator was complete, the block was published.
+   hprmat_b200_dev_wave_trace_read copies the stamps of the last forward sweep followed by
+   the last backward sweep (2 x units x 4 values, at most cap) and stores units. */
+int hprmat_b200_dev_wave_trace(hprmat_b200_ctx* ctx, int enable);
+int hprmat_b200_dev_wave_trace_read(hprmat_b200_ctx* ctx, long long* out, int cap, int* units);
+
 #ifdef __cplusplus
 }
 #endif
