@@ -83,6 +83,13 @@ __device__ __forceinline__ void tf32_split(float x, float& hi, float& lo) {
   lo = x - hi;
 }
 
+// Device clock in ns (for optional timing traces).
+__device__ __forceinline__ long long device_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
 // ---------------------------------------------------------------- device status words
 // Layout of the per-context device status block (int32 each).
 enum StatusWord {
@@ -123,6 +130,37 @@ __device__ inline bool grid_barrier(int* counter, int* timeout_flag, unsigned ta
   }
   __syncthreads();
   return s_ok != 0;
+}
+
+// The two halves of grid_barrier, so that a CTA can work between arriving and waiting.
+// grid_arrive is called by thread 0 after a __syncthreads that orders the CTA's writes.
+__device__ inline void grid_arrive(int* counter) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(counter) : "memory");
+}
+// All threads; false when the bounded wait gave up (the caller must return).
+__device__ inline bool grid_wait(int* counter, int* timeout_flag, unsigned target, int site) {
+  __shared__ int s_ok_w;
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    for (unsigned spins = 1;; ++spins) {
+      unsigned v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(counter) : "memory");
+      if (v >= target) break;
+      if ((spins & 4095u) == 0) {
+        int tf;
+        asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(tf) : "l"(timeout_flag) : "memory");
+        if (tf != 0) { ok = 0; break; }
+        if (spins >= (1u << 26)) {
+          atomicExch(timeout_flag, site);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    s_ok_w = ok;
+  }
+  __syncthreads();
+  return s_ok_w != 0;
 }
 
 }  // namespace hprmat

@@ -51,7 +51,11 @@ struct PanelArgs {
   float* lup;
   long lup_ld;
   long lup_plane;
+  // Optional timing trace, per column kPanelTraceW stamps: CTA 0 at column start, candidate
+  // posted, barrier passed, pivot row in place, update done; then every CTA's arrival.
+  long long* trace = nullptr;
 };
+constexpr int kPanelTraceW = 5 + 160;
 
 // Pivot key of a candidate: |re|+|im| (as float bits, monotone for non-negative values) in
 // the high word, the complement of the panel row in the low word, so that one 64-bit
@@ -88,15 +92,10 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
   if (tid == 0) s_growth = 0u;
   __syncthreads();
 
-  for (int j = 0; j < ncols; ++j) {
-    const int buf = j & 1;
-    // (1) local pivot candidate of column j: max |re|+|im| over rows >= j, lowest row on ties
-    float bv = -1.f;
-    int bi = 0x7fffffff;
-    for (int lr = max(j - r0, 0) + tid; lr < nloc; lr += NT) {
-      float v = (float)cabs1(P[(size_t)j * rpcp + lr]);
-      if (v > bv) { bv = v; bi = r0 + lr; }
-    }
+  // Column jc's pivot candidate: the largest |re|+|im| of the local rows >= jc (lowest row on
+  // ties) into s_piv, and its key into the column's global maximum.  v_of(lr) gives the
+  // current value of column jc in local row lr.
+  auto candidate = [&](int jc, float bv, int bi) {
     for (int o = 16; o > 0; o >>= 1) {
       float ov = __shfl_down_sync(0xffffffffu, bv, o);
       int oi = __shfl_down_sync(0xffffffffu, bi, o);
@@ -114,23 +113,66 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
       }
       if (tid == 0) {
         s_piv = bi;
-        if (bi != 0x7fffffff) atomicMax(a.keys + j, pivot_key(bv, bi));
+        if (bi != 0x7fffffff) atomicMax(a.keys + jc, pivot_key(bv, bi));
       }
     }
     __syncthreads();
-    // (2) post the candidate row and, from its owner, the current row j
-    {
-      const int ci = s_piv;
-      const bool have = ci != 0x7fffffff;
-      for (int c = tid; c < ncols; c += NT) {
-        if (have) a.cand_rows[((size_t)buf * a.G + b) * NB + c] = P[(size_t)c * rpcp + (ci - r0)];
-        if (j >= r0 && j < r1) a.rowj[(size_t)buf * NB + c] = P[(size_t)c * rpcp + (j - r0)];
+  };
+  // Post the candidate row of column jc and, from its owner, row jc.  Columns > jc still
+  // wait for the rank-1 update of column jc - 1 (multipliers in column jc - 1, pivot row in
+  // urow) when pend is set; the posted values include it.
+  auto post = [&](int jc, bool pend) {
+    const int pb = jc & 1;
+    const int ci = s_piv;
+    const bool have = ci != 0x7fffffff;
+    const bool own = jc >= r0 && jc < r1;
+    for (int c = tid; c < ncols; c += NT) {
+      if (have) {
+        T v = P[(size_t)c * rpcp + (ci - r0)];
+        if (pend && c > jc) cfms(v, P[(size_t)(jc - 1) * rpcp + (ci - r0)], urow[c]);
+        a.cand_rows[((size_t)pb * a.G + b) * NB + c] = v;
+      }
+      if (own) {
+        T v = P[(size_t)c * rpcp + (jc - r0)];
+        if (pend && c > jc) cfms(v, P[(size_t)(jc - 1) * rpcp + (jc - r0)], urow[c]);
+        a.rowj[(size_t)pb * NB + c] = v;
       }
     }
-    // (3) every CTA has posted
-    if (!grid_barrier(a.status + SW_BARRIER, a.status + SW_TIMEOUT, (unsigned)a.G * (j + 1), 1))
-      return;
-    // (4) the winning key names the pivot row; its owner CTA is row / rpc
+  };
+  auto arrive = [&](int jc) {
+    __syncthreads();
+    if (tid == 0) {
+      if (a.trace) {
+        const long long t = device_ns();
+        long long* tr = a.trace + (size_t)jc * kPanelTraceW;
+        if (b < 160) tr[5 + b] = t;
+        if (b == 0) tr[1] = t;
+      }
+      grid_arrive(a.status + SW_BARRIER);
+    }
+  };
+
+  // column 0: candidate, post, arrive
+  {
+    float bv = -1.f;
+    int bi = 0x7fffffff;
+    for (int lr = max(-r0, 0) + tid; lr < nloc; lr += NT) {
+      float v = (float)cabs1(P[lr]);
+      if (v > bv) { bv = v; bi = r0 + lr; }
+    }
+    candidate(0, bv, bi);
+    post(0, false);
+    arrive(0);
+  }
+  const int warp = tid >> 5, lane = tid & 31;
+  for (int j = 0; j < ncols; ++j) {
+    const int buf = j & 1;
+    long long* tr = a.trace ? a.trace + (size_t)j * kPanelTraceW : nullptr;
+    if (tr && b == 0 && tid == 0) tr[0] = device_ns();
+    // every CTA has posted its candidate of column j
+    if (!grid_wait(a.status + SW_BARRIER, a.status + SW_TIMEOUT, (unsigned)a.G * (j + 1), 1)) return;
+    if (tr && b == 0 && tid == 0) tr[2] = device_ns();
+    // the winning key names the pivot row; its owner CTA is row / rpc
     if (tid == 0) {
       unsigned long long key = __ldcg(a.keys + j);
       s_piv = (int)(0xFFFFFFFFu - (unsigned)(key & 0xFFFFFFFFull));
@@ -153,25 +195,65 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
     }
     if (tid == 0) s_loc_ipiv[j] = p;
     __syncthreads();
-    // (5) scale column j below the diagonal, then rank-1 update of the remaining columns
+    if (tr && b == 0 && tid == 0) tr[3] = device_ns();
+    // scale column j below the diagonal (multipliers; a zero pivot leaves them unscaled, as
+    // xGETF2 does, and is reported in info)
     const T piv = urow[j];
     const bool zero = (piv.x == R(0) && piv.y == R(0));
     if (zero && b == 0 && tid == 0) atomicCAS(a.status + SW_INFO, 0, a.k0 + j + 1);
     const T inv = zero ? czero<T>() : crecip(piv);
     const int lo = max(j + 1 - r0, 0);
-    for (int lr = lo + tid; lr < nloc; lr += NT) {
-      T l = P[(size_t)j * rpcp + lr];
-      if (!zero) {
-        l = cmul(l, inv);
-        P[(size_t)j * rpcp + lr] = l;
+    if (j + 1 < ncols) {
+      // column j + 1 first: scale, update, candidate; post it and arrive, then finish the
+      // rank-1 update of columns j + 2 .. while the other CTAs arrive
+      const int jn = j + 1;
+      float bv = -1.f;
+      int bi = 0x7fffffff;
+      for (int lr = lo + tid; lr < nloc; lr += NT) {
+        T l = P[(size_t)j * rpcp + lr];
+        if (!zero) {
+          l = cmul(l, inv);
+          P[(size_t)j * rpcp + lr] = l;
+        }
+        T v = P[(size_t)jn * rpcp + lr];
+        cfms(v, l, urow[jn]);
+        P[(size_t)jn * rpcp + lr] = v;
+        float av = (float)cabs1(v);
+        if (av > bv) { bv = av; bi = r0 + lr; }
       }
-      for (int c = j + 1; c < ncols; ++c) {
-        T v = P[(size_t)c * rpcp + lr];
-        cfms(v, l, urow[c]);
-        P[(size_t)c * rpcp + lr] = v;
+      candidate(jn, bv, bi);
+      post(jn, true);
+      arrive(jn);
+      // rank-1 update of columns j + 2 .. ncols - 1: lanes over rows, warps over columns,
+      // four independent columns per step
+      constexpr int NW = NT / 32;
+      for (int lr = lo + lane; lr < nloc; lr += 32) {
+        const T l = P[(size_t)j * rpcp + lr];
+        int c = jn + 1 + warp;
+        for (; c + 3 * NW < ncols; c += 4 * NW) {
+          T v[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) v[q] = P[(size_t)(c + q * NW) * rpcp + lr];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            cfms(v[q], l, urow[c + q * NW]);
+            P[(size_t)(c + q * NW) * rpcp + lr] = v[q];
+          }
+        }
+        for (; c < ncols; c += NW) {
+          T v = P[(size_t)c * rpcp + lr];
+          cfms(v, l, urow[c]);
+          P[(size_t)c * rpcp + lr] = v;
+        }
       }
+      __syncthreads();
+    } else {
+      for (int lr = lo + tid; lr < nloc; lr += NT) {
+        if (!zero) P[(size_t)j * rpcp + lr] = cmul(P[(size_t)j * rpcp + lr], inv);
+      }
+      __syncthreads();
     }
-    __syncthreads();
+    if (tr && b == 0 && tid == 0) tr[4] = device_ns();
   }
 
   // write the factored rows back

@@ -114,7 +114,7 @@ struct hprmat_b200_ctx {
   int w_N = 0, w_npad = 0;
   long w_xld = 0, w_xplane = 0;
   bool wave_trace = false;
-  DevBuf wtrace;
+  DevBuf wtrace, ptrace;
   int wtrace_units = 0;
   int* h_status = nullptr;  // pinned
   double* h_norms = nullptr;  // pinned
@@ -440,6 +440,12 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
     pa.lup = (mixed && k0 + ncols < N) ? c->lup.as<float>() : nullptr;
     pa.lup_ld = c->lup_ld;
     pa.lup_plane = c->lup_plane;
+    pa.trace = nullptr;
+    if (c->wave_trace && (s == 0 || s == nsteps / 2)) {
+      TRY(c->ptrace.ensure((size_t)2 * kMaxNB * kPanelTraceW * sizeof(long long)));
+      if (s == 0) HPR_CUDA_TRY(cudaMemsetAsync(c->ptrace.p, 0, c->ptrace.bytes, c->stream));
+      pa.trace = c->ptrace.as<long long>() + (s == 0 ? 0 : (size_t)kMaxNB * kPanelTraceW);
+    }
     void* args[] = {&pa};
     HPR_CUDA_TRY(cudaLaunchCooperativeKernel((void*)pk, dim3(G), dim3(NT), args, smem, c->stream));
     ++c->launches;
@@ -1520,6 +1526,18 @@ int hprmat_b200_dev_wave_trace_read(hprmat_b200_ctx* c, long long* out, int cap,
   if (n && c->wtrace.p) {
     HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
     HPR_CUDA_TRY(cudaMemcpy(out, c->wtrace.p, n * sizeof(long long), cudaMemcpyDeviceToHost));
+  }
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_dev_panel_trace_read(hprmat_b200_ctx* c, long long* out, int cap, int* width) {
+  TRY(check_ctx(c));
+  if (!out || !width || cap < 0) return fail(HPRMAT_B200_ERR_ARG, "null output");
+  *width = kPanelTraceW;
+  const size_t n = std::min((size_t)cap, c->ptrace.bytes / sizeof(long long));
+  if (n && c->ptrace.p) {
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    HPR_CUDA_TRY(cudaMemcpy(out, c->ptrace.p, n * sizeof(long long), cudaMemcpyDeviceToHost));
   }
   return HPRMAT_B200_OK;
 }

@@ -57,6 +57,14 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
 }
 
 
+// Prefetch of one TMA box into L2 (no shared-memory destination, no completion).
+__device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap* map, int c0, int c1, int c2) {
+  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(c0), "r"(c1), "r"(c2)
+               : "memory");
+}
+
 // Shared-memory matrix descriptor, K-major, 64-byte swizzle: rows of 64 bytes, 8-row
 // groups 512 bytes apart (stride byte offset), leading byte offset unused (1), version 1.
 __device__ __forceinline__ uint64_t sdesc_k_sw64(uint32_t saddr) {

@@ -444,6 +444,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       int stage = 0, inflight = 0;
       uint32_t phase = 0;
       bool ok = true;
+      auto next_stage = [&]() {
+        inflight = min(inflight + 1, kStages);
+        if (++stage == kStages) { stage = 0; phase ^= 1u; }
+      };
       for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
         const int r = u / G, h = u % G;
         const int j = FWD ? r : nsteps - 1 - r;
@@ -469,8 +473,7 @@ __global__ void __launch_bounds__(kThreads, 1)
               }
               tma_load_3d(sa + R::kABytes, &tmX, &full[stage], k * kNB + kc * kKC, h * UN, 0);
             }
-            inflight = min(inflight + 1, kStages);
-            if (++stage == kStages) { stage = 0; phase ^= 1u; }
+            next_stage();
             if (!ok) break;
           }
         }
@@ -535,22 +538,27 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int row = j * kNB + q * 32 + lane;
       const bool rv = row < N;
       const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 2 * UN);
+      constexpr int kCh = UN / 32;  // chunks of 16 columns per warp
+      float re[kCh][16], im[kCh][16];
 #pragma unroll
-      for (int i = 0; i < UN / 32; ++i) {
-        const int c0 = c_begin + 16 * i;
-        float re[16], im[16];
-        tmem_ld16(tl + c0, re);
-        tmem_ld16(tl + UN + c0, im);
-        tmem_wait_ld();
+      for (int i = 0; i < kCh; ++i) {
+        tmem_ld16(tl + c_begin + 16 * i, re[i]);
+        tmem_ld16(tl + UN + c_begin + 16 * i, im[i]);
+      }
+      tmem_wait_ld();
+      tc_fence_before();
+      mbar_arrive(&acc_empty[buf]);
+      // the planes are what other CTAs wait for: write them, make them visible to the TMA
+      // (async proxy) loads of the CTAs that acquire the flag, publish, then the FP32 output
+#pragma unroll
+      for (int i = 0; i < kCh; ++i) {
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
-          const int col = h * UN + c0 + e;
+          const int col = h * UN + c_begin + 16 * i + e;
           if (rv && col < p.nrhs) {
-            const float xr = -re[e], xi = -im[e];
-            if (p.xout) p.xout[(size_t)row + (size_t)col * p.ldx] = make_float2(xr, xi);
             float hr, lr, hi, li;
-            tf32_split(xr, hr, lr);
-            tf32_split(xi, hi, li);
+            tf32_split(-re[i][e], hr, lr);
+            tf32_split(-im[i][e], hi, li);
             float* d = p.xp + (size_t)col * p.xp_ld + row;
             d[0] = hr;
             d[p.xp_plane] = lr;
@@ -559,16 +567,22 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
         }
       }
-      tc_fence_before();
-      mbar_arrive(&acc_empty[buf]);
-      // publish this warp's part of block (j, h): its generic writes become visible to the
-      // TMA (async proxy) loads of the CTAs that acquire the flag
       fence_proxy_async_global();
-      __threadfence();
       __syncwarp();
       if (lane == 0) {
+        // release: cumulative over the warp's writes ordered before it by the warp barrier
         asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(p.flags + (size_t)j * G + h) : "memory");
         if (p.trace && warp == 2) p.trace[4 * (size_t)u + 3] = globaltimer_ns();
+      }
+      if (p.xout) {
+#pragma unroll
+        for (int i = 0; i < kCh; ++i) {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            const int col = h * UN + c_begin + 16 * i + e;
+            if (rv && col < p.nrhs) p.xout[(size_t)row + (size_t)col * p.ldx] = make_float2(-re[i][e], -im[i][e]);
+          }
+        }
       }
     }
   }

@@ -40,6 +40,11 @@ int hprmat_b200_dev_counters(hprmat_b200_ctx* ctx, unsigned long long* launches,
    the last backward sweep (2 x units x 4 values, at most cap) and stores units. */
 int hprmat_b200_dev_wave_trace(hprmat_b200_ctx* ctx, int enable);
 int hprmat_b200_dev_wave_trace_read(hprmat_b200_ctx* ctx, long long* out, int cap, int* units);
+/* With tracing enabled, the panel factorisations of block steps 0 and nsteps/2 also record
+   per column `width` device-clock stamps: CTA 0 at column start, candidate posted, grid
+   barrier passed, pivot row in place, update done, then each CTA's barrier arrival.
+   Copies 2 x 128 x width values (at most cap). */
+int hprmat_b200_dev_panel_trace_read(hprmat_b200_ctx* ctx, long long* out, int cap, int* width);
 
 #ifdef __cplusplus
 }
