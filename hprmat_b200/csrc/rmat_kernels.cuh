@@ -2,6 +2,7 @@
 // residual r = B - C X evaluated from C's generators, R-matrix extraction and the
 // collision-matrix (U) step, and the per-column FGMRES kernels of the refinement.
 #pragma once
+#include <type_traits>
 #include "common.cuh"
 
 namespace hprmat {
@@ -163,6 +164,122 @@ __global__ void resid_kinetic_kernel(MeshDev mesh, ChannelData ch, const double2
   ar = fma(d, xi.x, ar);
   ai = fma(d, xi.y, ai);
   out[(size_t)(c * nr + i) + (size_t)col * ldo] = make_double2(br - ar, -ai);
+}
+
+// ------------------------------------------------------------------ tiled residual products
+// The plain (uncompensated) operator products of the refinement as batched FP64 tiles:
+//   kinetic:  batch c,  out[c*nr + i, col]  = b(i, col) - sum_j K_c(i, j) X[c*nr + j, col],
+//             K_c = tc - bloch_c blo0 + diag(fac_c / r_i^2 + kk_c)  (real, built per tile);
+//   coupling: batch i,  out[c*nr + i, col] -= sum_c' cpot(r_i, c, c') X[c'*nr + i, col].
+// 256 threads compute a 64 x 64 tile (4 x 4 complex values each) from 16-deep K chunks
+// staged in shared memory; the same sums as resid_kinetic_kernel / resid_coupling_kernel in
+// a different order of summation.
+struct KineticTile {
+  MeshDev mesh;
+  ChannelData ch;
+  const double2* X;
+  long ldx;
+  int with_b;
+  __device__ double a(int c, int i, int j) const {
+    const int nr = mesh.nr;
+    double k = mesh.tc[i + (size_t)j * nr] - ch.bloch[c] * mesh.blo0[i + (size_t)j * nr];
+    if (i == j) {
+      const double rr = mesh.r[i];
+      k += ch.fac[c] / (rr * rr) + ch.kk[c];
+    }
+    return k;
+  }
+  __device__ double2 b(int c, int j, int col) const { return X[(size_t)c * mesh.nr + j + (size_t)col * ldx]; }
+  __device__ size_t o(int c, int i, int col, long ldo) const { return (size_t)c * mesh.nr + i + (size_t)col * ldo; }
+  __device__ double2 init(int c, int i, int col, const double2*, size_t) const {
+    return make_double2((with_b && c == col) ? mesh.q2[i] : 0.0, 0.0);
+  }
+};
+
+struct CouplingTile {
+  const double2* vt;  // cpot_transpose_kernel layout
+  const double2* X;
+  long ldx;
+  int nr, nch;
+  __device__ double2 a(int i, int c, int cp) const { return vt[((size_t)i * nch + cp) * nch + c]; }
+  __device__ double2 b(int i, int cp, int col) const { return X[(size_t)cp * nr + i + (size_t)col * ldx]; }
+  __device__ size_t o(int i, int c, int col, long ldo) const { return (size_t)c * nr + i + (size_t)col * ldo; }
+  __device__ double2 init(int, int, int, const double2* out, size_t idx) const { return out[idx]; }
+};
+
+template <class Op, bool REAL_A>
+__global__ void __launch_bounds__(256, 2) resid_tile_kernel(Op op, int M, int Ncol, int K, double2* out, long ldo) {
+  constexpr int BM = 64, BN = 64, BK = 16;
+  using AT = typename std::conditional<REAL_A, double, double2>::type;
+  __shared__ AT As[BK][BM];
+  __shared__ double2 Bs[BK][BN + 1];
+  const int z = blockIdx.z;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;
+  double2 acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[r][q] = make_double2(0.0, 0.0);
+  for (int k0 = 0; k0 < K; k0 += BK) {
+    // A tile: consecutive threads along m
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int idx = tid + 256 * e;
+      const int mm = idx % BM, kk = idx / BM;
+      const int m = m0 + mm, k = k0 + kk;
+      if constexpr (REAL_A) {
+        As[kk][mm] = (m < M && k < K) ? op.a(z, m, k) : 0.0;
+      } else {
+        As[kk][mm] = (m < M && k < K) ? op.a(z, m, k) : make_double2(0.0, 0.0);
+      }
+    }
+    // B tile: consecutive threads along k
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int idx = tid + 256 * e;
+      const int kk = idx % BK, nn = idx / BK;
+      const int n = n0 + nn, k = k0 + kk;
+      Bs[kk][nn] = (n < Ncol && k < K) ? op.b(z, k, n) : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      AT av[4];
+      double2 bv[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) av[r] = As[kk][tx + 16 * r];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) bv[q] = Bs[kk][ty + 16 * q];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if constexpr (REAL_A) {
+            acc[r][q].x = fma(av[r], bv[q].x, acc[r][q].x);
+            acc[r][q].y = fma(av[r], bv[q].y, acc[r][q].y);
+          } else {
+            acc[r][q].x = fma(av[r].x, bv[q].x, acc[r][q].x);
+            acc[r][q].x = fma(-av[r].y, bv[q].y, acc[r][q].x);
+            acc[r][q].y = fma(av[r].x, bv[q].y, acc[r][q].y);
+            acc[r][q].y = fma(av[r].y, bv[q].x, acc[r][q].y);
+          }
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int m = m0 + tx + 16 * r, n = n0 + ty + 16 * q;
+      if (m < M && n < Ncol) {
+        const size_t idx = op.o(z, m, n, ldo);
+        const double2 b = op.init(z, m, n, out, idx);
+        out[idx] = make_double2(b.x - acc[r][q].x, b.y - acc[r][q].y);
+      }
+    }
 }
 
 // Potential re-laid out per mesh point: vt[(i*nch + c')*nch + c] = cpot(r_i, c, c'), so the

@@ -708,6 +708,19 @@ struct Operator {
 static int apply_residual(hprmat_b200_ctx* c, const Operator& op, const double2* X, long ldx, int ncol,
                           double2* out, long ldo, bool with_b, bool absmode = false) {
   const int N = op.N;
+  if (op.structured && !with_b && !absmode) {
+    // plain product (inner iterations): tiled batched kernels
+    const int nr = op.mesh.nr;
+    KineticTile kt{op.mesh, op.ch, X, ldx, with_b ? 1 : 0};
+    resid_tile_kernel<KineticTile, true>
+        <<<dim3(cdiv_u(nr, 64), cdiv_u(ncol, 64), op.nch), 256, 0, c->stream>>>(kt, nr, ncol, nr, out, ldo);
+    LAUNCH_CHECK();
+    CouplingTile ct{op.vt, X, ldx, nr, op.nch};
+    resid_tile_kernel<CouplingTile, false>
+        <<<dim3(cdiv_u(op.nch, 64), cdiv_u(ncol, 64), nr), 256, 0, c->stream>>>(ct, op.nch, ncol, op.nch, out, ldo);
+    LAUNCH_CHECK();
+    return HPRMAT_B200_OK;
+  }
   if (op.structured) {
     const int nr = op.mesh.nr;
     // the outer residual (with B) is formed with compensated sums; low words in R64
