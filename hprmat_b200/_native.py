@@ -36,7 +36,7 @@ EXPORTED = (
     # include/hprmat_b200_dev.h
     "hprmat_b200_dev_tc_update", "hprmat_b200_dev_split_planes", "hprmat_b200_dev_set_profile",
     "hprmat_b200_dev_counters", "hprmat_b200_dev_wave_trace", "hprmat_b200_dev_wave_trace_read",
-    "hprmat_b200_dev_panel_trace_read",
+    "hprmat_b200_dev_panel_trace_read", "hprmat_b200_dev_set_tuning",
 )
 
 
@@ -108,6 +108,7 @@ def load():
         "hprmat_b200_dev_wave_trace": (I, [P, I]),
         "hprmat_b200_dev_wave_trace_read": (I, [P, ctypes.POINTER(ctypes.c_longlong), I, IP]),
         "hprmat_b200_dev_panel_trace_read": (I, [P, ctypes.POINTER(ctypes.c_longlong), I, IP]),
+        "hprmat_b200_dev_set_tuning": (I, [P, ctypes.c_char_p, I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

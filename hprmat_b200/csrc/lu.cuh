@@ -669,14 +669,14 @@ __global__ void __launch_bounds__(NB * CW) diag_apply_kernel(const T* __restrict
 //   tc_update: C -= (I - Linv) (P A12) with C = those rows of W, i.e. C = Linv P A12 = U12;
 //   u12_split_kernel: U12 -> B-operand planes of the trailing update and the LU planes.
 // Inverse of the unit lower triangle L11 in shared memory by recursive blocking: the
-// diagonal blocks of (up to) 32 x 32 are inverted by one warp each, all at once (column
+// diagonal blocks of (up to) 16 x 16 are inverted by one warp each, all at once (column
 // sweeps, as xTRTI2), then pairs of blocks are joined with
 //   [A 0; B C]^-1 = [A^-1 0; -C^-1 B A^-1  C^-1]
 // until the whole NB x NB block is done.  Dynamic shared memory: (NB*NB + (NB/2)^2) float2.
 template <int NB, int NT>
 __global__ void __launch_bounds__(NT) l11_inverse_planes_kernel(const float2* __restrict__ W, long ld, int k0,
                                                                  int ncols, float* planes, long plane) {
-  constexpr int B0 = NB < 32 ? NB : 32;
+  constexpr int B0 = NB < 16 ? NB : 16;
   static_assert(NT >= 32 * (NB / B0), "one warp per diagonal block");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* S = reinterpret_cast<float2*>(smem_raw);  // [NB][NB] column-major, L11 -> L11^-1 in place
@@ -718,9 +718,14 @@ __global__ void __launch_bounds__(NT) l11_inverse_planes_kernel(const float2* __
       int pr = idx / (h * h), r = idx % (h * h);
       int i = r % h, j = r / h;
       int a = pr * 2 * h;
-      float2 acc = make_float2(0.f, 0.f);
-      for (int k = j; k < h; ++k) cfma(acc, S[(a + h + i) + (a + k) * NB], S[(a + k) + (a + j) * NB]);
-      T[pr * h * h + i + j * h] = acc;
+      float2 acc = make_float2(0.f, 0.f), acc2 = make_float2(0.f, 0.f);  // two chains
+      int k = j;
+      for (; k + 1 < h; k += 2) {
+        cfma(acc, S[(a + h + i) + (a + k) * NB], S[(a + k) + (a + j) * NB]);
+        cfma(acc2, S[(a + h + i) + (a + k + 1) * NB], S[(a + k + 1) + (a + j) * NB]);
+      }
+      if (k < h) cfma(acc, S[(a + h + i) + (a + k) * NB], S[(a + k) + (a + j) * NB]);
+      T[pr * h * h + i + j * h] = make_float2(acc.x + acc2.x, acc.y + acc2.y);
     }
     __syncthreads();
     // B := -Cinv * T  (Cinv: rows/cols [a+h, a+2h), lower)
@@ -728,9 +733,14 @@ __global__ void __launch_bounds__(NT) l11_inverse_planes_kernel(const float2* __
       int pr = idx / (h * h), r = idx % (h * h);
       int i = r % h, j = r / h;
       int a = pr * 2 * h;
-      float2 acc = make_float2(0.f, 0.f);
-      for (int k = 0; k <= i; ++k) cfma(acc, S[(a + h + i) + (a + h + k) * NB], T[pr * h * h + k + j * h]);
-      S[(a + h + i) + (a + j) * NB] = make_float2(-acc.x, -acc.y);
+      float2 acc = make_float2(0.f, 0.f), acc2 = make_float2(0.f, 0.f);
+      int k = 0;
+      for (; k + 1 <= i; k += 2) {
+        cfma(acc, S[(a + h + i) + (a + h + k) * NB], T[pr * h * h + k + j * h]);
+        cfma(acc2, S[(a + h + i) + (a + h + k + 1) * NB], T[pr * h * h + k + 1 + j * h]);
+      }
+      if (k <= i) cfma(acc, S[(a + h + i) + (a + h + k) * NB], T[pr * h * h + k + j * h]);
+      S[(a + h + i) + (a + j) * NB] = make_float2(-(acc.x + acc2.x), -(acc.y + acc2.y));
     }
     __syncthreads();
   }

@@ -111,6 +111,8 @@ struct hprmat_b200_ctx {
   TcOperand op_wT, op_wdi, op_wbp, op_wyp, op_wxp;
   bool wave_ready = false;
   int wave_un = 64;
+  bool wave_enabled = true;  // wavefront solves (else block-step solves)
+  bool tc_trsm = true;       // U12 by the tensor cores from L11^-1 (else substitution)
   int w_N = 0, w_npad = 0;
   long w_xld = 0, w_xplane = 0;
   bool wave_trace = false;
@@ -249,8 +251,13 @@ static MeshDev mesh_dev(const hprmat_b200_ctx* c) {
 // ------------------------------------------------------------------ launch helpers
 template <typename K>
 static int set_smem(K kernel, size_t bytes) {
-  if (bytes > 48 * 1024)
-    HPR_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  // The 48 KB default covers static + dynamic shared memory.  Only ever raise the limit:
+  // kernels instantiated in more than one file share it.
+  cudaFuncAttributes fa;
+  HPR_CUDA_TRY(cudaFuncGetAttributes(&fa, kernel));
+  if ((int)bytes > fa.maxDynamicSharedSizeBytes || (int)(bytes + fa.sharedSizeBytes) > 48 * 1024)
+    HPR_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      std::max((int)bytes, fa.maxDynamicSharedSizeBytes)));
   return HPRMAT_B200_OK;
 }
 
@@ -447,17 +454,27 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
       pa.trace = c->ptrace.as<long long>() + (s == 0 ? 0 : (size_t)kMaxNB * kPanelTraceW);
     }
     void* args[] = {&pa};
-    HPR_CUDA_TRY(cudaLaunchCooperativeKernel((void*)pk, dim3(G), dim3(NT), args, smem, c->stream));
+    {
+      const cudaError_t e = cudaLaunchCooperativeKernel((void*)pk, dim3(G), dim3(NT), args, smem, c->stream);
+      if (e != cudaSuccess) {
+        int occ = -1;
+        cudaGetLastError();
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pk, NT, smem);
+        return fail(HPRMAT_B200_ERR_CUDA, "panel launch (step %d, %d CTAs of %d rows, %zu B shared, %d per SM): %s", s,
+                    G, rpc, smem, occ, cudaGetErrorString(e));
+      }
+    }
     ++c->launches;
     if (k0 + ncols >= N) break;
     // row interchanges + U12 = L11^-1 A12
-    if (mixed) {
+    if (mixed && c->tc_trsm) {
       // L11^-1 (as I - L11^-1 operand planes), P A12 gathered, U12 by one tensor-core GEMM
       constexpr int CW = 32;
       const size_t ism = ((size_t)NB * NB + (size_t)(NB / 2) * (NB / 2)) * sizeof(float2);
-      auto ik = l11_inverse_planes_kernel<NB, NT>;
+      constexpr int NTI = 512;
+      auto ik = l11_inverse_planes_kernel<NB, NTI>;
       TRY(set_smem(ik, ism));
-      ik<<<1, NT, ism, c->stream>>>(reinterpret_cast<const float2*>(W), ld, k0, ncols, c->linv.as<float>(),
+      ik<<<1, NTI, ism, c->stream>>>(reinterpret_cast<const float2*>(W), ld, k0, ncols, c->linv.as<float>(),
                                      (long)NB * NB);
       LAUNCH_CHECK();
       auto gk = swap_gather_kernel<NB, CW, NT>;
@@ -496,6 +513,14 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
       ta.c_begin = k0 + ncols;
       ta.c_end = N;
       ta.growth_bits = growth;
+      if (mixed) {  // U12 also as the B operand of the trailing update and into the LU planes
+        ta.bop = bop;
+        ta.bop_plane = plane;
+        ta.bop_col0 = k0 + ncols;
+        ta.lup = c->lup.as<float>();
+        ta.lup_ld = c->lup_ld;
+        ta.lup_plane = c->lup_plane;
+      }
       tk<<<cdiv_u(N - k0 - ncols, CW), NT, tsm, c->stream>>>(ta);
       LAUNCH_CHECK();
     }
@@ -533,7 +558,7 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
   }
   c->wave_ready = false;
   if constexpr (NB == 128 && std::is_same<T, float2>::value) {
-    if (mixed && nsteps >= 2) TRY(wave_prepare(c, st));
+    if (mixed && nsteps >= 2 && c->wave_enabled) TRY(wave_prepare(c, st));
   }
   HPR_CUDA_TRY(cudaMemcpyAsync(c->h_status, status, SW_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1553,6 +1578,25 @@ int hprmat_b200_dev_panel_trace_read(hprmat_b200_ctx* c, long long* out, int cap
     HPR_CUDA_TRY(cudaMemcpy(out, c->ptrace.p, n * sizeof(long long), cudaMemcpyDeviceToHost));
   }
   return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* c, const char* key, int value) {
+  TRY(check_ctx(c));
+  if (!key) return fail(HPRMAT_B200_ERR_ARG, "null key");
+  if (strcmp(key, "wave") == 0) {
+    c->wave_enabled = value != 0;
+    return HPRMAT_B200_OK;
+  }
+  if (strcmp(key, "tc_trsm") == 0) {
+    c->tc_trsm = value != 0;
+    return HPRMAT_B200_OK;
+  }
+  if (strcmp(key, "wave_un") == 0) {
+    if (value != 64 && value != 128) return fail(HPRMAT_B200_ERR_ARG, "wave_un must be 64 or 128");
+    c->wave_un = value;
+    return HPRMAT_B200_OK;
+  }
+  return fail(HPRMAT_B200_ERR_ARG, "unknown tuning key '%s'", key);
 }
 
 int hprmat_b200_dev_counters(hprmat_b200_ctx* c, unsigned long long* launches, double* tc_ms, double* tc_flops,

@@ -538,32 +538,33 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int row = j * kNB + q * 32 + lane;
       const bool rv = row < N;
       const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 2 * UN);
-      constexpr int kCh = UN / 32;  // chunks of 16 columns per warp
-      float re[kCh][16], im[kCh][16];
-#pragma unroll
-      for (int i = 0; i < kCh; ++i) {
-        tmem_ld16(tl + c_begin + 16 * i, re[i]);
-        tmem_ld16(tl + UN + c_begin + 16 * i, im[i]);
-      }
-      tmem_wait_ld();
-      tc_fence_before();
-      mbar_arrive(&acc_empty[buf]);
+      constexpr int kCh = UN / 32;  // chunks of 16 columns per warp, read two at a time
       // the planes are what other CTAs wait for: write them, make them visible to the TMA
       // (async proxy) loads of the CTAs that acquire the flag, publish, then the FP32 output
 #pragma unroll
-      for (int i = 0; i < kCh; ++i) {
+      for (int i0 = 0; i0 < kCh; i0 += 2) {
+        float re[2][16], im[2][16];
 #pragma unroll
-        for (int e = 0; e < 16; ++e) {
-          const int col = h * UN + c_begin + 16 * i + e;
-          if (rv && col < p.nrhs) {
-            float hr, lr, hi, li;
-            tf32_split(-re[i][e], hr, lr);
-            tf32_split(-im[i][e], hi, li);
-            float* d = p.xp + (size_t)col * p.xp_ld + row;
-            d[0] = hr;
-            d[p.xp_plane] = lr;
-            d[2 * p.xp_plane] = hi;
-            d[3 * p.xp_plane] = li;
+        for (int i = 0; i < 2; ++i) {
+          tmem_ld16(tl + c_begin + 16 * (i0 + i), re[i]);
+          tmem_ld16(tl + UN + c_begin + 16 * (i0 + i), im[i]);
+        }
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            const int col = h * UN + c_begin + 16 * (i0 + i) + e;
+            if (rv && col < p.nrhs) {
+              float hr, lr, hi, li;
+              tf32_split(-re[i][e], hr, lr);
+              tf32_split(-im[i][e], hi, li);
+              float* d = p.xp + (size_t)col * p.xp_ld + row;
+              d[0] = hr;
+              d[p.xp_plane] = lr;
+              d[2 * p.xp_plane] = hi;
+              d[3 * p.xp_plane] = li;
+            }
           }
         }
       }
@@ -576,14 +577,25 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       if (p.xout) {
 #pragma unroll
-        for (int i = 0; i < kCh; ++i) {
+        for (int i0 = 0; i0 < kCh; i0 += 2) {
+          float re[2][16], im[2][16];
 #pragma unroll
-          for (int e = 0; e < 16; ++e) {
-            const int col = h * UN + c_begin + 16 * i + e;
-            if (rv && col < p.nrhs) p.xout[(size_t)row + (size_t)col * p.ldx] = make_float2(-re[i][e], -im[i][e]);
+          for (int i = 0; i < 2; ++i) {
+            tmem_ld16(tl + c_begin + 16 * (i0 + i), re[i]);
+            tmem_ld16(tl + UN + c_begin + 16 * (i0 + i), im[i]);
           }
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+              const int col = h * UN + c_begin + 16 * (i0 + i) + e;
+              if (rv && col < p.nrhs) p.xout[(size_t)row + (size_t)col * p.ldx] = make_float2(-re[i][e], -im[i][e]);
+            }
         }
       }
+      tc_fence_before();
+      mbar_arrive(&acc_empty[buf]);
     }
   }
   tc_fence_before();

@@ -32,6 +32,10 @@ int hprmat_b200_dev_set_profile(hprmat_b200_ctx* ctx, int enable);
 int hprmat_b200_dev_counters(hprmat_b200_ctx* ctx, unsigned long long* launches, double* tc_ms, double* tc_flops,
                              int* tc_launches, int reset);
 
+/* Tuning knobs for benchmarks.  "wave_un": right-hand sides per unit of the wavefront
+   triangular solves (64 or 128). */
+int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* ctx, const char* key, int value);
+
 /* Tracing of the wavefront triangular solves of the mixed path.  With enable != 0 every
    later sweep records, per unit (block row x right-hand-side group, in dependency order),
    four device-clock stamps in ns: the producer starts the unit, the last dependency flag

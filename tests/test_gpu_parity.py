@@ -6,6 +6,7 @@ error of 1e-10 (the target of the solver), for both the plain FP64 LU and the mi
 checked on its own against an FP64 torch product to 3xTF32 accuracy (2e-6 relative).
 """
 import math
+import os
 
 import numpy as np
 import pytest
@@ -15,6 +16,8 @@ from hprmat_b200 import _native as nat
 from hprmat_b200 import api, workloads
 from oracle import rmatrix_oracle as orc
 from tests.example_inputs import ex1_setup, ex2_setup, ex4_setup
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 pytestmark = pytest.mark.gpu
 
@@ -128,6 +131,20 @@ def test_medium_production_generator(ctx, precision):
     cu, nopen = ctx.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
     assert nopen == ref.nopen
     assert _rel(cu[:nopen, :nopen], ref.cu) <= U_TOL, ctx.last_stats
+
+
+@pytest.mark.parametrize("nch", [32, 64])
+def test_production_generator_against_fixture(ctx, nch):
+    """Production generator at N = 6400 and 12800 (200 points x nch channels) against the
+    committed FP64 oracle collision matrices (tests/golden/make_production_u.py).  N = 6400
+    puts 44 panel rows on each of the 148 CTAs, the shape whose shared memory sits just
+    under the 48 KB default."""
+    fx = np.load(os.path.join(GOLDEN, f"production_u_nch{nch}.npz"))
+    w = workloads.production(nch=nch)
+    ctx.set_precision("mixed")
+    cu, nopen = ctx.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+    assert nopen == int(fx["nopen"])
+    assert _rel(cu[:nopen, :nopen], fx["u"]) <= U_TOL, ctx.last_stats
 
 
 def test_sweep_generator_closed_at_40mev(ctx):
