@@ -288,8 +288,16 @@ def main():
     bf16 = peaks.get("bf16_tflops_sustained") or 1400.0
     tf32_peak = bf16 / 2.0
     achieved = (tc_flops.value / max(tc_n.value, 1)) / ((tc_ms.value / max(tc_n.value, 1)) / 1e3) / 1e12
+    # DRAM traffic per launch: ncu measured 1.05x the algorithmic bytes (C read + write and the
+    # operand planes) for the trailing update at N = 12800 (profiles/tc_update_kernel_n12800.md);
+    # scaled here to the mean algorithmic bytes of this solve's trailing updates
+    nb_ = 128
+    ms_ = [n_full - (s + 1) * nb_ for s in range((n_full + nb_ - 1) // nb_ - 1)]
+    alg_bytes = float(np.mean([16.0 * m * m + 2.0 * m * nb_ * 16.0 for m in ms_])) if ms_ else 0.0
     roofline = {"bound": "tensor", "achieved": achieved, "peak": tf32_peak, "unit": "TFLOP/s",
-                "frac": achieved / tf32_peak, "traffic": None,
+                "frac": achieved / tf32_peak, "traffic": 1.05 * alg_bytes,
+                "traffic_note": "bytes per launch: 1.05 x the mean algorithmic bytes, ratio from one ncu capture "
+                                "at N = 12800 (dram__bytes_read.sum + dram__bytes_write.sum)",
                 "kernel": "tc_update_kernel (3xTF32 complex trailing update)",
                 "launches": tc_n.value, "ms_total": tc_ms.value,
                 "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained / 2 (dense TF32 = half of BF16)"
