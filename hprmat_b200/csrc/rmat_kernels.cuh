@@ -55,31 +55,34 @@ struct Acc2 {
 template <typename T>
 __global__ void assemble_kernel(MeshDev mesh, ChannelData ch, int nch, const double2* __restrict__ cpot,
                                 long ncp1, long ndim, T* W, long ld, int N, double* fro2) {
+  // thread: one row; block: 256 rows of the columns blockIdx.y, blockIdx.y + gridDim.y, ...
+  // (coalesced writes along the column), one atomic per block for ||C||_F^2
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  const int col = blockIdx.y;
   double sq = 0.0;
   if (row < N) {
-  const int nr = mesh.nr;
-  const int c = row / nr, i = row - c * nr;
-  const int cp = col / nr, j = col - cp * nr;
-  double re = 0.0, im = 0.0;
-  if (c == cp) {
-    re = mesh.tc[i + (size_t)j * nr] - ch.bloch[c] * mesh.blo0[i + (size_t)j * nr];
-    if (i == j) {
-      double rr = mesh.r[i];
-      re += ch.fac[c] / (rr * rr) + ch.kk[c];
+    const int nr = mesh.nr;
+    const int c = row / nr, i = row - c * nr;
+    const double rr = mesh.r[i];
+    const double dg = ch.fac[c] / (rr * rr) + ch.kk[c];
+    const double bl = ch.bloch[c];
+    for (int col = blockIdx.y; col < N; col += gridDim.y) {
+      const int cp = col / nr, j = col - cp * nr;
+      double re = 0.0, im = 0.0;
+      if (c == cp) {
+        re = mesh.tc[i + (size_t)j * nr] - bl * mesh.blo0[i + (size_t)j * nr];
+        if (i == j) re += dg;
+      }
+      if (i == j) {
+        double2 v = cpot[(size_t)i + ncp1 * ((size_t)c + ndim * (size_t)cp)];
+        re += v.x;
+        im += v.y;
+      }
+      T out;
+      out.x = (typename RealOf<T>::R)re;
+      out.y = (typename RealOf<T>::R)im;
+      W[(size_t)row + (size_t)col * ld] = out;
+      sq += re * re + im * im;
     }
-  }
-  if (i == j) {
-    double2 v = cpot[(size_t)i + ncp1 * ((size_t)c + ndim * (size_t)cp)];
-    re += v.x;
-    im += v.y;
-  }
-  T out;
-  out.x = (typename RealOf<T>::R)re;
-  out.y = (typename RealOf<T>::R)im;
-  W[(size_t)row + (size_t)col * ld] = out;
-  sq = re * re + im * im;
   }
   for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
   __shared__ double red[32];
@@ -105,75 +108,15 @@ __global__ void surface_rhs_kernel(const double* __restrict__ q2, int nr, int nc
   X[(size_t)row + (size_t)col * ldx] = v;
 }
 
-// out = beta*B - C X for the channel-diagonal part of C (kinetic, centrifugal, threshold,
-// closed-channel Bloch).  grid (ceil(nr/32), nch, ceil(ncol/8)), block (32, 8).
-// B is blockdiag(q2) (only when with_b != 0).
-// absmode != 0 instead forms |B| + |C_diag| |X| (moduli, real part only): the scale of the
-// rounding error of the residual.
-// With with_b the sums are compensated (Acc2); their low words go to lo_out (same layout as
-// out) when it is given, for resid_coupling_kernel to finish the compensated residual.
-__global__ void resid_kinetic_kernel(MeshDev mesh, ChannelData ch, const double2* __restrict__ X,
-                                     long ldx, int ncol, double2* out, long ldo, int with_b, int absmode,
-                                     double2* lo_out) {
-  const int nr = mesh.nr;
-  const int i = blockIdx.x * 32 + threadIdx.x;
-  const int c = blockIdx.y;
-  const int col = blockIdx.z * 8 + threadIdx.y;
-  if (i >= nr || col >= ncol) return;
-  const double bl = ch.bloch[c];
-  const double2* xc = X + (size_t)col * ldx + (size_t)c * nr;
-  double ar = 0.0, ai = 0.0;
-  const double rr = mesh.r[i];
-  const double d = ch.fac[c] / (rr * rr) + ch.kk[c];
-  const double br = (with_b && c == col) ? mesh.q2[i] : 0.0;
-  if (absmode) {
-    for (int j = 0; j < nr; ++j) {
-      double k = mesh.tc[i + (size_t)j * nr] - bl * mesh.blo0[i + (size_t)j * nr];
-      if (j == i) k += d;
-      double2 x = __ldg(xc + j);
-      ar = fma(fabs(k), hypot(x.x, x.y), ar);
-    }
-    out[(size_t)(c * nr + i) + (size_t)col * ldo] = make_double2(fabs(br) + ar, 0.0);
-    return;
-  }
-  if (with_b) {
-    // outer residual: compensated sums, B - sum starting from B
-    Acc2 sr, si;
-    sr.add(br);
-    for (int j = 0; j < nr; ++j) {
-      double k = mesh.tc[i + (size_t)j * nr] - bl * mesh.blo0[i + (size_t)j * nr];
-      double2 x = __ldg(xc + j);
-      sr.add_prod(-k, x.x);
-      si.add_prod(-k, x.y);
-    }
-    double2 xi = xc[i];
-    sr.add_prod(-d, xi.x);
-    si.add_prod(-d, xi.y);
-    // the low words ride along in a second output slot: (value, low part) packed by the caller
-    out[(size_t)(c * nr + i) + (size_t)col * ldo] = make_double2(sr.hi, si.hi);
-    if (lo_out) lo_out[(size_t)(c * nr + i) + (size_t)col * ldo] = make_double2(sr.lo, si.lo);
-    return;
-  }
-  for (int j = 0; j < nr; ++j) {
-    double k = mesh.tc[i + (size_t)j * nr] - bl * mesh.blo0[i + (size_t)j * nr];
-    double2 x = __ldg(xc + j);
-    ar = fma(k, x.x, ar);
-    ai = fma(k, x.y, ai);
-  }
-  double2 xi = xc[i];
-  ar = fma(d, xi.x, ar);
-  ai = fma(d, xi.y, ai);
-  out[(size_t)(c * nr + i) + (size_t)col * ldo] = make_double2(br - ar, -ai);
-}
 
 // ------------------------------------------------------------------ tiled residual products
-// The plain (uncompensated) operator products of the refinement as batched FP64 tiles:
+// The operator products of the refinement (structured C(E), FP64) as batched tiles:
 //   kinetic:  batch c,  out[c*nr + i, col]  = b(i, col) - sum_j K_c(i, j) X[c*nr + j, col],
 //             K_c = tc - bloch_c blo0 + diag(fac_c / r_i^2 + kk_c)  (real, built per tile);
-//   coupling: batch i,  out[c*nr + i, col] -= sum_c' cpot(r_i, c, c') X[c'*nr + i, col].
-// 256 threads compute a 64 x 64 tile (4 x 4 complex values each) from 16-deep K chunks
-// staged in shared memory; the same sums as resid_kinetic_kernel / resid_coupling_kernel in
-// a different order of summation.
+//   coupling: batch i,  out[c*nr + i, col] -= sum_c' cpot(r_i, c, c') X[c'*nr + i, col]
+// (src/rmatrix_hp.F90:246-293 for the matrix they multiply by).  resid_tile_kernel: 256
+// threads compute a 64 x 64 tile (4 x 4 complex values each) from 16-deep K chunks staged in
+// shared memory; resid_tile2_kernel the compensated and modulus variants of the outer steps.
 struct KineticTile {
   MeshDev mesh;
   ChannelData ch;
@@ -282,6 +225,117 @@ __global__ void __launch_bounds__(256, 2) resid_tile_kernel(Op op, int M, int Nc
     }
 }
 
+// The outer-step variants of the same products, 32 x 64 tiles (2 x 4 values per thread):
+//   kComp1:  kinetic, out = B - K_c X with compensated (Dot2) sums; the low words go to lo;
+//   kComp2:  coupling, out = (out + lo) - V X with compensated sums, rounded once;
+//   kAbs1:   kinetic, out = |B| + |K_c| |X| (real part; the rounding scale of the residual);
+//   kAbs2:   coupling, out += |V| |X| (real part).
+enum ResidTileMode { kComp1 = 0, kComp2 = 1, kAbs1 = 2, kAbs2 = 3 };
+
+template <class Op, bool REAL_A, int MODE>
+__global__ void __launch_bounds__(256) resid_tile2_kernel(Op op, int M, int Ncol, int K, double2* out, long ldo,
+                                                          double2* lo) {
+  constexpr int BM = 32, BN = 64, BK = 16;
+  using AT = typename std::conditional<REAL_A, double, double2>::type;
+  __shared__ AT As[BK][BM];
+  __shared__ double2 Bs[BK][BN + 1];
+  const int z = blockIdx.z;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;
+  Acc2 sr[2][4], si[2][4];
+  double ar[2][4];
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      ar[r][q] = 0.0;
+      const int m = m0 + tx + 16 * r, n = n0 + ty + 16 * q;
+      if (m < M && n < Ncol) {
+        const size_t idx = op.o(z, m, n, ldo);
+        if constexpr (MODE == kComp1) {
+          sr[r][q].add(op.init(z, m, n, out, idx).x);
+        } else if constexpr (MODE == kComp2) {
+          const double2 o = out[idx], l = lo[idx];
+          sr[r][q].hi = o.x;
+          sr[r][q].lo = l.x;
+          si[r][q].hi = o.y;
+          si[r][q].lo = l.y;
+        } else if constexpr (MODE == kAbs1) {
+          ar[r][q] = fabs(op.init(z, m, n, out, idx).x);
+        } else {
+          ar[r][q] = out[idx].x;
+        }
+      }
+    }
+  for (int k0 = 0; k0 < K; k0 += BK) {
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int idx = tid + 256 * e;
+      const int mm = idx % BM, kk = idx / BM;
+      const int m = m0 + mm, k = k0 + kk;
+      if constexpr (REAL_A) {
+        As[kk][mm] = (m < M && k < K) ? op.a(z, m, k) : 0.0;
+      } else {
+        As[kk][mm] = (m < M && k < K) ? op.a(z, m, k) : make_double2(0.0, 0.0);
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int idx = tid + 256 * e;
+      const int kk = idx % BK, nn = idx / BK;
+      const int n = n0 + nn, k = k0 + kk;
+      Bs[kk][nn] = (n < Ncol && k < K) ? op.b(z, k, n) : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < BK; ++kk) {
+      AT av[2];
+      double2 bv[4];
+#pragma unroll
+      for (int r = 0; r < 2; ++r) av[r] = As[kk][tx + 16 * r];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) bv[q] = Bs[kk][ty + 16 * q];
+#pragma unroll
+      for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if constexpr (MODE == kComp1) {
+            sr[r][q].add_prod(-av[r], bv[q].x);
+            si[r][q].add_prod(-av[r], bv[q].y);
+          } else if constexpr (MODE == kComp2) {
+            sr[r][q].add_prod(-av[r].x, bv[q].x);
+            sr[r][q].add_prod(av[r].y, bv[q].y);
+            si[r][q].add_prod(-av[r].x, bv[q].y);
+            si[r][q].add_prod(-av[r].y, bv[q].x);
+          } else if constexpr (MODE == kAbs1) {
+            ar[r][q] = fma(fabs(av[r]), hypot(bv[q].x, bv[q].y), ar[r][q]);
+          } else {
+            ar[r][q] = fma(hypot(av[r].x, av[r].y), hypot(bv[q].x, bv[q].y), ar[r][q]);
+          }
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int m = m0 + tx + 16 * r, n = n0 + ty + 16 * q;
+      if (m < M && n < Ncol) {
+        const size_t idx = op.o(z, m, n, ldo);
+        if constexpr (MODE == kComp1) {
+          out[idx] = make_double2(sr[r][q].hi, si[r][q].hi);
+          lo[idx] = make_double2(sr[r][q].lo, si[r][q].lo);
+        } else if constexpr (MODE == kComp2) {
+          out[idx] = make_double2(sr[r][q].value(), si[r][q].value());
+        } else {
+          out[idx] = make_double2(ar[r][q], 0.0);
+        }
+      }
+    }
+}
+
 // Potential re-laid out per mesh point: vt[(i*nch + c')*nch + c] = cpot(r_i, c, c'), so the
 // coupling residual reads it with consecutive channels in consecutive threads.
 __global__ void cpot_transpose_kernel(const double2* __restrict__ cpot, long ncp1, long ndim, int nr, int nch,
@@ -295,73 +349,6 @@ __global__ void cpot_transpose_kernel(const double2* __restrict__ cpot, long ncp
   vt[idx] = cpot[(size_t)i + ncp1 * ((size_t)c + ndim * (size_t)cp)];
 }
 
-// out -= V X for the coupling part: (V X)[(c,i), col] = sum_c' cpot(r_i, c, c') X[(c',i), col]
-// with V read from the per-point layout of cpot_transpose_kernel.  absmode != 0 adds
-// |V| |X| to the real part instead.  grid (nr, ceil(ncol/32)), block 256: thread ->
-// (channel c, column).
-// With lo (low words from resid_kinetic_kernel) the coupling sums are compensated too and
-// the result is rounded once: out = hi + lo.
-__global__ void resid_coupling_kernel(int nr, int nch, const double2* __restrict__ vt, const double2* __restrict__ X,
-                                      long ldx, int ncol, double2* out, long ldo, int absmode,
-                                      const double2* __restrict__ lo) {
-  extern __shared__ double2 xs[];  // [ncol_tile][nch] X values at radial point i
-  const int i = blockIdx.x;
-  const int ct = 32;
-  const int col0 = blockIdx.y * ct;
-  const int ncl = min(ct, ncol - col0);
-  for (int idx = threadIdx.x; idx < ncl * nch; idx += blockDim.x) {
-    int cp = idx % nch, cc = idx / nch;
-    xs[cc * nch + cp] = X[(size_t)(cp * nr + i) + (size_t)(col0 + cc) * ldx];
-  }
-  __syncthreads();
-  const double2* vi = vt + (size_t)i * nch * nch;
-  for (int idx = threadIdx.x; idx < ncl * nch; idx += blockDim.x) {
-    int c = idx % nch, cc = idx / nch;
-    double ar = 0.0, ai = 0.0;
-    if (absmode) {
-      for (int cp = 0; cp < nch; ++cp) {
-        double2 v = __ldg(vi + (size_t)cp * nch + c);
-        double2 x = xs[cc * nch + cp];
-        ar = fma(hypot(v.x, v.y), hypot(x.x, x.y), ar);
-      }
-      double2* p = out + (size_t)(c * nr + i) + (size_t)(col0 + cc) * ldo;
-      p->x += ar;
-      continue;
-    }
-    double2* p = out + (size_t)(c * nr + i) + (size_t)(col0 + cc) * ldo;
-    if (lo) {
-      const double2 l = lo[(size_t)(c * nr + i) + (size_t)(col0 + cc) * ldo];
-      Acc2 sr, si;
-      double2 o = *p;
-      sr.hi = o.x;
-      sr.lo = l.x;
-      si.hi = o.y;
-      si.lo = l.y;
-      for (int cp = 0; cp < nch; ++cp) {
-        double2 v = __ldg(vi + (size_t)cp * nch + c);
-        double2 x = xs[cc * nch + cp];
-        sr.add_prod(-v.x, x.x);
-        sr.add_prod(v.y, x.y);
-        si.add_prod(-v.x, x.y);
-        si.add_prod(-v.y, x.x);
-      }
-      *p = make_double2(sr.value(), si.value());
-      continue;
-    }
-    for (int cp = 0; cp < nch; ++cp) {
-      double2 v = __ldg(vi + (size_t)cp * nch + c);
-      double2 x = xs[cc * nch + cp];
-      ar = fma(v.x, x.x, ar);
-      ar = fma(-v.y, x.y, ar);
-      ai = fma(v.x, x.y, ai);
-      ai = fma(v.y, x.x, ai);
-    }
-    double2 o = *p;
-    o.x -= ar;
-    o.y -= ai;
-    *p = o;
-  }
-}
 
 // Per-column sums of |x|^2 of an N x ncol block; one CTA per column (deterministic).
 __global__ void colnorm2_kernel(const double2* __restrict__ X, long ldx, int N, double* out) {
@@ -409,13 +396,16 @@ __global__ void copy_d_kernel(const double2* __restrict__ src, long lds, double2
   dst[(size_t)r + (size_t)col * ldd] = src[(size_t)r + (size_t)col * lds];
 }
 // ||A||_F^2 of a dense FP64 complex matrix (column-major), accumulated into *fro2.
+// ||A||_F^2 (N x N): block = 256 rows of the columns blockIdx.y + k gridDim.y, one atomic per
+// block.
 __global__ void fro2_kernel(const double2* __restrict__ A, long lda, int N, double* fro2) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  const int col = blockIdx.y;
   double sq = 0.0;
   if (r < N) {
-    double2 v = A[(size_t)r + (size_t)col * lda];
-    sq = v.x * v.x + v.y * v.y;
+    for (int col = blockIdx.y; col < N; col += gridDim.y) {
+      double2 v = A[(size_t)r + (size_t)col * lda];
+      sq += v.x * v.x + v.y * v.y;
+    }
   }
   for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
   __shared__ double red[32];

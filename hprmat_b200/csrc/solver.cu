@@ -747,23 +747,31 @@ static int apply_residual(hprmat_b200_ctx* c, const Operator& op, const double2*
     return HPRMAT_B200_OK;
   }
   if (op.structured) {
+    // outer residual (compensated, low words in rlo) or its rounding scale (absmode)
     const int nr = op.mesh.nr;
-    // the outer residual (with B) is formed with compensated sums; low words in R64
     double2* lo = nullptr;
-    if (with_b && !absmode) {
+    if (!absmode) {
       TRY(c->rlo.ensure((size_t)ldo * ncol * sizeof(double2)));
       lo = c->rlo.as<double2>();
     }
-    dim3 g1(cdiv_u(nr, 32), op.nch, cdiv_u(ncol, 8));
-    resid_kinetic_kernel<<<g1, dim3(32, 8), 0, c->stream>>>(op.mesh, op.ch, X, ldx, ncol, out, ldo, with_b ? 1 : 0,
-                                                            absmode ? 1 : 0, lo);
+    KineticTile kt{op.mesh, op.ch, X, ldx, with_b ? 1 : 0};
+    CouplingTile ct{op.vt, X, ldx, nr, op.nch};
+    const dim3 gk(cdiv_u(nr, 32), cdiv_u(ncol, 64), op.nch), gc(cdiv_u(op.nch, 32), cdiv_u(ncol, 64), nr);
+    if (absmode) {
+      resid_tile2_kernel<KineticTile, true, kAbs1><<<gk, 256, 0, c->stream>>>(kt, nr, ncol, nr, out, ldo, lo);
+      LAUNCH_CHECK();
+      resid_tile2_kernel<CouplingTile, false, kAbs2><<<gc, 256, 0, c->stream>>>(ct, op.nch, ncol, op.nch, out, ldo,
+                                                                               lo);
+    } else {
+      resid_tile2_kernel<KineticTile, true, kComp1><<<gk, 256, 0, c->stream>>>(kt, nr, ncol, nr, out, ldo, lo);
+      LAUNCH_CHECK();
+      resid_tile2_kernel<CouplingTile, false, kComp2><<<gc, 256, 0, c->stream>>>(ct, op.nch, ncol, op.nch, out,
+                                                                                ldo, lo);
+    }
     LAUNCH_CHECK();
-    size_t sm = (size_t)32 * op.nch * sizeof(double2);
-    TRY(set_smem(resid_coupling_kernel, sm));
-    dim3 g2(nr, cdiv_u(ncol, 32));
-    resid_coupling_kernel<<<g2, 256, sm, c->stream>>>(nr, op.nch, op.vt, X, ldx, ncol, out, ldo, absmode ? 1 : 0, lo);
-    LAUNCH_CHECK();
-  } else {
+    return HPRMAT_B200_OK;
+  }
+  {
     dim3 g0(cdiv_u(N, 256), ncol);
     if (with_b) {
       copy_d_kernel<<<g0, 256, 0, c->stream>>>(op.B, op.ldb, out, ldo, N);
@@ -1065,7 +1073,7 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
   const double bnorm = sqrt(q2n * nch);
   LUState st;
   int status = HPRMAT_B200_OK;
-  dim3 ga(cdiv_u(N, 256), N);
+  dim3 ga(cdiv_u(N, 256), std::min(N, 512));  // assemble_kernel strides over the columns
   dim3 gr(cdiv_u(N, 256), nch);
   double* d_fro2 = reinterpret_cast<double*>(c->status.as<int>() + 32);
   HPR_CUDA_TRY(cudaMemsetAsync(d_fro2, 0, sizeof(double), c->stream));
@@ -1235,7 +1243,7 @@ static int solve_dense_core(hprmat_b200_ctx* c, const double2* dA, double2* dB, 
     if (bn == 0.0) bn = 1.0;
     double* d_fro2 = reinterpret_cast<double*>(c->status.as<int>() + 32);
     HPR_CUDA_TRY(cudaMemsetAsync(d_fro2, 0, sizeof(double), c->stream));
-    fro2_kernel<<<ga, 256, 0, c->stream>>>(dA, N, N, d_fro2);
+    fro2_kernel<<<dim3(cdiv_u(N, 256), std::min(N, 512)), 256, 0, c->stream>>>(dA, N, N, d_fro2);
     LAUNCH_CHECK();
     double cn2;
     HPR_CUDA_TRY(cudaMemcpyAsync(&cn2, d_fro2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
