@@ -83,8 +83,6 @@ struct DevBuf {
 };
 
 static constexpr int kSwapStride = 3 * kMaxNB + 4;  // ints per step in the swap store
-static constexpr int kGmresM = 12;                   // longest FGMRES cycle per outer step
-static constexpr double kInnerTol = 1e-7;            // cycle stops once the residual fell this much
 
 struct hprmat_b200_ctx {
   int device = 0;
@@ -107,12 +105,18 @@ struct hprmat_b200_ctx {
   int rop_nrhs = 0;
   // wavefront solves (mixed path, nb = 128): sigma maps and permutation, transposed
   // off-diagonal blocks, diagonal-inverse planes, right-side / solution planes, flags
-  DevBuf wsig, wperm, wT, wdi, wbp, wyp, wxp, wflags;
+  DevBuf wsig, wperm, wT, wdi, wbp, wyp, wxp, wflags, wdf1, wdf2, wptmp, wotmp;
   TcOperand op_wT, op_wdi, op_wbp, op_wyp, op_wxp;
   bool wave_ready = false;
-  int wave_un = 64;
+  int wave_un = 0;        // right-hand sides per unit (64, 128; 0: 128 when nrhs > 64)
+  int wave_sb = 0;        // blocks per diagonal super block of the scaled factors (1, 2, 4; 0: auto)
+  int wave_sb_ready = 1;  // the value the current factors were prepared with
   bool wave_enabled = true;  // wavefront solves (else block-step solves)
   bool tc_trsm = true;       // U12 by the tensor cores from L11^-1 (else substitution)
+  int panel_rpc_min = 32;    // fewest panel rows per CTA
+  int gmres_m = 12;          // longest FGMRES cycle per outer step (<= kGmresMaxM)
+  double inner_tol0 = 1e-7;  // first cycle stops once the residual fell this much
+  bool zero_start = false;   // refinement starts from X = 0 instead of the FP32 solution
   int w_N = 0, w_npad = 0;
   long w_xld = 0, w_xplane = 0;
   bool wave_trace = false;
@@ -289,6 +293,9 @@ static int pick_nb(const hprmat_b200_ctx* c, int N, size_t elem, int preferred) 
 static int wave_prepare(hprmat_b200_ctx* c, const LUState& st) {
   const int N = st.N, ns = st.nsteps;
   c->wave_ready = false;
+  // super blocks of 4 blocks (2 for nsteps < 4): a quarter of the dependency links, at the
+  // price of 4x larger diagonal inverses in the one-time preparation
+  const int sb = c->wave_sb > 0 ? c->wave_sb : (ns >= 4 ? 4 : 2);
   const long sig_ld = (N + 3) / 4 * 4;
   TRY(c->wsig.ensure((size_t)ns * sig_ld * sizeof(int)));
   TRY(c->wperm.ensure((size_t)3 * N * sizeof(int) + 64));
@@ -297,18 +304,37 @@ static int wave_prepare(hprmat_b200_ctx* c, const LUState& st) {
   const long ldt = (N + 3) / 4 * 4;
   const long tplane = ldt * (long)N;
   TRY(c->wT.ensure((size_t)4 * tplane * sizeof(float)));
-  const long di_plane = (long)2 * ns * 128 * 128;
-  TRY(c->wdi.ensure((size_t)4 * di_plane * sizeof(float)));
   if (wave_perm_chain(c->swaps.as<int>(), kSwapStride, N, ns, work, c->wsig.as<int>(), sig_ld, perm0, c->stream) ||
       wave_transpose_offdiag(c->lup.as<float>(), c->lup_ld, c->lup_plane, c->wsig.as<int>(), sig_ld, N, ns,
-                             c->wT.as<float>(), ldt, tplane, c->stream) ||
-      wave_dinv_planes(c->inv.as<float2>(), ns, c->wdi.as<float>(), di_plane, c->stream) ||
-      tc_make_operand(c->tcplan, c->op_wdi, c->wdi.as<float>(), 128, (long)2 * ns * 128, 128, di_plane, 128) ||
+                             c->wT.as<float>(), ldt, tplane, c->stream))
+    return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+  // inverses of the diagonal super blocks: doubling from the 128-row blocks
+  const float2* cur = c->inv.as<float2>();
+  int nblk = ns;
+  for (int h = 128, lvl = 0; h < 128 * sb; h *= 2, ++lvl) {
+    const int nsup = (nblk + 1) / 2;
+    TRY(c->wptmp.ensure((size_t)2 * nsup * h * h * sizeof(float2)));
+    TRY(c->wotmp.ensure((size_t)2 * nsup * h * h * sizeof(float2)));
+    DevBuf& dst = (lvl & 1) ? c->wdf2 : c->wdf1;
+    TRY(dst.ensure((size_t)2 * nsup * 4 * h * h * sizeof(float2)));
+    if (wave_dinv_double(cur, h, nblk, c->wT.as<float>(), ldt, tplane, N, c->wptmp.as<float2>(),
+                         c->wotmp.as<float2>(), dst.as<float2>(), c->stream))
+      return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+    cur = dst.as<float2>();
+    nblk = nsup;
+    c->launches += 3;
+  }
+  const int hs = 128 * sb;
+  const long di_plane = (long)2 * nblk * hs * hs;
+  TRY(c->wdi.ensure((size_t)4 * di_plane * sizeof(float)));
+  if (wave_dinv_planes(cur, nblk, hs, c->wdi.as<float>(), di_plane, c->stream) ||
+      tc_make_operand(c->tcplan, c->op_wdi, c->wdi.as<float>(), hs, (long)2 * nblk * hs, hs, di_plane, 128) ||
       tc_make_operand(c->tcplan, c->op_wT, c->wT.as<float>(), N, N, ldt, tplane, 128) ||
-      wave_scale_offdiag(c->tcplan, c->op_wdi, c->op_wT, N, ns, c->lup.as<float>(), c->lup_ld, c->lup_plane,
+      wave_scale_offdiag(c->tcplan, c->op_wdi, c->op_wT, N, ns, sb, c->lup.as<float>(), c->lup_ld, c->lup_plane,
                          c->stream))
     return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
-  c->launches += 4;
+  c->launches += 5;
+  c->wave_sb_ready = sb;
   c->wave_ready = true;
   return HPRMAT_B200_OK;
 }
@@ -317,7 +343,7 @@ static int wave_prepare(hprmat_b200_ctx* c, const LUState& st) {
 // planes of P X, forward sweep into the Y planes, backward sweep into X.
 static int lu_solve_wave(hprmat_b200_ctx* c, const LUState& st, float2* X, long ldx, int nrhs) {
   const int N = st.N, ns = st.nsteps;
-  const int un = c->wave_un;
+  const int un = c->wave_un > 0 ? c->wave_un : (nrhs > 64 ? 128 : 64);
   const int G = (nrhs + un - 1) / un;
   const int npad = G * un;
   const long xld = (N + 3) / 4 * 4;
@@ -347,6 +373,7 @@ static int lu_solve_wave(hprmat_b200_ctx* c, const LUState& st, float2* X, long 
   ws.nsteps = ns;
   ws.nrhs = nrhs;
   ws.un = un;
+  ws.sb = c->wave_sb_ready;
   ws.xp = c->wyp.as<float>();
   ws.xp_ld = xld;
   ws.xp_plane = xplane;
@@ -419,7 +446,11 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
     const int k0 = s * NB;
     const int ncols = std::min(NB, N - k0);
     const int m = N - k0;
-    const int G = std::min(G0, std::max(1, (m + 31) / 32));
+    // CTAs of the panel: at least panel_rpc_min rows each (fewer CTAs contend less for the
+    // per-column barrier), as many as the shared memory needs
+    const int rpc_max = (int)(((size_t)c->smem_optin - 8192) / sizeof(T) / NB) - 2;
+    const int G = std::min(G0, std::max(std::min(G0, std::max(1, (m + c->panel_rpc_min - 1) / c->panel_rpc_min)),
+                                        (m + rpc_max - 1) / rpc_max));
     const int rpc = (m + G - 1) / G;
     const size_t smem = ((size_t)NB * (rpc | 1) + NB) * sizeof(T);
     TRY(set_smem(pk, smem));
@@ -801,12 +832,12 @@ static int frob_norm(hprmat_b200_ctx* c, const double2* X, long ldx, int N, int 
 
 // Mixed path: X64 (N x nrhs, FP64) from the FP32 factors, refined with FGMRES on the FP64
 // operator.  Each outer step: r = B - C X; stop when |r|_F/|B|_F < tol; otherwise run
-// kGmresM flexible-GMRES iterations on C d = r, preconditioned by the FP32 LU solve, and
+// up to gmres_m flexible-GMRES iterations on C d = r, preconditioned by the FP32 LU solve, and
 // X += d.  Returns NOT_CONVERGED if max_refine outer corrections did not reach tol.
 static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W32, const LUState& st,
                         double2* X64, long ldx, int nrhs, double bnorm, double cnorm, hprmat_b200_stats* stats) {
   const int N = op.N;
-  const int m = kGmresM;
+  const int m = std::min(c->gmres_m, kGmresMaxM);
   const long ldv = st.ld;
   const long vstride = ldv * nrhs;
   TRY(c->V.ensure((size_t)(m + 1) * vstride * sizeof(double2)));
@@ -905,7 +936,7 @@ static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W3
     gmres_start_kernel<256><<<nrhs, 256, 0, c->stream>>>(gs);
     LAUNCH_CHECK();
     // the first cycle starts from the FP32 solution; later cycles only polish
-    const double inner_tol = outer == 0 ? kInnerTol : 1e-2;
+    const double inner_tol = outer == 0 ? c->inner_tol0 : 1e-2;
     int jdone = 0;
     double est = 1.0;
     for (int j = 0; j < m; ++j) {
@@ -1117,9 +1148,13 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
     float2* X32 = c->X.as<float2>();
     surface_rhs_kernel<float2><<<gr, 256, 0, c->stream>>>(md.q2, nr, nch, X32, ld, N, 1.0);
     LAUNCH_CHECK();
-    TRY(lu_solve_tc(c, st, X32, ld, nch));
-    f2d_kernel<<<gr, 256, 0, c->stream>>>(X32, ld, X64, ld, N, nullptr);
-    LAUNCH_CHECK();
+    if (c->zero_start) {
+      HPR_CUDA_TRY(cudaMemsetAsync(X64, 0, (size_t)ld * nch * sizeof(double2), c->stream));
+    } else {
+      TRY(lu_solve_tc(c, st, X32, ld, nch));
+      f2d_kernel<<<gr, 256, 0, c->stream>>>(X32, ld, X64, ld, N, nullptr);
+      LAUNCH_CHECK();
+    }
     if (stats) stats->ms_solve = ms_since(t2);
     auto t3 = Clock::now();
     double cn2;
@@ -1591,6 +1626,25 @@ int hprmat_b200_dev_panel_trace_read(hprmat_b200_ctx* c, long long* out, int cap
 int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* c, const char* key, int value) {
   TRY(check_ctx(c));
   if (!key) return fail(HPRMAT_B200_ERR_ARG, "null key");
+  if (strcmp(key, "gmres_m") == 0) {
+    if (value < 1 || value > kGmresMaxM) return fail(HPRMAT_B200_ERR_ARG, "gmres_m must be in 1..%d", kGmresMaxM);
+    c->gmres_m = value;
+    return HPRMAT_B200_OK;
+  }
+  if (strcmp(key, "inner_tol0_exp") == 0) {
+    if (value < 1 || value > 15) return fail(HPRMAT_B200_ERR_ARG, "inner_tol0_exp must be in 1..15");
+    c->inner_tol0 = pow(10.0, -value);
+    return HPRMAT_B200_OK;
+  }
+  if (strcmp(key, "zero_start") == 0) {
+    c->zero_start = value != 0;
+    return HPRMAT_B200_OK;
+  }
+  if (strcmp(key, "panel_rpc_min") == 0) {
+    if (value < 1) return fail(HPRMAT_B200_ERR_ARG, "panel_rpc_min must be positive");
+    c->panel_rpc_min = value;
+    return HPRMAT_B200_OK;
+  }
   if (strcmp(key, "wave") == 0) {
     c->wave_enabled = value != 0;
     return HPRMAT_B200_OK;
@@ -1599,8 +1653,15 @@ int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* c, const char* key, int value) {
     c->tc_trsm = value != 0;
     return HPRMAT_B200_OK;
   }
+  if (strcmp(key, "wave_sb") == 0) {
+    if (value != 0 && value != 1 && value != 2 && value != 4)
+      return fail(HPRMAT_B200_ERR_ARG, "wave_sb must be 0 (automatic), 1, 2 or 4");
+    c->wave_sb = value;
+    return HPRMAT_B200_OK;
+  }
   if (strcmp(key, "wave_un") == 0) {
-    if (value != 64 && value != 128) return fail(HPRMAT_B200_ERR_ARG, "wave_un must be 64 or 128");
+    if (value != 0 && value != 64 && value != 128)
+      return fail(HPRMAT_B200_ERR_ARG, "wave_un must be 0 (automatic), 64 or 128");
     c->wave_un = value;
     return HPRMAT_B200_OK;
   }

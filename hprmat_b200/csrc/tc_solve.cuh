@@ -17,6 +17,10 @@
 // each one persistent kernel: a unit is (block row j, group of UN right-hand sides); its
 // accumulator lives in TMEM while its CTA streams the blocks of row j and the published
 // solution blocks; the epilogue publishes block j through a per-unit flag.
+// With super blocks of sb blocks the diagonal inverses are those of the sb*128-row diagonal
+// blocks (built by doubling from the 128-row ones) and the sums skip the blocks of the own
+// super block, so the sb block rows of a super block do not depend on each other and the
+// dependency chain has nsteps / sb links.
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -39,13 +43,20 @@ int wave_perm_chain(const int* swaps, int swap_stride, int N, int nsteps, int* w
 int wave_transpose_offdiag(const float* lup, long lup_ld, long lup_plane, const int* sig, long sig_ld, int N,
                            int nsteps, float* T, long ldt, long tplane, cudaStream_t s);
 
-// DI planes, row-major 128 x 128 per block: row (2 j + u) * 128 + i (u = 0 for L_jj^-1,
-// 1 for U_jj^-1), from the column-major float2 inverses inv[(2 j + u) * 128 * 128].
-int wave_dinv_planes(const float2* inv, int nsteps, float* di, long di_plane, cudaStream_t s);
+// DI planes, row-major h x h per block: row (2 J + u) * h + i (u = 0 for L_JJ^-1, 1 for
+// U_JJ^-1), from the column-major float2 inverses inv[(2 J + u) * h * h], nblk blocks.
+int wave_dinv_planes(const float2* inv, int nblk, int h, float* di, long di_plane, cudaStream_t s);
 
-// Off-diagonal blocks of the LU planes <- D_jj^-1 * (block from T), on the tensor cores.
-int wave_scale_offdiag(TcGemmPlan& p, const TcOperand& opD, const TcOperand& opT, int N, int nsteps, float* lup,
-                       long lup_ld, long lup_plane, cudaStream_t s);
+// Inverses of the 2h x 2h diagonal super blocks from those of the h x h blocks (dfh, nblk
+// blocks) and the off-diagonal blocks in T; ptmp, otmp: 2 ceil(nblk/2) h^2 float2 each;
+// df2h: 2 ceil(nblk/2) (2h)^2 float2.
+int wave_dinv_double(const float2* dfh, int h, int nblk, const float* T, long ldt, long tplane, int N, float2* ptmp,
+                     float2* otmp, float2* df2h, cudaStream_t s);
+
+// Off-diagonal blocks of the LU planes outside the diagonal super blocks (sb blocks each)
+// <- D_JJ^-1 * (block from T), on the tensor cores.
+int wave_scale_offdiag(TcGemmPlan& p, const TcOperand& opD, const TcOperand& opT, int N, int nsteps, int sb,
+                       float* lup, long lup_ld, long lup_plane, cudaStream_t s);
 
 // B-operand planes of (P B): bp[p][c][i] = split(X[perm0[i] + c ldx]), i < N, c < nrhs.
 int wave_rhs_planes(const float2* X, long ldx, const int* perm0, int N, int nrhs, float* bp, long bld, long bplane,
@@ -53,6 +64,7 @@ int wave_rhs_planes(const float2* X, long ldx, const int* perm0, int N, int nrhs
 
 struct WaveSolve {
   int N = 0, nsteps = 0, nrhs = 0;
+  int sb = 1;                  // blocks per diagonal super block of the scaled factors
   int un = 64;                 // right-hand sides per unit (64 or 128)
   float* xp = nullptr;         // output planes (column c, row i at xp[p*xp_plane + c*xp_ld + i])
   long xp_ld = 0, xp_plane = 0;

@@ -32,8 +32,17 @@ int hprmat_b200_dev_set_profile(hprmat_b200_ctx* ctx, int enable);
 int hprmat_b200_dev_counters(hprmat_b200_ctx* ctx, unsigned long long* launches, double* tc_ms, double* tc_flops,
                              int* tc_launches, int reset);
 
-/* Tuning knobs for benchmarks.  "wave_un": right-hand sides per unit of the wavefront
-   triangular solves (64 or 128). */
+/* Tuning knobs for benchmarks and experiments (defaults in parentheses):
+     "wave_un"        right-hand sides per unit of the wavefront solves: 64, 128 (0: 128 when
+                      nrhs > 64, else 64);
+     "wave_sb"        blocks per diagonal super block of the solves' scaled factors: 1, 2, 4
+                      (0: 4, or 2 below 4 blocks); takes effect at the next factorisation;
+     "wave"           wavefront solves on/off (1);
+     "tc_trsm"        U12 by a tensor-core product with L11^-1 (1) or by substitution (0);
+     "panel_rpc_min"  fewest panel rows per CTA (32);
+     "gmres_m"        longest FGMRES cycle, <= 16 (12);
+     "inner_tol0_exp" first cycle runs until the residual fell 10^-value (7);
+     "zero_start"     refinement from X = 0 instead of the FP32 solution (0). */
 int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* ctx, const char* key, int value);
 
 /* Tracing of the wavefront triangular solves of the mixed path.  With enable != 0 every

@@ -147,6 +147,23 @@ def test_production_generator_against_fixture(ctx, nch):
     assert _rel(cu[:nopen, :nopen], fx["u"]) <= U_TOL, ctx.last_stats
 
 
+@pytest.mark.parametrize("sb,un", [(1, 64), (2, 128), (4, 64), (4, 128)])
+def test_wavefront_variants(sb, un):
+    """The wavefront solves with other super-block sizes and unit widths (dev tuning hooks),
+    on the production generator at N = 4200: 33 blocks of 128 rows, the last one partial and
+    without a partner block when the diagonal inverses are doubled."""
+    w = workloads.production(nch=21)
+    ref = _oracle_u(w)
+    c = api.Context(precision="mixed")
+    lib = nat.load()
+    nat.check(lib.hprmat_b200_dev_set_tuning(c._h, b"wave_sb", sb))
+    nat.check(lib.hprmat_b200_dev_set_tuning(c._h, b"wave_un", un))
+    cu, nopen = c.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+    assert nopen == ref.nopen
+    assert _rel(cu[:nopen, :nopen], ref.cu) <= U_TOL, c.last_stats
+    c.close()
+
+
 def test_sweep_generator_closed_at_40mev(ctx):
     w = workloads.sweep(20)
     ref = _oracle_u(w)
