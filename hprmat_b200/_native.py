@@ -32,7 +32,7 @@ EXPORTED = (
     "hprmat_b200_solve_linear", "hprmat_b200_solve_linear_device", "hprmat_b200_solve_rmatrix",
     "gpu_b200_solve_mixed_", "gpu_b200_solve_double_", "gpu_b200_finalize_", "hprmat_b200_status_string",
     "hprmat_b200_last_error", "hprmat_b200_version", "hprmat_b200_boundary",
-    "hprmat_b200_solve_linear_noalloc",
+    "hprmat_b200_solve_linear_noalloc", "hprmat_b200_rmatrix_scan",
     # include/hprmat_b200_dev.h
     "hprmat_b200_dev_tc_update", "hprmat_b200_dev_split_planes", "hprmat_b200_dev_set_profile",
     "hprmat_b200_dev_counters", "hprmat_b200_dev_wave_trace", "hprmat_b200_dev_wave_trace_read",
@@ -59,6 +59,14 @@ class Stats(ctypes.Structure):
         d["floor_history"] = [self.floor_history[i] for i in range(9) if self.floor_history[i] != 0.0]
         d["residual_history"] = [self.residual_history[i] for i in range(9) if self.residual_history[i] != 0.0]
         return d
+
+
+class ScanBlock(ctypes.Structure):
+    """hprmat_b200_scan_block (include/hprmat_b200.h)."""
+    _fields_ = [("nch", ctypes.c_int), ("lval", ctypes.POINTER(ctypes.c_int)), ("cpot", ctypes.POINTER(ctypes.c_double)),
+                ("ncp1", ctypes.c_int), ("nenergies", ctypes.c_int), ("qk", ctypes.POINTER(ctypes.c_double)),
+                ("eta", ctypes.POINTER(ctypes.c_double)), ("cu", ctypes.POINTER(ctypes.c_double)),
+                ("nopen", ctypes.POINTER(ctypes.c_int)), ("status", ctypes.POINTER(ctypes.c_int))]
 
 
 class HprmatError(RuntimeError):
@@ -90,6 +98,7 @@ def load():
         "hprmat_b200_rmat_ini": (I, [P, I, I, D, DP]),
         "hprmat_b200_rmatrix": (I, [P, I, IP, DP, DP, D, I, I, DP, I, I, DP, IP, SP]),
         "hprmat_b200_rmatrix_device": (I, [P, I, IP, DP, DP, D, I, I, P, I, I, P, IP, SP]),
+        "hprmat_b200_rmatrix_scan": (I, [P, I, ctypes.POINTER(ScanBlock), D, I, I, DP]),
         "hprmat_b200_solve_linear": (I, [P, DP, DP, I, I, SP]),
         "hprmat_b200_solve_linear_device": (I, [P, P, P, I, I, SP]),
         "hprmat_b200_solve_rmatrix": (I, [P, DP, DP, I, I, D, DP, SP]),

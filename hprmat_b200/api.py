@@ -117,6 +117,38 @@ class Context:
         nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
         return cu, nopen.value
 
+    def rmatrix_scan(self, blocks, rmax, nr, nworkers=0, allow_unconverged=False):
+        """Batched energy scan.  ``blocks``: sequence of (lval, cpot, qk, eta) with qk/eta of
+        shape (nenergies, nch), cpot (ncp1, nch, nch) complex, Fortran order.  Returns a list of
+        (cu (nenergies, nch, nch) with U in cu[e, :nopen, :nopen], nopen (nenergies,),
+        status (nenergies,)) and sets ``last_scan_seconds``."""
+        keep, arr, out = [], [], []
+        for lval, cpot, qk, eta in blocks:
+            lval = np.ascontiguousarray(lval, dtype=np.int32)
+            cpot = np.asfortranarray(cpot, dtype=np.complex128)
+            qk = np.ascontiguousarray(np.atleast_2d(qk), dtype=np.float64)
+            eta = np.ascontiguousarray(np.atleast_2d(eta), dtype=np.float64)
+            nE, nch = qk.shape
+            if cpot.shape[1] != nch or eta.shape != qk.shape or lval.shape[0] != nch:
+                raise ValueError("rmatrix_scan: inconsistent block shapes")
+            cu = np.zeros((nE, nch, nch), dtype=np.complex128)       # per energy (nch, nch) row-major view
+            nopen = np.zeros(nE, dtype=np.int32)
+            status = np.zeros(nE, dtype=np.int32)
+            keep += [lval, cpot, qk, eta]
+            b = nat.ScanBlock(nch, _iptr(lval), _dptr(cpot), cpot.shape[0], nE, _dptr(qk), _dptr(eta), _dptr(cu),
+                              _iptr(nopen), _iptr(status))
+            arr.append(b)
+            out.append((cu, nopen, status))
+        self._ensure_mesh(nr, 1, rmax)
+        blocks_c = (nat.ScanBlock * len(arr))(*arr)
+        secs = ctypes.c_double(0.0)
+        s = self._lib.hprmat_b200_rmatrix_scan(self._h, len(arr), blocks_c, float(rmax), int(nr), int(nworkers),
+                                               ctypes.byref(secs))
+        self.last_scan_seconds = secs.value
+        nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
+        # the library writes each U column-major (Fortran) into its (nch, nch) slot
+        return [(np.ascontiguousarray(cu.transpose(0, 2, 1)), nopen, status) for cu, nopen, status in out]
+
     def rmatrix_device(self, nch, lval, qk, eta, rmax, nr, ns, d_cpot, ncp1, ndim, d_cu, allow_unconverged=False):
         """Device-resident variant: ``d_cpot``/``d_cu`` are device addresses (ints)."""
         self._ensure_mesh(nr, ns, rmax)

@@ -3,13 +3,16 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -60,6 +63,10 @@ static int fail(int status, const char* fmt, ...) {
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
   int ensure(size_t b) {
     if (b <= bytes && p) return HPRMAT_B200_OK;
     release();
@@ -121,6 +128,9 @@ struct hprmat_b200_ctx {
   long w_xld = 0, w_xplane = 0;
   bool wave_trace = false;
   DevBuf wtrace, ptrace;
+  // batched energy scans: worker contexts (own stream and buffers) and the blocks' potentials
+  std::vector<hprmat_b200_ctx*> scan_workers;
+  std::vector<std::unique_ptr<DevBuf>> scan_cpot;
   int wtrace_units = 0;
   int* h_status = nullptr;  // pinned
   double* h_norms = nullptr;  // pinned
@@ -1375,6 +1385,9 @@ int hprmat_b200_destroy(hprmat_b200_ctx* c) {
                     &c->swaps, &c->ipiv, &c->stage, &c->status, &c->ops, &c->inv, &c->chan, &c->rmat,
                     &c->zwork, &c->cpot, &c->cu, &c->norms, &c->lup, &c->rop, &c->rsurf, &c->vt, &c->rlo, &c->linv};
   for (DevBuf* b : bufs) b->release();
+  for (hprmat_b200_ctx* w : c->scan_workers) hprmat_b200_destroy(w);
+  c->scan_workers.clear();
+  c->scan_cpot.clear();
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->h_norms) cudaFreeHost(c->h_norms);
@@ -1440,6 +1453,101 @@ int hprmat_b200_rmatrix(hprmat_b200_ctx* c, int nch, const int* lval, const doub
   }
   if (stats) stats->status = s;
   return s;
+}
+
+// Batched energy scan: every block's potential is copied once; (block, energy) units are
+// taken largest first by worker contexts, one host thread and one stream each, so that the
+// solves of different units overlap on the device.  Each unit is rmatrix_core as for one
+// energy.
+int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_scan_block* blocks, double rmax,
+                             int nr, int nworkers, double* seconds) {
+  TRY(check_ctx(c));
+  if (nblocks < 0 || (nblocks > 0 && !blocks) || nr <= 0 || !(rmax > 0.0))
+    return fail(HPRMAT_B200_ERR_ARG, "rmatrix_scan: invalid arguments");
+  auto t0 = Clock::now();
+  struct Unit {
+    int b, e;
+    long n;
+  };
+  std::vector<Unit> units;
+  for (int b = 0; b < nblocks; ++b) {
+    const hprmat_b200_scan_block& B = blocks[b];
+    if (B.nch <= 0 || B.nenergies < 0 || !B.lval || !B.cpot || B.ncp1 < nr || !B.cu || !B.nopen || !B.status ||
+        (B.nenergies > 0 && (!B.qk || !B.eta)))
+      return fail(HPRMAT_B200_ERR_ARG, "rmatrix_scan: invalid block %d", b);
+    for (int e = 0; e < B.nenergies; ++e) units.push_back({b, e, (long)B.nch * nr});
+  }
+  std::stable_sort(units.begin(), units.end(), [](const Unit& x, const Unit& y) { return x.n > y.n; });
+  // potentials on the device, once per block
+  HPR_CUDA_TRY(cudaSetDevice(c->device));
+  c->scan_cpot.clear();
+  for (int b = 0; b < nblocks; ++b) {
+    const hprmat_b200_scan_block& B = blocks[b];
+    const size_t pbytes = (size_t)B.ncp1 * B.nch * B.nch * sizeof(double2);
+    c->scan_cpot.emplace_back(new DevBuf());
+    TRY(c->scan_cpot.back()->ensure(pbytes));
+    HPR_CUDA_TRY(cudaMemcpyAsync(c->scan_cpot.back()->p, B.cpot, pbytes, cudaMemcpyHostToDevice, c->stream));
+  }
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  // workers
+  if (nworkers <= 0) nworkers = 4;
+  nworkers = std::max(1, std::min<int>(nworkers, (int)units.size()));
+  while ((int)c->scan_workers.size() < nworkers) {
+    hprmat_b200_ctx* w = nullptr;
+    TRY(hprmat_b200_create(c->device, &c->opts, &w));
+    c->scan_workers.push_back(w);
+  }
+  std::vector<double> zrma((size_t)nr);
+  for (int i = 0; i < nworkers; ++i) {
+    hprmat_b200_ctx* w = c->scan_workers[i];
+    w->opts = c->opts;
+    w->wave_sb = c->wave_sb;
+    w->wave_un = c->wave_un;
+    TRY(hprmat_b200_rmat_ini(w, nr, 1, rmax, zrma.data()));
+  }
+  std::atomic<size_t> next{0};
+  std::atomic<int> first_error{0};
+  std::mutex err_mu;
+  std::string err_msg;
+  auto work = [&](int wi) {
+    hprmat_b200_ctx* w = c->scan_workers[wi];
+    cudaSetDevice(w->device);
+    for (;;) {
+      const size_t k = next.fetch_add(1);
+      if (k >= units.size()) break;
+      const Unit& u = units[k];
+      const hprmat_b200_scan_block& B = blocks[u.b];
+      const size_t ubytes = (size_t)B.nch * B.nch * sizeof(double2);
+      int s = w->cu.ensure(ubytes);
+      int nopen = 0;
+      if (s == HPRMAT_B200_OK)
+        s = rmatrix_core(w, B.nch, B.lval, B.qk + (size_t)u.e * B.nch, B.eta + (size_t)u.e * B.nch, rmax, nr, 1,
+                         c->scan_cpot[u.b]->as<double2>(), B.ncp1, B.nch, w->cu.as<double2>(), &nopen, nullptr);
+      if (s == HPRMAT_B200_OK || s == HPRMAT_B200_NOT_CONVERGED) {
+        double* dst = B.cu + (size_t)u.e * B.nch * B.nch * 2;
+        if (cudaMemcpyAsync(dst, w->cu.p, ubytes, cudaMemcpyDeviceToHost, w->stream) != cudaSuccess ||
+            cudaStreamSynchronize(w->stream) != cudaSuccess)
+          s = HPRMAT_B200_ERR_CUDA;
+      }
+      B.nopen[u.e] = nopen;
+      B.status[u.e] = s;
+      if (s != HPRMAT_B200_OK) {
+        int z = 0;
+        if (first_error.compare_exchange_strong(z, s)) {
+          std::lock_guard<std::mutex> lk(err_mu);
+          err_msg = hprmat_b200_last_error();
+        }
+      }
+    }
+  };
+  std::vector<std::thread> threads;
+  for (int i = 1; i < nworkers; ++i) threads.emplace_back(work, i);
+  work(0);
+  for (auto& t : threads) t.join();
+  if (seconds) *seconds = std::chrono::duration<double>(Clock::now() - t0).count();
+  const int fe = first_error.load();
+  if (fe != HPRMAT_B200_OK && fe != HPRMAT_B200_NOT_CONVERGED) return fail(fe, "rmatrix_scan: %s", err_msg.c_str());
+  return fe;
 }
 
 int hprmat_b200_solve_linear_device(hprmat_b200_ctx* c, const void* d_A, void* d_B, int n, int nrhs,

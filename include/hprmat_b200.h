@@ -90,6 +90,32 @@ int hprmat_b200_set_stream(hprmat_b200_ctx* ctx, void* stream);
    src/rmatrix_hp.F90:61-159.  zrma (nr*ns doubles) may be NULL. */
 int hprmat_b200_rmat_ini(hprmat_b200_ctx* ctx, int nr, int ns, double rmax, double* zrma);
 
+/* One J-pi block of a batched energy scan (hprmat_b200_rmatrix_scan).  The reference has no
+   batched entry: its drivers call rmatrix once per energy in a host loop
+   (examples/Ex1/example1_hp.f90:102-110, examples/Ex4/example4_hp.f90:118-134). */
+typedef struct {
+  int nch;              /* channels of the block */
+  const int* lval;      /* [nch] angular momenta */
+  const double* cpot;   /* host, complex (ncp1, nch, nch) Fortran order; energy independent */
+  int ncp1;             /* leading dimension of cpot (>= nr) */
+  int nenergies;        /* energies of this block */
+  const double* qk;     /* [nenergies][nch] signed wave numbers (negative: closed) */
+  const double* eta;    /* [nenergies][nch] Sommerfeld parameters */
+  double* cu;           /* out: [nenergies] complex (nch, nch) collision matrices, as rmatrix's cu */
+  int* nopen;           /* out: [nenergies] open channels */
+  int* status;          /* out: [nenergies] status of each solve */
+} hprmat_b200_scan_block;
+
+/* Collision matrices of every (block, energy) unit, one interval on the mesh (nr, rmax) shared by
+   all blocks, precision and refinement from the context's options.  Each block's potential is
+   copied to the device once; the units run largest first on nworkers concurrent worker streams
+   (0: 4), each with its own working buffers, kept by the context for later scans.  Returns
+   HPRMAT_B200_OK, HPRMAT_B200_NOT_CONVERGED if some unit stopped above its tolerance, or the
+   error of the first unit that failed (the other units still run); seconds receives the wall
+   time of the call. */
+int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* ctx, int nblocks, const hprmat_b200_scan_block* blocks, double rmax,
+                             int nr, int nworkers, double* seconds);
+
 /* Collision matrix for one (J, pi, E): rmatrix(nch, lval, qk, eta, rmax, nr, ns, cpot, cu,
    ncp1, ndim, nopen, ...) of src/rmatrix_hp.F90:175-368, for local potentials (ncp2 = 0) and
    one interval (ns = 1).  Host buffers: cpot is complex (ncp1, ndim, ndim), cu is complex
