@@ -117,7 +117,7 @@ class Context:
         nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
         return cu, nopen.value
 
-    def rmatrix_scan(self, blocks, rmax, nr, nworkers=0, allow_unconverged=False):
+    def rmatrix_scan(self, blocks, rmax, nr, nworkers=0, allow_unconverged=False, raise_on_unit_error=True):
         """Batched energy scan.  ``blocks``: sequence of (lval, cpot, qk, eta) with qk/eta of
         shape (nenergies, nch), cpot (ncp1, nch, nch) complex, Fortran order.  Returns a list of
         (cu (nenergies, nch, nch) with U in cu[e, :nopen, :nopen], nopen (nenergies,),
@@ -145,7 +145,8 @@ class Context:
         s = self._lib.hprmat_b200_rmatrix_scan(self._h, len(arr), blocks_c, float(rmax), int(nr), int(nworkers),
                                                ctypes.byref(secs))
         self.last_scan_seconds = secs.value
-        nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
+        if raise_on_unit_error:
+            nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
         # the library writes each U column-major (Fortran) into its (nch, nch) slot
         return [(np.ascontiguousarray(cu.transpose(0, 2, 1)), nopen, status) for cu, nopen, status in out]
 
