@@ -33,6 +33,7 @@ EXPORTED = (
     "gpu_b200_solve_mixed_", "gpu_b200_solve_double_", "gpu_b200_finalize_", "hprmat_b200_status_string",
     "hprmat_b200_last_error", "hprmat_b200_version", "hprmat_b200_boundary",
     "hprmat_b200_solve_linear_noalloc", "hprmat_b200_rmatrix_scan",
+    "hprmat_b200_rmatrix_adjoint",
     # include/hprmat_b200_dev.h
     "hprmat_b200_dev_tc_update", "hprmat_b200_dev_split_planes", "hprmat_b200_dev_set_profile",
     "hprmat_b200_dev_counters", "hprmat_b200_dev_wave_trace", "hprmat_b200_dev_wave_trace_read",
@@ -99,6 +100,7 @@ def load():
         "hprmat_b200_rmatrix": (I, [P, I, IP, DP, DP, D, I, I, DP, I, I, DP, IP, SP]),
         "hprmat_b200_rmatrix_device": (I, [P, I, IP, DP, DP, D, I, I, P, I, I, P, IP, SP]),
         "hprmat_b200_rmatrix_scan": (I, [P, I, ctypes.POINTER(ScanBlock), D, I, I, DP]),
+        "hprmat_b200_rmatrix_adjoint": (I, [P, I, IP, DP, DP, D, I, I, DP, I, I, DP, DP, IP, DP, SP]),
         "hprmat_b200_solve_linear": (I, [P, DP, DP, I, I, SP]),
         "hprmat_b200_solve_linear_device": (I, [P, P, P, I, I, SP]),
         "hprmat_b200_solve_rmatrix": (I, [P, DP, DP, I, I, D, DP, SP]),

@@ -150,6 +150,30 @@ class Context:
         # the library writes each U column-major (Fortran) into its (nch, nch) slot
         return [(np.ascontiguousarray(cu.transpose(0, 2, 1)), nopen, status) for cu, nopen, status in out]
 
+    def rmatrix_adjoint(self, nch, lval, qk, eta, rmax, nr, cpot, gu):
+        """Collision matrix and the gradient of a real loss with respect to the potential.
+        ``gu``: dL/dU in the convention dL = Re sum conj(gu) dU (PyTorch's), nopen x nopen or
+        larger.  Returns (cu, nopen, grad) with grad shaped like cpot (same convention)."""
+        self._ensure_mesh(nr, 1, rmax)
+        lval = np.ascontiguousarray(lval, dtype=np.int32)
+        qk = np.ascontiguousarray(qk, dtype=np.float64)
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        cpot = np.asfortranarray(cpot, dtype=np.complex128)
+        ncp1, ndim = cpot.shape[0], cpot.shape[1]
+        g = np.zeros((ndim, ndim), dtype=np.complex128, order="F")
+        gu = np.asarray(gu, dtype=np.complex128)
+        g[:gu.shape[0], :gu.shape[1]] = gu
+        cu = np.zeros((ndim, ndim), dtype=np.complex128, order="F")
+        grad = np.zeros_like(cpot, order="F")
+        nopen = ctypes.c_int(0)
+        st = Stats()
+        s = self._lib.hprmat_b200_rmatrix_adjoint(self._h, int(nch), _iptr(lval), _dptr(qk), _dptr(eta), float(rmax),
+                                                  int(nr), 1, _dptr(cpot), int(ncp1), int(ndim), _dptr(g), _dptr(cu),
+                                                  ctypes.byref(nopen), _dptr(grad), ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        nat.check(s)
+        return cu, nopen.value, grad
+
     def rmatrix_device(self, nch, lval, qk, eta, rmax, nr, ns, d_cpot, ncp1, ndim, d_cu, allow_unconverged=False):
         """Device-resident variant: ``d_cpot``/``d_cu`` are device addresses (ints)."""
         self._ensure_mesh(nr, ns, rmax)

@@ -21,6 +21,7 @@
 #include "common.cuh"
 #include "coulomb.cuh"
 #include "lu.cuh"
+#include "adjoint.cuh"
 #include "rmat_kernels.cuh"
 #include "tc_gemm.cuh"
 #include "tc_solve.cuh"
@@ -128,6 +129,10 @@ struct hprmat_b200_ctx {
   long w_xld = 0, w_xplane = 0;
   bool wave_trace = false;
   DevBuf wtrace, ptrace;
+  // last FP64 factorisation of rmatrix (for the adjoint): N, ld, nb, nsteps; adjoint scratch
+  int f64_N = 0, f64_nb = 0, f64_nsteps = 0;
+  long f64_ld = 0;
+  DevBuf adj_y, adj_part, adj_grad;
   // batched energy scans: worker contexts (own stream and buffers) and the blocks' potentials
   std::vector<hprmat_b200_ctx*> scan_workers;
   std::vector<std::unique_ptr<DevBuf>> scan_cpot;
@@ -1130,6 +1135,10 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
     if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
     auto t1 = Clock::now();
     TRY(factor<double2>(c, W, ld, N, false, nb, st));
+    c->f64_N = st.N;
+    c->f64_ld = st.ld;
+    c->f64_nb = st.nb;
+    c->f64_nsteps = st.nsteps;
     if (stats) stats->ms_factor = ms_since(t1);
     auto t2 = Clock::now();
     TRY(lu_solve<double2>(c, W, st, X64, ld, nch));
@@ -1203,6 +1212,78 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
   }
   (void)t0;
   return status;
+}
+
+// X <- C^-T X with the FP64 factors in W (adjoint.cuh for the step order).
+static int lu_solve_trans(hprmat_b200_ctx* c, const double2* W, long ld, int N, int nb, int nsteps, double2* X,
+                          long ldx, int nrhs) {
+  const double2* inv = c->inv.as<double2>();
+  const int* swb = c->swaps.as<int>();
+  constexpr int kRowsPerSplit = 256;
+  auto update = [&](int acol, int ncols, int r0, int r1, int k0) -> int {  // X_block -= A(r0:r1, blk)^T X(r0:r1)
+    if (r1 <= r0) return HPRMAT_B200_OK;
+    const int nsplit = (r1 - r0 + kRowsPerSplit - 1) / kRowsPerSplit;
+    TRY(c->adj_part.ensure((size_t)nsplit * ncols * 128 * sizeof(double2)));
+    for (int cb = 0; cb < nrhs; cb += 128) {
+      const int nc = std::min(128, nrhs - cb);
+      trans_partial_kernel<<<nsplit, 256, 0, c->stream>>>(W, ld, acol, ncols, X + (size_t)cb * ldx, ldx, nc, r0, r1,
+                                                          kRowsPerSplit, c->adj_part.as<double2>());
+      LAUNCH_CHECK();
+      trans_reduce_kernel<<<cdiv_u(ncols * nc, 256), 256, 0, c->stream>>>(c->adj_part.as<double2>(), nsplit, ncols,
+                                                                          nc, X + (size_t)cb * ldx, ldx, k0);
+      LAUNCH_CHECK();
+    }
+    return HPRMAT_B200_OK;
+  };
+  for (int s = 0; s < nsteps; ++s) {
+    const int k0 = s * nb, ncols = std::min(nb, N - k0);
+    TRY(update(k0, ncols, 0, k0, k0));
+    diag_trans_kernel<<<nrhs, 128, 0, c->stream>>>(inv + ((size_t)2 * s + 1) * nb * nb, nb, ncols, k0, X, ldx);
+    LAUNCH_CHECK();
+  }
+  for (int s = nsteps - 1; s >= 0; --s) {
+    const int k0 = s * nb, ncols = std::min(nb, N - k0);
+    TRY(update(k0, ncols, k0 + ncols, N, k0));
+    diag_trans_kernel<<<nrhs, 128, 0, c->stream>>>(inv + (size_t)2 * s * nb * nb, nb, ncols, k0, X, ldx);
+    LAUNCH_CHECK();
+    perm_inv_kernel<<<nrhs, 256, 0, c->stream>>>(swb + (size_t)s * kSwapStride, kMaxNB, k0, ncols, X, ldx);
+    LAUNCH_CHECK();
+  }
+  c->launches += (size_t)nsteps * 5;
+  return HPRMAT_B200_OK;
+}
+
+// Small dense complex solve on the host (partial pivoting): A (n x n, column-major) X = B
+// (n x m); A and B are overwritten.  Returns false if A is singular.
+static bool host_csolve(std::vector<double2>& A, std::vector<double2>& B, int n, int m) {
+  auto at = [&](int i, int j) -> double2& { return A[(size_t)i + (size_t)j * n]; };
+  auto bt = [&](int i, int j) -> double2& { return B[(size_t)i + (size_t)j * n]; };
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    double best = -1.0;
+    for (int i = k; i < n; ++i) {
+      const double v = fabs(at(i, k).x) + fabs(at(i, k).y);
+      if (v > best) { best = v; p = i; }
+    }
+    if (!(best > 0.0)) return false;
+    if (p != k) {
+      for (int j = 0; j < n; ++j) std::swap(at(k, j), at(p, j));
+      for (int j = 0; j < m; ++j) std::swap(bt(k, j), bt(p, j));
+    }
+    const double2 inv = crecip(at(k, k));
+    for (int i = k + 1; i < n; ++i) {
+      const double2 l = cmul(at(i, k), inv);
+      for (int j = k + 1; j < n; ++j) cfms(at(i, j), l, at(k, j));
+      for (int j = 0; j < m; ++j) cfms(bt(i, j), l, bt(k, j));
+    }
+  }
+  for (int j = 0; j < m; ++j)
+    for (int i = n - 1; i >= 0; --i) {
+      double2 v = bt(i, j);
+      for (int k = i + 1; k < n; ++k) cfms(v, at(i, k), bt(k, j));
+      bt(i, j) = cmul(v, crecip(at(i, i)));
+    }
+  return true;
 }
 
 // Dense solve A X = B with device operands (A read only, B overwritten with X).
@@ -1548,6 +1629,108 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_
   const int fe = first_error.load();
   if (fe != HPRMAT_B200_OK && fe != HPRMAT_B200_NOT_CONVERGED) return fail(fe, "rmatrix_scan: %s", err_msg.c_str());
   return fe;
+}
+
+// Adjoint of one collision matrix: the forward solve on the FP64 path, then one solve with
+// C^T from the same factors (adjoint.cuh).  With G = gu (dL = Re sum conj(G) dU):
+//   M = W G^H Z_O^-1,  W = diag(cop) U - diag(conj cop)       (dU = Z_O^-1 dRt W)
+//   M2(i2, i1) = M(m2, m1) sqrt(k_i1 / k_i2)                  (Rt = R sqrt(k_i / k_j), open)
+//   C^T Y = Q M2^T,  Q = blockdiag(q2)                         (R = Q^T X / a)
+//   grad(r_i, c, c') = -conj(sum_col Y[(c,i), col] X[(c',i), col]) / a
+int hprmat_b200_rmatrix_adjoint(hprmat_b200_ctx* c, int nch, const int* lval, const double* qk, const double* eta,
+                                double rmax, int nr, int ns, const double* cpot, int ncp1, int ndim, const double* gu,
+                                double* cu, int* nopen, double* grad, hprmat_b200_stats* stats) {
+  TRY(check_ctx(c));
+  if (!cpot || !cu || !gu || !grad || !nopen || ndim < nch || ncp1 < nr || nch <= 0)
+    return fail(HPRMAT_B200_ERR_ARG, "rmatrix_adjoint: invalid arguments");
+  const size_t pbytes = (size_t)ncp1 * ndim * ndim * sizeof(double2);
+  const size_t ubytes = (size_t)ndim * ndim * sizeof(double2);
+  TRY(c->cpot.ensure(pbytes));
+  TRY(c->cu.ensure(ubytes));
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->cpot.p, cpot, pbytes, cudaMemcpyHostToDevice, c->stream));
+  const int prec = c->opts.precision;
+  c->opts.precision = HPRMAT_B200_PREC_FP64;
+  int s = rmatrix_core(c, nch, lval, qk, eta, rmax, nr, ns, c->cpot.as<double2>(), ncp1, ndim, c->cu.as<double2>(),
+                       nopen, stats);
+  c->opts.precision = prec;
+  if (s != HPRMAT_B200_OK && s != HPRMAT_B200_NOT_CONVERGED) return s;
+  if (c->f64_nb > 64) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "rmatrix_adjoint: panel_nb above 64");
+  HPR_CUDA_TRY(cudaMemcpyAsync(cu, c->cu.p, ubytes, cudaMemcpyDeviceToHost, c->stream));
+  std::vector<double2> R((size_t)nch * nch);
+  HPR_CUDA_TRY(cudaMemcpyAsync(R.data(), c->rmat.p, R.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const int N = c->f64_N;
+  const long ld = c->f64_ld;
+  const double a = rmax / ns;
+  TRY(c->adj_grad.ensure(pbytes));
+  HPR_CUDA_TRY(cudaMemsetAsync(c->adj_grad.p, 0, pbytes, c->stream));
+  Boundary bnd;
+  TRY(boundary_values(nch, lval, qk, eta, rmax, a, bnd));
+  const int no = bnd.nopen;
+  if (no > 0) {
+    const double2* U = reinterpret_cast<const double2*>(cu);
+    const double2* G = reinterpret_cast<const double2*>(gu);
+    auto sk = [&](int m1, int m2) { return sqrt(qk[bnd.open_idx[m1]] / qk[bnd.open_idx[m2]]); };
+    std::vector<double2> Zt((size_t)no * no), Pt((size_t)no * no);  // Z_O^T and (W G^H)^T
+    for (int m2 = 0; m2 < no; ++m2)
+      for (int m1 = 0; m1 < no; ++m1) {
+        double2 r = R[bnd.open_idx[m1] + (size_t)bnd.open_idx[m2] * nch];
+        const double sc = sk(m1, m2);
+        r.x *= sc;
+        r.y *= sc;
+        double2 z = cmul(r, bnd.cop[m2]);
+        z.x = -z.x;
+        z.y = -z.y;
+        if (m1 == m2) {
+          z.x += bnd.co[m1].x;
+          z.y += bnd.co[m1].y;
+        }
+        Zt[m2 + (size_t)m1 * no] = z;  // (Z_O^T)(m2, m1) = Z_O(m1, m2)
+      }
+    for (int a1 = 0; a1 < no; ++a1)
+      for (int b1 = 0; b1 < no; ++b1) {
+        double2 acc = mk(0.0, 0.0);  // (W G^H)(a1, b1) = sum_k W(a1, k) conj(G(b1, k))
+        for (int k = 0; k < no; ++k) {
+          double2 w = cmul(bnd.cop[a1], U[a1 + (size_t)k * ndim]);
+          if (a1 == k) {
+            w.x -= bnd.cop[a1].x;
+            w.y += bnd.cop[a1].y;
+          }
+          const double2 g = G[b1 + (size_t)k * ndim];
+          cfma(acc, w, mk(g.x, -g.y));
+        }
+        Pt[b1 + (size_t)a1 * no] = acc;
+      }
+    // M = (W G^H) Z_O^-1  <=>  Z_O^T M^T = (W G^H)^T
+    if (!host_csolve(Zt, Pt, no, no)) return fail(HPRMAT_B200_SINGULAR, "rmatrix_adjoint: singular Z_O");
+    // right-hand side Q M2^T: rhs[(c,i), col] = q2_i M2(col, c), M2(i2, i1) = M(m2, m1) sqrt(k_i1/k_i2)
+    std::vector<double2> M2((size_t)nch * nch, mk(0.0, 0.0));
+    for (int m1 = 0; m1 < no; ++m1)
+      for (int m2 = 0; m2 < no; ++m2) {
+        double2 v = Pt[m1 + (size_t)m2 * no];  // M^T(m1, m2) = M(m2, m1)
+        const double sc = sk(m1, m2);
+        M2[bnd.open_idx[m2] + (size_t)bnd.open_idx[m1] * nch] = mk(v.x * sc, v.y * sc);
+      }
+    std::vector<double2> rhs((size_t)ld * nch, mk(0.0, 0.0));
+    for (int col = 0; col < nch; ++col)
+      for (int ch = 0; ch < nch; ++ch) {
+        const double2 m = M2[col + (size_t)ch * nch];
+        if (m.x == 0.0 && m.y == 0.0) continue;
+        for (int i = 0; i < nr; ++i)
+          rhs[(size_t)(ch * nr + i) + (size_t)col * ld] = mk(c->q2[i] * m.x, c->q2[i] * m.y);
+      }
+    TRY(c->adj_y.ensure(rhs.size() * sizeof(double2)));
+    double2* Y = c->adj_y.as<double2>();
+    HPR_CUDA_TRY(cudaMemcpyAsync(Y, rhs.data(), rhs.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    TRY(lu_solve_trans(c, c->W.as<double2>(), ld, N, c->f64_nb, c->f64_nsteps, Y, ld, nch));
+    potential_grad_kernel<<<dim3(nr, nch), 128, 0, c->stream>>>(Y, c->X64.as<double2>(), ld, nr, nch, nch, 1.0 / a,
+                                                                c->adj_grad.as<double2>(), ncp1, ndim);
+    LAUNCH_CHECK();
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));  // rhs must outlive its copy
+  }
+  HPR_CUDA_TRY(cudaMemcpyAsync(grad, c->adj_grad.p, pbytes, cudaMemcpyDeviceToHost, c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return s;
 }
 
 int hprmat_b200_solve_linear_device(hprmat_b200_ctx* c, const void* d_A, void* d_B, int n, int nrhs,

@@ -90,6 +90,17 @@ int hprmat_b200_set_stream(hprmat_b200_ctx* ctx, void* stream);
    src/rmatrix_hp.F90:61-159.  zrma (nr*ns doubles) may be NULL. */
 int hprmat_b200_rmat_ini(hprmat_b200_ctx* ctx, int nr, int ns, double rmax, double* zrma);
 
+/* Adjoint of the collision matrix (no counterpart in the reference).  For the arguments of
+   hprmat_b200_rmatrix and the gradient gu of a real loss L with respect to U (complex (ndim,
+   ndim), leading nopen x nopen block used; convention dL = Re sum conj(gu_ij) dU_ij, i.e.
+   2 dL/dconj(U), so gu = 2 (U - T) for L = sum |U - T|^2), returns U in cu and in grad (complex
+   (ncp1, ndim, ndim), as cpot) the gradient of L with respect to the potential at the mesh
+   points in the same convention (dL = Re sum conj(grad) dcpot); rows >= nr are zero.  The
+   forward solve runs on the FP64 path and the adjoint solve with C^T reuses its LU factors. */
+int hprmat_b200_rmatrix_adjoint(hprmat_b200_ctx* ctx, int nch, const int* lval, const double* qk, const double* eta,
+                                double rmax, int nr, int ns, const double* cpot, int ncp1, int ndim, const double* gu,
+                                double* cu, int* nopen, double* grad, hprmat_b200_stats* stats);
+
 /* One J-pi block of a batched energy scan (hprmat_b200_rmatrix_scan).  The reference has no
    batched entry: its drivers call rmatrix once per energy in a host loop
    (examples/Ex1/example1_hp.f90:102-110, examples/Ex4/example4_hp.f90:118-134). */

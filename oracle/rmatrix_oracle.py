@@ -378,3 +378,43 @@ def rmatrix(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, solver: str = "dense") -
         crma0_prev = crma0
     cu = collision_matrix(crma0_prev, bnd, qk)
     return RMatrixResult(cu, bnd.nopen, crma0_prev, bnd, x_last if ns == 1 else None)
+
+
+def rmatrix_adjoint(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, gu):
+    """FP64 reference gradient of a real loss L through U (ns = 1, dense NumPy/LAPACK).
+
+    The reference has no derivatives; this is the checker of the device adjoint.  ``gu`` is
+    dL/dU in the convention dL = Re sum conj(gu) dU; returns (U, grad) with grad shaped like
+    cpot (nr rows used) in the same convention, from
+      dU = Z_O^-1 dRt W,  W = diag(cop) U - diag(conj cop),  Rt = R sqrt(k_i/k_j),  R = Q^T X / a,
+      dX = -C^-1 dC X,    C^T Y = Q M2^T,  grad(r_i, c, c') = -conj(sum Y[(c,i), :] X[(c',i), :]) / a.
+    """
+    qk = np.asarray(qk, dtype=np.float64)
+    res = rmatrix(nch, lval, qk, eta, rmax, mesh, cpot)
+    bnd, no = res.boundary, res.nopen
+    nr = mesh.nr
+    a = mesh.rmax0
+    grad = np.zeros_like(np.asarray(cpot, dtype=np.complex128))
+    if no == 0:
+        return res.cu, grad
+    idx = bnd.npo_open
+    s = np.array([[math.sqrt(qk[i1] / qk[i2]) for i2 in idx] for i1 in idx])
+    rt = res.rma[np.ix_(idx, idx)] * s
+    zo = np.diag(bnd.co) - rt * bnd.cop[None, :]
+    u = res.cu
+    w = bnd.cop[:, None] * u - np.diag(np.conj(bnd.cop))
+    g = np.asarray(gu, dtype=np.complex128)[:no, :no]
+    m = (w @ g.conj().T) @ np.linalg.inv(zo)
+    m2 = np.zeros((nch, nch), dtype=np.complex128)
+    for a1, i1 in enumerate(idx):
+        for a2, i2 in enumerate(idx):
+            m2[i2, i1] = m[a2, a1] * s[a1, a2]
+    q = surface_rhs(mesh.q2[:, 0].astype(np.complex128), nch)   # (N, nch)
+    C = assemble(mesh, 1, nch, lval, qk, bnd.xc, cpot)
+    y = np.linalg.solve(C.T, q @ m2.T)
+    x = res.x
+    for c in range(nch):
+        for cp in range(nch):
+            h = np.sum(y[c * nr:(c + 1) * nr, :] * x[cp * nr:(cp + 1) * nr, :], axis=1)
+            grad[:nr, c, cp] = -np.conj(h) / a
+    return u, grad
