@@ -48,9 +48,10 @@ def parse():
     ap.add_argument("--solves-only", action="store_true",
                     help="only the device-resident timed solves (for profiler launch lists)")
     ap.add_argument("--nch", type=int, default=128, help="channels of the production generator (N = 200 nch)")
-    ap.add_argument("--workload", choices=["production", "scan"], default="production",
+    ap.add_argument("--workload", choices=["production", "scan", "adjoint"], default="production",
                     help="production: one N = 25600 solve per step (the headline); scan: the batched energy "
-                         "scan, 12 J-pi blocks x 256 energies (3072 solves) per step")
+                         "scan, 12 J-pi blocks x 256 energies (3072 solves) per step; adjoint: loss and gradients "
+                         "over 64 energies at N = 3200 per step")
     ap.add_argument("--workers", type=int, default=4, help="worker streams of the batched scan")
     return ap.parse_args()
 
@@ -263,6 +264,92 @@ def run_scan(args):
     return 0
 
 
+# ------------------------------------------------------------------ adjoint gradients
+def run_adjoint(args):
+    """One step = loss sum_E sum |U - U_target|^2 over 64 energies at N = 3200 (32 channels x
+    100 points) and its gradient with respect to the 6 potential parameters and the potential
+    at all mesh points (torch.autograd through hprmat_b200_rmatrix_adjoint).  Checked once
+    against central finite differences (step 1e-6) of the device forward and against the FP64
+    oracle adjoint at two energies."""
+    import torch
+    from hprmat_b200 import api, workloads
+    from hprmat_b200.autograd import collision_matrix, potential_matrix
+    from oracle import rmatrix_oracle as orc
+    w, energies = workloads.adjoint_case()
+    r = torch.from_numpy(workloads.lagrange_radii(w.nr, w.rmax))
+    coup = torch.from_numpy(w.coupling)
+    p0 = torch.tensor(w.params.as_array(), dtype=torch.float64)
+    ptarget = p0 * torch.tensor([1.02, 0.97, 1.01, 1.03, 0.95, 1.04], dtype=torch.float64)
+    ctx = api.Context(precision="mixed", max_refine=8, tol=1e-12)
+    # energies where COULFG (the reference's algorithm) cannot evaluate an open channel just above
+    # its threshold are dropped (the oracle fails on them too)
+    from oracle import special_functions as sf
+
+    def coulfg_ok(qk, eta):
+        return all(sf.coulfg(qk[c] * w.rmax, eta[c], float(w.lval[c]))[4] == 0 for c in range(w.nch) if qk[c] > 0)
+
+    kin_all = [workloads.channel_kinematics(e, w.thresholds, w.hm, w.params.z1z2) for e in energies]
+    kin = [k for k in kin_all if coulfg_ok(*k)]
+    tgt = np.asfortranarray(potential_matrix(r, coup, ptarget, w.hm, w.params.z1z2).numpy())
+    targets = [ctx.rmatrix(w.nch, w.lval, qk, eta, w.rmax, w.nr, 1, tgt)[0] for qk, eta in kin]
+
+    def loss(p):
+        cp = potential_matrix(r, coup, p, w.hm, w.params.z1z2)
+        tot = 0.0
+        for (qk, eta), ut in zip(kin, targets):
+            u = collision_matrix(cp, ctx, w.lval, qk, eta, w.rmax, w.nr)
+            no = u.shape[0]
+            tot = tot + torch.sum(torch.abs(u - torch.from_numpy(ut[:no, :no])) ** 2)
+        return tot, cp
+
+    for _ in range(args.warmup):
+        p = p0.clone().requires_grad_(True)
+        L, _ = loss(p)
+        L.backward()
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        p = p0.clone().requires_grad_(True)
+        L, cp = loss(p)
+        cp.retain_grad()
+        L.backward()
+        times.append(time.perf_counter() - t)
+    g = p.grad.numpy().copy()
+    # central finite differences of the device forward, step 1e-6 (relative to the parameter)
+    fd_err = 0.0
+    for k in range(6):
+        e = torch.zeros(6, dtype=torch.float64)
+        e[k] = 1e-6 * max(1.0, abs(float(p0[k])))
+        with torch.no_grad():
+            fd = (float(loss(p0 + e)[0]) - float(loss(p0 - e)[0])) / (2 * float(e[k]))
+        fd_err = max(fd_err, abs(fd - g[k]) / max(abs(fd), 1e-300))
+    # FP64 CPU reference gradient (oracle adjoint) at the first and last energy
+    mesh = orc.rmat_ini(w.nr, 1, w.rmax)
+    c_np = np.asfortranarray(potential_matrix(r, coup, p0, w.hm, w.params.z1z2).numpy())
+    ref_err = 0.0
+    for i in (0, len(kin) - 1):
+        qk, eta = kin[i]
+        u0 = orc.rmatrix(w.nch, w.lval, qk, eta, w.rmax, mesh, c_np).cu
+        gu = 2 * (u0 - targets[i][:u0.shape[0], :u0.shape[0]])
+        _, gref = orc.rmatrix_adjoint(w.nch, w.lval, qk, eta, w.rmax, mesh, c_np, gu)
+        _, _, gdev = ctx.rmatrix_adjoint(w.nch, w.lval, qk, eta, w.rmax, w.nr, c_np, gu)
+        ref_err = max(ref_err, float(np.linalg.norm(gdev - gref) / np.linalg.norm(gref)))
+    sec = min(times)
+    print(json.dumps({
+        "metric": "adjoint gradient evaluations/s", "value": 1.0 / sec, "unit": "gradients/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
+        "scaling": "none", "vs_baseline": None, "dtype": "c64 3xTF32 forward + c128 refinement; c128 adjoint",
+        "data": "synthetic (seeded adjoint generator, hprmat_b200/workloads.py)",
+        "config": {"workload": "adjoint: 32 channels x 100 points (N = 3200), 64 energies, loss sum |U - U_target|^2, "
+                               "gradients w.r.t. 6 potential parameters and the potential at all mesh points"},
+        "energies_used": len(kin), "energies_dropped_coulfg": len(kin_all) - len(kin),
+        "solves_per_step": 3 * len(kin),
+        "fd_rel_err_max": fd_err, "fd_step": 1e-6, "oracle_grad_rel_err_max": ref_err,
+        "loss": float(L.detach())}))
+    ctx.close()
+    return 0
+
+
 # ------------------------------------------------------------------ our arm
 def main():
     args = parse()
@@ -270,6 +357,8 @@ def main():
         return run_reference(args)
     if args.workload == "scan":
         return run_scan(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
     rank, world, local = dist_info()
     import torch
     import torch.distributed as dist
