@@ -37,7 +37,7 @@ EXPORTED = (
     # include/hprmat_b200_dev.h
     "hprmat_b200_dev_tc_update", "hprmat_b200_dev_split_planes", "hprmat_b200_dev_set_profile",
     "hprmat_b200_dev_counters", "hprmat_b200_dev_wave_trace", "hprmat_b200_dev_wave_trace_read",
-    "hprmat_b200_dev_panel_trace_read", "hprmat_b200_dev_set_tuning",
+    "hprmat_b200_dev_panel_trace_read", "hprmat_b200_dev_set_tuning", "hprmat_b200_dev_mesh",
 )
 
 
@@ -120,6 +120,7 @@ def load():
         "hprmat_b200_dev_wave_trace_read": (I, [P, ctypes.POINTER(ctypes.c_longlong), I, IP]),
         "hprmat_b200_dev_panel_trace_read": (I, [P, ctypes.POINTER(ctypes.c_longlong), I, IP]),
         "hprmat_b200_dev_set_tuning": (I, [P, ctypes.c_char_p, I]),
+        "hprmat_b200_dev_mesh": (I, [I, I, D, DP, DP, DP, DP, DP]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

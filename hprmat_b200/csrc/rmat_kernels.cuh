@@ -14,13 +14,25 @@ struct ChannelData {
   const double* bloch;   // [nch] xc(c,1) / a for closed channels, 0 for open ones
 };
 
+// One interval of the mesh (src/rmatrix_hp.F90:61-159).  The right-hand sides of a solve are
+// nq1 columns blockdiag(q1) (inner-boundary values, intervals after the first of a propagated
+// problem: nq1 = nch) followed by nch columns blockdiag(q2) (outer-boundary values).
 struct MeshDev {
-  const double* tc;      // [nr*nr] kinetic + Bloch matrix / a^2 (column-major)
-  const double* blo0;    // [nr*nr] Bloch matrix / a
-  const double* r;       // [nr] mesh radii
-  const double* q2;      // [nr] surface values
+  const double* tc;      // [nr*nr] kinetic + Bloch matrix of the interval / a^2 (column-major)
+  const double* blo0;    // [nr*nr] closed-channel Bloch matrix of the interval, times a:
+                         //   blo0 / a (first interval), blo2 / is - blo1 / (is - 1) (interval is)
+  const double* r;       // [nr] mesh radii of the interval
+  const double* q2;      // [nr] outer-boundary values
+  const double* q1;      // [nr] inner-boundary values (nullptr when nq1 = 0)
   int nr;
+  int nq1;
 };
+
+// Right-hand side value at row (c, i), column col: blockdiag(q1) columns, then blockdiag(q2).
+__device__ __forceinline__ double surface_value(const MeshDev& m, int c, int i, int col) {
+  if (col < m.nq1) return c == col ? m.q1[i] : 0.0;
+  return c == col - m.nq1 ? m.q2[i] : 0.0;
+}
 
 // Compensated accumulation (Ogita-Rump-Oishi Dot2): sum += a*b with the rounding errors of
 // the product (FMA) and of the sum (TwoSum) kept in a second word.  Gives the residual of
@@ -95,16 +107,17 @@ __global__ void assemble_kernel(MeshDev mesh, ChannelData ch, int nch, const dou
   }
 }
 
-// Channel-surface right-hand sides X = blockdiag(q2) (src/rmatrix_hp.F90:456-461), scaled.
+// Channel-surface right-hand sides X = [blockdiag(q1) | blockdiag(q2)] (src/rmatrix_hp.F90:456-461,
+// :604-609 for the propagated intervals), scaled.  grid (N / 256, nq1 + nch).
 template <typename T>
-__global__ void surface_rhs_kernel(const double* __restrict__ q2, int nr, int nch, T* X, long ldx,
-                                   int N, double scale) {
+__global__ void surface_rhs_kernel(MeshDev mesh, T* X, long ldx, int N, double scale) {
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   const int col = blockIdx.y;
   if (row >= N) return;
+  const int nr = mesh.nr;
   const int c = row / nr, i = row - c * nr;
   T v = czero<T>();
-  if (c == col) v.x = (typename RealOf<T>::R)(q2[i] * scale);
+  v.x = (typename RealOf<T>::R)(surface_value(mesh, c, i, col) * scale);
   X[(size_t)row + (size_t)col * ldx] = v;
 }
 
@@ -135,7 +148,7 @@ struct KineticTile {
   __device__ double2 b(int c, int j, int col) const { return X[(size_t)c * mesh.nr + j + (size_t)col * ldx]; }
   __device__ size_t o(int c, int i, int col, long ldo) const { return (size_t)c * mesh.nr + i + (size_t)col * ldo; }
   __device__ double2 init(int c, int i, int col, const double2*, size_t) const {
-    return make_double2((with_b && c == col) ? mesh.q2[i] : 0.0, 0.0);
+    return make_double2(with_b ? surface_value(mesh, c, i, col) : 0.0, 0.0);
   }
 };
 
@@ -655,12 +668,14 @@ __global__ void rel_change_kernel(const double2* __restrict__ a, const double2* 
 }
 
 // ---------------------------------------------------------------- R and U
-// R(i, j) = sum_r q2(r) X((i-1) nr + r, j) / a  (src/rmatrix_hp.F90:466-474 and :337).
+// R(i, j) = sum_r q(r) X((i-1) nr + r, j) * scale for j < ncols, R with leading dimension nch
+// (src/rmatrix_hp.F90:466-474 and :337 with q = q2, scale 1/a; :622-630 for the q1 and q2
+// projections of a propagated interval).  grid (nch, ceil(ncols / 128)), 128 threads.
 __global__ void rmat_extract_kernel(const double2* __restrict__ X, long ldx, const double* __restrict__ q2,
-                                    int nr, int nch, double inv_a, double2* R) {
+                                    int nr, int nch, int ncols, double inv_a, double2* R) {
   const int i = blockIdx.x;
   const int jc = threadIdx.x + blockIdx.y * blockDim.x;
-  if (jc >= nch) return;
+  if (jc >= ncols) return;
   const double2* x = X + (size_t)jc * ldx + (size_t)i * nr;
   double ar = 0.0, ai = 0.0;
   for (int r = 0; r < nr; ++r) {
@@ -669,6 +684,95 @@ __global__ void rmat_extract_kernel(const double2* __restrict__ X, long ldx, con
     ai = fma(q2[r], v.y, ai);
   }
   R[i + (size_t)jc * nch] = make_double2(ar * inv_a, ai * inv_a);
+}
+
+// A Z = B in one CTA (A: n x n, ld n; B: n x nrhs, ld ldb; both overwritten, B <- Z) by
+// Gaussian elimination with partial pivoting on |re| + |im| (the LAPACK izamax measure; the
+// first row on ties).  *info = k + 1 at the first zero pivot k (0-based); the elimination
+// continues with a zero reciprocal so that every thread reaches every barrier.
+__device__ void cta_gauss_solve(double2* A, int n, double2* B, long ldb, int nrhs, int* info) {
+  const int tid = threadIdx.x, NT = blockDim.x;
+  __shared__ int s_p;
+  __shared__ double s_v[32];
+  __shared__ int s_i[32];
+  for (int k = 0; k < n; ++k) {
+    double bv = -1.0;
+    int bi = 0x7fffffff;
+    for (int r = k + tid; r < n; r += NT) {
+      double v = fabs(A[r + (size_t)k * n].x) + fabs(A[r + (size_t)k * n].y);
+      if (v > bv) { bv = v; bi = r; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      double ov = __shfl_down_sync(0xffffffffu, bv, o);
+      int oi = __shfl_down_sync(0xffffffffu, bi, o);
+      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    }
+    if ((tid & 31) == 0) { s_v[tid >> 5] = bv; s_i[tid >> 5] = bi; }
+    __syncthreads();
+    if (tid < 32) {
+      bv = (tid < NT / 32) ? s_v[tid] : -1.0;
+      bi = (tid < NT / 32) ? s_i[tid] : 0x7fffffff;
+      for (int o = 16; o > 0; o >>= 1) {
+        double ov = __shfl_down_sync(0xffffffffu, bv, o);
+        int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+      }
+      if (tid == 0) {
+        s_p = bi;
+        if (bv == 0.0 && *info == 0) *info = k + 1;
+      }
+    }
+    __syncthreads();
+    const int p = s_p;
+    if (p != k) {
+      for (int c = tid; c < n; c += NT) {
+        double2 t = A[k + (size_t)c * n];
+        A[k + (size_t)c * n] = A[p + (size_t)c * n];
+        A[p + (size_t)c * n] = t;
+      }
+      for (int c = tid; c < nrhs; c += NT) {
+        double2 t = B[k + (size_t)c * ldb];
+        B[k + (size_t)c * ldb] = B[p + (size_t)c * ldb];
+        B[p + (size_t)c * ldb] = t;
+      }
+    }
+    __syncthreads();
+    double2 piv = A[k + (size_t)k * n];
+    double2 inv = (piv.x == 0 && piv.y == 0) ? make_double2(0, 0) : crecip(piv);
+    for (int r = k + 1 + tid; r < n; r += NT) A[r + (size_t)k * n] = cmul(A[r + (size_t)k * n], inv);
+    __syncthreads();
+    const int nrow = n - k - 1;
+    const int nca = n - k - 1;  // columns k+1.. of A
+    const int total = nrow * (nca + nrhs);
+    for (int idx = tid; idx < total; idx += NT) {
+      int r = k + 1 + idx % nrow;
+      int c = idx / nrow;
+      double2 l = A[r + (size_t)k * n];
+      if (c < nca) {
+        int cc = k + 1 + c;
+        double2 v = A[r + (size_t)cc * n];
+        cfms(v, l, A[k + (size_t)cc * n]);
+        A[r + (size_t)cc * n] = v;
+      } else {
+        int cc = c - nca;
+        double2 v = B[r + (size_t)cc * ldb];
+        cfms(v, l, B[k + (size_t)cc * ldb]);
+        B[r + (size_t)cc * ldb] = v;
+      }
+    }
+    __syncthreads();
+  }
+  // back substitution, columns of B in parallel
+  for (int c = tid; c < nrhs; c += NT) {
+    for (int k = n - 1; k >= 0; --k) {
+      double2 v = B[k + (size_t)c * ldb];
+      for (int q = k + 1; q < n; ++q) cfms(v, A[k + (size_t)q * n], B[q + (size_t)c * ldb]);
+      double2 d = A[k + (size_t)k * n];
+      v = (d.x == 0 && d.y == 0) ? make_double2(0, 0) : cdiv(v, d);
+      B[k + (size_t)c * ldb] = v;
+    }
+  }
+  __syncthreads();
 }
 
 // Collision matrix (src/rmatrix_hp.F90:348-368): Z_O U = Z_I with
@@ -706,89 +810,41 @@ __global__ void __launch_bounds__(1024) umatrix_kernel(const double2* __restrict
     zi[idx] = b;
   }
   __syncthreads();
-  __shared__ int s_p;
-  __shared__ double s_v[32];
-  __shared__ int s_i[32];
-  for (int k = 0; k < no; ++k) {
-    double bv = -1.0;
-    int bi = 0x7fffffff;
-    for (int r = k + tid; r < no; r += NT) {
-      double v = fabs(zo[r + (size_t)k * no].x) + fabs(zo[r + (size_t)k * no].y);
-      if (v > bv) { bv = v; bi = r; }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      double ov = __shfl_down_sync(0xffffffffu, bv, o);
-      int oi = __shfl_down_sync(0xffffffffu, bi, o);
-      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
-    }
-    if ((tid & 31) == 0) { s_v[tid >> 5] = bv; s_i[tid >> 5] = bi; }
-    __syncthreads();
-    if (tid < 32) {
-      bv = (tid < NT / 32) ? s_v[tid] : -1.0;
-      bi = (tid < NT / 32) ? s_i[tid] : 0x7fffffff;
-      for (int o = 16; o > 0; o >>= 1) {
-        double ov = __shfl_down_sync(0xffffffffu, bv, o);
-        int oi = __shfl_down_sync(0xffffffffu, bi, o);
-        if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
-      }
-      if (tid == 0) {
-        s_p = bi;
-        if (bv == 0.0 && *info == 0) *info = k + 1;
-      }
-    }
-    __syncthreads();
-    const int p = s_p;
-    if (p != k) {
-      for (int c = tid; c < no; c += NT) {
-        double2 t = zo[k + (size_t)c * no];
-        zo[k + (size_t)c * no] = zo[p + (size_t)c * no];
-        zo[p + (size_t)c * no] = t;
-        t = zi[k + (size_t)c * no];
-        zi[k + (size_t)c * no] = zi[p + (size_t)c * no];
-        zi[p + (size_t)c * no] = t;
-      }
-    }
-    __syncthreads();
-    double2 piv = zo[k + (size_t)k * no];
-    double2 inv = (piv.x == 0 && piv.y == 0) ? make_double2(0, 0) : crecip(piv);
-    for (int r = k + 1 + tid; r < no; r += NT) zo[r + (size_t)k * no] = cmul(zo[r + (size_t)k * no], inv);
-    __syncthreads();
-    const int nrow = no - k - 1;
-    const int ncz = no - k - 1;  // columns k+1.. of zo
-    const int total = nrow * (ncz + no);
-    for (int idx = tid; idx < total; idx += NT) {
-      int r = k + 1 + idx % nrow;
-      int c = idx / nrow;
-      double2 l = zo[r + (size_t)k * no];
-      if (c < ncz) {
-        int cc = k + 1 + c;
-        double2 v = zo[r + (size_t)cc * no];
-        cfms(v, l, zo[k + (size_t)cc * no]);
-        zo[r + (size_t)cc * no] = v;
-      } else {
-        int cc = c - ncz;
-        double2 v = zi[r + (size_t)cc * no];
-        cfms(v, l, zi[k + (size_t)cc * no]);
-        zi[r + (size_t)cc * no] = v;
-      }
-    }
-    __syncthreads();
-  }
-  // back substitution, columns of zi in parallel
-  for (int c = tid; c < no; c += NT) {
-    for (int k = no - 1; k >= 0; --k) {
-      double2 v = zi[k + (size_t)c * no];
-      for (int q = k + 1; q < no; ++q) cfms(v, zo[k + (size_t)q * no], zi[q + (size_t)c * no]);
-      double2 d = zo[k + (size_t)k * no];
-      v = (d.x == 0 && d.y == 0) ? make_double2(0, 0) : cdiv(v, d);
-      zi[k + (size_t)c * no] = v;
-    }
-  }
-  __syncthreads();
+  cta_gauss_solve(zo, no, zi, no, no, info);
   for (int idx = tid; idx < no * no; idx += NT) {
     int m1 = idx % no, m2 = idx / no;
     cu[m1 + (size_t)m2 * ndim] = zi[idx];
   }
 }
+
+// One step of the R-matrix propagation (src/rmatrix_hp.F90:337-345): with R00, R01, R11 the
+// q1/q2 projections of interval is (nch x nch, ld nch) and rp the propagated R of the
+// intervals before it,
+//   rp <- (R11 - R01^T (R00 + rmax1 rp)^-1 R01) / rmax2      (plain transpose)
+// The reference inverts R00 + rmax1 rp explicitly; here it is solved for R01.  One CTA;
+// work arrays cz, z (nch^2).
+__global__ void __launch_bounds__(1024) propagate_kernel(const double2* __restrict__ R00,
+                                                         const double2* __restrict__ R01,
+                                                         const double2* __restrict__ R11, double2* rp, int nch,
+                                                         double rmax1, double rmax2, double2* cz, double2* z,
+                                                         int* info) {
+  const int tid = threadIdx.x, NT = blockDim.x;
+  const int nn = nch * nch;
+  for (int idx = tid; idx < nn; idx += NT) {
+    const double2 a = R00[idx], b = rp[idx];
+    cz[idx] = make_double2(a.x + rmax1 * b.x, a.y + rmax1 * b.y);
+    z[idx] = R01[idx];
+  }
+  __syncthreads();
+  cta_gauss_solve(cz, nch, z, nch, nch, info);
+  const double inv = 1.0 / rmax2;
+  for (int idx = tid; idx < nn; idx += NT) {
+    const int i = idx % nch, j = idx / nch;
+    double2 v = R11[idx];
+    for (int k = 0; k < nch; ++k) cfms(v, R01[k + (size_t)i * nch], z[k + (size_t)j * nch]);
+    rp[idx] = make_double2(v.x * inv, v.y * inv);
+  }
+}
+
 
 }  // namespace hprmat

@@ -102,8 +102,10 @@ struct hprmat_b200_ctx {
   // mesh (rmat_ini)
   int nr = 0, ns = 0;
   double rmax = 0.0;
-  std::vector<double> xle, wle, tc, blo0, q2, zrma;
-  DevBuf mesh;  // tc | blo0 | r | q2
+  // per interval is (nr values or nr x nr matrices each, interval-major): kinetic + Bloch tc,
+  // closed-channel Bloch matrix blo0 (MeshDev), outer and inner boundary values q2, q1
+  std::vector<double> xle, wle, tc, blo0, q2, q1, zrma;
+  DevBuf mesh;  // tc | blo0 | r | q2 | q1, each ns intervals
   // work buffers
   DevBuf W, A64, X, X64, R64, B64, V, Z, gm, swaps, ipiv, stage, status, ops, inv, chan, rmat,
       zwork, cpot, cu, norms, lup, rop, rsurf, vt, rlo, linv;
@@ -197,73 +199,126 @@ static void legzo(int n, std::vector<double>& x, std::vector<double>& w) {
   }
 }
 
-// Kinetic + Bloch matrix, Bloch matrix and surface values of the first interval:
-// src/rmatrix_hp.F90:85-151 (is = 1), scaled as at :146-151.
+// Kinetic + Bloch matrices, Bloch matrices and boundary values of every interval:
+// src/rmatrix_hp.F90:85-151, scaled as at :146-151.  The closed-channel Bloch term of interval
+// is (:268-276) is stored as one matrix times rmax0 so that the per-channel factor xc / rmax0
+// is the same in every interval: blo0 (is = 1), blo2 / is - blo1 / (is - 1) (is > 1).
+static void build_mesh_host(int nr, int ns, double rmax, std::vector<double>& xle, std::vector<double>& wle,
+                            std::vector<double>& tc, std::vector<double>& blo, std::vector<double>& q2,
+                            std::vector<double>& q1, std::vector<double>& zrma) {
+  legzo(nr, xle, wle);
+  const double rmax0 = rmax / ns;
+  const size_t nn = (size_t)nr * nr;
+  tc.assign(nn * ns, 0.0);
+  blo.assign(nn * ns, 0.0);
+  q2.assign((size_t)nr * ns, 0.0);
+  q1.assign((size_t)nr * ns, 0.0);
+  const double nn1 = (double)nr * (nr + 1);
+  for (int is = 1; is <= ns; ++is) {
+    double* t = tc.data() + (is - 1) * nn;
+    double* b = blo.data() + (is - 1) * nn;
+    for (int i1 = 1; i1 <= nr; ++i1) {
+      const double xi = xle[i1 - 1], xi2 = xi * (1 - xi);
+      double td, bd;
+      if (is == 1) {
+        td = (4 * nn1 + 3 + (1 - 6 * xi) / xi2) / (3 * xi2);
+        bd = 1 / xi2;
+      } else {
+        const double xlb = xi / (1 - xi) * (nn1 - 1 / (1 - xi));
+        const double xla = (1 - xi) / xi * (-nn1 + 1 / xi);
+        td = (nn1 + 6 - 2 / xi2) / (3 * xi2) + xlb - xla;
+        bd = xi / (1 - xi) / is - (1 - xi) / xi / (is - 1);
+      }
+      t[(i1 - 1) + (size_t)(i1 - 1) * nr] = td;
+      b[(i1 - 1) + (size_t)(i1 - 1) * nr] = bd;
+      for (int i2 = 1; i2 <= i1 - 1; ++i2) {
+        const double xj = xle[i2 - 1], xj2 = xj * (1 - xj);
+        double to, bo;
+        if (is == 1) {
+          const double d = xi - xj;
+          to = (nn1 + 1 + (xi + xj - 2 * xi * xj) / (d * d) - 1 / (1 - xi) - 1 / (1 - xj)) / sqrt(xi2 * xj2);
+          bo = 1 / sqrt(xi2 * xj2);
+        } else {
+          const double d = xj - xi;
+          const double yy = sqrt(xj2 / (xi2 * xi2 * xi2)) * (2 * xi * xj + 3 * xi - xj - 4 * xi * xi) / (d * d);
+          const double b2 = sqrt(xi * xj / (1 - xi) / (1 - xj));
+          const double b1 = sqrt((1 - xi) * (1 - xj) / xi / xj);
+          to = yy + b2 * (nn1 - 1 / (1 - xj)) - b1 * (-nn1 + 1 / xj);
+          bo = b2 / is - b1 / (is - 1);
+        }
+        if ((i1 + i2) % 2 == 1) {
+          to = -to;
+          // the reference negates blo0 in the loop over every interval (:119-124), so the
+          // first interval's matrix ends up negated ns times
+          if (is > 1 || ns % 2 == 1) bo = -bo;
+        }
+        t[(i1 - 1) + (size_t)(i2 - 1) * nr] = to;
+        t[(i2 - 1) + (size_t)(i1 - 1) * nr] = to;
+        b[(i1 - 1) + (size_t)(i2 - 1) * nr] = bo;
+        b[(i2 - 1) + (size_t)(i1 - 1) * nr] = bo;
+      }
+    }
+    for (int i = 0; i < nr; ++i) {
+      const double x = xle[i];
+      double v2, v1;
+      if (is == 1) {
+        v2 = 1 / sqrt(x * (1 - x));
+        v1 = 0.0;
+      } else {
+        v2 = sqrt(x / (1 - x));
+        v1 = -1 / v2;
+      }
+      if (nr % 2 == 1) v2 = -v2;
+      if (i % 2 == 0) {  // q(1:nr:2) = -q(1:nr:2)
+        v2 = -v2;
+        v1 = -v1;
+      }
+      q2[(size_t)(is - 1) * nr + i] = v2 / sqrt(rmax0);
+      q1[(size_t)(is - 1) * nr + i] = v1 / sqrt(rmax0);
+    }
+  }
+  for (auto& v : tc) v = v / (rmax0 * rmax0);
+  for (auto& v : blo) v = v / rmax0;
+  zrma.resize((size_t)nr * ns);
+  for (int is = 0; is < ns; ++is)
+    for (int i = 0; i < nr; ++i) zrma[(size_t)is * nr + i] = (is + xle[i]) * rmax0;
+}
+
 static void build_mesh(hprmat_b200_ctx* c, int nr, int ns, double rmax) {
   c->nr = nr;
   c->ns = ns;
   c->rmax = rmax;
-  legzo(nr, c->xle, c->wle);
-  const double rmax0 = rmax / ns;
-  c->tc.assign((size_t)nr * nr, 0.0);
-  c->blo0.assign((size_t)nr * nr, 0.0);
-  c->q2.assign(nr, 0.0);
-  for (int i1 = 1; i1 <= nr; ++i1) {
-    double xi = c->xle[i1 - 1], xi2 = xi * (1 - xi);
-    double xx = 4.0 * nr * (nr + 1) + 3 + (1 - 6 * xi) / xi2;
-    c->tc[(i1 - 1) + (size_t)(i1 - 1) * nr] = xx / (3 * xi2);
-    c->blo0[(i1 - 1) + (size_t)(i1 - 1) * nr] = 1 / xi2;
-    for (int i2 = 1; i2 <= i1 - 1; ++i2) {
-      double xj = c->xle[i2 - 1], xj2 = xj * (1 - xj);
-      double d = xi - xj;
-      double t = (double)nr * (nr + 1) + 1 + (xi + xj - 2 * xi * xj) / (d * d) - 1 / (1 - xi) - 1 / (1 - xj);
-      t = t / sqrt(xi2 * xj2);
-      double b = 1 / sqrt(xi2 * xj2);
-      if ((i1 + i2) % 2 == 1) {
-        t = -t;
-        b = -b;
-      }
-      c->tc[(i1 - 1) + (size_t)(i2 - 1) * nr] = t;
-      c->tc[(i2 - 1) + (size_t)(i1 - 1) * nr] = t;
-      c->blo0[(i1 - 1) + (size_t)(i2 - 1) * nr] = b;
-      c->blo0[(i2 - 1) + (size_t)(i1 - 1) * nr] = b;
-    }
-  }
-  for (int i = 0; i < nr; ++i) {
-    double q = 1 / sqrt(c->xle[i] * (1 - c->xle[i]));
-    if (nr % 2 == 1) q = -q;
-    if (i % 2 == 0) q = -q;  // q2(1:nr:2) = -q2(1:nr:2)
-    c->q2[i] = q / sqrt(rmax0);
-  }
-  for (auto& v : c->tc) v = v / (rmax0 * rmax0);
-  for (auto& v : c->blo0) v = v / rmax0;
-  c->zrma.resize((size_t)nr * ns);
-  for (int is = 0; is < ns; ++is)
-    for (int i = 0; i < nr; ++i) c->zrma[(size_t)is * nr + i] = (is + c->xle[i]) * rmax0;
+  build_mesh_host(nr, ns, rmax, c->xle, c->wle, c->tc, c->blo0, c->q2, c->q1, c->zrma);
 }
 
 static int upload_mesh(hprmat_b200_ctx* c) {
-  const int nr = c->nr;
-  size_t n = (size_t)2 * nr * nr + 2 * nr;
+  const size_t nn = (size_t)c->nr * c->nr, nv = (size_t)c->nr * c->ns;
+  const size_t n = 2 * nn * c->ns + 3 * nv;
   TRY(c->mesh.ensure(n * sizeof(double)));
   std::vector<double> h(n);
-  std::copy(c->tc.begin(), c->tc.end(), h.begin());
-  std::copy(c->blo0.begin(), c->blo0.end(), h.begin() + (size_t)nr * nr);
-  for (int i = 0; i < nr; ++i) h[(size_t)2 * nr * nr + i] = c->zrma[i];
-  for (int i = 0; i < nr; ++i) h[(size_t)2 * nr * nr + nr + i] = c->q2[i];
+  double* p = h.data();
+  p = std::copy(c->tc.begin(), c->tc.end(), p);
+  p = std::copy(c->blo0.begin(), c->blo0.end(), p);
+  p = std::copy(c->zrma.begin(), c->zrma.end(), p);
+  p = std::copy(c->q2.begin(), c->q2.end(), p);
+  std::copy(c->q1.begin(), c->q1.end(), p);
   HPR_CUDA_TRY(cudaMemcpyAsync(c->mesh.p, h.data(), n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
   return HPRMAT_B200_OK;
 }
 
-static MeshDev mesh_dev(const hprmat_b200_ctx* c) {
+// Device view of interval is (0-based); nq1 leading right-hand sides blockdiag(q1).
+static MeshDev mesh_dev(const hprmat_b200_ctx* c, int is = 0, int nq1 = 0) {
   const double* base = c->mesh.as<double>();
+  const size_t nn = (size_t)c->nr * c->nr, nv = (size_t)c->nr * c->ns;
   MeshDev m;
   m.nr = c->nr;
-  m.tc = base;
-  m.blo0 = base + (size_t)c->nr * c->nr;
-  m.r = base + (size_t)2 * c->nr * c->nr;
-  m.q2 = base + (size_t)2 * c->nr * c->nr + c->nr;
+  m.nq1 = nq1;
+  m.tc = base + is * nn;
+  m.blo0 = base + c->ns * nn + is * nn;
+  m.r = base + 2 * c->ns * nn + (size_t)is * c->nr;
+  m.q2 = base + 2 * c->ns * nn + nv + (size_t)is * c->nr;
+  m.q1 = nq1 > 0 ? base + 2 * c->ns * nn + 2 * nv + (size_t)is * c->nr : nullptr;
   return m;
 }
 
@@ -772,6 +827,7 @@ struct Operator {
   int N = 0;
   // R-matrix problems: surface projection R = q2^T X per channel block, for the stopping rule
   const double* q2 = nullptr;
+  const double* q1 = nullptr;  // propagated intervals: leading blockdiag(q1) right-hand sides
   int nr = 0;
 };
 
@@ -889,7 +945,9 @@ static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W3
   int inner_total = 0;
   const bool surf = op.q2 != nullptr;
   const int nchs = surf ? N / op.nr : 0;
-  if (surf) TRY(c->rsurf.ensure((size_t)2 * nchs * nchs * sizeof(double2) + 64));
+  // monitored surface projections: q2^T X, and q1^T X on a propagated interval
+  const size_t nsurf = (size_t)nchs * nrhs * (op.q1 ? 2 : 1);
+  if (surf) TRY(c->rsurf.ensure(2 * nsurf * sizeof(double2) + 64));
   (void)cnorm;
   if (stats) stats->surface_change = -1.0;
   for (int outer = 0;; ++outer) {
@@ -900,13 +958,19 @@ static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W3
     double change = -1.0;
     if (surf) {
       // R of the current iterate into slot (outer & 1); compare with the previous one
-      double2* Rn = c->rsurf.as<double2>() + (size_t)(outer & 1) * nchs * nchs;
-      rmat_extract_kernel<<<dim3(nchs, cdiv_u(nchs, 128)), 128, 0, c->stream>>>(X64, ldx, op.q2, op.nr, nchs, 1.0, Rn);
+      double2* Rn = c->rsurf.as<double2>() + (size_t)(outer & 1) * nsurf;
+      const dim3 ge(nchs, cdiv_u(nrhs, 128));
+      rmat_extract_kernel<<<ge, 128, 0, c->stream>>>(X64, ldx, op.q2, op.nr, nchs, nrhs, 1.0, Rn);
       LAUNCH_CHECK();
+      if (op.q1) {
+        rmat_extract_kernel<<<ge, 128, 0, c->stream>>>(X64, ldx, op.q1, op.nr, nchs, nrhs, 1.0,
+                                                       Rn + (size_t)nchs * nrhs);
+        LAUNCH_CHECK();
+      }
       if (outer > 0) {
-        const double2* Ro = c->rsurf.as<double2>() + (size_t)((outer - 1) & 1) * nchs * nchs;
+        const double2* Ro = c->rsurf.as<double2>() + (size_t)((outer - 1) & 1) * nsurf;
         TRY(c->norms.ensure(2 * sizeof(double) * 2));
-        rel_change_kernel<<<1, 256, 0, c->stream>>>(Rn, Ro, nchs * nchs, c->norms.as<double>());
+        rel_change_kernel<<<1, 256, 0, c->stream>>>(Rn, Ro, (int)nsurf, c->norms.as<double>());
         LAUNCH_CHECK();
         HPR_CUDA_TRY(cudaMemcpyAsync(c->h_norms, c->norms.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1047,21 +1111,133 @@ static double ms_since(Clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
 }
 
+// One interval (0-based is) of an rmatrix call: C(E) of the interval assembled on the device
+// (src/rmatrix_hp.F90:246-293), factorised, and solved for its md.nq1 + nch surface right-hand
+// sides into X64 (ld ldx): FP64 LU and one solve, or the mixed LU with FP64 refinement.
+// d_cpot points at the interval's first mesh row.  Statistics of the interval in *stats.
+static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData& chd, const MeshDev& md,
+                          const double2* d_cpot, int ncp1, int ndim, double2* X64, long ld,
+                          hprmat_b200_stats* stats) {
+  const int nr = md.nr;
+  const int N = nch * nr;
+  const int nrhs = md.nq1 + nch;
+  const bool mixed = c->opts.precision == HPRMAT_B200_PREC_MIXED;
+  Operator op;
+  op.structured = true;
+  op.mesh = md;
+  op.ch = chd;
+  op.nch = nch;
+  op.N = N;
+  TRY(c->vt.ensure((size_t)nr * nch * nch * sizeof(double2)));
+  {
+    const long tot = (long)nr * nch * nch;
+    cpot_transpose_kernel<<<cdiv_u(tot, 256), 256, 0, c->stream>>>(d_cpot, ncp1, ndim, nr, nch, c->vt.as<double2>());
+    LAUNCH_CHECK();
+  }
+  op.vt = c->vt.as<double2>();
+  op.q2 = md.q2;
+  op.q1 = md.q1;
+  op.nr = nr;
+  // |B|_F of [blockdiag(q1) | blockdiag(q2)]
+  double qn = 0.0;
+  for (int i = 0; i < nr; ++i) {
+    const double v2 = c->q2[(size_t)is * nr + i], v1 = c->q1[(size_t)is * nr + i];
+    qn += v2 * v2 + (md.nq1 > 0 ? v1 * v1 : 0.0);
+  }
+  const double bnorm = sqrt(qn * nch);
+  LUState st;
+  int status = HPRMAT_B200_OK;
+  dim3 ga(cdiv_u(N, 256), std::min(N, 512));  // assemble_kernel strides over the columns
+  dim3 gr(cdiv_u(N, 256), nrhs);
+  double* d_fro2 = reinterpret_cast<double*>(c->status.as<int>() + 32);
+  HPR_CUDA_TRY(cudaMemsetAsync(d_fro2, 0, sizeof(double), c->stream));
+  if (!mixed) {
+    TRY(c->W.ensure((size_t)ld * N * sizeof(double2)));
+    double2* W = c->W.as<double2>();
+    assemble_kernel<double2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2);
+    LAUNCH_CHECK();
+    surface_rhs_kernel<double2><<<gr, 256, 0, c->stream>>>(md, X64, ld, N, 1.0);
+    LAUNCH_CHECK();
+    int nb = pick_nb(c, N, sizeof(double2), 64);
+    if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
+    auto t1 = Clock::now();
+    TRY(factor<double2>(c, W, ld, N, false, nb, st));
+    c->f64_N = st.N;
+    c->f64_ld = st.ld;
+    c->f64_nb = st.nb;
+    c->f64_nsteps = st.nsteps;
+    stats->ms_factor = ms_since(t1);
+    auto t2 = Clock::now();
+    TRY(lu_solve<double2>(c, W, st, X64, ld, nrhs));
+    TRY(c->R64.ensure((size_t)ld * nrhs * sizeof(double2)));
+    TRY(apply_residual(c, op, X64, ld, nrhs, c->R64.as<double2>(), ld, true));
+    double rn;
+    TRY(frob_norm(c, c->R64.as<double2>(), ld, N, nrhs, &rn));
+    stats->surface_change = -1.0;
+    stats->rel_residual = rn / bnorm;
+    stats->residual_history[0] = rn / bnorm;
+    stats->ms_solve = ms_since(t2);
+  } else {
+    TRY(c->W.ensure((size_t)ld * N * sizeof(float2)));
+    float2* W = c->W.as<float2>();
+    assemble_kernel<float2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2);
+    LAUNCH_CHECK();
+    int nb = pick_nb(c, N, sizeof(float2), 128);
+    if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
+    auto t1 = Clock::now();
+    TRY(factor<float2>(c, W, ld, N, true, nb, st));
+    stats->ms_factor = ms_since(t1);
+    auto t2 = Clock::now();
+    TRY(c->X.ensure((size_t)ld * nrhs * sizeof(float2)));
+    float2* X32 = c->X.as<float2>();
+    surface_rhs_kernel<float2><<<gr, 256, 0, c->stream>>>(md, X32, ld, N, 1.0);
+    LAUNCH_CHECK();
+    if (c->zero_start) {
+      HPR_CUDA_TRY(cudaMemsetAsync(X64, 0, (size_t)ld * nrhs * sizeof(double2), c->stream));
+    } else {
+      TRY(lu_solve_tc(c, st, X32, ld, nrhs));
+      f2d_kernel<<<gr, 256, 0, c->stream>>>(X32, ld, X64, ld, N, nullptr);
+      LAUNCH_CHECK();
+    }
+    stats->ms_solve = ms_since(t2);
+    auto t3 = Clock::now();
+    double cn2;
+    HPR_CUDA_TRY(cudaMemcpyAsync(&cn2, d_fro2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    status = refine_mixed(c, op, W, st, X64, ld, nrhs, bnorm, sqrt(cn2), stats);
+    if (status != HPRMAT_B200_OK && status != HPRMAT_B200_NOT_CONVERGED) return status;
+    stats->ms_refine = ms_since(t3);
+  }
+  stats->nb = st.nb;
+  if (c->h_status[SW_INFO] != 0) {
+    stats->info = c->h_status[SW_INFO];
+    return fail(HPRMAT_B200_SINGULAR, "C(E) of interval %d is singular: zero pivot in column %d", is + 1,
+                c->h_status[SW_INFO]);
+  }
+  return status;
+}
+
+// rmatrix (src/rmatrix_hp.F90:175-368) on the device.  One interval: R = q2^T C^-1 q2 / a.
+// ns > 1 intervals (R-matrix propagation, :326-345 and :590-632): interval 1 gives
+// R11 / rmax0; every later interval is solved for [blockdiag(q1) | blockdiag(q2)] on the same
+// factors (the reference's second FP64 solve with 2 nch right-hand sides, done here at the
+// context's precision with the same refinement) and its projections R00 = q1^T X_1,
+// R01 = q1^T X_2, R11 = q2^T X_2 update the propagated R (propagate_kernel).
 static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const double* qk, const double* eta,
                         double rmax, int nr, int ns, const double2* d_cpot, int ncp1, int ndim, double2* d_cu,
                         int* nopen, hprmat_b200_stats* stats) {
   auto t_all = Clock::now();
-  if (nch <= 0 || nr <= 0 || !lval || !qk || !eta || !d_cpot || !d_cu || !nopen)
+  if (nch <= 0 || nr <= 0 || ns <= 0 || !lval || !qk || !eta || !d_cpot || !d_cu || !nopen)
     return fail(HPRMAT_B200_ERR_ARG, "rmatrix: invalid arguments");
-  if (ns != 1) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "rmatrix: only ns = 1 (one interval) is supported");
   if (ndim < nch || ncp1 < nr * ns) return fail(HPRMAT_B200_ERR_ARG, "rmatrix: ndim < nch or ncp1 < nr*ns");
   if (c->nr != nr || c->ns != ns || c->rmax != rmax)
     return fail(HPRMAT_B200_ERR_ARG, "rmatrix: call rmat_ini(nr=%d, ns=%d, rmax=%g) first", nr, ns, rmax);
   const long Nl = (long)nch * nr;
   if (Nl > 200000) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "rmatrix: N = %ld too large", Nl);
   const int N = (int)Nl;
+  const double rmax0 = rmax / ns;
   Boundary bnd;
-  TRY(boundary_values(nch, lval, qk, eta, rmax, rmax / ns, bnd));
+  TRY(boundary_values(nch, lval, qk, eta, rmax, rmax0, bnd));
   *nopen = bnd.nopen;
   // channel data: fac | kk | bloch | qk (doubles), then co | cop (double2), then open_idx
   const size_t nd = 4 * (size_t)nch;
@@ -1087,120 +1263,82 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
   const double2* d_cop = d_co + std::max(1, bnd.nopen);
   const int* d_open = reinterpret_cast<const int*>(d_cop + std::max(1, bnd.nopen));
 
-  const MeshDev md = mesh_dev(c);
   const long ld = (N + 3) / 4 * 4;
-  const bool mixed = c->opts.precision == HPRMAT_B200_PREC_MIXED;
+  const int nrhs_max = ns > 1 ? 2 * nch : nch;
   if (stats) {
     memset(stats, 0, sizeof(*stats));
     stats->n = N;
-    stats->nrhs = nch;
+    stats->nrhs = nrhs_max;
     stats->rel_residual = -1.0;
+    stats->surface_change = -1.0;
   }
-  TRY(c->X64.ensure((size_t)ld * nch * sizeof(double2)));
+  TRY(c->X64.ensure((size_t)ld * nrhs_max * sizeof(double2)));
   double2* X64 = c->X64.as<double2>();
-  Operator op;
-  op.structured = true;
-  op.mesh = md;
-  op.ch = chd;
-  op.nch = nch;
-  op.N = N;
-  TRY(c->vt.ensure((size_t)nr * nch * nch * sizeof(double2)));
-  {
-    const long tot = (long)nr * nch * nch;
-    cpot_transpose_kernel<<<cdiv_u(tot, 256), 256, 0, c->stream>>>(d_cpot, ncp1, ndim, nr, nch, c->vt.as<double2>());
-    LAUNCH_CHECK();
-  }
-  op.vt = c->vt.as<double2>();
-  op.q2 = md.q2;
-  op.nr = nr;
-  // |B|_F of blockdiag(q2)
-  double q2n = 0.0;
-  for (int i = 0; i < nr; ++i) q2n += c->q2[i] * c->q2[i];
-  const double bnorm = sqrt(q2n * nch);
-  LUState st;
-  int status = HPRMAT_B200_OK;
-  dim3 ga(cdiv_u(N, 256), std::min(N, 512));  // assemble_kernel strides over the columns
-  dim3 gr(cdiv_u(N, 256), nch);
-  double* d_fro2 = reinterpret_cast<double*>(c->status.as<int>() + 32);
-  HPR_CUDA_TRY(cudaMemsetAsync(d_fro2, 0, sizeof(double), c->stream));
-  auto t0 = Clock::now();
-  if (!mixed) {
-    TRY(c->W.ensure((size_t)ld * N * sizeof(double2)));
-    double2* W = c->W.as<double2>();
-    assemble_kernel<double2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2);
-    LAUNCH_CHECK();
-    surface_rhs_kernel<double2><<<gr, 256, 0, c->stream>>>(md.q2, nr, nch, X64, ld, N, 1.0);
-    LAUNCH_CHECK();
-    int nb = pick_nb(c, N, sizeof(double2), 64);
-    if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
-    auto t1 = Clock::now();
-    TRY(factor<double2>(c, W, ld, N, false, nb, st));
-    c->f64_N = st.N;
-    c->f64_ld = st.ld;
-    c->f64_nb = st.nb;
-    c->f64_nsteps = st.nsteps;
-    if (stats) stats->ms_factor = ms_since(t1);
-    auto t2 = Clock::now();
-    TRY(lu_solve<double2>(c, W, st, X64, ld, nch));
-    TRY(c->R64.ensure((size_t)ld * nch * sizeof(double2)));
-    TRY(apply_residual(c, op, X64, ld, nch, c->R64.as<double2>(), ld, true));
-    double rn;
-    TRY(frob_norm(c, c->R64.as<double2>(), ld, N, nch, &rn));
-    if (stats) {
-      stats->surface_change = -1.0;
-      stats->rel_residual = rn / bnorm;
-      stats->residual_history[0] = rn / bnorm;
-      stats->ms_solve = ms_since(t2);
-    }
-  } else {
-    TRY(c->W.ensure((size_t)ld * N * sizeof(float2)));
-    float2* W = c->W.as<float2>();
-    assemble_kernel<float2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2);
-    LAUNCH_CHECK();
-    int nb = pick_nb(c, N, sizeof(float2), 128);
-    if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
-    auto t1 = Clock::now();
-    TRY(factor<float2>(c, W, ld, N, true, nb, st));
-    if (stats) stats->ms_factor = ms_since(t1);
-    auto t2 = Clock::now();
-    TRY(c->X.ensure((size_t)ld * nch * sizeof(float2)));
-    float2* X32 = c->X.as<float2>();
-    surface_rhs_kernel<float2><<<gr, 256, 0, c->stream>>>(md.q2, nr, nch, X32, ld, N, 1.0);
-    LAUNCH_CHECK();
-    if (c->zero_start) {
-      HPR_CUDA_TRY(cudaMemsetAsync(X64, 0, (size_t)ld * nch * sizeof(double2), c->stream));
-    } else {
-      TRY(lu_solve_tc(c, st, X32, ld, nch));
-      f2d_kernel<<<gr, 256, 0, c->stream>>>(X32, ld, X64, ld, N, nullptr);
-      LAUNCH_CHECK();
-    }
-    if (stats) stats->ms_solve = ms_since(t2);
-    auto t3 = Clock::now();
-    double cn2;
-    HPR_CUDA_TRY(cudaMemcpyAsync(&cn2, d_fro2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    status = refine_mixed(c, op, W, st, X64, ld, nch, bnorm, sqrt(cn2), stats);
-    if (status != HPRMAT_B200_OK && status != HPRMAT_B200_NOT_CONVERGED) return status;
-    if (stats) stats->ms_refine = ms_since(t3);
-  }
-  if (stats) stats->nb = st.nb;
-  if (c->h_status[SW_INFO] != 0) {
-    if (stats) stats->info = c->h_status[SW_INFO];
-    return fail(HPRMAT_B200_SINGULAR, "C(E) is singular: zero pivot in column %d", c->h_status[SW_INFO]);
-  }
-  // R and U
-  auto t4 = Clock::now();
   const int no = bnd.nopen;
-  TRY(c->rmat.ensure((size_t)nch * nch * sizeof(double2) + 64));
-  TRY(c->zwork.ensure((size_t)2 * std::max(1, no * no) * sizeof(double2) + 64));
+  const size_t nn = (size_t)nch * nch;
+  // R | R01 | R11 | propagated R (nch^2 each); work: 2 max(nopen^2, nch^2)
+  TRY(c->rmat.ensure(4 * nn * sizeof(double2) + 64));
+  TRY(c->zwork.ensure((size_t)2 * std::max<size_t>(1, std::max<size_t>((size_t)no * no, ns > 1 ? nn : 0)) *
+                          sizeof(double2) + 64));
   double2* R = c->rmat.as<double2>();
-  rmat_extract_kernel<<<dim3(nch, cdiv_u(nch, 128)), 128, 0, c->stream>>>(X64, ld, md.q2, nr, nch, 1.0 / (rmax / ns), R);
-  LAUNCH_CHECK();
-  int* d_info = c->status.as<int>() + SW_INFO;
-  HPR_CUDA_TRY(cudaMemsetAsync(d_info, 0, sizeof(int), c->stream));
+  double2* R01 = R + nn;
+  double2* R11 = R + 2 * nn;
+  double2* rp = R + 3 * nn;
   double2* zo = c->zwork.as<double2>();
-  umatrix_kernel<<<1, 1024, 0, c->stream>>>(R, nch, d_open, d_qk, d_co, d_cop, no, zo, zo + std::max(1, no * no), d_cu,
-                                            ndim, d_info);
+  int* d_info = c->status.as<int>() + SW_INFO;
+  int status = HPRMAT_B200_OK;
+  for (int is = 0; is < ns; ++is) {
+    const MeshDev md = mesh_dev(c, is, is > 0 ? nch : 0);
+    hprmat_b200_stats si;
+    memset(&si, 0, sizeof(si));
+    si.rel_residual = -1.0;
+    si.surface_change = -1.0;
+    const int s = interval_solve(c, is, nch, chd, md, d_cpot + (size_t)is * nr, ncp1, ndim, X64, ld, &si);
+    if (stats) {
+      stats->info = si.info;
+      stats->nb = si.nb;
+      stats->refine_steps += si.refine_steps;
+      stats->inner_iterations += si.inner_iterations;
+      stats->ms_factor += si.ms_factor;
+      stats->ms_solve += si.ms_solve;
+      stats->ms_refine += si.ms_refine;
+      if (si.rel_residual > stats->rel_residual) {  // the worst interval's refinement record
+        stats->rel_residual = si.rel_residual;
+        stats->surface_change = si.surface_change;
+        stats->residual_floor = si.residual_floor;
+        memcpy(stats->residual_history, si.residual_history, sizeof(si.residual_history));
+        memcpy(stats->floor_history, si.floor_history, sizeof(si.floor_history));
+      }
+    }
+    if (s != HPRMAT_B200_OK && s != HPRMAT_B200_NOT_CONVERGED) return s;
+    if (s == HPRMAT_B200_NOT_CONVERGED) status = s;
+    const dim3 ge(nch, cdiv_u(nch, 128));
+    if (is == 0) {
+      // ns = 1: R / a;  ns > 1: the first interval's R11 / rmax2 (rmax2 = rmax0)
+      rmat_extract_kernel<<<ge, 128, 0, c->stream>>>(X64, ld, md.q2, nr, nch, nch, 1.0 / rmax0, ns > 1 ? rp : R);
+      LAUNCH_CHECK();
+      continue;
+    }
+    rmat_extract_kernel<<<ge, 128, 0, c->stream>>>(X64, ld, md.q1, nr, nch, nch, 1.0, R);  // R00
+    LAUNCH_CHECK();
+    rmat_extract_kernel<<<ge, 128, 0, c->stream>>>(X64 + (size_t)nch * ld, ld, md.q1, nr, nch, nch, 1.0, R01);
+    LAUNCH_CHECK();
+    rmat_extract_kernel<<<ge, 128, 0, c->stream>>>(X64 + (size_t)nch * ld, ld, md.q2, nr, nch, nch, 1.0, R11);
+    LAUNCH_CHECK();
+    HPR_CUDA_TRY(cudaMemsetAsync(d_info, 0, sizeof(int), c->stream));
+    propagate_kernel<<<1, 1024, 0, c->stream>>>(R, R01, R11, rp, nch, is * rmax0, (is + 1) * rmax0, zo, zo + nn,
+                                                d_info);
+    LAUNCH_CHECK();
+    HPR_CUDA_TRY(cudaMemcpyAsync(c->h_status, c->status.p, SW_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (c->h_status[SW_INFO] != 0)
+      return fail(HPRMAT_B200_SINGULAR, "singular R00 + rmax1 R in the propagation to interval %d", is + 1);
+  }
+  // U
+  auto t4 = Clock::now();
+  HPR_CUDA_TRY(cudaMemsetAsync(d_info, 0, sizeof(int), c->stream));
+  umatrix_kernel<<<1, 1024, 0, c->stream>>>(ns > 1 ? rp : R, nch, d_open, d_qk, d_co, d_cop, no, zo,
+                                            zo + std::max(1, no * no), d_cu, ndim, d_info);
   LAUNCH_CHECK();
   HPR_CUDA_TRY(cudaMemcpyAsync(c->h_status, c->status.p, SW_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1210,7 +1348,6 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
     stats->ms_total = ms_since(t_all);
     stats->status = status;
   }
-  (void)t0;
   return status;
 }
 
@@ -1643,6 +1780,7 @@ int hprmat_b200_rmatrix_adjoint(hprmat_b200_ctx* c, int nch, const int* lval, co
   TRY(check_ctx(c));
   if (!cpot || !cu || !gu || !grad || !nopen || ndim < nch || ncp1 < nr || nch <= 0)
     return fail(HPRMAT_B200_ERR_ARG, "rmatrix_adjoint: invalid arguments");
+  if (ns != 1) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "rmatrix_adjoint: one interval (ns = 1) only");
   const size_t pbytes = (size_t)ncp1 * ndim * ndim * sizeof(double2);
   const size_t ubytes = (size_t)ndim * ndim * sizeof(double2);
   TRY(c->cpot.ensure(pbytes));
@@ -1911,6 +2049,19 @@ int hprmat_b200_dev_panel_trace_read(hprmat_b200_ctx* c, long long* out, int cap
     HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
     HPR_CUDA_TRY(cudaMemcpy(out, c->ptrace.p, n * sizeof(long long), cudaMemcpyDeviceToHost));
   }
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_dev_mesh(int nr, int ns, double rmax, double* tc, double* blo, double* q2, double* q1,
+                         double* zrma) {
+  if (nr < 2 || ns < 1 || !(rmax > 0)) return fail(HPRMAT_B200_ERR_ARG, "dev_mesh: need nr >= 2, ns >= 1, rmax > 0");
+  std::vector<double> xle, wle, t, b, v2, v1, z;
+  build_mesh_host(nr, ns, rmax, xle, wle, t, b, v2, v1, z);
+  if (tc) std::copy(t.begin(), t.end(), tc);
+  if (blo) std::copy(b.begin(), b.end(), blo);
+  if (q2) std::copy(v2.begin(), v2.end(), q2);
+  if (q1) std::copy(v1.begin(), v1.end(), q1);
+  if (zrma) std::copy(z.begin(), z.end(), zrma);
   return HPRMAT_B200_OK;
 }
 

@@ -152,6 +152,19 @@ def sweep(nch: int, seed: int = 2) -> Workload:
     return production(seed=seed, nch=nch, closed_threshold=40.0, name=f"sweep{nch}")
 
 
+def with_intervals(w: Workload, ns: int) -> Workload:
+    """The same potential on ns intervals of w.nr points each over [0, w.rmax] (R-matrix
+    propagation, src/rmatrix_hp.F90:153-157 for the mesh): cpot has w.nr * ns rows."""
+    rmax0 = w.rmax / ns
+    x = lagrange_radii(w.nr, 1.0)
+    r = np.concatenate([(s + x) * rmax0 for s in range(ns)])
+    out = Workload(w.name, w.nch, w.nr, ns, w.rmax, w.energy, w.hm, w.lval, w.thresholds,
+                   w.coupling, w.params)
+    out.cpot = potential_matrix(r, w.nch, w.coupling, w.params, w.hm)
+    out.qk, out.eta = w.qk, w.eta
+    return out
+
+
 def at_energy(w: Workload, energy: float) -> Workload:
     """The same potential at another energy (only k and eta change)."""
     out = Workload(w.name, w.nch, w.nr, w.ns, w.rmax, energy, w.hm, w.lval, w.thresholds,

@@ -45,6 +45,15 @@ int hprmat_b200_dev_counters(hprmat_b200_ctx* ctx, unsigned long long* launches,
      "zero_start"     refinement from X = 0 instead of the FP32 solution (0). */
 int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* ctx, const char* key, int value);
 
+/* The Lagrange-mesh matrices the device assembly uses, computed on the host (no context, no
+   device): for every interval is (0-based, interval-major) tc[is][nr x nr] (kinetic + Bloch,
+   column-major, / rmax0^2), blo[is][nr x nr] (the closed-channel Bloch matrix times rmax0:
+   blo0 / rmax0 for the first interval, (blo2 / (is+1) - blo1 / is) / rmax0 after it), q2[is][nr],
+   q1[is][nr] and zrma[nr ns] -- src/rmatrix_hp.F90:61-159 with rmax0 = rmax / ns.  Any output
+   may be NULL. */
+int hprmat_b200_dev_mesh(int nr, int ns, double rmax, double* tc, double* blo, double* q2, double* q1,
+                         double* zrma);
+
 /* Tracing of the wavefront triangular solves of the mixed path.  With enable != 0 every
    later sweep records, per unit (block row x right-hand-side group, in dependency order),
    four device-clock stamps in ns: the producer starts the unit, the last dependency flag

@@ -98,3 +98,28 @@ def test_boundary_rejects_bad_arguments():
                                     z.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                     z.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 1.0,
                                     None, None, None, None, None) == nat.ERR_ARG
+
+
+@pytest.mark.parametrize("nr,ns,rmax", [(10, 1, 10.0), (30, 4, 16.0), (15, 3, 12.0), (40, 2, 20.0)])
+def test_mesh_matches_oracle(nr, ns, rmax):
+    """Per-interval kinetic/Bloch matrices and boundary values of the device assembly against
+    the oracle's rmat_ini (src/rmatrix_hp.F90:61-159), odd and even nr, one to four intervals."""
+    lib = nat.load()
+    tc = np.zeros(ns * nr * nr)
+    blo = np.zeros(ns * nr * nr)
+    q2 = np.zeros(ns * nr)
+    q1 = np.zeros(ns * nr)
+    zr = np.zeros(ns * nr)
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    nat.check(lib.hprmat_b200_dev_mesh(nr, ns, rmax, dp(tc), dp(blo), dp(q2), dp(q1), dp(zr)))
+    m = orc.rmat_ini(nr, ns, rmax)
+    for s in range(ns):
+        t = tc[s * nr * nr:(s + 1) * nr * nr].reshape(nr, nr, order="F")
+        b = blo[s * nr * nr:(s + 1) * nr * nr].reshape(nr, nr, order="F")
+        np.testing.assert_allclose(t, m.tc[:, :, s], rtol=1e-13, atol=1e-13 * np.abs(m.tc[:, :, s]).max())
+        # closed-channel Bloch term of interval s+1, times rmax0 (rmatrix_hp.F90:268-276)
+        ref = m.blo0 if s == 0 else (m.blo2 / ((s + 1) * m.rmax0) - m.blo1 / (s * m.rmax0)) * m.rmax0
+        np.testing.assert_allclose(b, ref, rtol=1e-13, atol=1e-13 * np.abs(ref).max())
+        np.testing.assert_allclose(q2[s * nr:(s + 1) * nr], m.q2[:, s], rtol=1e-14)
+        np.testing.assert_allclose(q1[s * nr:(s + 1) * nr], m.q1[:, s], rtol=1e-14, atol=0)
+    np.testing.assert_allclose(zr, m.zrma, rtol=1e-15)
