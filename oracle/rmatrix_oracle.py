@@ -16,6 +16,9 @@ pattern.  Reference paths are relative to the HPRMAT project root:
 * ``rmatrix``                -- ``src/rmatrix_hp.F90:175-368`` (propagation for ns > 1 at
   ``:326-345``, collision matrix at ``:348-368``)
 * ``solve_rmatrix_mixed``    -- ``src/rmat_solvers.F90:157-296`` (CGETRF + FP64 refinement)
+* ``rmatrix_wf``             -- ``src/rmatrix_hp.F90:378-431`` with C^-1 as
+  ``rmat_pierre/rmatrix.f:270-318`` (wave functions at the mesh points)
+* ``spline``/``splint``/``wf_print`` -- ``src/rmatrix_hp.F90:678-734, 786-841``
 
 Arrays follow the Fortran layout: C(E) is column-major with row index
 ``(channel-1)*nr + i``; ``cpot`` has shape ``(ncp1, ndim, ndim)`` (Fortran order,
@@ -378,6 +381,148 @@ def rmatrix(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, solver: str = "dense") -
         crma0_prev = crma0
     cu = collision_matrix(crma0_prev, bnd, qk)
     return RMatrixResult(cu, bnd.nopen, crma0_prev, bnd, x_last if ns == 1 else None)
+
+
+def rmatrix_wf(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, nvc):
+    """U and the internal wave functions (rmatrix with twf = .true., src/rmatrix_hp.F90:378-431).
+
+    ``nvc``: entrance channels, 1-based indices among the open channels.  Per interval the
+    dense solve is X = C^-1 [blockdiag(q1) | blockdiag(q2)] (ZGESV, 2 nch right-hand sides),
+    giving R00, R01, R11 and the propagated R as ``rmatrix``.  The surface amplitudes cfp of
+    the last interval follow from U (:380-386), are carried inwards with
+    (R00 + rin R)^-1 R01 (:388-394), and the wave function of interval is is
+    C_is^-1 (blockdiag(q2) cfp_is - blockdiag(q1) cfp_is-1) -- C^-1 as in Descouvemont's
+    original (rmat_pierre/rmatrix.f:286-301), where ``ch`` holds the inverse; the HPRMAT
+    version multiplies by C itself at :407.  Closed-channel amplitudes go to
+    cu[nopen + m, ic] (:414-419), and cf is divided by sqrt(rmax0 w_i) (:421-428).
+
+    Returns (cu (nch, nch) with U in [:nopen, :nopen], nopen, cf (nr ns, nch, len(nvc))).
+    """
+    lval = np.asarray(lval)
+    qk = np.asarray(qk, dtype=np.float64)
+    eta = np.asarray(eta, dtype=np.float64)
+    nr, ns, rmax0 = mesh.nr, mesh.ns, mesh.rmax0
+    n = nch * nr
+    bnd = boundary_values(nch, lval, qk, eta, rmax)
+    xs, crma, crma0 = [], [], []
+    for is_ in range(1, ns + 1):
+        s = is_ - 1
+        rmax1, rmax2 = (is_ - 1) * rmax0, is_ * rmax0
+        ch = assemble(mesh, is_, nch, lval, qk, bnd.xc, cpot)
+        q1, q2 = mesh.q1[:, s], mesh.q2[:, s]
+        rhs = np.zeros((n, 2 * nch), dtype=np.complex128, order="F")
+        for c in range(nch):
+            rhs[c * nr:(c + 1) * nr, c] = q1
+            rhs[c * nr:(c + 1) * nr, nch + c] = q2
+        x, info = _zgesv(ch, rhs)
+        if info != 0:
+            raise RuntimeError(f"singular C(E) in interval {is_}")
+        x1, x2 = x[:, :nch], x[:, nch:]
+        r00, r01, r11 = extract_r(x1, q1, nch), extract_r(x2, q1, nch), extract_r(x2, q2, nch)
+        if is_ == 1:
+            c0 = r11 / rmax2
+        else:
+            cz = r00 + crma0[-1] * rmax1
+            c0 = (r11 - r01.T @ np.linalg.solve(cz, r01)) / rmax2
+        xs.append((x1, x2))
+        crma.append((r00, r01, r11))
+        crma0.append(c0)
+    u = collision_matrix(crma0[-1], bnd, qk)
+    no = bnd.nopen
+    cu = np.zeros((nch, nch), dtype=np.complex128)
+    cu[:no, :no] = u
+    cf = np.zeros((nr * ns, nch, len(nvc)), dtype=np.complex128)
+    for ic, nvex in enumerate(nvc):
+        i2 = bnd.npo_open[nvex - 1]
+        cfp = np.zeros((nch, ns + 1), dtype=np.complex128)  # column is = 0..ns
+        for m1, i1 in enumerate(bnd.npo_open):
+            v = -u[m1, nvex - 1] * bnd.cop[m1] * math.sqrt(qk[i2] / qk[i1])
+            if i1 == i2:
+                v += np.conj(bnd.cop[m1])
+            cfp[i1, ns] = v
+        cfp[:, ns] /= rmax
+        for is_ in range(ns - 1, 0, -1):
+            cz = crma[is_][0] + is_ * rmax0 * crma0[is_ - 1]
+            cfp[:, is_] = np.linalg.solve(cz, crma[is_][1]) @ cfp[:, is_ + 1]
+        for is_ in range(1, ns + 1):
+            x1, x2 = xs[is_ - 1]
+            v = x2 @ cfp[:, is_] - x1 @ cfp[:, is_ - 1]
+            cf[(is_ - 1) * nr:is_ * nr, :, ic] = v.reshape(nch, nr).T
+        for m1, i1 in enumerate(bnd.npo_closed):
+            cy = np.sum(cf[(ns - 1) * nr:ns * nr, i1, ic] * mesh.q2[:, ns - 1])
+            cu[m1 + no, ic] = cy / bnd.xc[i1, 1]
+        for is_ in range(ns):
+            cf[is_ * nr:(is_ + 1) * nr, :, ic] /= np.sqrt(rmax0 * mesh.wle)[:, None]
+    return cu, no, cf
+
+
+def spline(x, y, ypn=None):
+    """Second derivatives of the cubic spline through (x, y) (src/rmatrix_hp.F90:787-816):
+    tridiagonal elimination.  Natural at the first point (wf_print's yp1 = 1e30); at the last
+    point natural (ypn None: wf_print's yp2 = 1e30) or with first derivative ypn."""
+    n = len(x)
+    y2 = np.zeros(n)
+    u = np.zeros(n)
+    for i in range(1, n - 1):
+        sig = (x[i] - x[i - 1]) / (x[i + 1] - x[i - 1])
+        p = sig * y2[i - 1] + 2.0
+        y2[i] = (sig - 1.0) / p
+        d = (y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1])
+        u[i] = (6.0 * d / (x[i + 1] - x[i - 1]) - sig * u[i - 1]) / p
+    if ypn is None:
+        y2[n - 1] = 0.0
+    else:
+        un = (3.0 / (x[n - 1] - x[n - 2])) * (ypn - (y[n - 1] - y[n - 2]) / (x[n - 1] - x[n - 2]))
+        y2[n - 1] = (un - 0.5 * u[n - 2]) / (0.5 * y2[n - 2] + 1.0)
+    for k in range(n - 2, -1, -1):
+        y2[k] = y2[k] * y2[k + 1] + u[k]
+    return y2
+
+
+def splint(xa, ya, y2a, x):
+    """Cubic-spline value at x (src/rmatrix_hp.F90:818-841): bisection for the bracketing
+    interval, then the cubic in the local coordinates."""
+    klo, khi = 0, len(xa) - 1
+    while khi - klo > 1:
+        k = (khi + klo) // 2
+        if xa[k] > x:
+            khi = k
+        else:
+            klo = k
+    h = xa[khi] - xa[klo]
+    a = (xa[khi] - x) / h
+    b = (x - xa[klo]) / h
+    return a * ya[klo] + b * ya[khi] + ((a ** 3 - a) * y2a[klo] + (b ** 3 - b) * y2a[khi]) * h * h / 6.0
+
+
+def wf_print(nch, lval, qk, eta, rmax, mesh: Mesh, cu, nopen, cf, iv, nom, npoin, h, ypn=None):
+    """Wave function of channel iv (1-based) for entrance nom on r = h, 2h, ..., npoin h
+    (src/rmatrix_hp.F90:678-734): the spline of the mesh values inside rmax, the Coulomb
+    (open) or Whittaker (closed) form outside.  ypn: the spline's end condition (None:
+    natural, as HPRMAT; Descouvemont's original passes an unset yp2, rmat_pierre/rmatrix.f:339,350)."""
+    qk = np.asarray(qk, dtype=np.float64)
+    zr = mesh.zrma
+    nop = sum(1 for w in range(iv) if qk[w] > 0)
+    nclo = nopen + sum(1 for w in range(iv) if qk[w] < 0)
+    xr, xi = cf[:, iv - 1, nom - 1].real.copy(), cf[:, iv - 1, nom - 1].imag.copy()
+    y2r, y2i = spline(zr, xr, ypn), spline(zr, xi, ypn)
+    out = np.zeros(npoin, dtype=np.complex128)
+    l = int(lval[iv - 1])
+    for i in range(1, npoin + 1):
+        r = i * h
+        if r <= rmax:
+            out[i - 1] = complex(splint(zr, xr, y2r, r), splint(zr, xi, y2i, r))
+        elif qk[iv - 1] > 0:
+            fc, gc, _, _, _ = coulfg(qk[iv - 1] * r, eta[iv - 1], float(l))
+            co = complex(gc, fc) * math.sqrt(qk[nom - 1] / qk[iv - 1])
+            v = -cu[nop - 1, nom - 1] * co
+            if iv == nom:
+                v += np.conj(co)
+            out[i - 1] = v
+        else:
+            f, _, _ = whit(eta[iv - 1], r, -qk[iv - 1], -qk[iv - 1] ** 2, l, 0)
+            out[i - 1] = cu[nclo - 1, nom - 1] * f[l]
+    return out
 
 
 def rmatrix_adjoint(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, gu):

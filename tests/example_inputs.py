@@ -2,7 +2,8 @@
 
 The potentials and kinematics follow examples/Ex1/example1_hp.f90:53-88,102-105
 (alpha + 208Pb), examples/Ex2/example2_hp.f90:32-73,86-88 (Reid NN, T=1) and
-examples/Ex4/example4_hp.f90:37-133 (12C + alpha, coupled channels with closed ones).
+examples/Ex4/example4_hp.f90:37-133 (12C + alpha, coupled channels with closed ones) and
+rmat_pierre/Ex3/example3.f:1-98 (16O + 44Ca, the same rotational-model couplings).
 The mesh-dependent arrays are evaluated at the abscissas `zrma` the caller passes in.
 """
 from __future__ import annotations
@@ -56,12 +57,11 @@ def ex2_setup(zrma, j):
     return cpot, kin
 
 
-def ex4_setup(zrma, j):
+def _deformed_setup(zrma, j, a1, a2, z1, z2, ispi, th, v0, w0, r0, an, lam, ben, bec):
+    """Coupled channels of a deformed Woods-Saxon + Coulomb potential (the drivers'
+    rotational-model couplings with 3j/6j coefficients)."""
     from sympy.physics.wigner import wigner_3j, wigner_6j
-    a1, a2, z1, z2 = 12, 4, 6, 2
-    ispi, th = [0, 2, 4], [0.0, 4.44, 14.08]
-    v0, w0, r0, an = 110, 20, 1.2, 0.5
-    lam, ben, bec = 2, 0.58, 0
+    ncha = len(ispi)
     pi4 = 4 * math.acos(-1.0)
     rn = r0 * (a1 ** (1.0 / 3) + a2 ** (1.0 / 3))
     rv = r0 * a1 ** (1.0 / 3)
@@ -69,7 +69,7 @@ def ex4_setup(zrma, j):
     ze = z1 * z2 * 1.44
     hm = 20.736 / rmu
     eta0 = ze / (2 * hm)
-    chans = [(n, ispi[n], l) for n in range(3) for l in range(abs(j - ispi[n]), j + ispi[n] + 1, 2)]
+    chans = [(n, ispi[n], l) for n in range(ncha) for l in range(abs(j - ispi[n]), j + ispi[n] + 1, 2)]
     nv = len(chans)
     xfac = np.zeros((nv, nv))
     for a, (n, ii, l) in enumerate(chans):
@@ -108,3 +108,13 @@ def ex4_setup(zrma, j):
         return np.array(lval, np.int32), np.array(qk), np.array(eta)
 
     return cpot, kin, nv
+
+
+def ex3_setup(zrma, j):
+    """16O + 44Ca (rmat_pierre/Ex3/example3.f:1-98): two states of 44Ca, 4 channels at J = 30."""
+    return _deformed_setup(zrma, j, 44, 16, 20, 8, [0, 2], [0.0, 1.156], 110, 20, 1.2, 0.5, 2, 0.40, 0.0)
+
+
+def ex4_setup(zrma, j):
+    """12C + alpha (examples/Ex4/example4_hp.f90:37-133): three states of 12C, closed channels."""
+    return _deformed_setup(zrma, j, 12, 4, 6, 2, [0, 2, 4], [0.0, 4.44, 14.08], 110, 20, 1.2, 0.5, 2, 0.58, 0)

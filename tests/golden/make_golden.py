@@ -6,12 +6,13 @@ Run in a container that has the HPRMAT sources mounted (read-only) at
     python tests/golden/make_golden.py [/root/reference]
 
 It reads Descouvemont's example inputs and printed outputs,
-``rmat_pierre/Ex{1,2,4}/data*`` and ``rmat_pierre/Ex{1,2,4}/output*.txt`` (the files the
-HPRMAT README compares its solvers against, README.md:113-121), and writes
-``tests/golden/reference_examples.json``.  Nothing else is transformed: the numbers are
+``rmat_pierre/Ex{1,2,3,4}/data*`` and ``rmat_pierre/Ex{1,2,3,4}/output*.txt`` (the files the
+HPRMAT README compares its solvers against, README.md:113-121), the wave functions the drivers
+write for their rmax < 0 card (``rmat_pierre/Ex{1,2,3,4}/wf*.txt``) and Ex3's wf_print output,
+and writes ``tests/golden/reference_examples.json``.  Nothing else is transformed: the numbers are
 the printed 5-significant-digit values.  The physics inputs of each example (potential
 forms, masses, charges) are restated by the tests from the example drivers
-(``examples/Ex{1,2,4}/example*_hp.f90``); only the mesh/energy cards and printed results
+(``examples/Ex{1,2,4}/example*_hp.f90``, ``rmat_pierre/Ex3/example3.f``); only the mesh/energy cards and printed results
 come from here.
 """
 from __future__ import annotations
@@ -24,8 +25,9 @@ import sys
 NUM = r"[-+]?\d+\.\d+E[-+]\d+"
 
 
-def parse_data(path):
-    """Input cards: (j, nr, ns, rmax) followed by (ne, e0, estep) lines, Ex1/2/4 layout."""
+def parse_data(path, with_print_mesh=False):
+    """Input cards: (j, nr, ns, rmax), for Ex3 then (npoin, h), followed by (ne, e0, estep)
+    lines."""
     cards = []
     with open(path) as f:
         lines = [ln.split("!")[0].split() for ln in f if ln.strip()]
@@ -36,6 +38,10 @@ def parse_data(path):
             break
         j, nr, ns, rmax = int(head[0]), int(head[1]), int(head[2]), float(head[3])
         i += 1
+        extra = {}
+        if with_print_mesh:
+            extra = {"npoin": int(lines[i][0]), "h": float(lines[i][1])}
+            i += 1
         energies = []
         while i < len(lines):
             ne, e0, es = int(lines[i][0]), float(lines[i][1]), float(lines[i][2])
@@ -43,7 +49,7 @@ def parse_data(path):
             if ne == 0:
                 break
             energies.append((ne, e0, es))
-        cards.append({"j": j, "nr": nr, "ns": ns, "rmax": rmax, "energies": energies})
+        cards.append({"j": j, "nr": nr, "ns": ns, "rmax": rmax, "energies": energies, **extra})
     return cards
 
 
@@ -72,15 +78,71 @@ def parse_output(path, key):
     return blocks
 
 
+def parse_wavefunctions(path):
+    """Blocks of the drivers' wave_functions.txt (rmat_pierre/Ex*/wf*.txt): per energy the
+    internal wave functions at the mesh points (r, then Re/Im per channel) and the external
+    ones at r = zrma(nr ns) + 0.2 i, i = 0..11."""
+    blocks = []
+    part = None
+    with open(path) as f:
+        for ln in f:
+            m = re.match(r"\s*Wave function, E=\s*([-\d.]+)\s+entrance channel=\s*(\d+)", ln)
+            if m:
+                blocks.append({"E": float(m.group(1)), "entrance": int(m.group(2)), "internal": [], "external": []})
+                continue
+            if "Internal wave functions" in ln:
+                part = "internal"
+                continue
+            if "External wave functions" in ln:
+                part = "external"
+                continue
+            vals = re.findall(NUM, ln)
+            if vals and blocks:
+                r = float(ln.split()[0])
+                blocks[-1][part].append([r] + [float(v) for v in vals])
+    return blocks
+
+
+def parse_fixed_step(path):
+    """wf_print output of Ex3 (rmat_pierre/Ex3/output3.txt): after each energy of the card that
+    asks for it, per channel the rows (r, Re, Im) on the uniform mesh."""
+    out = []
+    energy = None
+    cur = None
+    with open(path) as f:
+        for ln in f:
+            m = re.match(r"E \(MeV\)=\s*([-\d.]+)", ln)
+            if m:
+                energy = float(m.group(1))
+            if "Wave function at a fixed step size" in ln:
+                cur = {"E": energy, "channels": []}
+                out.append(cur)
+                continue
+            if re.match(r"\s*Channel\s+\d+", ln) and cur is not None:
+                cur["channels"].append([])
+                continue
+            vals = re.findall(NUM, ln)
+            if cur is not None and cur["channels"] and len(vals) == 2 and "E (MeV)" not in ln:
+                cur["channels"][-1].append([float(ln.split()[0])] + [float(v) for v in vals])
+    return out
+
+
 def main(ref):
-    out = {"source": "rmat_pierre/Ex{1,2,4}/output*.txt and data* of HPRMAT", "examples": {}}
+    out = {"source": "rmat_pierre/Ex{1,2,3,4}/output*.txt, wf*.txt and data* of HPRMAT", "examples": {}}
     spec = {
         "ex1": ("Ex1", "data1", "output1.txt", ["Collision matrix="]),
         "ex2": ("Ex2", "data2", "output2.txt", ["phase shift (rad.)="]),
+        "ex3": ("Ex3", "data3", "output3.txt", ["Amplitude=", "phase shift (rad.)="]),
         "ex4": ("Ex4", "data4", "output4.txt", ["Amplitude=", "phase shift (rad.)="]),
     }
+    out["wavefunctions"] = {}
     for name, (d, data, outp, keys) in spec.items():
-        cards = parse_data(os.path.join(ref, "rmat_pierre", d, data))
+        cards = parse_data(os.path.join(ref, "rmat_pierre", d, data), with_print_mesh=(name == "ex3"))
+        wf = os.path.join(ref, "rmat_pierre", d, "wf" + name[-1] + ".txt")
+        if os.path.exists(wf):
+            # written by the card with rmax < 0 (twf = .true. in the drivers)
+            out["wavefunctions"][name] = {"card": [i for i, c in enumerate(cards) if c["rmax"] < 0][0],
+                                          "blocks": parse_wavefunctions(wf)}
         res = {}
         for key in keys:
             res[key] = parse_output(os.path.join(ref, "rmat_pierre", d, outp), key)
@@ -88,6 +150,7 @@ def main(ref):
             for key in keys:
                 card.setdefault("printed", {})[key] = res[key][ic]["rows"]
         out["examples"][name] = cards
+    out["fixed_step"] = {"ex3": parse_fixed_step(os.path.join(ref, "rmat_pierre", "Ex3", "output3.txt"))}
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_examples.json")
     with open(dst, "w") as f:
         json.dump(out, f, indent=1)
