@@ -33,7 +33,8 @@ EXPORTED = (
     "gpu_b200_solve_mixed_", "gpu_b200_solve_double_", "gpu_b200_finalize_", "hprmat_b200_status_string",
     "hprmat_b200_last_error", "hprmat_b200_version", "hprmat_b200_boundary",
     "hprmat_b200_solve_linear_noalloc", "hprmat_b200_rmatrix_scan",
-    "hprmat_b200_rmatrix_adjoint",
+    "hprmat_b200_rmatrix_adjoint", "hprmat_b200_rmatrix_wf", "hprmat_b200_rmatrix_wf_device",
+    "hprmat_b200_wf_print",
     # include/hprmat_b200_dev.h
     "hprmat_b200_dev_tc_update", "hprmat_b200_dev_split_planes", "hprmat_b200_dev_set_profile",
     "hprmat_b200_dev_counters", "hprmat_b200_dev_wave_trace", "hprmat_b200_dev_wave_trace_read",
@@ -101,6 +102,9 @@ def load():
         "hprmat_b200_rmatrix_device": (I, [P, I, IP, DP, DP, D, I, I, P, I, I, P, IP, SP]),
         "hprmat_b200_rmatrix_scan": (I, [P, I, ctypes.POINTER(ScanBlock), D, I, I, DP]),
         "hprmat_b200_rmatrix_adjoint": (I, [P, I, IP, DP, DP, D, I, I, DP, I, I, DP, DP, IP, DP, SP]),
+        "hprmat_b200_rmatrix_wf": (I, [P, I, IP, DP, DP, D, I, I, DP, I, I, DP, IP, I, IP, DP, I, I, SP]),
+        "hprmat_b200_rmatrix_wf_device": (I, [P, I, IP, DP, DP, D, I, I, P, I, I, P, IP, I, IP, P, I, I, SP]),
+        "hprmat_b200_wf_print": (I, [I, IP, DP, DP, D, I, I, DP, I, I, DP, I, I, DP, I, I, I, D, DP]),
         "hprmat_b200_solve_linear": (I, [P, DP, DP, I, I, SP]),
         "hprmat_b200_solve_linear_device": (I, [P, P, P, I, I, SP]),
         "hprmat_b200_solve_rmatrix": (I, [P, DP, DP, I, I, D, DP, SP]),

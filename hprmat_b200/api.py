@@ -174,6 +174,31 @@ class Context:
         nat.check(s)
         return cu, nopen.value, grad
 
+    def rmatrix_wf(self, nch, lval, qk, eta, rmax, nr, ns, cpot, nvc=(1,), ndim=None, allow_unconverged=False):
+        """Collision matrix and internal wave functions (rmatrix with twf = .true.).  ``nvc``:
+        entrance channels, 1-based among the open channels.  Returns (cu, nopen, cf) with cf
+        complex (nr*ns, nch, len(nvc)) at the mesh points and the closed-channel amplitudes in
+        cu[nopen:, ic]."""
+        self._ensure_mesh(nr, ns, rmax)
+        lval = np.ascontiguousarray(lval, dtype=np.int32)
+        qk = np.ascontiguousarray(qk, dtype=np.float64)
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        nvc = np.ascontiguousarray(nvc, dtype=np.int32)
+        cpot = np.asfortranarray(cpot, dtype=np.complex128)
+        ncp1 = cpot.shape[0]
+        ndim = int(ndim or cpot.shape[1])
+        cu = np.zeros((ndim, ndim), dtype=np.complex128, order="F")
+        cf = np.zeros((nr * ns, nch, len(nvc)), dtype=np.complex128, order="F")
+        nopen = ctypes.c_int(0)
+        st = Stats()
+        s = self._lib.hprmat_b200_rmatrix_wf(self._h, int(nch), _iptr(lval), _dptr(qk), _dptr(eta), float(rmax),
+                                             int(nr), int(ns), _dptr(cpot), int(ncp1), ndim, _dptr(cu),
+                                             ctypes.byref(nopen), len(nvc), _iptr(nvc), _dptr(cf), nr * ns, int(nch),
+                                             ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
+        return cu, nopen.value, cf
+
     def rmatrix_device(self, nch, lval, qk, eta, rmax, nr, ns, d_cpot, ncp1, ndim, d_cu, allow_unconverged=False):
         """Device-resident variant: ``d_cpot``/``d_cu`` are device addresses (ints)."""
         self._ensure_mesh(nr, ns, rmax)
@@ -271,8 +296,29 @@ def solve_rmatrix(cmat, B_vector, nch, nlag, normfac=1.0, solver_type=SOLVER_B20
     return ctx.solve_rmatrix(cmat, B_vector, nch, nlag, normfac)
 
 
+def wf_print(lval, qk, eta, rmax, nr, ns, cu, nopen, cf, zrma, iv, nom, npoin, h):
+    """Wave function of channel ``iv`` for entrance channel ``nom`` (1-based) on r = h, ...,
+    npoin*h (src/rmatrix_hp.F90:678-734): spline inside rmax, Coulomb/Whittaker outside."""
+    lib = nat.load()
+    lval = np.ascontiguousarray(lval, dtype=np.int32)
+    qk = np.ascontiguousarray(qk, dtype=np.float64)
+    eta = np.ascontiguousarray(eta, dtype=np.float64)
+    cu = np.asfortranarray(cu, dtype=np.complex128)
+    cf = np.asfortranarray(cf, dtype=np.complex128)
+    if cf.ndim == 2:
+        cf = cf[:, :, None]
+    zrma = np.ascontiguousarray(zrma, dtype=np.float64)
+    out = np.zeros(int(npoin), dtype=np.complex128)
+    s = lib.hprmat_b200_wf_print(len(lval), _iptr(lval), _dptr(qk), _dptr(eta), float(rmax), int(nr), int(ns),
+                                 _dptr(cu), cu.shape[0], int(nopen), _dptr(cf), cf.shape[0], cf.shape[1],
+                                 _dptr(zrma), int(iv), int(nom), int(npoin), float(h), _dptr(out))
+    nat.check(s)
+    return out
+
+
 class RMatrixSolver:
-    """Mirror of the reference Python binding's ``RMatrixSolver`` for solver type 7."""
+    """Mirror of the reference Python binding's ``RMatrixSolver`` for solver type 7
+    (bindings/python/hprmat.py:79-303)."""
 
     def __init__(self, nr, ns, rmax, solver=SOLVER_B200, device=0, precision="mixed"):
         if solver != SOLVER_B200:
@@ -285,3 +331,20 @@ class RMatrixSolver:
         lval = np.asarray(lval, dtype=np.int32)
         cu, nopen = self.ctx.rmatrix(len(lval), lval, qk, eta, self.rmax, self.nr, self.ns, cpot)
         return cu, nopen
+
+    def solve_with_wavefunction(self, lval, qk, eta, cpot, entrance_channels=None, solver=None):
+        """(cu, cf, nopen) with cf (nr*ns, nch, n_entrance) as the reference binding
+        (bindings/python/hprmat.py:165-207); entrance channels 1-based, default [1]."""
+        lval = np.asarray(lval, dtype=np.int32)
+        nvc = [1] if entrance_channels is None else list(entrance_channels)
+        cu, nopen, cf = self.ctx.rmatrix_wf(len(lval), lval, qk, eta, self.rmax, self.nr, self.ns, cpot, nvc)
+        return cu, cf, nopen
+
+    def interpolate_wavefunction(self, lval, qk, eta, cu, cf, nopen, channel, entrance, npoin, h=None):
+        """(r, wf) on r = h, ..., npoin*h (bindings/python/hprmat.py:254-303); h defaults to
+        2 rmax / npoin."""
+        if h is None:
+            h = 2.0 * self.rmax / npoin
+        wf = wf_print(lval, qk, eta, self.rmax, self.nr, self.ns, cu, nopen, cf, self.mesh, channel, entrance,
+                      npoin, h)
+        return np.arange(1, npoin + 1) * h, wf

@@ -847,4 +847,105 @@ __global__ void __launch_bounds__(1024) propagate_kernel(const double2* __restri
 }
 
 
+// ------------------------------------------------------------------ wave functions
+// Internal wave functions (rmatrix with twf, src/rmatrix_hp.F90:378-431), built from the
+// solutions the R-matrix step already has: per interval X = C^-1 [blockdiag(q1) | blockdiag(q2)].
+// cfp holds the channel-surface amplitudes, (ns + 1) columns of nch per entrance channel:
+// element (i, is, ic) at i + nch (is + (ns + 1) ic), is = 0..ns (column 0 stays zero).
+
+// cfp(i1, ns) = (conj(cop_m1) [i1 = i2] - U(m1, nvex) cop_m1 sqrt(k_i2 / k_i1)) / rmax over the
+// open channels i1 = open_idx[m1], i2 = open_idx[nvex] (:380-386); everything else zero.
+// One CTA.  nvc: 0-based open-channel indices of the entrance channels.
+__global__ void wf_surface_kernel(const double2* __restrict__ cu, int ndim, const int* __restrict__ open_idx, int no,
+                                  const double* __restrict__ qk, const double2* __restrict__ cop,
+                                  const int* __restrict__ nvc, int nc, int nch, int ns, double rmax, double2* cfp) {
+  const int tot = nch * (ns + 1) * nc;
+  for (int i = threadIdx.x; i < tot; i += blockDim.x) cfp[i] = make_double2(0.0, 0.0);
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < no * nc; idx += blockDim.x) {
+    const int m1 = idx % no, ic = idx / no;
+    const int nvex = nvc[ic];
+    const int i1 = open_idx[m1], i2 = open_idx[nvex];
+    const double sc = sqrt(qk[i2] / qk[i1]);
+    const double2 p = cop[m1];
+    const double2 up = cmul(cu[m1 + (size_t)nvex * ndim], p);
+    double2 v = make_double2(-up.x * sc, -up.y * sc);
+    if (i1 == i2) {
+      v.x += p.x;
+      v.y -= p.y;
+    }
+    cfp[i1 + (size_t)nch * (ns + (size_t)(ns + 1) * ic)] = make_double2(v.x / rmax, v.y / rmax);
+  }
+}
+
+// cfp(:, is) = Z cfp(:, is + 1), Z = (R00 + rin R)^-1 R01 of interval is + 1 as the propagation
+// formed it (:388-394).  grid nc.
+__global__ void wf_back_kernel(const double2* __restrict__ Z, int nch, int ns, int is, double2* cfp) {
+  const int ic = blockIdx.x;
+  const double2* src = cfp + (size_t)nch * (is + 1 + (size_t)(ns + 1) * ic);
+  double2* dst = cfp + (size_t)nch * (is + (size_t)(ns + 1) * ic);
+  for (int i = threadIdx.x; i < nch; i += blockDim.x) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int k = 0; k < nch; ++k) cfma(acc, Z[i + (size_t)k * nch], src[k]);
+    dst[i] = acc;
+  }
+}
+
+// Unnormalised wave function of interval is (1-based): cf = X2 cfp(:, is) - X1 cfp(:, is - 1),
+// X1 the nq1 leading columns of X (C^-1 blockdiag(q1); none in the first interval), X2 the nch
+// after them (C^-1 blockdiag(q2)) -- C^-1 applied to the surface amplitudes as in
+// rmat_pierre/rmatrix.f:286-301.  cf complex (nwf1, nwf2, nc), rows (is - 1) nr + ir.
+// grid (ceil(nch nr / 256), nc), 256 threads, 2 nch double2 of dynamic shared memory.
+__global__ void wf_assemble_kernel(const double2* __restrict__ X, long ldx, int nq1, int nch, int nr, int ns, int is,
+                                   const double2* __restrict__ cfp, double2* cf, long nwf1, long nwf2) {
+  extern __shared__ double2 sc[];
+  const int ic = blockIdx.y;
+  const double2* c2 = cfp + (size_t)nch * (is + (size_t)(ns + 1) * ic);
+  const double2* c1 = cfp + (size_t)nch * (is - 1 + (size_t)(ns + 1) * ic);
+  for (int k = threadIdx.x; k < nch; k += blockDim.x) {
+    sc[k] = c2[k];
+    sc[nch + k] = c1[k];
+  }
+  __syncthreads();
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= nch * nr) return;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int k = 0; k < nch; ++k) cfma(acc, X[row + (size_t)(nq1 + k) * ldx], sc[k]);
+  for (int k = 0; k < nq1; ++k) cfms(acc, X[row + (size_t)k * ldx], sc[nch + k]);
+  const int i1 = row / nr, ir = row - i1 * nr;
+  cf[(size_t)((is - 1) * nr + ir) + nwf1 * ((size_t)i1 + nwf2 * ic)] = acc;
+}
+
+// Closed-channel amplitudes (:414-419): cu(nopen + m, ic) = sum_ir cf((ns-1) nr + ir, i1, ic)
+// q2(ir, ns) / W_i1 over the closed channels i1 = closed_idx[m], before the normalisation.
+// grid nc.
+__global__ void wf_closed_kernel(const double2* __restrict__ cf, long nwf1, long nwf2, int nr, int ns,
+                                 const double* __restrict__ q2last, const int* __restrict__ closed_idx, int ncl,
+                                 const double* __restrict__ xc2, int no, double2* cu, int ndim) {
+  const int ic = blockIdx.x;
+  for (int m = threadIdx.x; m < ncl; m += blockDim.x) {
+    const int i1 = closed_idx[m];
+    const double2* f = cf + (size_t)(ns - 1) * nr + nwf1 * ((size_t)i1 + nwf2 * ic);
+    double ar = 0.0, ai = 0.0;
+    for (int ir = 0; ir < nr; ++ir) {
+      ar = fma(f[ir].x, q2last[ir], ar);
+      ai = fma(f[ir].y, q2last[ir], ai);
+    }
+    const double w = xc2[i1];
+    cu[(size_t)(no + m) + (size_t)ic * ndim] = make_double2(ar / w, ai / w);
+  }
+}
+
+// cf(row, i1, ic) /= sqrt(rmax0 w_ir), row = (is - 1) nr + ir (:421-428).  grid
+// (ceil(nr ns / 256), nch, nc).
+__global__ void wf_normalize_kernel(double2* cf, long nwf1, long nwf2, int nr, int ns, const double* __restrict__ wle,
+                                    double rmax0) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= nr * ns) return;
+  const double sc = 1.0 / sqrt(rmax0 * wle[row % nr]);
+  double2* v = cf + (size_t)row + nwf1 * ((size_t)blockIdx.y + nwf2 * blockIdx.z);
+  v->x *= sc;
+  v->y *= sc;
+}
+
 }  // namespace hprmat

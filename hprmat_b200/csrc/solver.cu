@@ -105,10 +105,12 @@ struct hprmat_b200_ctx {
   // per interval is (nr values or nr x nr matrices each, interval-major): kinetic + Bloch tc,
   // closed-channel Bloch matrix blo0 (MeshDev), outer and inner boundary values q2, q1
   std::vector<double> xle, wle, tc, blo0, q2, q1, zrma;
-  DevBuf mesh;  // tc | blo0 | r | q2 | q1, each ns intervals
+  DevBuf mesh;  // tc | blo0 | r | q2 | q1, each ns intervals, then the weights wle (nr)
   // work buffers
   DevBuf W, A64, X, X64, R64, B64, V, Z, gm, swaps, ipiv, stage, status, ops, inv, chan, rmat,
       zwork, cpot, cu, norms, lup, rop, rsurf, vt, rlo, linv;
+  // wave functions: per-interval solutions and propagation matrices, surface amplitudes, cf
+  DevBuf wfx, wfz, wfc, wfcf;
   // tensor-core operand views of the current factorisation (mixed path)
   TcOperand op_lu, op_bop, op_rhs, op_linv;
   long lup_ld = 0, lup_plane = 0, rop_plane = 0;
@@ -293,7 +295,7 @@ static void build_mesh(hprmat_b200_ctx* c, int nr, int ns, double rmax) {
 
 static int upload_mesh(hprmat_b200_ctx* c) {
   const size_t nn = (size_t)c->nr * c->nr, nv = (size_t)c->nr * c->ns;
-  const size_t n = 2 * nn * c->ns + 3 * nv;
+  const size_t n = 2 * nn * c->ns + 3 * nv + c->nr;
   TRY(c->mesh.ensure(n * sizeof(double)));
   std::vector<double> h(n);
   double* p = h.data();
@@ -301,10 +303,16 @@ static int upload_mesh(hprmat_b200_ctx* c) {
   p = std::copy(c->blo0.begin(), c->blo0.end(), p);
   p = std::copy(c->zrma.begin(), c->zrma.end(), p);
   p = std::copy(c->q2.begin(), c->q2.end(), p);
-  std::copy(c->q1.begin(), c->q1.end(), p);
+  p = std::copy(c->q1.begin(), c->q1.end(), p);
+  std::copy(c->wle.begin(), c->wle.end(), p);
   HPR_CUDA_TRY(cudaMemcpyAsync(c->mesh.p, h.data(), n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
   return HPRMAT_B200_OK;
+}
+
+// Gauss-Legendre weights of the mesh on the device.
+static const double* mesh_wle(const hprmat_b200_ctx* c) {
+  return c->mesh.as<double>() + 2 * (size_t)c->ns * c->nr * c->nr + 3 * (size_t)c->nr * c->ns;
 }
 
 // Device view of interval is (0-based); nq1 leading right-hand sides blockdiag(q1).
@@ -1061,8 +1069,8 @@ static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W3
 // ------------------------------------------------------------------ boundary values
 struct Boundary {
   int nopen = 0;
-  std::vector<int> open_idx;
-  std::vector<double> fac, kk, bloch, qk;
+  std::vector<int> open_idx, closed_idx;
+  std::vector<double> fac, kk, bloch, qk, xc2;  // xc2: W(rmax) of closed channels (xc(c, 2))
   std::vector<double2> co, cop;
 };
 
@@ -1073,6 +1081,7 @@ static int boundary_values(int nch, const int* lval, const double* qk, const dou
   b.fac.resize(nch);
   b.kk.resize(nch);
   b.bloch.resize(nch);
+  b.xc2.assign(nch, 0.0);
   b.qk.assign(qk, qk + nch);
   for (int c = 0; c < nch; ++c) {
     const int l = lval[c];
@@ -1093,6 +1102,8 @@ static int boundary_values(int nch, const int* lval, const double* qk, const dou
       WhitOut w = whit_l(eta[c], rmax, qk2, l);
       double xc1 = rmax * w.wd / w.w;
       b.bloch[c] = xc1 / rmax2;
+      b.xc2[c] = w.w;
+      b.closed_idx.push_back(c);
     }
   }
   b.nopen = (int)b.open_idx.size();
@@ -1223,12 +1234,25 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
 // factors (the reference's second FP64 solve with 2 nch right-hand sides, done here at the
 // context's precision with the same refinement) and its projections R00 = q1^T X_1,
 // R01 = q1^T X_2, R11 = q2^T X_2 update the propagated R (propagate_kernel).
+// Wave functions requested from rmatrix_core (the twf arguments of rmatrix): nc entrance
+// channels nvc (host, 1-based indices among the open channels) and the device array cf,
+// complex (nwf1, nwf2, nc).
+struct WfRequest {
+  int nc = 0;
+  const int* nvc = nullptr;
+  double2* d_cf = nullptr;
+  long nwf1 = 0, nwf2 = 0;
+};
+
 static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const double* qk, const double* eta,
                         double rmax, int nr, int ns, const double2* d_cpot, int ncp1, int ndim, double2* d_cu,
-                        int* nopen, hprmat_b200_stats* stats) {
+                        int* nopen, hprmat_b200_stats* stats, const WfRequest* wf = nullptr) {
   auto t_all = Clock::now();
   if (nch <= 0 || nr <= 0 || ns <= 0 || !lval || !qk || !eta || !d_cpot || !d_cu || !nopen)
     return fail(HPRMAT_B200_ERR_ARG, "rmatrix: invalid arguments");
+  if (wf && (wf->nc <= 0 || !wf->nvc || !wf->d_cf || wf->nwf1 < (long)nr * ns || wf->nwf2 < nch || wf->nc > ndim))
+    return fail(HPRMAT_B200_ERR_ARG, "rmatrix: wave functions need nc >= 1, nvc, cf with nwf1 >= nr*ns, "
+                                     "nwf2 >= nch and nc <= ndim");
   if (ndim < nch || ncp1 < nr * ns) return fail(HPRMAT_B200_ERR_ARG, "rmatrix: ndim < nch or ncp1 < nr*ns");
   if (c->nr != nr || c->ns != ns || c->rmax != rmax)
     return fail(HPRMAT_B200_ERR_ARG, "rmatrix: call rmat_ini(nr=%d, ns=%d, rmax=%g) first", nr, ns, rmax);
@@ -1239,10 +1263,19 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
   Boundary bnd;
   TRY(boundary_values(nch, lval, qk, eta, rmax, rmax0, bnd));
   *nopen = bnd.nopen;
-  // channel data: fac | kk | bloch | qk (doubles), then co | cop (double2), then open_idx
-  const size_t nd = 4 * (size_t)nch;
+  const int ncl = (int)bnd.closed_idx.size();
+  const int nc = wf ? wf->nc : 0;
+  if (wf)
+    for (int ic = 0; ic < nc; ++ic)
+      if (wf->nvc[ic] < 1 || wf->nvc[ic] > bnd.nopen)
+        return fail(HPRMAT_B200_ERR_ARG, "rmatrix: entrance channel nvc(%d) = %d is not an open channel (nopen = %d)",
+                    ic + 1, wf->nvc[ic], bnd.nopen);
+  // channel data: fac | kk | bloch | qk | xc2 (doubles, padded to an even count so that the
+  // double2 arrays after them stay 16-byte aligned), then co | cop (double2), then
+  // open_idx | closed_idx | nvc - 1 (ints)
+  const size_t nd = (5 * (size_t)nch + 1) / 2 * 2;
   const size_t bytes = nd * sizeof(double) + 2 * (size_t)std::max(1, bnd.nopen) * sizeof(double2) +
-                       (size_t)std::max(1, bnd.nopen) * sizeof(int) + 64;
+                       ((size_t)std::max(1, bnd.nopen) + std::max(1, ncl) + std::max(1, nc)) * sizeof(int) + 64;
   TRY(c->chan.ensure(bytes));
   std::vector<unsigned char> h(bytes, 0);
   double* hd = reinterpret_cast<double*>(h.data());
@@ -1250,18 +1283,24 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
   std::copy(bnd.kk.begin(), bnd.kk.end(), hd + nch);
   std::copy(bnd.bloch.begin(), bnd.bloch.end(), hd + 2 * nch);
   std::copy(bnd.qk.begin(), bnd.qk.end(), hd + 3 * nch);
+  std::copy(bnd.xc2.begin(), bnd.xc2.end(), hd + 4 * nch);
   double2* hz = reinterpret_cast<double2*>(hd + nd);
   std::copy(bnd.co.begin(), bnd.co.end(), hz);
   std::copy(bnd.cop.begin(), bnd.cop.end(), hz + std::max(1, bnd.nopen));
   int* hi = reinterpret_cast<int*>(hz + 2 * std::max(1, bnd.nopen));
   std::copy(bnd.open_idx.begin(), bnd.open_idx.end(), hi);
+  std::copy(bnd.closed_idx.begin(), bnd.closed_idx.end(), hi + std::max(1, bnd.nopen));
+  for (int ic = 0; ic < nc; ++ic) hi[std::max(1, bnd.nopen) + std::max(1, ncl) + ic] = wf->nvc[ic] - 1;
   HPR_CUDA_TRY(cudaMemcpyAsync(c->chan.p, h.data(), bytes, cudaMemcpyHostToDevice, c->stream));
   const double* dd = c->chan.as<double>();
   ChannelData chd{dd, dd + nch, dd + 2 * nch};
   const double* d_qk = dd + 3 * nch;
+  const double* d_xc2 = dd + 4 * nch;
   const double2* d_co = reinterpret_cast<const double2*>(dd + nd);
   const double2* d_cop = d_co + std::max(1, bnd.nopen);
   const int* d_open = reinterpret_cast<const int*>(d_cop + std::max(1, bnd.nopen));
+  const int* d_closed = d_open + std::max(1, bnd.nopen);
+  const int* d_nvc = d_closed + std::max(1, ncl);
 
   const long ld = (N + 3) / 4 * 4;
   const int nrhs_max = ns > 1 ? 2 * nch : nch;
@@ -1286,9 +1325,18 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
   double2* rp = R + 3 * nn;
   double2* zo = c->zwork.as<double2>();
   int* d_info = c->status.as<int>() + SW_INFO;
+  // with wave functions every interval keeps its solutions (slot is, ld x nrhs_max) and its
+  // propagation matrix (R00 + rmax1 R)^-1 R01 (slot is, nch^2)
+  const size_t xslot = (size_t)ld * nrhs_max;
+  if (wf) {
+    TRY(c->wfx.ensure((size_t)ns * xslot * sizeof(double2)));
+    TRY(c->wfz.ensure((size_t)ns * nn * sizeof(double2)));
+    TRY(c->wfc.ensure((size_t)nch * (ns + 1) * nc * sizeof(double2)));
+  }
   int status = HPRMAT_B200_OK;
   for (int is = 0; is < ns; ++is) {
     const MeshDev md = mesh_dev(c, is, is > 0 ? nch : 0);
+    if (wf) X64 = c->wfx.as<double2>() + (size_t)is * xslot;
     hprmat_b200_stats si;
     memset(&si, 0, sizeof(si));
     si.rel_residual = -1.0;
@@ -1326,8 +1374,8 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
     rmat_extract_kernel<<<ge, 128, 0, c->stream>>>(X64 + (size_t)nch * ld, ld, md.q2, nr, nch, nch, 1.0, R11);
     LAUNCH_CHECK();
     HPR_CUDA_TRY(cudaMemsetAsync(d_info, 0, sizeof(int), c->stream));
-    propagate_kernel<<<1, 1024, 0, c->stream>>>(R, R01, R11, rp, nch, is * rmax0, (is + 1) * rmax0, zo, zo + nn,
-                                                d_info);
+    propagate_kernel<<<1, 1024, 0, c->stream>>>(R, R01, R11, rp, nch, is * rmax0, (is + 1) * rmax0, zo,
+                                                wf ? c->wfz.as<double2>() + (size_t)is * nn : zo + nn, d_info);
     LAUNCH_CHECK();
     HPR_CUDA_TRY(cudaMemcpyAsync(c->h_status, c->status.p, SW_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1343,6 +1391,33 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
   HPR_CUDA_TRY(cudaMemcpyAsync(c->h_status, c->status.p, SW_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
   if (c->h_status[SW_INFO] != 0) return fail(HPRMAT_B200_SINGULAR, "singular Z_O in the collision-matrix step");
+  if (wf) {
+    // surface amplitudes from U, carried inwards, then the wave function per interval
+    double2* cfp = c->wfc.as<double2>();
+    wf_surface_kernel<<<1, 256, 0, c->stream>>>(d_cu, ndim, d_open, no, d_qk, d_cop, d_nvc, nc, nch, ns, rmax, cfp);
+    LAUNCH_CHECK();
+    for (int is = ns - 1; is >= 1; --is) {  // 1-based interval is from interval is + 1
+      wf_back_kernel<<<nc, 128, 0, c->stream>>>(c->wfz.as<double2>() + (size_t)is * nn, nch, ns, is, cfp);
+      LAUNCH_CHECK();
+    }
+    const size_t smem = 2 * (size_t)nch * sizeof(double2);
+    if (smem > 48 * 1024) TRY(set_smem(wf_assemble_kernel, smem));
+    for (int is = 1; is <= ns; ++is) {
+      wf_assemble_kernel<<<dim3(cdiv_u(N, 256), nc), 256, smem, c->stream>>>(
+          c->wfx.as<double2>() + (size_t)(is - 1) * xslot, ld, is > 1 ? nch : 0, nch, nr, ns, is, cfp, wf->d_cf,
+          wf->nwf1, wf->nwf2);
+      LAUNCH_CHECK();
+    }
+    if (ncl > 0) {
+      wf_closed_kernel<<<nc, 128, 0, c->stream>>>(wf->d_cf, wf->nwf1, wf->nwf2, nr, ns,
+                                                   mesh_dev(c, ns - 1).q2, d_closed, ncl, d_xc2, no, d_cu, ndim);
+      LAUNCH_CHECK();
+    }
+    wf_normalize_kernel<<<dim3(cdiv_u(nr * ns, 256), nch, nc), 256, 0, c->stream>>>(wf->d_cf, wf->nwf1, wf->nwf2, nr,
+                                                                                    ns, mesh_wle(c), rmax0);
+    LAUNCH_CHECK();
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
   if (stats) {
     stats->ms_umatrix = ms_since(t4);
     stats->ms_total = ms_since(t_all);
@@ -1601,7 +1676,8 @@ int hprmat_b200_destroy(hprmat_b200_ctx* c) {
   cudaStreamSynchronize(c->stream);
   DevBuf* bufs[] = {&c->mesh, &c->W, &c->A64, &c->X, &c->X64, &c->R64, &c->B64, &c->V, &c->Z, &c->gm,
                     &c->swaps, &c->ipiv, &c->stage, &c->status, &c->ops, &c->inv, &c->chan, &c->rmat,
-                    &c->zwork, &c->cpot, &c->cu, &c->norms, &c->lup, &c->rop, &c->rsurf, &c->vt, &c->rlo, &c->linv};
+                    &c->zwork, &c->cpot, &c->cu, &c->norms, &c->lup, &c->rop, &c->rsurf, &c->vt, &c->rlo, &c->linv,
+                    &c->wfx, &c->wfz, &c->wfc, &c->wfcf};
   for (DevBuf* b : bufs) b->release();
   for (hprmat_b200_ctx* w : c->scan_workers) hprmat_b200_destroy(w);
   c->scan_workers.clear();
@@ -1671,6 +1747,142 @@ int hprmat_b200_rmatrix(hprmat_b200_ctx* c, int nch, const int* lval, const doub
   }
   if (stats) stats->status = s;
   return s;
+}
+
+int hprmat_b200_rmatrix_wf_device(hprmat_b200_ctx* c, int nch, const int* lval, const double* qk, const double* eta,
+                                  double rmax, int nr, int ns, const void* d_cpot, int ncp1, int ndim, void* d_cu,
+                                  int* nopen, int nc, const int* nvc, void* d_cf, int nwf1, int nwf2,
+                                  hprmat_b200_stats* stats) {
+  TRY(check_ctx(c));
+  WfRequest wf;
+  wf.nc = nc;
+  wf.nvc = nvc;
+  wf.d_cf = (double2*)d_cf;
+  wf.nwf1 = nwf1;
+  wf.nwf2 = nwf2;
+  int s = rmatrix_core(c, nch, lval, qk, eta, rmax, nr, ns, (const double2*)d_cpot, ncp1, ndim, (double2*)d_cu, nopen,
+                       stats, &wf);
+  if (stats) stats->status = s;
+  return s;
+}
+
+int hprmat_b200_rmatrix_wf(hprmat_b200_ctx* c, int nch, const int* lval, const double* qk, const double* eta,
+                           double rmax, int nr, int ns, const double* cpot, int ncp1, int ndim, double* cu, int* nopen,
+                           int nc, const int* nvc, double* cf, int nwf1, int nwf2, hprmat_b200_stats* stats) {
+  TRY(check_ctx(c));
+  if (!cpot || !cu || !cf || ndim <= 0 || ncp1 <= 0 || nc <= 0 || nwf1 <= 0 || nwf2 <= 0)
+    return fail(HPRMAT_B200_ERR_ARG, "rmatrix_wf: invalid arguments");
+  const size_t pbytes = (size_t)ncp1 * ndim * ndim * sizeof(double2);
+  const size_t ubytes = (size_t)ndim * ndim * sizeof(double2);
+  const size_t fbytes = (size_t)nwf1 * nwf2 * nc * sizeof(double2);
+  TRY(c->cpot.ensure(pbytes));
+  TRY(c->cu.ensure(ubytes));
+  TRY(c->wfcf.ensure(fbytes));
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->cpot.p, cpot, pbytes, cudaMemcpyHostToDevice, c->stream));
+  WfRequest wf;
+  wf.nc = nc;
+  wf.nvc = nvc;
+  wf.d_cf = c->wfcf.as<double2>();
+  wf.nwf1 = nwf1;
+  wf.nwf2 = nwf2;
+  int s = rmatrix_core(c, nch, lval, qk, eta, rmax, nr, ns, c->cpot.as<double2>(), ncp1, ndim, c->cu.as<double2>(),
+                       nopen, stats, &wf);
+  if (s == HPRMAT_B200_OK || s == HPRMAT_B200_NOT_CONVERGED) {
+    HPR_CUDA_TRY(cudaMemcpyAsync(cu, c->cu.p, ubytes, cudaMemcpyDeviceToHost, c->stream));
+    // only the written part of cf: rows 1..nr*ns of channels 1..nch per entrance channel
+    const size_t pitch = (size_t)nwf1 * sizeof(double2);
+    for (int ic = 0; ic < nc; ++ic) {
+      const size_t off = (size_t)ic * nwf1 * nwf2;
+      HPR_CUDA_TRY(cudaMemcpy2DAsync(reinterpret_cast<double2*>(cf) + off, pitch, c->wfcf.as<double2>() + off, pitch,
+                                     (size_t)nr * ns * sizeof(double2), nch, cudaMemcpyDeviceToHost, c->stream));
+    }
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
+  if (stats) stats->status = s;
+  return s;
+}
+
+// Complex value i of a caller's interleaved complex array, read as two doubles: a Fortran
+// complex*16 array need not be 16-byte aligned.
+static inline double2 host_c(const double* p, size_t i) { return mk(p[2 * i], p[2 * i + 1]); }
+
+// Natural cubic spline through (x, y), n >= 2: second derivatives y2 by the tridiagonal
+// (Thomas) elimination of the spline's continuity equations with y2 = 0 at both ends.
+static void natural_spline(const double* x, const double* y, int n, std::vector<double>& y2) {
+  y2.assign(n, 0.0);
+  std::vector<double> u(n, 0.0);
+  for (int i = 1; i < n - 1; ++i) {
+    const double sig = (x[i] - x[i - 1]) / (x[i + 1] - x[i - 1]);
+    const double p = sig * y2[i - 1] + 2.0;
+    y2[i] = (sig - 1.0) / p;
+    const double d = (y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1]);
+    u[i] = (6.0 * d / (x[i + 1] - x[i - 1]) - sig * u[i - 1]) / p;
+  }
+  y2[n - 1] = 0.0;
+  for (int k = n - 2; k >= 0; --k) y2[k] = y2[k] * y2[k + 1] + u[k];
+}
+
+// The spline's value at r: bracketing interval by bisection (the end intervals continue
+// beyond the first and last node), then the cubic in its local coordinates.
+static double spline_at(const double* x, const double* y, const std::vector<double>& y2, int n, double r) {
+  int lo = 0, hi = n - 1;
+  while (hi - lo > 1) {
+    const int k = (hi + lo) / 2;
+    if (x[k] > r)
+      hi = k;
+    else
+      lo = k;
+  }
+  const double h = x[hi] - x[lo];
+  const double a = (x[hi] - r) / h, b = (r - x[lo]) / h;
+  return a * y[lo] + b * y[hi] + ((a * a * a - a) * y2[lo] + (b * b * b - b) * y2[hi]) * h * h / 6.0;
+}
+
+int hprmat_b200_wf_print(int nch, const int* lval, const double* qk, const double* eta, double rmax, int nr, int ns,
+                         const double* cu, int ndim, int nopen, const double* cf, int nwf1, int nwf2,
+                         const double* zrma, int iv, int nom, int npoin, double h, double* cwftab) {
+  if (nch <= 0 || !lval || !qk || !eta || !cu || !cf || !zrma || !cwftab || nr * ns < 2 || nwf1 < nr * ns ||
+      nwf2 < nch || iv < 1 || iv > nch || nom < 1 || nom > nch || npoin < 0 || ndim < nch)
+    return fail(HPRMAT_B200_ERR_ARG, "wf_print: invalid arguments");
+  const int nsr = nr * ns;
+  int nop = 0, nclo = nopen;
+  for (int w = 0; w < iv; ++w) {
+    if (qk[w] > 0) ++nop;
+    if (qk[w] < 0) ++nclo;
+  }
+  const size_t f0 = (size_t)nwf1 * ((size_t)(iv - 1) + (size_t)nwf2 * (nom - 1));
+  std::vector<double> fr(nsr), fi(nsr), y2r, y2i;
+  for (int i = 0; i < nsr; ++i) {
+    fr[i] = cf[2 * (f0 + i)];
+    fi[i] = cf[2 * (f0 + i) + 1];
+  }
+  natural_spline(zrma, fr.data(), nsr, y2r);
+  natural_spline(zrma, fi.data(), nsr, y2i);
+  const int l = lval[iv - 1];
+  auto put = [&](int i, double2 v) {
+    cwftab[2 * i] = v.x;
+    cwftab[2 * i + 1] = v.y;
+  };
+  for (int i = 1; i <= npoin; ++i) {
+    const double r = i * h;
+    if (r <= rmax) {
+      put(i - 1, mk(spline_at(zrma, fr.data(), y2r, nsr, r), spline_at(zrma, fi.data(), y2i, nsr, r)));
+    } else if (qk[iv - 1] > 0) {
+      const CoulombFG fg = coulfg_single(qk[iv - 1] * r, eta[iv - 1], (double)l);
+      if (fg.ifail != 0) return fail(HPRMAT_B200_ERR_ARG, "wf_print: COULFG failed (ifail=%d) at r = %g", fg.ifail, r);
+      const double sc = sqrt(qk[nom - 1] / qk[iv - 1]);
+      const double2 co = mk(fg.g * sc, fg.f * sc);
+      double2 v = cmul(host_c(cu, (size_t)(nop - 1) + (size_t)(nom - 1) * ndim), co);
+      v = mk(-v.x, -v.y);
+      if (iv == nom) v = mk(v.x + co.x, v.y - co.y);
+      put(i - 1, v);
+    } else {
+      const WhitOut w = whit_l(eta[iv - 1], r, -qk[iv - 1], l);
+      const double2 a = host_c(cu, (size_t)(nclo - 1) + (size_t)(nom - 1) * ndim);
+      put(i - 1, mk(a.x * w.w, a.y * w.w));
+    }
+  }
+  return HPRMAT_B200_OK;
 }
 
 // Batched energy scan: every block's potential is copied once; (block, energy) units are
@@ -1806,8 +2018,6 @@ int hprmat_b200_rmatrix_adjoint(hprmat_b200_ctx* c, int nch, const int* lval, co
   TRY(boundary_values(nch, lval, qk, eta, rmax, a, bnd));
   const int no = bnd.nopen;
   if (no > 0) {
-    const double2* U = reinterpret_cast<const double2*>(cu);
-    const double2* G = reinterpret_cast<const double2*>(gu);
     auto sk = [&](int m1, int m2) { return sqrt(qk[bnd.open_idx[m1]] / qk[bnd.open_idx[m2]]); };
     std::vector<double2> Zt((size_t)no * no), Pt((size_t)no * no);  // Z_O^T and (W G^H)^T
     for (int m2 = 0; m2 < no; ++m2)
@@ -1829,12 +2039,12 @@ int hprmat_b200_rmatrix_adjoint(hprmat_b200_ctx* c, int nch, const int* lval, co
       for (int b1 = 0; b1 < no; ++b1) {
         double2 acc = mk(0.0, 0.0);  // (W G^H)(a1, b1) = sum_k W(a1, k) conj(G(b1, k))
         for (int k = 0; k < no; ++k) {
-          double2 w = cmul(bnd.cop[a1], U[a1 + (size_t)k * ndim]);
+          double2 w = cmul(bnd.cop[a1], host_c(cu, a1 + (size_t)k * ndim));
           if (a1 == k) {
             w.x -= bnd.cop[a1].x;
             w.y += bnd.cop[a1].y;
           }
-          const double2 g = G[b1 + (size_t)k * ndim];
+          const double2 g = host_c(gu, b1 + (size_t)k * ndim);
           cfma(acc, w, mk(g.x, -g.y));
         }
         Pt[b1 + (size_t)a1 * no] = acc;

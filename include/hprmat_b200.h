@@ -128,8 +128,8 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* ctx, int nblocks, const hprmat_b20
                              int nr, int nworkers, double* seconds);
 
 /* Collision matrix for one (J, pi, E): rmatrix(nch, lval, qk, eta, rmax, nr, ns, cpot, cu,
-   ncp1, ndim, nopen, ...) of src/rmatrix_hp.F90:175-368, for local potentials (ncp2 = 0) and
-   one interval (ns = 1).  Host buffers: cpot is complex (ncp1, ndim, ndim), cu is complex
+   ncp1, ndim, nopen, ...) of src/rmatrix_hp.F90:175-368, for local potentials (ncp2 = 0), on
+   one interval or propagated over ns > 1 intervals (:326-345).  Host buffers: cpot is complex (ncp1, ndim, ndim), cu is complex
    (ndim, ndim) and receives U in cu(1:nopen, 1:nopen); the rest of cu is zeroed as in the
    reference (:221).  The mesh must have been set by hprmat_b200_rmat_ini with the same
    nr, ns and rmax.  stats may be NULL. */
@@ -143,6 +143,35 @@ int hprmat_b200_rmatrix_device(hprmat_b200_ctx* ctx, int nch, const int* lval,
                                const double* qk, const double* eta, double rmax, int nr,
                                int ns, const void* d_cpot, int ncp1, int ndim, void* d_cu,
                                int* nopen, hprmat_b200_stats* stats);
+
+/* rmatrix with wave functions (twf = .true.; the cf, nwf1, nwf2, nc, nvc arguments of
+   src/rmatrix_hp.F90:175-186, computed at :378-431): as hprmat_b200_rmatrix, and for the nc
+   entrance channels nvc[0..nc-1] (1-based indices among the open channels) the internal wave
+   functions at the mesh points zrma in cf, complex (nwf1, nwf2, nc) with nwf1 >= nr*ns and
+   nwf2 >= nch (rows 1..nr*ns of channels 1..nch are written), and the closed-channel
+   amplitudes in cu(nopen+1.., ic).  The wave function applies C^-1 to the surface amplitudes,
+   as Descouvemont's original (rmat_pierre/rmatrix.f:286-301); HPRMAT's rmatrix_hp.F90:407
+   multiplies by C instead.  Built from the per-interval solutions of the R-matrix step: no
+   further factorisation or solve. */
+int hprmat_b200_rmatrix_wf(hprmat_b200_ctx* ctx, int nch, const int* lval, const double* qk,
+                           const double* eta, double rmax, int nr, int ns, const double* cpot,
+                           int ncp1, int ndim, double* cu, int* nopen, int nc, const int* nvc,
+                           double* cf, int nwf1, int nwf2, hprmat_b200_stats* stats);
+
+/* Same with cpot, cu and cf in device memory. */
+int hprmat_b200_rmatrix_wf_device(hprmat_b200_ctx* ctx, int nch, const int* lval, const double* qk,
+                                  const double* eta, double rmax, int nr, int ns, const void* d_cpot,
+                                  int ncp1, int ndim, void* d_cu, int* nopen, int nc, const int* nvc,
+                                  void* d_cf, int nwf1, int nwf2, hprmat_b200_stats* stats);
+
+/* wf_print (src/rmatrix_hp.F90:678-734): the wave function of channel iv for entrance channel
+   nom (both 1-based) at r = h, 2h, ..., npoin*h into cwftab (complex, npoin): a natural cubic
+   spline of cf(1:nr*ns, iv, nom) over zrma for r <= rmax, the Coulomb (open) or Whittaker
+   (closed) form with the amplitudes of cu beyond.  Host computation, no context. */
+int hprmat_b200_wf_print(int nch, const int* lval, const double* qk, const double* eta, double rmax, int nr,
+                         int ns, const double* cu, int ndim, int nopen, const double* cf, int nwf1,
+                         int nwf2, const double* zrma, int iv, int nom, int npoin, double h,
+                         double* cwftab);
 
 /* Dense solve C X = B: the solve inside solve_rmatrix (src/rmat_solvers.F90:49-90), same
    layout as gpu_solve_mixed_ (src/cusolver_interface.cu:321-443).  A (n x n complex,

@@ -383,7 +383,7 @@ def rmatrix(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, solver: str = "dense") -
     return RMatrixResult(cu, bnd.nopen, crma0_prev, bnd, x_last if ns == 1 else None)
 
 
-def rmatrix_wf(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, nvc):
+def rmatrix_wf(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, nvc, u=None):
     """U and the internal wave functions (rmatrix with twf = .true., src/rmatrix_hp.F90:378-431).
 
     ``nvc``: entrance channels, 1-based indices among the open channels.  Per interval the
@@ -395,6 +395,11 @@ def rmatrix_wf(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, nvc):
     original (rmat_pierre/rmatrix.f:286-301), where ``ch`` holds the inverse; the HPRMAT
     version multiplies by C itself at :407.  Closed-channel amplitudes go to
     cu[nopen + m, ic] (:414-419), and cf is divided by sqrt(rmax0 w_i) (:421-428).
+
+    ``u``: use this collision matrix (nopen x nopen or larger) for the surface amplitudes
+    instead of the oracle's own.  Where |U| ~ 1 deep under a barrier (e.g. Ex1, |cop| ~ 1e7)
+    the wave function's small components are set by the last bits of U, so a reconstruction
+    is compared with the oracle's from the same U.
 
     Returns (cu (nch, nch) with U in [:nopen, :nopen], nopen, cf (nr ns, nch, len(nvc))).
     """
@@ -427,8 +432,11 @@ def rmatrix_wf(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, nvc):
         xs.append((x1, x2))
         crma.append((r00, r01, r11))
         crma0.append(c0)
-    u = collision_matrix(crma0[-1], bnd, qk)
     no = bnd.nopen
+    if u is None:
+        u = collision_matrix(crma0[-1], bnd, qk)
+    else:
+        u = np.asarray(u, dtype=np.complex128)[:no, :no]
     cu = np.zeros((nch, nch), dtype=np.complex128)
     cu[:no, :no] = u
     cf = np.zeros((nr * ns, nch, len(nvc)), dtype=np.complex128)

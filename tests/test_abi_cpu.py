@@ -123,3 +123,35 @@ def test_mesh_matches_oracle(nr, ns, rmax):
         np.testing.assert_allclose(q2[s * nr:(s + 1) * nr], m.q2[:, s], rtol=1e-14)
         np.testing.assert_allclose(q1[s * nr:(s + 1) * nr], m.q1[:, s], rtol=1e-14, atol=0)
     np.testing.assert_allclose(zr, m.zrma, rtol=1e-15)
+
+
+def test_wf_print_matches_oracle():
+    """The library's host wf_print (spline inside rmax, Coulomb/Whittaker outside) against the
+    oracle's restatement on Ex3's wave function (oracle cu and cf as input), every channel."""
+    from tests.example_inputs import ex3_setup
+    nr, ns, rmax, j = 50, 2, 14.0, 30
+    mesh = orc.rmat_ini(nr, ns, rmax)
+    cpot, kin, nv = ex3_setup(mesh.zrma, j)
+    lval, qk, eta = kin(34.0)
+    cu, no, cf = orc.rmatrix_wf(nv, lval, qk, eta, rmax, mesh, cpot, [1])
+    for iv in range(1, nv + 1):
+        ref = orc.wf_print(nv, lval, qk, eta, rmax, mesh, cu, no, cf, iv, 1, 25, 0.8)
+        got = api.wf_print(lval, qk, eta, rmax, nr, ns, cu, no, cf, mesh.zrma, iv, 1, 25, 0.8)
+        np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-14 * np.abs(ref).max())
+    with pytest.raises(nat.HprmatError):
+        api.wf_print(lval, qk, eta, rmax, nr, ns, cu, no, cf, mesh.zrma, nv + 1, 1, 5, 1.0)
+
+
+def test_wf_print_closed_channel_tail():
+    """Closed channels outside rmax: the Whittaker form times the closed-channel amplitude."""
+    from tests.example_inputs import ex4_setup
+    nr, ns, rmax, j = 20, 4, 11.0, 3
+    mesh = orc.rmat_ini(nr, ns, rmax)
+    cpot, kin, nv = ex4_setup(mesh.zrma, j)
+    lval, qk, eta = kin(4.0)
+    assert (qk < 0).any()
+    cu, no, cf = orc.rmatrix_wf(nv, lval, qk, eta, rmax, mesh, cpot, [1])
+    for iv in range(1, nv + 1):
+        ref = orc.wf_print(nv, lval, qk, eta, rmax, mesh, cu, no, cf, iv, 1, 16, 1.0)
+        got = api.wf_print(lval, qk, eta, rmax, nr, ns, cu, no, cf, mesh.zrma, iv, 1, 16, 1.0)
+        np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-14 * max(np.abs(ref).max(), 1e-300))
