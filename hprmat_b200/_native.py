@@ -34,7 +34,7 @@ EXPORTED = (
     "hprmat_b200_last_error", "hprmat_b200_version", "hprmat_b200_boundary",
     "hprmat_b200_solve_linear_noalloc", "hprmat_b200_rmatrix_scan",
     "hprmat_b200_rmatrix_adjoint", "hprmat_b200_rmatrix_wf", "hprmat_b200_rmatrix_wf_device",
-    "hprmat_b200_wf_print",
+    "hprmat_b200_wf_print", "hprmat_b200_rmatrix_full",
     # include/hprmat_b200_dev.h
     "hprmat_b200_dev_tc_update", "hprmat_b200_dev_split_planes", "hprmat_b200_dev_set_profile",
     "hprmat_b200_dev_counters", "hprmat_b200_dev_wave_trace", "hprmat_b200_dev_wave_trace_read",
@@ -105,6 +105,8 @@ def load():
         "hprmat_b200_rmatrix_wf": (I, [P, I, IP, DP, DP, D, I, I, DP, I, I, DP, IP, I, IP, DP, I, I, SP]),
         "hprmat_b200_rmatrix_wf_device": (I, [P, I, IP, DP, DP, D, I, I, P, I, I, P, IP, I, IP, P, I, I, SP]),
         "hprmat_b200_wf_print": (I, [I, IP, DP, DP, D, I, I, DP, I, I, DP, I, I, DP, I, I, I, D, DP]),
+        "hprmat_b200_rmatrix_full": (I, [P, I, IP, DP, DP, D, I, I, DP, I, I, DP, IP, I, DP, I, I, I, IP, I, DP,
+                                         SP]),
         "hprmat_b200_solve_linear": (I, [P, DP, DP, I, I, SP]),
         "hprmat_b200_solve_linear_device": (I, [P, P, P, I, I, SP]),
         "hprmat_b200_solve_rmatrix": (I, [P, DP, DP, I, I, D, DP, SP]),

@@ -98,8 +98,40 @@ class Context:
             self.rmat_ini(nr, ns, rmax)
 
     # -- rmatrix ----------------------------------------------------------------
-    def rmatrix(self, nch, lval, qk, eta, rmax, nr, ns, cpot, ndim=None, allow_unconverged=False):
-        """Collision matrix ``cu`` (ndim x ndim, U in cu[:nopen, :nopen]) and ``nopen``."""
+    def _full(self, nch, lval, qk, eta, rmax, nr, ns, cpot, ndim, nvc, cpnl, allow_unconverged):
+        """hprmat_b200_rmatrix_full: wave functions when nvc is given, non-local cpnl if given."""
+        self._ensure_mesh(nr, ns, rmax)
+        lval = np.ascontiguousarray(lval, dtype=np.int32)
+        qk = np.ascontiguousarray(qk, dtype=np.float64)
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        cpot = np.asfortranarray(cpot, dtype=np.complex128)
+        ncp1 = cpot.shape[0]
+        ndim = int(ndim or cpot.shape[1])
+        cu = np.zeros((ndim, ndim), dtype=np.complex128, order="F")
+        twf = nvc is not None
+        nvc_a = np.ascontiguousarray(nvc if twf else [1], dtype=np.int32)
+        cf = np.zeros((nr * ns, nch, len(nvc_a)) if twf else (1, 1, 1), dtype=np.complex128, order="F")
+        if cpnl is not None:
+            cpnl = np.asfortranarray(cpnl, dtype=np.complex128)
+            ncp2, nl_ptr = cpnl.shape[0], _dptr(cpnl)
+        else:
+            ncp2, nl_ptr = 0, None
+        nopen = ctypes.c_int(0)
+        st = Stats()
+        s = self._lib.hprmat_b200_rmatrix_full(self._h, int(nch), _iptr(lval), _dptr(qk), _dptr(eta), float(rmax),
+                                               int(nr), int(ns), _dptr(cpot), int(ncp1), ndim, _dptr(cu),
+                                               ctypes.byref(nopen), int(twf), _dptr(cf), cf.shape[0], cf.shape[1],
+                                               len(nvc_a), _iptr(nvc_a), int(ncp2), nl_ptr, ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
+        return cu, nopen.value, (cf if twf else None)
+
+    def rmatrix(self, nch, lval, qk, eta, rmax, nr, ns, cpot, ndim=None, allow_unconverged=False, cpnl=None):
+        """Collision matrix ``cu`` (ndim x ndim, U in cu[:nopen, :nopen]) and ``nopen``.
+        ``cpnl``: non-local potential (ncp2 >= nr^2, nch, nch), one interval only."""
+        if cpnl is not None:
+            cu, nopen, _ = self._full(nch, lval, qk, eta, rmax, nr, ns, cpot, ndim, None, cpnl, allow_unconverged)
+            return cu, nopen
         self._ensure_mesh(nr, ns, rmax)
         lval = np.ascontiguousarray(lval, dtype=np.int32)
         qk = np.ascontiguousarray(qk, dtype=np.float64)
@@ -174,11 +206,14 @@ class Context:
         nat.check(s)
         return cu, nopen.value, grad
 
-    def rmatrix_wf(self, nch, lval, qk, eta, rmax, nr, ns, cpot, nvc=(1,), ndim=None, allow_unconverged=False):
+    def rmatrix_wf(self, nch, lval, qk, eta, rmax, nr, ns, cpot, nvc=(1,), ndim=None, allow_unconverged=False,
+                   cpnl=None):
         """Collision matrix and internal wave functions (rmatrix with twf = .true.).  ``nvc``:
         entrance channels, 1-based among the open channels.  Returns (cu, nopen, cf) with cf
         complex (nr*ns, nch, len(nvc)) at the mesh points and the closed-channel amplitudes in
-        cu[nopen:, ic]."""
+        cu[nopen:, ic].  ``cpnl``: non-local potential as in ``rmatrix``."""
+        if cpnl is not None:
+            return self._full(nch, lval, qk, eta, rmax, nr, ns, cpot, ndim, list(nvc), cpnl, allow_unconverged)
         self._ensure_mesh(nr, ns, rmax)
         lval = np.ascontiguousarray(lval, dtype=np.int32)
         qk = np.ascontiguousarray(qk, dtype=np.float64)
@@ -338,6 +373,15 @@ class RMatrixSolver:
         lval = np.asarray(lval, dtype=np.int32)
         nvc = [1] if entrance_channels is None else list(entrance_channels)
         cu, nopen, cf = self.ctx.rmatrix_wf(len(lval), lval, qk, eta, self.rmax, self.nr, self.ns, cpot, nvc)
+        return cu, cf, nopen
+
+    def solve_nonlocal(self, lval, qk, eta, cpot, cpnl, entrance_channels=None, solver=None):
+        """(cu, cf, nopen) with a non-local potential cpnl (nr*nr, nch, nch), as the reference
+        binding (bindings/python/hprmat.py:209-252)."""
+        lval = np.asarray(lval, dtype=np.int32)
+        nvc = [1] if entrance_channels is None else list(entrance_channels)
+        cu, nopen, cf = self.ctx.rmatrix_wf(len(lval), lval, qk, eta, self.rmax, self.nr, self.ns, cpot, nvc,
+                                            cpnl=cpnl)
         return cu, cf, nopen
 
     def interpolate_wavefunction(self, lval, qk, eta, cu, cf, nopen, channel, entrance, npoin, h=None):

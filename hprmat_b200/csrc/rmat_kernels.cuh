@@ -28,6 +28,16 @@ struct MeshDev {
   int nq1;
 };
 
+// Non-local potential of an rmatrix call (src/rmatrix_hp.F90:283-288): block (c, c') of C(E)
+// gains sqrt(w_i w_j) rmax0 cpnl(i nr + j, c, c'), cpnl complex (ncp2, ndim, ndim).  p = nullptr:
+// local potentials only.
+struct NonLocalDev {
+  const double2* p = nullptr;
+  long ncp2 = 0, ndim = 0;
+  const double* wle = nullptr;  // Gauss-Legendre weights (nr)
+  double rmax0 = 0.0;
+};
+
 // Right-hand side value at row (c, i), column col: blockdiag(q1) columns, then blockdiag(q2).
 __device__ __forceinline__ double surface_value(const MeshDev& m, int c, int i, int col) {
   if (col < m.nq1) return c == col ? m.q1[i] : 0.0;
@@ -58,15 +68,15 @@ struct Acc2 {
   __device__ __forceinline__ double value() const { return hi + lo; }
 };
 
-// C(E) of src/rmatrix_hp.F90:246-293 (one interval, local potentials):
+// C(E) of src/rmatrix_hp.F90:246-293 (one interval):
 //   channel block (c,c): tc + diag(l(l+1)/r^2 -+ k^2) - (xc/a) blo0 (closed channels)
-//   every block (c,c'):  + diag(cpot(r_i, c, c'))
+//   every block (c,c'):  + diag(cpot(r_i, c, c'))  [+ the non-local term, nl]
 // One thread per element, threads along rows (column-major, coalesced stores).  Writes T
 // (double2 or float2).
 // Also accumulates ||C||_F^2 (FP64) into *fro2 for the refinement's backward error.
 template <typename T>
 __global__ void assemble_kernel(MeshDev mesh, ChannelData ch, int nch, const double2* __restrict__ cpot,
-                                long ncp1, long ndim, T* W, long ld, int N, double* fro2) {
+                                long ncp1, long ndim, T* W, long ld, int N, double* fro2, NonLocalDev nl = {}) {
   // thread: one row; block: 256 rows of the columns blockIdx.y, blockIdx.y + gridDim.y, ...
   // (coalesced writes along the column), one atomic per block for ||C||_F^2
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
@@ -88,6 +98,12 @@ __global__ void assemble_kernel(MeshDev mesh, ChannelData ch, int nch, const dou
         double2 v = cpot[(size_t)i + ncp1 * ((size_t)c + ndim * (size_t)cp)];
         re += v.x;
         im += v.y;
+      }
+      if (nl.p) {
+        const double wf = sqrt(nl.wle[i] * nl.wle[j]) * nl.rmax0;
+        const double2 v = nl.p[(size_t)i * nr + j + nl.ncp2 * ((size_t)c + nl.ndim * (size_t)cp)];
+        re += wf * v.x;
+        im += wf * v.y;
       }
       T out;
       out.x = (typename RealOf<T>::R)re;

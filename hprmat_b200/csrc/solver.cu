@@ -1126,15 +1126,17 @@ static double ms_since(Clock::time_point t0) {
 // (src/rmatrix_hp.F90:246-293), factorised, and solved for its md.nq1 + nch surface right-hand
 // sides into X64 (ld ldx): FP64 LU and one solve, or the mixed LU with FP64 refinement.
 // d_cpot points at the interval's first mesh row.  Statistics of the interval in *stats.
+// With a non-local potential (nl.p set) C(E) has dense channel blocks: the refinement's FP64
+// operator is then a dense copy of C (A64) with a dense right-hand side (B64).
 static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData& chd, const MeshDev& md,
                           const double2* d_cpot, int ncp1, int ndim, double2* X64, long ld,
-                          hprmat_b200_stats* stats) {
+                          hprmat_b200_stats* stats, const NonLocalDev& nl) {
   const int nr = md.nr;
   const int N = nch * nr;
   const int nrhs = md.nq1 + nch;
   const bool mixed = c->opts.precision == HPRMAT_B200_PREC_MIXED;
   Operator op;
-  op.structured = true;
+  op.structured = nl.p == nullptr;
   op.mesh = md;
   op.ch = chd;
   op.nch = nch;
@@ -1162,10 +1164,24 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
   dim3 gr(cdiv_u(N, 256), nrhs);
   double* d_fro2 = reinterpret_cast<double*>(c->status.as<int>() + 32);
   HPR_CUDA_TRY(cudaMemsetAsync(d_fro2, 0, sizeof(double), c->stream));
+  if (!op.structured) {
+    TRY(c->A64.ensure((size_t)ld * N * sizeof(double2)));
+    TRY(c->B64.ensure((size_t)ld * nrhs * sizeof(double2)));
+    assemble_kernel<double2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, c->A64.as<double2>(), ld,
+                                                        N, d_fro2, nl);
+    LAUNCH_CHECK();
+    surface_rhs_kernel<double2><<<gr, 256, 0, c->stream>>>(md, c->B64.as<double2>(), ld, N, 1.0);
+    LAUNCH_CHECK();
+    op.A = c->A64.as<double2>();
+    op.lda = ld;
+    op.B = c->B64.as<double2>();
+    op.ldb = ld;
+    HPR_CUDA_TRY(cudaMemsetAsync(d_fro2, 0, sizeof(double), c->stream));
+  }
   if (!mixed) {
     TRY(c->W.ensure((size_t)ld * N * sizeof(double2)));
     double2* W = c->W.as<double2>();
-    assemble_kernel<double2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2);
+    assemble_kernel<double2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2, nl);
     LAUNCH_CHECK();
     surface_rhs_kernel<double2><<<gr, 256, 0, c->stream>>>(md, X64, ld, N, 1.0);
     LAUNCH_CHECK();
@@ -1191,7 +1207,7 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
   } else {
     TRY(c->W.ensure((size_t)ld * N * sizeof(float2)));
     float2* W = c->W.as<float2>();
-    assemble_kernel<float2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2);
+    assemble_kernel<float2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2, nl);
     LAUNCH_CHECK();
     int nb = pick_nb(c, N, sizeof(float2), 128);
     if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
@@ -1246,8 +1262,11 @@ struct WfRequest {
 
 static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const double* qk, const double* eta,
                         double rmax, int nr, int ns, const double2* d_cpot, int ncp1, int ndim, double2* d_cu,
-                        int* nopen, hprmat_b200_stats* stats, const WfRequest* wf = nullptr) {
+                        int* nopen, hprmat_b200_stats* stats, const WfRequest* wf = nullptr,
+                        const double2* d_cpnl = nullptr, int ncp2 = 0) {
   auto t_all = Clock::now();
+  if (d_cpnl && (ns != 1 || ncp2 < nr * nr))
+    return fail(HPRMAT_B200_ERR_ARG, "rmatrix: non-local potentials need ns = 1 and ncp2 >= nr*nr");
   if (nch <= 0 || nr <= 0 || ns <= 0 || !lval || !qk || !eta || !d_cpot || !d_cu || !nopen)
     return fail(HPRMAT_B200_ERR_ARG, "rmatrix: invalid arguments");
   if (wf && (wf->nc <= 0 || !wf->nvc || !wf->d_cf || wf->nwf1 < (long)nr * ns || wf->nwf2 < nch || wf->nc > ndim))
@@ -1341,7 +1360,15 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
     memset(&si, 0, sizeof(si));
     si.rel_residual = -1.0;
     si.surface_change = -1.0;
-    const int s = interval_solve(c, is, nch, chd, md, d_cpot + (size_t)is * nr, ncp1, ndim, X64, ld, &si);
+    NonLocalDev nl;
+    if (d_cpnl) {
+      nl.p = d_cpnl;
+      nl.ncp2 = ncp2;
+      nl.ndim = ndim;
+      nl.wle = mesh_wle(c);
+      nl.rmax0 = rmax0;
+    }
+    const int s = interval_solve(c, is, nch, chd, md, d_cpot + (size_t)is * nr, ncp1, ndim, X64, ld, &si, nl);
     if (stats) {
       stats->info = si.info;
       stats->nb = si.nb;
@@ -1805,6 +1832,54 @@ int hprmat_b200_rmatrix_wf(hprmat_b200_ctx* c, int nch, const int* lval, const d
 // Complex value i of a caller's interleaved complex array, read as two doubles: a Fortran
 // complex*16 array need not be 16-byte aligned.
 static inline double2 host_c(const double* p, size_t i) { return mk(p[2 * i], p[2 * i + 1]); }
+
+int hprmat_b200_rmatrix_full(hprmat_b200_ctx* c, int nch, const int* lval, const double* qk, const double* eta,
+                             double rmax, int nr, int ns, const double* cpot, int ncp1, int ndim, double* cu,
+                             int* nopen, int twf, double* cf, int nwf1, int nwf2, int nc, const int* nvc, int ncp2,
+                             const double* cpnl, hprmat_b200_stats* stats) {
+  TRY(check_ctx(c));
+  if (!cpot || !cu || ndim <= 0 || ncp1 <= 0 || (twf && (!cf || nc <= 0 || nwf1 <= 0 || nwf2 <= 0)) ||
+      (ncp2 > 0 && !cpnl) || ncp2 < 0)
+    return fail(HPRMAT_B200_ERR_ARG, "rmatrix_full: invalid arguments");
+  const size_t pbytes = (size_t)ncp1 * ndim * ndim * sizeof(double2);
+  const size_t ubytes = (size_t)ndim * ndim * sizeof(double2);
+  const size_t nlbytes = (size_t)ncp2 * ndim * ndim * sizeof(double2);
+  const size_t fbytes = twf ? (size_t)nwf1 * nwf2 * nc * sizeof(double2) : 0;
+  TRY(c->cpot.ensure(pbytes + nlbytes));
+  TRY(c->cu.ensure(ubytes));
+  if (twf) TRY(c->wfcf.ensure(fbytes));
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->cpot.p, cpot, pbytes, cudaMemcpyHostToDevice, c->stream));
+  const double2* d_cpnl = nullptr;
+  if (ncp2 > 0) {
+    d_cpnl = c->cpot.as<double2>() + (size_t)ncp1 * ndim * ndim;
+    HPR_CUDA_TRY(cudaMemcpyAsync((void*)d_cpnl, cpnl, nlbytes, cudaMemcpyHostToDevice, c->stream));
+  }
+  WfRequest wf;
+  if (twf) {
+    wf.nc = nc;
+    wf.nvc = nvc;
+    wf.d_cf = c->wfcf.as<double2>();
+    wf.nwf1 = nwf1;
+    wf.nwf2 = nwf2;
+  }
+  int s = rmatrix_core(c, nch, lval, qk, eta, rmax, nr, ns, c->cpot.as<double2>(), ncp1, ndim, c->cu.as<double2>(),
+                       nopen, stats, twf ? &wf : nullptr, d_cpnl, ncp2);
+  if (s == HPRMAT_B200_OK || s == HPRMAT_B200_NOT_CONVERGED) {
+    HPR_CUDA_TRY(cudaMemcpyAsync(cu, c->cu.p, ubytes, cudaMemcpyDeviceToHost, c->stream));
+    if (twf) {
+      const size_t pitch = (size_t)nwf1 * sizeof(double2);
+      for (int ic = 0; ic < nc; ++ic) {
+        const size_t off = (size_t)ic * nwf1 * nwf2;
+        HPR_CUDA_TRY(cudaMemcpy2DAsync(reinterpret_cast<double2*>(cf) + off, pitch, c->wfcf.as<double2>() + off,
+                                       pitch, (size_t)nr * ns * sizeof(double2), nch, cudaMemcpyDeviceToHost,
+                                       c->stream));
+      }
+    }
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
+  if (stats) stats->status = s;
+  return s;
+}
 
 // Natural cubic spline through (x, y), n >= 2: second derivatives y2 by the tridiagonal
 // (Thomas) elimination of the spline's continuity equations with y2 = 0 at both ends.

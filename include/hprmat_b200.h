@@ -158,6 +158,18 @@ int hprmat_b200_rmatrix_wf(hprmat_b200_ctx* ctx, int nch, const int* lval, const
                            int ncp1, int ndim, double* cu, int* nopen, int nc, const int* nvc,
                            double* cf, int nwf1, int nwf2, hprmat_b200_stats* stats);
 
+/* The complete argument list of rmatrix (src/rmatrix_hp.F90:175-186, host buffers): twf != 0
+   adds the wave functions (cf, nwf1, nwf2, nc, nvc as hprmat_b200_rmatrix_wf); ncp2 > 0 adds the
+   non-local potential cpnl, complex (ncp2, ndim, ndim) with ncp2 >= nr*nr: channel block
+   (c, c') of C(E) gains sqrt(w_i w_j) a cpnl((i-1) nr + j, c, c') (:283-288), one interval only
+   (ns = 1, as :205-209).  With a non-local potential the FP64 refinement multiplies by a dense
+   FP64 copy of C(E) (N^2 complex doubles on the device). */
+int hprmat_b200_rmatrix_full(hprmat_b200_ctx* ctx, int nch, const int* lval, const double* qk,
+                             const double* eta, double rmax, int nr, int ns, const double* cpot,
+                             int ncp1, int ndim, double* cu, int* nopen, int twf, double* cf, int nwf1,
+                             int nwf2, int nc, const int* nvc, int ncp2, const double* cpnl,
+                             hprmat_b200_stats* stats);
+
 /* Same with cpot, cu and cf in device memory. */
 int hprmat_b200_rmatrix_wf_device(hprmat_b200_ctx* ctx, int nch, const int* lval, const double* qk,
                                   const double* eta, double rmax, int nr, int ns, const void* d_cpot,

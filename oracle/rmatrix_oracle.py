@@ -201,8 +201,10 @@ def boundary_values(nch, lval, qk, eta, rmax) -> Boundary:
                     np.array(cop, dtype=np.complex128), xc)
 
 
-def assemble(mesh: Mesh, is_: int, nch, lval, qk, xc, cpot) -> np.ndarray:
-    """C(E) of interval ``is_`` (1-based), src/rmatrix_hp.F90:246-293 (local potentials)."""
+def assemble(mesh: Mesh, is_: int, nch, lval, qk, xc, cpot, cpnl=None) -> np.ndarray:
+    """C(E) of interval ``is_`` (1-based), src/rmatrix_hp.F90:246-293.  ``cpnl`` (ncp2 >= nr^2,
+    ndim, ndim): non-local potential, block (c, c') gains sqrt(w_i w_j) rmax0 cpnl(i nr + j, c, c')
+    (0-based i, j; :283-288, one interval)."""
     nr = mesh.nr
     rmax0 = mesh.rmax0
     rmax1 = (is_ - 1) * rmax0
@@ -232,6 +234,10 @@ def assemble(mesh: Mesh, is_: int, nch, lval, qk, xc, cpot) -> np.ndarray:
             m2 = i2 * nr
             idx = np.arange(nr)
             ch[m1 + idx, m2 + idx] += cpot[ms + idx, i1, i2]
+            if cpnl is not None:
+                ii0 = (is_ - 1) * nr * nr
+                nl = cpnl[ii0:ii0 + nr * nr, i1, i2].reshape(nr, nr)  # row i, column j
+                ch[m1:m1 + nr, m2:m2 + nr] += np.sqrt(np.outer(mesh.wle, mesh.wle)) * rmax0 * nl
     return ch
 
 
@@ -350,8 +356,11 @@ class RMatrixResult:
     x: np.ndarray | None  # solution of the ns = 1 solve, (N, nch)
 
 
-def rmatrix(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, solver: str = "dense") -> RMatrixResult:
-    """Collision matrix for one (J, pi, E), src/rmatrix_hp.F90:175-368 (local potentials)."""
+def rmatrix(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, solver: str = "dense", cpnl=None) -> RMatrixResult:
+    """Collision matrix for one (J, pi, E), src/rmatrix_hp.F90:175-368; ``cpnl``: non-local
+    potential (ns = 1 only, :205-209)."""
+    if cpnl is not None and mesh.ns != 1:
+        raise ValueError("ns must be ns=1 for non-local potentials")
     lval = np.asarray(lval)
     qk = np.asarray(qk, dtype=np.float64)
     eta = np.asarray(eta, dtype=np.float64)
@@ -362,7 +371,7 @@ def rmatrix(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, solver: str = "dense") -
     for is_ in range(1, ns + 1):
         rmax1 = (is_ - 1) * mesh.rmax0
         rmax2 = is_ * mesh.rmax0
-        ch = assemble(mesh, is_, nch, lval, qk, bnd.xc, cpot)
+        ch = assemble(mesh, is_, nch, lval, qk, bnd.xc, cpot, cpnl)
         bvec = mesh.q2[:, is_ - 1].astype(np.complex128)
         if solver == "dense":
             r11, x_last = solve_rmatrix_dense(ch, bvec, nch, nr)
@@ -383,7 +392,7 @@ def rmatrix(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, solver: str = "dense") -
     return RMatrixResult(cu, bnd.nopen, crma0_prev, bnd, x_last if ns == 1 else None)
 
 
-def rmatrix_wf(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, nvc, u=None):
+def rmatrix_wf(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, nvc, u=None, cpnl=None):
     """U and the internal wave functions (rmatrix with twf = .true., src/rmatrix_hp.F90:378-431).
 
     ``nvc``: entrance channels, 1-based indices among the open channels.  Per interval the
@@ -413,7 +422,7 @@ def rmatrix_wf(nch, lval, qk, eta, rmax, mesh: Mesh, cpot, nvc, u=None):
     for is_ in range(1, ns + 1):
         s = is_ - 1
         rmax1, rmax2 = (is_ - 1) * rmax0, is_ * rmax0
-        ch = assemble(mesh, is_, nch, lval, qk, bnd.xc, cpot)
+        ch = assemble(mesh, is_, nch, lval, qk, bnd.xc, cpot, cpnl)
         q1, q2 = mesh.q1[:, s], mesh.q2[:, s]
         rhs = np.zeros((n, 2 * nch), dtype=np.complex128, order="F")
         for c in range(nch):

@@ -118,3 +118,21 @@ def ex3_setup(zrma, j):
 def ex4_setup(zrma, j):
     """12C + alpha (examples/Ex4/example4_hp.f90:37-133): three states of 12C, closed channels."""
     return _deformed_setup(zrma, j, 12, 4, 6, 2, [0, 2, 4], [0.0, 4.44, 14.08], 110, 20, 1.2, 0.5, 2, 0.58, 0)
+
+
+def ex5_setup(zrma):
+    """Yamaguchi's separable non-local potential (rmat_pierre/Ex5/example5.f:12-41), one s-wave
+    channel, no Coulomb: cpot = 0 and cpnl((i-1) nr + j) = -2 beta (alpha + beta)^2
+    exp(-beta (r_i + r_j)) in fm^-2 (hbar^2/2mu = 41.472 MeV fm^2)."""
+    hm, al, be = 41.472, 0.2316053, 1.3918324
+    nr = len(zrma)
+    r = np.asarray(zrma)
+    cpot = np.zeros((nr, 1, 1), dtype=np.complex128, order="F")
+    cpnl = np.zeros((nr * nr, 1, 1), dtype=np.complex128, order="F")
+    cpnl[:, 0, 0] = (-2 * be * (al + be) ** 2 * np.exp(-be * (r[:, None] + r[None, :]))).reshape(-1)
+
+    def kin(e):
+        qk = math.sqrt(e / hm)
+        return np.array([0], np.int32), np.array([qk]), np.array([0.0])
+
+    return cpot, cpnl, kin

@@ -6,9 +6,9 @@ Run in a container that has the HPRMAT sources mounted (read-only) at
     python tests/golden/make_golden.py [/root/reference]
 
 It reads Descouvemont's example inputs and printed outputs,
-``rmat_pierre/Ex{1,2,3,4}/data*`` and ``rmat_pierre/Ex{1,2,3,4}/output*.txt`` (the files the
+``rmat_pierre/Ex{1,2,3,4,5}/data*`` and ``rmat_pierre/Ex{1,2,3,4,5}/output*.txt`` (the files the
 HPRMAT README compares its solvers against, README.md:113-121), the wave functions the drivers
-write for their rmax < 0 card (``rmat_pierre/Ex{1,2,3,4}/wf*.txt``) and Ex3's wf_print output,
+write for their rmax < 0 card (``rmat_pierre/Ex{1,2,3,4,5}/wf*.txt``) and Ex3's wf_print output,
 and writes ``tests/golden/reference_examples.json``.  Nothing else is transformed: the numbers are
 the printed 5-significant-digit values.  The physics inputs of each example (potential
 forms, masses, charges) are restated by the tests from the example drivers
@@ -50,6 +50,28 @@ def parse_data(path, with_print_mesh=False):
                 break
             energies.append((ne, e0, es))
         cards.append({"j": j, "nr": nr, "ns": ns, "rmax": rmax, "energies": energies, **extra})
+    return cards
+
+
+def parse_data_ex5(path):
+    """Ex5 cards: (nr, rmax) then (ne, e0, estep) lines; l = 0, ns = 1 in the driver."""
+    cards = []
+    with open(path) as f:
+        lines = [ln.split("!")[0].split() for ln in f if ln.strip()]
+    i = 0
+    while i < len(lines):
+        nr, rmax = int(lines[i][0]), float(lines[i][1])
+        if nr == 0:
+            break
+        i += 1
+        energies = []
+        while i < len(lines):
+            ne, e0, es = int(lines[i][0]), float(lines[i][1]), float(lines[i][2])
+            i += 1
+            if ne == 0:
+                break
+            energies.append((ne, e0, es))
+        cards.append({"j": 0, "nr": nr, "ns": 1, "rmax": rmax, "energies": energies})
     return cards
 
 
@@ -128,16 +150,20 @@ def parse_fixed_step(path):
 
 
 def main(ref):
-    out = {"source": "rmat_pierre/Ex{1,2,3,4}/output*.txt, wf*.txt and data* of HPRMAT", "examples": {}}
+    out = {"source": "rmat_pierre/Ex{1,2,3,4,5}/output*.txt, wf*.txt and data* of HPRMAT", "examples": {}}
     spec = {
         "ex1": ("Ex1", "data1", "output1.txt", ["Collision matrix="]),
         "ex2": ("Ex2", "data2", "output2.txt", ["phase shift (rad.)="]),
         "ex3": ("Ex3", "data3", "output3.txt", ["Amplitude=", "phase shift (rad.)="]),
         "ex4": ("Ex4", "data4", "output4.txt", ["Amplitude=", "phase shift (rad.)="]),
+        "ex5": ("Ex5", "data5", "output5.txt", ["phase shift (deg.)="]),
     }
     out["wavefunctions"] = {}
     for name, (d, data, outp, keys) in spec.items():
-        cards = parse_data(os.path.join(ref, "rmat_pierre", d, data), with_print_mesh=(name == "ex3"))
+        if name == "ex5":
+            cards = parse_data_ex5(os.path.join(ref, "rmat_pierre", d, data))
+        else:
+            cards = parse_data(os.path.join(ref, "rmat_pierre", d, data), with_print_mesh=(name == "ex3"))
         wf = os.path.join(ref, "rmat_pierre", d, "wf" + name[-1] + ".txt")
         if os.path.exists(wf):
             # written by the card with rmax < 0 (twf = .true. in the drivers)

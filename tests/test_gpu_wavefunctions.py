@@ -2,7 +2,8 @@
 
 The device builds the internal wave functions from the per-interval solutions of the R-matrix
 step (C^-1 of the propagated surface amplitudes).  Every example card that writes wave
-functions (rmat_pierre/Ex{1,2,3,4}/wf*.txt, ns = 2 to 5, Ex4 with closed channels) is checked
+functions (rmat_pierre/Ex{1,2,3,4,5}/wf*.txt, ns = 1 to 5, Ex4 with closed channels, Ex5 with
+Yamaguchi's non-local potential) is checked
 at both precisions: U against the oracle to 1e-10; cf and the closed-channel amplitudes
 against the oracle's reconstruction from the device's U to 1e-10 (relative, per entrance
 channel) -- where |U| ~ 1 under a barrier (Ex1: |cop| ~ 1e7) the small components of the
@@ -38,14 +39,14 @@ def ctx():
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("name", sorted(GOLD["wavefunctions"]))
 def test_wave_functions_against_oracle_and_golden(ctx, precision, name):
-    mesh, rmax, cpot, kin, nv, blocks = wf_case(name)
+    mesh, rmax, cpot, kin, nv, blocks, cpnl = wf_case(name)
     ctx.set_precision(precision)
     for b in blocks:
         lval, qk, eta = kin(b["E"])
-        cu, nopen, cf = ctx.rmatrix_wf(nv, lval, qk, eta, rmax, mesh.nr, mesh.ns, cpot, [1])
-        u_ref = orc.rmatrix(nv, lval, qk, eta, rmax, mesh, cpot).cu
+        cu, nopen, cf = ctx.rmatrix_wf(nv, lval, qk, eta, rmax, mesh.nr, mesh.ns, cpot, [1], cpnl=cpnl)
+        u_ref = orc.rmatrix(nv, lval, qk, eta, rmax, mesh, cpot, cpnl=cpnl).cu
         assert _rel(cu[:nopen, :nopen], u_ref) <= TOL, (name, b["E"], ctx.last_stats)
-        cu_ref, no_ref, cf_ref = orc.rmatrix_wf(nv, lval, qk, eta, rmax, mesh, cpot, [1], u=cu)
+        cu_ref, no_ref, cf_ref = orc.rmatrix_wf(nv, lval, qk, eta, rmax, mesh, cpot, [1], u=cu, cpnl=cpnl)
         assert nopen == no_ref
         assert _rel(cf[:, :, 0], cf_ref[:, :, 0]) <= TOL, (name, b["E"], ctx.last_stats)
         assert _rel(cu[:nv, 0], cu_ref[:, 0]) <= TOL, (name, b["E"])
@@ -91,7 +92,7 @@ def test_ex3_wf_print_on_device_result(ctx):
     HPRMAT's natural one, and the device result is compared with the oracle's natural spline."""
     c = GOLD["examples"]["ex3"][3]
     nr, ns, rmax = c["nr"], c["ns"], abs(c["rmax"])
-    mesh, _, cpot, kin, nv, _ = wf_case("ex3")
+    mesh, _, cpot, kin, nv, _, _ = wf_case("ex3")
     ctx.set_precision("mixed")
     for b in GOLD["fixed_step"]["ex3"]:
         lval, qk, eta = kin(b["E"])
@@ -113,7 +114,7 @@ def test_ex3_wf_print_on_device_result(ctx):
 
 
 def test_bad_entrance_channel(ctx):
-    mesh, rmax, cpot, kin, nv, blocks = wf_case("ex4")
+    mesh, rmax, cpot, kin, nv, blocks, _ = wf_case("ex4")
     lval, qk, eta = kin(blocks[0]["E"])
     nopen = int((qk > 0).sum())
     with pytest.raises(api.HprmatError):

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 from oracle import rmatrix_oracle as orc
-from tests.example_inputs import ex1_setup, ex2_setup, ex3_setup, ex4_setup
+from tests.example_inputs import ex1_setup, ex2_setup, ex3_setup, ex4_setup, ex5_setup
 from oracle.special_functions import coulfg, whit
 
 GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_examples.json")))
@@ -93,21 +93,41 @@ def test_ex3_amplitudes(card):
             assert abs(x - ref) <= 1.2e-4 * max(abs(ref), 1.0), (rp["E"], x, ref)
 
 
+@pytest.mark.parametrize("card", range(len(GOLD["examples"]["ex5"])))
+def test_ex5_nonlocal_phase_shifts(card):
+    """Yamaguchi's non-local potential (full nr x nr block term of rmatrix_hp.F90:283-288)."""
+    c = GOLD["examples"]["ex5"][card]
+    nr, rmax = c["nr"], abs(c["rmax"])
+    mesh = orc.rmat_ini(nr, 1, rmax)
+    cpot, cpnl, kin = ex5_setup(mesh.zrma)
+    for row in c["printed"]["phase shift (deg.)="]:
+        lval, qk, eta = kin(row["E"])
+        u = orc.rmatrix(1, lval, qk, eta, rmax, mesh, cpot, cpnl=cpnl).cu[0, 0]
+        delta = math.atan2(u.imag, u.real) / 2 * 180 / math.pi
+        assert _printed_close(delta, row["values"][0]), (row["E"], delta, row["values"])
+        assert _printed_close(abs(u), row["values"][1]), (row["E"], abs(u))
+
+
 def wf_case(name):
-    """(mesh, rmax, cpot, kin, nch, blocks) of the wave-function card of example ``name``."""
+    """(mesh, rmax, cpot, kin, nch, blocks, cpnl) of the wave-function card of example ``name``
+    (cpnl: the non-local potential of Ex5, else None)."""
     wf = GOLD["wavefunctions"][name]
     c = GOLD["examples"][name][wf["card"]]
     nr, ns, rmax = c["nr"], c["ns"], abs(c["rmax"])
     mesh = orc.rmat_ini(nr, ns, rmax)
+    cpnl = None
     if name == "ex1":
         cpot, k1 = ex1_setup(mesh.zrma)
         kin, nv = (lambda e: k1(e, c["j"])), 1
+    elif name == "ex5":
+        cpot, cpnl, kin = ex5_setup(mesh.zrma)
+        nv = 1
     elif name == "ex2":
         cpot, kin = ex2_setup(mesh.zrma, c["j"])
         nv = 2
     else:
         cpot, kin, nv = (ex3_setup if name == "ex3" else ex4_setup)(mesh.zrma, c["j"])
-    return mesh, rmax, cpot, kin, nv, wf["blocks"]
+    return mesh, rmax, cpot, kin, nv, wf["blocks"], cpnl
 
 
 def _close_in_channel(got, ref, rel=6e-5, floor=1e-3):
@@ -122,10 +142,10 @@ def test_wave_functions_internal_and_external(name):
     """Internal wave functions at the mesh points (C^-1 of the surface amplitudes) and the
     external Coulomb/Whittaker forms at r = zrma(nr ns) + 0.2 i, as the drivers print them
     (rmat_pierre/Ex*/example*.f, wave_functions.txt)."""
-    mesh, rmax, cpot, kin, nv, blocks = wf_case(name)
+    mesh, rmax, cpot, kin, nv, blocks, cpnl = wf_case(name)
     for b in blocks:
         lval, qk, eta = kin(b["E"])
-        cu, no, cf = orc.rmatrix_wf(nv, lval, qk, eta, rmax, mesh, cpot, [1])
+        cu, no, cf = orc.rmatrix_wf(nv, lval, qk, eta, rmax, mesh, cpot, [1], cpnl=cpnl)
         ref = np.array(b["internal"])
         np.testing.assert_allclose(ref[:, 0], mesh.zrma, atol=6e-4)
         refc = ref[:, 1::2] + 1j * ref[:, 2::2]
