@@ -53,6 +53,9 @@ def parse():
                          "scan, 12 J-pi blocks x 256 energies (3072 solves) per step; adjoint: loss and gradients "
                          "over 64 energies at N = 3200 per step")
     ap.add_argument("--workers", type=int, default=4, help="worker streams of the batched scan")
+    ap.add_argument("--reuse", type=int, default=1,
+                    help="scan/adjoint: keep a block's factorisation across energies as the refinement's "
+                         "preconditioner (opts.reuse_factors); 0 factorises every energy")
     return ap.parse_args()
 
 
@@ -188,10 +191,13 @@ def run_scan(args):
         inputs.append((w.lval, w.cpot, np.array([k[0] for k in ks]), np.array([k[1] for k in ks])))
         flops += len(energies) * 8.0 * float(w.n) ** 3 / 3.0
     nunits = sum(len(e) for _, e in mine)
-    ctx = api.Context(device=local, precision="mixed", max_refine=3, tol=1e-12)
+    ctx = api.Context(device=local, precision="mixed", max_refine=3, tol=1e-12, reuse_factors=bool(args.reuse))
+    from hprmat_b200 import _native as nat
+    lib = nat.load()
     for _ in range(args.warmup):
         ctx.rmatrix_scan(inputs[:1], 20.0, 60, nworkers=args.workers, allow_unconverged=True,
                          raise_on_unit_error=False)
+    lib.hprmat_b200_dev_factorizations(ctx._h, 1)
     secs = []
     res = None
     for _ in range(args.steps):
@@ -211,6 +217,7 @@ def run_scan(args):
         dist.all_reduce(tot_flops)
     wall = float(t_local.item())
     value = float(tot_units.item()) * args.steps / wall
+    nfact = int(lib.hprmat_b200_dev_factorizations(ctx._h, 1)) / max(1, args.steps)
     # sampled accuracy: the largest and smallest block at their first and last energy, vs the oracle
     errs = []
     mesh = orc.rmat_ini(60, 1, 20.0)
@@ -251,8 +258,9 @@ def run_scan(args):
             "data": "synthetic (seeded scan generator, hprmat_b200/workloads.py)",
             "config": {"workload": "batched energy scan: 12 J-pi blocks, nch ~ U{4..64} x 60 points "
                                    "(N = 240..3840), 256 energies each, 3072 solves",
-                       "workers": args.workers},
-            "complex_tflops": float(tot_flops.item()) * args.steps / wall / 1e12,
+                       "workers": args.workers, "reuse_factors": bool(args.reuse)},
+            "lu_equivalent_complex_tflops": float(tot_flops.item()) * args.steps / wall / 1e12,
+            "factorizations_per_step": nfact,
             "units_failed": bad, "units_failed_note": "COULFG ifail=-5 (high-l channels just above threshold); "
                                                       "the oracle fails on the same units",
             "units_not_converged": unconverged,
@@ -280,7 +288,9 @@ def run_adjoint(args):
     coup = torch.from_numpy(w.coupling)
     p0 = torch.tensor(w.params.as_array(), dtype=torch.float64)
     ptarget = p0 * torch.tensor([1.02, 0.97, 1.01, 1.03, 0.95, 1.04], dtype=torch.float64)
-    ctx = api.Context(precision="mixed", max_refine=8, tol=1e-12)
+    ctx = api.Context(precision="mixed", max_refine=8, tol=1e-12, reuse_factors=bool(args.reuse))
+    from hprmat_b200 import _native as nat
+    lib = nat.load()
     # energies where COULFG (the reference's algorithm) cannot evaluate an open channel just above
     # its threshold are dropped (the oracle fails on them too)
     from oracle import special_functions as sf
@@ -307,6 +317,7 @@ def run_adjoint(args):
         L, _ = loss(p)
         L.backward()
     times = []
+    lib.hprmat_b200_dev_factorizations(ctx._h, 1)
     for _ in range(args.steps):
         t = time.perf_counter()
         p = p0.clone().requires_grad_(True)
@@ -314,6 +325,7 @@ def run_adjoint(args):
         cp.retain_grad()
         L.backward()
         times.append(time.perf_counter() - t)
+    nfact = int(lib.hprmat_b200_dev_factorizations(ctx._h, 1)) / max(1, args.steps)
     g = p.grad.numpy().copy()
     # central finite differences of the device forward, step 1e-6 (relative to the parameter)
     fd_err = 0.0
@@ -343,7 +355,7 @@ def run_adjoint(args):
         "config": {"workload": "adjoint: 32 channels x 100 points (N = 3200), 64 energies, loss sum |U - U_target|^2, "
                                "gradients w.r.t. 6 potential parameters and the potential at all mesh points"},
         "energies_used": len(kin), "energies_dropped_coulfg": len(kin_all) - len(kin),
-        "solves_per_step": 3 * len(kin),
+        "solves_per_step": 2 * len(kin), "factorizations_per_step": nfact, "reuse_factors": bool(args.reuse),
         "fd_rel_err_max": fd_err, "fd_step": 1e-6, "oracle_grad_rel_err_max": ref_err,
         "loss": float(L.detach())}))
     ctx.close()

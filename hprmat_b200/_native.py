@@ -34,17 +34,19 @@ EXPORTED = (
     "hprmat_b200_last_error", "hprmat_b200_version", "hprmat_b200_boundary",
     "hprmat_b200_solve_linear_noalloc", "hprmat_b200_rmatrix_scan",
     "hprmat_b200_rmatrix_adjoint", "hprmat_b200_rmatrix_wf", "hprmat_b200_rmatrix_wf_device",
-    "hprmat_b200_wf_print", "hprmat_b200_rmatrix_full",
+    "hprmat_b200_wf_print", "hprmat_b200_rmatrix_full", "hprmat_b200_rmatrix_x", "hprmat_b200_adjoint_from_x",
     # include/hprmat_b200_dev.h
     "hprmat_b200_dev_tc_update", "hprmat_b200_dev_split_planes", "hprmat_b200_dev_set_profile",
     "hprmat_b200_dev_counters", "hprmat_b200_dev_wave_trace", "hprmat_b200_dev_wave_trace_read",
     "hprmat_b200_dev_panel_trace_read", "hprmat_b200_dev_set_tuning", "hprmat_b200_dev_mesh",
+    "hprmat_b200_dev_factorizations",
 )
 
 
 class Opts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("max_refine", ctypes.c_int), ("tol", ctypes.c_double),
-                ("surface_tol", ctypes.c_double), ("panel_nb", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
+                ("surface_tol", ctypes.c_double), ("panel_nb", ctypes.c_int), ("reuse_factors", ctypes.c_int),
+                ("reserved", ctypes.c_int * 3)]
 
 
 class Stats(ctypes.Structure):
@@ -54,7 +56,8 @@ class Stats(ctypes.Structure):
                 ("residual_floor", ctypes.c_double), ("floor_history", ctypes.c_double * 9),
                 ("residual_history", ctypes.c_double * 9),
                 ("ms_assemble", ctypes.c_double), ("ms_factor", ctypes.c_double), ("ms_solve", ctypes.c_double),
-                ("ms_refine", ctypes.c_double), ("ms_umatrix", ctypes.c_double), ("ms_total", ctypes.c_double)]
+                ("ms_refine", ctypes.c_double), ("ms_umatrix", ctypes.c_double), ("ms_total", ctypes.c_double),
+                ("factorizations", ctypes.c_int), ("reserved_stats", ctypes.c_int)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("residual_history", "floor_history")}
@@ -105,6 +108,8 @@ def load():
         "hprmat_b200_rmatrix_wf": (I, [P, I, IP, DP, DP, D, I, I, DP, I, I, DP, IP, I, IP, DP, I, I, SP]),
         "hprmat_b200_rmatrix_wf_device": (I, [P, I, IP, DP, DP, D, I, I, P, I, I, P, IP, I, IP, P, I, I, SP]),
         "hprmat_b200_wf_print": (I, [I, IP, DP, DP, D, I, I, DP, I, I, DP, I, I, DP, I, I, I, D, DP]),
+        "hprmat_b200_rmatrix_x": (I, [P, I, IP, DP, DP, D, I, DP, I, I, DP, IP, P, ctypes.c_long, SP]),
+        "hprmat_b200_adjoint_from_x": (I, [P, I, IP, DP, DP, D, I, DP, I, I, DP, P, ctypes.c_long, DP, DP]),
         "hprmat_b200_rmatrix_full": (I, [P, I, IP, DP, DP, D, I, I, DP, I, I, DP, IP, I, DP, I, I, I, IP, I, DP,
                                          SP]),
         "hprmat_b200_solve_linear": (I, [P, DP, DP, I, I, SP]),
@@ -127,6 +132,7 @@ def load():
         "hprmat_b200_dev_panel_trace_read": (I, [P, ctypes.POINTER(ctypes.c_longlong), I, IP]),
         "hprmat_b200_dev_set_tuning": (I, [P, ctypes.c_char_p, I]),
         "hprmat_b200_dev_mesh": (I, [I, I, D, DP, DP, DP, DP, DP]),
+        "hprmat_b200_dev_factorizations": (ctypes.c_longlong, [P, I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

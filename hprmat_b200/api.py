@@ -38,7 +38,7 @@ class Context:
     """One device context (stream + device buffers) of the C library."""
 
     def __init__(self, device: int = 0, precision: str = "mixed", max_refine: int = 3, tol: float = 1e-12,
-                 panel_nb: int = 0, surface_tol: float = 1e-11):
+                 panel_nb: int = 0, surface_tol: float = 1e-11, reuse_factors: bool = False):
         self._lib = nat.load()
         self._h = ctypes.c_void_p()
         self.opts = nat.Opts()
@@ -48,6 +48,7 @@ class Context:
         self.opts.tol = float(tol)
         self.opts.surface_tol = float(surface_tol)
         self.opts.panel_nb = int(panel_nb)
+        self.opts.reuse_factors = int(bool(reuse_factors))
         nat.check(self._lib.hprmat_b200_create(int(device), ctypes.byref(self.opts), ctypes.byref(self._h)))
         self.device = device
         self.mesh = None
@@ -70,6 +71,12 @@ class Context:
 
     def __exit__(self, *exc):
         self.close()
+
+    def set_reuse_factors(self, enable: bool):
+        """opts.reuse_factors: successive rmatrix calls on the same channel block (energy scans)
+        refine with the held factorisation instead of factorising every energy."""
+        self.opts.reuse_factors = int(bool(enable))
+        nat.check(self._lib.hprmat_b200_set_opts(self._h, ctypes.byref(self.opts)))
 
     def set_precision(self, precision: str, max_refine: int | None = None, tol: float | None = None,
                       surface_tol: float | None = None):
@@ -233,6 +240,50 @@ class Context:
         self.last_stats = st.as_dict()
         nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
         return cu, nopen.value, cf
+
+    def rmatrix_x(self, nch, lval, qk, eta, rmax, nr, cpot, allow_unconverged=False):
+        """rmatrix (one interval) that also returns the refined forward solution X = C^-1 Q as a
+        torch CUDA tensor (nch*nr, nch) complex128, for ``adjoint_from_x``."""
+        import torch
+        self._ensure_mesh(nr, 1, rmax)
+        lval = np.ascontiguousarray(lval, dtype=np.int32)
+        qk = np.ascontiguousarray(qk, dtype=np.float64)
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        cpot = np.asfortranarray(cpot, dtype=np.complex128)
+        ncp1, ndim = cpot.shape[0], cpot.shape[1]
+        n = int(nch) * int(nr)
+        x = torch.empty((int(nch), n), dtype=torch.complex128, device=f"cuda:{self.device}")  # column-major X
+        cu = np.zeros((ndim, ndim), dtype=np.complex128, order="F")
+        nopen = ctypes.c_int(0)
+        st = Stats()
+        s = self._lib.hprmat_b200_rmatrix_x(self._h, int(nch), _iptr(lval), _dptr(qk), _dptr(eta), float(rmax),
+                                            int(nr), _dptr(cpot), int(ncp1), int(ndim), _dptr(cu),
+                                            ctypes.byref(nopen), ctypes.c_void_p(x.data_ptr()), n, ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
+        return cu, nopen.value, x.T
+
+    def adjoint_from_x(self, nch, lval, qk, eta, rmax, nr, cpot, cu, x, gu):
+        """Potential gradient of a real loss from the forward solution ``x`` of ``rmatrix_x``
+        (symmetric potentials), in the convention of ``rmatrix_adjoint``."""
+        lval = np.ascontiguousarray(lval, dtype=np.int32)
+        qk = np.ascontiguousarray(qk, dtype=np.float64)
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        cpot = np.asfortranarray(cpot, dtype=np.complex128)
+        ncp1, ndim = cpot.shape[0], cpot.shape[1]
+        cu = np.asfortranarray(cu, dtype=np.complex128)
+        g = np.zeros((ndim, ndim), dtype=np.complex128, order="F")
+        gu = np.asarray(gu, dtype=np.complex128)
+        g[:gu.shape[0], :gu.shape[1]] = gu
+        xt = x.T  # (nch, n) row-major == column-major (n, nch)
+        assert xt.is_contiguous() and xt.shape == (int(nch), int(nch) * int(nr))
+        grad = np.zeros_like(cpot, order="F")
+        s = self._lib.hprmat_b200_adjoint_from_x(self._h, int(nch), _iptr(lval), _dptr(qk), _dptr(eta), float(rmax),
+                                                 int(nr), _dptr(cpot), int(ncp1), int(ndim), _dptr(cu),
+                                                 ctypes.c_void_p(xt.data_ptr()), int(nch) * int(nr), _dptr(g),
+                                                 _dptr(grad))
+        nat.check(s)
+        return grad
 
     def rmatrix_device(self, nch, lval, qk, eta, rmax, nr, ns, d_cpot, ncp1, ndim, d_cu, allow_unconverged=False):
         """Device-resident variant: ``d_cpot``/``d_cu`` are device addresses (ints)."""

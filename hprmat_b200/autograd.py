@@ -2,8 +2,9 @@
 
 ``collision_matrix(cpot, ...)`` returns U (nopen x nopen, complex128) from the potential at
 the Lagrange mesh points, cpot[i, c, c'] = V_cc'(r_i) / (hbar^2/2mu), as a
-``torch.autograd.Function``: the forward is the refined device solve, the backward the adjoint
-solve with C^T on the FP64 LU factors (``hprmat_b200_rmatrix_adjoint``).  Gradients with
+``torch.autograd.Function``: the forward is the refined device solve; the backward is the
+adjoint -- from the forward's kept solution for a symmetric potential, else a solve with C^T on
+FP64 LU factors (``hprmat_b200_rmatrix_adjoint``).  Gradients with
 respect to potential parameters follow from building ``cpot`` with differentiable torch
 operations (``potential_matrix`` mirrors the synthetic potentials of
 ``hprmat_b200.workloads``).  The reference has no derivatives; this is the adjoint row of the
@@ -20,22 +21,36 @@ __all__ = ["CollisionMatrix", "collision_matrix", "potential_matrix"]
 
 
 class CollisionMatrix(torch.autograd.Function):
+    """Forward: the refined device solve.  For a symmetric potential (C(E) complex symmetric)
+    the forward keeps its solution X = C^-1 Q on the device and the backward forms the gradient
+    from it without another solve (``Context.rmatrix_x`` / ``adjoint_from_x``); otherwise the
+    backward runs ``rmatrix_adjoint`` (FP64 forward and a solve with C^T)."""
+
     @staticmethod
     def forward(fctx, cpot, solver, lval, qk, eta, rmax, nr):
         c_np = np.asfortranarray(cpot.detach().cpu().numpy().astype(np.complex128))
         nch = c_np.shape[1]
-        cu, nopen = solver.rmatrix(nch, lval, qk, eta, rmax, nr, 1, c_np)
+        symmetric = bool(np.array_equal(c_np[:nr], c_np[:nr].transpose(0, 2, 1)))
+        x = None
+        if symmetric:
+            cu, nopen, x = solver.rmatrix_x(nch, lval, qk, eta, rmax, nr, c_np)
+        else:
+            cu, nopen = solver.rmatrix(nch, lval, qk, eta, rmax, nr, 1, c_np)
         fctx.save_for_backward(cpot.detach())
-        fctx.args = (solver, lval, qk, eta, rmax, nr, nopen)
+        fctx.args = (solver, lval, qk, eta, rmax, nr, nopen, x, cu)
         return torch.from_numpy(np.ascontiguousarray(cu[:nopen, :nopen])).to(cpot.device)
 
     @staticmethod
     def backward(fctx, grad_u):
         (cpot,) = fctx.saved_tensors
-        solver, lval, qk, eta, rmax, nr, nopen = fctx.args
+        solver, lval, qk, eta, rmax, nr, nopen, x, cu = fctx.args
         c_np = np.asfortranarray(cpot.cpu().numpy().astype(np.complex128))
         nch = c_np.shape[1]
-        _, _, grad = solver.rmatrix_adjoint(nch, lval, qk, eta, rmax, nr, c_np, grad_u.detach().cpu().numpy())
+        gu = grad_u.detach().cpu().numpy()
+        if x is not None:
+            grad = solver.adjoint_from_x(nch, lval, qk, eta, rmax, nr, c_np, cu, x, gu)
+        else:
+            _, _, grad = solver.rmatrix_adjoint(nch, lval, qk, eta, rmax, nr, c_np, gu)
         return torch.from_numpy(np.ascontiguousarray(grad)).to(cpot.device), None, None, None, None, None, None
 
 

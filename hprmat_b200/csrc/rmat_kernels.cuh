@@ -863,6 +863,32 @@ __global__ void __launch_bounds__(1024) propagate_kernel(const double2* __restri
 }
 
 
+// Order-independent 64-bit fingerprint of the potential entries a call uses (rows < nrows,
+// channels < nch of cpot (ncp1, ndim, ndim)): the sum over entries of a SplitMix64 mix of
+// their bits and position.  Identifies the channel block for the reuse of a factorisation.
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+__global__ void fingerprint_kernel(const double2* __restrict__ cpot, long ncp1, long ndim, int nrows, int nch,
+                                   unsigned long long* out) {
+  const long total = (long)nrows * nch * nch;
+  unsigned long long h = 0;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < total; idx += (long)gridDim.x * blockDim.x) {
+    const long i = idx % nrows, cc = idx / nrows;
+    const long c = cc % nch, cp = cc / nch;
+    const double2 v = cpot[i + ncp1 * (c + ndim * cp)];
+    const unsigned long long bx = (unsigned long long)__double_as_longlong(v.x);
+    const unsigned long long by = (unsigned long long)__double_as_longlong(v.y);
+    h += mix64(bx ^ mix64(by ^ mix64((unsigned long long)idx)));
+  }
+  for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, h);
+}
+
 // ------------------------------------------------------------------ wave functions
 // Internal wave functions (rmatrix with twf, src/rmatrix_hp.F90:378-431), built from the
 // solutions the R-matrix step already has: per interval X = C^-1 [blockdiag(q1) | blockdiag(q2)].

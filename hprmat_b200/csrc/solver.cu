@@ -111,6 +111,7 @@ struct hprmat_b200_ctx {
       zwork, cpot, cu, norms, lup, rop, rsurf, vt, rlo, linv;
   // wave functions: per-interval solutions and propagation matrices, surface amplitudes, cf
   DevBuf wfx, wfz, wfc, wfcf;
+  DevBuf fpbuf;  // potential fingerprint (opts.reuse_factors)
   // tensor-core operand views of the current factorisation (mixed path)
   TcOperand op_lu, op_bop, op_rhs, op_linv;
   long lup_ld = 0, lup_plane = 0, rop_plane = 0;
@@ -133,6 +134,17 @@ struct hprmat_b200_ctx {
   long w_xld = 0, w_xplane = 0;
   bool wave_trace = false;
   DevBuf wtrace, ptrace;
+  // the mixed factorisation held in W / lup / the wave buffers, for opts.reuse_factors: its
+  // LUState (N, ld, nb, nsteps) and the channel block it belongs to
+  bool lu_held = false;
+  int held_last_inner = 0;     // FGMRES iterations of the last solve on the held factors
+  int reuse_max_inner = 24;    // factorise again once a reuse solve needed more than this
+  long long factorizations = 0;  // LU factorisations run on this context
+  int held_N = 0, held_nb = 0, held_nsteps = 0, held_nch = 0, held_nr = 0;
+  long held_ld = 0;
+  double held_rmax = 0.0;
+  unsigned long long held_fp = 0;
+  std::vector<int> held_lval;
   // last FP64 factorisation of rmatrix (for the adjoint): N, ld, nb, nsteps; adjoint scratch
   int f64_N = 0, f64_nb = 0, f64_nsteps = 0;
   long f64_ld = 0;
@@ -479,6 +491,8 @@ template <typename T, int NB>
 static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUState& st) {
   constexpr int NT = 256;
   const int nsteps = (N + NB - 1) / NB;
+  c->lu_held = false;  // W, lup and the wave buffers are overwritten
+  ++c->factorizations;
   st.N = N;
   st.ld = ld;
   st.nb = NB;
@@ -914,7 +928,11 @@ static int frob_norm(hprmat_b200_ctx* c, const double2* X, long ldx, int N, int 
 // up to gmres_m flexible-GMRES iterations on C d = r, preconditioned by the FP32 LU solve, and
 // X += d.  Returns NOT_CONVERGED if max_refine outer corrections did not reach tol.
 static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W32, const LUState& st,
-                        double2* X64, long ldx, int nrhs, double bnorm, double cnorm, hprmat_b200_stats* stats) {
+                        double2* X64, long ldx, int nrhs, double bnorm, double cnorm, hprmat_b200_stats* stats,
+                        int max_outer = -1, bool error_based = false) {
+  // error_based (factors of another energy, opts.reuse_factors): a small residual alone does
+  // not stop the refinement -- the surface rule, which measures the error in R, must hold
+  if (max_outer < 0) max_outer = c->opts.max_refine;
   const int N = op.N;
   const int m = std::min(c->gmres_m, kGmresMaxM);
   const long ldv = st.ld;
@@ -999,7 +1017,7 @@ static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W3
       stats->surface_change = change;
       stats->residual_floor = floor_rel;
     }
-    if (!(rel >= c->opts.tol)) break;  // converged (also on rel == 0)
+    if (!(rel >= c->opts.tol) && !(error_based && surf && rel > 0.0)) break;  // converged (also on rel == 0)
     if (surf && outer > 0) {
       // change = size of the last correction in R, i.e. the error of the previous iterate;
       // the last cycle reduced that error by about last_est, which predicts the error left.
@@ -1007,14 +1025,16 @@ static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W3
       const double predicted = change * std::max(last_est, 1e-16);
       if (!(change >= c->opts.surface_tol) || 1e3 * predicted < c->opts.surface_tol) break;
       if (outer >= 2 && change > 0.5 * prev_change) {  // no longer improving
-        if (predicted > 1e-8) status = HPRMAT_B200_NOT_CONVERGED;
+        // on factors of another energy a stall means the preconditioner is too far off:
+        // report it, so that the caller factorises C(E) itself
+        if (predicted > 1e-8 || error_based) status = HPRMAT_B200_NOT_CONVERGED;
         break;
       }
     } else if (!surf && outer >= 1 && rel > 0.5 * prev_rel) {  // dense operator: residual stalled
       if (rel > 1e-8) status = HPRMAT_B200_NOT_CONVERGED;
       break;
     }
-    if (outer >= c->opts.max_refine) {
+    if (outer >= max_outer) {
       status = HPRMAT_B200_NOT_CONVERGED;
       break;
     }
@@ -1128,9 +1148,11 @@ static double ms_since(Clock::time_point t0) {
 // d_cpot points at the interval's first mesh row.  Statistics of the interval in *stats.
 // With a non-local potential (nl.p set) C(E) has dense channel blocks: the refinement's FP64
 // operator is then a dense copy of C (A64) with a dense right-hand side (B64).
+// reuse: keep the held mixed factorisation (opts.reuse_factors) as the refinement's
+// preconditioner instead of assembling and factorising C(E); up to 8 refinement cycles.
 static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData& chd, const MeshDev& md,
                           const double2* d_cpot, int ncp1, int ndim, double2* X64, long ld,
-                          hprmat_b200_stats* stats, const NonLocalDev& nl) {
+                          hprmat_b200_stats* stats, const NonLocalDev& nl, bool reuse = false) {
   const int nr = md.nr;
   const int N = nch * nr;
   const int nrhs = md.nq1 + nch;
@@ -1189,6 +1211,7 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
     if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
     auto t1 = Clock::now();
     TRY(factor<double2>(c, W, ld, N, false, nb, st));
+    stats->factorizations = 1;
     c->f64_N = st.N;
     c->f64_ld = st.ld;
     c->f64_nb = st.nb;
@@ -1207,13 +1230,25 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
   } else {
     TRY(c->W.ensure((size_t)ld * N * sizeof(float2)));
     float2* W = c->W.as<float2>();
-    assemble_kernel<float2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2, nl);
-    LAUNCH_CHECK();
-    int nb = pick_nb(c, N, sizeof(float2), 128);
-    if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
-    auto t1 = Clock::now();
-    TRY(factor<float2>(c, W, ld, N, true, nb, st));
-    stats->ms_factor = ms_since(t1);
+    if (reuse) {
+      st.N = c->held_N;
+      st.ld = c->held_ld;
+      st.nb = c->held_nb;
+      st.nsteps = c->held_nsteps;
+    } else {
+      assemble_kernel<float2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2, nl);
+      LAUNCH_CHECK();
+      int nb = pick_nb(c, N, sizeof(float2), 128);
+      if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
+      auto t1 = Clock::now();
+      TRY(factor<float2>(c, W, ld, N, true, nb, st));
+      stats->ms_factor = ms_since(t1);
+      stats->factorizations = 1;
+      c->held_N = st.N;
+      c->held_ld = st.ld;
+      c->held_nb = st.nb;
+      c->held_nsteps = st.nsteps;
+    }
     auto t2 = Clock::now();
     TRY(c->X.ensure((size_t)ld * nrhs * sizeof(float2)));
     float2* X32 = c->X.as<float2>();
@@ -1228,15 +1263,12 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
     }
     stats->ms_solve = ms_since(t2);
     auto t3 = Clock::now();
-    double cn2;
-    HPR_CUDA_TRY(cudaMemcpyAsync(&cn2, d_fro2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    status = refine_mixed(c, op, W, st, X64, ld, nrhs, bnorm, sqrt(cn2), stats);
+    status = refine_mixed(c, op, W, st, X64, ld, nrhs, bnorm, 0.0, stats, reuse ? 8 : -1, reuse);
     if (status != HPRMAT_B200_OK && status != HPRMAT_B200_NOT_CONVERGED) return status;
     stats->ms_refine = ms_since(t3);
   }
   stats->nb = st.nb;
-  if (c->h_status[SW_INFO] != 0) {
+  if (!reuse && c->h_status[SW_INFO] != 0) {
     stats->info = c->h_status[SW_INFO];
     return fail(HPRMAT_B200_SINGULAR, "C(E) of interval %d is singular: zero pivot in column %d", is + 1,
                 c->h_status[SW_INFO]);
@@ -1352,6 +1384,23 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
     TRY(c->wfz.ensure((size_t)ns * nn * sizeof(double2)));
     TRY(c->wfc.ensure((size_t)nch * (ns + 1) * nc * sizeof(double2)));
   }
+  // factor reuse (opts.reuse_factors): the held factorisation must be of this channel block
+  const bool mixed = c->opts.precision == HPRMAT_B200_PREC_MIXED;
+  const bool keyed = c->opts.reuse_factors && mixed && ns == 1 && !d_cpnl;
+  unsigned long long fp = 0;
+  if (keyed) {
+    TRY(c->fpbuf.ensure(sizeof(unsigned long long)));
+    HPR_CUDA_TRY(cudaMemsetAsync(c->fpbuf.p, 0, sizeof(unsigned long long), c->stream));
+    const long tot = (long)nr * nch * nch;
+    fingerprint_kernel<<<std::min<unsigned>(cdiv_u(tot, 256), 592), 256, 0, c->stream>>>(
+        d_cpot, ncp1, ndim, nr, nch, c->fpbuf.as<unsigned long long>());
+    LAUNCH_CHECK();
+    HPR_CUDA_TRY(cudaMemcpyAsync(&fp, c->fpbuf.p, sizeof(fp), cudaMemcpyDeviceToHost, c->stream));
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
+  const bool try_reuse = keyed && c->lu_held && c->held_N == N && c->held_nch == nch && c->held_nr == nr &&
+                         c->held_rmax == rmax && c->held_fp == fp && c->held_last_inner <= c->reuse_max_inner &&
+                         std::equal(lval, lval + nch, c->held_lval.begin(), c->held_lval.end());
   int status = HPRMAT_B200_OK;
   for (int is = 0; is < ns; ++is) {
     const MeshDev md = mesh_dev(c, is, is > 0 ? nch : 0);
@@ -1368,10 +1417,34 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
       nl.wle = mesh_wle(c);
       nl.rmax0 = rmax0;
     }
-    const int s = interval_solve(c, is, nch, chd, md, d_cpot + (size_t)is * nr, ncp1, ndim, X64, ld, &si, nl);
+    int s = interval_solve(c, is, nch, chd, md, d_cpot + (size_t)is * nr, ncp1, ndim, X64, ld, &si, nl, try_reuse);
+    if (try_reuse && s == HPRMAT_B200_NOT_CONVERGED) {
+      // the held factors were too far from C(E) for the refinement: factorise C(E)
+      hprmat_b200_stats s2;
+      memset(&s2, 0, sizeof(s2));
+      s2.rel_residual = -1.0;
+      s2.surface_change = -1.0;
+      s = interval_solve(c, is, nch, chd, md, d_cpot + (size_t)is * nr, ncp1, ndim, X64, ld, &s2, nl, false);
+      s2.refine_steps += si.refine_steps;
+      s2.inner_iterations += si.inner_iterations;
+      s2.ms_solve += si.ms_solve;
+      s2.ms_refine += si.ms_refine;
+      si = s2;
+    }
+    if (keyed && (s == HPRMAT_B200_OK || s == HPRMAT_B200_NOT_CONVERGED))
+      c->held_last_inner = si.factorizations > 0 ? 0 : si.inner_iterations;
+    if (keyed && (s == HPRMAT_B200_OK || s == HPRMAT_B200_NOT_CONVERGED) && si.factorizations > 0) {
+      c->lu_held = true;
+      c->held_nch = nch;
+      c->held_nr = nr;
+      c->held_rmax = rmax;
+      c->held_fp = fp;
+      c->held_lval.assign(lval, lval + nch);
+    }
     if (stats) {
       stats->info = si.info;
       stats->nb = si.nb;
+      stats->factorizations += si.factorizations;
       stats->refine_steps += si.refine_steps;
       stats->inner_iterations += si.inner_iterations;
       stats->ms_factor += si.ms_factor;
@@ -1704,7 +1777,7 @@ int hprmat_b200_destroy(hprmat_b200_ctx* c) {
   DevBuf* bufs[] = {&c->mesh, &c->W, &c->A64, &c->X, &c->X64, &c->R64, &c->B64, &c->V, &c->Z, &c->gm,
                     &c->swaps, &c->ipiv, &c->stage, &c->status, &c->ops, &c->inv, &c->chan, &c->rmat,
                     &c->zwork, &c->cpot, &c->cu, &c->norms, &c->lup, &c->rop, &c->rsurf, &c->vt, &c->rlo, &c->linv,
-                    &c->wfx, &c->wfz, &c->wfc, &c->wfcf};
+                    &c->wfx, &c->wfz, &c->wfc, &c->wfcf, &c->fpbuf};
   for (DevBuf* b : bufs) b->release();
   for (hprmat_b200_ctx* w : c->scan_workers) hprmat_b200_destroy(w);
   c->scan_workers.clear();
@@ -1970,17 +2043,35 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_
   if (nblocks < 0 || (nblocks > 0 && !blocks) || nr <= 0 || !(rmax > 0.0))
     return fail(HPRMAT_B200_ERR_ARG, "rmatrix_scan: invalid arguments");
   auto t0 = Clock::now();
+  // work items: runs of up to kChunk energies of one block in energy order (the first
+  // channel's signed k^2 orders the energies of a block), largest blocks first; with
+  // opts.reuse_factors a worker keeps one factorisation across the run
+  constexpr int kChunk = 32;
   struct Unit {
-    int b, e;
+    int b;
+    std::vector<int> es;
     long n;
   };
   std::vector<Unit> units;
+  size_t nunits = 0;
   for (int b = 0; b < nblocks; ++b) {
     const hprmat_b200_scan_block& B = blocks[b];
     if (B.nch <= 0 || B.nenergies < 0 || !B.lval || !B.cpot || B.ncp1 < nr || !B.cu || !B.nopen || !B.status ||
         (B.nenergies > 0 && (!B.qk || !B.eta)))
       return fail(HPRMAT_B200_ERR_ARG, "rmatrix_scan: invalid block %d", b);
-    for (int e = 0; e < B.nenergies; ++e) units.push_back({b, e, (long)B.nch * nr});
+    std::vector<int> order(B.nenergies);
+    for (int e = 0; e < B.nenergies; ++e) order[e] = e;
+    auto key = [&](int e) {
+      const double k = B.qk[(size_t)e * B.nch];
+      return k > 0 ? k * k : -k * k;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key(x) < key(y); });
+    for (int e0 = 0; e0 < B.nenergies; e0 += kChunk) {
+      Unit u{b, {}, (long)B.nch * nr};
+      u.es.assign(order.begin() + e0, order.begin() + std::min(B.nenergies, e0 + kChunk));
+      units.push_back(std::move(u));
+    }
+    nunits += B.nenergies;
   }
   std::stable_sort(units.begin(), units.end(), [](const Unit& x, const Unit& y) { return x.n > y.n; });
   // potentials on the device, once per block
@@ -1996,7 +2087,8 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_
   HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
   // workers
   if (nworkers <= 0) nworkers = 4;
-  nworkers = std::max(1, std::min<int>(nworkers, (int)units.size()));
+  nworkers = std::max(1, std::min<int>(nworkers, (int)std::max<size_t>(units.size(), 1)));
+  (void)nunits;
   while ((int)c->scan_workers.size() < nworkers) {
     hprmat_b200_ctx* w = nullptr;
     TRY(hprmat_b200_create(c->device, &c->opts, &w));
@@ -2008,6 +2100,8 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_
     w->opts = c->opts;
     w->wave_sb = c->wave_sb;
     w->wave_un = c->wave_un;
+    w->reuse_max_inner = c->reuse_max_inner;
+    w->lu_held = false;
     TRY(hprmat_b200_rmat_ini(w, nr, 1, rmax, zrma.data()));
   }
   std::atomic<size_t> next{0};
@@ -2023,24 +2117,26 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_
       const Unit& u = units[k];
       const hprmat_b200_scan_block& B = blocks[u.b];
       const size_t ubytes = (size_t)B.nch * B.nch * sizeof(double2);
-      int s = w->cu.ensure(ubytes);
-      int nopen = 0;
-      if (s == HPRMAT_B200_OK)
-        s = rmatrix_core(w, B.nch, B.lval, B.qk + (size_t)u.e * B.nch, B.eta + (size_t)u.e * B.nch, rmax, nr, 1,
-                         c->scan_cpot[u.b]->as<double2>(), B.ncp1, B.nch, w->cu.as<double2>(), &nopen, nullptr);
-      if (s == HPRMAT_B200_OK || s == HPRMAT_B200_NOT_CONVERGED) {
-        double* dst = B.cu + (size_t)u.e * B.nch * B.nch * 2;
-        if (cudaMemcpyAsync(dst, w->cu.p, ubytes, cudaMemcpyDeviceToHost, w->stream) != cudaSuccess ||
-            cudaStreamSynchronize(w->stream) != cudaSuccess)
-          s = HPRMAT_B200_ERR_CUDA;
-      }
-      B.nopen[u.e] = nopen;
-      B.status[u.e] = s;
-      if (s != HPRMAT_B200_OK) {
-        int z = 0;
-        if (first_error.compare_exchange_strong(z, s)) {
-          std::lock_guard<std::mutex> lk(err_mu);
-          err_msg = hprmat_b200_last_error();
+      for (const int e : u.es) {
+        int s = w->cu.ensure(ubytes);
+        int nopen = 0;
+        if (s == HPRMAT_B200_OK)
+          s = rmatrix_core(w, B.nch, B.lval, B.qk + (size_t)e * B.nch, B.eta + (size_t)e * B.nch, rmax, nr, 1,
+                           c->scan_cpot[u.b]->as<double2>(), B.ncp1, B.nch, w->cu.as<double2>(), &nopen, nullptr);
+        if (s == HPRMAT_B200_OK || s == HPRMAT_B200_NOT_CONVERGED) {
+          double* dst = B.cu + (size_t)e * B.nch * B.nch * 2;
+          if (cudaMemcpyAsync(dst, w->cu.p, ubytes, cudaMemcpyDeviceToHost, w->stream) != cudaSuccess ||
+              cudaStreamSynchronize(w->stream) != cudaSuccess)
+            s = HPRMAT_B200_ERR_CUDA;
+        }
+        B.nopen[e] = nopen;
+        B.status[e] = s;
+        if (s != HPRMAT_B200_OK) {
+          int z = 0;
+          if (first_error.compare_exchange_strong(z, s)) {
+            std::lock_guard<std::mutex> lk(err_mu);
+            err_msg = hprmat_b200_last_error();
+          }
         }
       }
     }
@@ -2055,12 +2151,108 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_
   return fe;
 }
 
-// Adjoint of one collision matrix: the forward solve on the FP64 path, then one solve with
-// C^T from the same factors (adjoint.cuh).  With G = gu (dL = Re sum conj(G) dU):
+// Adjoint of one collision matrix.  Symmetric potential: the forward solve at the context's
+// precision and Y = X M2^T (C^T = C).  Otherwise the forward solve on the FP64 path, then one
+// solve with C^T from the same factors (adjoint.cuh).  With G = gu (dL = Re sum conj(G) dU):
 //   M = W G^H Z_O^-1,  W = diag(cop) U - diag(conj cop)       (dU = Z_O^-1 dRt W)
 //   M2(i2, i1) = M(m2, m1) sqrt(k_i1 / k_i2)                  (Rt = R sqrt(k_i / k_j), open)
 //   C^T Y = Q M2^T,  Q = blockdiag(q2)                         (R = Q^T X / a)
 //   grad(r_i, c, c') = -conj(sum_col Y[(c,i), col] X[(c',i), col]) / a
+// M2 of the adjoint (the rhs of C^T Y = Q M2^T is Q M2^T): from R (host, nch x nch, R/a as the
+// U step uses it), U (host cu, ld ndim) and the loss gradient gu (ld ndim).  no = nopen.
+static int adjoint_m2(int nch, const int* lval, const double* qk, const double* eta, double rmax, double a,
+                      const std::vector<double2>& R, const double* cu, const double* gu, int ndim,
+                      std::vector<double2>& M2, int* no_out) {
+  Boundary bnd;
+  TRY(boundary_values(nch, lval, qk, eta, rmax, a, bnd));
+  const int no = bnd.nopen;
+  *no_out = no;
+  M2.assign((size_t)nch * nch, mk(0.0, 0.0));
+  if (no == 0) return HPRMAT_B200_OK;
+  auto sk = [&](int m1, int m2) { return sqrt(qk[bnd.open_idx[m1]] / qk[bnd.open_idx[m2]]); };
+  std::vector<double2> Zt((size_t)no * no), Pt((size_t)no * no);  // Z_O^T and (W G^H)^T
+  for (int m2 = 0; m2 < no; ++m2)
+    for (int m1 = 0; m1 < no; ++m1) {
+      double2 r = R[bnd.open_idx[m1] + (size_t)bnd.open_idx[m2] * nch];
+      const double sc = sk(m1, m2);
+      r.x *= sc;
+      r.y *= sc;
+      double2 z = cmul(r, bnd.cop[m2]);
+      z.x = -z.x;
+      z.y = -z.y;
+      if (m1 == m2) {
+        z.x += bnd.co[m1].x;
+        z.y += bnd.co[m1].y;
+      }
+      Zt[m2 + (size_t)m1 * no] = z;  // (Z_O^T)(m2, m1) = Z_O(m1, m2)
+    }
+  for (int a1 = 0; a1 < no; ++a1)
+    for (int b1 = 0; b1 < no; ++b1) {
+      double2 acc = mk(0.0, 0.0);  // (W G^H)(a1, b1) = sum_k W(a1, k) conj(G(b1, k))
+      for (int k = 0; k < no; ++k) {
+        double2 w = cmul(bnd.cop[a1], host_c(cu, a1 + (size_t)k * ndim));
+        if (a1 == k) {
+          w.x -= bnd.cop[a1].x;
+          w.y += bnd.cop[a1].y;
+        }
+        const double2 g = host_c(gu, b1 + (size_t)k * ndim);
+        cfma(acc, w, mk(g.x, -g.y));
+      }
+      Pt[b1 + (size_t)a1 * no] = acc;
+    }
+  // M = (W G^H) Z_O^-1  <=>  Z_O^T M^T = (W G^H)^T
+  if (!host_csolve(Zt, Pt, no, no)) return fail(HPRMAT_B200_SINGULAR, "rmatrix_adjoint: singular Z_O");
+  // M2(i2, i1) = M(m2, m1) sqrt(k_i1/k_i2), stored at [i2 + i1 nch]
+  for (int m1 = 0; m1 < no; ++m1)
+    for (int m2 = 0; m2 < no; ++m2) {
+      double2 v = Pt[m1 + (size_t)m2 * no];  // M^T(m1, m2) = M(m2, m1)
+      const double sc = sk(m1, m2);
+      M2[bnd.open_idx[m2] + (size_t)bnd.open_idx[m1] * nch] = mk(v.x * sc, v.y * sc);
+    }
+  return HPRMAT_B200_OK;
+}
+
+// Gradient at the mesh points for a symmetric C(E) from its forward solution X (device, N x nch,
+// ld ldx): Y = X M2^T, grad(r_i, c, c') = -conj(sum_col Y[(c,i), col] X[(c',i), col]) / a into the
+// device array d_grad (complex (ncp1, ndim, ndim), zeroed here).
+static int adjoint_grad_symmetric(hprmat_b200_ctx* c, int nch, int nr, int ndim, int ncp1, double a,
+                                  const std::vector<double2>& M2, const double2* X, long ldx, double2* d_grad) {
+  const int N = nch * nr;
+  HPR_CUDA_TRY(cudaMemsetAsync(d_grad, 0, (size_t)ncp1 * ndim * ndim * sizeof(double2), c->stream));
+  TRY(c->adj_y.ensure((size_t)ldx * nch * sizeof(double2)));
+  double2* Y = c->adj_y.as<double2>();
+  // C -= A B with A = X, B(ch, col) = -M2(col, ch), C = 0
+  std::vector<double2> nb((size_t)nch * nch);
+  for (int col = 0; col < nch; ++col)
+    for (int ch = 0; ch < nch; ++ch) {
+      const double2 m = M2[col + (size_t)ch * nch];
+      nb[ch + (size_t)col * nch] = mk(-m.x, -m.y);
+    }
+  TRY(c->adj_part.ensure(nb.size() * sizeof(double2)));
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->adj_part.p, nb.data(), nb.size() * sizeof(double2), cudaMemcpyHostToDevice,
+                               c->stream));
+  HPR_CUDA_TRY(cudaMemsetAsync(Y, 0, (size_t)ldx * nch * sizeof(double2), c->stream));
+  dim3 grid(cdiv_u(N, 64), cdiv_u(nch, 64));
+  cgemm_update_kernel<double2><<<grid, 256, 0, c->stream>>>(N, nch, nch, X, ldx, c->adj_part.as<double2>(), nch, Y,
+                                                            ldx);
+  LAUNCH_CHECK();
+  potential_grad_kernel<<<dim3(nr, nch), 128, 0, c->stream>>>(Y, X, ldx, nr, nch, nch, 1.0 / a, d_grad, ncp1, ndim);
+  LAUNCH_CHECK();
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));  // nb must outlive its copy
+  return HPRMAT_B200_OK;
+}
+
+static bool potential_symmetric(const double* cpot, int ncp1, int ndim, int nr, int nch) {
+  for (int cp = 0; cp < nch; ++cp)
+    for (int c1 = cp + 1; c1 < nch; ++c1)
+      for (int i = 0; i < nr; ++i) {
+        const size_t a1 = 2 * ((size_t)i + (size_t)ncp1 * (c1 + (size_t)ndim * cp));
+        const size_t a2 = 2 * ((size_t)i + (size_t)ncp1 * (cp + (size_t)ndim * c1));
+        if (cpot[a1] != cpot[a2] || cpot[a1 + 1] != cpot[a2 + 1]) return false;
+      }
+  return true;
+}
+
 int hprmat_b200_rmatrix_adjoint(hprmat_b200_ctx* c, int nch, const int* lval, const double* qk, const double* eta,
                                 double rmax, int nr, int ns, const double* cpot, int ncp1, int ndim, const double* gu,
                                 double* cu, int* nopen, double* grad, hprmat_b200_stats* stats) {
@@ -2073,87 +2265,106 @@ int hprmat_b200_rmatrix_adjoint(hprmat_b200_ctx* c, int nch, const int* lval, co
   TRY(c->cpot.ensure(pbytes));
   TRY(c->cu.ensure(ubytes));
   HPR_CUDA_TRY(cudaMemcpyAsync(c->cpot.p, cpot, pbytes, cudaMemcpyHostToDevice, c->stream));
+  // C(E) is complex symmetric when the potential is (the kinetic, Bloch, centrifugal and energy
+  // terms are): then C^-T = C^-1 and the adjoint solution is Y = X M2^T from the forward
+  // solution X = C^-1 Q, at the context's precision (refined) -- no transposed solve.  Otherwise
+  // the forward runs on the FP64 path and Y comes from a solve with C^T on its factors.
+  const bool symmetric = potential_symmetric(cpot, ncp1, ndim, nr, nch);
   const int prec = c->opts.precision;
-  c->opts.precision = HPRMAT_B200_PREC_FP64;
+  if (!symmetric) c->opts.precision = HPRMAT_B200_PREC_FP64;
   int s = rmatrix_core(c, nch, lval, qk, eta, rmax, nr, ns, c->cpot.as<double2>(), ncp1, ndim, c->cu.as<double2>(),
                        nopen, stats);
   c->opts.precision = prec;
   if (s != HPRMAT_B200_OK && s != HPRMAT_B200_NOT_CONVERGED) return s;
-  if (c->f64_nb > 64) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "rmatrix_adjoint: panel_nb above 64");
+  if (!symmetric && c->f64_nb > 64) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "rmatrix_adjoint: panel_nb above 64");
   HPR_CUDA_TRY(cudaMemcpyAsync(cu, c->cu.p, ubytes, cudaMemcpyDeviceToHost, c->stream));
   std::vector<double2> R((size_t)nch * nch);
   HPR_CUDA_TRY(cudaMemcpyAsync(R.data(), c->rmat.p, R.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
   HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  const int N = c->f64_N;
-  const long ld = c->f64_ld;
+  const int N = nch * nr;
+  const long ld = (N + 3) / 4 * 4;  // the layout rmatrix_core gave X (and the FP64 factors)
   const double a = rmax / ns;
   TRY(c->adj_grad.ensure(pbytes));
   HPR_CUDA_TRY(cudaMemsetAsync(c->adj_grad.p, 0, pbytes, c->stream));
-  Boundary bnd;
-  TRY(boundary_values(nch, lval, qk, eta, rmax, a, bnd));
-  const int no = bnd.nopen;
+  std::vector<double2> M2;
+  int no = 0;
+  TRY(adjoint_m2(nch, lval, qk, eta, rmax, a, R, cu, gu, ndim, M2, &no));
   if (no > 0) {
-    auto sk = [&](int m1, int m2) { return sqrt(qk[bnd.open_idx[m1]] / qk[bnd.open_idx[m2]]); };
-    std::vector<double2> Zt((size_t)no * no), Pt((size_t)no * no);  // Z_O^T and (W G^H)^T
-    for (int m2 = 0; m2 < no; ++m2)
-      for (int m1 = 0; m1 < no; ++m1) {
-        double2 r = R[bnd.open_idx[m1] + (size_t)bnd.open_idx[m2] * nch];
-        const double sc = sk(m1, m2);
-        r.x *= sc;
-        r.y *= sc;
-        double2 z = cmul(r, bnd.cop[m2]);
-        z.x = -z.x;
-        z.y = -z.y;
-        if (m1 == m2) {
-          z.x += bnd.co[m1].x;
-          z.y += bnd.co[m1].y;
+    if (symmetric) {
+      TRY(adjoint_grad_symmetric(c, nch, nr, ndim, ncp1, a, M2, c->X64.as<double2>(), ld, c->adj_grad.as<double2>()));
+    } else {
+      // C^T Y = Q M2^T: rhs[(c,i), col] = q2_i M2(col, c)
+      TRY(c->adj_y.ensure((size_t)ld * nch * sizeof(double2)));
+      double2* Y = c->adj_y.as<double2>();
+      std::vector<double2> rhs((size_t)ld * nch, mk(0.0, 0.0));
+      for (int col = 0; col < nch; ++col)
+        for (int ch = 0; ch < nch; ++ch) {
+          const double2 m = M2[col + (size_t)ch * nch];
+          if (m.x == 0.0 && m.y == 0.0) continue;
+          for (int i = 0; i < nr; ++i)
+            rhs[(size_t)(ch * nr + i) + (size_t)col * ld] = mk(c->q2[i] * m.x, c->q2[i] * m.y);
         }
-        Zt[m2 + (size_t)m1 * no] = z;  // (Z_O^T)(m2, m1) = Z_O(m1, m2)
-      }
-    for (int a1 = 0; a1 < no; ++a1)
-      for (int b1 = 0; b1 < no; ++b1) {
-        double2 acc = mk(0.0, 0.0);  // (W G^H)(a1, b1) = sum_k W(a1, k) conj(G(b1, k))
-        for (int k = 0; k < no; ++k) {
-          double2 w = cmul(bnd.cop[a1], host_c(cu, a1 + (size_t)k * ndim));
-          if (a1 == k) {
-            w.x -= bnd.cop[a1].x;
-            w.y += bnd.cop[a1].y;
-          }
-          const double2 g = host_c(gu, b1 + (size_t)k * ndim);
-          cfma(acc, w, mk(g.x, -g.y));
-        }
-        Pt[b1 + (size_t)a1 * no] = acc;
-      }
-    // M = (W G^H) Z_O^-1  <=>  Z_O^T M^T = (W G^H)^T
-    if (!host_csolve(Zt, Pt, no, no)) return fail(HPRMAT_B200_SINGULAR, "rmatrix_adjoint: singular Z_O");
-    // right-hand side Q M2^T: rhs[(c,i), col] = q2_i M2(col, c), M2(i2, i1) = M(m2, m1) sqrt(k_i1/k_i2)
-    std::vector<double2> M2((size_t)nch * nch, mk(0.0, 0.0));
-    for (int m1 = 0; m1 < no; ++m1)
-      for (int m2 = 0; m2 < no; ++m2) {
-        double2 v = Pt[m1 + (size_t)m2 * no];  // M^T(m1, m2) = M(m2, m1)
-        const double sc = sk(m1, m2);
-        M2[bnd.open_idx[m2] + (size_t)bnd.open_idx[m1] * nch] = mk(v.x * sc, v.y * sc);
-      }
-    std::vector<double2> rhs((size_t)ld * nch, mk(0.0, 0.0));
-    for (int col = 0; col < nch; ++col)
-      for (int ch = 0; ch < nch; ++ch) {
-        const double2 m = M2[col + (size_t)ch * nch];
-        if (m.x == 0.0 && m.y == 0.0) continue;
-        for (int i = 0; i < nr; ++i)
-          rhs[(size_t)(ch * nr + i) + (size_t)col * ld] = mk(c->q2[i] * m.x, c->q2[i] * m.y);
-      }
-    TRY(c->adj_y.ensure(rhs.size() * sizeof(double2)));
-    double2* Y = c->adj_y.as<double2>();
-    HPR_CUDA_TRY(cudaMemcpyAsync(Y, rhs.data(), rhs.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
-    TRY(lu_solve_trans(c, c->W.as<double2>(), ld, N, c->f64_nb, c->f64_nsteps, Y, ld, nch));
-    potential_grad_kernel<<<dim3(nr, nch), 128, 0, c->stream>>>(Y, c->X64.as<double2>(), ld, nr, nch, nch, 1.0 / a,
-                                                                c->adj_grad.as<double2>(), ncp1, ndim);
-    LAUNCH_CHECK();
-    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));  // rhs must outlive its copy
+      HPR_CUDA_TRY(cudaMemcpyAsync(Y, rhs.data(), rhs.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+      TRY(lu_solve_trans(c, c->W.as<double2>(), ld, N, c->f64_nb, c->f64_nsteps, Y, ld, nch));
+      potential_grad_kernel<<<dim3(nr, nch), 128, 0, c->stream>>>(Y, c->X64.as<double2>(), ld, nr, nch, nch, 1.0 / a,
+                                                                  c->adj_grad.as<double2>(), ncp1, ndim);
+      LAUNCH_CHECK();
+      HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));  // rhs must outlive its copy
+    }
   }
   HPR_CUDA_TRY(cudaMemcpyAsync(grad, c->adj_grad.p, pbytes, cudaMemcpyDeviceToHost, c->stream));
   HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
   return s;
+}
+
+
+int hprmat_b200_rmatrix_x(hprmat_b200_ctx* c, int nch, const int* lval, const double* qk, const double* eta,
+                          double rmax, int nr, const double* cpot, int ncp1, int ndim, double* cu, int* nopen,
+                          void* d_x, long ldx, hprmat_b200_stats* stats) {
+  TRY(check_ctx(c));
+  if (!d_x || ldx < (long)nch * nr) return fail(HPRMAT_B200_ERR_ARG, "rmatrix_x: need d_x with ldx >= nch*nr");
+  int s = hprmat_b200_rmatrix(c, nch, lval, qk, eta, rmax, nr, 1, cpot, ncp1, ndim, cu, nopen, stats);
+  if (s != HPRMAT_B200_OK && s != HPRMAT_B200_NOT_CONVERGED) return s;
+  const long N = (long)nch * nr, ld = (N + 3) / 4 * 4;
+  HPR_CUDA_TRY(cudaMemcpy2DAsync(d_x, (size_t)ldx * sizeof(double2), c->X64.p, (size_t)ld * sizeof(double2),
+                                 (size_t)N * sizeof(double2), nch, cudaMemcpyDeviceToDevice, c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return s;
+}
+
+int hprmat_b200_adjoint_from_x(hprmat_b200_ctx* c, int nch, const int* lval, const double* qk, const double* eta,
+                               double rmax, int nr, const double* cpot, int ncp1, int ndim, const double* cu,
+                               const void* d_x, long ldx, const double* gu, double* grad) {
+  TRY(check_ctx(c));
+  if (!cpot || !cu || !gu || !grad || !d_x || ndim < nch || ncp1 < nr || nch <= 0 || ldx < (long)nch * nr)
+    return fail(HPRMAT_B200_ERR_ARG, "adjoint_from_x: invalid arguments");
+  if (!potential_symmetric(cpot, ncp1, ndim, nr, nch))
+    return fail(HPRMAT_B200_ERR_UNSUPPORTED, "adjoint_from_x: the potential is not symmetric; use rmatrix_adjoint");
+  if (c->nr != nr || c->ns != 1 || c->rmax != rmax)
+    return fail(HPRMAT_B200_ERR_ARG, "adjoint_from_x: call rmat_ini(nr=%d, ns=1, rmax=%g) first", nr, rmax);
+  const double a = rmax;
+  const size_t pbytes = (size_t)ncp1 * ndim * ndim * sizeof(double2);
+  // R = q2^T X / a from the forward solution
+  TRY(c->rmat.ensure((size_t)nch * nch * sizeof(double2) + 64));
+  const MeshDev md = mesh_dev(c, 0);
+  rmat_extract_kernel<<<dim3(nch, cdiv_u(nch, 128)), 128, 0, c->stream>>>((const double2*)d_x, ldx, md.q2, nr, nch,
+                                                                         nch, 1.0 / a, c->rmat.as<double2>());
+  LAUNCH_CHECK();
+  std::vector<double2> R((size_t)nch * nch);
+  HPR_CUDA_TRY(cudaMemcpyAsync(R.data(), c->rmat.p, R.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  std::vector<double2> M2;
+  int no = 0;
+  TRY(adjoint_m2(nch, lval, qk, eta, rmax, a, R, cu, gu, ndim, M2, &no));
+  TRY(c->adj_grad.ensure(pbytes));
+  if (no > 0) {
+    TRY(adjoint_grad_symmetric(c, nch, nr, ndim, ncp1, a, M2, (const double2*)d_x, ldx, c->adj_grad.as<double2>()));
+  } else {
+    HPR_CUDA_TRY(cudaMemsetAsync(c->adj_grad.p, 0, pbytes, c->stream));
+  }
+  HPR_CUDA_TRY(cudaMemcpyAsync(grad, c->adj_grad.p, pbytes, cudaMemcpyDeviceToHost, c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return HPRMAT_B200_OK;
 }
 
 int hprmat_b200_solve_linear_device(hprmat_b200_ctx* c, const void* d_A, void* d_B, int n, int nrhs,
@@ -2337,6 +2548,17 @@ int hprmat_b200_dev_panel_trace_read(hprmat_b200_ctx* c, long long* out, int cap
   return HPRMAT_B200_OK;
 }
 
+long long hprmat_b200_dev_factorizations(hprmat_b200_ctx* c, int reset) {
+  if (!c) return -1;
+  long long n = c->factorizations;
+  for (hprmat_b200_ctx* w : c->scan_workers) n += w->factorizations;
+  if (reset) {
+    c->factorizations = 0;
+    for (hprmat_b200_ctx* w : c->scan_workers) w->factorizations = 0;
+  }
+  return n;
+}
+
 int hprmat_b200_dev_mesh(int nr, int ns, double rmax, double* tc, double* blo, double* q2, double* q1,
                          double* zrma) {
   if (nr < 2 || ns < 1 || !(rmax > 0)) return fail(HPRMAT_B200_ERR_ARG, "dev_mesh: need nr >= 2, ns >= 1, rmax > 0");
@@ -2365,6 +2587,11 @@ int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* c, const char* key, int value) {
   }
   if (strcmp(key, "zero_start") == 0) {
     c->zero_start = value != 0;
+    return HPRMAT_B200_OK;
+  }
+  if (strcmp(key, "reuse_max_inner") == 0) {
+    if (value < 0) return fail(HPRMAT_B200_ERR_ARG, "reuse_max_inner must be >= 0");
+    c->reuse_max_inner = value;
     return HPRMAT_B200_OK;
   }
   if (strcmp(key, "panel_rpc_min") == 0) {

@@ -53,7 +53,14 @@ typedef struct {
                          projection R = q2^T X (what the collision matrix depends on) by less
                          than surface_tol relative (Frobenius; default 1e-11) */
   int panel_nb;    /* LU block size; 0 = automatic */
-  int reserved[4];
+  int reuse_factors; /* mixed path, one interval, local potentials: when nonzero and the previous
+                        factorisation on this context was of the same channel block (same
+                        potential -- checked by a fingerprint of cpot --, lval, mesh), rmatrix
+                        keeps it as the preconditioner of the FP64 refinement instead of
+                        factorising C(E) again: between energies C(E) changes only on the
+                        diagonal (-k^2 and the closed-channel Bloch terms).  If the refinement
+                        does not converge it factorises C(E) and solves again.  Default 0. */
+  int reserved[3];
 } hprmat_b200_opts;
 
 typedef struct {
@@ -70,6 +77,8 @@ typedef struct {
   double floor_history[9];  /* the floor estimate at each outer step */
   double residual_history[9];
   double ms_assemble, ms_factor, ms_solve, ms_refine, ms_umatrix, ms_total;
+  int factorizations;       /* LU factorisations the call ran (0: reused, opts.reuse_factors) */
+  int reserved_stats;
 } hprmat_b200_stats;
 
 /* Defaults for hprmat_b200_opts. */
@@ -95,11 +104,28 @@ int hprmat_b200_rmat_ini(hprmat_b200_ctx* ctx, int nr, int ns, double rmax, doub
    ndim), leading nopen x nopen block used; convention dL = Re sum conj(gu_ij) dU_ij, i.e.
    2 dL/dconj(U), so gu = 2 (U - T) for L = sum |U - T|^2), returns U in cu and in grad (complex
    (ncp1, ndim, ndim), as cpot) the gradient of L with respect to the potential at the mesh
-   points in the same convention (dL = Re sum conj(grad) dcpot); rows >= nr are zero.  The
-   forward solve runs on the FP64 path and the adjoint solve with C^T reuses its LU factors. */
+   points in the same convention (dL = Re sum conj(grad) dcpot); rows >= nr are zero.  With a
+   symmetric potential (cpot(i, c, c') = cpot(i, c', c)) C(E) is complex symmetric, so the
+   adjoint solution is the forward solution times a small matrix: one forward solve at the
+   context's precision (refined; opts.reuse_factors applies).  Otherwise the forward runs on
+   the FP64 path and the adjoint solve with C^T reuses its LU factors. */
 int hprmat_b200_rmatrix_adjoint(hprmat_b200_ctx* ctx, int nch, const int* lval, const double* qk, const double* eta,
                                 double rmax, int nr, int ns, const double* cpot, int ncp1, int ndim, const double* gu,
                                 double* cu, int* nopen, double* grad, hprmat_b200_stats* stats);
+
+/* The two halves of the adjoint for a symmetric potential, for callers that run all forward
+   solves before the gradients (reverse-mode autodiff): hprmat_b200_rmatrix_x is
+   hprmat_b200_rmatrix (ns = 1) that also copies the refined forward solution X = C^-1 Q
+   (complex FP64, nch*nr x nch, column-major, leading dimension ldx) into the device buffer d_x;
+   hprmat_b200_adjoint_from_x then returns the potential gradient of hprmat_b200_rmatrix_adjoint
+   from that X and the forward's U (host cu) without solving again (Y = X M2^T, C^T = C).  It
+   returns HPRMAT_B200_ERR_UNSUPPORTED for a potential that is not symmetric. */
+int hprmat_b200_rmatrix_x(hprmat_b200_ctx* ctx, int nch, const int* lval, const double* qk, const double* eta,
+                          double rmax, int nr, const double* cpot, int ncp1, int ndim, double* cu, int* nopen,
+                          void* d_x, long ldx, hprmat_b200_stats* stats);
+int hprmat_b200_adjoint_from_x(hprmat_b200_ctx* ctx, int nch, const int* lval, const double* qk, const double* eta,
+                               double rmax, int nr, const double* cpot, int ncp1, int ndim, const double* cu,
+                               const void* d_x, long ldx, const double* gu, double* grad);
 
 /* One J-pi block of a batched energy scan (hprmat_b200_rmatrix_scan).  The reference has no
    batched entry: its drivers call rmatrix once per energy in a host loop

@@ -42,8 +42,15 @@ int hprmat_b200_dev_counters(hprmat_b200_ctx* ctx, unsigned long long* launches,
      "panel_rpc_min"  fewest panel rows per CTA (32);
      "gmres_m"        longest FGMRES cycle, <= 16 (12);
      "inner_tol0_exp" first cycle runs until the residual fell 10^-value (7);
-     "zero_start"     refinement from X = 0 instead of the FP32 solution (0). */
+     "zero_start"     refinement from X = 0 instead of the FP32 solution (0);
+     "reuse_max_inner" with opts.reuse_factors, factorise again once a solve on the held
+                      factors needed more FGMRES iterations than this (24). */
 int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* ctx, const char* key, int value);
+
+/* LU factorisations run on the context and its scan workers since the last reset (opts.reuse_factors
+   makes energy scans run fewer); reset != 0 clears the count after reading.  -1 for a null
+   context. */
+long long hprmat_b200_dev_factorizations(hprmat_b200_ctx* ctx, int reset);
 
 /* The Lagrange-mesh matrices the device assembly uses, computed on the host (no context, no
    device): for every interval is (0-based, interval-major) tc[is][nr x nr] (kinetic + Bloch,

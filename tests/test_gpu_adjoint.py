@@ -34,6 +34,48 @@ def test_adjoint_matches_oracle_gradient(name):
     ctx.close()
 
 
+def test_adjoint_nonsymmetric_potential_uses_transposed_solve():
+    """A potential with cpot(c, c') != cpot(c', c): C(E) is not symmetric, the device solves with
+    C^T on its FP64 factors; the gradient agrees with the oracle's dense C^T solve."""
+    w = workloads.production(nch=10, nr=50, rmax=14.0)
+    cpot = np.array(w.cpot, order="F")
+    rng = np.random.default_rng(11)
+    tri = np.triu(rng.uniform(-0.05, 0.05, (w.nch, w.nch)), 1)
+    cpot += (tri * np.exp(-(workloads.lagrange_radii(w.nr, w.rmax) / 3.0) ** 2)[:, None, None]) / w.hm
+    assert not np.allclose(cpot, cpot.transpose(0, 2, 1))
+    mesh = orc.rmat_ini(w.nr, 1, w.rmax)
+    u_ref = orc.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, mesh, cpot).cu
+    gu = np.conj(u_ref) * 0.3 + 0.1
+    _, g_ref = orc.rmatrix_adjoint(w.nch, w.lval, w.qk, w.eta, w.rmax, mesh, cpot, gu)
+    ctx = api.Context(precision="mixed")
+    cu, nopen, g = ctx.rmatrix_adjoint(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, cpot, gu)
+    assert np.linalg.norm(cu[:nopen, :nopen] - u_ref) <= 1e-10 * np.linalg.norm(u_ref)
+    assert ctx.last_stats["factorizations"] == 1
+    err = np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref)
+    assert err <= 1e-8, err
+    ctx.close()
+
+
+def test_adjoint_with_factor_reuse_over_energies():
+    """reuse_factors on: the symmetric-potential adjoint at consecutive energies keeps one
+    factorisation; every gradient still matches the oracle."""
+    w = workloads.production(nch=16, nr=60, rmax=15.0)
+    mesh = orc.rmat_ini(w.nr, 1, w.rmax)
+    ctx = api.Context(precision="mixed", reuse_factors=True)
+    facts = 0
+    for e in (8.0, 8.4, 8.8, 9.2):
+        wk = workloads.at_energy(w, e)
+        u_ref = orc.rmatrix(w.nch, w.lval, wk.qk, wk.eta, w.rmax, mesh, w.cpot).cu
+        gu = 2 * (u_ref - np.eye(u_ref.shape[0]))
+        _, g_ref = orc.rmatrix_adjoint(w.nch, w.lval, wk.qk, wk.eta, w.rmax, mesh, w.cpot, gu)
+        cu, nopen, g = ctx.rmatrix_adjoint(w.nch, w.lval, wk.qk, wk.eta, w.rmax, w.nr, w.cpot, gu)
+        facts += ctx.last_stats["factorizations"]
+        assert np.linalg.norm(cu[:nopen, :nopen] - u_ref) <= 1e-10 * np.linalg.norm(u_ref)
+        assert np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref) <= 1e-8
+    assert facts < 4, facts
+    ctx.close()
+
+
 def test_parameter_gradients_match_central_differences():
     w = workloads.production(nch=12, nr=60, rmax=15.0)
     energies = [6.0, 12.0, 19.0]
@@ -65,4 +107,27 @@ def test_parameter_gradients_match_central_differences():
         e[k] = h * max(1.0, abs(float(p0[k])))
         fd = (float(loss(p0 + e, False)) - float(loss(p0 - e, False))) / (2 * float(e[k]))
         assert abs(fd - g[k]) <= 1e-6 * max(abs(fd), 1e-12) + 1e-9, (k, fd, g[k])
+    ctx.close()
+
+
+def test_adjoint_from_kept_forward_solution():
+    """rmatrix_x keeps X = C^-1 Q on the device; adjoint_from_x forms the gradient from it with no
+    further solve and matches rmatrix_adjoint and the oracle."""
+    w = workloads.production(nch=14, nr=60, rmax=15.0)
+    mesh = orc.rmat_ini(w.nr, 1, w.rmax)
+    u_ref = orc.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, mesh, w.cpot).cu
+    gu = 2 * (u_ref - 0.5 * np.eye(u_ref.shape[0]))
+    _, g_ref = orc.rmatrix_adjoint(w.nch, w.lval, w.qk, w.eta, w.rmax, mesh, w.cpot, gu)
+    ctx = api.Context(precision="mixed")
+    cu, nopen, x = ctx.rmatrix_x(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, w.cpot)
+    assert x.is_cuda and tuple(x.shape) == (w.nch * w.nr, w.nch)
+    assert np.linalg.norm(cu[:nopen, :nopen] - u_ref) <= 1e-10 * np.linalg.norm(u_ref)
+    g = ctx.adjoint_from_x(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, w.cpot, cu, x, gu)
+    assert np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref) <= 1e-8
+    _, _, g2 = ctx.rmatrix_adjoint(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, w.cpot, gu)
+    assert np.linalg.norm(g - g2) / np.linalg.norm(g2) <= 1e-10
+    bad = np.array(w.cpot, order="F")
+    bad[:, 0, 1] += 1e-3
+    with pytest.raises(api.HprmatError):
+        ctx.adjoint_from_x(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, bad, cu, x, gu)
     ctx.close()

@@ -51,3 +51,69 @@ def test_scan_rejects_inconsistent_blocks():
     with pytest.raises(ValueError):
         ctx.rmatrix_scan([(w.lval, w.cpot, np.zeros((2, 3)), np.zeros((2, 3)))], 10.0, 50)
     ctx.close()
+
+
+def _dense_scan_blocks():
+    """Two blocks with 24 energies each on 1..29 MeV (spacing ~1.2 MeV), unsorted, so that a
+    worker walks them in energy order and keeps its factorisation across a run."""
+    rng = np.random.default_rng(9)
+    out = []
+    for b, nch in enumerate([9, 30]):
+        w = workloads.production(seed=700 + b, nch=nch, nr=60, rmax=20.0, energy=1.0, name=f"dscan{b}")
+        energies = rng.permutation(np.linspace(1.0, 29.0, 24))
+        ks = [workloads.channel_kinematics(e, w.thresholds, w.hm, w.params.z1z2) for e in energies]
+        out.append((w, np.array([k[0] for k in ks]), np.array([k[1] for k in ks])))
+    return out
+
+
+def test_scan_with_factor_reuse_matches_oracle():
+    """opts.reuse_factors: the refinement runs on the factors of a nearby energy of the same
+    block (C(E) changes only on the diagonal between energies); every unit still agrees with
+    the oracle to 1e-10, with fewer factorisations than units."""
+    from hprmat_b200 import _native as nat
+    lib = nat.load()
+    blocks = _dense_scan_blocks()
+    ctx = api.Context(precision="mixed", reuse_factors=True)
+    lib.hprmat_b200_dev_factorizations(ctx._h, 1)
+    res = ctx.rmatrix_scan([(w.lval, w.cpot, qk, eta) for w, qk, eta in blocks], 20.0, 60, nworkers=2,
+                           raise_on_unit_error=False)
+    nfact = lib.hprmat_b200_dev_factorizations(ctx._h, 1)
+    mesh = orc.rmat_ini(60, 1, 20.0)
+    nunits = 0
+    for (w, qk, eta), (cu, nopen, status) in zip(blocks, res):
+        for e in range(qk.shape[0]):
+            if status[e] != 0:
+                continue  # COULFG cannot evaluate some channels just above threshold
+            ref = orc.rmatrix(w.nch, w.lval, qk[e], eta[e], 20.0, mesh, w.cpot)
+            no = ref.nopen
+            err = np.linalg.norm(cu[e, :no, :no] - ref.cu) / np.linalg.norm(ref.cu)
+            assert err <= U_TOL, (w.nch, e, err)
+            nunits += 1
+    assert nunits >= 40
+    assert 0 < nfact < nunits, (nfact, nunits)
+    ctx.close()
+
+
+def test_reuse_across_energies_single_calls():
+    """rmatrix with reuse_factors on one context, energies of one block in order and one far jump:
+    every result equals the oracle's (the far jump is refactorised if the refinement on the held
+    factors does not converge), and a different potential is never solved on held factors."""
+    w = workloads.production(seed=3, nch=20, nr=60, rmax=16.0)
+    mesh = orc.rmat_ini(60, 1, 16.0)
+    ctx = api.Context(precision="mixed", reuse_factors=True)
+    facts = []
+    for e in [6.0, 6.3, 6.6, 7.0, 25.0]:
+        wk = workloads.at_energy(w, e)
+        cu, nopen = ctx.rmatrix(w.nch, w.lval, wk.qk, wk.eta, 16.0, 60, 1, w.cpot)
+        ref = orc.rmatrix(w.nch, w.lval, wk.qk, wk.eta, 16.0, mesh, w.cpot)
+        err = np.linalg.norm(cu[:nopen, :nopen] - ref.cu) / np.linalg.norm(ref.cu)
+        assert err <= U_TOL, (e, err, ctx.last_stats)
+        facts.append(ctx.last_stats["factorizations"])
+    assert facts[0] == 1 and sum(facts[1:4]) == 0, facts
+    # a different potential is never solved with the held factors
+    w2 = workloads.production(seed=4, nch=20, nr=60, rmax=16.0)
+    cu, nopen = ctx.rmatrix(w2.nch, w2.lval, w2.qk, w2.eta, 16.0, 60, 1, w2.cpot)
+    assert ctx.last_stats["factorizations"] == 1
+    ref = orc.rmatrix(w2.nch, w2.lval, w2.qk, w2.eta, 16.0, mesh, w2.cpot)
+    assert np.linalg.norm(cu[:nopen, :nopen] - ref.cu) / np.linalg.norm(ref.cu) <= U_TOL
+    ctx.close()
