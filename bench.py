@@ -53,9 +53,10 @@ def parse():
                          "scan, 12 J-pi blocks x 256 energies (3072 solves) per step; adjoint: loss and gradients "
                          "over 64 energies at N = 3200 per step")
     ap.add_argument("--workers", type=int, default=4, help="worker streams of the batched scan")
-    ap.add_argument("--reuse", type=int, default=1,
+    ap.add_argument("--reuse", type=int, default=-1,
                     help="scan/adjoint: keep a block's factorisation across energies as the refinement's "
-                         "preconditioner (opts.reuse_factors); 0 factorises every energy")
+                         "preconditioner (opts.reuse_factors); 0 factorises every energy; default: on for "
+                         "the scan, off for the adjoint (measured faster that way)")
     return ap.parse_args()
 
 
@@ -191,6 +192,8 @@ def run_scan(args):
         inputs.append((w.lval, w.cpot, np.array([k[0] for k in ks]), np.array([k[1] for k in ks])))
         flops += len(energies) * 8.0 * float(w.n) ** 3 / 3.0
     nunits = sum(len(e) for _, e in mine)
+    if args.reuse < 0:
+        args.reuse = 1
     ctx = api.Context(device=local, precision="mixed", max_refine=3, tol=1e-12, reuse_factors=bool(args.reuse))
     from hprmat_b200 import _native as nat
     lib = nat.load()
@@ -276,7 +279,8 @@ def run_scan(args):
 def run_adjoint(args):
     """One step = loss sum_E sum |U - U_target|^2 over 64 energies at N = 3200 (32 channels x
     100 points) and its gradient with respect to the 6 potential parameters and the potential
-    at all mesh points (torch.autograd through hprmat_b200_rmatrix_adjoint).  Checked once
+    at all mesh points (torch.autograd: forward solves keep X on the device, the backward forms
+    the gradient from it, hprmat_b200_rmatrix_x / hprmat_b200_adjoint_from_x).  Checked once
     against central finite differences (step 1e-6) of the device forward and against the FP64
     oracle adjoint at two energies."""
     import torch
@@ -288,6 +292,8 @@ def run_adjoint(args):
     coup = torch.from_numpy(w.coupling)
     p0 = torch.tensor(w.params.as_array(), dtype=torch.float64)
     ptarget = p0 * torch.tensor([1.02, 0.97, 1.01, 1.03, 0.95, 1.04], dtype=torch.float64)
+    if args.reuse < 0:
+        args.reuse = 0
     ctx = api.Context(precision="mixed", max_refine=8, tol=1e-12, reuse_factors=bool(args.reuse))
     from hprmat_b200 import _native as nat
     lib = nat.load()
@@ -355,7 +361,8 @@ def run_adjoint(args):
         "config": {"workload": "adjoint: 32 channels x 100 points (N = 3200), 64 energies, loss sum |U - U_target|^2, "
                                "gradients w.r.t. 6 potential parameters and the potential at all mesh points"},
         "energies_used": len(kin), "energies_dropped_coulfg": len(kin_all) - len(kin),
-        "solves_per_step": 2 * len(kin), "factorizations_per_step": nfact, "reuse_factors": bool(args.reuse),
+        "solves_per_step": len(kin), "factorizations_per_step": nfact, "reuse_factors": bool(args.reuse),
+        "backward": "symmetric potential: gradient from the forward solution kept on the device (no second solve)",
         "fd_rel_err_max": fd_err, "fd_step": 1e-6, "oracle_grad_rel_err_max": ref_err,
         "loss": float(L.detach())}))
     ctx.close()
