@@ -19,6 +19,8 @@
 // forward solve applies each step's interchanges to the right-hand side just before that
 // step's block column, which is consistent with the factors stored that way.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 
 namespace hprmat {
@@ -64,6 +66,80 @@ constexpr int kPanelTraceW = 5 + 160;
 // of each other are equally good pivots.)
 __device__ __forceinline__ unsigned long long pivot_key(float v, int row) {
   return ((unsigned long long)__float_as_uint(v) << 32) | (unsigned long long)(0xFFFFFFFFu - (unsigned)row);
+}
+
+// End of a panel factorisation, shared by both panel kernels: the CTA's factored rows back
+// into W, its L21 rows into the LU planes (mixed path), and from CTA 0 the pivots, the growth
+// and the step's row-interchange list.
+template <typename T, int NB, int NT>
+__device__ void panel_finish(const PanelArgs<T>& a, const T* P, int rpcp, int r0, int nloc, const int* s_loc_ipiv,
+                             unsigned s_growth, int b, int tid) {
+  const int ncols = a.ncols;
+  // write the factored rows back
+  for (int c = 0; c < ncols; ++c)
+    for (int lr = tid; lr < nloc; lr += NT)
+      a.W[(size_t)(a.k0 + r0 + lr) + (size_t)(a.k0 + c) * a.ld] = P[(size_t)c * rpcp + lr];
+  // L21 rows into the LU planes (mixed path): global row k0 + g, columns k0 .. k0+ncols
+  if (a.lup != nullptr) {
+    const int lr0 = max(ncols - r0, 0);
+    const int nl = nloc - lr0;
+    for (int idx = tid; idx < nl * ncols; idx += NT) {
+      int c = idx % ncols;
+      int lr = lr0 + idx / ncols;
+      size_t off = (size_t)(a.k0 + r0 + lr) * a.lup_ld + (size_t)(a.k0 + c);
+      float hr, lrr, hi_, li;
+      T v = P[(size_t)c * rpcp + lr];
+      tf32_split((float)v.x, hr, lrr);
+      tf32_split((float)v.y, hi_, li);
+      a.lup[off] = hr;
+      a.lup[a.lup_plane + off] = lrr;
+      a.lup[2 * a.lup_plane + off] = hi_;
+      a.lup[3 * a.lup_plane + off] = li;
+    }
+  }
+  if (b == 0) {
+    __syncthreads();
+    if (tid < ncols) a.ipiv[a.k0 + tid] = a.k0 + s_loc_ipiv[tid];
+    if (tid == 0 && a.growth_bits) atomicMax(a.growth_bits, s_growth);
+    // Row-interchange list of this step: simulate the swaps on the touched positions.
+    if (tid < 32) {
+      __shared__ int pos[2 * NB], src[2 * NB];
+      __shared__ int cnt;
+      for (int j = tid; j < ncols; j += 32) { pos[j] = a.k0 + j; src[j] = a.k0 + j; }
+      if (tid == 0) cnt = ncols;
+      __syncwarp();
+      for (int j = 0; j < ncols; ++j) {
+        int bp = a.k0 + s_loc_ipiv[j];
+        if (bp == a.k0 + j) continue;
+        int slot;
+        if (bp < a.k0 + ncols) {
+          slot = bp - a.k0;
+        } else {
+          int found = -1;
+          for (int base = ncols; base < cnt; base += 32) {
+            int s = base + tid;
+            unsigned m_ = __ballot_sync(0xffffffffu, s < cnt && pos[s] == bp);
+            if (m_) { found = base + __ffs(m_) - 1; break; }
+          }
+          if (found < 0) {
+            if (tid == 0) { pos[cnt] = bp; src[cnt] = bp; cnt = cnt + 1; }
+            __syncwarp();
+            found = cnt - 1;
+          }
+          slot = found;
+        }
+        if (tid == 0) { int t = src[j]; src[j] = src[slot]; src[slot] = t; }
+        __syncwarp();
+      }
+      for (int j = tid; j < ncols; j += 32) a.sw.top_src[j] = src[j];
+      if (tid == 0) {
+        int ne = 0;
+        for (int s = ncols; s < cnt; ++s)
+          if (src[s] != pos[s]) { a.sw.extra_dst[ne] = pos[s]; a.sw.extra_src[ne] = src[s]; ++ne; }
+        *a.sw.n_extra = ne;
+      }
+    }
+  }
 }
 
 template <typename T, int NB, int NT>
@@ -256,71 +332,204 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
     if (tr && b == 0 && tid == 0) tr[4] = device_ns();
   }
 
-  // write the factored rows back
+  panel_finish<T, NB, NT>(a, P, rpcp, r0, nloc, s_loc_ipiv, s_growth, b, tid);
+}
+
+// -------------------------------------------------------------------------------------
+// The panel factorisation of panel_kernel for panels whose rows fit in one thread-block
+// cluster (G <= 16 CTAs, the whole grid): the same algorithm and look-ahead, with the
+// per-column exchange in distributed shared memory instead of global memory.  Each CTA posts
+// its pivot key, its candidate row and (the owner) row j in its own shared memory; after the
+// hardware cluster barrier every CTA reads the G keys, picks the same pivot and reads the two
+// rows from their owners.  Double buffering by column parity is safe because a CTA posts
+// column j + 2 only after the barrier of column j + 1, which every CTA reaches after reading
+// column j.  There is no polling: the waits are the cluster barrier's.  Dynamic shared
+// memory: P [NB][rpc|1], urow [NB], candidate rows [2][NB], rows j [2][NB], keys [2].
+namespace cgx = cooperative_groups;
+
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+
+template <typename T>
+__host__ __device__ constexpr size_t panel_cluster_smem(int rpc, int nb) {
+  return ((size_t)nb * (size_t)(rpc | 1) + 5 * (size_t)nb) * sizeof(T) + 2 * sizeof(unsigned long long) + 16;
+}
+
+template <typename T, int NB, int NT>
+__global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(PanelArgs<T> a) {
+  using R = typename RealOf<T>::R;
+  cgx::cluster_group cluster = cgx::this_cluster();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int m = a.N - a.k0;
+  const int b = (int)cluster.block_rank();
+  const int r0 = b * a.rpc;
+  const int r1 = min(r0 + a.rpc, m);
+  const int nloc = max(r1 - r0, 0);
+  const int rpcp = a.rpc | 1;
+  T* P = reinterpret_cast<T*>(smem_raw);  // [NB][rpcp] column-major
+  T* urow = P + (size_t)NB * rpcp;        // [NB]
+  T* xrow = urow + NB;                    // [2][NB] candidate row posted by this CTA
+  T* xrowj = xrow + 2 * NB;               // [2][NB] row j, posted by its owner
+  unsigned long long* xkey = reinterpret_cast<unsigned long long*>(xrowj + 2 * NB);  // [2]
+  __shared__ float red_v[NT / 32];
+  __shared__ int red_i[NT / 32];
+  __shared__ int s_piv, s_loc_ipiv[NB];
+  __shared__ unsigned s_growth;
+  __shared__ unsigned long long s_key;
+  const int tid = threadIdx.x;
+  const int ncols = a.ncols;
+
   for (int c = 0; c < ncols; ++c)
     for (int lr = tid; lr < nloc; lr += NT)
-      a.W[(size_t)(a.k0 + r0 + lr) + (size_t)(a.k0 + c) * a.ld] = P[(size_t)c * rpcp + lr];
-  // L21 rows into the LU planes (mixed path): global row k0 + g, columns k0 .. k0+ncols
-  if (a.lup != nullptr) {
-    const int lr0 = max(ncols - r0, 0);
-    const int nl = nloc - lr0;
-    for (int idx = tid; idx < nl * ncols; idx += NT) {
-      int c = idx % ncols;
-      int lr = lr0 + idx / ncols;
-      size_t off = (size_t)(a.k0 + r0 + lr) * a.lup_ld + (size_t)(a.k0 + c);
-      float hr, lrr, hi_, li;
-      T v = P[(size_t)c * rpcp + lr];
-      tf32_split((float)v.x, hr, lrr);
-      tf32_split((float)v.y, hi_, li);
-      a.lup[off] = hr;
-      a.lup[a.lup_plane + off] = lrr;
-      a.lup[2 * a.lup_plane + off] = hi_;
-      a.lup[3 * a.lup_plane + off] = li;
+      P[(size_t)c * rpcp + lr] = a.W[(size_t)(a.k0 + r0 + lr) + (size_t)(a.k0 + c) * a.ld];
+  if (tid == 0) s_growth = 0u;
+  __syncthreads();
+
+  // column jc's local candidate into s_piv and its key into xkey[jc & 1]
+  auto candidate = [&](int jc, float bv, int bi) {
+    for (int o = 16; o > 0; o >>= 1) {
+      float ov = __shfl_down_sync(0xffffffffu, bv, o);
+      int oi = __shfl_down_sync(0xffffffffu, bi, o);
+      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
     }
-  }
-  if (b == 0) {
+    if ((tid & 31) == 0) { red_v[tid >> 5] = bv; red_i[tid >> 5] = bi; }
     __syncthreads();
-    if (tid < ncols) a.ipiv[a.k0 + tid] = a.k0 + s_loc_ipiv[tid];
-    if (tid == 0 && a.growth_bits) atomicMax(a.growth_bits, s_growth);
-    // Row-interchange list of this step: simulate the swaps on the touched positions.
     if (tid < 32) {
-      __shared__ int pos[2 * NB], src[2 * NB];
-      __shared__ int cnt;
-      for (int j = tid; j < ncols; j += 32) { pos[j] = a.k0 + j; src[j] = a.k0 + j; }
-      if (tid == 0) cnt = ncols;
-      __syncwarp();
-      for (int j = 0; j < ncols; ++j) {
-        int bp = a.k0 + s_loc_ipiv[j];
-        if (bp == a.k0 + j) continue;
-        int slot;
-        if (bp < a.k0 + ncols) {
-          slot = bp - a.k0;
-        } else {
-          int found = -1;
-          for (int base = ncols; base < cnt; base += 32) {
-            int s = base + tid;
-            unsigned m_ = __ballot_sync(0xffffffffu, s < cnt && pos[s] == bp);
-            if (m_) { found = base + __ffs(m_) - 1; break; }
-          }
-          if (found < 0) {
-            if (tid == 0) { pos[cnt] = bp; src[cnt] = bp; cnt = cnt + 1; }
-            __syncwarp();
-            found = cnt - 1;
-          }
-          slot = found;
-        }
-        if (tid == 0) { int t = src[j]; src[j] = src[slot]; src[slot] = t; }
-        __syncwarp();
+      bv = (tid < NT / 32) ? red_v[tid] : -1.f;
+      bi = (tid < NT / 32) ? red_i[tid] : 0x7fffffff;
+      for (int o = 16; o > 0; o >>= 1) {
+        float ov = __shfl_down_sync(0xffffffffu, bv, o);
+        int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
       }
-      for (int j = tid; j < ncols; j += 32) a.sw.top_src[j] = src[j];
       if (tid == 0) {
-        int ne = 0;
-        for (int s = ncols; s < cnt; ++s)
-          if (src[s] != pos[s]) { a.sw.extra_dst[ne] = pos[s]; a.sw.extra_src[ne] = src[s]; ++ne; }
-        *a.sw.n_extra = ne;
+        s_piv = bi;
+        xkey[jc & 1] = bi != 0x7fffffff ? pivot_key(bv, bi) : 0ull;
       }
     }
+    __syncthreads();
+  };
+  auto post = [&](int jc, bool pend) {
+    const int pb = jc & 1;
+    const int ci = s_piv;
+    const bool have = ci != 0x7fffffff;
+    const bool own = jc >= r0 && jc < r1;
+    for (int c = tid; c < ncols; c += NT) {
+      if (have) {
+        T v = P[(size_t)c * rpcp + (ci - r0)];
+        if (pend && c > jc) cfms(v, P[(size_t)(jc - 1) * rpcp + (ci - r0)], urow[c]);
+        xrow[pb * NB + c] = v;
+      }
+      if (own) {
+        T v = P[(size_t)c * rpcp + (jc - r0)];
+        if (pend && c > jc) cfms(v, P[(size_t)(jc - 1) * rpcp + (jc - r0)], urow[c]);
+        xrowj[pb * NB + c] = v;
+      }
+    }
+  };
+
+  {
+    float bv = -1.f;
+    int bi = 0x7fffffff;
+    for (int lr = tid; lr < nloc; lr += NT) {
+      float v = (float)cabs1(P[lr]);
+      if (v > bv) { bv = v; bi = r0 + lr; }
+    }
+    candidate(0, bv, bi);
+    post(0, false);
+    cluster_arrive();
   }
+  const int warp = tid >> 5, lane = tid & 31;
+  for (int j = 0; j < ncols; ++j) {
+    const int buf = j & 1;
+    cluster_wait();
+    // the largest posted key names the pivot row (the lowest row among equal moduli)
+    if (tid < 32) {
+      unsigned long long k = 0ull;
+      for (int t = tid; t < a.G; t += 32) {
+        const unsigned long long v = *cluster.map_shared_rank(xkey + buf, (unsigned)t);
+        k = v > k ? v : k;
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long v = __shfl_down_sync(0xffffffffu, k, o);
+        k = v > k ? v : k;
+      }
+      if (tid == 0) s_key = k;
+    }
+    __syncthreads();
+    const int p = (int)(0xFFFFFFFFu - (unsigned)(s_key & 0xFFFFFFFFull));
+    const T* wrow = cluster.map_shared_rank(xrow + buf * NB, (unsigned)(p / a.rpc));
+    const T* jrow = cluster.map_shared_rank(xrowj + buf * NB, (unsigned)(j / a.rpc));
+    float g = 0.f;
+    for (int c = tid; c < ncols; c += NT) {
+      T u = wrow[c];
+      urow[c] = u;
+      if (p != j && p >= r0 && p < r1) P[(size_t)c * rpcp + (p - r0)] = jrow[c];
+      if (p != j && j >= r0 && j < r1) P[(size_t)c * rpcp + (j - r0)] = u;
+      if (c >= j) g = fmaxf(g, (float)cabs1(u));
+    }
+    if (tid < ((ncols + 31) & ~31)) {
+      for (int o = 16; o > 0; o >>= 1) g = fmaxf(g, __shfl_down_sync(0xffffffffu, g, o));
+      if ((tid & 31) == 0 && g > 0.f) atomicMax(&s_growth, __float_as_uint(g));
+    }
+    if (tid == 0) s_loc_ipiv[j] = p;
+    __syncthreads();
+    const T piv = urow[j];
+    const bool zero = (piv.x == R(0) && piv.y == R(0));
+    if (zero && b == 0 && tid == 0) atomicCAS(a.status + SW_INFO, 0, a.k0 + j + 1);
+    const T inv = zero ? czero<T>() : crecip(piv);
+    const int lo = max(j + 1 - r0, 0);
+    if (j + 1 < ncols) {
+      const int jn = j + 1;
+      float bv = -1.f;
+      int bi = 0x7fffffff;
+      for (int lr = lo + tid; lr < nloc; lr += NT) {
+        T l = P[(size_t)j * rpcp + lr];
+        if (!zero) {
+          l = cmul(l, inv);
+          P[(size_t)j * rpcp + lr] = l;
+        }
+        T v = P[(size_t)jn * rpcp + lr];
+        cfms(v, l, urow[jn]);
+        P[(size_t)jn * rpcp + lr] = v;
+        float av = (float)cabs1(v);
+        if (av > bv) { bv = av; bi = r0 + lr; }
+      }
+      candidate(jn, bv, bi);
+      post(jn, true);
+      cluster_arrive();
+      constexpr int NW = NT / 32;
+      for (int lr = lo + lane; lr < nloc; lr += 32) {
+        const T l = P[(size_t)j * rpcp + lr];
+        int c = jn + 1 + warp;
+        for (; c + 3 * NW < ncols; c += 4 * NW) {
+          T v[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) v[q] = P[(size_t)(c + q * NW) * rpcp + lr];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            cfms(v[q], l, urow[c + q * NW]);
+            P[(size_t)(c + q * NW) * rpcp + lr] = v[q];
+          }
+        }
+        for (; c < ncols; c += NW) {
+          T v = P[(size_t)c * rpcp + lr];
+          cfms(v, l, urow[c]);
+          P[(size_t)c * rpcp + lr] = v;
+        }
+      }
+      __syncthreads();
+    } else {
+      for (int lr = lo + tid; lr < nloc; lr += NT) {
+        if (!zero) P[(size_t)j * rpcp + lr] = cmul(P[(size_t)j * rpcp + lr], inv);
+      }
+      __syncthreads();
+    }
+  }
+  // no CTA leaves while another may still read its shared memory
+  cluster_arrive();
+  cluster_wait();
+  panel_finish<T, NB, NT>(a, P, rpcp, r0, nloc, s_loc_ipiv, s_growth, b, tid);
 }
 
 // -------------------------------------------------------------------------------------

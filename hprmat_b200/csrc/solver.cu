@@ -127,6 +127,9 @@ struct hprmat_b200_ctx {
   bool wave_enabled = true;  // wavefront solves (else block-step solves)
   bool tc_trsm = true;       // U12 by the tensor cores from L11^-1 (else substitution)
   int panel_rpc_min = 32;    // fewest panel rows per CTA
+  bool panel_cluster = true;  // panels that fit in one 16-CTA cluster use panel_cluster_kernel
+  signed char cluster_ok[2][17] = {};  // per element size (float2, double2) and cluster size:
+                                       // 0 unknown, 1 schedulable, -1 not
   int gmres_m = 12;          // longest FGMRES cycle per outer step (<= kGmresMaxM)
   double inner_tol0 = 1e-7;  // first cycle stops once the residual fell this much
   bool zero_start = false;   // refinement starts from X = 0 instead of the FP32 solution
@@ -533,11 +536,177 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
     }
   }
 
+  // after the panel of step s: row interchanges, U12 = L11^-1 P A12 and the trailing update
+  auto after_panel = [&](int s, int k0, int ncols, const StepSwaps& sw) -> int {
+    (void)s;
+    // row interchanges + U12 = L11^-1 A12
+    if (mixed && c->tc_trsm) {
+      // L11^-1 (as I - L11^-1 operand planes), P A12 gathered, U12 by one tensor-core GEMM
+      constexpr int CW = 32;
+      const size_t ism = ((size_t)NB * NB + (size_t)(NB / 2) * (NB / 2)) * sizeof(float2);
+      constexpr int NTI = 512;
+      auto ik = l11_inverse_planes_kernel<NB, NTI>;
+      TRY(set_smem(ik, ism));
+      ik<<<1, NTI, ism, c->stream>>>(reinterpret_cast<const float2*>(W), ld, k0, ncols, c->linv.as<float>(),
+                                     (long)NB * NB);
+      LAUNCH_CHECK();
+      auto gk = swap_gather_kernel<NB, CW, NT>;
+      const size_t gsm = (size_t)CW * (NB + 1) * sizeof(float2) + (size_t)CW * NB * sizeof(float2);
+      TRY(set_smem(gk, gsm));
+      gk<<<cdiv_u(N - k0 - ncols, CW), NT, gsm, c->stream>>>(reinterpret_cast<float2*>(W), ld, k0, ncols,
+                                                              sw.top_src, sw.extra_dst, sw.extra_src,
+                                                              sw.n_extra, k0 + ncols, N, bop, plane);
+      LAUNCH_CHECK();
+      if (tc_update(c->tcplan, c->op_linv, 0, 0, c->op_bop, 0, 0, NB,
+                    reinterpret_cast<float2*>(W) + k0 + (size_t)(k0 + ncols) * ld, ld, ncols, N - k0 - ncols, 128,
+                    c->stream))
+        return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+      ++c->launches;
+      auto uk = u12_split_kernel<NB, CW, NT>;
+      uk<<<cdiv_u(N - k0 - ncols, CW), NT, 0, c->stream>>>(reinterpret_cast<const float2*>(W), ld, k0, ncols,
+                                                             k0 + ncols, N, bop, plane, c->lup.as<float>(),
+                                                             c->lup_ld, c->lup_plane, growth);
+      LAUNCH_CHECK();
+    } else {
+      constexpr int CW = 32;
+      auto tk = trsm_lower_kernel<T, NB, CW, NT>;
+      size_t tsm = (size_t)CW * (NB + 1) * sizeof(T) + (size_t)CW * NB * sizeof(T);
+      TRY(set_smem(tk, tsm));
+      TrsmArgs<T> ta{};
+      ta.W = W;
+      ta.ld = ld;
+      ta.k0 = k0;
+      ta.ncols = ncols;
+      ta.top_src = sw.top_src;
+      ta.extra_dst = sw.extra_dst;
+      ta.extra_src = sw.extra_src;
+      ta.n_extra = sw.n_extra;
+      ta.X = W;
+      ta.ldx = ld;
+      ta.c_begin = k0 + ncols;
+      ta.c_end = N;
+      ta.growth_bits = growth;
+      if (mixed) {  // U12 also as the B operand of the trailing update and into the LU planes
+        ta.bop = bop;
+        ta.bop_plane = plane;
+        ta.bop_col0 = k0 + ncols;
+        ta.lup = c->lup.as<float>();
+        ta.lup_ld = c->lup_ld;
+        ta.lup_plane = c->lup_plane;
+      }
+      tk<<<cdiv_u(N - k0 - ncols, CW), NT, tsm, c->stream>>>(ta);
+      LAUNCH_CHECK();
+    }
+    // trailing update A22 -= L21 U12
+    const int M2 = N - k0 - ncols;
+    if (mixed) {
+      const bool prof = c->profile && c->ev_used + 2 <= (int)c->ev.size();
+      if (prof) HPR_CUDA_TRY(cudaEventRecord(c->ev[c->ev_used], c->stream));
+      if (tc_update(c->tcplan, c->op_lu, k0, k0 + ncols, c->op_bop, 0, 0, NB,
+                    reinterpret_cast<float2*>(W) + (k0 + ncols) + (size_t)(k0 + ncols) * ld, ld, M2, M2, 128,
+                    c->stream))
+        return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+      ++c->launches;
+      if (prof) {
+        HPR_CUDA_TRY(cudaEventRecord(c->ev[c->ev_used + 1], c->stream));
+        c->ev_flops.push_back(8.0 * (double)M2 * (double)M2 * (double)NB);
+        c->ev_used += 2;
+      }
+    } else {
+      dim3 grid(cdiv_u(M2, 64), cdiv_u(M2, 64));
+      cgemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(M2, M2, ncols, W + (k0 + ncols) + (size_t)k0 * ld, ld,
+                                                         W + k0 + (size_t)(k0 + ncols) * ld, ld,
+                                                         W + (k0 + ncols) + (size_t)(k0 + ncols) * ld, ld);
+      LAUNCH_CHECK();
+    }
+    return HPRMAT_B200_OK;
+  };
   auto pk = panel_kernel<T, NB, NT>;
+  auto pkc = panel_cluster_kernel<T, NB, NT>;
+  // the largest rows per CTA of a cluster panel (shared memory of the opt-in limit, less the
+  // static arrays)
+  int rpc_max_c = 0;
+  while (panel_cluster_smem<T>(rpc_max_c + 1, NB) + 4096 <= (size_t)c->smem_optin) ++rpc_max_c;
+  auto cluster_fits = [&](int g) -> bool {  // can the GPU hold a cluster of g such CTAs
+    signed char& ok = c->cluster_ok[sizeof(T) == sizeof(double2)][g];
+    if (ok == 0) {
+      const size_t sm = panel_cluster_smem<T>(rpc_max_c, NB);
+      ok = -1;
+      if (cudaFuncSetAttribute((const void*)pkc, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess &&
+          set_smem(pkc, sm) == HPRMAT_B200_OK) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(g);
+        cfg.blockDim = dim3(NT);
+        cfg.dynamicSmemBytes = sm;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = g;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, (const void*)pkc, &cfg) == cudaSuccess && n >= 1) ok = 1;
+      }
+      cudaGetLastError();
+    }
+    return ok == 1;
+  };
   for (int s = 0; s < nsteps; ++s) {
     const int k0 = s * NB;
     const int ncols = std::min(NB, N - k0);
     const int m = N - k0;
+    if (c->panel_cluster && rpc_max_c > 0 && m <= 16 * rpc_max_c) {
+      // the whole panel in one cluster: as many CTAs as panel_rpc_min rows allow, at most 16
+      const int Gc = std::min(16, std::max((m + rpc_max_c - 1) / rpc_max_c, (m + c->panel_rpc_min - 1) / c->panel_rpc_min));
+      if (cluster_fits(Gc)) {
+        const int rpcc = (m + Gc - 1) / Gc;
+        const size_t smc = panel_cluster_smem<T>(rpcc, NB);
+        TRY(set_smem(pkc, smc));
+        PanelArgs<T> pa;
+        pa.W = W;
+        pa.ld = ld;
+        pa.N = N;
+        pa.k0 = k0;
+        pa.ncols = ncols;
+        pa.rpc = rpcc;
+        pa.G = Gc;
+        pa.ipiv = c->ipiv.as<int>();
+        pa.cand_rows = nullptr;
+        pa.keys = nullptr;
+        pa.rowj = nullptr;
+        pa.status = status;
+        int* swb = c->swaps.as<int>() + (size_t)s * kSwapStride;
+        pa.sw.top_src = swb;
+        pa.sw.extra_dst = swb + kMaxNB;
+        pa.sw.extra_src = swb + 2 * kMaxNB;
+        pa.sw.n_extra = swb + 3 * kMaxNB;
+        pa.growth_bits = growth;
+        pa.lup = (mixed && k0 + ncols < N) ? c->lup.as<float>() : nullptr;
+        pa.lup_ld = c->lup_ld;
+        pa.lup_plane = c->lup_plane;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(Gc);
+        cfg.blockDim = dim3(NT);
+        cfg.dynamicSmemBytes = smc;
+        cfg.stream = c->stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = Gc;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        const cudaError_t e = cudaLaunchKernelEx(&cfg, pkc, pa);
+        if (e != cudaSuccess)
+          return fail(HPRMAT_B200_ERR_CUDA, "cluster panel launch (step %d, %d CTAs of %d rows, %zu B shared): %s", s,
+                      Gc, rpcc, smc, cudaGetErrorString(e));
+        ++c->launches;
+        if (k0 + ncols >= N) break;
+        TRY(after_panel(s, k0, ncols, pa.sw));
+        continue;
+      }
+    }
     // CTAs of the panel: at least panel_rpc_min rows each (fewer CTAs contend less for the
     // per-column barrier), as many as the shared memory needs
     const int rpc_max = (int)(((size_t)c->smem_optin - 8192) / sizeof(T) / NB) - 2;
@@ -589,86 +758,7 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
     }
     ++c->launches;
     if (k0 + ncols >= N) break;
-    // row interchanges + U12 = L11^-1 A12
-    if (mixed && c->tc_trsm) {
-      // L11^-1 (as I - L11^-1 operand planes), P A12 gathered, U12 by one tensor-core GEMM
-      constexpr int CW = 32;
-      const size_t ism = ((size_t)NB * NB + (size_t)(NB / 2) * (NB / 2)) * sizeof(float2);
-      constexpr int NTI = 512;
-      auto ik = l11_inverse_planes_kernel<NB, NTI>;
-      TRY(set_smem(ik, ism));
-      ik<<<1, NTI, ism, c->stream>>>(reinterpret_cast<const float2*>(W), ld, k0, ncols, c->linv.as<float>(),
-                                     (long)NB * NB);
-      LAUNCH_CHECK();
-      auto gk = swap_gather_kernel<NB, CW, NT>;
-      const size_t gsm = (size_t)CW * (NB + 1) * sizeof(float2) + (size_t)CW * NB * sizeof(float2);
-      TRY(set_smem(gk, gsm));
-      gk<<<cdiv_u(N - k0 - ncols, CW), NT, gsm, c->stream>>>(reinterpret_cast<float2*>(W), ld, k0, ncols,
-                                                              pa.sw.top_src, pa.sw.extra_dst, pa.sw.extra_src,
-                                                              pa.sw.n_extra, k0 + ncols, N, bop, plane);
-      LAUNCH_CHECK();
-      if (tc_update(c->tcplan, c->op_linv, 0, 0, c->op_bop, 0, 0, NB,
-                    reinterpret_cast<float2*>(W) + k0 + (size_t)(k0 + ncols) * ld, ld, ncols, N - k0 - ncols, 128,
-                    c->stream))
-        return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
-      ++c->launches;
-      auto uk = u12_split_kernel<NB, CW, NT>;
-      uk<<<cdiv_u(N - k0 - ncols, CW), NT, 0, c->stream>>>(reinterpret_cast<const float2*>(W), ld, k0, ncols,
-                                                             k0 + ncols, N, bop, plane, c->lup.as<float>(),
-                                                             c->lup_ld, c->lup_plane, growth);
-      LAUNCH_CHECK();
-    } else {
-      constexpr int CW = 32;
-      auto tk = trsm_lower_kernel<T, NB, CW, NT>;
-      size_t tsm = (size_t)CW * (NB + 1) * sizeof(T) + (size_t)CW * NB * sizeof(T);
-      TRY(set_smem(tk, tsm));
-      TrsmArgs<T> ta{};
-      ta.W = W;
-      ta.ld = ld;
-      ta.k0 = k0;
-      ta.ncols = ncols;
-      ta.top_src = pa.sw.top_src;
-      ta.extra_dst = pa.sw.extra_dst;
-      ta.extra_src = pa.sw.extra_src;
-      ta.n_extra = pa.sw.n_extra;
-      ta.X = W;
-      ta.ldx = ld;
-      ta.c_begin = k0 + ncols;
-      ta.c_end = N;
-      ta.growth_bits = growth;
-      if (mixed) {  // U12 also as the B operand of the trailing update and into the LU planes
-        ta.bop = bop;
-        ta.bop_plane = plane;
-        ta.bop_col0 = k0 + ncols;
-        ta.lup = c->lup.as<float>();
-        ta.lup_ld = c->lup_ld;
-        ta.lup_plane = c->lup_plane;
-      }
-      tk<<<cdiv_u(N - k0 - ncols, CW), NT, tsm, c->stream>>>(ta);
-      LAUNCH_CHECK();
-    }
-    // trailing update A22 -= L21 U12
-    const int M2 = N - k0 - ncols;
-    if (mixed) {
-      const bool prof = c->profile && c->ev_used + 2 <= (int)c->ev.size();
-      if (prof) HPR_CUDA_TRY(cudaEventRecord(c->ev[c->ev_used], c->stream));
-      if (tc_update(c->tcplan, c->op_lu, k0, k0 + ncols, c->op_bop, 0, 0, NB,
-                    reinterpret_cast<float2*>(W) + (k0 + ncols) + (size_t)(k0 + ncols) * ld, ld, M2, M2, 128,
-                    c->stream))
-        return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
-      ++c->launches;
-      if (prof) {
-        HPR_CUDA_TRY(cudaEventRecord(c->ev[c->ev_used + 1], c->stream));
-        c->ev_flops.push_back(8.0 * (double)M2 * (double)M2 * (double)NB);
-        c->ev_used += 2;
-      }
-    } else {
-      dim3 grid(cdiv_u(M2, 64), cdiv_u(M2, 64));
-      cgemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(M2, M2, ncols, W + (k0 + ncols) + (size_t)k0 * ld, ld,
-                                                         W + k0 + (size_t)(k0 + ncols) * ld, ld,
-                                                         W + (k0 + ncols) + (size_t)(k0 + ncols) * ld, ld);
-      LAUNCH_CHECK();
-    }
+    TRY(after_panel(s, k0, ncols, pa.sw));
   }
   // explicit inverses of the diagonal blocks for the solves
   {
@@ -2587,6 +2677,10 @@ int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* c, const char* key, int value) {
   }
   if (strcmp(key, "zero_start") == 0) {
     c->zero_start = value != 0;
+    return HPRMAT_B200_OK;
+  }
+  if (strcmp(key, "panel_cluster") == 0) {
+    c->panel_cluster = value != 0;
     return HPRMAT_B200_OK;
   }
   if (strcmp(key, "reuse_max_inner") == 0) {

@@ -40,6 +40,8 @@ int hprmat_b200_dev_counters(hprmat_b200_ctx* ctx, unsigned long long* launches,
      "wave"           wavefront solves on/off (1);
      "tc_trsm"        U12 by a tensor-core product with L11^-1 (1) or by substitution (0);
      "panel_rpc_min"  fewest panel rows per CTA (32);
+     "panel_cluster"  panels that fit in one cluster of at most 16 CTAs exchange pivots in
+                      distributed shared memory (1) or always through global memory (0);
      "gmres_m"        longest FGMRES cycle, <= 16 (12);
      "inner_tol0_exp" first cycle runs until the residual fell 10^-value (7);
      "zero_start"     refinement from X = 0 instead of the FP32 solution (0);
