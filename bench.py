@@ -173,8 +173,10 @@ def run_reference(args):
 # ------------------------------------------------------------------ batched energy scan
 def run_scan(args):
     """One step = the whole scan: 12 J-pi blocks (nch ~ U{4..64}, 60 mesh points, N = 240..3840)
-    x 256 energies = 3072 collision matrices, through hprmat_b200_rmatrix_scan.  Rank r of N
-    takes the blocks b with b % N == r (independent units, no collective)."""
+    x 256 energies = 3072 collision matrices, through hprmat_b200_rmatrix_scan.  With N ranks
+    the blocks are sharded by cost (hprmat_b200.scan_shard.lpt_shards: greedy longest
+    processing time on nenergies x N^3 over runs of 32 energies), independent units, no
+    collective on the data path."""
     rank, world, local = dist_info()
     import torch
     import torch.distributed as dist
@@ -183,14 +185,16 @@ def run_scan(args):
     torch.cuda.set_device(local)
     from hprmat_b200 import api, workloads
     from oracle import rmatrix_oracle as orc
+    from hprmat_b200.scan_shard import shard_units
     blocks = workloads.scan_blocks()
-    mine = [bw for i, bw in enumerate(blocks) if i % world == rank]
-    inputs = []
-    flops = 0.0
-    for w, energies in mine:
+    all_inputs = []
+    for w, energies in blocks:
         ks = [workloads.channel_kinematics(e, w.thresholds, w.hm, w.params.z1z2) for e in energies]
-        inputs.append((w.lval, w.cpot, np.array([k[0] for k in ks]), np.array([k[1] for k in ks])))
-        flops += len(energies) * 8.0 * float(w.n) ** 3 / 3.0
+        all_inputs.append((w.lval, w.cpot, np.array([k[0] for k in ks]), np.array([k[1] for k in ks])))
+    # this rank's runs of 32 energies (one run per block when alone), sharded by cost
+    units, inputs = shard_units(all_inputs, 60, rank, world, chunk=None if world == 1 else 32)
+    mine = [(blocks[b][0], np.asarray(blocks[b][1])[idx]) for b, idx in units]
+    flops = sum(len(e) * 8.0 * float(w.n) ** 3 / 3.0 for w, e in mine)
     nunits = sum(len(e) for _, e in mine)
     if args.reuse < 0:
         args.reuse = 1
