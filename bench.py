@@ -289,7 +289,7 @@ def run_adjoint(args):
     oracle adjoint at two energies."""
     import torch
     from hprmat_b200 import api, workloads
-    from hprmat_b200.autograd import collision_matrix, potential_matrix
+    from hprmat_b200.autograd import collision_matrices, potential_matrix
     from oracle import rmatrix_oracle as orc
     w, energies = workloads.adjoint_case()
     r = torch.from_numpy(workloads.lagrange_radii(w.nr, w.rmax))
@@ -313,11 +313,15 @@ def run_adjoint(args):
     tgt = np.asfortranarray(potential_matrix(r, coup, ptarget, w.hm, w.params.z1z2).numpy())
     targets = [ctx.rmatrix(w.nch, w.lval, qk, eta, w.rmax, w.nr, 1, tgt)[0] for qk, eta in kin]
 
+    # the energies' solves run concurrently on a pool of contexts (one host thread and stream each)
+    pool = [ctx] + [api.Context(precision="mixed", max_refine=8, tol=1e-12, reuse_factors=bool(args.reuse))
+                    for _ in range(max(1, args.workers) - 1)]
+
     def loss(p):
         cp = potential_matrix(r, coup, p, w.hm, w.params.z1z2)
+        us = collision_matrices(cp, pool, w.lval, kin, w.rmax, w.nr)
         tot = 0.0
-        for (qk, eta), ut in zip(kin, targets):
-            u = collision_matrix(cp, ctx, w.lval, qk, eta, w.rmax, w.nr)
+        for u, ut in zip(us, targets):
             no = u.shape[0]
             tot = tot + torch.sum(torch.abs(u - torch.from_numpy(ut[:no, :no])) ** 2)
         return tot, cp
@@ -327,7 +331,8 @@ def run_adjoint(args):
         L, _ = loss(p)
         L.backward()
     times = []
-    lib.hprmat_b200_dev_factorizations(ctx._h, 1)
+    for c in pool:
+        lib.hprmat_b200_dev_factorizations(c._h, 1)
     for _ in range(args.steps):
         t = time.perf_counter()
         p = p0.clone().requires_grad_(True)
@@ -335,9 +340,13 @@ def run_adjoint(args):
         cp.retain_grad()
         L.backward()
         times.append(time.perf_counter() - t)
-    nfact = int(lib.hprmat_b200_dev_factorizations(ctx._h, 1)) / max(1, args.steps)
+    nfact = sum(int(lib.hprmat_b200_dev_factorizations(c._h, 1)) for c in pool) / max(1, args.steps)
     g = p.grad.numpy().copy()
-    # central finite differences of the device forward, step 1e-6 (relative to the parameter)
+    # central finite differences of the device forward, step 1e-6 (relative to the parameter);
+    # the forward solves of the differences run to tighter tolerances, so that the noise of U
+    # (~1e-11 at the default surface tolerance) does not dominate the difference quotient
+    for c in pool:
+        c.set_precision("mixed", tol=1e-14, surface_tol=1e-13)
     fd_err = 0.0
     for k in range(6):
         e = torch.zeros(6, dtype=torch.float64)
@@ -363,13 +372,15 @@ def run_adjoint(args):
         "scaling": "none", "vs_baseline": None, "dtype": "c64 3xTF32 forward + c128 refinement; c128 adjoint",
         "data": "synthetic (seeded adjoint generator, hprmat_b200/workloads.py)",
         "config": {"workload": "adjoint: 32 channels x 100 points (N = 3200), 64 energies, loss sum |U - U_target|^2, "
-                               "gradients w.r.t. 6 potential parameters and the potential at all mesh points"},
+                               "gradients w.r.t. 6 potential parameters and the potential at all mesh points",
+                   "workers": len(pool)},
         "energies_used": len(kin), "energies_dropped_coulfg": len(kin_all) - len(kin),
         "solves_per_step": len(kin), "factorizations_per_step": nfact, "reuse_factors": bool(args.reuse),
         "backward": "symmetric potential: gradient from the forward solution kept on the device (no second solve)",
         "fd_rel_err_max": fd_err, "fd_step": 1e-6, "oracle_grad_rel_err_max": ref_err,
         "loss": float(L.detach())}))
-    ctx.close()
+    for c in pool:
+        c.close()
     return 0
 
 

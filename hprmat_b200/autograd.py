@@ -17,7 +17,7 @@ import torch
 
 from . import workloads
 
-__all__ = ["CollisionMatrix", "collision_matrix", "potential_matrix"]
+__all__ = ["CollisionMatrix", "CollisionMatrices", "collision_matrix", "collision_matrices", "potential_matrix"]
 
 
 class CollisionMatrix(torch.autograd.Function):
@@ -57,6 +57,80 @@ class CollisionMatrix(torch.autograd.Function):
 def collision_matrix(cpot: torch.Tensor, solver, lval, qk, eta, rmax: float, nr: int) -> torch.Tensor:
     """U (nopen x nopen) from cpot (nr, nch, nch) complex128; differentiable in cpot."""
     return CollisionMatrix.apply(cpot, solver, lval, qk, eta, rmax, nr)
+
+
+def _round_robin(pool, n, fn):
+    """fn(context, i) for i < n, energy i on context i % len(pool); each context's energies in
+    order on one host thread (a context is used by one thread at a time), results in order."""
+    from concurrent.futures import ThreadPoolExecutor
+    out = [None] * n
+
+    def run(w):
+        for i in range(w, n, len(pool)):
+            out[i] = fn(pool[w], i)
+
+    nw = min(len(pool), n)
+    if nw <= 1:
+        run(0) if n else None
+        return out
+    with ThreadPoolExecutor(nw) as ex:
+        for f in [ex.submit(run, w) for w in range(nw)]:
+            f.result()
+    return out
+
+
+class CollisionMatrices(torch.autograd.Function):
+    """U at several energies of one channel block, differentiable in the potential.  The
+    forward solves run concurrently on a pool of contexts (one host thread and one CUDA stream
+    each), so that the small solves of different energies overlap on the GPU.  Symmetric
+    potential: each forward keeps its solution X on the device and the backward forms the
+    energy's gradient from it (no second solve); otherwise the backward runs
+    ``rmatrix_adjoint`` per energy.  The gradient is the sum over the energies."""
+
+    @staticmethod
+    def forward(fctx, cpot, pool, lval, kin, rmax, nr):
+        c_np = np.asfortranarray(cpot.detach().cpu().numpy().astype(np.complex128))
+        nch = c_np.shape[1]
+        symmetric = bool(np.array_equal(c_np[:nr], c_np[:nr].transpose(0, 2, 1)))
+
+        def fwd(ctx, i):
+            qk, eta = kin[i]
+            if symmetric:
+                return ctx.rmatrix_x(nch, lval, qk, eta, rmax, nr, c_np)
+            cu, nopen = ctx.rmatrix(nch, lval, qk, eta, rmax, nr, 1, c_np)
+            return cu, nopen, None
+
+        res = _round_robin(pool, len(kin), fwd)
+        fctx.save_for_backward(cpot.detach())
+        fctx.args = (pool, lval, kin, rmax, nr, res, symmetric)
+        return tuple(torch.from_numpy(np.ascontiguousarray(cu[:no, :no])).to(cpot.device) for cu, no, _ in res)
+
+    @staticmethod
+    def backward(fctx, *grads):
+        (cpot,) = fctx.saved_tensors
+        pool, lval, kin, rmax, nr, res, symmetric = fctx.args
+        c_np = np.asfortranarray(cpot.cpu().numpy().astype(np.complex128))
+        nch = c_np.shape[1]
+
+        def bwd(ctx, i):
+            qk, eta = kin[i]
+            cu, _, x = res[i]
+            gu = grads[i].detach().cpu().numpy()
+            if symmetric:
+                return ctx.adjoint_from_x(nch, lval, qk, eta, rmax, nr, c_np, cu, x, gu)
+            return ctx.rmatrix_adjoint(nch, lval, qk, eta, rmax, nr, c_np, gu)[2]
+
+        total = np.zeros_like(c_np)
+        for g in _round_robin(pool, len(kin), bwd):
+            total += g
+        return torch.from_numpy(np.ascontiguousarray(total)).to(cpot.device), None, None, None, None, None
+
+
+def collision_matrices(cpot: torch.Tensor, pool, lval, kin, rmax: float, nr: int):
+    """U (nopen_E x nopen_E) for every (qk, eta) in ``kin``, from cpot (nr, nch, nch); ``pool``:
+    a list of ``api.Context`` (the forward solves of different energies run concurrently, one
+    per context).  Differentiable in cpot."""
+    return CollisionMatrices.apply(cpot, list(pool), lval, list(kin), rmax, nr)
 
 
 def potential_matrix(r: torch.Tensor, coupling: torch.Tensor, params: torch.Tensor, hm: float,

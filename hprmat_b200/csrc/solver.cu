@@ -349,7 +349,11 @@ static MeshDev mesh_dev(const hprmat_b200_ctx* c, int is = 0, int nq1 = 0) {
 template <typename K>
 static int set_smem(K kernel, size_t bytes) {
   // The 48 KB default covers static + dynamic shared memory.  Only ever raise the limit:
-  // kernels instantiated in more than one file share it.
+  // kernels instantiated in more than one file share it.  Contexts used from several host
+  // threads (scan workers) read and raise it under one lock, so that no thread lowers the
+  // limit another one has just raised.
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
   cudaFuncAttributes fa;
   HPR_CUDA_TRY(cudaFuncGetAttributes(&fa, kernel));
   if ((int)bytes > fa.maxDynamicSharedSizeBytes || (int)(bytes + fa.sharedSizeBytes) > 48 * 1024)

@@ -131,3 +131,34 @@ def test_adjoint_from_kept_forward_solution():
     with pytest.raises(api.HprmatError):
         ctx.adjoint_from_x(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, bad, cu, x, gu)
     ctx.close()
+
+
+def test_batched_collision_matrices_match_per_energy():
+    """collision_matrices over a pool of 3 contexts (concurrent solves) gives the same U and the
+    same parameter gradient as collision_matrix energy by energy."""
+    from hprmat_b200.autograd import collision_matrices
+    w = workloads.production(nch=10, nr=50, rmax=15.0)
+    energies = [5.0, 7.5, 10.0, 12.5, 15.0]
+    kin = [workloads.channel_kinematics(e, w.thresholds, w.hm, w.params.z1z2) for e in energies]
+    r = torch.from_numpy(workloads.lagrange_radii(w.nr, w.rmax))
+    coup = torch.from_numpy(w.coupling)
+    p0 = torch.tensor(w.params.as_array(), dtype=torch.float64)
+    pool = [api.Context(precision="mixed") for _ in range(3)]
+    ctx = api.Context(precision="mixed")
+
+    p = p0.clone().requires_grad_(True)
+    us = collision_matrices(potential_matrix(r, coup, p, w.hm, w.params.z1z2), pool, w.lval, kin, w.rmax, w.nr)
+    L1 = sum(torch.sum(torch.abs(u) ** 2 * (1 + k)) for k, u in enumerate(us))
+    L1.backward()
+    g1 = p.grad.clone()
+
+    q = p0.clone().requires_grad_(True)
+    cp = potential_matrix(r, coup, q, w.hm, w.params.z1z2)
+    us2 = [collision_matrix(cp, ctx, w.lval, qk, eta, w.rmax, w.nr) for qk, eta in kin]
+    L2 = sum(torch.sum(torch.abs(u) ** 2 * (1 + k)) for k, u in enumerate(us2))
+    L2.backward()
+    for a, b in zip(us, us2):
+        assert torch.allclose(a, b, rtol=0, atol=1e-12 * float(b.abs().max()))
+    assert torch.allclose(g1, q.grad, rtol=1e-10, atol=1e-12 * float(q.grad.abs().max()))
+    for c in pool + [ctx]:
+        c.close()
