@@ -52,7 +52,8 @@ def parse():
                     help="production: one N = 25600 solve per step (the headline); scan: the batched energy "
                          "scan, 12 J-pi blocks x 256 energies (3072 solves) per step; adjoint: loss and gradients "
                          "over 64 energies at N = 3200 per step")
-    ap.add_argument("--workers", type=int, default=4, help="worker streams of the batched scan")
+    ap.add_argument("--workers", type=int, default=8,
+                    help="worker contexts (host thread + stream each) of the batched scan and the adjoint")
     ap.add_argument("--reuse", type=int, default=-1,
                     help="scan/adjoint: keep a block's factorisation across energies as the refinement's "
                          "preconditioner (opts.reuse_factors); 0 factorises every energy; default: on for "
