@@ -919,37 +919,61 @@ __global__ void __launch_bounds__(NT) l11_inverse_planes_kernel(const float2* __
     }
   }
   __syncthreads();
-  // join blocks of size h into blocks of size 2h
+  // join blocks of size h into blocks of size 2h; every thread computes 2 x 4 tiles of the
+  // h x h products, so that six shared-memory loads feed eight complex FMAs.  The zeros above
+  // the diagonal of S make the triangular ranges rectangular within a tile.
   for (int h = B0; h < NB; h *= 2) {
     const int npair = NB / (2 * h);
-    // T = B * Ainv for every pair (B: rows [a+h, a+2h), cols [a, a+h))
-    for (int idx = tid; idx < npair * h * h; idx += NT) {
-      int pr = idx / (h * h), r = idx % (h * h);
-      int i = r % h, j = r / h;
-      int a = pr * 2 * h;
-      float2 acc = make_float2(0.f, 0.f), acc2 = make_float2(0.f, 0.f);  // two chains
-      int k = j;
-      for (; k + 1 < h; k += 2) {
-        cfma(acc, S[(a + h + i) + (a + k) * NB], S[(a + k) + (a + j) * NB]);
-        cfma(acc2, S[(a + h + i) + (a + k + 1) * NB], S[(a + k + 1) + (a + j) * NB]);
+    const int th = h / 2, tw = h / 4;  // tiles per pair: th x tw
+    // T = B * Ainv for every pair (B: rows [a+h, a+2h), cols [a, a+h); Ainv(k, j) = 0, k < j)
+    for (int t = tid; t < npair * th * tw; t += NT) {
+      const int pr = t / (th * tw), r = t % (th * tw);
+      const int i0 = 2 * (r % th), j0 = 4 * (r / th);
+      const int a = pr * 2 * h;
+      float2 acc[2][4];
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[u][q] = make_float2(0.f, 0.f);
+      for (int k = j0; k < h; ++k) {
+        const float2 b0 = S[(a + h + i0) + (a + k) * NB], b1 = S[(a + h + i0 + 1) + (a + k) * NB];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float2 v = S[(a + k) + (a + j0 + q) * NB];
+          cfma(acc[0][q], b0, v);
+          cfma(acc[1][q], b1, v);
+        }
       }
-      if (k < h) cfma(acc, S[(a + h + i) + (a + k) * NB], S[(a + k) + (a + j) * NB]);
-      T[pr * h * h + i + j * h] = make_float2(acc.x + acc2.x, acc.y + acc2.y);
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) T[pr * h * h + (i0 + u) + (j0 + q) * h] = acc[u][q];
     }
     __syncthreads();
-    // B := -Cinv * T  (Cinv: rows/cols [a+h, a+2h), lower)
-    for (int idx = tid; idx < npair * h * h; idx += NT) {
-      int pr = idx / (h * h), r = idx % (h * h);
-      int i = r % h, j = r / h;
-      int a = pr * 2 * h;
-      float2 acc = make_float2(0.f, 0.f), acc2 = make_float2(0.f, 0.f);
-      int k = 0;
-      for (; k + 1 <= i; k += 2) {
-        cfma(acc, S[(a + h + i) + (a + h + k) * NB], T[pr * h * h + k + j * h]);
-        cfma(acc2, S[(a + h + i) + (a + h + k + 1) * NB], T[pr * h * h + k + 1 + j * h]);
+    // B := -Cinv * T  (Cinv: rows/cols [a+h, a+2h), lower: Cinv(i, k) = 0 for k > i)
+    for (int t = tid; t < npair * th * tw; t += NT) {
+      const int pr = t / (th * tw), r = t % (th * tw);
+      const int i0 = 2 * (r % th), j0 = 4 * (r / th);
+      const int a = pr * 2 * h;
+      float2 acc[2][4];
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[u][q] = make_float2(0.f, 0.f);
+      for (int k = 0; k <= i0 + 1; ++k) {
+        const float2 c0 = S[(a + h + i0) + (a + h + k) * NB], c1 = S[(a + h + i0 + 1) + (a + h + k) * NB];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float2 v = T[pr * h * h + k + (j0 + q) * h];
+          cfma(acc[0][q], c0, v);
+          cfma(acc[1][q], c1, v);
+        }
       }
-      if (k <= i) cfma(acc, S[(a + h + i) + (a + h + k) * NB], T[pr * h * h + k + j * h]);
-      S[(a + h + i) + (a + j) * NB] = make_float2(-(acc.x + acc2.x), -(acc.y + acc2.y));
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          S[(a + h + i0 + u) + (a + j0 + q) * NB] = make_float2(-acc[u][q].x, -acc[u][q].y);
     }
     __syncthreads();
   }
