@@ -529,6 +529,66 @@ __global__ void __launch_bounds__(NT) gmres_start_kernel(GmresState s) {
   if (threadIdx.x == 0) s.beta[col] = beta;
 }
 
+// w -= V_{0..J} (V^H w), twice (classical Gram-Schmidt with one reorthogonalisation): all J + 1
+// projections in one pass over w and the basis and one block reduction, then one update pass;
+// the projections are added into h[0..J].  One CTA per right-hand side; J a compile-time bound
+// so that the J + 1 accumulators stay in registers.
+template <int NT, int J>
+__device__ void cgs2(const GmresState& s, int col, double2* w, double2* h) {
+  __shared__ double2 part[J + 1][NT / 32];
+  __shared__ double2 hp[J + 1];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const double2* V = s.V + (size_t)col * s.ldv;
+  for (int pass = 0; pass < 2; ++pass) {
+    double2 acc[J + 1];
+#pragma unroll
+    for (int i = 0; i <= J; ++i) acc[i] = make_double2(0, 0);
+    for (int r = threadIdx.x; r < s.N; r += NT) {
+      const double2 b = w[r];
+#pragma unroll
+      for (int i = 0; i <= J; ++i) {
+        const double2 a = V[(size_t)i * s.vstride + r];
+        acc[i].x = fma(a.x, b.x, fma(a.y, b.y, acc[i].x));  // conj(a) * b
+        acc[i].y = fma(a.x, b.y, fma(-a.y, b.x, acc[i].y));
+      }
+    }
+#pragma unroll
+    for (int i = 0; i <= J; ++i) {
+      double2 v = acc[i];
+      for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+      }
+      if (lane == 0) part[i][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x <= J) {
+      const int i = threadIdx.x;
+      double2 v = make_double2(0, 0);
+      for (int q = 0; q < NT / 32; ++q) {
+        v.x += part[i][q].x;
+        v.y += part[i][q].y;
+      }
+      hp[i] = v;
+      h[i].x += v.x;
+      h[i].y += v.y;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < s.N; r += NT) {
+      double2 b = w[r];
+#pragma unroll
+      for (int i = 0; i <= J; ++i) {
+        const double2 a = V[(size_t)i * s.vstride + r];
+        const double2 hi = hp[i];
+        b.x -= hi.x * a.x - hi.y * a.y;
+        b.y -= hi.x * a.y + hi.y * a.x;
+      }
+      w[r] = b;
+    }
+    __syncthreads();
+  }
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT) gmres_arnoldi_kernel(GmresState s, int j) {
   __shared__ double2 red[33];
@@ -538,25 +598,14 @@ __global__ void __launch_bounds__(NT) gmres_arnoldi_kernel(GmresState s, int j) 
   double2* w = s.V + (size_t)(j + 1) * s.vstride + (size_t)col * s.ldv;
   for (int i = threadIdx.x; i <= j; i += NT) h[i] = make_double2(0, 0);
   __syncthreads();
-  for (int pass = 0; pass < 2; ++pass) {
-    for (int i = 0; i <= j; ++i) {
-      const double2* vi = s.V + (size_t)i * s.vstride + (size_t)col * s.ldv;
-      double2 acc = make_double2(0, 0);
-      for (int r = threadIdx.x; r < s.N; r += NT) {
-        double2 a = vi[r], b = w[r];
-        acc.x = fma(a.x, b.x, fma(a.y, b.y, acc.x));   // conj(a) * b
-        acc.y = fma(a.x, b.y, fma(-a.y, b.x, acc.y));
-      }
-      double2 hi = block_sum2<NT>(acc, red);
-      for (int r = threadIdx.x; r < s.N; r += NT) {
-        double2 a = vi[r], b = w[r];
-        b.x -= hi.x * a.x - hi.y * a.y;
-        b.y -= hi.x * a.y + hi.y * a.x;
-        w[r] = b;
-      }
-      if (threadIdx.x == 0) { h[i].x += hi.x; h[i].y += hi.y; }
-      __syncthreads();
-    }
+  switch (j) {  // the loops over the basis at compile-time length
+#define HPR_CGS2_CASE(J) \
+  case J: cgs2<NT, J>(s, col, w, h); break;
+    HPR_CGS2_CASE(0) HPR_CGS2_CASE(1) HPR_CGS2_CASE(2) HPR_CGS2_CASE(3) HPR_CGS2_CASE(4) HPR_CGS2_CASE(5)
+    HPR_CGS2_CASE(6) HPR_CGS2_CASE(7) HPR_CGS2_CASE(8) HPR_CGS2_CASE(9) HPR_CGS2_CASE(10) HPR_CGS2_CASE(11)
+    HPR_CGS2_CASE(12) HPR_CGS2_CASE(13) HPR_CGS2_CASE(14) HPR_CGS2_CASE(15)
+#undef HPR_CGS2_CASE
+    default: break;
   }
   double2 acc = make_double2(0, 0);
   for (int r = threadIdx.x; r < s.N; r += NT) {
