@@ -133,7 +133,7 @@ struct hprmat_b200_ctx {
   int gmres_m = 12;          // longest FGMRES cycle per outer step (<= kGmresMaxM)
   double inner_tol0 = 1e-7;  // first cycle stops once the residual fell this much
   bool zero_start = false;   // refinement starts from X = 0 instead of the FP32 solution
-  int w_N = 0, w_npad = 0;
+  int w_N = 0, w_npad = 0, w_un = 0;  // key of the wave right-hand-side buffers and their TMA maps
   long w_xld = 0, w_xplane = 0;
   bool wave_trace = false;
   DevBuf wtrace, ptrace;
@@ -445,7 +445,8 @@ static int lu_solve_wave(hprmat_b200_ctx* c, const LUState& st, float2* X, long 
   const int npad = G * un;
   const long xld = (N + 3) / 4 * 4;
   const long xplane = xld * (long)npad;
-  if (c->w_N != N || c->w_npad != npad || c->w_xld != xld || !c->wbp.p) {
+  // the TMA maps' box is un rows: a new unit width needs new maps even when npad is unchanged
+  if (c->w_N != N || c->w_npad != npad || c->w_xld != xld || c->w_un != un || !c->wbp.p) {
     c->w_N = 0;
     const size_t bytes = (size_t)4 * xplane * sizeof(float);
     TRY(c->wbp.ensure(bytes));
@@ -460,6 +461,7 @@ static int lu_solve_wave(hprmat_b200_ctx* c, const LUState& st, float2* X, long 
       return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
     c->w_N = N;
     c->w_npad = npad;
+    c->w_un = un;
     c->w_xld = xld;
     c->w_xplane = xplane;
   }

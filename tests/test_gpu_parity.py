@@ -164,6 +164,22 @@ def test_wavefront_variants(sb, un):
     c.close()
 
 
+def test_wavefront_unit_width_switch_on_one_context():
+    """Changing the unit width of the wavefront solves on a live context: with 100 right-hand
+    sides one 128-column unit and two 64-column units pad to the same width, and the solves must
+    still rebuild their operand maps for the new unit (100 channels x 24 points, N = 2400)."""
+    w = workloads.production(nch=100, nr=24, rmax=10.0)
+    ref = _oracle_u(w)
+    c = api.Context(precision="mixed")
+    lib = nat.load()
+    for un in (128, 64, 128):
+        nat.check(lib.hprmat_b200_dev_set_tuning(c._h, b"wave_un", un))
+        cu, nopen = c.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+        assert nopen == ref.nopen
+        assert _rel(cu[:nopen, :nopen], ref.cu) <= U_TOL, (un, c.last_stats)
+    c.close()
+
+
 def test_sweep_generator_closed_at_40mev(ctx):
     w = workloads.sweep(20)
     ref = _oracle_u(w)
