@@ -115,7 +115,7 @@ struct hprmat_b200_ctx {
   // tensor-core operand views of the current factorisation (mixed path)
   TcOperand op_lu, op_bop, op_rhs, op_linv;
   long lup_ld = 0, lup_plane = 0, rop_plane = 0;
-  int rop_nrhs = 0;
+  int rop_nrhs = 0, rop_nb = 0;  // key of the solves' right-hand-side planes and their TMA map
   // wavefront solves (mixed path, nb = 128): sigma maps and permutation, transposed
   // off-diagonal blocks, diagonal-inverse planes, right-side / solution planes, flags
   DevBuf wsig, wperm, wT, wdi, wbp, wyp, wxp, wflags, wdf1, wdf2, wptmp, wotmp;
@@ -867,13 +867,14 @@ static int lu_solve_tc_impl(hprmat_b200_ctx* c, const LUState& st, float2* X, lo
   const size_t dsm = ((size_t)NB * NB + 2 * DCW * NB) * sizeof(float2);
   TRY(set_smem(dk, dsm));
   const int npad = (nrhs + 127) / 128 * 128;
-  if (c->rop_nrhs != npad || !c->rop.p) {
+  if (c->rop_nrhs != npad || c->rop_nb != NB || !c->rop.p) {  // the map's K extent is NB
     c->rop_plane = (long)npad * NB;
     TRY(c->rop.ensure((size_t)4 * c->rop_plane * sizeof(float)));
     HPR_CUDA_TRY(cudaMemsetAsync(c->rop.p, 0, (size_t)4 * c->rop_plane * sizeof(float), c->stream));
     if (tc_make_operand(c->tcplan, c->op_rhs, c->rop.as<float>(), NB, npad, NB, c->rop_plane, 128))
       return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
     c->rop_nrhs = npad;
+    c->rop_nb = NB;
   }
   float* rop = c->rop.as<float>();
   const int* swb = c->swaps.as<int>();

@@ -180,6 +180,24 @@ def test_wavefront_unit_width_switch_on_one_context():
     c.close()
 
 
+def test_block_size_change_on_one_context():
+    """The block-step solves of the mixed path keep their right-hand-side planes between calls;
+    a context that solved with 64-column blocks and then with 128-column ones at the same
+    padded width must rebuild them (2 channels x 50 points: two blocks of 64, then one of 128)."""
+    import ctypes
+    w = workloads.production(nch=2, nr=50, rmax=10.0)
+    ref = _oracle_u(w)
+    lib = nat.load()
+    c = api.Context(precision="mixed", panel_nb=64)
+    for nb in (64, 0, 64, 0):
+        c.opts.panel_nb = nb
+        nat.check(lib.hprmat_b200_set_opts(c._h, ctypes.byref(c.opts)))
+        cu, nopen = c.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+        assert _rel(cu[:nopen, :nopen], ref.cu) <= U_TOL, (nb, c.last_stats)
+        assert c.last_stats["nb"] == (nb or 128)
+    c.close()
+
+
 def test_sweep_generator_closed_at_40mev(ctx):
     w = workloads.sweep(20)
     ref = _oracle_u(w)
