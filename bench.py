@@ -56,8 +56,8 @@ def parse():
                     help="worker contexts (host thread + stream each) of the batched scan and the adjoint")
     ap.add_argument("--reuse", type=int, default=-1,
                     help="scan/adjoint: keep a block's factorisation across energies as the refinement's "
-                         "preconditioner (opts.reuse_factors); 0 factorises every energy; default: on for "
-                         "the scan, off for the adjoint (measured faster that way)")
+                         "preconditioner (opts.reuse_factors); default off (measured faster that way for "
+                         "both workloads)")
     return ap.parse_args()
 
 
@@ -198,7 +198,7 @@ def run_scan(args):
     flops = sum(len(e) * 8.0 * float(w.n) ** 3 / 3.0 for w, e in mine)
     nunits = sum(len(e) for _, e in mine)
     if args.reuse < 0:
-        args.reuse = 1
+        args.reuse = 0
     ctx = api.Context(device=local, precision="mixed", max_refine=3, tol=1e-12, reuse_factors=bool(args.reuse))
     from hprmat_b200 import _native as nat
     lib = nat.load()
