@@ -1139,8 +1139,10 @@ static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W3
     prev_change = change;
     gmres_start_kernel<256><<<nrhs, 256, 0, c->stream>>>(gs);
     LAUNCH_CHECK();
-    // the first cycle starts from the FP32 solution; later cycles only polish
-    const double inner_tol = outer == 0 ? c->inner_tol0 : 1e-2;
+    // the first cycle starts from the FP32 solution; a later cycle aims at what is left to
+    // the tolerance (a tenth of tol / rel), so that one polishing cycle usually ends it
+    const double inner_tol =
+        outer == 0 ? c->inner_tol0 : std::min(1e-2, std::max(1e-8, 0.1 * c->opts.tol / std::max(rel, 1e-300)));
     int jdone = 0;
     double est = 1.0;
     for (int j = 0; j < m; ++j) {

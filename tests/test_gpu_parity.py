@@ -198,6 +198,25 @@ def test_block_size_change_on_one_context():
     c.close()
 
 
+def test_sweep_maximum_size_mixed_against_fp64():
+    """The largest point of the precision sweep, 256 channels x 200 points (N = 51200, closed
+    channels at 40 MeV; 69 GB on the device for the mixed path, 90 GB with the FP64 one): the
+    panel no longer fits 128 columns, so the mixed path runs with 64-column blocks and the
+    block-step solves.  No CPU oracle finishes at this size; the mixed U is checked against
+    the device FP64 LU's (an independent algorithm and precision) and must converge within
+    the default three refinement steps."""
+    w = workloads.sweep(256)
+    c = api.Context(precision="mixed")
+    cu_m, nopen = c.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+    st = c.last_stats
+    assert st["nb"] == 64 and st["refine_steps"] <= 3 and st["rel_residual"] < 1e-10, st
+    c.set_precision("fp64")
+    cu_d, nopen_d = c.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+    assert nopen == nopen_d == int((w.qk > 0).sum())
+    assert _rel(cu_m[:nopen, :nopen], cu_d[:nopen, :nopen]) <= U_TOL
+    c.close()
+
+
 def test_sweep_generator_closed_at_40mev(ctx):
     w = workloads.sweep(20)
     ref = _oracle_u(w)
