@@ -338,21 +338,25 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
 // -------------------------------------------------------------------------------------
 // The panel factorisation of panel_kernel for panels whose rows fit in one thread-block
 // cluster (G <= 16 CTAs, the whole grid): the same algorithm and look-ahead, with the
-// per-column exchange in distributed shared memory instead of global memory.  Each CTA posts
-// its pivot key, its candidate row and (the owner) row j in its own shared memory; after the
-// hardware cluster barrier every CTA reads the G keys, picks the same pivot and reads the two
-// rows from their owners.  Double buffering by column parity is safe because a CTA posts
-// column j + 2 only after the barrier of column j + 1, which every CTA reaches after reading
-// column j.  There is no polling: the waits are the cluster barrier's.  Dynamic shared
-// memory: P [NB][rpc|1], urow [NB], candidate rows [2][NB], rows j [2][NB], keys [2].
+// per-column exchange in distributed shared memory instead of global memory.  Each CTA pushes
+// its pivot key into every CTA's shared memory and posts its candidate row and (the owner)
+// row j in its own; after the hardware cluster barrier every CTA reduces the G keys locally,
+// picks the same pivot and reads the two rows from their owners (one remote round trip).
+// Double buffering by column parity is safe because a CTA posts column j + 2 only after the
+// barrier of column j + 1, which every CTA reaches after reading column j.  There is no
+// polling: the waits are the cluster barrier's.  Dynamic shared memory: P [NB][rpc|1],
+// urow [NB], candidate rows [2][NB], rows j [2][NB], keys [2][16].
 namespace cgx = cooperative_groups;
 
 __device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
 __device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
 
+constexpr int kMaxClusterCTAs = 16;
+
 template <typename T>
 __host__ __device__ constexpr size_t panel_cluster_smem(int rpc, int nb) {
-  return ((size_t)nb * (size_t)(rpc | 1) + 5 * (size_t)nb) * sizeof(T) + 2 * sizeof(unsigned long long) + 16;
+  return ((size_t)nb * (size_t)(rpc | 1) + 5 * (size_t)nb) * sizeof(T) +
+         2 * kMaxClusterCTAs * sizeof(unsigned long long) + 16;
 }
 
 template <typename T, int NB, int NT>
@@ -370,12 +374,12 @@ __global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(PanelArgs<T> a) {
   T* urow = P + (size_t)NB * rpcp;        // [NB]
   T* xrow = urow + NB;                    // [2][NB] candidate row posted by this CTA
   T* xrowj = xrow + 2 * NB;               // [2][NB] row j, posted by its owner
-  unsigned long long* xkey = reinterpret_cast<unsigned long long*>(xrowj + 2 * NB);  // [2]
+  // [2][kMaxClusterCTAs]: every CTA's pivot key, pushed into every CTA before the barrier
+  unsigned long long* xkey = reinterpret_cast<unsigned long long*>(xrowj + 2 * NB);
   __shared__ float red_v[NT / 32];
   __shared__ int red_i[NT / 32];
   __shared__ int s_piv, s_loc_ipiv[NB];
   __shared__ unsigned s_growth;
-  __shared__ unsigned long long s_key;
   const int tid = threadIdx.x;
   const int ncols = a.ncols;
 
@@ -385,7 +389,8 @@ __global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(PanelArgs<T> a) {
   if (tid == 0) s_growth = 0u;
   __syncthreads();
 
-  // column jc's local candidate into s_piv and its key into xkey[jc & 1]
+  // column jc's local candidate into s_piv, and its key into slot b of xkey[jc & 1] of every
+  // CTA of the cluster (lane t of warp 0 stores into CTA t)
   auto candidate = [&](int jc, float bv, int bi) {
     for (int o = 16; o > 0; o >>= 1) {
       float ov = __shfl_down_sync(0xffffffffu, bv, o);
@@ -402,10 +407,9 @@ __global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(PanelArgs<T> a) {
         int oi = __shfl_down_sync(0xffffffffu, bi, o);
         if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
       }
-      if (tid == 0) {
-        s_piv = bi;
-        xkey[jc & 1] = bi != 0x7fffffff ? pivot_key(bv, bi) : 0ull;
-      }
+      if (tid == 0) s_piv = bi;
+      const unsigned long long key = __shfl_sync(0xffffffffu, bi != 0x7fffffff ? pivot_key(bv, bi) : 0ull, 0);
+      if (tid < a.G) *cluster.map_shared_rank(xkey + (jc & 1) * kMaxClusterCTAs + b, (unsigned)tid) = key;
     }
     __syncthreads();
   };
@@ -443,21 +447,19 @@ __global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(PanelArgs<T> a) {
   for (int j = 0; j < ncols; ++j) {
     const int buf = j & 1;
     cluster_wait();
-    // the largest posted key names the pivot row (the lowest row among equal moduli)
-    if (tid < 32) {
-      unsigned long long k = 0ull;
-      for (int t = tid; t < a.G; t += 32) {
-        const unsigned long long v = *cluster.map_shared_rank(xkey + buf, (unsigned)t);
-        k = v > k ? v : k;
-      }
+    // the largest key names the pivot row (the lowest row among equal moduli); every warp
+    // reduces the G keys, now in local shared memory, itself
+    unsigned long long kmax;
+    {
+      const int lane_ = tid & 31;
+      unsigned long long k = lane_ < a.G ? xkey[buf * kMaxClusterCTAs + lane_] : 0ull;
       for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long v = __shfl_down_sync(0xffffffffu, k, o);
+        const unsigned long long v = __shfl_xor_sync(0xffffffffu, k, o);
         k = v > k ? v : k;
       }
-      if (tid == 0) s_key = k;
+      kmax = k;
     }
-    __syncthreads();
-    const int p = (int)(0xFFFFFFFFu - (unsigned)(s_key & 0xFFFFFFFFull));
+    const int p = (int)(0xFFFFFFFFu - (unsigned)(kmax & 0xFFFFFFFFull));
     const T* wrow = cluster.map_shared_rank(xrow + buf * NB, (unsigned)(p / a.rpc));
     const T* jrow = cluster.map_shared_rank(xrowj + buf * NB, (unsigned)(j / a.rpc));
     float g = 0.f;
