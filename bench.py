@@ -423,6 +423,7 @@ def run_sweep(args):
                      "complex_tflops": 8.0 * n ** 3 / 3.0 / (best * 1e-3) / 1e12, "nb": st["nb"],
                      "refine_steps": st["refine_steps"], "inner_iterations": st["inner_iterations"],
                      "rel_residual": st["rel_residual"], "residual_floor": st["residual_floor"],
+                     "pivot_growth": st["pivot_growth"], "fp64_fallback": st["fp64_fallback"],
                      "u_rel_diff_vs_device_fp64": diff, "device_fp64_ms": fp64_ms,
                      "mixed_over_fp64": fp64_ms / best})
         ctx.close()
@@ -640,7 +641,8 @@ def main():
         "u_rel_err": u_err,
         "refine": {"steps": last.get("refine_steps"), "rel_residual": last.get("rel_residual"),
                    "history": last.get("residual_history"), "ms_factor": last.get("ms_factor"),
-                   "ms_refine": last.get("ms_refine")},
+                   "ms_refine": last.get("ms_refine"), "pivot_growth": last.get("pivot_growth"),
+                   "fp64_fallback": last.get("fp64_fallback")},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h_cpot.numel() * 8),
                 "d2h_bytes_per_step": int(h_cu.numel() * 8)},
         "gpu_launches": int(launches.value),

@@ -68,19 +68,36 @@ struct Acc2 {
   __device__ __forceinline__ double value() const { return hi + lo; }
 };
 
+// Block-wide maximum of a non-negative float into *out (as float bits, which order like the
+// values for non-negative numbers), one atomic per block.  All threads of the block call it.
+__device__ __forceinline__ void block_max_atomic(float v, unsigned* out) {
+  __shared__ float red_m[32];
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) red_m[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < (blockDim.x >> 5) ? red_m[threadIdx.x] : 0.f;
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0 && v > 0.f) atomicMax(out, __float_as_uint(v));
+  }
+}
+
 // C(E) of src/rmatrix_hp.F90:246-293 (one interval):
 //   channel block (c,c): tc + diag(l(l+1)/r^2 -+ k^2) - (xc/a) blo0 (closed channels)
 //   every block (c,c'):  + diag(cpot(r_i, c, c'))  [+ the non-local term, nl]
 // One thread per element, threads along rows (column-major, coalesced stores).  Writes T
 // (double2 or float2).
-// Also accumulates ||C||_F^2 (FP64) into *fro2 for the refinement's backward error.
+// Also accumulates ||C||_F^2 (FP64) into *fro2 for the refinement's backward error and, with
+// amax, the largest |re| + |im| of C for the pivot-growth check.
 template <typename T>
 __global__ void assemble_kernel(MeshDev mesh, ChannelData ch, int nch, const double2* __restrict__ cpot,
-                                long ncp1, long ndim, T* W, long ld, int N, double* fro2, NonLocalDev nl = {}) {
+                                long ncp1, long ndim, T* W, long ld, int N, double* fro2, NonLocalDev nl = {},
+                                unsigned* amax = nullptr) {
   // thread: one row; block: 256 rows of the columns blockIdx.y, blockIdx.y + gridDim.y, ...
   // (coalesced writes along the column), one atomic per block for ||C||_F^2
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   double sq = 0.0;
+  float am = 0.f;
   if (row < N) {
     const int nr = mesh.nr;
     const int c = row / nr, i = row - c * nr;
@@ -110,8 +127,10 @@ __global__ void assemble_kernel(MeshDev mesh, ChannelData ch, int nch, const dou
       out.y = (typename RealOf<T>::R)im;
       W[(size_t)row + (size_t)col * ld] = out;
       sq += re * re + im * im;
+      am = fmaxf(am, (float)(fabs(re) + fabs(im)));
     }
   }
+  if (amax) block_max_atomic(am, amax);
   for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
   __shared__ double red[32];
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
@@ -427,15 +446,19 @@ __global__ void copy_d_kernel(const double2* __restrict__ src, long lds, double2
 // ||A||_F^2 of a dense FP64 complex matrix (column-major), accumulated into *fro2.
 // ||A||_F^2 (N x N): block = 256 rows of the columns blockIdx.y + k gridDim.y, one atomic per
 // block.
-__global__ void fro2_kernel(const double2* __restrict__ A, long lda, int N, double* fro2) {
+// ||A||_F^2 into *fro2 and, with amax, the largest |re| + |im| of A (pivot-growth check).
+__global__ void fro2_kernel(const double2* __restrict__ A, long lda, int N, double* fro2, unsigned* amax = nullptr) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   double sq = 0.0;
+  float am = 0.f;
   if (r < N) {
     for (int col = blockIdx.y; col < N; col += gridDim.y) {
       double2 v = A[(size_t)r + (size_t)col * lda];
       sq += v.x * v.x + v.y * v.y;
+      am = fmaxf(am, (float)(fabs(v.x) + fabs(v.y)));
     }
   }
+  if (amax) block_max_atomic(am, amax);
   for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
   __shared__ double red[32];
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
@@ -447,12 +470,18 @@ __global__ void fro2_kernel(const double2* __restrict__ A, long lda, int N, doub
   }
 }
 
-__global__ void d2f_matrix_kernel(const double2* __restrict__ src, long lds, float2* dst, long ldd, int N) {
+// FP64 -> FP32 copy of a matrix; with amax also the largest |re| + |im| (pivot-growth check).
+__global__ void d2f_matrix_kernel(const double2* __restrict__ src, long lds, float2* dst, long ldd, int N,
+                                  unsigned* amax = nullptr) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   const int col = blockIdx.y;
-  if (r >= N) return;
-  double2 v = src[(size_t)r + (size_t)col * lds];
-  dst[(size_t)r + (size_t)col * ldd] = make_float2((float)v.x, (float)v.y);
+  float am = 0.f;
+  if (r < N) {
+    double2 v = src[(size_t)r + (size_t)col * lds];
+    dst[(size_t)r + (size_t)col * ldd] = make_float2((float)v.x, (float)v.y);
+    am = (float)(fabs(v.x) + fabs(v.y));
+  }
+  if (amax) block_max_atomic(am, amax);
 }
 
 // ---------------------------------------------------------------- FGMRES (per column)

@@ -127,6 +127,7 @@ struct hprmat_b200_ctx {
   bool wave_enabled = true;  // wavefront solves (else block-step solves)
   bool tc_trsm = true;       // U12 by the tensor cores from L11^-1 (else substitution)
   int panel_rpc_min = 32;    // fewest panel rows per CTA
+  double growth_limit = 1e6;  // mixed path: pivot growth above which C(E) is factorised in FP64
   bool panel_cluster = true;  // panels that fit in one 16-CTA cluster use panel_cluster_kernel
   signed char cluster_ok[2][17] = {};  // per element size (float2, double2) and cluster size:
                                        // 0 unknown, 1 schedulable, -1 not
@@ -1241,6 +1242,26 @@ static double ms_since(Clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
 }
 
+// Status-block slot of the largest |re| + |im| of the matrix (float bits), written by the
+// assembly / conversion kernels for the pivot-growth check.
+constexpr int kAmaxSlot = 40;
+
+// Pivot growth of the last factorisation: the largest |re| + |im| of U (accumulated by the
+// panel and U12 kernels into the status block, copied to h_status by factor) over that of the
+// matrix (kAmaxSlot).  0 for a zero matrix.
+static int pivot_growth(hprmat_b200_ctx* c, double* rho) {
+  unsigned abits = 0;
+  HPR_CUDA_TRY(cudaMemcpyAsync(&abits, c->status.as<int>() + kAmaxSlot, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                               c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const unsigned gbits = (unsigned)c->h_status[SW_COUNT - 1];
+  float g, am;
+  memcpy(&g, &gbits, sizeof(float));
+  memcpy(&am, &abits, sizeof(float));
+  *rho = am > 0.f ? (double)g / (double)am : 0.0;
+  return HPRMAT_B200_OK;
+}
+
 // One interval (0-based is) of an rmatrix call: C(E) of the interval assembled on the device
 // (src/rmatrix_hp.F90:246-293), factorised, and solved for its md.nq1 + nch surface right-hand
 // sides into X64 (ld ldx): FP64 LU and one solve, or the mixed LU with FP64 refinement.
@@ -1284,7 +1305,9 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
   dim3 ga(cdiv_u(N, 256), std::min(N, 512));  // assemble_kernel strides over the columns
   dim3 gr(cdiv_u(N, 256), nrhs);
   double* d_fro2 = reinterpret_cast<double*>(c->status.as<int>() + 32);
+  unsigned* d_amax = reinterpret_cast<unsigned*>(c->status.as<int>() + kAmaxSlot);
   HPR_CUDA_TRY(cudaMemsetAsync(d_fro2, 0, sizeof(double), c->stream));
+  HPR_CUDA_TRY(cudaMemsetAsync(d_amax, 0, sizeof(unsigned), c->stream));
   if (!op.structured) {
     TRY(c->A64.ensure((size_t)ld * N * sizeof(double2)));
     TRY(c->B64.ensure((size_t)ld * nrhs * sizeof(double2)));
@@ -1299,10 +1322,62 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
     op.ldb = ld;
     HPR_CUDA_TRY(cudaMemsetAsync(d_fro2, 0, sizeof(double), c->stream));
   }
-  if (!mixed) {
+  if (mixed) {
+    TRY(c->W.ensure((size_t)ld * N * sizeof(float2)));
+    float2* W = c->W.as<float2>();
+    if (reuse) {
+      st.N = c->held_N;
+      st.ld = c->held_ld;
+      st.nb = c->held_nb;
+      st.nsteps = c->held_nsteps;
+    } else {
+      assemble_kernel<float2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2, nl,
+                                                         d_amax);
+      LAUNCH_CHECK();
+      int nb = pick_nb(c, N, sizeof(float2), 128);
+      if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
+      auto t1 = Clock::now();
+      TRY(factor<float2>(c, W, ld, N, true, nb, st));
+      stats->ms_factor = ms_since(t1);
+      stats->factorizations += 1;
+      c->held_N = st.N;
+      c->held_ld = st.ld;
+      c->held_nb = st.nb;
+      c->held_nsteps = st.nsteps;
+      // FP32 factors with a large pivot growth (or an exact zero FP32 pivot) cannot carry the
+      // refinement: factorise C(E) in FP64 instead (the reference's Type 2 falls back to ZGESV
+      // on CGETRF info != 0, src/rmat_solvers.F90:233-236)
+      TRY(pivot_growth(c, &stats->pivot_growth));
+      if (c->h_status[SW_INFO] != 0 || !(stats->pivot_growth <= c->growth_limit)) {
+        stats->fp64_fallback = 1;
+        HPR_CUDA_TRY(cudaMemsetAsync(d_amax, 0, sizeof(unsigned), c->stream));
+      }
+    }
+    if (!stats->fp64_fallback) {
+      auto t2 = Clock::now();
+      TRY(c->X.ensure((size_t)ld * nrhs * sizeof(float2)));
+      float2* X32 = c->X.as<float2>();
+      surface_rhs_kernel<float2><<<gr, 256, 0, c->stream>>>(md, X32, ld, N, 1.0);
+      LAUNCH_CHECK();
+      if (c->zero_start) {
+        HPR_CUDA_TRY(cudaMemsetAsync(X64, 0, (size_t)ld * nrhs * sizeof(double2), c->stream));
+      } else {
+        TRY(lu_solve_tc(c, st, X32, ld, nrhs));
+        f2d_kernel<<<gr, 256, 0, c->stream>>>(X32, ld, X64, ld, N, nullptr);
+        LAUNCH_CHECK();
+      }
+      stats->ms_solve = ms_since(t2);
+      auto t3 = Clock::now();
+      status = refine_mixed(c, op, W, st, X64, ld, nrhs, bnorm, 0.0, stats, reuse ? 8 : -1, reuse);
+      if (status != HPRMAT_B200_OK && status != HPRMAT_B200_NOT_CONVERGED) return status;
+      stats->ms_refine = ms_since(t3);
+    }
+  }
+  if (!mixed || stats->fp64_fallback) {
     TRY(c->W.ensure((size_t)ld * N * sizeof(double2)));
     double2* W = c->W.as<double2>();
-    assemble_kernel<double2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2, nl);
+    assemble_kernel<double2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2, nl,
+                                                        d_amax);
     LAUNCH_CHECK();
     surface_rhs_kernel<double2><<<gr, 256, 0, c->stream>>>(md, X64, ld, N, 1.0);
     LAUNCH_CHECK();
@@ -1310,7 +1385,8 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
     if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
     auto t1 = Clock::now();
     TRY(factor<double2>(c, W, ld, N, false, nb, st));
-    stats->factorizations = 1;
+    stats->factorizations += 1;
+    TRY(pivot_growth(c, &stats->pivot_growth));
     c->f64_N = st.N;
     c->f64_ld = st.ld;
     c->f64_nb = st.nb;
@@ -1326,48 +1402,9 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
     stats->rel_residual = rn / bnorm;
     stats->residual_history[0] = rn / bnorm;
     stats->ms_solve = ms_since(t2);
-  } else {
-    TRY(c->W.ensure((size_t)ld * N * sizeof(float2)));
-    float2* W = c->W.as<float2>();
-    if (reuse) {
-      st.N = c->held_N;
-      st.ld = c->held_ld;
-      st.nb = c->held_nb;
-      st.nsteps = c->held_nsteps;
-    } else {
-      assemble_kernel<float2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2, nl);
-      LAUNCH_CHECK();
-      int nb = pick_nb(c, N, sizeof(float2), 128);
-      if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
-      auto t1 = Clock::now();
-      TRY(factor<float2>(c, W, ld, N, true, nb, st));
-      stats->ms_factor = ms_since(t1);
-      stats->factorizations = 1;
-      c->held_N = st.N;
-      c->held_ld = st.ld;
-      c->held_nb = st.nb;
-      c->held_nsteps = st.nsteps;
-    }
-    auto t2 = Clock::now();
-    TRY(c->X.ensure((size_t)ld * nrhs * sizeof(float2)));
-    float2* X32 = c->X.as<float2>();
-    surface_rhs_kernel<float2><<<gr, 256, 0, c->stream>>>(md, X32, ld, N, 1.0);
-    LAUNCH_CHECK();
-    if (c->zero_start) {
-      HPR_CUDA_TRY(cudaMemsetAsync(X64, 0, (size_t)ld * nrhs * sizeof(double2), c->stream));
-    } else {
-      TRY(lu_solve_tc(c, st, X32, ld, nrhs));
-      f2d_kernel<<<gr, 256, 0, c->stream>>>(X32, ld, X64, ld, N, nullptr);
-      LAUNCH_CHECK();
-    }
-    stats->ms_solve = ms_since(t2);
-    auto t3 = Clock::now();
-    status = refine_mixed(c, op, W, st, X64, ld, nrhs, bnorm, 0.0, stats, reuse ? 8 : -1, reuse);
-    if (status != HPRMAT_B200_OK && status != HPRMAT_B200_NOT_CONVERGED) return status;
-    stats->ms_refine = ms_since(t3);
   }
   stats->nb = st.nb;
-  if (!reuse && c->h_status[SW_INFO] != 0) {
+  if ((!reuse || stats->fp64_fallback) && c->h_status[SW_INFO] != 0) {
     stats->info = c->h_status[SW_INFO];
     return fail(HPRMAT_B200_SINGULAR, "C(E) of interval %d is singular: zero pivot in column %d", is + 1,
                 c->h_status[SW_INFO]);
@@ -1532,7 +1569,8 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
     }
     if (keyed && (s == HPRMAT_B200_OK || s == HPRMAT_B200_NOT_CONVERGED))
       c->held_last_inner = si.factorizations > 0 ? 0 : si.inner_iterations;
-    if (keyed && (s == HPRMAT_B200_OK || s == HPRMAT_B200_NOT_CONVERGED) && si.factorizations > 0) {
+    if (keyed && (s == HPRMAT_B200_OK || s == HPRMAT_B200_NOT_CONVERGED) && si.factorizations > 0 &&
+        !si.fp64_fallback) {
       c->lu_held = true;
       c->held_nch = nch;
       c->held_nr = nr;
@@ -1544,6 +1582,8 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
       stats->info = si.info;
       stats->nb = si.nb;
       stats->factorizations += si.factorizations;
+      stats->fp64_fallback |= si.fp64_fallback;
+      stats->pivot_growth = std::max(stats->pivot_growth, si.pivot_growth);
       stats->refine_steps += si.refine_steps;
       stats->inner_iterations += si.inner_iterations;
       stats->ms_factor += si.ms_factor;
@@ -1717,44 +1757,32 @@ static int solve_dense_core(hprmat_b200_ctx* c, const double2* dA, double2* dB, 
   int status = HPRMAT_B200_OK;
   dim3 ga(cdiv_u(N, 256), N);
   dim3 gr(cdiv_u(N, 256), nrhs);
-  if (!mixed) {
-    TRY(c->W.ensure((size_t)ld * N * sizeof(double2)));
-    double2* W = c->W.as<double2>();
-    HPR_CUDA_TRY(cudaMemcpy2DAsync(W, ld * sizeof(double2), dA, (size_t)N * sizeof(double2),
-                                   (size_t)N * sizeof(double2), N, cudaMemcpyDeviceToDevice, c->stream));
-    int nb = pick_nb(c, N, sizeof(double2), 64);
-    if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
-    auto t1 = Clock::now();
-    TRY(factor<double2>(c, W, ld, N, false, nb, st));
-    if (stats) stats->ms_factor = ms_since(t1);
-    if (c->h_status[SW_INFO] != 0) {
-      if (stats) stats->info = c->h_status[SW_INFO];
-      return fail(HPRMAT_B200_SINGULAR, "matrix is singular: zero pivot in column %d", c->h_status[SW_INFO]);
-    }
-    auto t2 = Clock::now();
-    TRY(c->X64.ensure((size_t)ld * nrhs * sizeof(double2)));
-    double2* X = c->X64.as<double2>();
-    copy_d_kernel<<<gr, 256, 0, c->stream>>>(dB, N, X, ld, N);
-    LAUNCH_CHECK();
-    TRY(lu_solve<double2>(c, W, st, X, ld, nrhs));
-    copy_d_kernel<<<gr, 256, 0, c->stream>>>(X, ld, dB, N, N);
-    LAUNCH_CHECK();
-    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    if (stats) stats->ms_solve = ms_since(t2);
-  } else {
+  bool fallback = false;
+  if (mixed) {
     TRY(c->W.ensure((size_t)ld * N * sizeof(float2)));
     float2* W = c->W.as<float2>();
-    d2f_matrix_kernel<<<ga, 256, 0, c->stream>>>(dA, N, W, ld, N);
+    unsigned* d_amax = reinterpret_cast<unsigned*>(c->status.as<int>() + kAmaxSlot);
+    HPR_CUDA_TRY(cudaMemsetAsync(d_amax, 0, sizeof(unsigned), c->stream));
+    d2f_matrix_kernel<<<ga, 256, 0, c->stream>>>(dA, N, W, ld, N, d_amax);
     LAUNCH_CHECK();
     int nb = pick_nb(c, N, sizeof(float2), 128);
     if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
     auto t1 = Clock::now();
     TRY(factor<float2>(c, W, ld, N, true, nb, st));
     if (stats) stats->ms_factor = ms_since(t1);
-    if (c->h_status[SW_INFO] != 0) {
-      if (stats) stats->info = c->h_status[SW_INFO];
-      return fail(HPRMAT_B200_SINGULAR, "matrix is singular: zero pivot in column %d", c->h_status[SW_INFO]);
+    double rho = 0.0;
+    TRY(pivot_growth(c, &rho));
+    if (stats) {
+      stats->factorizations = 1;
+      stats->pivot_growth = rho;
     }
+    // an exact zero FP32 pivot or a pivot growth beyond what the FP32 factors can carry through
+    // the refinement: factorise A in FP64 (Type 2's ZGESV fallback, src/rmat_solvers.F90:233-236)
+    fallback = c->h_status[SW_INFO] != 0 || !(rho <= c->growth_limit);
+    if (stats) stats->fp64_fallback = fallback;
+  }
+  if (mixed && !fallback) {
+    float2* W = c->W.as<float2>();
     auto t2 = Clock::now();
     TRY(c->X.ensure((size_t)ld * nrhs * sizeof(float2)));
     TRY(c->X64.ensure((size_t)ld * nrhs * sizeof(double2)));
@@ -1792,6 +1820,42 @@ static int solve_dense_core(hprmat_b200_ctx* c, const double2* dA, double2* dB, 
     LAUNCH_CHECK();
     HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (stats) stats->ms_refine = ms_since(t3);
+  }
+  if (!mixed || fallback) {
+    TRY(c->W.ensure((size_t)ld * N * sizeof(double2)));
+    double2* W = c->W.as<double2>();
+    HPR_CUDA_TRY(cudaMemcpy2DAsync(W, ld * sizeof(double2), dA, (size_t)N * sizeof(double2),
+                                   (size_t)N * sizeof(double2), N, cudaMemcpyDeviceToDevice, c->stream));
+    if (stats && !fallback) {  // max |a_ij| for the reported pivot growth (the mixed path has it)
+      unsigned* d_amax = reinterpret_cast<unsigned*>(c->status.as<int>() + kAmaxSlot);
+      double* d_fro2 = reinterpret_cast<double*>(c->status.as<int>() + 32);
+      HPR_CUDA_TRY(cudaMemsetAsync(d_amax, 0, sizeof(unsigned), c->stream));
+      fro2_kernel<<<dim3(cdiv_u(N, 256), std::min(N, 512)), 256, 0, c->stream>>>(dA, N, N, d_fro2, d_amax);
+      LAUNCH_CHECK();
+    }
+    int nb = pick_nb(c, N, sizeof(double2), 64);
+    if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
+    auto t1 = Clock::now();
+    TRY(factor<double2>(c, W, ld, N, false, nb, st));
+    if (stats) stats->ms_factor = ms_since(t1);
+    if (stats) {
+      stats->factorizations += 1;
+      TRY(pivot_growth(c, &stats->pivot_growth));
+    }
+    if (c->h_status[SW_INFO] != 0) {
+      if (stats) stats->info = c->h_status[SW_INFO];
+      return fail(HPRMAT_B200_SINGULAR, "matrix is singular: zero pivot in column %d", c->h_status[SW_INFO]);
+    }
+    auto t2 = Clock::now();
+    TRY(c->X64.ensure((size_t)ld * nrhs * sizeof(double2)));
+    double2* X = c->X64.as<double2>();
+    copy_d_kernel<<<gr, 256, 0, c->stream>>>(dB, N, X, ld, N);
+    LAUNCH_CHECK();
+    TRY(lu_solve<double2>(c, W, st, X, ld, nrhs));
+    copy_d_kernel<<<gr, 256, 0, c->stream>>>(X, ld, dB, N, N);
+    LAUNCH_CHECK();
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (stats) stats->ms_solve = ms_since(t2);
   }
   if (stats) {
     stats->nb = st.nb;
@@ -2690,6 +2754,11 @@ int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* c, const char* key, int value) {
   }
   if (strcmp(key, "panel_cluster") == 0) {
     c->panel_cluster = value != 0;
+    return HPRMAT_B200_OK;
+  }
+  if (strcmp(key, "growth_limit_exp") == 0) {
+    if (value < -30 || value > 30) return fail(HPRMAT_B200_ERR_ARG, "growth_limit_exp must be in -30..30");
+    c->growth_limit = pow(10.0, value);
     return HPRMAT_B200_OK;
   }
   if (strcmp(key, "reuse_max_inner") == 0) {

@@ -78,7 +78,10 @@ typedef struct {
   double residual_history[9];
   double ms_assemble, ms_factor, ms_solve, ms_refine, ms_umatrix, ms_total;
   int factorizations;       /* LU factorisations the call ran (0: reused, opts.reuse_factors) */
-  int reserved_stats;
+  int fp64_fallback;        /* mixed path: 1 if the FP32 factorisation was replaced by the FP64 one
+                               (pivot growth above the limit, or an exact zero FP32 pivot, as the
+                               reference's Type 2 falls back on CGETRF info != 0) */
+  double pivot_growth;      /* max |u_ij| / max |c_ij| (|re| + |im|) of the last factorisation */
 } hprmat_b200_stats;
 
 /* Defaults for hprmat_b200_opts. */

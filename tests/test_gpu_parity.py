@@ -306,6 +306,94 @@ def test_solve_rmatrix_matches_oracle(ctx):
     assert _rel(rm, ref) <= 1e-10
 
 
+def _growth_matrix(nw=40, n=300, seed=5):
+    """blockdiag(W, D): W (nw x nw) has 1 on the diagonal, -1/2 below it and 1 in its last
+    column, so partial pivoting swaps nothing and |U| grows as 1.5^k (7.4e6 at nw = 40; the
+    classic growth example for GEPP); D is diagonally dominant with entries below 1.  The whole
+    matrix is turned by one complex phase.  X = 1 is exact: every row sum of W is exact."""
+    A = np.zeros((n, n), np.complex128)
+    W = np.eye(nw)
+    W[np.tril_indices(nw, -1)] = -0.5
+    W[:, -1] = 1.0
+    A[:nw, :nw] = W
+    rng = np.random.default_rng(seed)
+    m = n - nw
+    D = (rng.random((m, m)) + 1j * rng.random((m, m))) / (4 * m)
+    D[np.arange(m), np.arange(m)] += 0.5
+    A[nw:, nw:] = D
+    A = np.asfortranarray(A * np.exp(0.3j))
+    Xt = np.ones((n, 3), np.complex128)
+    return A, Xt
+
+
+def _growth_of(A):
+    """max |u_ij| / max |a_ij| with |z| = |re| + |im| (the solver's measure), numpy LU."""
+    import scipy.linalg as sl
+    _p, _l, u = sl.lu(A)
+    m1 = lambda z: np.abs(z.real) + np.abs(z.imag)
+    return float(m1(u).max() / m1(A).max())
+
+
+def test_pivot_growth_falls_back_to_fp64(ctx):
+    """The mixed solve measures the pivot growth of its FP32 factors and, above 10^6,
+    factorises A in FP64 instead (the FP32 factors of this matrix carry no correct digit in
+    the last column of W)."""
+    A, Xt = _growth_matrix()
+    B = np.asfortranarray(A @ Xt)
+    rho = _growth_of(A)
+    assert rho > 1e6
+    ctx.set_precision("mixed", max_refine=3, tol=1e-12)
+    X = ctx.solve_linear(A, B)
+    st = ctx.last_stats
+    assert st["fp64_fallback"] == 1 and st["factorizations"] == 2, st
+    assert abs(st["pivot_growth"] / rho - 1.0) < 1e-3, (st["pivot_growth"], rho)
+    err_np = _rel(np.linalg.solve(A, B), Xt)
+    assert _rel(X, Xt) <= max(10 * err_np, 1e-9), (_rel(X, Xt), err_np)
+    # the same matrix through the FP64 path reports the same growth, without a fallback
+    ctx.set_precision("fp64")
+    X = ctx.solve_linear(A, B)
+    st = ctx.last_stats
+    assert st["fp64_fallback"] == 0 and st["factorizations"] == 1
+    assert abs(st["pivot_growth"] / rho - 1.0) < 1e-3
+    assert _rel(X, Xt) <= max(10 * err_np, 1e-9)
+    ctx.set_precision("mixed", max_refine=3, tol=1e-12)
+
+
+def test_pivot_growth_limit_is_the_trigger():
+    """With the limit raised to 10^12 the same matrix stays on the FP32 factors; a
+    well-conditioned matrix reports a growth of order 1 and no fallback."""
+    lib = nat.load()
+    with api.Context(precision="mixed") as c:
+        nat.check(lib.hprmat_b200_dev_set_tuning(c._h, b"growth_limit_exp", 12))
+        A, Xt = _growth_matrix()
+        c.solve_linear(A, np.asfortranarray(A @ Xt), allow_unconverged=True)
+        assert c.last_stats["fp64_fallback"] == 0 and c.last_stats["factorizations"] == 1
+        assert c.last_stats["pivot_growth"] > 1e6
+        A, B = _diag_dominant(500, 4, 9)
+        c.solve_linear(A, B)
+        assert c.last_stats["fp64_fallback"] == 0 and 0.5 < c.last_stats["pivot_growth"] < 2.0
+        assert lib.hprmat_b200_dev_set_tuning(c._h, b"growth_limit_exp", 31) == nat.ERR_ARG
+
+
+def test_rmatrix_fp64_fallback_matches_oracle():
+    """The R-matrix path's fallback, forced by a growth limit of 10^-30: C(E) factorised in
+    FP32, then again in FP64, and U as the oracle's to 1e-10.  The production C(E) itself has
+    a small growth and stays on the mixed path."""
+    lib = nat.load()
+    w = workloads.production(nch=8)
+    ref = _oracle_u(w)
+    with api.Context(precision="mixed") as c:
+        c.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+        st = c.last_stats
+        assert st["fp64_fallback"] == 0 and st["factorizations"] == 1 and st["pivot_growth"] < 1e3, st
+        nat.check(lib.hprmat_b200_dev_set_tuning(c._h, b"growth_limit_exp", -30))
+        cu, nopen = c.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+        st = c.last_stats
+        assert st["fp64_fallback"] == 1 and st["factorizations"] == 2, st
+        assert nopen == ref.nopen
+        assert _rel(cu[:nopen, :nopen], ref.cu) <= U_TOL
+
+
 # ---------------------------------------------------------------- failures
 def test_singular_matrix_reports_status(ctx):
     n = 300
