@@ -393,6 +393,7 @@ def run_sweep(args):
     --steps after --warmup, CUDA-event time on the context's stream), its refinement record,
     and its U against the device FP64 LU's (an independent algorithm and precision; no CPU
     oracle finishes at the larger sizes)."""
+    import ctypes
     import torch
     from hprmat_b200 import api, workloads
     rows = []
@@ -414,9 +415,21 @@ def run_sweep(args):
             ms = e0.elapsed_time(e1)
             best = ms if best is None else min(best, ms)
         st = ctx.last_stats
+        # tensor-pipe use: one more mixed solve with the trailing updates bracketed by events
+        lib = ctx._lib
+        lib.hprmat_b200_dev_counters(ctx._h, None, None, None, None, 1)
+        lib.hprmat_b200_dev_set_profile(ctx._h, 1)
+        ctx.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+        lib.hprmat_b200_dev_set_profile(ctx._h, 0)
+        tc_ms, tc_flops, tc_n = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_int(0)
+        lib.hprmat_b200_dev_counters(ctx._h, None, ctypes.byref(tc_ms), ctypes.byref(tc_flops), ctypes.byref(tc_n), 1)
+        # the FP64 LU of the same C(E), with its 1-norm condition estimate (Hager-Higham on the
+        # FP64 factors; reported separately from the timed mixed solves)
         ctx.set_precision("fp64")
+        ctx.set_estimate_condition(True)
         cu_d, _ = ctx.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
         fp64_ms = ctx.last_stats["ms_total"]
+        kappa1 = ctx.last_stats["cond_estimate"]
         diff = float(np.linalg.norm(cu_m[:nopen, :nopen] - cu_d[:nopen, :nopen]) / np.linalg.norm(cu_d[:nopen, :nopen]))
         n = w.n
         rows.append({"N": n, "nch": nch, "nopen": nopen, "ms_per_solve": best, "solves_per_s": 1e3 / best,
@@ -425,7 +438,9 @@ def run_sweep(args):
                      "rel_residual": st["rel_residual"], "residual_floor": st["residual_floor"],
                      "pivot_growth": st["pivot_growth"], "fp64_fallback": st["fp64_fallback"],
                      "u_rel_diff_vs_device_fp64": diff, "device_fp64_ms": fp64_ms,
-                     "mixed_over_fp64": fp64_ms / best})
+                     "mixed_over_fp64": fp64_ms / best, "cond1_estimate": kappa1,
+                     "tc_update_tflops": tc_flops.value / max(tc_ms.value, 1e-9) / 1e9,
+                     "tc_update_share": tc_ms.value / best})
         ctx.close()
         del cu_m, cu_d
         torch.cuda.empty_cache()

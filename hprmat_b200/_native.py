@@ -46,7 +46,7 @@ EXPORTED = (
 class Opts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("max_refine", ctypes.c_int), ("tol", ctypes.c_double),
                 ("surface_tol", ctypes.c_double), ("panel_nb", ctypes.c_int), ("reuse_factors", ctypes.c_int),
-                ("reserved", ctypes.c_int * 3)]
+                ("estimate_condition", ctypes.c_int), ("reserved", ctypes.c_int * 2)]
 
 
 class Stats(ctypes.Structure):
@@ -57,7 +57,8 @@ class Stats(ctypes.Structure):
                 ("residual_history", ctypes.c_double * 9),
                 ("ms_assemble", ctypes.c_double), ("ms_factor", ctypes.c_double), ("ms_solve", ctypes.c_double),
                 ("ms_refine", ctypes.c_double), ("ms_umatrix", ctypes.c_double), ("ms_total", ctypes.c_double),
-                ("factorizations", ctypes.c_int), ("fp64_fallback", ctypes.c_int), ("pivot_growth", ctypes.c_double)]
+                ("factorizations", ctypes.c_int), ("fp64_fallback", ctypes.c_int), ("pivot_growth", ctypes.c_double),
+                ("cond_estimate", ctypes.c_double)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("residual_history", "floor_history")}

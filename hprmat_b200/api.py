@@ -78,6 +78,12 @@ class Context:
         self.opts.reuse_factors = int(bool(enable))
         nat.check(self._lib.hprmat_b200_set_opts(self._h, ctypes.byref(self.opts)))
 
+    def set_estimate_condition(self, enable: bool):
+        """opts.estimate_condition: FP64 factorisations also estimate the 1-norm condition number
+        of the factorised matrix (``last_stats["cond_estimate"]``, as LAPACK ZGECON's 1/rcond)."""
+        self.opts.estimate_condition = int(bool(enable))
+        nat.check(self._lib.hprmat_b200_set_opts(self._h, ctypes.byref(self.opts)))
+
     def set_precision(self, precision: str, max_refine: int | None = None, tol: float | None = None,
                       surface_tol: float | None = None):
         self.opts.precision = _PREC[precision]

@@ -470,6 +470,23 @@ __global__ void fro2_kernel(const double2* __restrict__ A, long lda, int N, doub
   }
 }
 
+// ||A||_1 = max over columns of sum_i |a_ij| (LAPACK's 1-norm, |z| the modulus) into *out as
+// the bits of a non-negative double (which order like the values).  One block per column.
+__global__ void colabs_max_kernel(const double2* __restrict__ A, long lda, int N, unsigned long long* out) {
+  const double2* col = A + (size_t)blockIdx.x * lda;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) s += hypot(col[i].x, col[i].y);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) atomicMax(out, (unsigned long long)__double_as_longlong(s));
+  }
+}
+
 // FP64 -> FP32 copy of a matrix; with amax also the largest |re| + |im| (pivot-growth check).
 __global__ void d2f_matrix_kernel(const double2* __restrict__ src, long lds, float2* dst, long ldd, int N,
                                   unsigned* amax = nullptr) {

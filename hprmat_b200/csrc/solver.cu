@@ -112,6 +112,7 @@ struct hprmat_b200_ctx {
   // wave functions: per-interval solutions and propagation matrices, surface amplitudes, cf
   DevBuf wfx, wfz, wfc, wfcf;
   DevBuf fpbuf;  // potential fingerprint (opts.reuse_factors)
+  DevBuf cond_v;  // condition estimate: one right-hand side (opts.estimate_condition)
   // tensor-core operand views of the current factorisation (mixed path)
   TcOperand op_lu, op_bop, op_rhs, op_linv;
   long lup_ld = 0, lup_plane = 0, rop_plane = 0;
@@ -1245,6 +1246,20 @@ static double ms_since(Clock::time_point t0) {
 // Status-block slot of the largest |re| + |im| of the matrix (float bits), written by the
 // assembly / conversion kernels for the pivot-growth check.
 constexpr int kAmaxSlot = 40;
+// Status-block slot (int offset, 8-byte aligned) of ||C||_1 as double bits, written by
+// colabs_max_kernel before an FP64 factorisation when opts.estimate_condition is set.
+constexpr int kAnormSlot = 42;
+
+static int condest_fp64(hprmat_b200_ctx* c, const double2* W, const LUState& st, double* kappa);
+
+// Start of a condition estimate: ||A||_1 of the matrix about to be factorised in FP64.
+static int anorm_begin(hprmat_b200_ctx* c, const double2* A, long lda, int N) {
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(c->status.as<int>() + kAnormSlot);
+  HPR_CUDA_TRY(cudaMemsetAsync(d, 0, sizeof(unsigned long long), c->stream));
+  colabs_max_kernel<<<N, 256, 0, c->stream>>>(A, lda, N, d);
+  LAUNCH_CHECK();
+  return HPRMAT_B200_OK;
+}
 
 // Pivot growth of the last factorisation: the largest |re| + |im| of U (accumulated by the
 // panel and U12 kernels into the status block, copied to h_status by factor) over that of the
@@ -1383,6 +1398,7 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
     LAUNCH_CHECK();
     int nb = pick_nb(c, N, sizeof(double2), 64);
     if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
+    if (c->opts.estimate_condition) TRY(anorm_begin(c, W, ld, N));
     auto t1 = Clock::now();
     TRY(factor<double2>(c, W, ld, N, false, nb, st));
     stats->factorizations += 1;
@@ -1402,6 +1418,7 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
     stats->rel_residual = rn / bnorm;
     stats->residual_history[0] = rn / bnorm;
     stats->ms_solve = ms_since(t2);
+    if (c->opts.estimate_condition && c->h_status[SW_INFO] == 0) TRY(condest_fp64(c, W, st, &stats->cond_estimate));
   }
   stats->nb = st.nb;
   if ((!reuse || stats->fp64_fallback) && c->h_status[SW_INFO] != 0) {
@@ -1584,6 +1601,7 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
       stats->factorizations += si.factorizations;
       stats->fp64_fallback |= si.fp64_fallback;
       stats->pivot_growth = std::max(stats->pivot_growth, si.pivot_growth);
+      stats->cond_estimate = std::max(stats->cond_estimate, si.cond_estimate);
       stats->refine_steps += si.refine_steps;
       stats->inner_iterations += si.inner_iterations;
       stats->ms_factor += si.ms_factor;
@@ -1701,6 +1719,83 @@ static int lu_solve_trans(hprmat_b200_ctx* c, const double2* W, long ld, int N, 
     LAUNCH_CHECK();
   }
   c->launches += (size_t)nsteps * 5;
+  return HPRMAT_B200_OK;
+}
+
+// 1-norm condition number of the matrix factorised in FP64 (factors W, st; ||A||_1 left in the
+// status block by anorm_begin): ||A^-1||_1 by the Hager-Higham estimator (N. J. Higham, ACM
+// TOMS 14 (1988) 381-396, the method of LAPACK's ZLACN2 behind ZGECON): x = 1/n; repeat
+// y = A^-1 x, stop when ||y||_1 no longer grows, x = e_j with j = argmax |(A^-H sign(y))_j|,
+// stop when j repeats (at most 5 passes); then the extra vector x_i = (-1)^i (1 + i/(n-1)),
+// estimate 2 ||A^-1 x||_1 / (3n), against matrices that defeat the iteration.  Solves with A on
+// the factors (lu_solve), with A^H as conj(A^-T conj v) (lu_solve_trans); one right-hand side
+// each, vectors on the host.  *kappa = 0 when not available (block size above 64).
+static int condest_fp64(hprmat_b200_ctx* c, const double2* W, const LUState& st, double* kappa) {
+  *kappa = 0.0;
+  const int N = st.N;
+  if (N <= 0 || st.nb > 64) return HPRMAT_B200_OK;
+  unsigned long long abits = 0;
+  HPR_CUDA_TRY(cudaMemcpyAsync(&abits, c->status.as<int>() + kAnormSlot, sizeof(abits), cudaMemcpyDeviceToHost,
+                               c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  double anorm;
+  memcpy(&anorm, &abits, sizeof(double));
+  if (!(anorm > 0.0)) return HPRMAT_B200_OK;
+  TRY(c->cond_v.ensure((size_t)st.ld * sizeof(double2)));
+  double2* dv = c->cond_v.as<double2>();
+  std::vector<double2> v(N);
+  auto solve = [&](bool herm) -> int {
+    if (herm)
+      for (auto& z : v) z.y = -z.y;
+    HPR_CUDA_TRY(cudaMemcpyAsync(dv, v.data(), (size_t)N * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    if (herm) {
+      TRY(lu_solve_trans(c, W, st.ld, N, st.nb, st.nsteps, dv, st.ld, 1));
+    } else {
+      TRY(lu_solve<double2>(c, W, st, dv, st.ld, 1));
+    }
+    HPR_CUDA_TRY(cudaMemcpyAsync(v.data(), dv, (size_t)N * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (herm)
+      for (auto& z : v) z.y = -z.y;
+    return HPRMAT_B200_OK;
+  };
+  auto norm1 = [&]() {
+    double t = 0.0;
+    for (const auto& z : v) t += hypot(z.x, z.y);
+    return t;
+  };
+  for (auto& z : v) z = mk(1.0 / N, 0.0);
+  double est = 0.0;
+  int jlast = -1;
+  for (int pass = 0; pass < 5; ++pass) {
+    TRY(solve(false));
+    const double e = norm1();
+    if (!std::isfinite(e) || (pass > 0 && e <= est)) break;
+    est = e;
+    for (auto& z : v) {
+      const double m = hypot(z.x, z.y);
+      z = m > 0.0 ? mk(z.x / m, z.y / m) : mk(1.0, 0.0);
+    }
+    TRY(solve(true));
+    int j = 0;
+    double best = -1.0;
+    for (int i = 0; i < N; ++i) {
+      const double m = hypot(v[i].x, v[i].y);
+      if (m > best) {
+        best = m;
+        j = i;
+      }
+    }
+    if (j == jlast) break;
+    jlast = j;
+    std::fill(v.begin(), v.end(), mk(0.0, 0.0));
+    v[j] = mk(1.0, 0.0);
+  }
+  for (int i = 0; i < N; ++i)
+    v[i] = mk((i & 1 ? -1.0 : 1.0) * (1.0 + (N > 1 ? (double)i / (N - 1) : 0.0)), 0.0);
+  TRY(solve(false));
+  est = std::max(est, 2.0 * norm1() / (3.0 * N));
+  *kappa = anorm * est;
   return HPRMAT_B200_OK;
 }
 
@@ -1835,6 +1930,7 @@ static int solve_dense_core(hprmat_b200_ctx* c, const double2* dA, double2* dB, 
     }
     int nb = pick_nb(c, N, sizeof(double2), 64);
     if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
+    if (stats && c->opts.estimate_condition) TRY(anorm_begin(c, dA, N, N));
     auto t1 = Clock::now();
     TRY(factor<double2>(c, W, ld, N, false, nb, st));
     if (stats) stats->ms_factor = ms_since(t1);
@@ -1856,6 +1952,7 @@ static int solve_dense_core(hprmat_b200_ctx* c, const double2* dA, double2* dB, 
     LAUNCH_CHECK();
     HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (stats) stats->ms_solve = ms_since(t2);
+    if (stats && c->opts.estimate_condition) TRY(condest_fp64(c, W, st, &stats->cond_estimate));
   }
   if (stats) {
     stats->nb = st.nb;

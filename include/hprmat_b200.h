@@ -60,7 +60,12 @@ typedef struct {
                         factorising C(E) again: between energies C(E) changes only on the
                         diagonal (-k^2 and the closed-channel Bloch terms).  If the refinement
                         does not converge it factorises C(E) and solves again.  Default 0. */
-  int reserved[3];
+  int estimate_condition; /* when nonzero, FP64 factorisations (the FP64 path and the mixed
+                             path's FP64 fallback) also estimate the 1-norm condition number of
+                             the matrix (stats.cond_estimate; LAPACK ZGECON's quantity, by the
+                             Hager-Higham estimator on the factors: ~11 extra solves with one
+                             right-hand side).  Default 0. */
+  int reserved[2];
 } hprmat_b200_opts;
 
 typedef struct {
@@ -82,6 +87,8 @@ typedef struct {
                                (pivot growth above the limit, or an exact zero FP32 pivot, as the
                                reference's Type 2 falls back on CGETRF info != 0) */
   double pivot_growth;      /* max |u_ij| / max |c_ij| (|re| + |im|) of the last factorisation */
+  double cond_estimate;     /* opts.estimate_condition: estimate of ||C||_1 ||C^-1||_1 (largest
+                               over the intervals); 0 when not estimated */
 } hprmat_b200_stats;
 
 /* Defaults for hprmat_b200_opts. */

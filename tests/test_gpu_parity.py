@@ -394,6 +394,57 @@ def test_rmatrix_fp64_fallback_matches_oracle():
         assert _rel(cu[:nopen, :nopen], ref.cu) <= U_TOL
 
 
+@pytest.mark.parametrize("kappa", [1e3, 1e8])
+def test_condition_estimate_dense(kappa):
+    """opts.estimate_condition on the FP64 path: the Hager-Higham estimate of ||A||_1 ||A^-1||_1
+    against numpy's exact 1-norm condition number (a lower bound, within a factor 3 here),
+    for the exact-kappa Householder matrices and a diagonally dominant one."""
+    n = 700
+    rng = np.random.default_rng(3)
+    v = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    v /= np.linalg.norm(v)
+    H = np.eye(n) - 2 * np.outer(v, v.conj())
+    d = kappa ** (-np.arange(n) / (n - 1))
+    A = np.asfortranarray((H * d[None, :]) @ H)
+    B = np.asfortranarray(A @ np.ones((n, 2), np.complex128))
+    exact = float(np.linalg.cond(A, 1))
+    with api.Context(precision="fp64") as c:
+        c.solve_linear(A, B)
+        assert c.last_stats["cond_estimate"] == 0.0  # off by default
+        c.set_estimate_condition(True)
+        X = c.solve_linear(A, B)
+        est = c.last_stats["cond_estimate"]
+        assert exact / 3.0 <= est <= exact * (1 + 1e-6), (est, exact)
+        assert _rel(X, np.linalg.solve(A, B)) <= 1e-12 * max(1.0, kappa / 1e3)
+        A2, B2 = _diag_dominant(500, 2, 4)
+        c.solve_linear(A2, B2)
+        ex2 = float(np.linalg.cond(A2, 1))
+        assert ex2 / 3.0 <= c.last_stats["cond_estimate"] <= ex2 * (1 + 1e-6)
+
+
+def test_condition_estimate_rmatrix_and_fallback():
+    """The same estimate of C(E) on the R-matrix FP64 path (against numpy on the oracle's
+    assembled C) and after a forced FP64 fallback of the mixed path; none on the mixed path."""
+    lib = nat.load()
+    w = workloads.small()
+    mesh = orc.rmat_ini(w.nr, 1, w.rmax)
+    bnd = orc.boundary_values(w.nch, w.lval, w.qk, w.eta, w.rmax)
+    C = orc.assemble(mesh, 1, w.nch, w.lval, w.qk, bnd.xc, w.cpot)
+    exact = float(np.linalg.cond(C, 1))
+    with api.Context(precision="fp64") as c:
+        c.set_estimate_condition(True)
+        c.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+        est = c.last_stats["cond_estimate"]
+        assert exact / 3.0 <= est <= exact * (1 + 1e-6), (est, exact)
+        c.set_precision("mixed")
+        c.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+        assert c.last_stats["cond_estimate"] == 0.0
+        nat.check(lib.hprmat_b200_dev_set_tuning(c._h, b"growth_limit_exp", -30))
+        c.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+        assert c.last_stats["fp64_fallback"] == 1
+        assert abs(c.last_stats["cond_estimate"] / est - 1.0) < 1e-6
+
+
 # ---------------------------------------------------------------- failures
 def test_singular_matrix_reports_status(ctx):
     n = 300
