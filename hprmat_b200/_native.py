@@ -58,7 +58,7 @@ class Stats(ctypes.Structure):
                 ("ms_assemble", ctypes.c_double), ("ms_factor", ctypes.c_double), ("ms_solve", ctypes.c_double),
                 ("ms_refine", ctypes.c_double), ("ms_umatrix", ctypes.c_double), ("ms_total", ctypes.c_double),
                 ("factorizations", ctypes.c_int), ("fp64_fallback", ctypes.c_int), ("pivot_growth", ctypes.c_double),
-                ("cond_estimate", ctypes.c_double)]
+                ("cond_estimate", ctypes.c_double), ("ms_condest", ctypes.c_double)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("residual_history", "floor_history")}

@@ -1418,7 +1418,11 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
     stats->rel_residual = rn / bnorm;
     stats->residual_history[0] = rn / bnorm;
     stats->ms_solve = ms_since(t2);
-    if (c->opts.estimate_condition && c->h_status[SW_INFO] == 0) TRY(condest_fp64(c, W, st, &stats->cond_estimate));
+    if (c->opts.estimate_condition && c->h_status[SW_INFO] == 0) {
+      auto t4 = Clock::now();
+      TRY(condest_fp64(c, W, st, &stats->cond_estimate));
+      stats->ms_condest = ms_since(t4);
+    }
   }
   stats->nb = st.nb;
   if ((!reuse || stats->fp64_fallback) && c->h_status[SW_INFO] != 0) {
@@ -1602,6 +1606,7 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
       stats->fp64_fallback |= si.fp64_fallback;
       stats->pivot_growth = std::max(stats->pivot_growth, si.pivot_growth);
       stats->cond_estimate = std::max(stats->cond_estimate, si.cond_estimate);
+      stats->ms_condest += si.ms_condest;
       stats->refine_steps += si.refine_steps;
       stats->inner_iterations += si.inner_iterations;
       stats->ms_factor += si.ms_factor;
@@ -1952,7 +1957,11 @@ static int solve_dense_core(hprmat_b200_ctx* c, const double2* dA, double2* dB, 
     LAUNCH_CHECK();
     HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (stats) stats->ms_solve = ms_since(t2);
-    if (stats && c->opts.estimate_condition) TRY(condest_fp64(c, W, st, &stats->cond_estimate));
+    if (stats && c->opts.estimate_condition) {
+      auto t4 = Clock::now();
+      TRY(condest_fp64(c, W, st, &stats->cond_estimate));
+      stats->ms_condest = ms_since(t4);
+    }
   }
   if (stats) {
     stats->nb = st.nb;

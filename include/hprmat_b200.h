@@ -89,6 +89,7 @@ typedef struct {
   double pivot_growth;      /* max |u_ij| / max |c_ij| (|re| + |im|) of the last factorisation */
   double cond_estimate;     /* opts.estimate_condition: estimate of ||C||_1 ||C^-1||_1 (largest
                                over the intervals); 0 when not estimated */
+  double ms_condest;        /* host time of the condition estimate (included in ms_total) */
 } hprmat_b200_stats;
 
 /* Defaults for hprmat_b200_opts. */
