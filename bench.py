@@ -59,6 +59,12 @@ def parse():
                     help="scan/adjoint: keep a block's factorisation across energies as the refinement's "
                          "preconditioner (opts.reuse_factors); default off (measured faster that way for "
                          "both workloads)")
+    ap.add_argument("--autotune", type=int, default=0,
+                    help="scan: run the scan autotuner (hprmat_b200_scan_autotune) on the scan's blocks before "
+                         "the warm-up, outside the timed region")
+    ap.add_argument("--tune-cache", default="",
+                    help="scan with --autotune: JSON file of the tuned table; loaded when present, written "
+                         "after tuning otherwise")
     return ap.parse_args()
 
 
@@ -203,6 +209,20 @@ def run_scan(args):
     ctx = api.Context(device=local, precision="mixed", max_refine=3, tol=1e-12, reuse_factors=bool(args.reuse))
     from hprmat_b200 import _native as nat
     lib = nat.load()
+    tune = None
+    if args.autotune:
+        if args.tune_cache and os.path.exists(args.tune_cache):
+            with open(args.tune_cache) as f:
+                table = json.load(f)["table"]
+            ctx.set_scan_tune_table(table)
+            tune = {"source": args.tune_cache, "table": ctx.scan_tune_table()}
+        else:
+            table = ctx.scan_autotune(inputs, 20.0, 60, nworkers=args.workers)
+            tune = {"source": "tuned", "seconds": ctx.last_autotune_seconds, "table": table}
+            if args.tune_cache and rank == 0:
+                import torch as _t
+                with open(args.tune_cache, "w") as f:
+                    json.dump({"device": _t.cuda.get_device_name(local), "workers": args.workers, "table": table}, f)
     for _ in range(args.warmup):
         ctx.rmatrix_scan(inputs[:1], 20.0, 60, nworkers=args.workers, allow_unconverged=True,
                          raise_on_unit_error=False)
@@ -267,7 +287,9 @@ def run_scan(args):
             "data": "synthetic (seeded scan generator, hprmat_b200/workloads.py)",
             "config": {"workload": "batched energy scan: 12 J-pi blocks, nch ~ U{4..64} x 60 points "
                                    "(N = 240..3840), 256 energies each, 3072 solves",
-                       "workers": args.workers, "reuse_factors": bool(args.reuse)},
+                       "workers": args.workers, "reuse_factors": bool(args.reuse),
+                       "autotune": bool(args.autotune)},
+            "autotune": tune,
             "lu_equivalent_complex_tflops": float(tot_flops.item()) * args.steps / wall / 1e12,
             "factorizations_per_step": nfact,
             "units_failed": bad, "units_failed_note": "COULFG ifail=-5 (high-l channels just above threshold); "

@@ -32,7 +32,8 @@ EXPORTED = (
     "hprmat_b200_solve_linear", "hprmat_b200_solve_linear_device", "hprmat_b200_solve_rmatrix",
     "gpu_b200_solve_mixed_", "gpu_b200_solve_double_", "gpu_b200_finalize_", "hprmat_b200_status_string",
     "hprmat_b200_last_error", "hprmat_b200_version", "hprmat_b200_boundary",
-    "hprmat_b200_solve_linear_noalloc", "hprmat_b200_rmatrix_scan",
+    "hprmat_b200_solve_linear_noalloc", "hprmat_b200_rmatrix_scan", "hprmat_b200_scan_autotune",
+    "hprmat_b200_scan_tune_get", "hprmat_b200_scan_tune_set",
     "hprmat_b200_rmatrix_adjoint", "hprmat_b200_rmatrix_wf", "hprmat_b200_rmatrix_wf_device",
     "hprmat_b200_wf_print", "hprmat_b200_rmatrix_full", "hprmat_b200_rmatrix_x", "hprmat_b200_adjoint_from_x",
     # include/hprmat_b200_dev.h
@@ -105,6 +106,9 @@ def load():
         "hprmat_b200_rmatrix": (I, [P, I, IP, DP, DP, D, I, I, DP, I, I, DP, IP, SP]),
         "hprmat_b200_rmatrix_device": (I, [P, I, IP, DP, DP, D, I, I, P, I, I, P, IP, SP]),
         "hprmat_b200_rmatrix_scan": (I, [P, I, ctypes.POINTER(ScanBlock), D, I, I, DP]),
+        "hprmat_b200_scan_autotune": (I, [P, I, ctypes.POINTER(ScanBlock), D, I, I, DP]),
+        "hprmat_b200_scan_tune_get": (I, [P, IP, DP, I]),
+        "hprmat_b200_scan_tune_set": (I, [P, IP, I]),
         "hprmat_b200_rmatrix_adjoint": (I, [P, I, IP, DP, DP, D, I, I, DP, I, I, DP, DP, IP, DP, SP]),
         "hprmat_b200_rmatrix_wf": (I, [P, I, IP, DP, DP, D, I, I, DP, I, I, DP, IP, I, IP, DP, I, I, SP]),
         "hprmat_b200_rmatrix_wf_device": (I, [P, I, IP, DP, DP, D, I, I, P, I, I, P, IP, I, IP, P, I, I, SP]),

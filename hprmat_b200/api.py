@@ -167,6 +167,50 @@ class Context:
         shape (nenergies, nch), cpot (ncp1, nch, nch) complex, Fortran order.  Returns a list of
         (cu (nenergies, nch, nch) with U in cu[e, :nopen, :nopen], nopen (nenergies,),
         status (nenergies,)) and sets ``last_scan_seconds``."""
+        keep, arr, out = self._scan_blocks(blocks)
+        self._ensure_mesh(nr, 1, rmax)
+        blocks_c = (nat.ScanBlock * len(arr))(*arr)
+        secs = ctypes.c_double(0.0)
+        s = self._lib.hprmat_b200_rmatrix_scan(self._h, len(arr), blocks_c, float(rmax), int(nr), int(nworkers),
+                                               ctypes.byref(secs))
+        self.last_scan_seconds = secs.value
+        if raise_on_unit_error:
+            nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
+        # the library writes each U column-major (Fortran) into its (nch, nch) slot
+        return [(np.ascontiguousarray(cu.transpose(0, 2, 1)), nopen, status) for cu, nopen, status in out]
+
+    TUNE_KEYS = ("N", "nb", "panel_cluster", "panel_rpc_min", "wave_sb", "gmres_m")
+
+    def scan_autotune(self, blocks, rmax, nr, nworkers=0):
+        """Autotune the scan's per-order settings on these blocks (hprmat_b200_scan_autotune);
+        returns the table (``scan_tune_table``) and sets ``last_autotune_seconds``."""
+        keep, arr, _out = self._scan_blocks(blocks)
+        self._ensure_mesh(nr, 1, rmax)
+        blocks_c = (nat.ScanBlock * len(arr))(*arr)
+        secs = ctypes.c_double(0.0)
+        nat.check(self._lib.hprmat_b200_scan_autotune(self._h, len(arr), blocks_c, float(rmax), int(nr),
+                                                      int(nworkers), ctypes.byref(secs)))
+        self.last_autotune_seconds = secs.value
+        del keep
+        return self.scan_tune_table()
+
+    def scan_tune_table(self):
+        """The autotuner's rows as dicts (keys TUNE_KEYS and the trial time ``ms``)."""
+        n = self._lib.hprmat_b200_scan_tune_get(self._h, None, None, 0)
+        rows = np.zeros((max(n, 1), 6), np.int32)
+        ms = np.zeros(max(n, 1))
+        self._lib.hprmat_b200_scan_tune_get(self._h, _iptr(rows), _dptr(ms), n)
+        return [dict(zip(self.TUNE_KEYS, map(int, rows[i])), ms=float(ms[i])) for i in range(n)]
+
+    def set_scan_tune_table(self, table):
+        """Load a table (rows as ``scan_tune_table`` returns them, e.g. from a JSON cache)."""
+        rows = np.array([[int(r[k]) for k in self.TUNE_KEYS] for r in table], np.int32).reshape(-1, 6)
+        nat.check(self._lib.hprmat_b200_scan_tune_set(self._h, _iptr(np.ascontiguousarray(rows)), len(rows)))
+
+    @staticmethod
+    def _scan_blocks(blocks):
+        """ScanBlock records for (lval, cpot, qk, eta) blocks, the arrays they point into (keep
+        them alive) and the output arrays (cu, nopen, status) per block."""
         keep, arr, out = [], [], []
         for lval, cpot, qk, eta in blocks:
             lval = np.ascontiguousarray(lval, dtype=np.int32)
@@ -184,16 +228,7 @@ class Context:
                               _iptr(nopen), _iptr(status))
             arr.append(b)
             out.append((cu, nopen, status))
-        self._ensure_mesh(nr, 1, rmax)
-        blocks_c = (nat.ScanBlock * len(arr))(*arr)
-        secs = ctypes.c_double(0.0)
-        s = self._lib.hprmat_b200_rmatrix_scan(self._h, len(arr), blocks_c, float(rmax), int(nr), int(nworkers),
-                                               ctypes.byref(secs))
-        self.last_scan_seconds = secs.value
-        if raise_on_unit_error:
-            nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
-        # the library writes each U column-major (Fortran) into its (nch, nch) slot
-        return [(np.ascontiguousarray(cu.transpose(0, 2, 1)), nopen, status) for cu, nopen, status in out]
+        return keep, arr, out
 
     def rmatrix_adjoint(self, nch, lval, qk, eta, rmax, nr, cpot, gu):
         """Collision matrix and the gradient of a real loss with respect to the potential.

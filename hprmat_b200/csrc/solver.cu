@@ -92,6 +92,13 @@ struct DevBuf {
 
 static constexpr int kSwapStride = 3 * kMaxNB + 4;  // ints per step in the swap store
 
+// One row of the scan autotuner's table: the settings chosen for the units of order N, and the
+// time of the tuned trial (all workers solving one energy of order N at once).
+struct ScanTune {
+  int N, nb, cluster, rpc_min, sb, gmres_m;
+  double ms;
+};
+
 struct hprmat_b200_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -157,6 +164,7 @@ struct hprmat_b200_ctx {
   // batched energy scans: worker contexts (own stream and buffers) and the blocks' potentials
   std::vector<hprmat_b200_ctx*> scan_workers;
   std::vector<std::unique_ptr<DevBuf>> scan_cpot;
+  std::vector<ScanTune> scan_tune;  // autotuner table, applied per unit by rmatrix_scan
   int wtrace_units = 0;
   int* h_status = nullptr;  // pinned
   double* h_norms = nullptr;  // pinned
@@ -2305,45 +2313,21 @@ int hprmat_b200_wf_print(int nch, const int* lval, const double* qk, const doubl
 // Batched energy scan: every block's potential is copied once; (block, energy) units are
 // taken largest first by worker contexts, one host thread and one stream each, so that the
 // solves of different units overlap on the device.  Each unit is rmatrix_core as for one
-// energy.
-int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_scan_block* blocks, double rmax,
-                             int nr, int nworkers, double* seconds) {
-  TRY(check_ctx(c));
+// energy, with the autotuner's settings for its order when the table has them.
+static int scan_check_blocks(int nblocks, const hprmat_b200_scan_block* blocks, double rmax, int nr, const char* who) {
   if (nblocks < 0 || (nblocks > 0 && !blocks) || nr <= 0 || !(rmax > 0.0))
-    return fail(HPRMAT_B200_ERR_ARG, "rmatrix_scan: invalid arguments");
-  auto t0 = Clock::now();
-  // work items: runs of up to kChunk energies of one block in energy order (the first
-  // channel's signed k^2 orders the energies of a block), largest blocks first; with
-  // opts.reuse_factors a worker keeps one factorisation across the run
-  constexpr int kChunk = 32;
-  struct Unit {
-    int b;
-    std::vector<int> es;
-    long n;
-  };
-  std::vector<Unit> units;
-  size_t nunits = 0;
+    return fail(HPRMAT_B200_ERR_ARG, "%s: invalid arguments", who);
   for (int b = 0; b < nblocks; ++b) {
     const hprmat_b200_scan_block& B = blocks[b];
     if (B.nch <= 0 || B.nenergies < 0 || !B.lval || !B.cpot || B.ncp1 < nr || !B.cu || !B.nopen || !B.status ||
         (B.nenergies > 0 && (!B.qk || !B.eta)))
-      return fail(HPRMAT_B200_ERR_ARG, "rmatrix_scan: invalid block %d", b);
-    std::vector<int> order(B.nenergies);
-    for (int e = 0; e < B.nenergies; ++e) order[e] = e;
-    auto key = [&](int e) {
-      const double k = B.qk[(size_t)e * B.nch];
-      return k > 0 ? k * k : -k * k;
-    };
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key(x) < key(y); });
-    for (int e0 = 0; e0 < B.nenergies; e0 += kChunk) {
-      Unit u{b, {}, (long)B.nch * nr};
-      u.es.assign(order.begin() + e0, order.begin() + std::min(B.nenergies, e0 + kChunk));
-      units.push_back(std::move(u));
-    }
-    nunits += B.nenergies;
+      return fail(HPRMAT_B200_ERR_ARG, "%s: invalid block %d", who, b);
   }
-  std::stable_sort(units.begin(), units.end(), [](const Unit& x, const Unit& y) { return x.n > y.n; });
-  // potentials on the device, once per block
+  return HPRMAT_B200_OK;
+}
+
+// The blocks' potentials on the device (c->scan_cpot), once per block.
+static int scan_upload(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_scan_block* blocks) {
   HPR_CUDA_TRY(cudaSetDevice(c->device));
   c->scan_cpot.clear();
   for (int b = 0; b < nblocks; ++b) {
@@ -2354,10 +2338,11 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_
     HPR_CUDA_TRY(cudaMemcpyAsync(c->scan_cpot.back()->p, B.cpot, pbytes, cudaMemcpyHostToDevice, c->stream));
   }
   HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  // workers
-  if (nworkers <= 0) nworkers = 4;
-  nworkers = std::max(1, std::min<int>(nworkers, (int)std::max<size_t>(units.size(), 1)));
-  (void)nunits;
+  return HPRMAT_B200_OK;
+}
+
+// nworkers worker contexts with the context's options and settings and the scan's mesh.
+static int scan_workers_ready(hprmat_b200_ctx* c, int nworkers, int nr, double rmax) {
   while ((int)c->scan_workers.size() < nworkers) {
     hprmat_b200_ctx* w = nullptr;
     TRY(hprmat_b200_create(c->device, &c->opts, &w));
@@ -2369,10 +2354,71 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_
     w->opts = c->opts;
     w->wave_sb = c->wave_sb;
     w->wave_un = c->wave_un;
+    w->panel_cluster = c->panel_cluster;
+    w->panel_rpc_min = c->panel_rpc_min;
+    w->gmres_m = c->gmres_m;
     w->reuse_max_inner = c->reuse_max_inner;
     w->lu_held = false;
     TRY(hprmat_b200_rmat_ini(w, nr, 1, rmax, zrma.data()));
   }
+  return HPRMAT_B200_OK;
+}
+
+// Settings of a worker for one unit: the row t, or the context's own settings (t null).
+static void scan_apply(hprmat_b200_ctx* w, const hprmat_b200_ctx* c, const ScanTune* t) {
+  w->opts.panel_nb = t ? t->nb : c->opts.panel_nb;
+  w->panel_cluster = t ? t->cluster != 0 : c->panel_cluster;
+  w->panel_rpc_min = t ? t->rpc_min : c->panel_rpc_min;
+  w->wave_sb = t ? t->sb : c->wave_sb;
+  w->gmres_m = t ? t->gmres_m : c->gmres_m;
+}
+
+static const ScanTune* scan_row(const hprmat_b200_ctx* c, long N) {
+  for (const ScanTune& t : c->scan_tune)
+    if (t.N == N) return &t;
+  return nullptr;
+}
+
+// The block's energies in the scan's order (the first channel's signed k^2).
+static std::vector<int> scan_energy_order(const hprmat_b200_scan_block& B) {
+  std::vector<int> order(B.nenergies);
+  for (int e = 0; e < B.nenergies; ++e) order[e] = e;
+  auto key = [&](int e) {
+    const double k = B.qk[(size_t)e * B.nch];
+    return k > 0 ? k * k : -k * k;
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return key(x) < key(y); });
+  return order;
+}
+
+int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_scan_block* blocks, double rmax,
+                             int nr, int nworkers, double* seconds) {
+  TRY(check_ctx(c));
+  TRY(scan_check_blocks(nblocks, blocks, rmax, nr, "rmatrix_scan"));
+  auto t0 = Clock::now();
+  // work items: runs of up to kChunk energies of one block in energy order, largest blocks
+  // first; with opts.reuse_factors a worker keeps one factorisation across the run
+  constexpr int kChunk = 32;
+  struct Unit {
+    int b;
+    std::vector<int> es;
+    long n;
+  };
+  std::vector<Unit> units;
+  for (int b = 0; b < nblocks; ++b) {
+    const hprmat_b200_scan_block& B = blocks[b];
+    const std::vector<int> order = scan_energy_order(B);
+    for (int e0 = 0; e0 < B.nenergies; e0 += kChunk) {
+      Unit u{b, {}, (long)B.nch * nr};
+      u.es.assign(order.begin() + e0, order.begin() + std::min(B.nenergies, e0 + kChunk));
+      units.push_back(std::move(u));
+    }
+  }
+  std::stable_sort(units.begin(), units.end(), [](const Unit& x, const Unit& y) { return x.n > y.n; });
+  TRY(scan_upload(c, nblocks, blocks));
+  if (nworkers <= 0) nworkers = 4;
+  nworkers = std::max(1, std::min<int>(nworkers, (int)std::max<size_t>(units.size(), 1)));
+  TRY(scan_workers_ready(c, nworkers, nr, rmax));
   std::atomic<size_t> next{0};
   std::atomic<int> first_error{0};
   std::mutex err_mu;
@@ -2386,6 +2432,7 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_
       const Unit& u = units[k];
       const hprmat_b200_scan_block& B = blocks[u.b];
       const size_t ubytes = (size_t)B.nch * B.nch * sizeof(double2);
+      scan_apply(w, c, scan_row(c, u.n));
       for (const int e : u.es) {
         int s = w->cu.ensure(ubytes);
         int nopen = 0;
@@ -2418,6 +2465,162 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_
   const int fe = first_error.load();
   if (fe != HPRMAT_B200_OK && fe != HPRMAT_B200_NOT_CONVERGED) return fail(fe, "rmatrix_scan: %s", err_msg.c_str());
   return fe;
+}
+
+// Scan autotuner (see the header).  A trial runs one energy of a block on every worker at once
+// (a warm-up round, then the best of two timed rounds, host wall clock around the joined
+// threads, each worker's stream synchronised): the device under the scan's own concurrency.
+int hprmat_b200_scan_autotune(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_scan_block* blocks, double rmax,
+                              int nr, int nworkers, double* seconds) {
+  TRY(check_ctx(c));
+  TRY(scan_check_blocks(nblocks, blocks, rmax, nr, "scan_autotune"));
+  auto t0 = Clock::now();
+  TRY(scan_upload(c, nblocks, blocks));
+  if (nworkers <= 0) nworkers = 4;
+  TRY(scan_workers_ready(c, nworkers, nr, rmax));
+  std::vector<ScanTune> table;
+  auto trial = [&](const ScanTune& t, int b, int e, double* ms) -> int {
+    const hprmat_b200_scan_block& B = blocks[b];
+    const size_t ubytes = (size_t)B.nch * B.nch * sizeof(double2);
+    std::atomic<int> err{0};
+    auto run = [&](int wi) {
+      hprmat_b200_ctx* w = c->scan_workers[wi];
+      cudaSetDevice(w->device);
+      scan_apply(w, c, &t);
+      w->lu_held = false;
+      int nopen = 0;
+      int s = w->cu.ensure(ubytes);
+      if (s == HPRMAT_B200_OK)
+        s = rmatrix_core(w, B.nch, B.lval, B.qk + (size_t)e * B.nch, B.eta + (size_t)e * B.nch, rmax, nr, 1,
+                         c->scan_cpot[b]->as<double2>(), B.ncp1, B.nch, w->cu.as<double2>(), &nopen, nullptr);
+      if ((s == HPRMAT_B200_OK || s == HPRMAT_B200_NOT_CONVERGED) && cudaStreamSynchronize(w->stream) != cudaSuccess)
+        s = HPRMAT_B200_ERR_CUDA;
+      if (s != HPRMAT_B200_OK && s != HPRMAT_B200_NOT_CONVERGED) {
+        int z = 0;
+        err.compare_exchange_strong(z, s);
+      }
+    };
+    double best = 0.0;
+    for (int round = 0; round < 3; ++round) {
+      auto r0 = Clock::now();
+      std::vector<std::thread> th;
+      for (int i = 1; i < nworkers; ++i) th.emplace_back(run, i);
+      run(0);
+      for (auto& x : th) x.join();
+      const double dt = ms_since(r0);
+      if (err.load() != 0) return err.load();
+      if (round == 1 || (round == 2 && dt < best)) best = dt;
+    }
+    *ms = best;
+    return HPRMAT_B200_OK;
+  };
+  std::vector<long> done;
+  for (int b = 0; b < nblocks; ++b) {
+    const hprmat_b200_scan_block& B = blocks[b];
+    const long N = (long)B.nch * nr;
+    if (B.nenergies == 0 || std::find(done.begin(), done.end(), N) != done.end()) continue;
+    done.push_back(N);
+    const std::vector<int> order = scan_energy_order(B);
+    ScanTune cur{(int)N, c->opts.panel_nb > 0 ? c->opts.panel_nb : 128, c->panel_cluster ? 1 : 0, c->panel_rpc_min,
+                 c->wave_sb, c->gmres_m, 0.0};
+    // a representative energy whose solve succeeds: the middle one, else the first or last
+    int e = -1;
+    double best = 0.0;
+    for (const int cand : {order[order.size() / 2], order.front(), order.back()}) {
+      if (trial(cur, b, cand, &best) == HPRMAT_B200_OK) {
+        e = cand;
+        break;
+      }
+    }
+    if (e < 0) continue;
+    // a setting is taken when it is 5% faster twice: once against the incumbent's best time,
+    // then again against a fresh trial of the incumbent (concurrent trials vary by a few %)
+    auto consider = [&](ScanTune t) -> int {
+      double ms = 0.0;
+      if (trial(t, b, e, &ms) != HPRMAT_B200_OK || !(ms < 0.95 * best)) return HPRMAT_B200_OK;
+      double ms_inc = 0.0, ms2 = 0.0;
+      if (trial(cur, b, e, &ms_inc) != HPRMAT_B200_OK || trial(t, b, e, &ms2) != HPRMAT_B200_OK)
+        return HPRMAT_B200_OK;
+      ms = std::min(ms, ms2);
+      best = std::min(best, ms_inc);
+      if (ms < 0.95 * best) {
+        best = ms;
+        cur = t;
+      }
+      return HPRMAT_B200_OK;
+    };
+    for (const int v : {128, 64, 32}) {
+      if (v == cur.nb || pick_nb(c, (int)N, sizeof(float2), v) != v) continue;
+      ScanTune t = cur;
+      t.nb = v;
+      TRY(consider(t));
+    }
+    {
+      ScanTune t = cur;
+      t.cluster = !cur.cluster;
+      TRY(consider(t));
+    }
+    for (const int v : {16, 32, 64}) {
+      if (v == cur.rpc_min) continue;
+      ScanTune t = cur;
+      t.rpc_min = v;
+      TRY(consider(t));
+    }
+    for (const int v : {0, 2, 1}) {
+      if (v == cur.sb) continue;
+      ScanTune t = cur;
+      t.sb = v;
+      TRY(consider(t));
+    }
+    for (const int v : {12, 8, 16}) {
+      if (v == cur.gmres_m) continue;
+      ScanTune t = cur;
+      t.gmres_m = v;
+      TRY(consider(t));
+    }
+    cur.ms = best;
+    table.push_back(cur);
+  }
+  for (int i = 0; i < nworkers; ++i) scan_apply(c->scan_workers[i], c, nullptr);
+  c->scan_tune = table;
+  if (seconds) *seconds = std::chrono::duration<double>(Clock::now() - t0).count();
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_scan_tune_get(hprmat_b200_ctx* c, int* rows, double* ms, int max) {
+  if (!c) return -1;
+  const int n = (int)c->scan_tune.size();
+  const int m = max > 0 ? std::min(max, n) : 0;
+  for (int i = 0; i < m; ++i) {
+    const ScanTune& t = c->scan_tune[i];
+    if (rows) {
+      int* r = rows + (size_t)6 * i;
+      r[0] = t.N;
+      r[1] = t.nb;
+      r[2] = t.cluster;
+      r[3] = t.rpc_min;
+      r[4] = t.sb;
+      r[5] = t.gmres_m;
+    }
+    if (ms) ms[i] = t.ms;
+  }
+  return n;
+}
+
+int hprmat_b200_scan_tune_set(hprmat_b200_ctx* c, const int* rows, int n) {
+  TRY(check_ctx(c));
+  if (n < 0 || (n > 0 && !rows)) return fail(HPRMAT_B200_ERR_ARG, "scan_tune_set: invalid arguments");
+  std::vector<ScanTune> table;
+  for (int i = 0; i < n; ++i) {
+    const int* r = rows + (size_t)6 * i;
+    const bool ok = r[0] > 0 && (r[1] == 16 || r[1] == 32 || r[1] == 64 || r[1] == 128) && (r[2] == 0 || r[2] == 1) &&
+                    r[3] >= 1 && (r[4] == 0 || r[4] == 1 || r[4] == 2 || r[4] == 4) && r[5] >= 1 &&
+                    r[5] <= kGmresMaxM;
+    if (!ok) return fail(HPRMAT_B200_ERR_ARG, "scan_tune_set: invalid row %d", i);
+    table.push_back(ScanTune{r[0], r[1], r[2], r[3], r[4], r[5], 0.0});
+  }
+  c->scan_tune = table;
+  return HPRMAT_B200_OK;
 }
 
 // Adjoint of one collision matrix.  Symmetric potential: the forward solve at the context's

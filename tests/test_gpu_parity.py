@@ -189,7 +189,7 @@ def test_block_size_change_on_one_context():
     ref = _oracle_u(w)
     lib = nat.load()
     c = api.Context(precision="mixed", panel_nb=64)
-    for nb in (64, 0, 64, 0):
+    for nb in (64, 0, 64, 0, 32, 0):
         c.opts.panel_nb = nb
         nat.check(lib.hprmat_b200_set_opts(c._h, ctypes.byref(c.opts)))
         cu, nopen = c.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)

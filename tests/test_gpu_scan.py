@@ -117,3 +117,45 @@ def test_reuse_across_energies_single_calls():
     ref = orc.rmatrix(w2.nch, w2.lval, w2.qk, w2.eta, 16.0, mesh, w2.cpot)
     assert np.linalg.norm(cu[:nopen, :nopen] - ref.cu) / np.linalg.norm(ref.cu) <= U_TOL
     ctx.close()
+
+
+def test_scan_autotune_table_and_parity():
+    """hprmat_b200_scan_autotune: one row per distinct order with settings from its candidate
+    sets; a scan with the table gives every unit to 1e-10 of the oracle; the table survives a
+    get/set round trip, rejects an invalid row, and clears."""
+    from hprmat_b200 import _native as nat
+    blocks = _blocks()
+    args = [(w.lval, w.cpot, qk, eta) for w, qk, eta in blocks]
+    ctx = api.Context(precision="mixed")
+    table = ctx.scan_autotune(args, 20.0, 60, nworkers=2)
+    assert ctx.last_autotune_seconds > 0.0
+    assert sorted(r["N"] for r in table) == sorted(w.nch * 60 for w, _q, _e in blocks)
+    for r in table:
+        assert r["nb"] in (32, 64, 128) and r["panel_cluster"] in (0, 1)
+        assert r["panel_rpc_min"] in (16, 32, 64) and r["wave_sb"] in (0, 1, 2)
+        assert r["gmres_m"] in (8, 12, 16) and r["ms"] > 0.0
+    res = ctx.rmatrix_scan(args, 20.0, 60, nworkers=3)
+    mesh = orc.rmat_ini(60, 1, 20.0)
+    for (w, qk, eta), (cu, nopen, status) in zip(blocks, res):
+        for e in range(qk.shape[0]):
+            ref = orc.rmatrix(w.nch, w.lval, qk[e], eta[e], 20.0, mesh, w.cpot)
+            assert status[e] == 0 and nopen[e] == ref.nopen
+            no = ref.nopen
+            assert np.linalg.norm(cu[e, :no, :no] - ref.cu) / np.linalg.norm(ref.cu) <= U_TOL
+    # a table forcing 64-column blocks, grid panels and short cycles for every order still agrees
+    forced = [dict(N=w.nch * 60, nb=64, panel_cluster=0, panel_rpc_min=16, wave_sb=1, gmres_m=8)
+              for w, _q, _e in blocks]
+    ctx.set_scan_tune_table(forced)
+    assert [{k: r[k] for k in api.Context.TUNE_KEYS} for r in ctx.scan_tune_table()] == forced
+    res = ctx.rmatrix_scan(args, 20.0, 60, nworkers=2)
+    for (w, qk, eta), (cu, nopen, status) in zip(blocks, res):
+        ref = orc.rmatrix(w.nch, w.lval, qk[-1], eta[-1], 20.0, mesh, w.cpot)
+        no = ref.nopen
+        assert status[-1] == 0
+        assert np.linalg.norm(cu[-1, :no, :no] - ref.cu) / np.linalg.norm(ref.cu) <= U_TOL
+    bad = dict(forced[0], nb=96)
+    with pytest.raises(nat.HprmatError):
+        ctx.set_scan_tune_table([bad])
+    ctx.set_scan_tune_table([])
+    assert ctx.scan_tune_table() == []
+    ctx.close()
