@@ -158,6 +158,7 @@ def test_batched_collision_matrices_match_per_energy():
     L2 = sum(torch.sum(torch.abs(u) ** 2 * (1 + k)) for k, u in enumerate(us2))
     L2.backward()
     for a, b in zip(us, us2):
+        a, b = a.detach(), b.detach()
         assert torch.allclose(a, b, rtol=0, atol=1e-12 * float(b.abs().max()))
     assert torch.allclose(g1, q.grad, rtol=1e-10, atol=1e-12 * float(q.grad.abs().max()))
     for c in pool + [ctx]:
