@@ -92,6 +92,15 @@ struct DevBuf {
 
 static constexpr int kSwapStride = 3 * kMaxNB + 4;  // ints per step in the swap store
 
+// Status-block slots beyond the factorisation's own (SW_*; int offsets into the 64-int block):
+// the largest |re| + |im| of the matrix about to be factorised (float bits, written by the
+// assembly / conversion kernels for the pivot-growth check) and ||C||_1 (double bits, 8-byte
+// aligned, written by colabs_max_kernel when opts.estimate_condition is set).  The
+// factorisation copies the first kStatusCopy ints to h_status when it ends.
+constexpr int kAmaxSlot = 40;
+constexpr int kAnormSlot = 42;
+constexpr int kStatusCopy = 44;
+
 // One row of the scan autotuner's table: the settings chosen for the units of order N, and the
 // time of the tuned trial (all workers solving one energy of order N at once).
 struct ScanTune {
@@ -789,7 +798,7 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
   if constexpr (NB == 128 && std::is_same<T, float2>::value) {
     if (mixed && nsteps >= 2 && c->wave_enabled) TRY(wave_prepare(c, st));
   }
-  HPR_CUDA_TRY(cudaMemcpyAsync(c->h_status, status, SW_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->h_status, status, kStatusCopy * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
   if (c->h_status[SW_TIMEOUT] != 0)
     return fail(HPRMAT_B200_ERR_TIMEOUT, "panel factorisation: grid barrier wait limit exceeded (site %d)",
@@ -1251,12 +1260,6 @@ static double ms_since(Clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
 }
 
-// Status-block slot of the largest |re| + |im| of the matrix (float bits), written by the
-// assembly / conversion kernels for the pivot-growth check.
-constexpr int kAmaxSlot = 40;
-// Status-block slot (int offset, 8-byte aligned) of ||C||_1 as double bits, written by
-// colabs_max_kernel before an FP64 factorisation when opts.estimate_condition is set.
-constexpr int kAnormSlot = 42;
 
 static int condest_fp64(hprmat_b200_ctx* c, const double2* W, const LUState& st, double* kappa);
 
@@ -1270,13 +1273,10 @@ static int anorm_begin(hprmat_b200_ctx* c, const double2* A, long lda, int N) {
 }
 
 // Pivot growth of the last factorisation: the largest |re| + |im| of U (accumulated by the
-// panel and U12 kernels into the status block, copied to h_status by factor) over that of the
-// matrix (kAmaxSlot).  0 for a zero matrix.
+// panel and U12 kernels into the status block) over that of the matrix (kAmaxSlot), both from
+// the copy factor made.  0 for a zero matrix.
 static int pivot_growth(hprmat_b200_ctx* c, double* rho) {
-  unsigned abits = 0;
-  HPR_CUDA_TRY(cudaMemcpyAsync(&abits, c->status.as<int>() + kAmaxSlot, sizeof(unsigned), cudaMemcpyDeviceToHost,
-                               c->stream));
-  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const unsigned abits = (unsigned)c->h_status[kAmaxSlot];
   const unsigned gbits = (unsigned)c->h_status[SW_COUNT - 1];
   float g, am;
   memcpy(&g, &gbits, sizeof(float));
@@ -1736,7 +1736,7 @@ static int lu_solve_trans(hprmat_b200_ctx* c, const double2* W, long ld, int N, 
 }
 
 // 1-norm condition number of the matrix factorised in FP64 (factors W, st; ||A||_1 left in the
-// status block by anorm_begin): ||A^-1||_1 by the Hager-Higham estimator (N. J. Higham, ACM
+// status block by anorm_begin and copied to h_status by factor): ||A^-1||_1 by the Hager-Higham estimator (N. J. Higham, ACM
 // TOMS 14 (1988) 381-396, the method of LAPACK's ZLACN2 behind ZGECON): x = 1/n; repeat
 // y = A^-1 x, stop when ||y||_1 no longer grows, x = e_j with j = argmax |(A^-H sign(y))_j|,
 // stop when j repeats (at most 5 passes); then the extra vector x_i = (-1)^i (1 + i/(n-1)),
@@ -1747,12 +1747,8 @@ static int condest_fp64(hprmat_b200_ctx* c, const double2* W, const LUState& st,
   *kappa = 0.0;
   const int N = st.N;
   if (N <= 0 || st.nb > 64) return HPRMAT_B200_OK;
-  unsigned long long abits = 0;
-  HPR_CUDA_TRY(cudaMemcpyAsync(&abits, c->status.as<int>() + kAnormSlot, sizeof(abits), cudaMemcpyDeviceToHost,
-                               c->stream));
-  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  double anorm;
-  memcpy(&anorm, &abits, sizeof(double));
+  double anorm;  // from the copy factor made of the status block
+  memcpy(&anorm, c->h_status + kAnormSlot, sizeof(double));
   if (!(anorm > 0.0)) return HPRMAT_B200_OK;
   TRY(c->cond_v.ensure((size_t)st.ld * sizeof(double2)));
   double2* dv = c->cond_v.as<double2>();
