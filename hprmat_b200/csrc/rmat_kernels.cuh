@@ -104,30 +104,43 @@ __global__ void assemble_kernel(MeshDev mesh, ChannelData ch, int nch, const dou
     const double rr = mesh.r[i];
     const double dg = ch.fac[c] / (rr * rr) + ch.kk[c];
     const double bl = ch.bloch[c];
+    // column col = cp nr + j, stepped by gridDim.y without a division per element
+    const int cstep = gridDim.y / nr, jstep = gridDim.y - cstep * nr;
+    int cp = blockIdx.y / nr, j = blockIdx.y - cp * nr;
     for (int col = blockIdx.y; col < N; col += gridDim.y) {
-      const int cp = col / nr, j = col - cp * nr;
-      double re = 0.0, im = 0.0;
-      if (c == cp) {
-        re = mesh.tc[i + (size_t)j * nr] - bl * mesh.blo0[i + (size_t)j * nr];
-        if (i == j) re += dg;
-      }
-      if (i == j) {
-        double2 v = cpot[(size_t)i + ncp1 * ((size_t)c + ndim * (size_t)cp)];
-        re += v.x;
-        im += v.y;
-      }
-      if (nl.p) {
-        const double wf = sqrt(nl.wle[i] * nl.wle[j]) * nl.rmax0;
-        const double2 v = nl.p[(size_t)i * nr + j + nl.ncp2 * ((size_t)c + nl.ndim * (size_t)cp)];
-        re += wf * v.x;
-        im += wf * v.y;
-      }
       T out;
-      out.x = (typename RealOf<T>::R)re;
-      out.y = (typename RealOf<T>::R)im;
+      if (c == cp || i == j || nl.p) {
+        double re = 0.0, im = 0.0;
+        if (c == cp) {
+          re = mesh.tc[i + (size_t)j * nr] - bl * mesh.blo0[i + (size_t)j * nr];
+          if (i == j) re += dg;
+        }
+        if (i == j) {
+          double2 v = cpot[(size_t)i + ncp1 * ((size_t)c + ndim * (size_t)cp)];
+          re += v.x;
+          im += v.y;
+        }
+        if (nl.p) {
+          const double wf = sqrt(nl.wle[i] * nl.wle[j]) * nl.rmax0;
+          const double2 v = nl.p[(size_t)i * nr + j + nl.ncp2 * ((size_t)c + nl.ndim * (size_t)cp)];
+          re += wf * v.x;
+          im += wf * v.y;
+        }
+        out.x = (typename RealOf<T>::R)re;
+        out.y = (typename RealOf<T>::R)im;
+        sq += re * re + im * im;
+        am = fmaxf(am, (float)(fabs(re) + fabs(im)));
+      } else {  // off the channel's block and off the mesh diagonal: C is zero there
+        out.x = 0;
+        out.y = 0;
+      }
       W[(size_t)row + (size_t)col * ld] = out;
-      sq += re * re + im * im;
-      am = fmaxf(am, (float)(fabs(re) + fabs(im)));
+      cp += cstep;
+      j += jstep;
+      if (j >= nr) {
+        j -= nr;
+        ++cp;
+      }
     }
   }
   if (amax) block_max_atomic(am, amax);
