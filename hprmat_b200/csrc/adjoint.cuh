@@ -47,7 +47,8 @@ __global__ void __launch_bounds__(256) trans_partial_kernel(const double2* __res
     for (int r = 0; r < nrow; ++r) {
       const double2 a = As[r][j];
 #pragma unroll
-      for (int q = 0; q < 32; ++q) cfma(acc[q], a, Ys[r][cb + 4 * q]);
+      for (int q = 0; q < 32; ++q)
+        if (cb + 4 * q < nrhs) cfma(acc[q], a, Ys[r][cb + 4 * q]);  // few right-hand sides: skip the rest
     }
     __syncthreads();
   }

@@ -746,6 +746,43 @@ __global__ void __launch_bounds__(256) cgemm_update_kernel(int M, int N, int K, 
   }
 }
 
+// C[M x N] -= A[M x K] * B[K x N] for few columns (N <= 8, K <= 128): the block updates of
+// triangular solves with one or a few right-hand sides, where the 64 x 64 tiles of
+// cgemm_update_kernel would compute mostly empty columns.  One thread per row of A (coalesced
+// column reads), B staged in shared memory.
+template <typename T>
+__global__ void __launch_bounds__(256) cgemv_update_kernel(int M, int N, int K, const T* __restrict__ A, long lda,
+                                                           const T* __restrict__ B, long ldb, T* C, long ldc) {
+  constexpr int kMaxN = 8, kMaxK = 128;
+  __shared__ T Bs[kMaxN][kMaxK];
+  for (int e = threadIdx.x; e < K * N; e += blockDim.x) {
+    const int k = e % K, n = e / K;
+    Bs[n][k] = B[(size_t)k + (size_t)n * ldb];
+  }
+  __syncthreads();
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  T acc[kMaxN];
+#pragma unroll
+  for (int n = 0; n < kMaxN; ++n) acc[n] = czero<T>();
+  for (int k = 0; k < K; ++k) {
+    const T a = A[(size_t)m + (size_t)k * lda];
+#pragma unroll
+    for (int n = 0; n < kMaxN; ++n)
+      if (n < N) cfma(acc[n], a, Bs[n][k]);
+  }
+#pragma unroll
+  for (int n = 0; n < kMaxN; ++n) {
+    if (n < N) {
+      T* p = C + (size_t)m + (size_t)n * ldc;
+      T v = *p;
+      v.x -= acc[n].x;
+      v.y -= acc[n].y;
+      *p = v;
+    }
+  }
+}
+
 // -------------------------------------------------------------------------------------
 // Explicit inverses of the diagonal blocks, used by the triangular solves with many
 // right-hand sides (each block solve becomes a small dense product instead of a chain of

@@ -851,7 +851,11 @@ static int lu_solve_impl(hprmat_b200_ctx* c, const T* W, const LUState& st, T* X
                                    sw + 3 * kMaxNB, X, ldx, nrhs, nullptr, 0);
     LAUNCH_CHECK();
     const int M2 = N - k0 - ncols;
-    if (M2 > 0) {
+    if (M2 > 0 && nrhs <= 8) {
+      cgemv_update_kernel<T><<<cdiv_u(M2, 256), 256, 0, c->stream>>>(
+          M2, nrhs, ncols, W + (k0 + ncols) + (size_t)k0 * ld, ld, X + k0, ldx, X + k0 + ncols, ldx);
+      LAUNCH_CHECK();
+    } else if (M2 > 0) {
       dim3 grid(cdiv_u(M2, 64), cdiv_u(nrhs, 64));
       cgemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(M2, nrhs, ncols, W + (k0 + ncols) + (size_t)k0 * ld, ld,
                                                          X + k0, ldx, X + k0 + ncols, ldx);
@@ -863,7 +867,11 @@ static int lu_solve_impl(hprmat_b200_ctx* c, const T* W, const LUState& st, T* X
     dk<<<cdiv_u(nrhs, DCW), NB * DCW, dsm, c->stream>>>(inv + ((size_t)2 * s + 1) * NB * NB, ncols, k0, nullptr, nullptr, nullptr,
                                    nullptr, X, ldx, nrhs, nullptr, 0);
     LAUNCH_CHECK();
-    if (k0 > 0) {
+    if (k0 > 0 && nrhs <= 8) {
+      cgemv_update_kernel<T><<<cdiv_u(k0, 256), 256, 0, c->stream>>>(k0, nrhs, ncols, W + (size_t)k0 * ld, ld,
+                                                                     X + k0, ldx, X, ldx);
+      LAUNCH_CHECK();
+    } else if (k0 > 0) {
       dim3 grid(cdiv_u(k0, 64), cdiv_u(nrhs, 64));
       cgemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(k0, nrhs, ncols, W + (size_t)k0 * ld, ld, X + k0, ldx,
                                                          X, ldx);
