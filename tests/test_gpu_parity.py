@@ -445,6 +445,39 @@ def test_condition_estimate_rmatrix_and_fallback():
         assert abs(c.last_stats["cond_estimate"] / est - 1.0) < 1e-6
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("nch,nr", [(5, 37), (3, 51), (1, 600)])
+def test_odd_and_long_meshes(ctx, precision, nch, nr):
+    """Mesh sizes that are odd, or longer than the assembly's column stride (512): the
+    assembly steps the (channel, point) pair of a column instead of dividing, so these check
+    its wrap-around against the oracle."""
+    w = workloads.production(seed=41 + nr, nch=nch, nr=nr, rmax=20.0, energy=10.0, name=f"mesh{nr}")
+    ref = _oracle_u(w)
+    # at nr = 600 (one channel) C has kappa_2 = 9.4e9 and the oracle's own unrefined zgesv U is
+    # only good to ~8e-10: the reference U here is the oracle's, refined with residuals in
+    # extended precision until it no longer changes
+    mesh = orc.rmat_ini(w.nr, 1, w.rmax)
+    bnd = orc.boundary_values(w.nch, w.lval, w.qk, w.eta, w.rmax)
+    C = orc.assemble(mesh, 1, w.nch, w.lval, w.qk, bnd.xc, w.cpot)
+    bvec = mesh.q2[:, 0].astype(np.complex128)
+    B = orc.surface_rhs(bvec, w.nch)
+    X = np.linalg.solve(C, B)
+    for _ in range(3):
+        r = (B.astype(np.clongdouble) - C.astype(np.clongdouble) @ X.astype(np.clongdouble)).astype(np.complex128)
+        X = X + np.linalg.solve(C, r)
+    u_ref = orc.collision_matrix(orc.extract_r(X, bvec, w.nch) / w.rmax, bnd, w.qk)
+    ctx.set_precision(precision)
+    cu, nopen = ctx.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+    assert nopen == ref.nopen
+    if nopen:
+        oracle_err = _rel(ref.cu, u_ref)
+        # the refined mixed path reaches the refined U; a plain FP64 LU (here and in the oracle)
+        # stops at its rounding level
+        tol = U_TOL if precision == "mixed" else max(U_TOL, 5 * oracle_err)
+        assert _rel(cu[:nopen, :nopen], u_ref) <= tol, (oracle_err, ctx.last_stats)
+    ctx.set_precision("mixed")
+
+
 # ---------------------------------------------------------------- failures
 def test_singular_matrix_reports_status(ctx):
     n = 300
