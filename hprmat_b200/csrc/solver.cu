@@ -92,6 +92,11 @@ struct DevBuf {
 
 static constexpr int kSwapStride = 3 * kMaxNB + 4;  // ints per step in the swap store
 
+// Threads per CTA of the FGMRES Arnoldi step (one CTA per right-hand side, 128 CTAs in a
+// production solve): the step streams the basis, so more warps per SM keep more loads in
+// flight.
+constexpr int kArnoldiNT = 512;
+
 // Status-block slots beyond the factorisation's own (SW_*; int offsets into the 64-int block):
 // the largest |re| + |im| of the matrix about to be factorised (float bits, written by the
 // assembly / conversion kernels for the pivot-growth check) and ||C||_1 (double bits, 8-byte
@@ -1180,7 +1185,7 @@ static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W3
       LAUNCH_CHECK();
       // V_{j+1} = -C Z_j: FGMRES runs on the operator -C, so the correction is subtracted
       TRY(apply_residual(c, op, Z + (size_t)j * vstride, ldv, nrhs, V + (size_t)(j + 1) * vstride, ldv, false));
-      gmres_arnoldi_kernel<256><<<nrhs, 256, 0, c->stream>>>(gs, j);
+      gmres_arnoldi_kernel<kArnoldiNT><<<nrhs, kArnoldiNT, 0, c->stream>>>(gs, j);
       LAUNCH_CHECK();
       jdone = j + 1;
       // residual estimate of the cycle (worst column) from the Givens-rotated right side
