@@ -55,7 +55,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lcublas"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

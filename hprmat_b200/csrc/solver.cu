@@ -1,5 +1,6 @@
 // Host runtime of the B200 R-matrix solver: context, mesh, LU / solve drivers, FP64
 // refinement and the C ABI declared in include/hprmat_b200.h.
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -134,6 +135,7 @@ struct hprmat_b200_ctx {
   DevBuf wfx, wfz, wfc, wfcf;
   DevBuf fpbuf;  // potential fingerprint (opts.reuse_factors)
   DevBuf cond_v;  // condition estimate: one right-hand side (opts.estimate_condition)
+  cublasHandle_t blas = nullptr;  // ZGEMM of the FP64 LU's trailing update (created on first use)
   // tensor-core operand views of the current factorisation (mixed path)
   TcOperand op_lu, op_bop, op_rhs, op_linv;
   long lup_ld = 0, lup_plane = 0, rop_plane = 0;
@@ -520,6 +522,27 @@ static int lu_solve_wave(hprmat_b200_ctx* c, const LUState& st, float2* X, long 
   return HPRMAT_B200_OK;
 }
 
+// C[M x N] -= A[M x K] B[K x N] in complex FP64 (column-major) by cuBLAS ZGEMM on the
+// context's stream; the handle is created on first use and kept by the context.
+static int zgemm_update(hprmat_b200_ctx* c, int M, int N, int K, const double2* A, long lda, const double2* B,
+                        long ldb, double2* C, long ldc) {
+  if (!c->blas) {
+    const cublasStatus_t e = cublasCreate(&c->blas);
+    if (e != CUBLAS_STATUS_SUCCESS) {
+      c->blas = nullptr;
+      return fail(HPRMAT_B200_ERR_CUDA, "cublasCreate failed (status %d)", (int)e);
+    }
+  }
+  cublasStatus_t e = cublasSetStream(c->blas, c->stream);
+  const cuDoubleComplex minus_one = make_cuDoubleComplex(-1.0, 0.0), one = make_cuDoubleComplex(1.0, 0.0);
+  if (e == CUBLAS_STATUS_SUCCESS)
+    e = cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, N, K, &minus_one,
+                    reinterpret_cast<const cuDoubleComplex*>(A), (int)lda, reinterpret_cast<const cuDoubleComplex*>(B),
+                    (int)ldb, &one, reinterpret_cast<cuDoubleComplex*>(C), (int)ldc);
+  if (e != CUBLAS_STATUS_SUCCESS) return fail(HPRMAT_B200_ERR_CUDA, "cublasZgemm failed (status %d)", (int)e);
+  return HPRMAT_B200_OK;
+}
+
 template <typename T, int NB>
 static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUState& st) {
   constexpr int NT = 256;
@@ -642,6 +665,12 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
         c->ev_flops.push_back(8.0 * (double)M2 * (double)M2 * (double)NB);
         c->ev_used += 2;
       }
+    } else if constexpr (std::is_same<T, double2>::value) {
+      // FP64 path: the trailing update is a plain complex GEMM, C -= A B, done by cuBLAS ZGEMM
+      // (the LU's own work -- panels, pivoting, U12 -- stays in this library's kernels)
+      if (M2 > 0) TRY(zgemm_update(c, M2, M2, ncols, W + (k0 + ncols) + (size_t)k0 * ld, ld,
+                                   W + k0 + (size_t)(k0 + ncols) * ld, ld,
+                                   W + (k0 + ncols) + (size_t)(k0 + ncols) * ld, ld));
     } else {
       dim3 grid(cdiv_u(M2, 64), cdiv_u(M2, 64));
       cgemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(M2, M2, ncols, W + (k0 + ncols) + (size_t)k0 * ld, ld,
@@ -2069,6 +2098,7 @@ int hprmat_b200_destroy(hprmat_b200_ctx* c) {
   c->scan_workers.clear();
   c->scan_cpot.clear();
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
+  if (c->blas) cublasDestroy(c->blas);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->h_norms) cudaFreeHost(c->h_norms);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
