@@ -890,10 +890,15 @@ static int lu_solve_impl(hprmat_b200_ctx* c, const T* W, const LUState& st, T* X
           M2, nrhs, ncols, W + (k0 + ncols) + (size_t)k0 * ld, ld, X + k0, ldx, X + k0 + ncols, ldx);
       LAUNCH_CHECK();
     } else if (M2 > 0) {
-      dim3 grid(cdiv_u(M2, 64), cdiv_u(nrhs, 64));
-      cgemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(M2, nrhs, ncols, W + (k0 + ncols) + (size_t)k0 * ld, ld,
-                                                         X + k0, ldx, X + k0 + ncols, ldx);
-      LAUNCH_CHECK();
+      if constexpr (std::is_same<T, double2>::value) {
+        TRY(zgemm_update(c, M2, nrhs, ncols, W + (k0 + ncols) + (size_t)k0 * ld, ld, X + k0, ldx, X + k0 + ncols,
+                         ldx));
+      } else {
+        dim3 grid(cdiv_u(M2, 64), cdiv_u(nrhs, 64));
+        cgemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(M2, nrhs, ncols, W + (k0 + ncols) + (size_t)k0 * ld, ld,
+                                                           X + k0, ldx, X + k0 + ncols, ldx);
+        LAUNCH_CHECK();
+      }
     }
   }
   for (int s = st.nsteps - 1; s >= 0; --s) {
@@ -906,10 +911,14 @@ static int lu_solve_impl(hprmat_b200_ctx* c, const T* W, const LUState& st, T* X
                                                                      X + k0, ldx, X, ldx);
       LAUNCH_CHECK();
     } else if (k0 > 0) {
-      dim3 grid(cdiv_u(k0, 64), cdiv_u(nrhs, 64));
-      cgemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(k0, nrhs, ncols, W + (size_t)k0 * ld, ld, X + k0, ldx,
-                                                         X, ldx);
-      LAUNCH_CHECK();
+      if constexpr (std::is_same<T, double2>::value) {
+        TRY(zgemm_update(c, k0, nrhs, ncols, W + (size_t)k0 * ld, ld, X + k0, ldx, X, ldx));
+      } else {
+        dim3 grid(cdiv_u(k0, 64), cdiv_u(nrhs, 64));
+        cgemm_update_kernel<T><<<grid, 256, 0, c->stream>>>(k0, nrhs, ncols, W + (size_t)k0 * ld, ld, X + k0, ldx,
+                                                           X, ldx);
+        LAUNCH_CHECK();
+      }
     }
   }
   return HPRMAT_B200_OK;
