@@ -1070,9 +1070,8 @@ static int apply_residual(hprmat_b200_ctx* c, const Operator& op, const double2*
       HPR_CUDA_TRY(cudaMemset2DAsync(out, ldo * sizeof(double2), 0, (size_t)N * sizeof(double2), ncol, c->stream));
     }
     LAUNCH_CHECK();
-    dim3 grid(cdiv_u(N, 64), cdiv_u(ncol, 64));
-    cgemm_update_kernel<double2><<<grid, 256, 0, c->stream>>>(N, ncol, N, op.A, op.lda, X, ldx, out, ldo);
-    LAUNCH_CHECK();
+    // dense operator (solve_linear, non-local potentials): a plain FP64 GEMM, by ZGEMM
+    TRY(zgemm_update(c, N, ncol, N, op.A, op.lda, X, ldx, out, ldo));
   }
   return HPRMAT_B200_OK;
 }
