@@ -179,7 +179,7 @@ class Context:
         # the library writes each U column-major (Fortran) into its (nch, nch) slot
         return [(np.ascontiguousarray(cu.transpose(0, 2, 1)), nopen, status) for cu, nopen, status in out]
 
-    TUNE_KEYS = ("N", "nb", "panel_cluster", "panel_rpc_min", "wave_sb", "gmres_m")
+    TUNE_KEYS = ("N", "nb", "panel_cluster", "panel_rpc_min", "wave_sb", "gmres_m", "tc_grid")
 
     def scan_autotune(self, blocks, rmax, nr, nworkers=0):
         """Autotune the scan's per-order settings on these blocks (hprmat_b200_scan_autotune);
@@ -197,14 +197,15 @@ class Context:
     def scan_tune_table(self):
         """The autotuner's rows as dicts (keys TUNE_KEYS and the trial time ``ms``)."""
         n = self._lib.hprmat_b200_scan_tune_get(self._h, None, None, 0)
-        rows = np.zeros((max(n, 1), 6), np.int32)
+        rows = np.zeros((max(n, 1), len(self.TUNE_KEYS)), np.int32)
         ms = np.zeros(max(n, 1))
         self._lib.hprmat_b200_scan_tune_get(self._h, _iptr(rows), _dptr(ms), n)
         return [dict(zip(self.TUNE_KEYS, map(int, rows[i])), ms=float(ms[i])) for i in range(n)]
 
     def set_scan_tune_table(self, table):
         """Load a table (rows as ``scan_tune_table`` returns them, e.g. from a JSON cache)."""
-        rows = np.array([[int(r[k]) for k in self.TUNE_KEYS] for r in table], np.int32).reshape(-1, 6)
+        rows = np.array([[int(r.get(k, 0)) for k in self.TUNE_KEYS] for r in table], np.int32).reshape(
+            -1, len(self.TUNE_KEYS))
         nat.check(self._lib.hprmat_b200_scan_tune_set(self._h, _iptr(np.ascontiguousarray(rows)), len(rows)))
 
     @staticmethod

@@ -110,9 +110,10 @@ constexpr int kStatusCopy = 44;
 // One row of the scan autotuner's table: the settings chosen for the units of order N, and the
 // time of the tuned trial (all workers solving one energy of order N at once).
 struct ScanTune {
-  int N, nb, cluster, rpc_min, sb, gmres_m;
+  int N, nb, cluster, rpc_min, sb, gmres_m, tc_grid;
   double ms;
 };
+constexpr int kTuneInts = 7;  // ints per row of the public table
 
 struct hprmat_b200_ctx {
   int device = 0;
@@ -2404,6 +2405,7 @@ static int scan_workers_ready(hprmat_b200_ctx* c, int nworkers, int nr, double r
     w->panel_cluster = c->panel_cluster;
     w->panel_rpc_min = c->panel_rpc_min;
     w->gmres_m = c->gmres_m;
+    w->tcplan.max_grid = c->tcplan.max_grid;
     w->reuse_max_inner = c->reuse_max_inner;
     w->lu_held = false;
     TRY(hprmat_b200_rmat_ini(w, nr, 1, rmax, zrma.data()));
@@ -2413,6 +2415,7 @@ static int scan_workers_ready(hprmat_b200_ctx* c, int nworkers, int nr, double r
 
 // Settings of a worker for one unit: the row t, or the context's own settings (t null).
 static void scan_apply(hprmat_b200_ctx* w, const hprmat_b200_ctx* c, const ScanTune* t) {
+  w->tcplan.max_grid = t ? t->tc_grid : c->tcplan.max_grid;
   w->opts.panel_nb = t ? t->nb : c->opts.panel_nb;
   w->panel_cluster = t ? t->cluster != 0 : c->panel_cluster;
   w->panel_rpc_min = t ? t->rpc_min : c->panel_rpc_min;
@@ -2569,7 +2572,7 @@ int hprmat_b200_scan_autotune(hprmat_b200_ctx* c, int nblocks, const hprmat_b200
     done.push_back(N);
     const std::vector<int> order = scan_energy_order(B);
     ScanTune cur{(int)N, c->opts.panel_nb > 0 ? c->opts.panel_nb : 128, c->panel_cluster ? 1 : 0, c->panel_rpc_min,
-                 c->wave_sb, c->gmres_m, 0.0};
+                 c->wave_sb, c->gmres_m, c->tcplan.max_grid, 0.0};
     // a representative energy whose solve succeeds: the middle one, else the first or last
     int e = -1;
     double best = 0.0;
@@ -2625,6 +2628,12 @@ int hprmat_b200_scan_autotune(hprmat_b200_ctx* c, int nblocks, const hprmat_b200
       t.gmres_m = v;
       TRY(consider(t));
     }
+    for (const int v : {0, c->nsm / 2, c->nsm / 4}) {  // trailing-update CTAs: all SMs, half, a quarter
+      if (v == cur.tc_grid) continue;
+      ScanTune t = cur;
+      t.tc_grid = v;
+      TRY(consider(t));
+    }
     cur.ms = best;
     table.push_back(cur);
   }
@@ -2641,13 +2650,14 @@ int hprmat_b200_scan_tune_get(hprmat_b200_ctx* c, int* rows, double* ms, int max
   for (int i = 0; i < m; ++i) {
     const ScanTune& t = c->scan_tune[i];
     if (rows) {
-      int* r = rows + (size_t)6 * i;
+      int* r = rows + (size_t)kTuneInts * i;
       r[0] = t.N;
       r[1] = t.nb;
       r[2] = t.cluster;
       r[3] = t.rpc_min;
       r[4] = t.sb;
       r[5] = t.gmres_m;
+      r[6] = t.tc_grid;
     }
     if (ms) ms[i] = t.ms;
   }
@@ -2659,12 +2669,12 @@ int hprmat_b200_scan_tune_set(hprmat_b200_ctx* c, const int* rows, int n) {
   if (n < 0 || (n > 0 && !rows)) return fail(HPRMAT_B200_ERR_ARG, "scan_tune_set: invalid arguments");
   std::vector<ScanTune> table;
   for (int i = 0; i < n; ++i) {
-    const int* r = rows + (size_t)6 * i;
+    const int* r = rows + (size_t)kTuneInts * i;
     const bool ok = r[0] > 0 && (r[1] == 16 || r[1] == 32 || r[1] == 64 || r[1] == 128) && (r[2] == 0 || r[2] == 1) &&
                     r[3] >= 1 && (r[4] == 0 || r[4] == 1 || r[4] == 2 || r[4] == 4) && r[5] >= 1 &&
-                    r[5] <= kGmresMaxM;
+                    r[5] <= kGmresMaxM && r[6] >= 0;
     if (!ok) return fail(HPRMAT_B200_ERR_ARG, "scan_tune_set: invalid row %d", i);
-    table.push_back(ScanTune{r[0], r[1], r[2], r[3], r[4], r[5], 0.0});
+    table.push_back(ScanTune{r[0], r[1], r[2], r[3], r[4], r[5], r[6], 0.0});
   }
   c->scan_tune = table;
   return HPRMAT_B200_OK;
@@ -3110,6 +3120,11 @@ int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* c, const char* key, int value) {
   }
   if (strcmp(key, "panel_cluster") == 0) {
     c->panel_cluster = value != 0;
+    return HPRMAT_B200_OK;
+  }
+  if (strcmp(key, "tc_grid") == 0) {
+    if (value < 0) return fail(HPRMAT_B200_ERR_ARG, "tc_grid must be >= 0");
+    c->tcplan.max_grid = value;
     return HPRMAT_B200_OK;
   }
   if (strcmp(key, "growth_limit_exp") == 0) {

@@ -318,13 +318,14 @@ int tc_update(TcGemmPlan& p, const TcOperand& A, int a_k0, int a_row0, const TcO
     return -1;
   }
   TcArgs args{a_k0, a_row0, b_k0, b_row0, K / kKC, C, ldc, M, Nc, p.d_err};
+  const int cap = (p.max_grid > 0 && p.max_grid < p.nsm) ? p.max_grid : p.nsm;
   if (bn == 256) {
     const int ntiles = ((M + kBM - 1) / kBM) * ((Nc + 255) / 256);
-    const int grid = ntiles < p.nsm ? ntiles : p.nsm;
+    const int grid = ntiles < cap ? ntiles : cap;
     tc_update_kernel<256><<<grid, kThreads, TileCfg<256>::kSmemBytes, s>>>(A.map, B.map, args);
   } else if (bn == 128) {
     const int ntiles = ((M + kBM - 1) / kBM) * ((Nc + 127) / 128);
-    const int grid = ntiles < p.nsm ? ntiles : p.nsm;
+    const int grid = ntiles < cap ? ntiles : cap;
     tc_update_kernel<128><<<grid, kThreads, TileCfg<128>::kSmemBytes, s>>>(A.map, B.map, args);
   } else {
     set_last_error_msg("tensor-core update: bn must be 128 or 256");

@@ -12,6 +12,8 @@ struct TcGemmPlan {
   int nsm = 0;
   void* encode = nullptr;  // cuTensorMapEncodeTiled, fetched through the runtime
   int* d_err = nullptr;    // device word: nonzero if a bounded wait gave up
+  int max_grid = 0;        // most CTAs of a persistent update (0: one per SM); concurrent
+                           // solves (scan workers) leave SMs to each other with a smaller grid
 };
 
 // A TMA view of an operand stored as 4 planes of floats (Re hi, Re lo, Im hi, Im lo of the

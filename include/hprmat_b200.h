@@ -170,7 +170,9 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* ctx, int nblocks, const hprmat_b20
    nworkers worker streams at once -- the load the scan itself puts on the device -- and picks,
    one setting at a time from the context's own, the LU block size (128, 64, 32), the panel
    variant (thread-block cluster or grid), the panel's fewest rows per CTA (16, 32, 64), the
-   solves' super-block size (automatic, 2, 1) and the FGMRES cycle length (12, 8, 16); a change
+   solves' super-block size (automatic, 2, 1), the FGMRES cycle length (12, 8, 16) and the CTAs of
+   the persistent trailing update (one per SM, half, a quarter: concurrent solves share the
+   SMs); a change
    is kept when it is 5% faster than the incumbent twice (against its best trial, then against
    a fresh one).  The resulting table replaces the context's; later scans
    apply each unit's row (units of other orders run with the context's settings).  seconds
@@ -178,13 +180,14 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* ctx, int nblocks, const hprmat_b20
 int hprmat_b200_scan_autotune(hprmat_b200_ctx* ctx, int nblocks, const hprmat_b200_scan_block* blocks, double rmax,
                               int nr, int nworkers, double* seconds);
 
-/* The autotuner's table: up to max rows of 6 ints (N, LU block size, panel cluster 0/1, panel
-   rows per CTA, solve super-block size, FGMRES cycle length) into rows and the tuned trial time
+/* The autotuner's table: up to max rows of 7 ints (N, LU block size, panel cluster 0/1, panel
+   rows per CTA, solve super-block size, FGMRES cycle length, trailing-update CTAs with 0 for one
+   per SM) into rows and the tuned trial time
    in ms into ms (either may be NULL).  Returns the number of rows in the table; -1 for a null
    context. */
 int hprmat_b200_scan_tune_get(hprmat_b200_ctx* ctx, int* rows, double* ms, int max);
 
-/* Replace the table with n rows of 6 ints as above (a table kept from an earlier tuning on the
+/* Replace the table with n rows of 7 ints as above (a table kept from an earlier tuning on the
    same device model); n = 0 clears it. */
 int hprmat_b200_scan_tune_set(hprmat_b200_ctx* ctx, const int* rows, int n);
 

@@ -42,6 +42,7 @@ int hprmat_b200_dev_counters(hprmat_b200_ctx* ctx, unsigned long long* launches,
      "panel_rpc_min"  fewest panel rows per CTA (32);
      "panel_cluster"  panels that fit in one cluster of at most 16 CTAs exchange pivots in
                       distributed shared memory (1) or always through global memory (0);
+     "tc_grid"        most CTAs of the persistent trailing update (0: one per SM);
      "growth_limit_exp" mixed path: an FP32 factorisation whose pivot growth exceeds 10^value
                       (-30..30) is replaced by the FP64 one (6);
      "gmres_m"        longest FGMRES cycle, <= 16 (12);

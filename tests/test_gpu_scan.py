@@ -133,7 +133,7 @@ def test_scan_autotune_table_and_parity():
     for r in table:
         assert r["nb"] in (32, 64, 128) and r["panel_cluster"] in (0, 1)
         assert r["panel_rpc_min"] in (16, 32, 64) and r["wave_sb"] in (0, 1, 2)
-        assert r["gmres_m"] in (8, 12, 16) and r["ms"] > 0.0
+        assert r["gmres_m"] in (8, 12, 16) and r["tc_grid"] >= 0 and r["ms"] > 0.0
     res = ctx.rmatrix_scan(args, 20.0, 60, nworkers=3)
     mesh = orc.rmat_ini(60, 1, 20.0)
     for (w, qk, eta), (cu, nopen, status) in zip(blocks, res):
@@ -142,8 +142,9 @@ def test_scan_autotune_table_and_parity():
             assert status[e] == 0 and nopen[e] == ref.nopen
             no = ref.nopen
             assert np.linalg.norm(cu[e, :no, :no] - ref.cu) / np.linalg.norm(ref.cu) <= U_TOL
-    # a table forcing 64-column blocks, grid panels and short cycles for every order still agrees
-    forced = [dict(N=w.nch * 60, nb=64, panel_cluster=0, panel_rpc_min=16, wave_sb=1, gmres_m=8)
+    # a table forcing 64-column blocks, grid panels, short cycles and a trailing update on 37
+    # CTAs for every order still agrees
+    forced = [dict(N=w.nch * 60, nb=64, panel_cluster=0, panel_rpc_min=16, wave_sb=1, gmres_m=8, tc_grid=37)
               for w, _q, _e in blocks]
     ctx.set_scan_tune_table(forced)
     assert [{k: r[k] for k in api.Context.TUNE_KEYS} for r in ctx.scan_tune_table()] == forced
