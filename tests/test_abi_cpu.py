@@ -155,3 +155,43 @@ def test_wf_print_closed_channel_tail():
         ref = orc.wf_print(nv, lval, qk, eta, rmax, mesh, cu, no, cf, iv, 1, 16, 1.0)
         got = api.wf_print(lval, qk, eta, rmax, nr, ns, cu, no, cf, mesh.zrma, iv, 1, 16, 1.0)
         np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-14 * max(np.abs(ref).max(), 1e-300))
+
+
+def test_struct_mirrors_match_the_header(tmp_path):
+    """The ctypes mirrors of hprmat_b200_opts / hprmat_b200_stats / hprmat_b200_scan_block have
+    the C header's size and field offsets (compiled with gcc against include/hprmat_b200.h)."""
+    mirrors = {"hprmat_b200_opts": nat.Opts, "hprmat_b200_stats": nat.Stats, "hprmat_b200_scan_block": nat.ScanBlock}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "hprmat_b200.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _t in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {}
+    for ln in out:
+        if ln.strip():
+            cname, field, val = ln.split()
+            got[(cname, field)] = int(val)
+    for cname, py in mirrors.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for fname, _t in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_scan_blocks_are_checked_on_the_host():
+    """Scan inputs are validated and laid out before any device call."""
+    w = workloads.small()
+    qk = np.tile(np.asarray(w.qk, float), (3, 1))
+    eta = np.tile(np.asarray(w.eta, float), (3, 1))
+    _keep, arr, out = api.Context._scan_blocks([(w.lval, w.cpot, qk, eta)])
+    assert arr[0].nch == w.nch and arr[0].nenergies == 3 and arr[0].ncp1 == w.cpot.shape[0]
+    assert out[0][0].shape == (3, w.nch, w.nch)
+    with pytest.raises(ValueError):
+        api.Context._scan_blocks([(w.lval, w.cpot, qk[:, :-1], eta)])
+    with pytest.raises(ValueError):
+        api.Context._scan_blocks([(w.lval[:-1], w.cpot, qk, eta)])
