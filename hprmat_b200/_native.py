@@ -40,7 +40,7 @@ EXPORTED = (
     "hprmat_b200_dev_tc_update", "hprmat_b200_dev_split_planes", "hprmat_b200_dev_set_profile",
     "hprmat_b200_dev_counters", "hprmat_b200_dev_wave_trace", "hprmat_b200_dev_wave_trace_read",
     "hprmat_b200_dev_panel_trace_read", "hprmat_b200_dev_set_tuning", "hprmat_b200_dev_mesh",
-    "hprmat_b200_dev_factorizations",
+    "hprmat_b200_dev_factorizations", "hprmat_b200_dev_wait_probe",
 )
 
 
@@ -138,6 +138,7 @@ def load():
         "hprmat_b200_dev_set_tuning": (I, [P, ctypes.c_char_p, I]),
         "hprmat_b200_dev_mesh": (I, [I, I, D, DP, DP, DP, DP, DP]),
         "hprmat_b200_dev_factorizations": (ctypes.c_longlong, [P, I]),
+        "hprmat_b200_dev_wait_probe": (I, [P, I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

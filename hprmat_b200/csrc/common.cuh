@@ -137,8 +137,10 @@ __device__ inline bool grid_barrier(int* counter, int* timeout_flag, unsigned ta
 __device__ inline void grid_arrive(int* counter) {
   asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(counter) : "memory");
 }
-// All threads; false when the bounded wait gave up (the caller must return).
-__device__ inline bool grid_wait(int* counter, int* timeout_flag, unsigned target, int site) {
+// All threads; false when the bounded wait gave up (the caller must return): after `limit`
+// polls (checked every 4096) it records `site` in *timeout_flag.
+__device__ inline bool grid_wait(int* counter, int* timeout_flag, unsigned target, int site,
+                                 unsigned limit = (1u << 26)) {
   __shared__ int s_ok_w;
   if (threadIdx.x == 0) {
     int ok = 1;
@@ -150,7 +152,7 @@ __device__ inline bool grid_wait(int* counter, int* timeout_flag, unsigned targe
         int tf;
         asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(tf) : "l"(timeout_flag) : "memory");
         if (tf != 0) { ok = 0; break; }
-        if (spins >= (1u << 26)) {
+        if (spins >= limit) {
           atomicExch(timeout_flag, site);
           ok = 0;
           break;

@@ -523,6 +523,12 @@ static int lu_solve_wave(hprmat_b200_ctx* c, const LUState& st, float2* X, long 
   return HPRMAT_B200_OK;
 }
 
+// One CTA waits, with a limit of `limit` polls, on a counter that nothing increments: the
+// bounded wait of the panel's grid barrier, run out on purpose to check the failure report.
+__global__ void wait_probe_kernel(int* counter, int* timeout_flag, unsigned limit) {
+  grid_wait(counter, timeout_flag, 1u, 99, limit);
+}
+
 // C[M x N] -= A[M x K] B[K x N] in complex FP64 (column-major) by cuBLAS ZGEMM on the
 // context's stream; the handle is created on first use and kept by the context.
 static int zgemm_update(hprmat_b200_ctx* c, int M, int N, int K, const double2* A, long lda, const double2* B,
@@ -2640,6 +2646,22 @@ int hprmat_b200_scan_autotune(hprmat_b200_ctx* c, int nblocks, const hprmat_b200
   for (int i = 0; i < nworkers; ++i) scan_apply(c->scan_workers[i], c, nullptr);
   c->scan_tune = table;
   if (seconds) *seconds = std::chrono::duration<double>(Clock::now() - t0).count();
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_dev_wait_probe(hprmat_b200_ctx* c, int spins) {
+  TRY(check_ctx(c));
+  if (spins < 4096 || spins > (1 << 24)) return fail(HPRMAT_B200_ERR_ARG, "wait_probe: spins must be in 4096..2^24");
+  int* status = c->status.as<int>();
+  HPR_CUDA_TRY(cudaMemsetAsync(status, 0, SW_COUNT * sizeof(int), c->stream));
+  wait_probe_kernel<<<1, 32, 0, c->stream>>>(status + SW_BARRIER, status + SW_TIMEOUT, (unsigned)spins);
+  LAUNCH_CHECK();
+  HPR_CUDA_TRY(cudaMemcpyAsync(c->h_status, status, SW_COUNT * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const int site = c->h_status[SW_TIMEOUT];
+  HPR_CUDA_TRY(cudaMemsetAsync(status, 0, SW_COUNT * sizeof(int), c->stream));  // leave the block clean
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (site != 0) return fail(HPRMAT_B200_ERR_TIMEOUT, "wait_probe: bounded wait gave up as designed (site %d)", site);
   return HPRMAT_B200_OK;
 }
 

@@ -52,6 +52,12 @@ int hprmat_b200_dev_counters(hprmat_b200_ctx* ctx, unsigned long long* launches,
                       factors needed more FGMRES iterations than this (24). */
 int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* ctx, const char* key, int value);
 
+/* Failure-path check: one CTA waits, with a limit of `spins` polls (4096 .. 2^24), on a device
+   counter that nothing increments -- the bounded wait of the panel's grid barrier.  Returns
+   HPRMAT_B200_ERR_TIMEOUT with the site in the error message when the wait gave up, as it is
+   meant to (the context stays usable); any other value is a failure of the check. */
+int hprmat_b200_dev_wait_probe(hprmat_b200_ctx* ctx, int spins);
+
 /* LU factorisations run on the context and its scan workers since the last reset (opts.reuse_factors
    makes energy scans run fewer); reset != 0 clears the count after reading.  -1 for a null
    context. */

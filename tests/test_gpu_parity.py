@@ -491,6 +491,21 @@ def test_singular_matrix_reports_status(ctx):
         assert ctx.last_stats["info"] == 18
 
 
+def test_bounded_wait_reports_timeout_and_context_survives(ctx):
+    """The panel barrier's bounded wait, run out on purpose on a counter nothing increments
+    (2^14 polls, ~10 ms): the host reads HPRMAT_B200_ERR_TIMEOUT with the site, and the same
+    context then solves correctly."""
+    lib = nat.load()
+    assert lib.hprmat_b200_dev_wait_probe(ctx._h, 1 << 14) == nat.ERR_TIMEOUT
+    assert b"site 99" in lib.hprmat_b200_last_error()
+    assert lib.hprmat_b200_dev_wait_probe(ctx._h, 100) == nat.ERR_ARG
+    w = workloads.small()
+    ref = _oracle_u(w)
+    ctx.set_precision("mixed")
+    cu, nopen = ctx.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+    assert _rel(cu[:nopen, :nopen], ref.cu) <= U_TOL
+
+
 def test_refinement_cap_reports_not_converged(ctx):
     """max_refine = 0 with a tolerance the FP32-accurate factors cannot reach."""
     w = workloads.production(nch=20)
