@@ -19,6 +19,7 @@ ERR_TIMEOUT = -4
 ERR_UNSUPPORTED = -5
 ERR_NODEVICE = -6
 SINGULAR = 1
+PIVOT_GROWTH = 2
 NOT_CONVERGED = 99
 
 PREC_FP64 = 0
@@ -47,7 +48,8 @@ EXPORTED = (
 class Opts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("max_refine", ctypes.c_int), ("tol", ctypes.c_double),
                 ("surface_tol", ctypes.c_double), ("panel_nb", ctypes.c_int), ("reuse_factors", ctypes.c_int),
-                ("estimate_condition", ctypes.c_int), ("reserved", ctypes.c_int * 2)]
+                ("estimate_condition", ctypes.c_int), ("growth_error", ctypes.c_int),
+                ("reserved", ctypes.c_int * 1)]
 
 
 class Stats(ctypes.Structure):

@@ -1429,6 +1429,9 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
       // on CGETRF info != 0, src/rmat_solvers.F90:233-236)
       TRY(pivot_growth(c, &stats->pivot_growth));
       if (c->h_status[SW_INFO] != 0 || !(stats->pivot_growth <= c->growth_limit)) {
+        if (c->h_status[SW_INFO] == 0 && c->opts.growth_error)
+          return fail(HPRMAT_B200_PIVOT_GROWTH, "C(E) of interval %d: pivot growth %.3g of the FP32 factors above %.3g",
+                      is + 1, stats->pivot_growth, c->growth_limit);
         stats->fp64_fallback = 1;
         HPR_CUDA_TRY(cudaMemsetAsync(d_amax, 0, sizeof(unsigned), c->stream));
       }
@@ -1940,6 +1943,8 @@ static int solve_dense_core(hprmat_b200_ctx* c, const double2* dA, double2* dB, 
     // an exact zero FP32 pivot or a pivot growth beyond what the FP32 factors can carry through
     // the refinement: factorise A in FP64 (Type 2's ZGESV fallback, src/rmat_solvers.F90:233-236)
     fallback = c->h_status[SW_INFO] != 0 || !(rho <= c->growth_limit);
+    if (fallback && c->h_status[SW_INFO] == 0 && c->opts.growth_error)
+      return fail(HPRMAT_B200_PIVOT_GROWTH, "pivot growth %.3g of the FP32 factors above %.3g", rho, c->growth_limit);
     if (stats) stats->fp64_fallback = fallback;
   }
   if (mixed && !fallback) {
@@ -3280,6 +3285,7 @@ const char* hprmat_b200_status_string(int s) {
     case HPRMAT_B200_ERR_UNSUPPORTED: return "unsupported input";
     case HPRMAT_B200_ERR_NODEVICE: return "no usable sm_100 device";
     case HPRMAT_B200_SINGULAR: return "singular matrix";
+    case HPRMAT_B200_PIVOT_GROWTH: return "pivot growth exceeded";
     case HPRMAT_B200_NOT_CONVERGED: return "refinement did not converge";
   }
   return "unknown status";

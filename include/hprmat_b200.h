@@ -30,6 +30,8 @@ extern "C" {
 #define HPRMAT_B200_ERR_UNSUPPORTED -5   /* input outside what this build handles */
 #define HPRMAT_B200_ERR_NODEVICE    -6   /* no usable sm_100 device */
 #define HPRMAT_B200_SINGULAR         1   /* exactly zero pivot; stats.info = its 1-based column */
+#define HPRMAT_B200_PIVOT_GROWTH     2   /* mixed path with opts.growth_error: the FP32 factors'
+                                            pivot growth (stats.pivot_growth) exceeded the limit */
 #define HPRMAT_B200_NOT_CONVERGED   99   /* refinement stopped above tol (as info=99 in
                                             src/cusolver_interface.cu:1577-1589) */
 
@@ -65,7 +67,11 @@ typedef struct {
                              the matrix (stats.cond_estimate; LAPACK ZGECON's quantity, by the
                              Hager-Higham estimator on the factors: ~11 extra solves with one
                              right-hand side).  Default 0. */
-  int reserved[2];
+  int growth_error;       /* mixed path: when nonzero, FP32 factors whose pivot growth exceeds the
+                             limit (10^6) make the call return HPRMAT_B200_PIVOT_GROWTH instead of
+                             factorising in FP64 (an exact zero FP32 pivot still falls back, as
+                             the reference's Type 2 does).  Default 0: fall back. */
+  int reserved[1];
 } hprmat_b200_opts;
 
 typedef struct {

@@ -50,6 +50,8 @@ def test_default_opts_and_status_strings():
     assert o.panel_nb == 0
     assert lib.hprmat_b200_status_string(nat.SINGULAR) == b"singular matrix"
     assert lib.hprmat_b200_status_string(nat.NOT_CONVERGED) == b"refinement did not converge"
+    assert lib.hprmat_b200_status_string(nat.PIVOT_GROWTH) == b"pivot growth exceeded"
+    assert o.estimate_condition == 0 and o.growth_error == 0
 
 
 def test_create_without_device_fails_loudly():

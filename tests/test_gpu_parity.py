@@ -375,6 +375,24 @@ def test_pivot_growth_limit_is_the_trigger():
         assert lib.hprmat_b200_dev_set_tuning(c._h, b"growth_limit_exp", 31) == nat.ERR_ARG
 
 
+def test_pivot_growth_error_on_request():
+    """opts.growth_error: the same growth matrix makes the mixed solve return
+    HPRMAT_B200_PIVOT_GROWTH (with the growth in the stats) instead of factorising in FP64."""
+    import ctypes
+    lib = nat.load()
+    A, Xt = _growth_matrix()
+    with api.Context(precision="mixed") as c:
+        c.opts.growth_error = 1
+        nat.check(lib.hprmat_b200_set_opts(c._h, ctypes.byref(c.opts)))
+        with pytest.raises(nat.HprmatError) as e:
+            c.solve_linear(A, np.asfortranarray(A @ Xt))
+        assert e.value.status == nat.PIVOT_GROWTH
+        assert c.last_stats["pivot_growth"] > 1e6 and c.last_stats["fp64_fallback"] == 0
+        A2, B2 = _diag_dominant(300, 2, 6)
+        X2 = c.solve_linear(A2, B2)
+        assert _rel(X2, np.linalg.solve(A2, B2)) <= 1e-12
+
+
 def test_rmatrix_fp64_fallback_matches_oracle():
     """The R-matrix path's fallback, forced by a growth limit of 10^-30: C(E) factorised in
     FP32, then again in FP64, and U as the oracle's to 1e-10.  The production C(E) itself has
