@@ -455,6 +455,7 @@ def run_sweep(args):
         cu_d, _ = ctx.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
         fp64_ms = ctx.last_stats["ms_total"] - ctx.last_stats["ms_condest"]
         kappa1 = ctx.last_stats["cond_estimate"]
+        condest_ms = ctx.last_stats["ms_condest"]
         diff = float(np.linalg.norm(cu_m[:nopen, :nopen] - cu_d[:nopen, :nopen]) / np.linalg.norm(cu_d[:nopen, :nopen]))
         n = w.n
         rows.append({"N": n, "nch": nch, "nopen": nopen, "ms_per_solve": best, "solves_per_s": 1e3 / best,
@@ -463,7 +464,7 @@ def run_sweep(args):
                      "rel_residual": st["rel_residual"], "residual_floor": st["residual_floor"],
                      "pivot_growth": st["pivot_growth"], "fp64_fallback": st["fp64_fallback"],
                      "u_rel_diff_vs_device_fp64": diff, "device_fp64_ms": fp64_ms,
-                     "mixed_over_fp64": fp64_ms / best, "cond1_estimate": kappa1,
+                     "mixed_over_fp64": fp64_ms / best, "cond1_estimate": kappa1, "cond1_estimate_ms": condest_ms,
                      "tc_update_tflops": tc_flops.value / max(tc_ms.value, 1e-9) / 1e9,
                      "tc_update_share": tc_ms.value / best})
         ctx.close()
