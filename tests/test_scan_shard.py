@@ -98,3 +98,21 @@ def test_two_rank_gloo_sharded_scan_matches_single_process():
         for b in range(len(blocks)):
             np.testing.assert_array_equal(o[1][b], single[b][0])
             np.testing.assert_array_equal(o[2][b], single[b][1])
+
+
+def test_more_ranks_than_units_leaves_some_ranks_empty():
+    """With whole blocks as units and more ranks than blocks, the extra ranks get no unit (and
+    solve nothing), every unit is still on exactly one rank, and a rank's results hold only
+    its own blocks."""
+    b = _blocks()
+    world = len(b) + 2
+    owners = []
+    empty = 0
+    for r in range(world):
+        mine, subs = shard_units(b, NR, r, world, chunk=None)
+        assert len(mine) == len(subs)
+        empty += not mine
+        owners += [u for u, _idx in mine]
+    assert sorted(owners) == list(range(len(b))) and empty == 2
+    res, mine = run_sharded_scan(b, NR, _oracle_solve, rank=world - 1, world=world, gather=False, chunk=None)
+    assert all(r is None for r in res) == (not mine)
