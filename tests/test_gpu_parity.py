@@ -433,6 +433,7 @@ def test_condition_estimate_dense(kappa):
         X = c.solve_linear(A, B)
         est = c.last_stats["cond_estimate"]
         assert exact / 3.0 <= est <= exact * (1 + 1e-6), (est, exact)
+        assert abs(est / orc.cond1_estimate(A) - 1.0) < 1e-6  # the oracle's steps, the same estimate
         assert _rel(X, np.linalg.solve(A, B)) <= 1e-12 * max(1.0, kappa / 1e3)
         A2, B2 = _diag_dominant(500, 2, 4)
         c.solve_linear(A2, B2)
@@ -454,6 +455,7 @@ def test_condition_estimate_rmatrix_and_fallback():
         c.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
         est = c.last_stats["cond_estimate"]
         assert exact / 3.0 <= est <= exact * (1 + 1e-6), (est, exact)
+        assert abs(est / orc.cond1_estimate(C) - 1.0) < 1e-6
         c.set_precision("mixed")
         c.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
         assert c.last_stats["cond_estimate"] == 0.0

@@ -210,3 +210,27 @@ def test_legzo_matches_numpy_gauss_legendre():
         xr, wr = np.polynomial.legendre.leggauss(n)
         assert np.allclose(x, (np.sort(xr) + 1) / 2, rtol=0, atol=1e-14)
         assert np.allclose(w, wr[np.argsort(xr)] / 2, rtol=1e-9, atol=0)
+
+
+def test_oracle_condition_estimate_against_exact():
+    """The oracle's Hager-Higham estimate (the checker of opts.estimate_condition) is a lower
+    bound of numpy's exact 1-norm condition number, within a factor 3, on exact-kappa
+    Householder matrices and the small workload's C(E)."""
+    from hprmat_b200 import workloads
+    n = 300
+    rng = np.random.default_rng(3)
+    v = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    v /= np.linalg.norm(v)
+    H = np.eye(n) - 2 * np.outer(v, v.conj())
+    cases = []
+    for kappa in (1e3, 1e8):
+        d = kappa ** (-np.arange(n) / (n - 1))
+        cases.append((H * d[None, :]) @ H)
+    w = workloads.small()
+    mesh = orc.rmat_ini(w.nr, 1, w.rmax)
+    bnd = orc.boundary_values(w.nch, w.lval, w.qk, w.eta, w.rmax)
+    cases.append(orc.assemble(mesh, 1, w.nch, w.lval, w.qk, bnd.xc, w.cpot))
+    for A in cases:
+        exact = float(np.linalg.cond(A, 1))
+        est = orc.cond1_estimate(A)
+        assert exact / 3.0 <= est <= exact * (1 + 1e-6), (est, exact)
