@@ -22,6 +22,9 @@ SINGULAR = 1
 PIVOT_GROWTH = 2
 NOT_CONVERGED = 99
 
+# HPRMAT_B200_ABI_VERSION of include/hprmat_b200.h: the struct mirrors below follow it
+ABI_VERSION = 101
+
 PREC_FP64 = 0
 PREC_MIXED = 1
 SOLVER_B200 = 7
@@ -146,6 +149,10 @@ def load():
         f = getattr(lib, name)
         f.restype = res
         f.argtypes = args
+    got = lib.hprmat_b200_version()
+    if got != ABI_VERSION:
+        raise ImportError(f"{LIB_PATH} has ABI version {got}, these bindings expect {ABI_VERSION}; rebuild it with "
+                          "`python -m hprmat_b200.build`")
     _lib = lib
     return lib
 

@@ -3293,6 +3293,6 @@ const char* hprmat_b200_status_string(int s) {
 
 const char* hprmat_b200_last_error(void) { return g_last_error.c_str(); }
 
-int hprmat_b200_version(void) { return 100; }
+int hprmat_b200_version(void) { return HPRMAT_B200_ABI_VERSION; }
 
 }  // extern "C"

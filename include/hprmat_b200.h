@@ -314,6 +314,12 @@ int hprmat_b200_boundary(int nch, const int* lval, const double* qk, const doubl
 /* Human-readable status and the last CUDA error message of this thread's calls. */
 const char* hprmat_b200_status_string(int status);
 const char* hprmat_b200_last_error(void);
+
+/* Version of the ABI: the structs above and the entry points' signatures.  It changes whenever
+   one of them does (101: stats gained factorizations, fp64_fallback, pivot_growth,
+   cond_estimate and ms_condest; opts gained estimate_condition and growth_error).  A caller
+   built against another value must be rebuilt. */
+#define HPRMAT_B200_ABI_VERSION 101
 int hprmat_b200_version(void);
 
 #ifdef __cplusplus

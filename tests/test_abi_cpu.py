@@ -36,6 +36,12 @@ def test_library_exports_every_declared_symbol():
         assert re.search(r"\bT " + re.escape(name) + r"$", out, re.M), name
 
 
+def test_abi_version_agrees_across_header_library_and_bindings():
+    src = open(os.path.join(ROOT, "include", "hprmat_b200.h")).read()
+    m = re.search(r"#define HPRMAT_B200_ABI_VERSION (\d+)", src)
+    assert m and int(m.group(1)) == nat.ABI_VERSION == nat.load().hprmat_b200_version()
+
+
 def test_library_is_built_for_sm100a():
     out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", nat.LIB_PATH], capture_output=True,
                          text=True).stdout
