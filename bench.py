@@ -14,8 +14,11 @@ workload (independent solves; no collective on the data path) and the throughput
 sum over ranks, timed as the max over ranks.
 
 `--impl reference` times the reference's own algorithm on the host cores instead: the
-FP64 restatement of HPRMAT's Type 1 path (LAPACK zgesv through OpenBLAS), on a bounded
-sample of the same workload, extrapolated to N = 25600 by the N^3 cost of the LU.
+FP64 restatement of HPRMAT's Type 1 path (assembly, LAPACK zgesv through OpenBLAS on all
+host cores, R, U) on the same N = 25600 workload, after the reference's own warm-up of the
+BLAS thread pool (a 512 x 512 zgetrf, examples/Ex0/benchmark_large.f90:84-98).  One such solve
+takes about a minute on 16 cores, so the arm times as many whole solves as fit in
+--ref-budget-s (at least one) and reports that count with the reason.
 """
 from __future__ import annotations
 
@@ -62,6 +65,9 @@ def parse():
     ap.add_argument("--autotune", type=int, default=0,
                     help="scan: run the scan autotuner (hprmat_b200_scan_autotune) on the scan's blocks before "
                          "the warm-up, outside the timed region")
+    ap.add_argument("--ref-budget-s", type=float, default=150.0,
+                    help="--impl reference and the cpu_baseline leg: wall-time budget of the timed N = 25600 CPU "
+                         "solves; a solve starts only while the projected end stays inside it (at least one runs)")
     ap.add_argument("--tune-cache", default="",
                     help="scan with --autotune: JSON file of the tuned table; loaded when present, written "
                          "after tuning otherwise")
@@ -117,22 +123,6 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ CPU baseline
-def cpu_sample(nch: int = 32, repeats: int = 1):
-    """Time the oracle (Type 1 path restated: assembly, zgesv, R, U) on the production
-    generator at `nch` channels; returns (seconds per solve, N)."""
-    from hprmat_b200 import workloads
-    from oracle import rmatrix_oracle as orc
-    w = workloads.production(nch=nch)
-    mesh = orc.rmat_ini(w.nr, 1, w.rmax)
-    orc.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, mesh, w.cpot)  # warm-up
-    ts = []
-    for _ in range(repeats):
-        t = time.perf_counter()
-        orc.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, mesh, w.cpot)
-        ts.append(time.perf_counter() - t)
-    return min(ts), w.n
-
-
 def cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -140,38 +130,62 @@ def cores():
         return os.cpu_count() or 1
 
 
+def blas_warmup(times: int = 1):
+    """The reference's warm-up of the BLAS thread pool before its timed solves: a 512 x 512
+    zgetrf (examples/Ex0/benchmark_large.f90:84-98)."""
+    from scipy.linalg import lapack
+    ww = np.ones((512, 512), dtype=np.complex128, order="F")
+    ww[np.arange(512), np.arange(512)] = 1024.0
+    for _ in range(max(times, 1)):
+        lapack.zgetrf(ww.copy(order="F"))
+
+
+def cpu_type1_solves(nch: int, max_solves: int, budget_s: float):
+    """Time whole Type 1 solves (the oracle's restatement of src/rmatrix_hp.F90:246-368 with
+    LAPACK zgesv, the call of src/rmat_solvers.F90:127) of the production workload at `nch`
+    channels, one after another, while the projected end of the next solve stays inside
+    budget_s (at least one solve).  Returns (seconds of each solve, N, U of the last solve)."""
+    from hprmat_b200 import workloads
+    from oracle import rmatrix_oracle as orc
+    w = workloads.production(nch=nch)
+    mesh = orc.rmat_ini(w.nr, 1, w.rmax)
+    ts, res = [], None
+    t_begin = time.perf_counter()
+    while len(ts) < max(max_solves, 1):
+        if ts and (time.perf_counter() - t_begin) + max(ts) > budget_s:
+            break
+        t = time.perf_counter()
+        res = orc.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, mesh, w.cpot)
+        ts.append(time.perf_counter() - t)
+    return ts, w.n, res.cu
+
+
 def run_reference(args):
     rank, world, _ = dist_info()
     if rank != 0:
         return 0
     os.environ.setdefault("OPENBLAS_NUM_THREADS", str(cores()))
-    nch = 32  # N = 6400: a few seconds per solve on 8 cores
-    from hprmat_b200 import workloads
-    from oracle import rmatrix_oracle as orc
-    w = workloads.production(nch=nch)
-    mesh = orc.rmat_ini(w.nr, 1, w.rmax)
-    for _ in range(max(args.warmup, 1)):
-        orc.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, mesh, w.cpot)
-    ts = []
-    for _ in range(args.steps):
-        t = time.perf_counter()
-        orc.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, mesh, w.cpot)
-        ts.append(time.perf_counter() - t)
-    t_sample = statistics.median(ts)
-    scale = (N_FULL / w.n) ** 3
-    value = 1.0 / (t_sample * scale)
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    blas_warmup(args.warmup)
+    ts, n, _ = cpu_type1_solves(args.nch, args.steps, args.ref_budget_s)
+    t_mean = sum(ts) / len(ts)
+    value = 1.0 / t_mean
+    nthreads = int(os.environ["OPENBLAS_NUM_THREADS"])
+    why = ("" if len(ts) == args.steps else
+           f"; {len(ts)} of the {args.steps} requested steps timed: one solve takes {t_mean:.0f} s, and the "
+           f"arm stops starting solves once the next would end after its {args.ref_budget_s:.0f} s budget")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_sample * scale * 1e3,
+        "steps": len(ts), "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": t_mean * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
-        "data": "synthetic (seeded production generator)",
+        "data": "synthetic (seeded production generator, hprmat_b200/workloads.py)",
         "config": {"workload": "production: 128 channels x 200 points, N=25600, nrhs=128, E=10 MeV",
-                   "N": N_FULL, "nrhs": 128},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": int(os.environ["OPENBLAS_NUM_THREADS"]),
-                         "kind": "port",
-                         "sample": f"oracle Type 1 path (assembly, OpenBLAS zgesv, R, U) on the production generator "
-                                   f"at {nch} channels (N={w.n}), median of {args.steps} solves "
-                                   f"({t_sample:.2f} s each), scaled by (25600/{w.n})^3"},
+                   "N": n, "nrhs": args.nch},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
+                         "sample": f"oracle Type 1 path (assembly, OpenBLAS zgesv on {nthreads} threads, R, U) on "
+                                   f"the production workload itself (N={n}); warm-up: {args.warmup} x 512^2 "
+                                   f"zgetrf as examples/Ex0/benchmark_large.f90:84-98; wall time per whole solve "
+                                   f"{', '.join(f'{t:.1f}' for t in ts)} s" + why},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -514,6 +528,8 @@ def main():
     lib = nat.load()
 
     def step_device():
+        # a step that stops at max_refine above its tolerance is recorded (status 99), not hidden:
+        # the timed loop keeps every step's status and the run exits nonzero if one did not converge
         return ctx.rmatrix_device(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, d_cpot.data_ptr(), ncp1, ndim,
                                   d_cu.data_ptr(), allow_unconverged=True)
 
@@ -613,8 +629,8 @@ def main():
     tf32_peak = bf16 / 2.0
     achieved = (tc_flops.value / max(tc_n.value, 1)) / ((tc_ms.value / max(tc_n.value, 1)) / 1e3) / 1e12
     # DRAM traffic per launch: ncu measured 1.05x the algorithmic bytes (C read + write and the
-    # operand planes) for the trailing update at N = 12800 (profiles/tc_update_kernel_n12800.md);
-    # scaled here to the mean algorithmic bytes of this solve's trailing updates
+    # operand planes) for the trailing update at N = 12800; scaled here to the mean algorithmic
+    # bytes of this solve's trailing updates
     nb_ = 128
     ms_ = [n_full - (s + 1) * nb_ for s in range((n_full + nb_ - 1) // nb_ - 1)]
     alg_bytes = float(np.mean([16.0 * m * m + 2.0 * m * nb_ * 16.0 for m in ms_])) if ms_ else 0.0
@@ -629,16 +645,27 @@ def main():
                 "note": "achieved counts algorithmic complex-LU flops (8 M^2 nb per update); the tensor cores "
                         "execute 3x that (4 real products x 3 TF32 terms / 4 = 3)"}
 
-    # ---- FP64 device comparators (untimed for the headline)
+    # ---- FP64 device comparators (outside the headline's timed region): each the median of
+    # n_cmp runs timed with CUDA events on the stream the work is ordered on, after a warm-up
     comparators = {}
     if not args.no_comparators:
+        n_cmp = 3
+
+        def event_ms(fn, s):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(dev)
+            a.record(s)
+            fn()
+            b.record(s)
+            torch.cuda.synchronize(dev)
+            return a.elapsed_time(b)
+
         ctx.set_precision("fp64")
-        step_device()  # warm-up: FP64 buffers and the ZGEMM handle, as the mixed steps had theirs
-        torch.cuda.synchronize(dev)
-        t = time.perf_counter()
-        step_device()
-        torch.cuda.synchronize(dev)
-        comparators["own_fp64_lu_solves_per_s"] = 1.0 / (time.perf_counter() - t)
+        step_device()  # warm-up: FP64 buffers, as the mixed steps had theirs
+        ts64 = [event_ms(step_device, stream) for _ in range(n_cmp)]
+        comparators["own_fp64_lu_solves_per_s"] = 1e3 / statistics.median(ts64)
+        comparators["own_fp64_lu_ms"] = ts64
         cu64 = d_cu.cpu().numpy().view(np.complex128).reshape(ndim, ndim, order="F")
         if u_err is not None:
             comparators["own_fp64_lu_u_rel_err"] = float(np.linalg.norm(cu64[:nopen, :nopen] - ref) /
@@ -647,30 +674,38 @@ def main():
         try:
             A = torch.randn(N_FULL, N_FULL, dtype=torch.complex128, device=dev)
             A.diagonal().add_(2.0 * N_FULL)
+            cur = torch.cuda.current_stream(dev)
             torch.linalg.lu_factor(A[:512, :512])
-            torch.cuda.synchronize(dev)
-            t = time.perf_counter()
-            LU, piv = torch.linalg.lu_factor(A)
-            torch.cuda.synchronize(dev)
-            comparators["library_zgetrf_solves_per_s"] = 1.0 / (time.perf_counter() - t)
-            comparators["library_zgetrf"] = "torch.linalg.lu_factor(complex128) (cuSOLVER getrf), factorisation only"
-            del A, LU, piv
+            tsl = []
+            for _ in range(n_cmp):
+                tsl.append(event_ms(lambda: torch.linalg.lu_factor(A), cur))
+            comparators["library_zgetrf_solves_per_s"] = 1e3 / statistics.median(tsl)
+            comparators["library_zgetrf_ms"] = tsl
+            comparators["library_zgetrf"] = ("torch.linalg.lu_factor(complex128) (cuSOLVER getrf), factorisation "
+                                             "only, of a diagonally dominant random matrix of the same order")
+            del A
         except Exception as e:  # noqa: BLE001
             comparators["library_zgetrf_error"] = str(e)[:200]
         best = max(v for k, v in comparators.items() if k.endswith("solves_per_s"))
         comparators["mixed_over_best_fp64"] = value / world / best
+        comparators["timing"] = f"median of {n_cmp} CUDA-event-timed runs after one warm-up"
 
-    # ---- CPU baseline (rank 0, N = 1 only)
+    # ---- CPU baseline (rank 0, N = 1 only): one whole Type 1 solve of this same workload
     cpu = None
     if rank == 0 and world == 1:
         os.environ.setdefault("OPENBLAS_NUM_THREADS", str(cores()))
-        t_s, n_s = cpu_sample(nch=32)
-        scale = (N_FULL / n_s) ** 3
-        cpu = {"value": 1.0 / (t_s * scale), "unit": UNIT, "cores": cores(), "kind": "port",
-               "sample": f"oracle Type 1 path (assembly, OpenBLAS zgesv, R, U) at 32 channels (N={n_s}), "
-                         f"{t_s:.2f} s per solve, scaled by (25600/{n_s})^3"}
+        os.environ.setdefault("OMP_NUM_THREADS", "1")
+        blas_warmup()
+        ts_cpu, n_s, cu_cpu = cpu_type1_solves(args.nch, 1, args.ref_budget_s)
+        cpu = {"value": 1.0 / ts_cpu[0], "unit": UNIT, "cores": int(os.environ["OPENBLAS_NUM_THREADS"]),
+               "kind": "port",
+               "sample": f"one whole oracle Type 1 solve (assembly, OpenBLAS zgesv, R, U) of this workload "
+                         f"(N={n_s}) after a 512^2 zgetrf warm-up: {ts_cpu[0]:.1f} s",
+               "u_rel_err_vs_gpu": float(np.linalg.norm(cu_cpu - cu[:nopen, :nopen]) / np.linalg.norm(cu_cpu))}
 
     last = stats[-1] if stats else st_warm
+    step_status = [int(s_.get("status", -1)) for s_ in stats]
+    not_converged = sum(1 for v in step_status if v == nat.NOT_CONVERGED)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -681,6 +716,10 @@ def main():
                    "l2": "inputs larger than L2 (5.2 GB complex64 working matrix per solve)"},
         "complex_tflops": value * FLOPS_PER_SOLVE / 1e12,
         "u_rel_err": u_err,
+        "step_status": {"ok": sum(1 for v in step_status if v == nat.OK), "not_converged": not_converged,
+                        "refine_steps": [int(s_.get("refine_steps", -1)) for s_ in stats],
+                        "surface_change_max": max((float(s_.get("surface_change", -1)) for s_ in stats),
+                                                  default=None)},
         "refine": {"steps": last.get("refine_steps"), "rel_residual": last.get("rel_residual"),
                    "history": last.get("residual_history"), "ms_factor": last.get("ms_factor"),
                    "ms_refine": last.get("ms_refine"), "pivot_growth": last.get("pivot_growth"),
@@ -699,6 +738,9 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+    if not_converged:
+        print(f"bench: {not_converged} timed step(s) ended with HPRMAT_B200_NOT_CONVERGED", file=sys.stderr)
+        return 1
     return 0
 
 

@@ -40,11 +40,12 @@ EXPORTED = (
     "hprmat_b200_scan_tune_get", "hprmat_b200_scan_tune_set",
     "hprmat_b200_rmatrix_adjoint", "hprmat_b200_rmatrix_wf", "hprmat_b200_rmatrix_wf_device",
     "hprmat_b200_wf_print", "hprmat_b200_rmatrix_full", "hprmat_b200_rmatrix_x", "hprmat_b200_adjoint_from_x",
+    "hprmat_b200_rmatrix_x_device", "hprmat_b200_adjoint_from_x_device",
     # include/hprmat_b200_dev.h
     "hprmat_b200_dev_tc_update", "hprmat_b200_dev_split_planes", "hprmat_b200_dev_set_profile",
     "hprmat_b200_dev_counters", "hprmat_b200_dev_wave_trace", "hprmat_b200_dev_wave_trace_read",
     "hprmat_b200_dev_panel_trace_read", "hprmat_b200_dev_set_tuning", "hprmat_b200_dev_mesh",
-    "hprmat_b200_dev_factorizations", "hprmat_b200_dev_wait_probe",
+    "hprmat_b200_dev_factorizations", "hprmat_b200_dev_wait_probe", "hprmat_b200_dev_binary_version",
 )
 
 
@@ -120,6 +121,8 @@ def load():
         "hprmat_b200_wf_print": (I, [I, IP, DP, DP, D, I, I, DP, I, I, DP, I, I, DP, I, I, I, D, DP]),
         "hprmat_b200_rmatrix_x": (I, [P, I, IP, DP, DP, D, I, DP, I, I, DP, IP, P, ctypes.c_long, SP]),
         "hprmat_b200_adjoint_from_x": (I, [P, I, IP, DP, DP, D, I, DP, I, I, DP, P, ctypes.c_long, DP, DP]),
+        "hprmat_b200_rmatrix_x_device": (I, [P, I, IP, DP, DP, D, I, P, I, I, P, IP, P, ctypes.c_long, SP]),
+        "hprmat_b200_adjoint_from_x_device": (I, [P, I, IP, DP, DP, D, I, P, I, I, DP, P, ctypes.c_long, DP, P]),
         "hprmat_b200_rmatrix_full": (I, [P, I, IP, DP, DP, D, I, I, DP, I, I, DP, IP, I, DP, I, I, I, IP, I, DP,
                                          SP]),
         "hprmat_b200_solve_linear": (I, [P, DP, DP, I, I, SP]),
@@ -144,6 +147,7 @@ def load():
         "hprmat_b200_dev_mesh": (I, [I, I, D, DP, DP, DP, DP, DP]),
         "hprmat_b200_dev_factorizations": (ctypes.c_longlong, [P, I]),
         "hprmat_b200_dev_wait_probe": (I, [P, I]),
+        "hprmat_b200_dev_binary_version": (I, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -34,6 +34,13 @@ def _iptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
 
 
+def _fortran_device(t):
+    """A torch CUDA tensor (d0, d1, d2) as contiguous Fortran-order (column-major) memory: the
+    returned tensor's storage is t laid out with d0 fastest (a copy only when t is not already
+    so), for device pointers handed to the C ABI."""
+    return t.permute(2, 1, 0).contiguous()
+
+
 class Context:
     """One device context (stream + device buffers) of the C library."""
 
@@ -304,6 +311,58 @@ class Context:
         self.last_stats = st.as_dict()
         nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
         return cu, nopen.value, x.T
+
+    def rmatrix_x_device(self, nch, lval, qk, eta, rmax, nr, cpot, allow_unconverged=False):
+        """rmatrix_x with the potential already on this context's device: ``cpot`` is a torch
+        CUDA tensor (ncp1, nch, nch) complex128 (any strides).  Returns (U as a torch CUDA tensor
+        (ndim, ndim), nopen, X as a torch CUDA tensor (nch*nr, nch)); nothing of size cpot or X
+        crosses to the host."""
+        import torch
+        self._ensure_mesh(nr, 1, rmax)
+        lval = np.ascontiguousarray(lval, dtype=np.int32)
+        qk = np.ascontiguousarray(qk, dtype=np.float64)
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        cf = _fortran_device(cpot)
+        ncp1, ndim = cpot.shape[0], cpot.shape[1]
+        n = int(nch) * int(nr)
+        x = torch.empty((int(nch), n), dtype=torch.complex128, device=cpot.device)  # column-major X
+        d_cu = torch.empty((ndim, ndim), dtype=torch.complex128, device=cpot.device)  # column-major U (as U^T)
+        # the library works on the context's own stream: the potential (and its copy) must be complete
+        torch.cuda.current_stream(cpot.device).synchronize()
+        nopen = ctypes.c_int(0)
+        st = Stats()
+        s = self._lib.hprmat_b200_rmatrix_x_device(self._h, int(nch), _iptr(lval), _dptr(qk), _dptr(eta),
+                                                   float(rmax), int(nr), ctypes.c_void_p(cf.data_ptr()), int(ncp1),
+                                                   int(ndim), ctypes.c_void_p(d_cu.data_ptr()), ctypes.byref(nopen),
+                                                   ctypes.c_void_p(x.data_ptr()), n, ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
+        return d_cu.T, nopen.value, x.T
+
+    def adjoint_from_x_device(self, nch, lval, qk, eta, rmax, nr, cpot, cu, x, gu):
+        """adjoint_from_x with cpot, x and the returned gradient as torch CUDA tensors (the
+        gradient has cpot's shape); cu and gu (nopen-sized) may be host or device."""
+        import torch
+        lval = np.ascontiguousarray(lval, dtype=np.int32)
+        qk = np.ascontiguousarray(qk, dtype=np.float64)
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        cf = _fortran_device(cpot)
+        ncp1, ndim = cpot.shape[0], cpot.shape[1]
+        cu_h = np.asfortranarray(cu.detach().cpu().numpy() if torch.is_tensor(cu) else cu, dtype=np.complex128)
+        g = np.zeros((ndim, ndim), dtype=np.complex128, order="F")
+        gu_h = np.asarray(gu.detach().cpu().numpy() if torch.is_tensor(gu) else gu, dtype=np.complex128)
+        g[:gu_h.shape[0], :gu_h.shape[1]] = gu_h
+        xt = x.T
+        assert xt.is_contiguous() and xt.shape == (int(nch), int(nch) * int(nr))
+        grad = torch.empty((ndim, ndim, ncp1), dtype=torch.complex128, device=cpot.device)  # Fortran (ncp1, ndim, ndim)
+        torch.cuda.current_stream(cpot.device).synchronize()
+        s = self._lib.hprmat_b200_adjoint_from_x_device(self._h, int(nch), _iptr(lval), _dptr(qk), _dptr(eta),
+                                                        float(rmax), int(nr), ctypes.c_void_p(cf.data_ptr()),
+                                                        int(ncp1), int(ndim), _dptr(cu_h),
+                                                        ctypes.c_void_p(xt.data_ptr()), int(nch) * int(nr), _dptr(g),
+                                                        ctypes.c_void_p(grad.data_ptr()))
+        nat.check(s)
+        return grad.permute(2, 1, 0)
 
     def adjoint_from_x(self, nch, lval, qk, eta, rmax, nr, cpot, cu, x, gu):
         """Potential gradient of a real loss from the forward solution ``x`` of ``rmatrix_x``

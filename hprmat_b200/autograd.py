@@ -20,32 +20,54 @@ from . import workloads
 __all__ = ["CollisionMatrix", "CollisionMatrices", "collision_matrix", "collision_matrices", "potential_matrix"]
 
 
+def _symmetric(cpot: torch.Tensor, nr: int) -> bool:
+    """cpot(i, c, c') == cpot(i, c', c) at the mesh points (compared where cpot lives)."""
+    return bool(torch.equal(cpot[:nr], cpot[:nr].transpose(1, 2)))
+
+
+def _device_path(cpot: torch.Tensor, solver) -> bool:
+    """A CUDA potential on the solver's device: the solve and the gradient stay on the device."""
+    return cpot.is_cuda and cpot.device.index == solver.device
+
+
 class CollisionMatrix(torch.autograd.Function):
     """Forward: the refined device solve.  For a symmetric potential (C(E) complex symmetric)
     the forward keeps its solution X = C^-1 Q on the device and the backward forms the gradient
-    from it without another solve (``Context.rmatrix_x`` / ``adjoint_from_x``); otherwise the
-    backward runs ``rmatrix_adjoint`` (FP64 forward and a solve with C^T)."""
+    from it without another solve (``Context.rmatrix_x`` / ``adjoint_from_x``); a potential that
+    is a CUDA tensor on the solver's device is handed to the library by its device address
+    (``rmatrix_x_device`` / ``adjoint_from_x_device``: only O(nch^2) values cross to the host).
+    Otherwise the backward runs ``rmatrix_adjoint`` (FP64 forward and a solve with C^T)."""
 
     @staticmethod
     def forward(fctx, cpot, solver, lval, qk, eta, rmax, nr):
-        c_np = np.asfortranarray(cpot.detach().cpu().numpy().astype(np.complex128))
-        nch = c_np.shape[1]
-        symmetric = bool(np.array_equal(c_np[:nr], c_np[:nr].transpose(0, 2, 1)))
+        cpot = cpot.detach().to(torch.complex128)
+        symmetric = _symmetric(cpot, nr)
+        nch = cpot.shape[1]
         x = None
-        if symmetric:
-            cu, nopen, x = solver.rmatrix_x(nch, lval, qk, eta, rmax, nr, c_np)
+        on_dev = symmetric and _device_path(cpot, solver)
+        if on_dev:
+            cu, nopen, x = solver.rmatrix_x_device(nch, lval, qk, eta, rmax, nr, cpot)
+            u = cu[:nopen, :nopen].contiguous()
         else:
-            cu, nopen = solver.rmatrix(nch, lval, qk, eta, rmax, nr, 1, c_np)
-        fctx.save_for_backward(cpot.detach())
-        fctx.args = (solver, lval, qk, eta, rmax, nr, nopen, x, cu)
-        return torch.from_numpy(np.ascontiguousarray(cu[:nopen, :nopen])).to(cpot.device)
+            c_np = np.asfortranarray(cpot.cpu().numpy())
+            if symmetric:
+                cu, nopen, x = solver.rmatrix_x(nch, lval, qk, eta, rmax, nr, c_np)
+            else:
+                cu, nopen = solver.rmatrix(nch, lval, qk, eta, rmax, nr, 1, c_np)
+            u = torch.from_numpy(np.ascontiguousarray(cu[:nopen, :nopen])).to(cpot.device)
+        fctx.save_for_backward(cpot)
+        fctx.args = (solver, lval, qk, eta, rmax, nr, nopen, x, cu, on_dev)
+        return u
 
     @staticmethod
     def backward(fctx, grad_u):
         (cpot,) = fctx.saved_tensors
-        solver, lval, qk, eta, rmax, nr, nopen, x, cu = fctx.args
-        c_np = np.asfortranarray(cpot.cpu().numpy().astype(np.complex128))
-        nch = c_np.shape[1]
+        solver, lval, qk, eta, rmax, nr, nopen, x, cu, on_dev = fctx.args
+        nch = cpot.shape[1]
+        if on_dev:
+            grad = solver.adjoint_from_x_device(nch, lval, qk, eta, rmax, nr, cpot, cu, x, grad_u)
+            return grad, None, None, None, None, None, None
+        c_np = np.asfortranarray(cpot.cpu().numpy())
         gu = grad_u.detach().cpu().numpy()
         if x is not None:
             grad = solver.adjoint_from_x(nch, lval, qk, eta, rmax, nr, c_np, cu, x, gu)
@@ -89,39 +111,50 @@ class CollisionMatrices(torch.autograd.Function):
 
     @staticmethod
     def forward(fctx, cpot, pool, lval, kin, rmax, nr):
-        c_np = np.asfortranarray(cpot.detach().cpu().numpy().astype(np.complex128))
-        nch = c_np.shape[1]
-        symmetric = bool(np.array_equal(c_np[:nr], c_np[:nr].transpose(0, 2, 1)))
+        cpot = cpot.detach().to(torch.complex128)
+        nch = cpot.shape[1]
+        symmetric = _symmetric(cpot, nr)
+        on_dev = symmetric and all(_device_path(cpot, ctx) for ctx in pool)
+        c_np = None if on_dev else np.asfortranarray(cpot.cpu().numpy())
 
         def fwd(ctx, i):
             qk, eta = kin[i]
+            if on_dev:
+                return ctx.rmatrix_x_device(nch, lval, qk, eta, rmax, nr, cpot)
             if symmetric:
                 return ctx.rmatrix_x(nch, lval, qk, eta, rmax, nr, c_np)
             cu, nopen = ctx.rmatrix(nch, lval, qk, eta, rmax, nr, 1, c_np)
             return cu, nopen, None
 
         res = _round_robin(pool, len(kin), fwd)
-        fctx.save_for_backward(cpot.detach())
-        fctx.args = (pool, lval, kin, rmax, nr, res, symmetric)
+        fctx.save_for_backward(cpot)
+        fctx.args = (pool, lval, kin, rmax, nr, res, symmetric, on_dev)
+        if on_dev:
+            return tuple(cu[:no, :no].contiguous() for cu, no, _ in res)
         return tuple(torch.from_numpy(np.ascontiguousarray(cu[:no, :no])).to(cpot.device) for cu, no, _ in res)
 
     @staticmethod
     def backward(fctx, *grads):
         (cpot,) = fctx.saved_tensors
-        pool, lval, kin, rmax, nr, res, symmetric = fctx.args
-        c_np = np.asfortranarray(cpot.cpu().numpy().astype(np.complex128))
-        nch = c_np.shape[1]
+        pool, lval, kin, rmax, nr, res, symmetric, on_dev = fctx.args
+        nch = cpot.shape[1]
+        c_np = None if on_dev else np.asfortranarray(cpot.cpu().numpy())
 
         def bwd(ctx, i):
             qk, eta = kin[i]
             cu, _, x = res[i]
+            if on_dev:
+                return ctx.adjoint_from_x_device(nch, lval, qk, eta, rmax, nr, cpot, cu, x, grads[i])
             gu = grads[i].detach().cpu().numpy()
             if symmetric:
                 return ctx.adjoint_from_x(nch, lval, qk, eta, rmax, nr, c_np, cu, x, gu)
             return ctx.rmatrix_adjoint(nch, lval, qk, eta, rmax, nr, c_np, gu)[2]
 
+        parts = _round_robin(pool, len(kin), bwd)
+        if on_dev:
+            return torch.stack(parts).sum(0), None, None, None, None, None
         total = np.zeros_like(c_np)
-        for g in _round_robin(pool, len(kin), bwd):
+        for g in parts:
             total += g
         return torch.from_numpy(np.ascontiguousarray(total)).to(cpot.device), None, None, None, None, None
 
@@ -148,6 +181,6 @@ def potential_matrix(r: torch.Tensor, coupling: torch.Tensor, params: torch.Tens
     g = torch.exp(-(r / 2.0) ** 2)
     nch = coupling.shape[0]
     cp = (cscale * coupling)[None, :, :] * g[:, None, None]
-    eye = torch.eye(nch, dtype=torch.bool)
+    eye = torch.eye(nch, dtype=torch.bool, device=coupling.device)
     cp = torch.where(eye[None, :, :], (ws + vc).to(cp.dtype)[:, None, None], cp)
     return cp / hm

@@ -126,4 +126,16 @@ __global__ void potential_grad_kernel(const double2* __restrict__ Y, const doubl
   }
 }
 
+// Sets *flag when the potential (complex (ncp1, ndim, ndim), rows < nr) is not symmetric in its
+// channel indices: cpot(i, c, c') != cpot(i, c', c) for some mesh point i.  Grid (rows / 128,
+// nch, nch), exact comparison as the host check does.
+__global__ void potential_asym_kernel(const double2* __restrict__ cpot, long ncp1, long ndim, int nr, int* flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y, cp = blockIdx.z;
+  if (i >= nr || cp >= c) return;
+  const double2 a = cpot[(size_t)i + ncp1 * ((size_t)c + ndim * (size_t)cp)];
+  const double2 b = cpot[(size_t)i + ncp1 * ((size_t)cp + ndim * (size_t)c)];
+  if (a.x != b.x || a.y != b.y) atomicExch(flag, 1);
+}
+
 }  // namespace hprmat

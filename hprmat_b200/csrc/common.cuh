@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <string.h>
 
 namespace hprmat {
 
@@ -65,6 +66,51 @@ template <typename T> __host__ __device__ inline T crecip(T a) {
 }
 // a/b (Smith)
 template <typename T> __host__ __device__ inline T cdiv(T a, T b) { return cmul(a, crecip(b)); }
+
+// ---------------------------------------------------------------- magnitude keys
+// Integer keys that order like non-negative magnitudes, for atomicMax reductions.
+//
+// Pivot keys (64 bits): the candidate's |re|+|im| in the high bits, the complement of its row
+// in the low bits, so that one 64-bit atomicMax picks the largest modulus and, among equal
+// ones, the lowest row (LAPACK izamax).  The magnitude part is never 0 for a real candidate
+// (0 means "none").  FP32 panels keep all float bits; FP64 panels keep the top 44 bits of the
+// double (sign, 11 exponent bits, 32 mantissa bits), which orders the whole double range --
+// magnitudes below 1e-38 or above 3e38 included -- with rows below 2^20.
+template <typename T> struct PivotKey;
+template <> struct PivotKey<float2> {
+  using M = unsigned;
+  static constexpr int kMaxRows = 0x7fffffff;
+  __device__ static __forceinline__ M mag(float2 v) { return __float_as_uint(fabsf(v.x) + fabsf(v.y)) + 1u; }
+  __device__ static __forceinline__ unsigned long long key(M m, int row) {
+    return ((unsigned long long)m << 32) | (unsigned long long)(0xFFFFFFFFu - (unsigned)row);
+  }
+  __device__ static __forceinline__ int row(unsigned long long k) {
+    return (int)(0xFFFFFFFFu - (unsigned)(k & 0xFFFFFFFFull));
+  }
+};
+template <> struct PivotKey<double2> {
+  using M = unsigned long long;
+  static constexpr int kMaxRows = 1 << 20;
+  __device__ static __forceinline__ M mag(double2 v) {
+    return ((unsigned long long)__double_as_longlong(fabs(v.x) + fabs(v.y)) >> 20) + 1ull;
+  }
+  __device__ static __forceinline__ unsigned long long key(M m, int row) {
+    return (m << 20) | (unsigned long long)(0xFFFFFu - (unsigned)row);
+  }
+  __device__ static __forceinline__ int row(unsigned long long k) { return (int)(0xFFFFFu - (unsigned)(k & 0xFFFFFull)); }
+};
+
+// 32-bit key of a non-negative magnitude over the whole double range: the high word of its
+// IEEE-754 double (11 exponent bits, 20 mantissa bits).  The pivot-growth and max |c_ij|
+// words of the status block hold such keys (atomicMax), on both precisions.
+__device__ __forceinline__ unsigned mag_hi(double v) { return (unsigned)__double2hiint(v); }
+// The magnitude a key stands for (within a relative 2^-20 below the value it was made from).
+__host__ inline double mag_hi_value(unsigned k) {
+  const unsigned long long b = (unsigned long long)k << 32;
+  double v;
+  memcpy(&v, &b, sizeof(v));
+  return v;
+}
 
 __host__ __device__ inline float2 to_f(double2 a) { return make_float2((float)a.x, (float)a.y); }
 __host__ __device__ inline double2 to_d(float2 a) { return make_double2((double)a.x, (double)a.y); }

@@ -46,7 +46,7 @@ struct PanelArgs {
   T* rowj;                        // [2][NB]
   int* status;                    // device status block
   StepSwaps sw;
-  unsigned* growth_bits;          // running max |u_ij| (as float bits, non-negative)
+  unsigned* growth_bits;          // running max |u_ij| (mag_hi key)
   // Optional (mixed path): the "LU planes", hi/lo TF32 splits of Re/Im of the factors,
   // row-major (row stride lup_ld floats, planes lup_plane floats apart).  The panel writes
   // its L21 rows there; they are the K-major A operand of the tensor-core updates.
@@ -59,14 +59,9 @@ struct PanelArgs {
 };
 constexpr int kPanelTraceW = 5 + 160;
 
-// Pivot key of a candidate: |re|+|im| (as float bits, monotone for non-negative values) in
-// the high word, the complement of the panel row in the low word, so that one 64-bit
-// atomicMax picks the largest modulus and, among equal ones, the lowest row.  (On the FP64
-// path the modulus is compared after rounding to float; candidates within a relative 6e-8
-// of each other are equally good pivots.)
-__device__ __forceinline__ unsigned long long pivot_key(float v, int row) {
-  return ((unsigned long long)__float_as_uint(v) << 32) | (unsigned long long)(0xFFFFFFFFu - (unsigned)row);
-}
+// Pivot candidates are compared by PivotKey<T> (common.cuh): |re|+|im| as an integer key
+// that orders over the element type's whole range (FP64 panels: magnitudes far outside the
+// float range too), with the lowest row winning among equal moduli.
 
 // End of a panel factorisation, shared by both panel kernels: the CTA's factored rows back
 // into W, its L21 rows into the LU planes (mixed path), and from CTA 0 the pivots, the growth
@@ -154,7 +149,9 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
   const int rpcp = a.rpc | 1;  // odd column stride: conflict-free row gathers
   T* P = reinterpret_cast<T*>(smem_raw);                 // [NB][rpcp] column-major
   T* urow = P + (size_t)NB * rpcp;                       // [NB]
-  __shared__ float red_v[NT / 32];
+  using PK = PivotKey<T>;
+  using PM = typename PK::M;
+  __shared__ PM red_v[NT / 32];
   __shared__ int red_i[NT / 32];
   __shared__ int s_piv, s_loc_ipiv[NB];
   __shared__ unsigned s_growth;
@@ -171,25 +168,25 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
   // Column jc's pivot candidate: the largest |re|+|im| of the local rows >= jc (lowest row on
   // ties) into s_piv, and its key into the column's global maximum.  v_of(lr) gives the
   // current value of column jc in local row lr.
-  auto candidate = [&](int jc, float bv, int bi) {
+  auto candidate = [&](int jc, PM bv, int bi) {
     for (int o = 16; o > 0; o >>= 1) {
-      float ov = __shfl_down_sync(0xffffffffu, bv, o);
+      PM ov = __shfl_down_sync(0xffffffffu, bv, o);
       int oi = __shfl_down_sync(0xffffffffu, bi, o);
       if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
     }
     if ((tid & 31) == 0) { red_v[tid >> 5] = bv; red_i[tid >> 5] = bi; }
     __syncthreads();
     if (tid < 32) {
-      bv = (tid < NT / 32) ? red_v[tid] : -1.f;
+      bv = (tid < NT / 32) ? red_v[tid] : PM(0);
       bi = (tid < NT / 32) ? red_i[tid] : 0x7fffffff;
       for (int o = 16; o > 0; o >>= 1) {
-        float ov = __shfl_down_sync(0xffffffffu, bv, o);
+        PM ov = __shfl_down_sync(0xffffffffu, bv, o);
         int oi = __shfl_down_sync(0xffffffffu, bi, o);
         if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
       }
       if (tid == 0) {
         s_piv = bi;
-        if (bi != 0x7fffffff) atomicMax(a.keys + jc, pivot_key(bv, bi));
+        if (bi != 0x7fffffff) atomicMax(a.keys + jc, PK::key(bv, bi));
       }
     }
     __syncthreads();
@@ -230,10 +227,10 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
 
   // column 0: candidate, post, arrive
   {
-    float bv = -1.f;
+    PM bv = 0;
     int bi = 0x7fffffff;
     for (int lr = max(-r0, 0) + tid; lr < nloc; lr += NT) {
-      float v = (float)cabs1(P[lr]);
+      const PM v = PK::mag(P[lr]);
       if (v > bv) { bv = v; bi = r0 + lr; }
     }
     candidate(0, bv, bi);
@@ -251,23 +248,23 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
     // the winning key names the pivot row; its owner CTA is row / rpc
     if (tid == 0) {
       unsigned long long key = __ldcg(a.keys + j);
-      s_piv = (int)(0xFFFFFFFFu - (unsigned)(key & 0xFFFFFFFFull));
+      s_piv = PK::row(key);
     }
     __syncthreads();
     const int p = s_piv;
     const int win = p / a.rpc;
-    float g = 0.f;  // pivot growth: largest |re|+|im| in the U part of the pivot row
+    unsigned g = 0u;  // pivot growth: largest |re|+|im| in the U part of the pivot row (mag_hi key)
     for (int c = tid; c < ncols; c += NT) {
       T u = __ldcg(reinterpret_cast<const T*>(a.cand_rows) + ((size_t)buf * a.G + win) * NB + c);
       urow[c] = u;
       if (p != j && p >= r0 && p < r1)
         P[(size_t)c * rpcp + (p - r0)] = __ldcg(reinterpret_cast<const T*>(a.rowj) + (size_t)buf * NB + c);
       if (p != j && j >= r0 && j < r1) P[(size_t)c * rpcp + (j - r0)] = u;
-      if (c >= j) g = fmaxf(g, (float)cabs1(u));
+      if (c >= j) g = max(g, mag_hi((double)cabs1(u)));
     }
     if (tid < ((ncols + 31) & ~31)) {  // whole warps that may hold entries
-      for (int o = 16; o > 0; o >>= 1) g = fmaxf(g, __shfl_down_sync(0xffffffffu, g, o));
-      if ((tid & 31) == 0 && g > 0.f) atomicMax(&s_growth, __float_as_uint(g));
+      for (int o = 16; o > 0; o >>= 1) g = max(g, __shfl_down_sync(0xffffffffu, g, o));
+      if ((tid & 31) == 0 && g > 0u) atomicMax(&s_growth, g);
     }
     if (tid == 0) s_loc_ipiv[j] = p;
     __syncthreads();
@@ -283,7 +280,7 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
       // column j + 1 first: scale, update, candidate; post it and arrive, then finish the
       // rank-1 update of columns j + 2 .. while the other CTAs arrive
       const int jn = j + 1;
-      float bv = -1.f;
+      PM bv = 0;
       int bi = 0x7fffffff;
       for (int lr = lo + tid; lr < nloc; lr += NT) {
         T l = P[(size_t)j * rpcp + lr];
@@ -294,7 +291,7 @@ __global__ void __launch_bounds__(NT, 1) panel_kernel(PanelArgs<T> a) {
         T v = P[(size_t)jn * rpcp + lr];
         cfms(v, l, urow[jn]);
         P[(size_t)jn * rpcp + lr] = v;
-        float av = (float)cabs1(v);
+        const PM av = PK::mag(v);
         if (av > bv) { bv = av; bi = r0 + lr; }
       }
       candidate(jn, bv, bi);
@@ -376,7 +373,9 @@ __global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(PanelArgs<T> a) {
   T* xrowj = xrow + 2 * NB;               // [2][NB] row j, posted by its owner
   // [2][kMaxClusterCTAs]: every CTA's pivot key, pushed into every CTA before the barrier
   unsigned long long* xkey = reinterpret_cast<unsigned long long*>(xrowj + 2 * NB);
-  __shared__ float red_v[NT / 32];
+  using PK = PivotKey<T>;
+  using PM = typename PK::M;
+  __shared__ PM red_v[NT / 32];
   __shared__ int red_i[NT / 32];
   __shared__ int s_piv, s_loc_ipiv[NB];
   __shared__ unsigned s_growth;
@@ -391,24 +390,24 @@ __global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(PanelArgs<T> a) {
 
   // column jc's local candidate into s_piv, and its key into slot b of xkey[jc & 1] of every
   // CTA of the cluster (lane t of warp 0 stores into CTA t)
-  auto candidate = [&](int jc, float bv, int bi) {
+  auto candidate = [&](int jc, PM bv, int bi) {
     for (int o = 16; o > 0; o >>= 1) {
-      float ov = __shfl_down_sync(0xffffffffu, bv, o);
+      PM ov = __shfl_down_sync(0xffffffffu, bv, o);
       int oi = __shfl_down_sync(0xffffffffu, bi, o);
       if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
     }
     if ((tid & 31) == 0) { red_v[tid >> 5] = bv; red_i[tid >> 5] = bi; }
     __syncthreads();
     if (tid < 32) {
-      bv = (tid < NT / 32) ? red_v[tid] : -1.f;
+      bv = (tid < NT / 32) ? red_v[tid] : PM(0);
       bi = (tid < NT / 32) ? red_i[tid] : 0x7fffffff;
       for (int o = 16; o > 0; o >>= 1) {
-        float ov = __shfl_down_sync(0xffffffffu, bv, o);
+        PM ov = __shfl_down_sync(0xffffffffu, bv, o);
         int oi = __shfl_down_sync(0xffffffffu, bi, o);
         if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
       }
       if (tid == 0) s_piv = bi;
-      const unsigned long long key = __shfl_sync(0xffffffffu, bi != 0x7fffffff ? pivot_key(bv, bi) : 0ull, 0);
+      const unsigned long long key = __shfl_sync(0xffffffffu, bi != 0x7fffffff ? PK::key(bv, bi) : 0ull, 0);
       if (tid < a.G) *cluster.map_shared_rank(xkey + (jc & 1) * kMaxClusterCTAs + b, (unsigned)tid) = key;
     }
     __syncthreads();
@@ -433,10 +432,10 @@ __global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(PanelArgs<T> a) {
   };
 
   {
-    float bv = -1.f;
+    PM bv = 0;
     int bi = 0x7fffffff;
     for (int lr = tid; lr < nloc; lr += NT) {
-      float v = (float)cabs1(P[lr]);
+      const PM v = PK::mag(P[lr]);
       if (v > bv) { bv = v; bi = r0 + lr; }
     }
     candidate(0, bv, bi);
@@ -459,20 +458,20 @@ __global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(PanelArgs<T> a) {
       }
       kmax = k;
     }
-    const int p = (int)(0xFFFFFFFFu - (unsigned)(kmax & 0xFFFFFFFFull));
+    const int p = PK::row(kmax);
     const T* wrow = cluster.map_shared_rank(xrow + buf * NB, (unsigned)(p / a.rpc));
     const T* jrow = cluster.map_shared_rank(xrowj + buf * NB, (unsigned)(j / a.rpc));
-    float g = 0.f;
+    unsigned g = 0u;
     for (int c = tid; c < ncols; c += NT) {
       T u = wrow[c];
       urow[c] = u;
       if (p != j && p >= r0 && p < r1) P[(size_t)c * rpcp + (p - r0)] = jrow[c];
       if (p != j && j >= r0 && j < r1) P[(size_t)c * rpcp + (j - r0)] = u;
-      if (c >= j) g = fmaxf(g, (float)cabs1(u));
+      if (c >= j) g = max(g, mag_hi((double)cabs1(u)));
     }
     if (tid < ((ncols + 31) & ~31)) {
-      for (int o = 16; o > 0; o >>= 1) g = fmaxf(g, __shfl_down_sync(0xffffffffu, g, o));
-      if ((tid & 31) == 0 && g > 0.f) atomicMax(&s_growth, __float_as_uint(g));
+      for (int o = 16; o > 0; o >>= 1) g = max(g, __shfl_down_sync(0xffffffffu, g, o));
+      if ((tid & 31) == 0 && g > 0u) atomicMax(&s_growth, g);
     }
     if (tid == 0) s_loc_ipiv[j] = p;
     __syncthreads();
@@ -483,7 +482,7 @@ __global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(PanelArgs<T> a) {
     const int lo = max(j + 1 - r0, 0);
     if (j + 1 < ncols) {
       const int jn = j + 1;
-      float bv = -1.f;
+      PM bv = 0;
       int bi = 0x7fffffff;
       for (int lr = lo + tid; lr < nloc; lr += NT) {
         T l = P[(size_t)j * rpcp + lr];
@@ -494,7 +493,7 @@ __global__ void __launch_bounds__(NT, 1) panel_cluster_kernel(PanelArgs<T> a) {
         T v = P[(size_t)jn * rpcp + lr];
         cfms(v, l, urow[jn]);
         P[(size_t)jn * rpcp + lr] = v;
-        float av = (float)cabs1(v);
+        const PM av = PK::mag(v);
         if (av > bv) { bv = av; bi = r0 + lr; }
       }
       candidate(jn, bv, bi);
@@ -607,7 +606,7 @@ __global__ void __launch_bounds__(NT) trsm_lower_kernel(TrsmArgs<T> a) {
   }
   if (a.growth_bits) {
     for (int o = 16; o > 0; o >>= 1) gmax = fmax(gmax, __shfl_down_sync(0xffffffffu, gmax, o));
-    if ((tid & 31) == 0) atomicMax(a.growth_bits, __float_as_uint((float)gmax));
+    if ((tid & 31) == 0) atomicMax(a.growth_bits, mag_hi((double)gmax));
   }
   if (a.lup != nullptr) {
     for (int idx = tid; idx < ncw * ncols; idx += NT) {
@@ -1118,7 +1117,7 @@ __global__ void __launch_bounds__(NT) u12_split_kernel(const float2* __restrict_
   }
   if (growth_bits) {
     for (int o = 16; o > 0; o >>= 1) gmax = fmaxf(gmax, __shfl_down_sync(0xffffffffu, gmax, o));
-    if ((tid & 31) == 0 && gmax > 0.f) atomicMax(growth_bits, __float_as_uint(gmax));
+    if ((tid & 31) == 0 && gmax > 0.f) atomicMax(growth_bits, mag_hi((double)gmax));
   }
 }
 

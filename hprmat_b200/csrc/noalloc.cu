@@ -13,7 +13,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <mutex>
 
 #include "../../include/hprmat_b200.h"
 #include "common.cuh"
@@ -48,28 +47,17 @@ constexpr size_t kScratchBytes = align256(kOffStatus + 64 * sizeof(int));  // ab
 // from cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-unsigned char* g_scratch_addr[kMaxDevices] = {};
-
+// The array's device address on the current device, looked up on every call: a cached
+// address would go stale if the application reset the device (cudaDeviceReset) or its
+// primary context was created again.  The lookup is cheap next to the solve.
 int scratch_for_current_device(unsigned char** out) {
-  int dev = 0;
-  HPR_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) {
-    set_last_error_msg("solve_linear_noalloc: device index out of range");
-    return HPRMAT_B200_ERR_UNSUPPORTED;
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || p == nullptr) {
+    set_last_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
+    return HPRMAT_B200_ERR_CUDA;
   }
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || p == nullptr) {
-      set_last_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
-      return HPRMAT_B200_ERR_CUDA;
-    }
-    g_scratch_addr[dev] = static_cast<unsigned char*>(p);
-  }
-  *out = g_scratch_addr[dev];
+  *out = static_cast<unsigned char*>(p);
   return HPRMAT_B200_OK;
 }
 

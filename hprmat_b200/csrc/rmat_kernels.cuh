@@ -68,17 +68,18 @@ struct Acc2 {
   __device__ __forceinline__ double value() const { return hi + lo; }
 };
 
-// Block-wide maximum of a non-negative float into *out (as float bits, which order like the
-// values for non-negative numbers), one atomic per block.  All threads of the block call it.
-__device__ __forceinline__ void block_max_atomic(float v, unsigned* out) {
-  __shared__ float red_m[32];
-  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
-  if ((threadIdx.x & 31) == 0) red_m[threadIdx.x >> 5] = v;
+// Block-wide maximum of a non-negative magnitude into *out as a mag_hi key (orders like the
+// values over the whole double range), one atomic per block.  All threads of the block call it.
+__device__ __forceinline__ void block_max_atomic(double v, unsigned* out) {
+  __shared__ unsigned red_m[32];
+  unsigned k = mag_hi(v);
+  for (int o = 16; o > 0; o >>= 1) k = max(k, __shfl_down_sync(0xffffffffu, k, o));
+  if ((threadIdx.x & 31) == 0) red_m[threadIdx.x >> 5] = k;
   __syncthreads();
   if (threadIdx.x < 32) {
-    v = threadIdx.x < (blockDim.x >> 5) ? red_m[threadIdx.x] : 0.f;
-    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
-    if (threadIdx.x == 0 && v > 0.f) atomicMax(out, __float_as_uint(v));
+    k = threadIdx.x < (blockDim.x >> 5) ? red_m[threadIdx.x] : 0u;
+    for (int o = 16; o > 0; o >>= 1) k = max(k, __shfl_down_sync(0xffffffffu, k, o));
+    if (threadIdx.x == 0 && k > 0u) atomicMax(out, k);
   }
 }
 
@@ -97,7 +98,7 @@ __global__ void assemble_kernel(MeshDev mesh, ChannelData ch, int nch, const dou
   // (coalesced writes along the column), one atomic per block for ||C||_F^2
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   double sq = 0.0;
-  float am = 0.f;
+  double am = 0.0;
   if (row < N) {
     const int nr = mesh.nr;
     const int c = row / nr, i = row - c * nr;
@@ -129,7 +130,7 @@ __global__ void assemble_kernel(MeshDev mesh, ChannelData ch, int nch, const dou
         out.x = (typename RealOf<T>::R)re;
         out.y = (typename RealOf<T>::R)im;
         sq += re * re + im * im;
-        am = fmaxf(am, (float)(fabs(re) + fabs(im)));
+        am = fmax(am, fabs(re) + fabs(im));
       } else {  // off the channel's block and off the mesh diagonal: C is zero there
         out.x = 0;
         out.y = 0;
@@ -463,12 +464,12 @@ __global__ void copy_d_kernel(const double2* __restrict__ src, long lds, double2
 __global__ void fro2_kernel(const double2* __restrict__ A, long lda, int N, double* fro2, unsigned* amax = nullptr) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   double sq = 0.0;
-  float am = 0.f;
+  double am = 0.0;
   if (r < N) {
     for (int col = blockIdx.y; col < N; col += gridDim.y) {
       double2 v = A[(size_t)r + (size_t)col * lda];
       sq += v.x * v.x + v.y * v.y;
-      am = fmaxf(am, (float)(fabs(v.x) + fabs(v.y)));
+      am = fmax(am, fabs(v.x) + fabs(v.y));
     }
   }
   if (amax) block_max_atomic(am, amax);
@@ -505,11 +506,11 @@ __global__ void d2f_matrix_kernel(const double2* __restrict__ src, long lds, flo
                                   unsigned* amax = nullptr) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   const int col = blockIdx.y;
-  float am = 0.f;
+  double am = 0.0;
   if (r < N) {
     double2 v = src[(size_t)r + (size_t)col * lds];
     dst[(size_t)r + (size_t)col * ldd] = make_float2((float)v.x, (float)v.y);
-    am = (float)(fabs(v.x) + fabs(v.y));
+    am = fabs(v.x) + fabs(v.y);
   }
   if (amax) block_max_atomic(am, amax);
 }

@@ -2,6 +2,7 @@
 // refinement and the C ABI declared in include/hprmat_b200.h.
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <atomic>
@@ -28,6 +29,16 @@
 #include "tc_solve.cuh"
 
 using namespace hprmat;
+
+// NVTX range over one phase of a solve (assembly, factorisation, triangular solves,
+// refinement, condition estimate, collision matrix), visible on a profiler's timeline.
+// Header-only NVTX v3: with no tool attached a range costs a few nanoseconds.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // ------------------------------------------------------------------ error reporting
 static thread_local std::string g_last_error;
@@ -99,13 +110,14 @@ static constexpr int kSwapStride = 3 * kMaxNB + 4;  // ints per step in the swap
 constexpr int kArnoldiNT = 512;
 
 // Status-block slots beyond the factorisation's own (SW_*; int offsets into the 64-int block):
-// the largest |re| + |im| of the matrix about to be factorised (float bits, written by the
+// the largest |re| + |im| of the matrix about to be factorised (mag_hi key, written by the
 // assembly / conversion kernels for the pivot-growth check) and ||C||_1 (double bits, 8-byte
 // aligned, written by colabs_max_kernel when opts.estimate_condition is set).  The
 // factorisation copies the first kStatusCopy ints to h_status when it ends.
 constexpr int kAmaxSlot = 40;
 constexpr int kAnormSlot = 42;
 constexpr int kStatusCopy = 44;
+constexpr int kSymSlot = 48;  // nonzero when a device potential is not symmetric (adjoint_from_x_device)
 
 // One row of the scan autotuner's table: the settings chosen for the units of order N, and the
 // time of the tuned trial (all workers solving one energy of order N at once).
@@ -865,6 +877,9 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
 
 template <typename T>
 static int factor(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, int nb, LUState& st) {
+  NvtxRange nv(mixed ? "hprmat.factor.mixed" : "hprmat.factor.fp64");
+  if (N >= PivotKey<T>::kMaxRows)
+    return fail(HPRMAT_B200_ERR_UNSUPPORTED, "order %d beyond the pivot keys' row range", N);
   switch (nb) {
     case 128: return factor_impl<T, 128>(c, W, ld, N, mixed, st);
     case 64: return factor_impl<T, 64>(c, W, ld, N, mixed, st);
@@ -985,6 +1000,7 @@ static int lu_solve_tc_impl(hprmat_b200_ctx* c, const LUState& st, float2* X, lo
 }
 
 static int lu_solve_tc(hprmat_b200_ctx* c, const LUState& st, float2* X, long ldx, int nrhs) {
+  NvtxRange nv("hprmat.solve.mixed");
   switch (st.nb) {
     case 128: return lu_solve_tc_impl<128>(c, st, X, ldx, nrhs);
     case 64: return lu_solve_tc_impl<64>(c, st, X, ldx, nrhs);
@@ -996,6 +1012,7 @@ static int lu_solve_tc(hprmat_b200_ctx* c, const LUState& st, float2* X, long ld
 
 template <typename T>
 static int lu_solve(hprmat_b200_ctx* c, const T* W, const LUState& st, T* X, long ldx, int nrhs) {
+  NvtxRange nv("hprmat.solve");
   switch (st.nb) {
     case 128: return lu_solve_impl<T, 128>(c, W, st, X, ldx, nrhs);
     case 64: return lu_solve_impl<T, 64>(c, W, st, X, ldx, nrhs);
@@ -1103,6 +1120,7 @@ static int frob_norm(hprmat_b200_ctx* c, const double2* X, long ldx, int N, int 
 static int refine_mixed(hprmat_b200_ctx* c, const Operator& op, const float2* W32, const LUState& st,
                         double2* X64, long ldx, int nrhs, double bnorm, double cnorm, hprmat_b200_stats* stats,
                         int max_outer = -1, bool error_based = false) {
+  NvtxRange nv("hprmat.refine");
   // error_based (factors of another energy, opts.reuse_factors): a small residual alone does
   // not stop the refinement -- the surface rule, which measures the error in R, must hold
   if (max_outer < 0) max_outer = c->opts.max_refine;
@@ -1333,12 +1351,9 @@ static int anorm_begin(hprmat_b200_ctx* c, const double2* A, long lda, int N) {
 // panel and U12 kernels into the status block) over that of the matrix (kAmaxSlot), both from
 // the copy factor made.  0 for a zero matrix.
 static int pivot_growth(hprmat_b200_ctx* c, double* rho) {
-  const unsigned abits = (unsigned)c->h_status[kAmaxSlot];
-  const unsigned gbits = (unsigned)c->h_status[SW_COUNT - 1];
-  float g, am;
-  memcpy(&g, &gbits, sizeof(float));
-  memcpy(&am, &abits, sizeof(float));
-  *rho = am > 0.f ? (double)g / (double)am : 0.0;
+  const double am = mag_hi_value((unsigned)c->h_status[kAmaxSlot]);
+  const double g = mag_hi_value((unsigned)c->h_status[SW_COUNT - 1]);
+  *rho = am > 0.0 ? g / am : 0.0;
   return HPRMAT_B200_OK;
 }
 
@@ -1411,9 +1426,12 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
       st.nb = c->held_nb;
       st.nsteps = c->held_nsteps;
     } else {
-      assemble_kernel<float2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2, nl,
-                                                         d_amax);
-      LAUNCH_CHECK();
+      {
+        NvtxRange nv("hprmat.assemble");
+        assemble_kernel<float2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2, nl,
+                                                           d_amax);
+        LAUNCH_CHECK();
+      }
       int nb = pick_nb(c, N, sizeof(float2), 128);
       if (!nb) return fail(HPRMAT_B200_ERR_UNSUPPORTED, "N = %d too large for the panel kernel", N);
       auto t1 = Clock::now();
@@ -1459,9 +1477,12 @@ static int interval_solve(hprmat_b200_ctx* c, int is, int nch, const ChannelData
   if (!mixed || stats->fp64_fallback) {
     TRY(c->W.ensure((size_t)ld * N * sizeof(double2)));
     double2* W = c->W.as<double2>();
-    assemble_kernel<double2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2, nl,
-                                                        d_amax);
-    LAUNCH_CHECK();
+    {
+      NvtxRange nv("hprmat.assemble");
+      assemble_kernel<double2><<<ga, 256, 0, c->stream>>>(md, chd, nch, d_cpot, ncp1, ndim, W, ld, N, d_fro2, nl,
+                                                          d_amax);
+      LAUNCH_CHECK();
+    }
     surface_rhs_kernel<double2><<<gr, 256, 0, c->stream>>>(md, X64, ld, N, 1.0);
     LAUNCH_CHECK();
     int nb = pick_nb(c, N, sizeof(double2), 64);
@@ -1714,6 +1735,7 @@ static int rmatrix_core(hprmat_b200_ctx* c, int nch, const int* lval, const doub
   }
   // U
   auto t4 = Clock::now();
+  NvtxRange nv_u("hprmat.umatrix");
   HPR_CUDA_TRY(cudaMemsetAsync(d_info, 0, sizeof(int), c->stream));
   umatrix_kernel<<<1, 1024, 0, c->stream>>>(ns > 1 ? rp : R, nch, d_open, d_qk, d_co, d_cop, no, zo,
                                             zo + std::max(1, no * no), d_cu, ndim, d_info);
@@ -1804,6 +1826,7 @@ static int lu_solve_trans(hprmat_b200_ctx* c, const double2* W, long ld, int N, 
 // the factors (lu_solve), with A^H as conj(A^-T conj v) (lu_solve_trans); one right-hand side
 // each, vectors on the host.  *kappa = 0 when not available (block size above 64).
 static int condest_fp64(hprmat_b200_ctx* c, const double2* W, const LUState& st, double* kappa) {
+  NvtxRange nv("hprmat.condest");
   *kappa = 0.0;
   const int N = st.N;
   if (N <= 0 || st.nb > 64) return HPRMAT_B200_OK;
@@ -2923,6 +2946,60 @@ int hprmat_b200_adjoint_from_x(hprmat_b200_ctx* c, int nch, const int* lval, con
   return HPRMAT_B200_OK;
 }
 
+int hprmat_b200_rmatrix_x_device(hprmat_b200_ctx* c, int nch, const int* lval, const double* qk, const double* eta,
+                                 double rmax, int nr, const void* d_cpot, int ncp1, int ndim, void* d_cu, int* nopen,
+                                 void* d_x, long ldx, hprmat_b200_stats* stats) {
+  TRY(check_ctx(c));
+  if (!d_x || ldx < (long)nch * nr) return fail(HPRMAT_B200_ERR_ARG, "rmatrix_x_device: need d_x with ldx >= nch*nr");
+  int s = hprmat_b200_rmatrix_device(c, nch, lval, qk, eta, rmax, nr, 1, d_cpot, ncp1, ndim, d_cu, nopen, stats);
+  if (s != HPRMAT_B200_OK && s != HPRMAT_B200_NOT_CONVERGED) return s;
+  const long N = (long)nch * nr, ld = (N + 3) / 4 * 4;
+  HPR_CUDA_TRY(cudaMemcpy2DAsync(d_x, (size_t)ldx * sizeof(double2), c->X64.p, (size_t)ld * sizeof(double2),
+                                 (size_t)N * sizeof(double2), nch, cudaMemcpyDeviceToDevice, c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return s;
+}
+
+int hprmat_b200_adjoint_from_x_device(hprmat_b200_ctx* c, int nch, const int* lval, const double* qk,
+                                      const double* eta, double rmax, int nr, const void* d_cpot, int ncp1, int ndim,
+                                      const double* cu, const void* d_x, long ldx, const double* gu, void* d_grad) {
+  TRY(check_ctx(c));
+  if (!d_cpot || !cu || !gu || !d_grad || !d_x || ndim < nch || ncp1 < nr || nch <= 0 || ldx < (long)nch * nr)
+    return fail(HPRMAT_B200_ERR_ARG, "adjoint_from_x_device: invalid arguments");
+  if (c->nr != nr || c->ns != 1 || c->rmax != rmax)
+    return fail(HPRMAT_B200_ERR_ARG, "adjoint_from_x_device: call rmat_ini(nr=%d, ns=1, rmax=%g) first", nr, rmax);
+  // the potential must be symmetric (C(E) complex symmetric): checked on the device
+  int* d_flag = c->status.as<int>() + kSymSlot;
+  HPR_CUDA_TRY(cudaMemsetAsync(d_flag, 0, sizeof(int), c->stream));
+  potential_asym_kernel<<<dim3(cdiv_u(nr, 128), nch, nch), 128, 0, c->stream>>>((const double2*)d_cpot, ncp1, ndim, nr,
+                                                                               d_flag);
+  LAUNCH_CHECK();
+  int asym = 0;
+  HPR_CUDA_TRY(cudaMemcpyAsync(&asym, d_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  const double a = rmax;
+  TRY(c->rmat.ensure((size_t)nch * nch * sizeof(double2) + 64));
+  const MeshDev md = mesh_dev(c, 0);
+  rmat_extract_kernel<<<dim3(nch, cdiv_u(nch, 128)), 128, 0, c->stream>>>((const double2*)d_x, ldx, md.q2, nr, nch,
+                                                                         nch, 1.0 / a, c->rmat.as<double2>());
+  LAUNCH_CHECK();
+  std::vector<double2> R((size_t)nch * nch);
+  HPR_CUDA_TRY(cudaMemcpyAsync(R.data(), c->rmat.p, R.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (asym)
+    return fail(HPRMAT_B200_ERR_UNSUPPORTED,
+                "adjoint_from_x_device: the potential is not symmetric; use rmatrix_adjoint");
+  std::vector<double2> M2;
+  int no = 0;
+  TRY(adjoint_m2(nch, lval, qk, eta, rmax, a, R, cu, gu, ndim, M2, &no));
+  if (no > 0) {
+    TRY(adjoint_grad_symmetric(c, nch, nr, ndim, ncp1, a, M2, (const double2*)d_x, ldx, (double2*)d_grad));
+  } else {
+    HPR_CUDA_TRY(cudaMemsetAsync(d_grad, 0, (size_t)ncp1 * ndim * ndim * sizeof(double2), c->stream));
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
+  return HPRMAT_B200_OK;
+}
+
 int hprmat_b200_solve_linear_device(hprmat_b200_ctx* c, const void* d_A, void* d_B, int n, int nrhs,
                                     hprmat_b200_stats* stats) {
   TRY(check_ctx(c));
@@ -3218,6 +3295,16 @@ __global__ void split_planes_kernel(const float2* __restrict__ src, int rows, in
   dst[plane + idx] = lr;
   dst[2 * plane + idx] = hi;
   dst[3 * plane + idx] = li;
+}
+
+int hprmat_b200_dev_binary_version(void) {
+  cudaFuncAttributes fa;
+  const cudaError_t e = cudaFuncGetAttributes(&fa, (const void*)split_planes_kernel);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(HPRMAT_B200_ERR_NODEVICE, "no device can load the library's kernels: %s", cudaGetErrorString(e));
+  }
+  return fa.binaryVersion;
 }
 
 int hprmat_b200_dev_split_planes(hprmat_b200_ctx* c, const void* src, int rows, int nb, float* dst, long plane) {

@@ -144,6 +144,17 @@ int hprmat_b200_adjoint_from_x(hprmat_b200_ctx* ctx, int nch, const int* lval, c
                                double rmax, int nr, const double* cpot, int ncp1, int ndim, const double* cu,
                                const void* d_x, long ldx, const double* gu, double* grad);
 
+/* Device-resident variants of the two halves above, for callers whose potential already lives
+   in device memory (a torch CUDA tensor in reverse-mode autodiff): d_cpot, d_cu, d_x and d_grad
+   are device pointers; lval/qk/eta, cu and gu (O(nch^2)) stay host arrays.  The potential's
+   symmetry is checked on the device (HPRMAT_B200_ERR_UNSUPPORTED when it is not symmetric). */
+int hprmat_b200_rmatrix_x_device(hprmat_b200_ctx* ctx, int nch, const int* lval, const double* qk, const double* eta,
+                                 double rmax, int nr, const void* d_cpot, int ncp1, int ndim, void* d_cu, int* nopen,
+                                 void* d_x, long ldx, hprmat_b200_stats* stats);
+int hprmat_b200_adjoint_from_x_device(hprmat_b200_ctx* ctx, int nch, const int* lval, const double* qk,
+                                      const double* eta, double rmax, int nr, const void* d_cpot, int ncp1, int ndim,
+                                      const double* cu, const void* d_x, long ldx, const double* gu, void* d_grad);
+
 /* One J-pi block of a batched energy scan (hprmat_b200_rmatrix_scan).  The reference has no
    batched entry: its drivers call rmatrix once per energy in a host loop
    (examples/Ex1/example1_hp.f90:102-110, examples/Ex4/example4_hp.f90:118-134). */
@@ -295,10 +306,11 @@ int gpu_b200_finalize_(void);                       /* cf. gpu_solver_finalize_ 
    X) are device pointers; the work is ordered on `stream` (a cudaStream_t, NULL = default
    stream) and complete when the call returns.  *info (may be NULL) receives the first zero
    pivot (1-based) when the status is HPRMAT_B200_SINGULAR.
-   The first call on a device looks up the array's device address (cudaGetSymbolAddress);
-   make that first call before any stream capture.  All calls share the one array: calls
-   whose GPU work overlaps (other threads or streams) race and must be serialised by the
-   caller. */
+   Every call looks up the array's device address on the current device
+   (cudaGetSymbolAddress), so a device reset does not leave a stale address behind; the
+   first call on a device also loads the array there, so make it before any stream capture.
+   All calls share the one array: calls whose GPU work overlaps (other threads or streams)
+   race and must be serialised by the caller. */
 int hprmat_b200_solve_linear_noalloc(const void* d_A, void* d_B, int n, int nrhs, void* stream,
                                      int* info);
 

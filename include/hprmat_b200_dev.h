@@ -58,6 +58,11 @@ int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* ctx, const char* key, int value)
    meant to (the context stays usable); any other value is a failure of the check. */
 int hprmat_b200_dev_wait_probe(hprmat_b200_ctx* ctx, int spins);
 
+/* The binary architecture the library's kernels were compiled for, as the CUDA runtime reports
+   it for one of them (cudaFuncAttributes.binaryVersion: 100 for sm_100a), on the current
+   device; a negative status when no device can load them. */
+int hprmat_b200_dev_binary_version(void);
+
 /* LU factorisations run on the context and its scan workers since the last reset (opts.reuse_factors
    makes energy scans run fewer); reset != 0 clears the count after reading.  -1 for a null
    context. */

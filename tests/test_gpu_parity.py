@@ -40,6 +40,11 @@ def ctx():
     c.close()
 
 
+def test_kernels_report_sm100_binary():
+    """The CUDA runtime reports the loaded kernels as sm_100 binaries (binaryVersion 100)."""
+    assert nat.load().hprmat_b200_dev_binary_version() == 100
+
+
 # ---------------------------------------------------------------- tensor-core kernel
 @pytest.mark.parametrize("M,Nc,nb,bn", [(128, 256, 128, 256), (300, 520, 128, 256), (1000, 700, 64, 256),
                                         (77, 33, 32, 256), (640, 128, 128, 128), (129, 200, 64, 128),
@@ -133,18 +138,36 @@ def test_medium_production_generator(ctx, precision):
     assert _rel(cu[:nopen, :nopen], ref.cu) <= U_TOL, ctx.last_stats
 
 
-@pytest.mark.parametrize("nch", [32, 64])
+@pytest.mark.parametrize("nch", [32, 64, 128])
 def test_production_generator_against_fixture(ctx, nch):
-    """Production generator at N = 6400 and 12800 (200 points x nch channels) against the
-    committed FP64 oracle collision matrices (tests/golden/make_production_u.py).  N = 6400
+    """Production generator at N = 6400, 12800 and 25600 (200 points x nch channels) against
+    the committed FP64 oracle collision matrices (tests/golden/make_production_u.py).  N = 6400
     puts 44 panel rows on each of the 148 CTAs, the shape whose shared memory sits just
-    under the 48 KB default."""
+    under the 48 KB default; N = 25600 (128 channels) is the headline configuration, where the
+    call must also end with HPRMAT_B200_OK (refinement converged within its three steps)."""
     fx = np.load(os.path.join(GOLDEN, f"production_u_nch{nch}.npz"))
     w = workloads.production(nch=nch)
     ctx.set_precision("mixed")
     cu, nopen = ctx.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+    st = ctx.last_stats
+    assert st["status"] == nat.OK and st["refine_steps"] <= 3, st
     assert nopen == int(fx["nopen"])
-    assert _rel(cu[:nopen, :nopen], fx["u"]) <= U_TOL, ctx.last_stats
+    assert _rel(cu[:nopen, :nopen], fx["u"]) <= U_TOL, st
+
+
+@pytest.mark.parametrize("nch", [50, 80, 128])
+def test_sweep_generator_against_fixture(ctx, nch):
+    """Precision-sweep generator (closed channels at 40 MeV) at N = 10000, 16000 and 25600
+    against committed FP64 oracle collision matrices (tests/golden/make_production_u.py
+    --sweep): the mixed path, refined to HPRMAT_B200_OK, within 1e-10 of LAPACK zgesv."""
+    fx = np.load(os.path.join(GOLDEN, f"sweep_u_nch{nch}.npz"))
+    w = workloads.sweep(nch)
+    ctx.set_precision("mixed")
+    cu, nopen = ctx.rmatrix(w.nch, w.lval, w.qk, w.eta, w.rmax, w.nr, 1, w.cpot)
+    st = ctx.last_stats
+    assert st["status"] == nat.OK, st
+    assert nopen == int(fx["nopen"])
+    assert _rel(cu[:nopen, :nopen], fx["u"]) <= U_TOL, st
 
 
 @pytest.mark.parametrize("sb,un", [(1, 64), (2, 128), (4, 64), (4, 128)])
@@ -495,6 +518,26 @@ def test_odd_and_long_meshes(ctx, precision, nch, nr):
         # stops at its rounding level
         tol = U_TOL if precision == "mixed" else max(U_TOL, 5 * oracle_err)
         assert _rel(cu[:nopen, :nopen], u_ref) <= tol, (oracle_err, ctx.last_stats)
+    ctx.set_precision("mixed")
+
+
+@pytest.mark.parametrize("scale", [1e-300, 1e300])
+def test_fp64_pivoting_outside_float_range(ctx, scale):
+    """FP64 dense solve of a matrix whose entries lie far outside the float range (1e-300 or
+    1e300 times O(1) values) with a zero diagonal, so every column needs a row interchange:
+    the FP64 panels compare pivot candidates over the whole double range (as zgetrf does),
+    so they pivot to the largest entry instead of reporting a false zero pivot."""
+    rng = np.random.default_rng(21)
+    n, nrhs = 300, 5
+    A0 = rng.uniform(0.5, 1.5, (n, n)) + 1j * rng.uniform(-0.5, 0.5, (n, n))
+    A0[np.arange(n), np.arange(n)] = 0.0
+    A = np.asfortranarray(A0 * scale)
+    B = np.asfortranarray(rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs)))
+    Xnp = np.linalg.solve(A, B)
+    ctx.set_precision("fp64")
+    X = ctx.solve_linear(A, B)
+    assert ctx.last_stats["status"] == nat.OK and ctx.last_stats["info"] == 0
+    assert _rel(X, Xnp) <= 1e-12
     ctx.set_precision("mixed")
 
 
