@@ -46,6 +46,7 @@ EXPORTED = (
     "hprmat_b200_dev_counters", "hprmat_b200_dev_wave_trace", "hprmat_b200_dev_wave_trace_read",
     "hprmat_b200_dev_panel_trace_read", "hprmat_b200_dev_set_tuning", "hprmat_b200_dev_mesh",
     "hprmat_b200_dev_factorizations", "hprmat_b200_dev_wait_probe", "hprmat_b200_dev_binary_version",
+    "hprmat_b200_dev_zgemm",
 )
 
 
@@ -148,6 +149,7 @@ def load():
         "hprmat_b200_dev_factorizations": (ctypes.c_longlong, [P, I]),
         "hprmat_b200_dev_wait_probe": (I, [P, I]),
         "hprmat_b200_dev_binary_version": (I, []),
+        "hprmat_b200_dev_zgemm": (I, [P, P, ctypes.c_long, P, ctypes.c_long, P, ctypes.c_long, I, I, I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libhprmat_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
-SOURCES = ["solver.cu", "tc_gemm.cu", "tc_solve.cu", "noalloc.cu"]
+SOURCES = ["solver.cu", "tc_gemm.cu", "tc_solve.cu", "zgemm_f64.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-Xcompiler", "-Wall", "-Wno-deprecated-declarations"]
@@ -55,7 +55,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lcublas"]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -1,6 +1,5 @@
 // Host runtime of the B200 R-matrix solver: context, mesh, LU / solve drivers, FP64
 // refinement and the C ABI declared in include/hprmat_b200.h.
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 
@@ -27,6 +26,7 @@
 #include "rmat_kernels.cuh"
 #include "tc_gemm.cuh"
 #include "tc_solve.cuh"
+#include "zgemm_f64.cuh"
 
 using namespace hprmat;
 
@@ -148,7 +148,6 @@ struct hprmat_b200_ctx {
   DevBuf wfx, wfz, wfc, wfcf;
   DevBuf fpbuf;  // potential fingerprint (opts.reuse_factors)
   DevBuf cond_v;  // condition estimate: one right-hand side (opts.estimate_condition)
-  cublasHandle_t blas = nullptr;  // ZGEMM of the FP64 LU's trailing update (created on first use)
   // tensor-core operand views of the current factorisation (mixed path)
   TcOperand op_lu, op_bop, op_rhs, op_linv;
   long lup_ld = 0, lup_plane = 0, rop_plane = 0;
@@ -541,24 +540,13 @@ __global__ void wait_probe_kernel(int* counter, int* timeout_flag, unsigned limi
   grid_wait(counter, timeout_flag, 1u, 99, limit);
 }
 
-// C[M x N] -= A[M x K] B[K x N] in complex FP64 (column-major) by cuBLAS ZGEMM on the
-// context's stream; the handle is created on first use and kept by the context.
+// C[M x N] -= A[M x K] B[K x N] in complex FP64 (column-major) on the context's stream, by
+// this library's DMMA kernel (zgemm_f64.cu).
 static int zgemm_update(hprmat_b200_ctx* c, int M, int N, int K, const double2* A, long lda, const double2* B,
                         long ldb, double2* C, long ldc) {
-  if (!c->blas) {
-    const cublasStatus_t e = cublasCreate(&c->blas);
-    if (e != CUBLAS_STATUS_SUCCESS) {
-      c->blas = nullptr;
-      return fail(HPRMAT_B200_ERR_CUDA, "cublasCreate failed (status %d)", (int)e);
-    }
-  }
-  cublasStatus_t e = cublasSetStream(c->blas, c->stream);
-  const cuDoubleComplex minus_one = make_cuDoubleComplex(-1.0, 0.0), one = make_cuDoubleComplex(1.0, 0.0);
-  if (e == CUBLAS_STATUS_SUCCESS)
-    e = cublasZgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, M, N, K, &minus_one,
-                    reinterpret_cast<const cuDoubleComplex*>(A), (int)lda, reinterpret_cast<const cuDoubleComplex*>(B),
-                    (int)ldb, &one, reinterpret_cast<cuDoubleComplex*>(C), (int)ldc);
-  if (e != CUBLAS_STATUS_SUCCESS) return fail(HPRMAT_B200_ERR_CUDA, "cublasZgemm failed (status %d)", (int)e);
+  if (zgemm_f64_update(M, N, K, A, lda, B, ldb, C, ldc, c->stream))
+    return fail(HPRMAT_B200_ERR_CUDA, "FP64 complex GEMM update: %s", hprmat_b200_last_error());
+  ++c->launches;
   return HPRMAT_B200_OK;
 }
 
@@ -685,8 +673,7 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
         c->ev_used += 2;
       }
     } else if constexpr (std::is_same<T, double2>::value) {
-      // FP64 path: the trailing update is a plain complex GEMM, C -= A B, done by cuBLAS ZGEMM
-      // (the LU's own work -- panels, pivoting, U12 -- stays in this library's kernels)
+      // FP64 path: the trailing update C -= A B on the FP64 tensor cores (zgemm_f64.cu)
       if (M2 > 0) TRY(zgemm_update(c, M2, M2, ncols, W + (k0 + ncols) + (size_t)k0 * ld, ld,
                                    W + k0 + (size_t)(k0 + ncols) * ld, ld,
                                    W + (k0 + ncols) + (size_t)(k0 + ncols) * ld, ld));
@@ -1094,7 +1081,7 @@ static int apply_residual(hprmat_b200_ctx* c, const Operator& op, const double2*
       HPR_CUDA_TRY(cudaMemset2DAsync(out, ldo * sizeof(double2), 0, (size_t)N * sizeof(double2), ncol, c->stream));
     }
     LAUNCH_CHECK();
-    // dense operator (solve_linear, non-local potentials): a plain FP64 GEMM, by ZGEMM
+    // dense operator (solve_linear, non-local potentials): a plain FP64 GEMM (zgemm_f64.cu)
     TRY(zgemm_update(c, N, ncol, N, op.A, op.lda, X, ldx, out, ldo));
   }
   return HPRMAT_B200_OK;
@@ -2141,7 +2128,6 @@ int hprmat_b200_destroy(hprmat_b200_ctx* c) {
   c->scan_workers.clear();
   c->scan_cpot.clear();
   for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
-  if (c->blas) cublasDestroy(c->blas);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->h_norms) cudaFreeHost(c->h_norms);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -3295,6 +3281,15 @@ __global__ void split_planes_kernel(const float2* __restrict__ src, int rows, in
   dst[plane + idx] = lr;
   dst[2 * plane + idx] = hi;
   dst[3 * plane + idx] = li;
+}
+
+int hprmat_b200_dev_zgemm(hprmat_b200_ctx* c, const void* A, long lda, const void* B, long ldb, void* C, long ldc,
+                          int M, int N, int K) {
+  TRY(check_ctx(c));
+  if (!A || !B || !C || M <= 0 || N <= 0 || K <= 0) return fail(HPRMAT_B200_ERR_ARG, "dev_zgemm: invalid arguments");
+  TRY(zgemm_update(c, M, N, K, (const double2*)A, lda, (const double2*)B, ldb, (double2*)C, ldc));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return HPRMAT_B200_OK;
 }
 
 int hprmat_b200_dev_binary_version(void) {

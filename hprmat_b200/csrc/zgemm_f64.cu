@@ -1,0 +1,178 @@
+// Complex FP64 GEMM update C -= A B on the FP64 tensor cores (sm_100a DMMA).
+//
+// The plain FP64 path of the solver (the "plain FP64 device LU" the mixed path is measured
+// against, the mixed path's FP64 fallback, the condition estimate and the non-symmetric
+// adjoint) spends its O(N^3) work in one shape of product: C[M x N] -= A[M x K] B[K x N] with
+// complex double operands in column-major storage -- the LU's trailing update (K = the block
+// size), the block updates of its triangular solves, and the dense operator's residual
+// B - C X of the refinement (K = N).
+//
+// Each complex product is 4 real products on mma.sync.aligned.m8n8k4.f64 (DMMA):
+//   Re += Ar Br + (-Ai) Bi,   Im += Ar Bi + Ai Br,
+// FP64 products and FP64 accumulation throughout.  A CTA of 4 warps computes a 64 x 64
+// complex tile of C (each warp 32 x 32: 4 x 4 blocks of 8 x 8, Re and Im accumulators in
+// registers) over K in chunks of 16, staged in shared memory by cp.async in a 3-deep ring:
+//   A chunk as [k][m] (m contiguous, as A's columns), row stride 66 complex, and
+//   B chunk as [n][k] (k contiguous, as B's columns), row stride 20 complex,
+// so that the fragment loads -- one 16-byte (re, im) load per 8 x 4 A block and per 4 x 8 B
+// block -- hit 8 distinct 16-byte bank groups in every quarter warp.  Elements beyond M, N or K
+// are zero-filled by the copies (src-size 0) and never stored.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+#include "zgemm_f64.cuh"
+
+namespace hprmat {
+namespace {
+
+constexpr int kBM = 64, kBN = 64, kBK = 16;
+constexpr int kStages = 3;
+constexpr int kThreads = 128;
+constexpr int kALd = kBM + 2;  // complex elements per k row of the A stage
+constexpr int kBLd = kBK + 4;  // complex elements per n row of the B stage
+constexpr int kAStage = kBK * kALd;
+constexpr int kBStage = kBN * kBLd;
+constexpr size_t kSmemBytes = (size_t)kStages * (kAStage + kBStage) * sizeof(double2);
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc, bool valid) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+  const int n = valid ? 16 : 0;  // 0: nothing read, 16 zero bytes written
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gsrc), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// d += a b for one 8 x 8 x 4 FP64 block (fragments as mma.m8n8k4 .f64 lays them out: a at
+// row lane/4, column lane%4; b at row lane%4, column lane/4; d at row lane/4, columns
+// 2 (lane%4) and 2 (lane%4) + 1).
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+    zgemm_dmma_kernel(int M, int N, int K, const double2* __restrict__ A, long lda, const double2* __restrict__ B,
+                      long ldb, double2* __restrict__ C, long ldc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* As = reinterpret_cast<double2*>(smem_raw);
+  double2* Bs = As + kStages * kAStage;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+  const int nchunks = (K + kBK - 1) / kBK;
+
+  auto load_stage = [&](int stage, int kc) {
+    const int k0 = kc * kBK;
+    double2* as = As + stage * kAStage;
+    double2* bs = Bs + stage * kBStage;
+#pragma unroll
+    for (int i = 0; i < (kBM * kBK) / kThreads; ++i) {
+      const int idx = tid + i * kThreads;
+      const int k = idx / kBM, m = idx % kBM;
+      const bool ok = (m0 + m < M) && (k0 + k < K);
+      const double2* src = ok ? A + (size_t)(m0 + m) + (size_t)(k0 + k) * lda : A;
+      cp_async16(as + k * kALd + m, src, ok);
+    }
+#pragma unroll
+    for (int i = 0; i < (kBN * kBK) / kThreads; ++i) {
+      const int idx = tid + i * kThreads;
+      const int n = idx / kBK, k = idx % kBK;
+      const bool ok = (n0 + n < N) && (k0 + k < K);
+      const double2* src = ok ? B + (size_t)(k0 + k) + (size_t)(n0 + n) * ldb : B;
+      cp_async16(bs + n * kBLd + k, src, ok);
+    }
+  };
+
+  double accr[4][4][2], acci[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      accr[i][j][0] = accr[i][j][1] = 0.0;
+      acci[i][j][0] = acci[i][j][1] = 0.0;
+    }
+
+#pragma unroll
+  for (int s = 0; s < kStages - 1; ++s) {
+    if (s < nchunks) load_stage(s, s);
+    cp_async_commit();
+  }
+  const int fr = lane >> 2, fk = lane & 3;
+  for (int kc = 0; kc < nchunks; ++kc) {
+    cp_async_wait<kStages - 2>();
+    __syncthreads();
+    // refill the slot consumed in the previous iteration (every warp has passed the barrier)
+    if (kc + kStages - 1 < nchunks) load_stage((kc + kStages - 1) % kStages, kc + kStages - 1);
+    cp_async_commit();
+    const double2* as = As + (kc % kStages) * kAStage;
+    const double2* bs = Bs + (kc % kStages) * kBStage;
+#pragma unroll
+    for (int kk = 0; kk < kBK; kk += 4) {
+      double2 a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = as[(kk + fk) * kALd + wm + 8 * i + fr];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = bs[(wn + 8 * j + fr) * kBLd + kk + fk];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const double nai = -a[i].y;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          dmma(accr[i][j], a[i].x, b[j].x);
+          dmma(acci[i][j], a[i].x, b[j].y);
+          dmma(accr[i][j], nai, b[j].y);
+          dmma(acci[i][j], a[i].y, b[j].x);
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+  // C -= acc
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int row = m0 + wm + 8 * i + fr;
+    if (row >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int col = n0 + wn + 8 * j + 2 * fk + e;
+        if (col < N) {
+          double2* p = C + (size_t)row + (size_t)col * ldc;
+          double2 v = *p;
+          v.x -= accr[i][j][e];
+          v.y -= acci[i][j][e];
+          *p = v;
+        }
+      }
+    }
+  }
+}
+
+}  // namespace
+
+int zgemm_f64_update(int M, int N, int K, const double2* A, long lda, const double2* B, long ldb, double2* C,
+                     long ldc, cudaStream_t s) {
+  if (M <= 0 || N <= 0 || K <= 0) return 0;
+  if (((uintptr_t)A & 15) || ((uintptr_t)B & 15) || ((uintptr_t)C & 15) || lda < M || ldb < K || ldc < M) {
+    set_last_error_msg("zgemm_f64_update: misaligned operand or leading dimension too small");
+    return -1;
+  }
+  // per device and cheap next to a launch: set on every call (any thread, any device)
+  HPR_CUDA_TRY(cudaFuncSetAttribute(zgemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
+  const dim3 grid((unsigned)((M + kBM - 1) / kBM), (unsigned)((N + kBN - 1) / kBN));
+  if (grid.y > 65535u) {
+    set_last_error_msg("zgemm_f64_update: N too large for one launch");
+    return -5;
+  }
+  zgemm_dmma_kernel<<<grid, kThreads, kSmemBytes, s>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  HPR_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace hprmat

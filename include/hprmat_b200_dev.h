@@ -18,6 +18,12 @@ extern "C" {
 int hprmat_b200_dev_tc_update(hprmat_b200_ctx* ctx, const float* aop, const float* bop, long plane, int nb,
                               void* C, long ldc, int M, int Nc, int bn);
 
+/* C[M x N] -= A[M x K] B[K x N] in complex FP64 on the FP64 tensor cores (the DMMA kernel of the
+   FP64 path's trailing updates, solves and dense residuals): device pointers to interleaved
+   complex doubles, column-major with leading dimensions lda >= M, ldb >= K, ldc >= M. */
+int hprmat_b200_dev_zgemm(hprmat_b200_ctx* ctx, const void* A, long lda, const void* B, long ldb, void* C, long ldc,
+                          int M, int N, int K);
+
 /* Split complex float values into the 4 TF32 planes used by hprmat_b200_dev_tc_update:
    src is rows x nb (row-major complex float, i.e. K contiguous), dst gets 4 planes of
    rows x nb floats, `plane` floats apart. */

@@ -45,6 +45,32 @@ def test_kernels_report_sm100_binary():
     assert nat.load().hprmat_b200_dev_binary_version() == 100
 
 
+@pytest.mark.parametrize("M,N,K", [(64, 64, 16), (1, 1, 1), (77, 33, 5), (300, 129, 64), (1000, 700, 64),
+                                   (130, 8, 600), (2053, 37, 64), (4096, 1100, 64)])
+def test_fp64_zgemm_kernel_matches_torch(ctx, M, N, K):
+    """The FP64 path's complex GEMM update C -= A B (DMMA kernel) against torch's FP64 product,
+    with leading dimensions larger than the rows (sub-matrix views, as the LU passes them)."""
+    lib = nat.load()
+    g = torch.Generator(device="cpu").manual_seed(M * 7 + N * 3 + K)
+    lda, ldb, ldc = M + 3, K + 1, M + 5
+    A = torch.randn(K, lda, 2, generator=g, dtype=torch.float64)   # column-major complex (lda x K)
+    B = torch.randn(N, ldb, 2, generator=g, dtype=torch.float64)
+    C = torch.randn(N, ldc, 2, generator=g, dtype=torch.float64)
+    dA, dB, dC = A.cuda(), B.cuda(), C.cuda()
+    nat.check(lib.hprmat_b200_dev_zgemm(ctx._h, dA.data_ptr(), lda, dB.data_ptr(), ldb, dC.data_ptr(), ldc, M, N, K))
+    Az = torch.complex(A[..., 0], A[..., 1]).T[:M, :K]
+    Bz = torch.complex(B[..., 0], B[..., 1]).T[:K, :N]
+    Cz = torch.complex(C[..., 0], C[..., 1]).T
+    ref = Cz.clone()
+    ref[:M, :N] -= Az @ Bz
+    got = dC.cpu()
+    got = torch.complex(got[..., 0], got[..., 1]).T
+    assert torch.equal(got[M:, :], ref[M:, :])  # rows beyond M untouched
+    err = (got - ref).abs().max().item()
+    scale = (Az.abs() @ Bz.abs()).max().item()
+    assert err <= 1e-14 * scale, (err, scale)
+
+
 # ---------------------------------------------------------------- tensor-core kernel
 @pytest.mark.parametrize("M,Nc,nb,bn", [(128, 256, 128, 256), (300, 520, 128, 256), (1000, 700, 64, 256),
                                         (77, 33, 32, 256), (640, 128, 128, 128), (129, 200, 64, 128),
