@@ -62,6 +62,10 @@ def parse():
                     help="scan/adjoint: keep a block's factorisation across energies as the refinement's "
                          "preconditioner (opts.reuse_factors); default off (measured faster that way for "
                          "both workloads)")
+    ap.add_argument("--scan-method", choices=["lu", "shifted"], default="lu",
+                    help="scan: lu (every energy by its own mixed LU on concurrent worker streams) or shifted (one "
+                         "Hessenberg reduction per J-pi block, O(N^2 nch) FP64 work per energy, "
+                         "hprmat_b200_rmatrix_scan_shifted)")
     ap.add_argument("--autotune", type=int, default=0,
                     help="scan: run the scan autotuner (hprmat_b200_scan_autotune) on the scan's blocks before "
                          "the warm-up, outside the timed region")
@@ -239,7 +243,7 @@ def run_scan(args):
                     json.dump({"device": _t.cuda.get_device_name(local), "workers": args.workers, "table": table}, f)
     for _ in range(args.warmup):
         ctx.rmatrix_scan(inputs[:1], 20.0, 60, nworkers=args.workers, allow_unconverged=True,
-                         raise_on_unit_error=False)
+                         raise_on_unit_error=False, method=args.scan_method)
     lib.hprmat_b200_dev_factorizations(ctx._h, 1)
     secs = []
     res = None
@@ -247,7 +251,7 @@ def run_scan(args):
         if world > 1:
             dist.barrier()
         res = ctx.rmatrix_scan(inputs, 20.0, 60, nworkers=args.workers, allow_unconverged=True,
-                               raise_on_unit_error=False)
+                               raise_on_unit_error=False, method=args.scan_method)
         secs.append(ctx.last_scan_seconds)
     t = max(secs) / 1.0
     t_local = torch.tensor([sum(secs)], dtype=torch.float64, device=f"cuda:{local}")
@@ -297,10 +301,13 @@ def run_scan(args):
         print(json.dumps({
             "metric": "scan solves/s", "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": "c64 via 3xTF32 tensor cores + c128 refinement",
+            "scaling": "strong", "vs_baseline": None,
+            "dtype": ("c128 (Hessenberg reduction, shifted solves, FP64 refinement)" if args.scan_method == "shifted"
+                      else "c64 via 3xTF32 tensor cores + c128 refinement"),
             "data": "synthetic (seeded scan generator, hprmat_b200/workloads.py)",
             "config": {"workload": "batched energy scan: 12 J-pi blocks, nch ~ U{4..64} x 60 points "
                                    "(N = 240..3840), 256 energies each, 3072 solves",
+                       "method": args.scan_method,
                        "workers": args.workers, "reuse_factors": bool(args.reuse),
                        "autotune": bool(args.autotune)},
             "autotune": tune,

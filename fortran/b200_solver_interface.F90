@@ -37,7 +37,8 @@ module b200_solver_interface
   public :: hprmat_b200_set_stream, hprmat_b200_rmat_ini, hprmat_b200_rmatrix, hprmat_b200_rmatrix_device
   public :: hprmat_b200_rmatrix_wf, hprmat_b200_rmatrix_full, hprmat_b200_solve_linear
   public :: hprmat_b200_solve_linear_device, hprmat_b200_solve_rmatrix, hprmat_b200_boundary
-  public :: hprmat_b200_rmatrix_adjoint, hprmat_b200_rmatrix_scan, hprmat_b200_solve_linear_noalloc
+  public :: hprmat_b200_rmatrix_adjoint, hprmat_b200_rmatrix_scan, hprmat_b200_rmatrix_scan_shifted
+  public :: hprmat_b200_solve_linear_noalloc
   public :: hprmat_b200_status_string, hprmat_b200_last_error, hprmat_b200_version
   public :: B200_OK, B200_NOT_CONVERGED, B200_PREC_FP64, B200_PREC_MIXED, B200_ABI_VERSION
 
@@ -244,6 +245,17 @@ module b200_solver_interface
       type(b200_scan_block), intent(in) :: blocks(*)
       real(c_double), value :: rmax
       integer(c_int), value :: nr, nworkers
+      real(c_double), intent(out) :: seconds
+    end function
+
+    integer(c_int) function hprmat_b200_rmatrix_scan_shifted(ctx, nblocks, blocks, rmax, nr, seconds) &
+        bind(C, name="hprmat_b200_rmatrix_scan_shifted")
+      import :: c_int, c_ptr, c_double, b200_scan_block
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: nblocks
+      type(b200_scan_block), intent(in) :: blocks(*)
+      real(c_double), value :: rmax
+      integer(c_int), value :: nr
       real(c_double), intent(out) :: seconds
     end function
 

@@ -37,7 +37,7 @@ EXPORTED = (
     "gpu_b200_solve_mixed_", "gpu_b200_solve_double_", "gpu_b200_finalize_", "hprmat_b200_status_string",
     "hprmat_b200_last_error", "hprmat_b200_version", "hprmat_b200_boundary",
     "hprmat_b200_solve_linear_noalloc", "hprmat_b200_rmatrix_scan", "hprmat_b200_scan_autotune",
-    "hprmat_b200_scan_tune_get", "hprmat_b200_scan_tune_set",
+    "hprmat_b200_scan_tune_get", "hprmat_b200_scan_tune_set", "hprmat_b200_rmatrix_scan_shifted",
     "hprmat_b200_rmatrix_adjoint", "hprmat_b200_rmatrix_wf", "hprmat_b200_rmatrix_wf_device",
     "hprmat_b200_wf_print", "hprmat_b200_rmatrix_full", "hprmat_b200_rmatrix_x", "hprmat_b200_adjoint_from_x",
     "hprmat_b200_rmatrix_x_device", "hprmat_b200_adjoint_from_x_device",
@@ -46,7 +46,7 @@ EXPORTED = (
     "hprmat_b200_dev_counters", "hprmat_b200_dev_wave_trace", "hprmat_b200_dev_wave_trace_read",
     "hprmat_b200_dev_panel_trace_read", "hprmat_b200_dev_set_tuning", "hprmat_b200_dev_mesh",
     "hprmat_b200_dev_factorizations", "hprmat_b200_dev_wait_probe", "hprmat_b200_dev_binary_version",
-    "hprmat_b200_dev_zgemm",
+    "hprmat_b200_dev_zgemm", "hprmat_b200_dev_hessenberg",
 )
 
 
@@ -114,6 +114,7 @@ def load():
         "hprmat_b200_rmatrix_device": (I, [P, I, IP, DP, DP, D, I, I, P, I, I, P, IP, SP]),
         "hprmat_b200_rmatrix_scan": (I, [P, I, ctypes.POINTER(ScanBlock), D, I, I, DP]),
         "hprmat_b200_scan_autotune": (I, [P, I, ctypes.POINTER(ScanBlock), D, I, I, DP]),
+        "hprmat_b200_rmatrix_scan_shifted": (I, [P, I, ctypes.POINTER(ScanBlock), D, I, DP]),
         "hprmat_b200_scan_tune_get": (I, [P, IP, DP, I]),
         "hprmat_b200_scan_tune_set": (I, [P, IP, I]),
         "hprmat_b200_rmatrix_adjoint": (I, [P, I, IP, DP, DP, D, I, I, DP, I, I, DP, DP, IP, DP, SP]),
@@ -150,6 +151,7 @@ def load():
         "hprmat_b200_dev_wait_probe": (I, [P, I]),
         "hprmat_b200_dev_binary_version": (I, []),
         "hprmat_b200_dev_zgemm": (I, [P, P, ctypes.c_long, P, ctypes.c_long, P, ctypes.c_long, I, I, I]),
+        "hprmat_b200_dev_hessenberg": (I, [P, P, ctypes.c_long, I, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -169,17 +169,26 @@ class Context:
         nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))
         return cu, nopen.value
 
-    def rmatrix_scan(self, blocks, rmax, nr, nworkers=0, allow_unconverged=False, raise_on_unit_error=True):
+    def rmatrix_scan(self, blocks, rmax, nr, nworkers=0, allow_unconverged=False, raise_on_unit_error=True,
+                     method="lu"):
         """Batched energy scan.  ``blocks``: sequence of (lval, cpot, qk, eta) with qk/eta of
         shape (nenergies, nch), cpot (ncp1, nch, nch) complex, Fortran order.  Returns a list of
         (cu (nenergies, nch, nch) with U in cu[e, :nopen, :nopen], nopen (nenergies,),
-        status (nenergies,)) and sets ``last_scan_seconds``."""
+        status (nenergies,)) and sets ``last_scan_seconds``.  ``method``: "lu" (every energy
+        by its own LU on concurrent worker streams, hprmat_b200_rmatrix_scan) or "shifted" (one
+        Hessenberg reduction per block and O(N^2 nch) per energy, hprmat_b200_rmatrix_scan_shifted)."""
         keep, arr, out = self._scan_blocks(blocks)
         self._ensure_mesh(nr, 1, rmax)
         blocks_c = (nat.ScanBlock * len(arr))(*arr)
         secs = ctypes.c_double(0.0)
-        s = self._lib.hprmat_b200_rmatrix_scan(self._h, len(arr), blocks_c, float(rmax), int(nr), int(nworkers),
-                                               ctypes.byref(secs))
+        if method == "shifted":
+            s = self._lib.hprmat_b200_rmatrix_scan_shifted(self._h, len(arr), blocks_c, float(rmax), int(nr),
+                                                           ctypes.byref(secs))
+        elif method == "lu":
+            s = self._lib.hprmat_b200_rmatrix_scan(self._h, len(arr), blocks_c, float(rmax), int(nr), int(nworkers),
+                                                   ctypes.byref(secs))
+        else:
+            raise ValueError(f"unknown scan method {method!r}")
         self.last_scan_seconds = secs.value
         if raise_on_unit_error:
             nat.check(s, (nat.OK, nat.NOT_CONVERGED) if allow_unconverged else (nat.OK,))

@@ -1,0 +1,565 @@
+// Kernels of the shifted (Hessenberg) energy scan.
+//
+// Between the energies of one J-pi block the R-matrix C(E) changes only by a multiple of the
+// identity and by the closed channels' Bloch terms, which are rank one per channel:
+//   C(E) = C0 + delta(E) I + Q D(E) Q^T,   Q = blockdiag(q2) (N x nch),
+// delta(E) the common change of the diagonal energy term (-k_c^2 for open, +k_c^2 for closed
+// channels: -(E - threshold_c)/hm for every c), D(E) = diag(-xc_c / a) over the closed channels
+// (the device Bloch matrix of one interval is q2 q2^T).  C0 is reduced once to upper Hessenberg
+// form by Householder similarity transformations, C0 = P H P^H (P unitary); then for every
+// energy (H + delta I) Y = P^H Q costs O(N^2 nch) (an LU of a Hessenberg matrix needs only
+// row-pair pivoting and N - 1 eliminations) instead of the O(N^3) LU of C(E), and the Bloch
+// terms enter through the Woodbury identity on the nch x nch matrix S = Q^T P Y:
+//   Q^T C(E)^-1 Q = S (I + D S)^-1,   C(E)^-1 Q = P Y T,   T = I - D (I + S D)^-1 S.
+// The reduction is backward stable in norm only (entries of C0 span many orders of magnitude),
+// so every energy then takes FP64 refinement steps against the structured C(E) (r = Q - C(E) X,
+// correction through the same Hessenberg factors).
+//
+// Householder convention: for x (m entries) with ||x|| > 0, gamma = -e^{i arg x0} ||x|| and
+// u = (x - gamma e1) / ||x - gamma e1||; H = I - 2 u u^H is Hermitian and unitary with
+// H x = gamma e1, and A <- H A H is a similarity.  After the steps k = 0 .. N-3,
+// C0 = P H_final P^H with P = H_0 H_1 ... H_{N-3}.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace hprmat {
+
+constexpr int kHessThreads = 256;
+
+__device__ __forceinline__ double2 hz_conj(double2 a) { return make_double2(a.x, -a.y); }
+
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < NT / 32 ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) red[0] = v;
+  }
+  __syncthreads();
+  const double out = red[0];
+  __syncthreads();
+  return out;
+}
+
+// Reflector of column k of A (N x N, column-major, lda): x = A[k+1 .., k], m = N - k - 1 >= 2.
+// Writes u into ustore[k+1 .., k] (column k of the reflector store; u = 0 when x = 0) and
+// replaces the column by gamma e1.  One CTA.
+__global__ void __launch_bounds__(kHessThreads) hess_reflector_kernel(double2* A, long lda, int N, int k,
+                                                                      double2* ustore, long ldu) {
+  __shared__ double red[32];
+  const int m = N - k - 1;
+  double2* x = A + (size_t)k * lda + (k + 1);
+  double2* u = ustore + (size_t)k * ldu + (k + 1);
+  double ss = 0.0;
+  for (int i = threadIdx.x; i < m; i += kHessThreads) ss += x[i].x * x[i].x + x[i].y * x[i].y;
+  ss = block_sum<kHessThreads>(ss, red);
+  const double2 x0 = x[0];
+  __syncthreads();  // every thread has read x0 before thread 0 overwrites it
+  if (ss == 0.0) {
+    for (int i = threadIdx.x; i < m; i += kHessThreads) u[i] = make_double2(0.0, 0.0);
+    return;
+  }
+  const double nrm = sqrt(ss);
+  const double a0 = hypot(x0.x, x0.y);
+  const double2 ph = a0 > 0.0 ? make_double2(x0.x / a0, x0.y / a0) : make_double2(1.0, 0.0);
+  const double2 gamma = make_double2(-ph.x * nrm, -ph.y * nrm);
+  // ||x - gamma e1||^2 = 2 ||x||^2 + 2 ||x|| |x0|
+  const double winv = 1.0 / sqrt(2.0 * ss + 2.0 * nrm * a0);
+  for (int i = threadIdx.x; i < m; i += kHessThreads) {
+    double2 w = x[i];
+    if (i == 0) {
+      w.x -= gamma.x;
+      w.y -= gamma.y;
+    }
+    u[i] = make_double2(w.x * winv, w.y * winv);
+    x[i] = i == 0 ? gamma : make_double2(0.0, 0.0);
+  }
+}
+
+// A[r0 .., c] <- H A[r0 .., c] for the columns c in [c0, N) of A (column-major, lda), H = I - 2 u u^H
+// with u the m = N - r0 entries of column k of the reflector store (rows r0 ..): per column
+// w = u^H A[r0.., c], A[r0.., c] -= 2 u w.  One warp per column.
+__global__ void __launch_bounds__(kHessThreads) hess_left_kernel(double2* A, long lda, int N, int r0, int c0,
+                                                                 const double2* ustore, long ldu, int k) {
+  const int warp = (blockIdx.x * kHessThreads + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int c = c0 + warp;
+  if (c >= N) return;
+  const int m = N - r0;
+  const double2* u = ustore + (size_t)k * ldu + r0;
+  double2* a = A + (size_t)c * lda + r0;
+  double wr = 0.0, wi = 0.0;  // sum conj(u_i) a_i
+  for (int i = lane; i < m; i += 32) {
+    const double2 ui = u[i], ai = a[i];
+    wr += ui.x * ai.x + ui.y * ai.y;
+    wi += ui.x * ai.y - ui.y * ai.x;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    wr += __shfl_xor_sync(0xffffffffu, wr, o);
+    wi += __shfl_xor_sync(0xffffffffu, wi, o);
+  }
+  wr *= 2.0;
+  wi *= 2.0;
+  for (int i = lane; i < m; i += 32) {
+    const double2 ui = u[i];
+    double2 ai = a[i];
+    ai.x -= ui.x * wr - ui.y * wi;
+    ai.y -= ui.x * wi + ui.y * wr;
+    a[i] = ai;
+  }
+}
+
+// Right application A[:, k+1 ..] <- A[:, k+1 ..] H, rows 0 .. N-1: first p = A[:, k+1 ..] u in
+// column chunks (part[chunk][row]), then A_ij -= 2 p_i conj(u_j).  Grid (row blocks of 256,
+// column chunks of kHessChunk).
+constexpr int kHessChunk = 128;
+__global__ void __launch_bounds__(kHessThreads) hess_right_partial_kernel(const double2* __restrict__ A, long lda,
+                                                                          int N, int k, const double2* ustore,
+                                                                          long ldu, double2* part) {
+  const int row = blockIdx.x * kHessThreads + threadIdx.x;
+  const int j0 = k + 1 + blockIdx.y * kHessChunk;
+  const int j1 = min(j0 + kHessChunk, N);
+  __shared__ double2 us[kHessChunk];
+  for (int j = j0 + threadIdx.x; j < j1; j += kHessThreads) us[j - j0] = ustore[(size_t)k * ldu + j];
+  __syncthreads();
+  if (row >= N) return;
+  double pr = 0.0, pi = 0.0;
+  for (int j = j0; j < j1; ++j) {
+    const double2 a = A[(size_t)j * lda + row], u = us[j - j0];
+    pr += a.x * u.x - a.y * u.y;
+    pi += a.x * u.y + a.y * u.x;
+  }
+  part[(size_t)blockIdx.y * N + row] = make_double2(pr, pi);
+}
+
+__global__ void __launch_bounds__(kHessThreads) hess_right_update_kernel(double2* A, long lda, int N, int k,
+                                                                         const double2* ustore, long ldu,
+                                                                         const double2* __restrict__ part,
+                                                                         int nchunks) {
+  const int row = blockIdx.x * kHessThreads + threadIdx.x;
+  const int j0 = k + 1 + blockIdx.y * kHessChunk;
+  const int j1 = min(j0 + kHessChunk, N);
+  __shared__ double2 us[kHessChunk];
+  for (int j = j0 + threadIdx.x; j < j1; j += kHessThreads) us[j - j0] = ustore[(size_t)k * ldu + j];
+  __syncthreads();
+  if (row >= N) return;
+  double pr = 0.0, pi = 0.0;
+  for (int c = 0; c < nchunks; ++c) {
+    const double2 v = part[(size_t)c * N + row];
+    pr += v.x;
+    pi += v.y;
+  }
+  pr *= 2.0;
+  pi *= 2.0;
+  for (int j = j0; j < j1; ++j) {
+    const double2 u = us[j - j0];
+    double2 a = A[(size_t)j * lda + row];
+    // a -= p conj(u)
+    a.x -= pr * u.x + pi * u.y;
+    a.y -= pi * u.x - pr * u.y;
+    A[(size_t)j * lda + row] = a;
+  }
+}
+
+// dst (row-major, ldd) = the upper Hessenberg part of src (column-major, lds) plus nothing else;
+// and PH (column-major, ldp) = P^H.  Grid (N / 32, N / 32), block (32, 8).
+__global__ void hess_transpose_kernel(const double2* __restrict__ src, long lds, int N, double2* dst, long ldd,
+                                      bool conj_, bool hessenberg_only) {
+  __shared__ double2 tile[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  for (int j = threadIdx.y; j < 32; j += 8) {
+    const int r = bx + threadIdx.x, c = by + j;
+    if (r < N && c < N) {
+      double2 v = src[(size_t)c * lds + r];
+      if (hessenberg_only && r > c + 1) v = make_double2(0.0, 0.0);
+      tile[j][threadIdx.x] = conj_ ? hz_conj(v) : v;
+    }
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += 8) {
+    const int r = by + threadIdx.x, c = bx + j;  // dst element (row c of src's transpose)
+    if (r < N && c < N) dst[(size_t)c * ldd + r] = tile[threadIdx.x][j];
+  }
+}
+
+// A (column-major, lda) = identity (N x N).
+__global__ void identity_kernel(double2* A, long lda, int N) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (r < N) A[(size_t)c * lda + r] = make_double2(r == c ? 1.0 : 0.0, 0.0);
+}
+
+// W (column-major, ldw) = P^H Q for Q = blockdiag(q2) (nch blocks of nr rows): W[i, c] =
+// sum_r PH[i, c nr + r] q2[r].  Grid (N / 256, nch).
+__global__ void hess_wq_kernel(const double2* __restrict__ PH, long ldp, int N, int nr, const double* __restrict__ q2,
+                               double2* W, long ldw) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (i >= N) return;
+  double wr = 0.0, wi = 0.0;
+  for (int r = 0; r < nr; ++r) {
+    const double2 p = PH[(size_t)(c * nr + r) * ldp + i];
+    wr += p.x * q2[r];
+    wi += p.y * q2[r];
+  }
+  W[(size_t)c * ldw + i] = make_double2(wr, wi);
+}
+
+// WH (column-major nch x N, ldwh) = W^H = (P^H Q)^H = Q^T P: WH[c, i] = sum_r q2[r] P[c nr + r, i].
+// Grid (N / 256, nch).
+__global__ void hess_whq_kernel(const double2* __restrict__ P, long ldp, int N, int nr, const double* __restrict__ q2,
+                                double2* WH, long ldwh) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (i >= N) return;
+  double wr = 0.0, wi = 0.0;
+  const double2* col = P + (size_t)i * ldp + (size_t)c * nr;
+  for (int r = 0; r < nr; ++r) {
+    wr += col[r].x * q2[r];
+    wi += col[r].y * q2[r];
+  }
+  WH[(size_t)i * ldwh + c] = make_double2(wr, wi);
+}
+
+// ---------------------------------------------------------------- per-energy Hessenberg solves
+// One CTA per unit (energy): the LU of Hs = H + delta I (H upper Hessenberg, row-major Hr,
+// ldh) with partial pivoting between the two candidate rows of each column (the larger
+// |re| + |im|, the working row on ties, as izamax), applied to the nch right-hand sides of
+// W (column-major, ldw; shared by all units); then back substitution.  Per unit (stride
+// arguments): the upper factor Ue (row-major, ldh), the multipliers lm[k] and row swaps sw[k]
+// of step k, and the solution Y (column-major, ldy).  info[u] = first zero pivot (1-based).
+struct HessSolveArgs {
+  const double2* Hr;
+  long ldh;
+  int N, nch;
+  const double* delta;   // [units]
+  const double2* W;      // RHS (forward solve) or nullptr: refine from Y's own content
+  long ldw;
+  double2* Ue;           // [units] N x ldh row-major
+  long sUe;
+  double2* lm;           // [units] N
+  int* sw;               // [units] N
+  double2* Y;            // [units] N x nch column-major, ldy
+  long ldy, sY;
+  int* info;             // [units]
+};
+
+constexpr int kHsRows = 32;   // rows per back-substitution block
+constexpr int kHsMaxRhs = 64;
+
+// Back substitution Y = Ue^-1 Z in place on the unit's Y (column-major, ldy).  Blocks of 32
+// rows from the bottom: the block's rows minus Ue[rows, below] Y[below] (each thread 2 rows x 4
+// right-hand sides, 32-column chunks staged in shared memory), then the 32 x 32 triangle.
+__device__ void hess_back_substitute(const double2* Ue, long ldh, int N, int nch, double2* Y, long ldy,
+                                     double2* smem) {
+  double2* us = smem;                          // [32][33] Ue tile (row-major)
+  double2* ys = us + kHsRows * (kHsRows + 1);  // [32][kHsMaxRhs] Y chunk rows
+  double2* acc_s = ys + kHsRows * kHsMaxRhs;   // [32][kHsMaxRhs] block accumulators
+  const int tid = threadIdx.x;
+  const int rp = tid / 16, cq = tid % 16;      // row pair, column quad
+  const int nblk = (N + kHsRows - 1) / kHsRows;
+  for (int b = nblk - 1; b >= 0; --b) {
+    const int k0 = b * kHsRows, k1 = min(k0 + kHsRows, N);
+    double2 acc[2][4];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = k0 + 2 * rp + a, c = 4 * cq + q;
+        acc[a][q] = (r < k1 && c < nch) ? Y[(size_t)c * ldy + r] : make_double2(0.0, 0.0);
+      }
+    for (int j0 = k1; j0 < N; j0 += kHsRows) {
+      const int jn = min(kHsRows, N - j0);
+      __syncthreads();
+      for (int idx = tid; idx < kHsRows * kHsRows; idx += kHessThreads) {
+        const int r = idx / kHsRows, j = idx % kHsRows;
+        us[r * (kHsRows + 1) + j] =
+            (k0 + r < k1 && j < jn) ? Ue[(size_t)(k0 + r) * ldh + j0 + j] : make_double2(0.0, 0.0);
+      }
+      for (int idx = tid; idx < kHsRows * nch; idx += kHessThreads) {
+        const int j = idx % kHsRows, c = idx / kHsRows;
+        ys[j * kHsMaxRhs + c] = j < jn ? Y[(size_t)c * ldy + j0 + j] : make_double2(0.0, 0.0);
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int j = 0; j < kHsRows; ++j) {
+        const double2 u0 = us[(2 * rp) * (kHsRows + 1) + j], u1 = us[(2 * rp + 1) * (kHsRows + 1) + j];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double2 y = ys[j * kHsMaxRhs + 4 * cq + q];
+          cfms(acc[0][q], u0, y);
+          cfms(acc[1][q], u1, y);
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc_s[(2 * rp + a) * kHsMaxRhs + 4 * cq + q] = acc[a][q];
+    for (int idx = tid; idx < kHsRows * kHsRows; idx += kHessThreads) {
+      const int r = idx / kHsRows, j = idx % kHsRows;
+      us[r * (kHsRows + 1) + j] = (k0 + r < k1 && k0 + j < k1) ? Ue[(size_t)(k0 + r) * ldh + k0 + j]
+                                                                 : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    // the triangle, one right-hand side per thread
+    if (tid < nch) {
+      for (int r = k1 - k0 - 1; r >= 0; --r) {
+        double2 v = acc_s[r * kHsMaxRhs + tid];
+        for (int j = r + 1; j < k1 - k0; ++j) cfms(v, us[r * (kHsRows + 1) + j], acc_s[j * kHsMaxRhs + tid]);
+        const double2 d = us[r * (kHsRows + 1) + r];
+        v = (d.x == 0.0 && d.y == 0.0) ? make_double2(0.0, 0.0) : cdiv(v, d);
+        acc_s[r * kHsMaxRhs + tid] = v;
+        Y[(size_t)tid * ldy + k0 + r] = v;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+constexpr size_t kHessSolveSmem =
+    ((size_t)kHsRows * (kHsRows + 1) + 2 * (size_t)kHsRows * kHsMaxRhs) * sizeof(double2);
+
+// Factor and solve (W given) or re-solve with the stored factors (W == nullptr: the unit's Y
+// holds the right-hand sides).  Dynamic shared memory: max(kHessSolveSmem, N complex) bytes.
+__global__ void __launch_bounds__(kHessThreads) hess_solve_kernel(HessSolveArgs a) {
+  extern __shared__ __align__(16) double2 hsm[];
+  const int unit = blockIdx.x;
+  const int N = a.N, nch = a.nch, tid = threadIdx.x;
+  double2* Ue = a.Ue + (size_t)unit * a.sUe;
+  double2* lm = a.lm + (size_t)unit * N;
+  int* sw = a.sw + (size_t)unit * N;
+  double2* Y = a.Y + (size_t)unit * a.sY;
+  if (a.W != nullptr) {
+    // LU of Hs with the working row in shared memory; the right-hand sides follow row by row
+    const double dl = a.delta[unit];
+    double2* cur = hsm;  // working row, columns k .. N-1
+    __shared__ int s_info;
+    for (int j = tid; j < N; j += kHessThreads) {
+      double2 v = a.Hr[j];
+      if (j == 0) v.x += dl;
+      cur[j] = v;
+    }
+    // right-hand-side working row (thread c < nch keeps column c)
+    double2 zc = tid < nch ? a.W[(size_t)tid * a.ldw] : make_double2(0.0, 0.0);
+    if (tid == 0) s_info = 0;
+    __syncthreads();
+    for (int k = 0; k < N - 1; ++k) {
+      const double2* hn = a.Hr + (size_t)(k + 1) * a.ldh;  // row k + 1 of H (columns k ..)
+      double2 bk = hn[k];
+      const double2 ak = cur[k];
+      const bool swap = (fabs(bk.x) + fabs(bk.y)) > (fabs(ak.x) + fabs(ak.y));
+      const double2 piv = swap ? bk : ak, oth = swap ? ak : bk;
+      const bool zero = piv.x == 0.0 && piv.y == 0.0;
+      const double2 l = zero ? make_double2(0.0, 0.0) : cdiv(oth, piv);
+      if (zero && tid == 0 && s_info == 0) s_info = k + 1;
+      for (int j = k + tid; j < N; j += kHessThreads) {
+        double2 b = hn[j];
+        if (j == k + 1) b.x += dl;
+        const double2 c = cur[j];
+        const double2 p = swap ? b : c, o = swap ? c : b;
+        Ue[(size_t)k * a.ldh + j] = p;
+        if (j > k) {
+          double2 nv = o;
+          cfms(nv, l, p);
+          cur[j] = nv;
+        }
+      }
+      if (tid == 0) {
+        lm[k] = l;
+        sw[k] = swap ? 1 : 0;
+      }
+      if (tid < nch) {
+        const double2 zb = a.W[(size_t)tid * a.ldw + k + 1];
+        const double2 zp = swap ? zb : zc, zo = swap ? zc : zb;
+        Y[(size_t)tid * a.ldy + k] = zp;
+        double2 nz = zo;
+        cfms(nz, l, zp);
+        zc = nz;
+      }
+      __syncthreads();
+    }
+    if (tid == 0) {
+      const double2 d = cur[N - 1];
+      Ue[(size_t)(N - 1) * a.ldh + (N - 1)] = d;
+      if (d.x == 0.0 && d.y == 0.0 && s_info == 0) s_info = N;
+      a.info[unit] = s_info;
+    }
+    if (tid < nch) Y[(size_t)tid * a.ldy + N - 1] = zc;
+    __syncthreads();
+  } else {
+    // forward elimination of the unit's right-hand sides with the stored steps
+    if (tid < nch) {
+      double2* y = Y + (size_t)tid * a.ldy;
+      double2 zc = y[0];
+      for (int k = 0; k < N - 1; ++k) {
+        const double2 zb = y[k + 1];
+        const bool swap = sw[k] != 0;
+        const double2 zp = swap ? zb : zc, zo = swap ? zc : zb;
+        y[k] = zp;
+        double2 nz = zo;
+        cfms(nz, lm[k], zp);
+        zc = nz;
+      }
+      y[N - 1] = zc;
+    }
+    __syncthreads();
+  }
+  hess_back_substitute(Ue, a.ldh, N, nch, Y, a.ldy, hsm);
+}
+
+// ---------------------------------------------------------------- per-unit Woodbury terms
+// One CTA per unit, nch <= 64, matrices column-major nch x nch with stride nch^2 per unit.
+// mode 0 (after the first solve; S given as -S by the preceding GEMM):
+//   F = (I + S D)^-1 S,  T = I - D F  (-> Tout),  R0 = S T = S - S D F  (-> Rout)
+// mode 1 (refinement correction G = W^H y_r): Delta = (I + S D)^-1 G, Rout += Delta, and the
+//   relative change ||Delta||_F / ||Rout||_F into chg[unit]; Delta also to Dout (for X updates).
+// Gaussian elimination with partial pivoting (|re| + |im|) in shared memory.
+__global__ void __launch_bounds__(kHessThreads) hess_woodbury_kernel(int nch, const double2* Sneg, const double* D,
+                                                                     int ldD, int mode, const double2* G,
+                                                                     double2* Tout, double2* Rout, double2* Dout,
+                                                                     double* chg, int* info) {
+  extern __shared__ __align__(16) double2 wsm[];
+  const int unit = blockIdx.x, tid = threadIdx.x;
+  const size_t nn = (size_t)nch * nch;
+  const double2* Sg = Sneg + unit * nn;
+  const double* d = D + (size_t)unit * ldD;
+  double2* M = wsm;           // I + S D (column-major)
+  double2* Bm = M + nn;       // right-hand sides (nch columns)
+  double2* Sv = Bm + nn;      // S
+  __shared__ int piv_row;
+  __shared__ double red[32];
+  for (int idx = tid; idx < (int)nn; idx += kHessThreads) {
+    const int r = idx % nch, c = idx / nch;
+    const double2 s = make_double2(-Sg[idx].x, -Sg[idx].y);
+    Sv[idx] = s;
+    double2 m = make_double2(s.x * d[c], s.y * d[c]);
+    if (r == c) m.x += 1.0;
+    M[idx] = m;
+    Bm[idx] = mode == 0 ? s : G[unit * nn + idx];
+  }
+  __syncthreads();
+  // elimination, column j: pivot search by warp 0, swap, eliminate below
+  for (int j = 0; j < nch; ++j) {
+    if (tid < 32) {
+      double bv = -1.0;
+      int bi = j;
+      for (int r = j + tid; r < nch; r += 32) {
+        const double v = fabs(M[j * nch + r].x) + fabs(M[j * nch + r].y);
+        if (v > bv || (v == bv && r < bi)) {
+          bv = v;
+          bi = r;
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_down_sync(0xffffffffu, bv, o);
+        const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ov > bv || (ov == bv && oi < bi)) {
+          bv = ov;
+          bi = oi;
+        }
+      }
+      if (tid == 0) piv_row = bi;
+    }
+    __syncthreads();
+    const int p = piv_row;
+    if (p != j)
+      for (int c = tid; c < 2 * nch; c += kHessThreads) {
+        double2* base = c < nch ? M + (size_t)c * nch : Bm + (size_t)(c - nch) * nch;
+        const double2 t = base[j];
+        base[j] = base[p];
+        base[p] = t;
+      }
+    __syncthreads();
+    const double2 pv = M[j * nch + j];
+    if (pv.x == 0.0 && pv.y == 0.0) {
+      if (tid == 0) info[unit] = j + 1;
+      continue;
+    }
+    // rows r > j: l_r = M[r, j] / pv; row r -= l_r row j (columns > j of M and all of Bm)
+    for (int idx = tid; idx < (nch - j - 1) * (2 * nch - j - 1); idx += kHessThreads) {
+      const int r = j + 1 + idx % (nch - j - 1);
+      const int cc = j + 1 + idx / (nch - j - 1);  // column index over [M cols j+1.. | Bm cols]
+      const double2 l = cdiv(M[j * nch + r], pv);
+      double2* col = cc < nch ? M + (size_t)cc * nch : Bm + (size_t)(cc - nch) * nch;
+      double2 v = col[r];
+      cfms(v, l, col[j]);
+      col[r] = v;
+    }
+    __syncthreads();
+  }
+  // back substitution, one right-hand side per thread
+  if (tid < nch) {
+    double2* b = Bm + (size_t)tid * nch;
+    for (int r = nch - 1; r >= 0; --r) {
+      double2 v = b[r];
+      for (int c = r + 1; c < nch; ++c) cfms(v, M[(size_t)c * nch + r], b[c]);
+      const double2 dd = M[(size_t)r * nch + r];
+      b[r] = (dd.x == 0.0 && dd.y == 0.0) ? make_double2(0.0, 0.0) : cdiv(v, dd);
+    }
+  }
+  __syncthreads();
+  double2* R = Rout + unit * nn;
+  if (mode == 0) {
+    // F = Bm.  T = I - D F (T[r, c] = delta_rc - d_r F[r, c]);  R0 = S T = S - S D F
+    double2* T = Tout + unit * nn;
+    for (int idx = tid; idx < (int)nn; idx += kHessThreads) {
+      const int r = idx % nch, c = idx / nch;
+      const double2 f = Bm[idx];
+      T[idx] = make_double2((r == c ? 1.0 : 0.0) - d[r] * f.x, -d[r] * f.y);
+      double2 v = Sv[idx];
+      for (int q = 0; q < nch; ++q) {
+        const double2 s = Sv[(size_t)q * nch + r];
+        const double2 df = make_double2(d[q] * Bm[(size_t)c * nch + q].x, d[q] * Bm[(size_t)c * nch + q].y);
+        cfms(v, s, df);
+      }
+      R[idx] = v;
+    }
+  } else {
+    double2* Dl = Dout + unit * nn;
+    double dn = 0.0, rn = 0.0;
+    for (int idx = tid; idx < (int)nn; idx += kHessThreads) {
+      const double2 dv = Bm[idx];
+      double2 v = R[idx];
+      v.x += dv.x;
+      v.y += dv.y;
+      R[idx] = v;
+      Dl[idx] = dv;
+      dn += dv.x * dv.x + dv.y * dv.y;
+      rn += v.x * v.x + v.y * v.y;
+    }
+    dn = block_sum<kHessThreads>(dn, red);
+    rn = block_sum<kHessThreads>(rn, red);
+    if (tid == 0) chg[unit] = rn > 0.0 ? sqrt(dn / rn) : 0.0;
+  }
+}
+
+constexpr size_t hess_woodbury_smem(int nch) { return (size_t)3 * nch * nch * sizeof(double2); }
+
+// out[unit] (nch x nch, column-major) = -diag(d_unit) Dl[unit]: the right factor of the X update
+// X += P (y_r - Y D Delta).  Grid (nch^2 / 256, units).
+__global__ void hess_scale_rows_kernel(const double2* __restrict__ Dl, const double* __restrict__ D, int ldD, int nch,
+                                       double2* out) {
+  const long nn = (long)nch * nch;
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nn) return;
+  const int unit = blockIdx.y;
+  const double d = D[(size_t)unit * ldD + (i % nch)];
+  const double2 v = Dl[(size_t)unit * nn + i];
+  out[(size_t)unit * nn + i] = make_double2(-d * v.x, -d * v.y);
+}
+
+// C (column-major nch x nch, per unit stride nch^2) = scale * Rsrc, zeroing nothing else: the
+// R-matrix of a unit R = (Q^T X) / a from the accumulated Q^T X.
+__global__ void scale_copy_kernel(const double2* src, double2* dst, long n, double scale) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = make_double2(src[i].x * scale, src[i].y * scale);
+}
+
+}  // namespace hprmat

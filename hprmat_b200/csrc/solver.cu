@@ -23,6 +23,7 @@
 #include "coulomb.cuh"
 #include "lu.cuh"
 #include "adjoint.cuh"
+#include "hessenberg.cuh"
 #include "rmat_kernels.cuh"
 #include "tc_gemm.cuh"
 #include "tc_solve.cuh"
@@ -189,6 +190,13 @@ struct hprmat_b200_ctx {
   int f64_N = 0, f64_nb = 0, f64_nsteps = 0;
   long f64_ld = 0;
   DevBuf adj_y, adj_part, adj_grad;
+  // shifted (Hessenberg) scan: per block C0 -> H (hA), P, P^H, reflectors, row-major H, partial
+  // sums, W = P^H Q, W^H; per batch of energies the factors and work arrays of every unit
+  DevBuf hA, hP, hPH, hU, hHr, hPart, hW, hWH, hChan, hUe, hLm, hSw, hY, hX, hR, hYr, hYT, hS, hT, hRacc, hG,
+      hDl, hUnit, hCu, hZo;
+  double hess_budget_gb = 16.0;  // device memory for one batch of energies
+  int hess_steps_last = 0;       // refinement steps of the last batch
+  int hess_fallback_last = 0;    // energies the last shifted scan sent to the LU path
   // batched energy scans: worker contexts (own stream and buffers) and the blocks' potentials
   std::vector<hprmat_b200_ctx*> scan_workers;
   std::vector<std::unique_ptr<DevBuf>> scan_cpot;
@@ -2537,6 +2545,389 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_
   return fe;
 }
 
+// ------------------------------------------------------------------ shifted (Hessenberg) scan
+// Householder reduction of A (N x N, column-major, ld) to upper Hessenberg form in place,
+// A = P H P^H, with P (ld) accumulated from the reflectors (kept in hU, column k: rows k+1 ..).
+static int hess_reduce(hprmat_b200_ctx* c, double2* A, long ld, int N, double2* P) {
+  NvtxRange nv("hprmat.hess.reduce");
+  TRY(c->hU.ensure((size_t)ld * N * sizeof(double2)));
+  const int nchunk_max = (N + kHessChunk - 1) / kHessChunk;
+  TRY(c->hPart.ensure((size_t)nchunk_max * N * sizeof(double2)));
+  double2* U = c->hU.as<double2>();
+  for (int k = 0; k + 2 < N; ++k) {
+    hess_reflector_kernel<<<1, kHessThreads, 0, c->stream>>>(A, ld, N, k, U, ld);
+    LAUNCH_CHECK();
+    const int ncol = N - k - 1;
+    hess_left_kernel<<<cdiv_u((long)ncol * 32, kHessThreads), kHessThreads, 0, c->stream>>>(A, ld, N, k + 1, k + 1, U,
+                                                                                          ld, k);
+    LAUNCH_CHECK();
+    const int nchunk = (ncol + kHessChunk - 1) / kHessChunk;
+    const dim3 gr(cdiv_u(N, kHessThreads), nchunk);
+    hess_right_partial_kernel<<<gr, kHessThreads, 0, c->stream>>>(A, ld, N, k, U, ld, c->hPart.as<double2>());
+    LAUNCH_CHECK();
+    hess_right_update_kernel<<<gr, kHessThreads, 0, c->stream>>>(A, ld, N, k, U, ld, c->hPart.as<double2>(), nchunk);
+    LAUNCH_CHECK();
+  }
+  // P = H_0 H_1 ... accumulated backwards from the identity
+  identity_kernel<<<dim3(cdiv_u(N, 256), N), 256, 0, c->stream>>>(P, ld, N);
+  LAUNCH_CHECK();
+  for (int k = N - 3; k >= 0; --k) {
+    hess_left_kernel<<<cdiv_u((long)(N - k - 1) * 32, kHessThreads), kHessThreads, 0, c->stream>>>(P, ld, N, k + 1,
+                                                                                                   k + 1, U, ld, k);
+    LAUNCH_CHECK();
+  }
+  return HPRMAT_B200_OK;
+}
+
+
+// One J-pi block of hprmat_b200_rmatrix_scan_shifted (hessenberg.cuh for the algebra): C0 is
+// reduced to Hessenberg form once, then the block's energies are solved in batches by O(N^2 nch)
+// work each, refined in FP64 against the structured C(E).  Energies whose kinematics do not fit
+// the shifted form (channels whose diagonal energy terms do not move together) or whose
+// Hessenberg or Woodbury pivots vanish are listed in `fallback` for the LU path.  COULFG
+// failures get their status as in rmatrix.
+static int hess_scan_block(hprmat_b200_ctx* c, int bi, const hprmat_b200_scan_block& B, double rmax, int nr,
+                           std::vector<int>& fallback, int* first_error, std::string* err_msg) {
+  const int nch = B.nch, N = nch * nr;
+  const long ld = N;
+  const double2* d_cpot = c->scan_cpot[bi]->as<double2>();
+  auto note = [&](int s) {
+    if (s != HPRMAT_B200_OK && *first_error == HPRMAT_B200_OK) {
+      *first_error = s;
+      *err_msg = hprmat_b200_last_error();
+    }
+  };
+  // host: boundary values of every energy, the shifts and the Bloch factors
+  std::vector<Boundary> bd(B.nenergies);
+  std::vector<int> good;
+  for (int e = 0; e < B.nenergies; ++e) {
+    const int s = boundary_values(nch, B.lval, B.qk + (size_t)e * nch, B.eta + (size_t)e * nch, rmax, rmax, bd[e]);
+    B.status[e] = s;
+    B.nopen[e] = s == HPRMAT_B200_OK ? bd[e].nopen : 0;
+    if (s == HPRMAT_B200_OK) good.push_back(e);
+    else note(s);
+  }
+  if (good.empty()) return HPRMAT_B200_OK;
+  const std::vector<double>& kref = bd[good[0]].kk;
+  std::vector<int> units;
+  std::vector<double> delta;
+  for (const int e : good) {
+    const double dl = bd[e].kk[0] - kref[0];
+    bool ok = true;
+    for (int ch = 0; ch < nch && ok; ++ch) {
+      const double d = bd[e].kk[ch] - kref[ch];
+      ok = fabs(d - dl) <= 1e-12 * std::max({1.0, fabs(bd[e].kk[ch]), fabs(kref[ch])});
+    }
+    if (ok) {
+      units.push_back(e);
+      delta.push_back(dl);
+    } else {
+      fallback.push_back(e);
+    }
+  }
+  if (units.empty()) return HPRMAT_B200_OK;
+  const MeshDev md = mesh_dev(c, 0, 0);
+  // C0 = C(E_ref) without the closed channels' Bloch terms
+  {
+    std::vector<double> h(3 * (size_t)nch, 0.0);
+    std::copy(bd[good[0]].fac.begin(), bd[good[0]].fac.end(), h.begin());
+    std::copy(kref.begin(), kref.end(), h.begin() + nch);
+    TRY(c->hChan.ensure(h.size() * sizeof(double)));
+    HPR_CUDA_TRY(cudaMemcpyAsync(c->hChan.p, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const double* dh = c->hChan.as<double>();
+    ChannelData chd0{dh, dh + nch, dh + 2 * nch};
+    TRY(c->hA.ensure((size_t)ld * N * sizeof(double2)));
+    double* d_fro2 = reinterpret_cast<double*>(c->status.as<int>() + 32);
+    NvtxRange nv("hprmat.hess.assemble");
+    assemble_kernel<double2><<<dim3(cdiv_u(N, 256), std::min(N, 512)), 256, 0, c->stream>>>(
+        md, chd0, nch, d_cpot, B.ncp1, nch, c->hA.as<double2>(), ld, N, d_fro2);
+    LAUNCH_CHECK();
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));  // h outlives its copy
+  }
+  double2* A = c->hA.as<double2>();
+  {
+    TRY(c->hP.ensure((size_t)ld * N * sizeof(double2)));
+    double2* P = c->hP.as<double2>();
+    TRY(hess_reduce(c, A, ld, N, P));
+    TRY(c->hHr.ensure((size_t)ld * N * sizeof(double2)));
+    TRY(c->hPH.ensure((size_t)ld * N * sizeof(double2)));
+    const dim3 gt(cdiv_u(N, 32), cdiv_u(N, 32)), bt(32, 8);
+    hess_transpose_kernel<<<gt, bt, 0, c->stream>>>(A, ld, N, c->hHr.as<double2>(), ld, false, true);
+    LAUNCH_CHECK();
+    hess_transpose_kernel<<<gt, bt, 0, c->stream>>>(P, ld, N, c->hPH.as<double2>(), ld, true, false);
+    LAUNCH_CHECK();
+    TRY(c->hW.ensure((size_t)ld * nch * sizeof(double2)));
+    TRY(c->hWH.ensure((size_t)nch * N * sizeof(double2)));
+    hess_wq_kernel<<<dim3(cdiv_u(N, 256), nch), 256, 0, c->stream>>>(c->hPH.as<double2>(), ld, N, nr, md.q2,
+                                                                     c->hW.as<double2>(), ld);
+    LAUNCH_CHECK();
+    hess_whq_kernel<<<dim3(cdiv_u(N, 256), nch), 256, 0, c->stream>>>(P, ld, N, nr, md.q2, c->hWH.as<double2>(),
+                                                                      nch);
+    LAUNCH_CHECK();
+  }
+  // the potential per mesh point for the structured residual
+  TRY(c->vt.ensure((size_t)nr * nch * nch * sizeof(double2)));
+  {
+    const long tot = (long)nr * nch * nch;
+    cpot_transpose_kernel<<<cdiv_u(tot, 256), 256, 0, c->stream>>>(d_cpot, B.ncp1, nch, nr, nch, c->vt.as<double2>());
+    LAUNCH_CHECK();
+  }
+  // batches of energies
+  const size_t nn = (size_t)nch * nch;
+  const size_t per_unit = (size_t)ld * N * sizeof(double2) + (size_t)N * (sizeof(double2) + sizeof(int)) +
+                          5 * (size_t)ld * nch * sizeof(double2) + 6 * nn * sizeof(double2) + 4096;
+  const int nb = (int)std::max<size_t>(1, std::min<size_t>(units.size(), (size_t)(c->hess_budget_gb * 1e9) / per_unit));
+  TRY(c->hUe.ensure((size_t)nb * ld * N * sizeof(double2)));
+  TRY(c->hLm.ensure((size_t)nb * N * sizeof(double2)));
+  TRY(c->hSw.ensure((size_t)nb * N * sizeof(int)));
+  for (DevBuf* b : {&c->hY, &c->hX, &c->hR, &c->hYr, &c->hYT}) TRY(b->ensure((size_t)nb * ld * nch * sizeof(double2)));
+  for (DevBuf* b : {&c->hS, &c->hT, &c->hRacc, &c->hG, &c->hDl}) TRY(b->ensure((size_t)nb * nn * sizeof(double2)));
+  TRY(c->hCu.ensure((size_t)nb * nn * sizeof(double2)));
+  TRY(c->hZo.ensure((size_t)2 * std::max<size_t>(nn, 1) * sizeof(double2)));
+  // per-unit block of the unit buffer: delta | D (nch) | kk (nch) | bloch (nch) | qk (nch) | fac (nch)
+  // as doubles, then co | cop (nch each, double2), open_idx (nch ints), then info | info2 | uinfo
+  const size_t ud = (1 + 5 * (size_t)nch + 1) / 2 * 2;  // doubles per unit, even: co follows 16-byte aligned
+  const size_t ub = ud * sizeof(double) + 2 * (size_t)nch * sizeof(double2) + (size_t)nch * sizeof(int) + 16;
+  const size_t ubp = (ub + 255) / 256 * 256;
+  TRY(c->hUnit.ensure((size_t)nb * ubp + (size_t)3 * nb * sizeof(int) + (size_t)nb * sizeof(double) + 256));
+  unsigned char* ubase = c->hUnit.as<unsigned char>();
+  int* d_info = reinterpret_cast<int*>(ubase + (size_t)nb * ubp);
+  int* d_info2 = d_info + nb;
+  int* d_uinfo = d_info2 + nb;
+  double* d_chg = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(d_uinfo + nb) + 8 -
+                                           (reinterpret_cast<uintptr_t>(d_uinfo + nb) & 7));
+  std::vector<double> d_delta_host(nb);
+  TRY(c->hChan.ensure((size_t)nb * sizeof(double) + 64));
+  const size_t smem_solve = std::max(kHessSolveSmem, (size_t)N * sizeof(double2));
+  TRY(set_smem(hess_solve_kernel, smem_solve));
+  TRY(set_smem(hess_woodbury_kernel, hess_woodbury_smem(nch)));
+  std::vector<unsigned char> hu((size_t)nb * ubp);
+  std::vector<int> hinfo(3 * (size_t)nb);
+  std::vector<double> hchg(nb);
+  const double2* P = c->hP.as<double2>();
+  const double2* PH = c->hPH.as<double2>();
+  const double2* WH = c->hWH.as<double2>();
+  for (size_t u0 = 0; u0 < units.size(); u0 += nb) {
+    const int m = (int)std::min<size_t>(nb, units.size() - u0);
+    // per-unit data
+    std::fill(hu.begin(), hu.end(), 0);
+    for (int j = 0; j < m; ++j) {
+      const Boundary& b = bd[units[u0 + j]];
+      double* hd = reinterpret_cast<double*>(hu.data() + (size_t)j * ubp);
+      hd[0] = delta[u0 + j];
+      for (int ch = 0; ch < nch; ++ch) {
+        hd[1 + ch] = -b.bloch[ch];
+        hd[1 + nch + ch] = b.kk[ch];
+        hd[1 + 2 * nch + ch] = b.bloch[ch];
+        hd[1 + 3 * nch + ch] = b.qk[ch];
+        hd[1 + 4 * nch + ch] = b.fac[ch];
+      }
+      double2* hz = reinterpret_cast<double2*>(hd + ud);
+      std::copy(b.co.begin(), b.co.end(), hz);
+      std::copy(b.cop.begin(), b.cop.end(), hz + nch);
+      int* hi = reinterpret_cast<int*>(hz + 2 * nch);
+      std::copy(b.open_idx.begin(), b.open_idx.end(), hi);
+      d_delta_host[j] = delta[u0 + j];
+    }
+    HPR_CUDA_TRY(cudaMemcpyAsync(ubase, hu.data(), (size_t)m * ubp, cudaMemcpyHostToDevice, c->stream));
+    HPR_CUDA_TRY(cudaMemcpyAsync(c->hChan.p, d_delta_host.data(), (size_t)m * sizeof(double), cudaMemcpyHostToDevice,
+                                 c->stream));
+    HPR_CUDA_TRY(cudaMemsetAsync(d_info, 0, 3 * (size_t)nb * sizeof(int), c->stream));
+    auto unit_d = [&](int j) { return reinterpret_cast<double*>(ubase + (size_t)j * ubp); };
+    // D of every unit at stride ubp / 8 doubles: the Woodbury kernel reads D + unit * ldD
+    const double* dD = unit_d(0) + 1;
+    const int ldD = (int)(ubp / sizeof(double));
+    // 1. Y = (H + delta I)^-1 W
+    HessSolveArgs ha{};
+    ha.Hr = c->hHr.as<double2>();
+    ha.ldh = ld;
+    ha.N = N;
+    ha.nch = nch;
+    ha.delta = c->hChan.as<double>();
+    ha.W = c->hW.as<double2>();
+    ha.ldw = ld;
+    ha.Ue = c->hUe.as<double2>();
+    ha.sUe = ld * N;
+    ha.lm = c->hLm.as<double2>();
+    ha.sw = c->hSw.as<int>();
+    ha.Y = c->hY.as<double2>();
+    ha.ldy = ld;
+    ha.sY = ld * nch;
+    ha.info = d_info;
+    {
+      NvtxRange nv("hprmat.hess.solve");
+      hess_solve_kernel<<<m, kHessThreads, smem_solve, c->stream>>>(ha);
+      LAUNCH_CHECK();
+    }
+    const long sN = ld * nch;
+    // 2. -S = -W^H Y;  T, R0 = S T
+    HPR_CUDA_TRY(cudaMemsetAsync(c->hS.p, 0, (size_t)m * nn * sizeof(double2), c->stream));
+    if (zgemm_f64_update_batched(nch, nch, N, WH, nch, 0, c->hY.as<double2>(), ld, sN, c->hS.as<double2>(), nch,
+                                 (long)nn, m, c->stream))
+      return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+    hess_woodbury_kernel<<<m, kHessThreads, hess_woodbury_smem(nch), c->stream>>>(
+        nch, c->hS.as<double2>(), dD, ldD, 0, nullptr, c->hT.as<double2>(), c->hRacc.as<double2>(), nullptr, nullptr,
+        d_info2);
+    LAUNCH_CHECK();
+    // 3. X = P Y T  (-YT first)
+    HPR_CUDA_TRY(cudaMemsetAsync(c->hYT.p, 0, (size_t)m * sN * sizeof(double2), c->stream));
+    if (zgemm_f64_update_batched(N, nch, nch, c->hY.as<double2>(), ld, sN, c->hT.as<double2>(), nch, (long)nn,
+                                 c->hYT.as<double2>(), ld, sN, m, c->stream))
+      return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+    HPR_CUDA_TRY(cudaMemsetAsync(c->hX.p, 0, (size_t)m * sN * sizeof(double2), c->stream));
+    if (zgemm_f64_update_batched(N, nch, N, P, ld, 0, c->hYT.as<double2>(), ld, sN, c->hX.as<double2>(), ld, sN, m,
+                                 c->stream))
+      return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+    // 4. refinement steps against the structured C(E)
+    std::vector<char> done(m, 0);
+    int steps = 0;
+    const int max_steps = std::max(1, c->opts.max_refine);
+    for (; steps < max_steps; ++steps) {
+      NvtxRange nv("hprmat.hess.refine");
+      for (int j = 0; j < m; ++j) {
+        const double* ud_ = unit_d(j);
+        Operator op;
+        op.structured = true;
+        op.mesh = md;
+        op.ch = ChannelData{ud_ + 1 + 4 * nch, ud_ + 1 + nch, ud_ + 1 + 2 * nch};
+        op.nch = nch;
+        op.N = N;
+        op.vt = c->vt.as<double2>();
+        op.q2 = md.q2;
+        op.q1 = md.q1;
+        op.nr = nr;
+        TRY(apply_residual(c, op, c->hX.as<double2>() + (size_t)j * sN, ld, nch, c->hR.as<double2>() + (size_t)j * sN,
+                           ld, true));
+      }
+      // -y_r = -(H + delta I)^-1 P^H r
+      HPR_CUDA_TRY(cudaMemsetAsync(c->hYr.p, 0, (size_t)m * sN * sizeof(double2), c->stream));
+      if (zgemm_f64_update_batched(N, nch, N, PH, ld, 0, c->hR.as<double2>(), ld, sN, c->hYr.as<double2>(), ld, sN, m,
+                                   c->stream))
+        return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+      HessSolveArgs hr = ha;
+      hr.W = nullptr;
+      hr.Y = c->hYr.as<double2>();
+      hess_solve_kernel<<<m, kHessThreads, smem_solve, c->stream>>>(hr);
+      LAUNCH_CHECK();
+      // G = W^H y_r; Delta = (I + S D)^-1 G; R += Delta
+      HPR_CUDA_TRY(cudaMemsetAsync(c->hG.p, 0, (size_t)m * nn * sizeof(double2), c->stream));
+      if (zgemm_f64_update_batched(nch, nch, N, WH, nch, 0, c->hYr.as<double2>(), ld, sN, c->hG.as<double2>(), nch,
+                                   (long)nn, m, c->stream))
+        return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+      hess_woodbury_kernel<<<m, kHessThreads, hess_woodbury_smem(nch), c->stream>>>(
+          nch, c->hS.as<double2>(), dD, ldD, 1, c->hG.as<double2>(), nullptr, c->hRacc.as<double2>(),
+          c->hDl.as<double2>(), d_chg, d_info2);
+      LAUNCH_CHECK();
+      HPR_CUDA_TRY(cudaMemcpyAsync(hchg.data(), d_chg, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+      bool all = true;
+      for (int j = 0; j < m; ++j) all = all && hchg[j] < c->opts.surface_tol;
+      if (all || steps + 1 == max_steps) {
+        ++steps;
+        break;
+      }
+      // X += P (y_r - Y D Delta):  hYr = -y_r + Y D Delta, then X -= P hYr
+      hess_scale_rows_kernel<<<dim3(cdiv_u((long)nn, 256), m), 256, 0, c->stream>>>(c->hDl.as<double2>(), dD, ldD,
+                                                                                    nch, c->hT.as<double2>());
+      LAUNCH_CHECK();
+      if (zgemm_f64_update_batched(N, nch, nch, c->hY.as<double2>(), ld, sN, c->hT.as<double2>(), nch, (long)nn,
+                                   c->hYr.as<double2>(), ld, sN, m, c->stream) ||
+          zgemm_f64_update_batched(N, nch, N, P, ld, 0, c->hYr.as<double2>(), ld, sN, c->hX.as<double2>(), ld, sN, m,
+                                   c->stream))
+        return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+      // T now holds -D Delta; the next step's Woodbury reads only S, D and G
+    }
+    // 5. U of every unit from R = Racc / a
+    HPR_CUDA_TRY(cudaMemcpyAsync(hinfo.data(), d_info, 2 * (size_t)nb * sizeof(int), cudaMemcpyDeviceToHost,
+                                 c->stream));
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    scale_copy_kernel<<<cdiv_u((long)m * nn, 256), 256, 0, c->stream>>>(c->hRacc.as<double2>(), c->hRacc.as<double2>(),
+                                                                        (long)m * nn, 1.0 / rmax);
+    LAUNCH_CHECK();
+    for (int j = 0; j < m; ++j) {
+      const int e = units[u0 + j];
+      if (hinfo[j] != 0 || hinfo[nb + j] != 0) continue;  // zero Hessenberg / Woodbury pivot: LU path
+      const double* ud_ = unit_d(j);
+      const double2* dz = reinterpret_cast<const double2*>(ud_ + ud);
+      const int* d_open = reinterpret_cast<const int*>(dz + 2 * nch);
+      const int no = bd[e].nopen;
+      umatrix_kernel<<<1, 1024, 0, c->stream>>>(c->hRacc.as<double2>() + (size_t)j * nn, nch, d_open, ud_ + 1 + 3 * nch,
+                                                dz, dz + nch, no, c->hZo.as<double2>(),
+                                                c->hZo.as<double2>() + std::max<size_t>(1, (size_t)no * no),
+                                                c->hCu.as<double2>() + (size_t)j * nn, nch, d_uinfo + j);
+      LAUNCH_CHECK();
+    }
+    HPR_CUDA_TRY(cudaMemcpyAsync(hinfo.data() + 2 * nb, d_uinfo, (size_t)nb * sizeof(int), cudaMemcpyDeviceToHost,
+                                 c->stream));
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (int j = 0; j < m; ++j) {
+      const int e = units[u0 + j];
+      if (hinfo[j] != 0 || hinfo[nb + j] != 0) {
+        fallback.push_back(e);
+        continue;
+      }
+      int s = hinfo[2 * nb + j] != 0 ? HPRMAT_B200_SINGULAR : HPRMAT_B200_OK;
+      if (s == HPRMAT_B200_OK && !(hchg[j] < c->opts.surface_tol)) s = HPRMAT_B200_NOT_CONVERGED;
+      if (s == HPRMAT_B200_SINGULAR) set_last_error_msg("rmatrix_scan_shifted: singular Z_O in the collision-matrix step");
+      if (s != HPRMAT_B200_SINGULAR) {
+        HPR_CUDA_TRY(cudaMemcpyAsync(B.cu + (size_t)e * nn * 2, c->hCu.as<double2>() + (size_t)j * nn,
+                                     nn * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+      }
+      B.status[e] = s;
+      note(s);
+    }
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->hess_steps_last = steps;
+  }
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_rmatrix_scan_shifted(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_scan_block* blocks,
+                                     double rmax, int nr, double* seconds) {
+  TRY(check_ctx(c));
+  TRY(scan_check_blocks(nblocks, blocks, rmax, nr, "rmatrix_scan_shifted"));
+  if (c->nr != nr || c->ns != 1 || c->rmax != rmax) TRY(hprmat_b200_rmat_ini(c, nr, 1, rmax, nullptr));
+  auto t0 = Clock::now();
+  TRY(scan_upload(c, nblocks, blocks));
+  int first_error = HPRMAT_B200_OK;
+  std::string err_msg;
+  c->hess_fallback_last = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    const hprmat_b200_scan_block& B = blocks[b];
+    std::vector<int> fallback;
+    if (B.nch > kHsMaxRhs) {
+      for (int e = 0; e < B.nenergies; ++e) fallback.push_back(e);
+    } else {
+      TRY(hess_scan_block(c, b, B, rmax, nr, fallback, &first_error, &err_msg));
+    }
+    // the LU path for what the shifted form does not take
+    c->hess_fallback_last += (int)fallback.size();
+    const size_t ubytes = (size_t)B.nch * B.nch * sizeof(double2);
+    for (const int e : fallback) {
+      int nopen = 0;
+      int s = c->cu.ensure(ubytes);
+      if (s == HPRMAT_B200_OK)
+        s = rmatrix_core(c, B.nch, B.lval, B.qk + (size_t)e * B.nch, B.eta + (size_t)e * B.nch, rmax, nr, 1,
+                         c->scan_cpot[b]->as<double2>(), B.ncp1, B.nch, c->cu.as<double2>(), &nopen, nullptr);
+      if (s == HPRMAT_B200_OK || s == HPRMAT_B200_NOT_CONVERGED) {
+        HPR_CUDA_TRY(cudaMemcpyAsync(B.cu + (size_t)e * B.nch * B.nch * 2, c->cu.p, ubytes, cudaMemcpyDeviceToHost,
+                                     c->stream));
+        HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+      }
+      B.nopen[e] = nopen;
+      B.status[e] = s;
+      if (s != HPRMAT_B200_OK && first_error == HPRMAT_B200_OK) {
+        first_error = s;
+        err_msg = hprmat_b200_last_error();
+      }
+    }
+  }
+  if (seconds) *seconds = std::chrono::duration<double>(Clock::now() - t0).count();
+  if (first_error != HPRMAT_B200_OK && first_error != HPRMAT_B200_NOT_CONVERGED)
+    return fail(first_error, "rmatrix_scan_shifted: %s", err_msg.c_str());
+  return first_error;
+}
+
 // Scan autotuner (see the header).  A trial runs one energy of a block on every worker at once
 // (a warm-up round, then the best of two timed rounds, host wall clock around the joined
 // threads, each worker's stream synchronised): the device under the scan's own concurrency.
@@ -3288,6 +3679,14 @@ int hprmat_b200_dev_zgemm(hprmat_b200_ctx* c, const void* A, long lda, const voi
   TRY(check_ctx(c));
   if (!A || !B || !C || M <= 0 || N <= 0 || K <= 0) return fail(HPRMAT_B200_ERR_ARG, "dev_zgemm: invalid arguments");
   TRY(zgemm_update(c, M, N, K, (const double2*)A, lda, (const double2*)B, ldb, (double2*)C, ldc));
+  HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_dev_hessenberg(hprmat_b200_ctx* c, void* A, long lda, int N, void* P) {
+  TRY(check_ctx(c));
+  if (!A || !P || N < 3 || lda < N) return fail(HPRMAT_B200_ERR_ARG, "dev_hessenberg: invalid arguments");
+  TRY(hess_reduce(c, (double2*)A, lda, N, (double2*)P));
   HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
   return HPRMAT_B200_OK;
 }

@@ -49,16 +49,21 @@ __device__ __forceinline__ void cp_async_wait() {
 // d += a b for one 8 x 8 x 4 FP64 block (fragments as mma.m8n8k4 .f64 lays them out: a at
 // row lane/4, column lane%4; b at row lane%4, column lane/4; d at row lane/4, columns
 // 2 (lane%4) and 2 (lane%4) + 1).
+// Not volatile: the compiler may interleave independent products to hide the DMMA latency.
 __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-               : "+d"(d[0]), "+d"(d[1])
-               : "d"(a), "d"(b));
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
 }
 
 __global__ void __launch_bounds__(kThreads, 2)
     zgemm_dmma_kernel(int M, int N, int K, const double2* __restrict__ A, long lda, const double2* __restrict__ B,
-                      long ldb, double2* __restrict__ C, long ldc) {
+                      long ldb, double2* __restrict__ C, long ldc, long sA, long sB, long sC) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  // problem blockIdx.z of a batch: operands sA, sB, sC complex elements apart
+  A += (size_t)blockIdx.z * sA;
+  B += (size_t)blockIdx.z * sB;
+  C += (size_t)blockIdx.z * sC;
   double2* As = reinterpret_cast<double2*>(smem_raw);
   double2* Bs = As + kStages * kAStage;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -118,13 +123,20 @@ __global__ void __launch_bounds__(kThreads, 2)
       for (int i = 0; i < 4; ++i) a[i] = as[(kk + fk) * kALd + wm + 8 * i + fr];
 #pragma unroll
       for (int j = 0; j < 4; ++j) b[j] = bs[(wn + 8 * j + fr) * kBLd + kk + fk];
+      // the 32 independent first products, then the 32 second ones (each accumulator's two
+      // products 32 instructions apart)
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          dmma(accr[i][j], a[i].x, b[j].x);
+          dmma(acci[i][j], a[i].x, b[j].y);
+        }
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const double nai = -a[i].y;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          dmma(accr[i][j], a[i].x, b[j].x);
-          dmma(acci[i][j], a[i].x, b[j].y);
           dmma(accr[i][j], nai, b[j].y);
           dmma(acci[i][j], a[i].y, b[j].x);
         }
@@ -158,19 +170,25 @@ __global__ void __launch_bounds__(kThreads, 2)
 
 int zgemm_f64_update(int M, int N, int K, const double2* A, long lda, const double2* B, long ldb, double2* C,
                      long ldc, cudaStream_t s) {
-  if (M <= 0 || N <= 0 || K <= 0) return 0;
-  if (((uintptr_t)A & 15) || ((uintptr_t)B & 15) || ((uintptr_t)C & 15) || lda < M || ldb < K || ldc < M) {
+  return zgemm_f64_update_batched(M, N, K, A, lda, 0, B, ldb, 0, C, ldc, 0, 1, s);
+}
+
+int zgemm_f64_update_batched(int M, int N, int K, const double2* A, long lda, long sA, const double2* B, long ldb,
+                             long sB, double2* C, long ldc, long sC, int batch, cudaStream_t s) {
+  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0) return 0;
+  if (((uintptr_t)A & 15) || ((uintptr_t)B & 15) || ((uintptr_t)C & 15) || lda < M || ldb < K || ldc < M || sA < 0 ||
+      sB < 0 || sC < 0) {
     set_last_error_msg("zgemm_f64_update: misaligned operand or leading dimension too small");
     return -1;
   }
   // per device and cheap next to a launch: set on every call (any thread, any device)
   HPR_CUDA_TRY(cudaFuncSetAttribute(zgemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
-  const dim3 grid((unsigned)((M + kBM - 1) / kBM), (unsigned)((N + kBN - 1) / kBN));
-  if (grid.y > 65535u) {
-    set_last_error_msg("zgemm_f64_update: N too large for one launch");
+  const dim3 grid((unsigned)((M + kBM - 1) / kBM), (unsigned)((N + kBN - 1) / kBN), (unsigned)batch);
+  if (grid.y > 65535u || batch > 65535) {
+    set_last_error_msg("zgemm_f64_update: N or the batch too large for one launch");
     return -5;
   }
-  zgemm_dmma_kernel<<<grid, kThreads, kSmemBytes, s>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  zgemm_dmma_kernel<<<grid, kThreads, kSmemBytes, s>>>(M, N, K, A, lda, B, ldb, C, ldc, sA, sB, sC);
   HPR_CUDA_TRY(cudaGetLastError());
   return 0;
 }

@@ -181,6 +181,22 @@ typedef struct {
 int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* ctx, int nblocks, const hprmat_b200_scan_block* blocks, double rmax,
                              int nr, int nworkers, double* seconds);
 
+/* The same scan by a structure-exploiting method (no counterpart in the reference, which solves
+   every energy by its own LU): between the energies of one block C(E) changes only by a common
+   shift of its diagonal and by the closed channels' Bloch terms, rank one each,
+   C(E) = C0 + delta(E) I + Q D(E) Q^T with Q = blockdiag(q2).  Each block's C0 is reduced once
+   on the device to Hessenberg form, C0 = P H P^H (Householder similarity transformations, FP64);
+   every energy then costs O(N^2 nch) -- an LU of H + delta I with row-pair pivoting, the
+   back substitution for P^H Q, and the Woodbury identity for the Bloch terms on an nch x nch
+   system -- followed by FP64 refinement steps against the structured C(E) (at most
+   opts.max_refine; converged when a step changes R by less than opts.surface_tol).  Energies
+   are solved in batches of independent units per launch.  Units the shifted form cannot take
+   (blocks with more than 64 channels, channels whose energy terms do not move together, a zero
+   Hessenberg or Woodbury pivot) run the LU path of hprmat_b200_rmatrix.  Outputs, statuses and
+   return value as hprmat_b200_rmatrix_scan; precision is FP64 throughout. */
+int hprmat_b200_rmatrix_scan_shifted(hprmat_b200_ctx* ctx, int nblocks, const hprmat_b200_scan_block* blocks,
+                                     double rmax, int nr, double* seconds);
+
 /* Scan autotuner, run before hprmat_b200_rmatrix_scan on the same blocks (or a sample of them).
    For every distinct order N = nch nr among the blocks it times one energy of the block (the
    middle one in the scan's energy order; the first or last if that solve fails) solved on all

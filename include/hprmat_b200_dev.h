@@ -24,6 +24,11 @@ int hprmat_b200_dev_tc_update(hprmat_b200_ctx* ctx, const float* aop, const floa
 int hprmat_b200_dev_zgemm(hprmat_b200_ctx* ctx, const void* A, long lda, const void* B, long ldb, void* C, long ldc,
                           int M, int N, int K);
 
+/* Householder reduction of A (device, N x N complex double, column-major, lda) in place to upper
+   Hessenberg form H with A = P H P^H; P (device, N x N, leading dimension lda) receives the
+   accumulated unitary factor.  The reduction of the shifted energy scan. */
+int hprmat_b200_dev_hessenberg(hprmat_b200_ctx* ctx, void* A, long lda, int N, void* P);
+
 /* Split complex float values into the 4 TF32 planes used by hprmat_b200_dev_tc_update:
    src is rows x nb (row-major complex float, i.e. K contiguous), dst gets 4 planes of
    rows x nb floats, `plane` floats apart. */

@@ -563,7 +563,8 @@ def test_fp64_pivoting_outside_float_range(ctx, scale):
     ctx.set_precision("fp64")
     X = ctx.solve_linear(A, B)
     assert ctx.last_stats["status"] == nat.OK and ctx.last_stats["info"] == 0
-    assert _rel(X, Xnp) <= 1e-12
+    s = 1.0 / np.abs(Xnp).max()  # norms of 1e300-sized values overflow: compare scaled copies
+    assert _rel(X * s, Xnp * s) <= 1e-12
     ctx.set_precision("mixed")
 
 

@@ -160,3 +160,79 @@ def test_scan_autotune_table_and_parity():
     ctx.set_scan_tune_table([])
     assert ctx.scan_tune_table() == []
     ctx.close()
+
+
+def test_hessenberg_reduction_is_a_unitary_similarity():
+    """The device Householder reduction: A = P H P^H with P unitary and H upper Hessenberg, on a
+    random complex matrix and on a C(E)-like matrix with a wide range of entry sizes."""
+    import torch
+    from hprmat_b200 import _native as nat
+    lib = nat.load()
+    ctx = api.Context(precision="fp64")
+    rng = np.random.default_rng(3)
+    w = workloads.production(seed=41, nch=5, nr=60, rmax=20.0)
+    mesh = orc.rmat_ini(60, 1, 20.0)
+    bnd = orc.boundary_values(w.nch, w.lval, w.qk, w.eta, 20.0)
+    cases = [rng.standard_normal((300, 300)) + 1j * rng.standard_normal((300, 300)),
+             orc.assemble(mesh, 1, w.nch, w.lval, w.qk, bnd.xc, w.cpot)]
+    for A in cases:
+        n = A.shape[0]
+        lda = n + 2
+        buf = np.zeros((n, lda), complex)  # column-major (lda x n)
+        buf[:, :n] = A.T
+        dA = torch.from_numpy(buf.view(np.float64).copy()).cuda()
+        dP = torch.zeros_like(dA)
+        nat.check(lib.hprmat_b200_dev_hessenberg(ctx._h, dA.data_ptr(), lda, n, dP.data_ptr()))
+        H = dA.cpu().numpy().view(complex).reshape(n, lda)[:, :n].T
+        P = dP.cpu().numpy().view(complex).reshape(n, lda)[:, :n].T
+        assert np.abs(np.tril(H, -2)).max() == 0.0
+        assert np.abs(P.conj().T @ P - np.eye(n)).max() <= 1e-13
+        assert np.linalg.norm(P @ H @ P.conj().T - A) <= 1e-14 * np.linalg.norm(A) * n ** 0.5
+    ctx.close()
+
+
+def test_shifted_scan_matches_oracle_per_unit():
+    """The shifted (Hessenberg) scan: one reduction per block, O(N^2 nch) per energy plus FP64
+    refinement; every unit agrees with the oracle to 1e-10, without sending units to the LU path."""
+    from hprmat_b200 import _native as nat
+    blocks = _blocks()
+    ctx = api.Context(precision="mixed")
+    res = ctx.rmatrix_scan([(w.lval, w.cpot, qk, eta) for w, qk, eta in blocks], 20.0, 60, method="shifted")
+    mesh = orc.rmat_ini(60, 1, 20.0)
+    for (w, qk, eta), (cu, nopen, status) in zip(blocks, res):
+        for e in range(qk.shape[0]):
+            ref = orc.rmatrix(w.nch, w.lval, qk[e], eta[e], 20.0, mesh, w.cpot)
+            assert status[e] == nat.OK
+            assert nopen[e] == ref.nopen
+            no = ref.nopen
+            err = np.linalg.norm(cu[e, :no, :no] - ref.cu) / np.linalg.norm(ref.cu)
+            assert err <= U_TOL, (w.nch, e, err)
+    ctx.close()
+
+
+def test_shifted_scan_on_a_config3_sample():
+    """A sample of the energy-scan configuration (blocks of 4..64 channels x 60 points, energies
+    in 1-30 MeV): the shifted scan against the oracle on every fourth energy of three blocks,
+    and against the LU scan on all of them."""
+    from oracle import special_functions as sf
+    blocks = workloads.scan_blocks()
+    picked = []
+    for w, energies in [blocks[i] for i in (0, 5, 9)]:
+        ks = [workloads.channel_kinematics(e, w.thresholds, w.hm, w.params.z1z2) for e in energies[::16]]
+        ks = [k for k in ks if all(sf.coulfg(k[0][c] * w.rmax, k[1][c], float(w.lval[c]))[4] == 0
+                                   for c in range(w.nch) if k[0][c] > 0)]
+        picked.append((w, np.array([k[0] for k in ks]), np.array([k[1] for k in ks])))
+    args = [(w.lval, w.cpot, qk, eta) for w, qk, eta in picked]
+    ctx = api.Context(precision="mixed")
+    res_s = ctx.rmatrix_scan(args, 20.0, 60, method="shifted")
+    res_l = ctx.rmatrix_scan(args, 20.0, 60, nworkers=2)
+    mesh = orc.rmat_ini(60, 1, 20.0)
+    for (w, qk, eta), (cu, nopen, st), (cl, nl, sl) in zip(picked, res_s, res_l):
+        for e in range(qk.shape[0]):
+            no = nopen[e]
+            assert st[e] == 0 and sl[e] == 0 and nl[e] == no
+            assert np.linalg.norm(cu[e, :no, :no] - cl[e, :no, :no]) <= U_TOL * np.linalg.norm(cl[e, :no, :no])
+            if e % 4 == 0:
+                ref = orc.rmatrix(w.nch, w.lval, qk[e], eta[e], 20.0, mesh, w.cpot)
+                assert np.linalg.norm(cu[e, :no, :no] - ref.cu) <= U_TOL * np.linalg.norm(ref.cu), (w.nch, e)
+    ctx.close()
