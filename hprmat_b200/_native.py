@@ -46,7 +46,7 @@ EXPORTED = (
     "hprmat_b200_dev_counters", "hprmat_b200_dev_wave_trace", "hprmat_b200_dev_wave_trace_read",
     "hprmat_b200_dev_panel_trace_read", "hprmat_b200_dev_set_tuning", "hprmat_b200_dev_mesh",
     "hprmat_b200_dev_factorizations", "hprmat_b200_dev_wait_probe", "hprmat_b200_dev_binary_version",
-    "hprmat_b200_dev_zgemm", "hprmat_b200_dev_hessenberg",
+    "hprmat_b200_dev_zgemm", "hprmat_b200_dev_hessenberg", "hprmat_b200_dev_hess_timings",
 )
 
 
@@ -152,6 +152,7 @@ def load():
         "hprmat_b200_dev_binary_version": (I, []),
         "hprmat_b200_dev_zgemm": (I, [P, P, ctypes.c_long, P, ctypes.c_long, P, ctypes.c_long, I, I, I]),
         "hprmat_b200_dev_hessenberg": (I, [P, P, ctypes.c_long, I, P]),
+        "hprmat_b200_dev_hess_timings": (I, [P, DP, IP, I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -197,6 +197,7 @@ struct hprmat_b200_ctx {
   double hess_budget_gb = 16.0;  // device memory for one batch of energies
   int hess_steps_last = 0;       // refinement steps of the last batch
   int hess_fallback_last = 0;    // energies the last shifted scan sent to the LU path
+  double hess_ms[6] = {};        // with profiling: reduce, solve, products, refine, U, fallback (ms)
   // batched energy scans: worker contexts (own stream and buffers) and the blocks' potentials
   std::vector<hprmat_b200_ctx*> scan_workers;
   std::vector<std::unique_ptr<DevBuf>> scan_cpot;
@@ -2627,6 +2628,15 @@ static int hess_scan_block(hprmat_b200_ctx* c, int bi, const hprmat_b200_scan_bl
   }
   if (units.empty()) return HPRMAT_B200_OK;
   const MeshDev md = mesh_dev(c, 0, 0);
+  // with profiling, every phase ends with a stream synchronisation and adds its host time
+  auto tmark = Clock::now();
+  auto phase = [&](int slot) -> int {
+    if (!c->profile) return HPRMAT_B200_OK;
+    HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->hess_ms[slot] += ms_since(tmark);
+    tmark = Clock::now();
+    return HPRMAT_B200_OK;
+  };
   // C0 = C(E_ref) without the closed channels' Bloch terms
   {
     std::vector<double> h(3 * (size_t)nch, 0.0);
@@ -2665,6 +2675,7 @@ static int hess_scan_block(hprmat_b200_ctx* c, int bi, const hprmat_b200_scan_bl
                                                                       nch);
     LAUNCH_CHECK();
   }
+  TRY(phase(0));
   // the potential per mesh point for the structured residual
   TRY(c->vt.ensure((size_t)nr * nch * nch * sizeof(double2)));
   {
@@ -2759,6 +2770,7 @@ static int hess_scan_block(hprmat_b200_ctx* c, int bi, const hprmat_b200_scan_bl
       hess_solve_kernel<<<m, kHessThreads, smem_solve, c->stream>>>(ha);
       LAUNCH_CHECK();
     }
+    TRY(phase(1));
     const long sN = ld * nch;
     // 2. -S = -W^H Y;  T, R0 = S T
     HPR_CUDA_TRY(cudaMemsetAsync(c->hS.p, 0, (size_t)m * nn * sizeof(double2), c->stream));
@@ -2778,8 +2790,8 @@ static int hess_scan_block(hprmat_b200_ctx* c, int bi, const hprmat_b200_scan_bl
     if (zgemm_f64_update_batched(N, nch, N, P, ld, 0, c->hYT.as<double2>(), ld, sN, c->hX.as<double2>(), ld, sN, m,
                                  c->stream))
       return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+    TRY(phase(2));
     // 4. refinement steps against the structured C(E)
-    std::vector<char> done(m, 0);
     int steps = 0;
     const int max_steps = std::max(1, c->opts.max_refine);
     for (; steps < max_steps; ++steps) {
@@ -2837,6 +2849,7 @@ static int hess_scan_block(hprmat_b200_ctx* c, int bi, const hprmat_b200_scan_bl
         return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
       // T now holds -D Delta; the next step's Woodbury reads only S, D and G
     }
+    TRY(phase(3));
     // 5. U of every unit from R = Racc / a
     HPR_CUDA_TRY(cudaMemcpyAsync(hinfo.data(), d_info, 2 * (size_t)nb * sizeof(int), cudaMemcpyDeviceToHost,
                                  c->stream));
@@ -2877,6 +2890,7 @@ static int hess_scan_block(hprmat_b200_ctx* c, int bi, const hprmat_b200_scan_bl
       note(s);
     }
     HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    TRY(phase(4));
     c->hess_steps_last = steps;
   }
   return HPRMAT_B200_OK;
@@ -2902,6 +2916,7 @@ int hprmat_b200_rmatrix_scan_shifted(hprmat_b200_ctx* c, int nblocks, const hprm
     }
     // the LU path for what the shifted form does not take
     c->hess_fallback_last += (int)fallback.size();
+    auto tfb = Clock::now();
     const size_t ubytes = (size_t)B.nch * B.nch * sizeof(double2);
     for (const int e : fallback) {
       int nopen = 0;
@@ -2921,6 +2936,7 @@ int hprmat_b200_rmatrix_scan_shifted(hprmat_b200_ctx* c, int nblocks, const hprm
         err_msg = hprmat_b200_last_error();
       }
     }
+    if (c->profile) c->hess_ms[5] += ms_since(tfb);
   }
   if (seconds) *seconds = std::chrono::duration<double>(Clock::now() - t0).count();
   if (first_error != HPRMAT_B200_OK && first_error != HPRMAT_B200_NOT_CONVERGED)
@@ -3680,6 +3696,17 @@ int hprmat_b200_dev_zgemm(hprmat_b200_ctx* c, const void* A, long lda, const voi
   if (!A || !B || !C || M <= 0 || N <= 0 || K <= 0) return fail(HPRMAT_B200_ERR_ARG, "dev_zgemm: invalid arguments");
   TRY(zgemm_update(c, M, N, K, (const double2*)A, lda, (const double2*)B, ldb, (double2*)C, ldc));
   HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return HPRMAT_B200_OK;
+}
+
+int hprmat_b200_dev_hess_timings(hprmat_b200_ctx* c, double* ms, int* counts, int reset) {
+  TRY(check_ctx(c));
+  if (ms) std::copy(c->hess_ms, c->hess_ms + 6, ms);
+  if (counts) {
+    counts[0] = c->hess_steps_last;
+    counts[1] = c->hess_fallback_last;
+  }
+  if (reset) std::fill(c->hess_ms, c->hess_ms + 6, 0.0);
   return HPRMAT_B200_OK;
 }
 

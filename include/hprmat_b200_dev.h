@@ -29,6 +29,13 @@ int hprmat_b200_dev_zgemm(hprmat_b200_ctx* ctx, const void* A, long lda, const v
    accumulated unitary factor.  The reduction of the shifted energy scan. */
 int hprmat_b200_dev_hessenberg(hprmat_b200_ctx* ctx, void* A, long lda, int N, void* P);
 
+/* Phase times of the shifted scans run on the context while profiling is enabled
+   (hprmat_b200_dev_set_profile): ms[6] = reduction to Hessenberg form (with the assembly of C0),
+   per-energy Hessenberg solves, products for S, T and X, refinement steps, collision matrices,
+   units run by the LU path; counts[2] = refinement steps of the last batch, units sent to the LU
+   path by the last scan.  reset != 0 clears the times. */
+int hprmat_b200_dev_hess_timings(hprmat_b200_ctx* ctx, double* ms, int* counts, int reset);
+
 /* Split complex float values into the 4 TF32 planes used by hprmat_b200_dev_tc_update:
    src is rows x nb (row-major complex float, i.e. K contiguous), dst gets 4 planes of
    rows x nb floats, `plane` floats apart. */
