@@ -21,6 +21,7 @@
 // C0 = P H_final P^H with P = H_0 H_1 ... H_{N-3}.
 #pragma once
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 #include "common.cuh"
 
@@ -252,79 +253,126 @@ struct HessSolveArgs {
 constexpr int kHsRows = 32;   // rows per back-substitution block
 constexpr int kHsMaxRhs = 64;
 
+// d += a b for one 8 x 8 x 4 FP64 block on the DMMA units (fragments as mma.m8n8k4 .f64 lays
+// them out: a at row lane/4, column lane%4; b at row lane%4, column lane/4; d at row lane/4,
+// columns 2 (lane%4) and 2 (lane%4) + 1).
+__device__ __forceinline__ void hs_dmma(double (&d)[2], double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
+}
+__device__ __forceinline__ void hs_cp16(void* dst, const void* src, bool valid) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+
+constexpr int kHsUs = kHsRows + 4;       // row stride of the Ue tile (complex): conflict-free A fragments
+constexpr int kHsYs = kHsMaxRhs + 2;     // row stride of the Y chunk: conflict-free B fragments
+constexpr int kHsUsTile = kHsRows * kHsUs;
+constexpr int kHsYsTile = kHsRows * kHsYs;
+
 // Back substitution Y = Ue^-1 Z in place on the unit's Y (column-major, ldy).  Blocks of 32
-// rows from the bottom: the block's rows minus Ue[rows, below] Y[below] (each thread 2 rows x 4
-// right-hand sides, 32-column chunks staged in shared memory), then the 32 x 32 triangle.
+// rows from the bottom.  The block's rows minus Ue[rows, below] Y[below] on the FP64 tensor
+// units: 8 warps as 4 (8 rows) x 2 (32 right-hand sides), 32-column chunks of Ue and 32-row
+// chunks of Y double-buffered in shared memory by cp.async; then the 32 x 32 triangle, one
+// right-hand side per thread.
 __device__ void hess_back_substitute(const double2* Ue, long ldh, int N, int nch, double2* Y, long ldy,
                                      double2* smem) {
-  double2* us = smem;                          // [32][33] Ue tile (row-major)
-  double2* ys = us + kHsRows * (kHsRows + 1);  // [32][kHsMaxRhs] Y chunk rows
-  double2* acc_s = ys + kHsRows * kHsMaxRhs;   // [32][kHsMaxRhs] block accumulators
-  const int tid = threadIdx.x;
-  const int rp = tid / 16, cq = tid % 16;      // row pair, column quad
+  double2* us = smem;                       // [2][32][kHsUs]
+  double2* ys = us + 2 * kHsUsTile;         // [2][32][kHsYs]
+  double2* acc_s = ys + 2 * kHsYsTile;      // [32][kHsMaxRhs]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wr = warp & 3, wc = warp >> 2;
+  const int fr = lane >> 2, fk = lane & 3;
   const int nblk = (N + kHsRows - 1) / kHsRows;
   for (int b = nblk - 1; b >= 0; --b) {
     const int k0 = b * kHsRows, k1 = min(k0 + kHsRows, N);
-    double2 acc[2][4];
+    const int nrow = k1 - k0;
+    double accr[4][2], acci[4][2];
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int r = k0 + 2 * rp + a, c = 4 * cq + q;
-        acc[a][q] = (r < k1 && c < nch) ? Y[(size_t)c * ldy + r] : make_double2(0.0, 0.0);
-      }
-    for (int j0 = k1; j0 < N; j0 += kHsRows) {
-      const int jn = min(kHsRows, N - j0);
-      __syncthreads();
+    for (int q = 0; q < 4; ++q) accr[q][0] = accr[q][1] = acci[q][0] = acci[q][1] = 0.0;
+    const int nchk = (N - k1 + kHsRows - 1) / kHsRows;
+    auto load = [&](int ci, int buf) {
+      const int j0 = k1 + ci * kHsRows;
+      double2* u_ = us + buf * kHsUsTile;
+      double2* y_ = ys + buf * kHsYsTile;
       for (int idx = tid; idx < kHsRows * kHsRows; idx += kHessThreads) {
         const int r = idx / kHsRows, j = idx % kHsRows;
-        us[r * (kHsRows + 1) + j] =
-            (k0 + r < k1 && j < jn) ? Ue[(size_t)(k0 + r) * ldh + j0 + j] : make_double2(0.0, 0.0);
+        const bool ok = r < nrow && j0 + j < N;
+        hs_cp16(u_ + r * kHsUs + j, ok ? Ue + (size_t)(k0 + r) * ldh + j0 + j : Ue, ok);
       }
-      for (int idx = tid; idx < kHsRows * nch; idx += kHessThreads) {
+      for (int idx = tid; idx < kHsRows * kHsMaxRhs; idx += kHessThreads) {
         const int j = idx % kHsRows, c = idx / kHsRows;
-        ys[j * kHsMaxRhs + c] = j < jn ? Y[(size_t)c * ldy + j0 + j] : make_double2(0.0, 0.0);
+        const bool ok = c < nch && j0 + j < N;
+        hs_cp16(y_ + j * kHsYs + c, ok ? Y + (size_t)c * ldy + j0 + j : Y, ok);
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (nchk > 0) load(0, 0);
+    for (int ci = 0; ci < nchk; ++ci) {
+      if (ci + 1 < nchk) {
+        load(ci + 1, (ci + 1) & 1);
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+      } else {
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
       }
       __syncthreads();
-#pragma unroll 4
-      for (int j = 0; j < kHsRows; ++j) {
-        const double2 u0 = us[(2 * rp) * (kHsRows + 1) + j], u1 = us[(2 * rp + 1) * (kHsRows + 1) + j];
+      const double2* u_ = us + (ci & 1) * kHsUsTile;
+      const double2* y_ = ys + (ci & 1) * kHsYsTile;
+#pragma unroll
+      for (int kk = 0; kk < kHsRows; kk += 4) {
+        const double2 a = u_[(8 * wr + fr) * kHsUs + kk + fk];
+        double2 bb[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) bb[q] = y_[(kk + fk) * kHsYs + 32 * wc + 8 * q + fr];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const double2 y = ys[j * kHsMaxRhs + 4 * cq + q];
-          cfms(acc[0][q], u0, y);
-          cfms(acc[1][q], u1, y);
+          hs_dmma(accr[q], a.x, bb[q].x);
+          hs_dmma(acci[q], a.x, bb[q].y);
+        }
+        const double nai = -a.y;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          hs_dmma(accr[q], nai, bb[q].y);
+          hs_dmma(acci[q], a.y, bb[q].x);
         }
       }
+      __syncthreads();  // the buffer is refilled two chunks later
     }
-    __syncthreads();
+    // the block's right-hand sides minus the products, into shared memory
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
+    for (int q = 0; q < 4; ++q)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) acc_s[(2 * rp + a) * kHsMaxRhs + 4 * cq + q] = acc[a][q];
+      for (int e = 0; e < 2; ++e) {
+        const int r = 8 * wr + fr, c = 32 * wc + 8 * q + 2 * fk + e;
+        double2 z = (r < nrow && c < nch) ? Y[(size_t)c * ldy + k0 + r] : make_double2(0.0, 0.0);
+        z.x -= accr[q][e];
+        z.y -= acci[q][e];
+        acc_s[r * kHsMaxRhs + c] = z;
+      }
+    // the diagonal tile
     for (int idx = tid; idx < kHsRows * kHsRows; idx += kHessThreads) {
       const int r = idx / kHsRows, j = idx % kHsRows;
-      us[r * (kHsRows + 1) + j] = (k0 + r < k1 && k0 + j < k1) ? Ue[(size_t)(k0 + r) * ldh + k0 + j]
-                                                                 : make_double2(0.0, 0.0);
+      us[r * kHsUs + j] = (r < nrow && j < nrow) ? Ue[(size_t)(k0 + r) * ldh + k0 + j] : make_double2(0.0, 0.0);
     }
     __syncthreads();
     // the triangle, one right-hand side per thread
     if (tid < nch) {
-      for (int r = k1 - k0 - 1; r >= 0; --r) {
+      for (int r = nrow - 1; r >= 0; --r) {
         double2 v = acc_s[r * kHsMaxRhs + tid];
-        for (int j = r + 1; j < k1 - k0; ++j) cfms(v, us[r * (kHsRows + 1) + j], acc_s[j * kHsMaxRhs + tid]);
-        const double2 d = us[r * (kHsRows + 1) + r];
+        for (int j = r + 1; j < nrow; ++j) cfms(v, us[r * kHsUs + j], acc_s[j * kHsMaxRhs + tid]);
+        const double2 d = us[r * kHsUs + r];
         v = (d.x == 0.0 && d.y == 0.0) ? make_double2(0.0, 0.0) : cdiv(v, d);
         acc_s[r * kHsMaxRhs + tid] = v;
         Y[(size_t)tid * ldy + k0 + r] = v;
       }
     }
+    __syncthreads();
   }
-  __syncthreads();
 }
 
 constexpr size_t kHessSolveSmem =
-    ((size_t)kHsRows * (kHsRows + 1) + 2 * (size_t)kHsRows * kHsMaxRhs) * sizeof(double2);
+    (2 * (size_t)kHsUsTile + 2 * (size_t)kHsYsTile + (size_t)kHsRows * kHsMaxRhs) * sizeof(double2);
 
 // Factor and solve (W given) or re-solve with the stored factors (W == nullptr: the unit's Y
 // holds the right-hand sides).  Dynamic shared memory: max(kHessSolveSmem, N complex) bytes.

@@ -9,9 +9,10 @@
 //
 // Each complex product is 4 real products on mma.sync.aligned.m8n8k4.f64 (DMMA):
 //   Re += Ar Br + (-Ai) Bi,   Im += Ar Bi + Ai Br,
-// FP64 products and FP64 accumulation throughout.  A CTA of 4 warps computes a 64 x 64
-// complex tile of C (each warp 32 x 32: 4 x 4 blocks of 8 x 8, Re and Im accumulators in
-// registers) over K in chunks of 16, staged in shared memory by cp.async in a 3-deep ring:
+// FP64 products and FP64 accumulation throughout.  A CTA of 4 warps computes 64 x 64 complex
+// tiles of C (each warp 32 x 32: 4 x 4 blocks of 8 x 8, Re and Im accumulators in registers),
+// two persistent CTAs per SM, over K in chunks of 16 staged in shared memory by cp.async in a
+// 3-deep ring that runs on across the CTA's tiles:
 //   A chunk as [k][m] (m contiguous, as A's columns), row stride 66 complex, and
 //   B chunk as [n][k] (k contiguous, as B's columns), row stride 20 complex,
 // so that the fragment loads -- one 16-byte (re, im) load per 8 x 4 A block and per 4 x 8 B
@@ -56,23 +57,33 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
       : "d"(a), "d"(b));
 }
 
+// Persistent: a CTA walks the tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... of all batch
+// problems (rows fastest), and its K chunks form one stream across its tiles, so the ring
+// prefetches the next tile's first chunks while the current tile finishes and writes C.
 __global__ void __launch_bounds__(kThreads, 2)
     zgemm_dmma_kernel(int M, int N, int K, const double2* __restrict__ A, long lda, const double2* __restrict__ B,
-                      long ldb, double2* __restrict__ C, long ldc, long sA, long sB, long sC) {
+                      long ldb, double2* __restrict__ C, long ldc, long sA, long sB, long sC, int batch) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  // problem blockIdx.z of a batch: operands sA, sB, sC complex elements apart
-  A += (size_t)blockIdx.z * sA;
-  B += (size_t)blockIdx.z * sB;
-  C += (size_t)blockIdx.z * sC;
   double2* As = reinterpret_cast<double2*>(smem_raw);
   double2* Bs = As + kStages * kAStage;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
   const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
   const int nchunks = (K + kBK - 1) / kBK;
+  const int mt = (M + kBM - 1) / kBM, nt = (N + kBN - 1) / kBN;
+  const long ntiles = (long)mt * nt * batch;
+  const long mytiles = ntiles > blockIdx.x ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const long nstream = mytiles * nchunks;  // chunks of all this CTA's tiles
 
-  auto load_stage = [&](int stage, int kc) {
-    const int k0 = kc * kBK;
+  // chunk g of the stream -> its tile's operands
+  auto load_chunk = [&](long g) {
+    const long t = blockIdx.x + (g / nchunks) * (long)gridDim.x;
+    const int kc = (int)(g % nchunks);
+    const int z = (int)(t / ((long)mt * nt));
+    const int r = (int)(t % ((long)mt * nt));
+    const int m0 = (r % mt) * kBM, n0 = (r / mt) * kBN, k0 = kc * kBK;
+    const double2* Az = A + (size_t)z * sA;
+    const double2* Bz = B + (size_t)z * sB;
+    const int stage = (int)(g % kStages);
     double2* as = As + stage * kAStage;
     double2* bs = Bs + stage * kBStage;
 #pragma unroll
@@ -80,7 +91,7 @@ __global__ void __launch_bounds__(kThreads, 2)
       const int idx = tid + i * kThreads;
       const int k = idx / kBM, m = idx % kBM;
       const bool ok = (m0 + m < M) && (k0 + k < K);
-      const double2* src = ok ? A + (size_t)(m0 + m) + (size_t)(k0 + k) * lda : A;
+      const double2* src = ok ? Az + (size_t)(m0 + m) + (size_t)(k0 + k) * lda : Az;
       cp_async16(as + k * kALd + m, src, ok);
     }
 #pragma unroll
@@ -88,7 +99,7 @@ __global__ void __launch_bounds__(kThreads, 2)
       const int idx = tid + i * kThreads;
       const int n = idx / kBK, k = idx % kBK;
       const bool ok = (n0 + n < N) && (k0 + k < K);
-      const double2* src = ok ? B + (size_t)(k0 + k) + (size_t)(n0 + n) * ldb : B;
+      const double2* src = ok ? Bz + (size_t)(k0 + k) + (size_t)(n0 + n) * ldb : Bz;
       cp_async16(bs + n * kBLd + k, src, ok);
     }
   };
@@ -104,18 +115,19 @@ __global__ void __launch_bounds__(kThreads, 2)
 
 #pragma unroll
   for (int s = 0; s < kStages - 1; ++s) {
-    if (s < nchunks) load_stage(s, s);
+    if (s < nstream) load_chunk(s);
     cp_async_commit();
   }
   const int fr = lane >> 2, fk = lane & 3;
-  for (int kc = 0; kc < nchunks; ++kc) {
+  for (long g = 0; g < nstream; ++g) {
     cp_async_wait<kStages - 2>();
     __syncthreads();
     // refill the slot consumed in the previous iteration (every warp has passed the barrier)
-    if (kc + kStages - 1 < nchunks) load_stage((kc + kStages - 1) % kStages, kc + kStages - 1);
+    if (g + kStages - 1 < nstream) load_chunk(g + kStages - 1);
     cp_async_commit();
-    const double2* as = As + (kc % kStages) * kAStage;
-    const double2* bs = Bs + (kc % kStages) * kBStage;
+    const int stage = (int)(g % kStages);
+    const double2* as = As + stage * kAStage;
+    const double2* bs = Bs + stage * kBStage;
 #pragma unroll
     for (int kk = 0; kk < kBK; kk += 4) {
       double2 a[4], b[4];
@@ -142,28 +154,36 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
       }
     }
-  }
-  cp_async_wait<0>();
-  // C -= acc
+    if ((int)(g % nchunks) == nchunks - 1) {
+      // the tile is complete: C -= acc, then start the next tile's accumulators at zero
+      const long t = blockIdx.x + (g / nchunks) * (long)gridDim.x;
+      const int z = (int)(t / ((long)mt * nt));
+      const int r = (int)(t % ((long)mt * nt));
+      const int m0 = (r % mt) * kBM, n0 = (r / mt) * kBN;
+      double2* Cz = C + (size_t)z * sC;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int row = m0 + wm + 8 * i + fr;
-    if (row >= M) continue;
+      for (int i = 0; i < 4; ++i) {
+        const int row = m0 + wm + 8 * i + fr;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < 4; ++j) {
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int col = n0 + wn + 8 * j + 2 * fk + e;
-        if (col < N) {
-          double2* p = C + (size_t)row + (size_t)col * ldc;
-          double2 v = *p;
-          v.x -= accr[i][j][e];
-          v.y -= acci[i][j][e];
-          *p = v;
+          for (int e = 0; e < 2; ++e) {
+            const int col = n0 + wn + 8 * j + 2 * fk + e;
+            if (row < M && col < N) {
+              double2* p = Cz + (size_t)row + (size_t)col * ldc;
+              double2 v = *p;
+              v.x -= accr[i][j][e];
+              v.y -= acci[i][j][e];
+              *p = v;
+            }
+            accr[i][j][e] = 0.0;
+            acci[i][j][e] = 0.0;
+          }
         }
       }
     }
   }
+  cp_async_wait<0>();
 }
 
 }  // namespace
@@ -183,12 +203,12 @@ int zgemm_f64_update_batched(int M, int N, int K, const double2* A, long lda, lo
   }
   // per device and cheap next to a launch: set on every call (any thread, any device)
   HPR_CUDA_TRY(cudaFuncSetAttribute(zgemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));
-  const dim3 grid((unsigned)((M + kBM - 1) / kBM), (unsigned)((N + kBN - 1) / kBN), (unsigned)batch);
-  if (grid.y > 65535u || batch > 65535) {
-    set_last_error_msg("zgemm_f64_update: N or the batch too large for one launch");
-    return -5;
-  }
-  zgemm_dmma_kernel<<<grid, kThreads, kSmemBytes, s>>>(M, N, K, A, lda, B, ldb, C, ldc, sA, sB, sC);
+  int dev = 0, nsm = 0;
+  HPR_CUDA_TRY(cudaGetDevice(&dev));
+  HPR_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const long ntiles = (long)((M + kBM - 1) / kBM) * ((N + kBN - 1) / kBN) * batch;
+  const long grid = ntiles < 2L * nsm ? ntiles : 2L * nsm;  // two resident CTAs per SM
+  zgemm_dmma_kernel<<<(unsigned)grid, kThreads, kSmemBytes, s>>>(M, N, K, A, lda, B, ldb, C, ldc, sA, sB, sC, batch);
   HPR_CUDA_TRY(cudaGetLastError());
   return 0;
 }
