@@ -227,6 +227,214 @@ __global__ void hess_whq_kernel(const double2* __restrict__ P, long ldp, int N, 
   WH[(size_t)i * ldwh + c] = make_double2(wr, wi);
 }
 
+// ---------------------------------------------------------------- blocked reduction
+// Panels of kHbB columns (the method of LAPACK's xGEHRD with xLAHR2, in this file's reflector
+// convention, tau = 2): the reflectors u_1 .. u_b of columns k .. k+b-1 are kept in V (the
+// reflector store, column c holding u for column c, zero above row c+1), their product is
+// H_1 ... H_b = I - V T V^H (T upper triangular, b x b) and Y = A0 V T for the matrix A0 at the
+// panel's start.  Column c = k + i of the panel is first brought up to date,
+//   x = A0[:, c] - Y[:, <i] V[c, <i]^H,   x[k+1..] -= V[k+1.., <i] T^H V[k+1.., <i]^H x[k+1..],
+// its reflector is formed from x[c+1..], then y_i = tau (A0[:, c+1..] u_i - Y[:, <i] (V^H u_i)) and
+// T[<i, i] = -tau T (V^H u_i).  After the panel the trailing columns get A -= Y V^H (all rows) and
+// A[k+1.., ] -= V T^H (V^H A[k+1.., ]), three GEMMs.
+constexpr int kHbB = 32;           // panel width
+constexpr int kHbThreads = 256;    // the column kernel's CTA (32 complex partial sums per thread)
+constexpr int kHbMaxN = 12288;     // the column kernel keeps x (N complex) in shared memory
+
+// Sum over the CTA of per-thread partial sums part[0 .. n) (complex), n <= kHbB; the totals go to
+// out[0 .. n) (shared).  red: shared [warps][kHbB] complex.
+__device__ void hb_multi_sum(double2 (&part)[kHbB], int n, double2* red, double2* out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < kHbB; ++j) {
+    if (j >= n) break;
+    double re = part[j].x, im = part[j].y;
+    for (int o = 16; o > 0; o >>= 1) {
+      re += __shfl_xor_sync(0xffffffffu, re, o);
+      im += __shfl_xor_sync(0xffffffffu, im, o);
+    }
+    if (lane == 0) red[warp * kHbB + j] = make_double2(re, im);
+  }
+  __syncthreads();
+  if (threadIdx.x < n) {
+    double re = 0.0, im = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      re += red[w * kHbB + threadIdx.x].x;
+      im += red[w * kHbB + threadIdx.x].y;
+    }
+    out[threadIdx.x] = make_double2(re, im);
+  }
+  __syncthreads();
+}
+
+// Column c = k + i of the panel (one CTA of kHbThreads).  Y: N x kHbB (column-major, ldy), V: the
+// reflector store (ldv), T: kHbB x kHbB (column-major) of this panel, sv: kHbB (out: V^H u_i).
+// Dynamic shared memory: N complex (x).
+__global__ void __launch_bounds__(kHbThreads) hb_column_kernel(double2* A, long lda, int N, int k, int i,
+                                                               const double2* Y, long ldy, double2* V, long ldv,
+                                                               double2* T, double2* sv) {
+  extern __shared__ __align__(16) double2 x[];
+  __shared__ double2 red[(kHbThreads / 32) * kHbB];
+  __shared__ double2 w[kHbB], z[kHbB];
+  __shared__ double s_norm2, s_a0;
+  const int tid = threadIdx.x;
+  const int c = k + i;
+  // x = A[:, c] - Y[:, <i] conj(V[c, k + <i])
+  for (int r = tid; r < N; r += kHbThreads) {
+    double2 v = A[(size_t)c * lda + r];
+    for (int j = 0; j < i; ++j) {
+      const double2 vc = V[(size_t)(k + j) * ldv + c];
+      cfms(v, Y[(size_t)j * ldy + r], make_double2(vc.x, -vc.y));
+    }
+    x[r] = v;
+  }
+  __syncthreads();
+  if (i > 0) {
+    // w = V[k+1.., <i]^H x[k+1..]
+    double2 part[kHbB];
+#pragma unroll
+    for (int j = 0; j < kHbB; ++j) part[j] = make_double2(0.0, 0.0);
+    for (int r = k + 1 + tid; r < N; r += kHbThreads) {
+      const double2 xr = x[r];
+#pragma unroll
+      for (int j = 0; j < kHbB; ++j) {
+        if (j >= i) break;
+        const double2 v = V[(size_t)(k + j) * ldv + r];
+        cfma(part[j], make_double2(v.x, -v.y), xr);
+      }
+    }
+    hb_multi_sum(part, i, red, w);
+    // z = T^H w  (z_j = sum_{l <= j} conj(T[l, j]) w_l)
+    if (tid < i) {
+      double2 acc = make_double2(0.0, 0.0);
+      for (int l = 0; l <= tid; ++l) {
+        const double2 t = T[(size_t)tid * kHbB + l];
+        cfma(acc, make_double2(t.x, -t.y), w[l]);
+      }
+      z[tid] = acc;
+    }
+    __syncthreads();
+    for (int r = k + 1 + tid; r < N; r += kHbThreads) {
+      double2 v = x[r];
+      for (int j = 0; j < i; ++j) cfms(v, V[(size_t)(k + j) * ldv + r], z[j]);
+      x[r] = v;
+    }
+    __syncthreads();
+  }
+  // reflector of x[c+1 ..]
+  {
+    double ss = 0.0;
+    for (int r = c + 1 + tid; r < N; r += kHbThreads) ss += x[r].x * x[r].x + x[r].y * x[r].y;
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    double* rd = reinterpret_cast<double*>(red);
+    if ((tid & 31) == 0) rd[tid >> 5] = ss;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0.0;
+      for (int q = 0; q < kHbThreads / 32; ++q) t += rd[q];
+      s_norm2 = t;
+      s_a0 = hypot(x[c + 1].x, x[c + 1].y);
+    }
+    __syncthreads();
+  }
+  const double ss = s_norm2, a0 = s_a0;
+  const double2 x0 = x[c + 1];
+  double2 gamma = x0;
+  double winv = 0.0;
+  if (ss > 0.0) {
+    const double nrm = sqrt(ss);
+    const double2 ph = a0 > 0.0 ? make_double2(x0.x / a0, x0.y / a0) : make_double2(1.0, 0.0);
+    gamma = make_double2(-ph.x * nrm, -ph.y * nrm);
+    winv = 1.0 / sqrt(2.0 * ss + 2.0 * nrm * a0);
+  }
+  for (int r = tid; r < N; r += kHbThreads) {
+    double2 u = make_double2(0.0, 0.0);
+    if (r > c && ss > 0.0) {
+      u = x[r];
+      if (r == c + 1) {
+        u.x -= gamma.x;
+        u.y -= gamma.y;
+      }
+      u.x *= winv;
+      u.y *= winv;
+    }
+    V[(size_t)c * ldv + r] = u;
+    A[(size_t)c * lda + r] = r <= c ? x[r] : (r == c + 1 ? gamma : make_double2(0.0, 0.0));
+  }
+  __syncthreads();
+  // s = V[:, <i]^H u_i and the new column of T
+  double2 part[kHbB];
+#pragma unroll
+  for (int j = 0; j < kHbB; ++j) part[j] = make_double2(0.0, 0.0);
+  if (i > 0) {
+    for (int r = c + 1 + tid; r < N; r += kHbThreads) {
+      const double2 u = V[(size_t)c * ldv + r];
+#pragma unroll
+      for (int j = 0; j < kHbB; ++j) {
+        if (j >= i) break;
+        const double2 v = V[(size_t)(k + j) * ldv + r];
+        cfma(part[j], make_double2(v.x, -v.y), u);
+      }
+    }
+  }
+  hb_multi_sum(part, i, red, w);
+  if (tid < kHbB) {
+    // T[:, i]: rows < i from -2 T[<i, <i] s, row i = 2 (or 0 for an identity reflector), rest 0
+    double2 t = make_double2(0.0, 0.0);
+    if (tid < i) {
+      for (int m = tid; m < i; ++m) cfma(t, T[(size_t)m * kHbB + tid], w[m]);
+      t = make_double2(-2.0 * t.x, -2.0 * t.y);
+    } else if (tid == i) {
+      t = make_double2(ss > 0.0 ? 2.0 : 0.0, 0.0);
+    }
+    T[(size_t)i * kHbB + tid] = t;
+    if (tid < i) sv[tid] = w[tid];
+  }
+}
+
+// y_i = 2 (A0[:, c+1 ..] u_i - Y[:, <i] s): the GEMV's chunk partial sums (hess_right_partial_kernel
+// with k = c) and s = V^H u_i from hb_column_kernel.  One thread per row.
+__global__ void hb_y_kernel(int N, int i, const double2* __restrict__ part, int nchunks, const double2* __restrict__ sv,
+                            double2* Y, long ldy, double uzero) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= N) return;
+  double2 p = make_double2(0.0, 0.0);
+  for (int ch = 0; ch < nchunks; ++ch) {
+    p.x += part[(size_t)ch * N + r].x;
+    p.y += part[(size_t)ch * N + r].y;
+  }
+  for (int j = 0; j < i; ++j) cfms(p, Y[(size_t)j * ldy + r], sv[j]);
+  Y[(size_t)i * ldy + r] = make_double2(2.0 * p.x * uzero, 2.0 * p.y * uzero);
+}
+
+// Per panel (b columns at k): VH = V[:, k..k+b)^H (b x N, column-major, ld kHbB) and
+// VT = -V T^H (conj_t) or -V T (N x kHbB, column-major, ld N) for rows r of the grid.
+__global__ void hb_prep_kernel(int N, int k, int b, const double2* __restrict__ V, long ldv,
+                               const double2* __restrict__ T, double2* VH, double2* VT, bool conj_t) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= N) return;
+  double2 v[kHbB];
+#pragma unroll
+  for (int j = 0; j < kHbB; ++j) v[j] = j < b ? V[(size_t)(k + j) * ldv + r] : make_double2(0.0, 0.0);
+#pragma unroll
+  for (int j = 0; j < kHbB; ++j) VH[(size_t)r * kHbB + j] = make_double2(v[j].x, -v[j].y);
+  for (int j = 0; j < kHbB; ++j) {
+    double2 acc = make_double2(0.0, 0.0);
+    if (j < b) {
+      // (V T^H)[r, j] = sum_{l >= j} V[r, l] conj(T[j, l]);  (V T)[r, j] = sum_{l <= j} V[r, l] T[l, j]
+      if (conj_t) {
+        for (int l = j; l < b; ++l) {
+          const double2 t = T[(size_t)l * kHbB + j];
+          cfma(acc, v[l], make_double2(t.x, -t.y));
+        }
+      } else {
+        for (int l = 0; l <= j; ++l) cfma(acc, v[l], T[(size_t)j * kHbB + l]);
+      }
+    }
+    VT[(size_t)j * N + r] = make_double2(-acc.x, -acc.y);
+  }
+}
+
 // ---------------------------------------------------------------- per-energy Hessenberg solves
 // One CTA per unit (energy): the LU of Hs = H + delta I (H upper Hessenberg, row-major Hr,
 // ldh) with partial pivoting between the two candidate rows of each column (the larger

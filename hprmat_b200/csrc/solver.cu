@@ -198,6 +198,8 @@ struct hprmat_b200_ctx {
   int hess_steps_last = 0;       // refinement steps of the last batch
   int hess_fallback_last = 0;    // energies the last shifted scan sent to the LU path
   double hess_ms[6] = {};        // with profiling: reduce, solve, products, refine, U, fallback (ms)
+  bool hess_blocked = true;      // blocked (panel + GEMM) Hessenberg reduction
+  DevBuf hbY, hbT, hbS, hbVH, hbVT, hbW;
   // batched energy scans: worker contexts (own stream and buffers) and the blocks' potentials
   std::vector<hprmat_b200_ctx*> scan_workers;
   std::vector<std::unique_ptr<DevBuf>> scan_cpot;
@@ -2549,7 +2551,10 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_
 // ------------------------------------------------------------------ shifted (Hessenberg) scan
 // Householder reduction of A (N x N, column-major, ld) to upper Hessenberg form in place,
 // A = P H P^H, with P (ld) accumulated from the reflectors (kept in hU, column k: rows k+1 ..).
+static int hess_reduce_blocked(hprmat_b200_ctx* c, double2* A, long ld, int N, double2* P);
+
 static int hess_reduce(hprmat_b200_ctx* c, double2* A, long ld, int N, double2* P) {
+  if (c->hess_blocked && N <= kHbMaxN && N > kHbB + 2) return hess_reduce_blocked(c, A, ld, N, P);
   NvtxRange nv("hprmat.hess.reduce");
   TRY(c->hU.ensure((size_t)ld * N * sizeof(double2)));
   const int nchunk_max = (N + kHessChunk - 1) / kHessChunk;
@@ -2580,6 +2585,80 @@ static int hess_reduce(hprmat_b200_ctx* c, double2* A, long ld, int N, double2* 
   return HPRMAT_B200_OK;
 }
 
+
+// The same reduction in panels of kHbB columns (hessenberg.cuh, "blocked reduction"): per column
+// one CTA brings the column up to date and forms its reflector, a GEMV of the trailing matrix
+// gives the column of Y; per panel three DMMA GEMMs update the trailing columns.  P is
+// accumulated backwards from the identity, panel by panel, by two GEMMs each.
+static int hess_reduce_blocked(hprmat_b200_ctx* c, double2* A, long ld, int N, double2* P) {
+  NvtxRange nv("hprmat.hess.reduce_blocked");
+  const int ncols = N - 2;  // columns 0 .. N-3 get a reflector
+  const int np = (ncols + kHbB - 1) / kHbB;
+  const int nchunk_max = (N + kHessChunk - 1) / kHessChunk;
+  TRY(c->hU.ensure((size_t)ld * N * sizeof(double2)));
+  TRY(c->hPart.ensure((size_t)nchunk_max * N * sizeof(double2)));
+  TRY(c->hbY.ensure((size_t)N * kHbB * sizeof(double2)));
+  TRY(c->hbT.ensure((size_t)np * kHbB * kHbB * sizeof(double2)));
+  TRY(c->hbS.ensure((size_t)kHbB * sizeof(double2)));
+  TRY(c->hbVH.ensure((size_t)kHbB * N * sizeof(double2)));
+  TRY(c->hbVT.ensure((size_t)N * kHbB * sizeof(double2)));
+  TRY(c->hbW.ensure((size_t)kHbB * N * sizeof(double2)));
+  double2* V = c->hU.as<double2>();
+  double2* Y = c->hbY.as<double2>();
+  double2* VH = c->hbVH.as<double2>();
+  double2* VT = c->hbVT.as<double2>();
+  double2* W = c->hbW.as<double2>();
+  const size_t xsm = (size_t)N * sizeof(double2);
+  TRY(set_smem(hb_column_kernel, xsm));
+  auto gemm = [&](int M, int Nc, int K, const double2* Aop, long lda, const double2* Bop, long ldb, double2* Cop,
+                  long ldc) -> int {
+    if (zgemm_f64_update(M, Nc, K, Aop, lda, Bop, ldb, Cop, ldc, c->stream))
+      return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+    ++c->launches;
+    return HPRMAT_B200_OK;
+  };
+  for (int p = 0; p < np; ++p) {
+    const int k = p * kHbB, b = std::min(kHbB, ncols - k);
+    double2* Tp = c->hbT.as<double2>() + (size_t)p * kHbB * kHbB;
+    for (int i = 0; i < b; ++i) {
+      const int col = k + i;
+      hb_column_kernel<<<1, kHbThreads, xsm, c->stream>>>(A, ld, N, k, i, Y, N, V, ld, Tp, c->hbS.as<double2>());
+      LAUNCH_CHECK();
+      const int nchunk = (N - col - 1 + kHessChunk - 1) / kHessChunk;
+      hess_right_partial_kernel<<<dim3(cdiv_u(N, kHessThreads), nchunk), kHessThreads, 0, c->stream>>>(
+          A, ld, N, col, V, ld, c->hPart.as<double2>());
+      LAUNCH_CHECK();
+      hb_y_kernel<<<cdiv_u(N, 256), 256, 0, c->stream>>>(N, i, c->hPart.as<double2>(), nchunk, c->hbS.as<double2>(), Y,
+                                                         N, 1.0);
+      LAUNCH_CHECK();
+    }
+    if (k + b < N) {
+      const int nt = N - k - b;
+      hb_prep_kernel<<<cdiv_u(N, 128), 128, 0, c->stream>>>(N, k, b, V, ld, Tp, VH, VT, true);
+      LAUNCH_CHECK();
+      // A[:, k+b ..] -= Y V[k+b .., ]^H
+      TRY(gemm(N, nt, b, Y, N, VH + (size_t)(k + b) * kHbB, kHbB, A + (size_t)(k + b) * ld, ld));
+      // W = -V[k+1 .., ]^H A[k+1 .., k+b ..];  A[k+1 .., k+b ..] -= (-V T^H) W
+      HPR_CUDA_TRY(cudaMemsetAsync(W, 0, (size_t)kHbB * nt * sizeof(double2), c->stream));
+      TRY(gemm(b, nt, N - k - 1, VH + (size_t)(k + 1) * kHbB, kHbB, A + (k + 1) + (size_t)(k + b) * ld, ld, W, kHbB));
+      TRY(gemm(N - k - 1, nt, b, VT + (k + 1), N, W, kHbB, A + (k + 1) + (size_t)(k + b) * ld, ld));
+    }
+  }
+  // P = Q_0 Q_1 ... (Q_p = I - V_p T_p V_p^H), backwards from the identity on rows/columns k+1 ..
+  identity_kernel<<<dim3(cdiv_u(N, 256), N), 256, 0, c->stream>>>(P, ld, N);
+  LAUNCH_CHECK();
+  for (int p = np - 1; p >= 0; --p) {
+    const int k = p * kHbB, b = std::min(kHbB, ncols - k);
+    const double2* Tp = c->hbT.as<double2>() + (size_t)p * kHbB * kHbB;
+    const int m = N - k - 1;
+    hb_prep_kernel<<<cdiv_u(N, 128), 128, 0, c->stream>>>(N, k, b, V, ld, Tp, VH, VT, false);
+    LAUNCH_CHECK();
+    HPR_CUDA_TRY(cudaMemsetAsync(W, 0, (size_t)kHbB * m * sizeof(double2), c->stream));
+    TRY(gemm(b, m, m, VH + (size_t)(k + 1) * kHbB, kHbB, P + (k + 1) + (size_t)(k + 1) * ld, ld, W, kHbB));
+    TRY(gemm(m, m, b, VT + (k + 1), N, W, kHbB, P + (k + 1) + (size_t)(k + 1) * ld, ld));
+  }
+  return HPRMAT_B200_OK;
+}
 
 // One J-pi block of hprmat_b200_rmatrix_scan_shifted (hessenberg.cuh for the algebra): C0 is
 // reduced to Hessenberg form once, then the block's energies are solved in batches by O(N^2 nch)
@@ -3632,6 +3711,10 @@ int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* c, const char* key, int value) {
   if (strcmp(key, "reuse_max_inner") == 0) {
     if (value < 0) return fail(HPRMAT_B200_ERR_ARG, "reuse_max_inner must be >= 0");
     c->reuse_max_inner = value;
+    return HPRMAT_B200_OK;
+  }
+  if (strcmp(key, "hess_blocked") == 0) {
+    c->hess_blocked = value != 0;
     return HPRMAT_B200_OK;
   }
   if (strcmp(key, "panel_rpc_min") == 0) {

@@ -162,18 +162,23 @@ def test_scan_autotune_table_and_parity():
     ctx.close()
 
 
-def test_hessenberg_reduction_is_a_unitary_similarity():
-    """The device Householder reduction: A = P H P^H with P unitary and H upper Hessenberg, on a
-    random complex matrix and on a C(E)-like matrix with a wide range of entry sizes."""
+@pytest.mark.parametrize("blocked", [1, 0])
+def test_hessenberg_reduction_is_a_unitary_similarity(blocked):
+    """The device Householder reduction, in panels with GEMM updates (blocked) and column by
+    column: A = P H P^H with P unitary and H upper Hessenberg, on random complex matrices (one
+    order a multiple of the panel width plus two, one not) and on a C(E)-like matrix with a wide
+    range of entry sizes."""
     import torch
     from hprmat_b200 import _native as nat
     lib = nat.load()
     ctx = api.Context(precision="fp64")
+    nat.check(lib.hprmat_b200_dev_set_tuning(ctx._h, b"hess_blocked", blocked))
     rng = np.random.default_rng(3)
     w = workloads.production(seed=41, nch=5, nr=60, rmax=20.0)
     mesh = orc.rmat_ini(60, 1, 20.0)
     bnd = orc.boundary_values(w.nch, w.lval, w.qk, w.eta, 20.0)
     cases = [rng.standard_normal((300, 300)) + 1j * rng.standard_normal((300, 300)),
+             rng.standard_normal((98, 98)) + 1j * rng.standard_normal((98, 98)),
              orc.assemble(mesh, 1, w.nch, w.lval, w.qk, bnd.xc, w.cpot)]
     for A in cases:
         n = A.shape[0]
