@@ -905,13 +905,10 @@ __device__ void cta_gauss_solve(double2* A, int n, double2* B, long ldb, int nrh
 //   Rt(m1,m2) = R(i1,i2) sqrt(k_i1/k_i2) over open channels; solved by Gaussian
 // elimination with partial pivoting (|re|+|im|) in one CTA.  cu (ndim x ndim) is zeroed
 // and receives U in its leading nopen x nopen block.  Work arrays: zo, zi (nopen^2).
-__global__ void __launch_bounds__(1024) umatrix_kernel(const double2* __restrict__ R, int nch,
-                                                       const int* __restrict__ open_idx,
-                                                       const double* __restrict__ qk,
-                                                       const double2* __restrict__ co,
-                                                       const double2* __restrict__ cop, int no,
-                                                       double2* zo, double2* zi, double2* cu,
-                                                       int ndim, int* info) {
+__device__ void umatrix_body(const double2* __restrict__ R, int nch, const int* __restrict__ open_idx,
+                             const double* __restrict__ qk, const double2* __restrict__ co,
+                             const double2* __restrict__ cop, int no, double2* zo, double2* zi, double2* cu, int ndim,
+                             int* info) {
   const int tid = threadIdx.x, NT = blockDim.x;
   for (int idx = tid; idx < ndim * ndim; idx += NT) cu[idx] = make_double2(0, 0);
   for (int idx = tid; idx < no * no; idx += NT) {
@@ -940,6 +937,37 @@ __global__ void __launch_bounds__(1024) umatrix_kernel(const double2* __restrict
     int m1 = idx % no, m2 = idx / no;
     cu[m1 + (size_t)m2 * ndim] = zi[idx];
   }
+}
+
+__global__ void __launch_bounds__(1024) umatrix_kernel(const double2* __restrict__ R, int nch,
+                                                       const int* __restrict__ open_idx,
+                                                       const double* __restrict__ qk,
+                                                       const double2* __restrict__ co,
+                                                       const double2* __restrict__ cop, int no,
+                                                       double2* zo, double2* zi, double2* cu,
+                                                       int ndim, int* info) {
+  umatrix_body(R, nch, open_idx, qk, co, cop, no, zo, zi, cu, ndim, info);
+}
+
+// The collision-matrix step of many independent units in one launch, one CTA per unit; a unit
+// whose skip word is nonzero is left alone.
+struct UmatUnit {
+  const double2* R;
+  const int* open_idx;
+  const double* qk;
+  const double2* co;
+  const double2* cop;
+  int no;
+  double2* zo;
+  double2* zi;
+  double2* cu;
+  int* info;
+  const int* skip;
+};
+__global__ void __launch_bounds__(1024) umatrix_batch_kernel(const UmatUnit* __restrict__ units, int nch) {
+  const UmatUnit u = units[blockIdx.x];
+  if (*u.skip != 0) return;
+  umatrix_body(u.R, nch, u.open_idx, u.qk, u.co, u.cop, u.no, u.zo, u.zi, u.cu, nch, u.info);
 }
 
 // One step of the R-matrix propagation (src/rmatrix_hp.F90:337-345): with R00, R01, R11 the

@@ -194,12 +194,12 @@ struct hprmat_b200_ctx {
   // sums, W = P^H Q, W^H; per batch of energies the factors and work arrays of every unit
   DevBuf hA, hP, hPH, hU, hHr, hPart, hW, hWH, hChan, hUe, hLm, hSw, hY, hX, hR, hYr, hYT, hS, hT, hRacc, hG,
       hDl, hUnit, hCu, hZo;
-  double hess_budget_gb = 16.0;  // device memory for one batch of energies
+  double hess_budget_gb = 48.0;  // device memory for one batch of energies
   int hess_steps_last = 0;       // refinement steps of the last batch
   int hess_fallback_last = 0;    // energies the last shifted scan sent to the LU path
   double hess_ms[6] = {};        // with profiling: reduce, solve, products, refine, U, fallback (ms)
   bool hess_blocked = true;      // blocked (panel + GEMM) Hessenberg reduction
-  DevBuf hbY, hbT, hbS, hbVH, hbVT, hbW;
+  DevBuf hbY, hbT, hbS, hbVH, hbVT, hbW, hUmat;
   // batched energy scans: worker contexts (own stream and buffers) and the blocks' potentials
   std::vector<hprmat_b200_ctx*> scan_workers;
   std::vector<std::unique_ptr<DevBuf>> scan_cpot;
@@ -2936,18 +2936,33 @@ static int hess_scan_block(hprmat_b200_ctx* c, int bi, const hprmat_b200_scan_bl
     scale_copy_kernel<<<cdiv_u((long)m * nn, 256), 256, 0, c->stream>>>(c->hRacc.as<double2>(), c->hRacc.as<double2>(),
                                                                         (long)m * nn, 1.0 / rmax);
     LAUNCH_CHECK();
-    for (int j = 0; j < m; ++j) {
-      const int e = units[u0 + j];
-      if (hinfo[j] != 0 || hinfo[nb + j] != 0) continue;  // zero Hessenberg / Woodbury pivot: LU path
-      const double* ud_ = unit_d(j);
-      const double2* dz = reinterpret_cast<const double2*>(ud_ + ud);
-      const int* d_open = reinterpret_cast<const int*>(dz + 2 * nch);
-      const int no = bd[e].nopen;
-      umatrix_kernel<<<1, 1024, 0, c->stream>>>(c->hRacc.as<double2>() + (size_t)j * nn, nch, d_open, ud_ + 1 + 3 * nch,
-                                                dz, dz + nch, no, c->hZo.as<double2>(),
-                                                c->hZo.as<double2>() + std::max<size_t>(1, (size_t)no * no),
-                                                c->hCu.as<double2>() + (size_t)j * nn, nch, d_uinfo + j);
+    // one launch for the batch's collision matrices (a unit with a zero Hessenberg or Woodbury
+    // pivot is skipped: it goes to the LU path)
+    {
+      std::vector<UmatUnit> uu(m);
+      TRY(c->hZo.ensure((size_t)2 * m * std::max<size_t>(nn, 1) * sizeof(double2)));
+      for (int jj = 0; jj < m; ++jj) {
+        const double* ud_ = unit_d(jj);
+        const double2* dz = reinterpret_cast<const double2*>(ud_ + ud);
+        UmatUnit& q = uu[jj];
+        q.R = c->hRacc.as<double2>() + (size_t)jj * nn;
+        q.open_idx = reinterpret_cast<const int*>(dz + 2 * nch);
+        q.qk = ud_ + 1 + 3 * nch;
+        q.co = dz;
+        q.cop = dz + nch;
+        q.no = bd[units[u0 + jj]].nopen;
+        q.zo = c->hZo.as<double2>() + (size_t)2 * jj * std::max<size_t>(nn, 1);
+        q.zi = q.zo + std::max<size_t>(nn, 1);
+        q.cu = c->hCu.as<double2>() + (size_t)jj * nn;
+        q.info = d_uinfo + jj;
+        q.skip = hinfo[jj] != 0 ? d_info + jj : d_info2 + jj;
+      }
+      TRY(c->hUmat.ensure((size_t)m * sizeof(UmatUnit)));
+      HPR_CUDA_TRY(cudaMemcpyAsync(c->hUmat.p, uu.data(), (size_t)m * sizeof(UmatUnit), cudaMemcpyHostToDevice,
+                                   c->stream));
+      umatrix_batch_kernel<<<m, 1024, 0, c->stream>>>(c->hUmat.as<UmatUnit>(), nch);
       LAUNCH_CHECK();
+      HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));  // uu outlives its copy
     }
     HPR_CUDA_TRY(cudaMemcpyAsync(hinfo.data() + 2 * nb, d_uinfo, (size_t)nb * sizeof(int), cudaMemcpyDeviceToHost,
                                  c->stream));
