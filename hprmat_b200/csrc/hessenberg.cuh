@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(kHessThreads) hess_left_kernel(double2* A, lon
 // Right application A[:, k+1 ..] <- A[:, k+1 ..] H, rows 0 .. N-1: first p = A[:, k+1 ..] u in
 // column chunks (part[chunk][row]), then A_ij -= 2 p_i conj(u_j).  Grid (row blocks of 256,
 // column chunks of kHessChunk).
-constexpr int kHessChunk = 128;
+constexpr int kHessChunk = 64;
 __global__ void __launch_bounds__(kHessThreads) hess_right_partial_kernel(const double2* __restrict__ A, long lda,
                                                                           int N, int k, const double2* ustore,
                                                                           long ldu, double2* part) {
@@ -129,13 +129,26 @@ __global__ void __launch_bounds__(kHessThreads) hess_right_partial_kernel(const 
   for (int j = j0 + threadIdx.x; j < j1; j += kHessThreads) us[j - j0] = ustore[(size_t)k * ldu + j];
   __syncthreads();
   if (row >= N) return;
-  double pr = 0.0, pi = 0.0;
-  for (int j = j0; j < j1; ++j) {
-    const double2 a = A[(size_t)j * lda + row], u = us[j - j0];
-    pr += a.x * u.x - a.y * u.y;
-    pi += a.x * u.y + a.y * u.x;
+  // four independent sums, four loads in flight per thread
+  double pr[4] = {0.0, 0.0, 0.0, 0.0}, pi[4] = {0.0, 0.0, 0.0, 0.0};
+  int j = j0;
+  for (; j + 3 < j1; j += 4) {
+    double2 a[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) a[q] = A[(size_t)(j + q) * lda + row];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double2 u = us[j + q - j0];
+      pr[q] += a[q].x * u.x - a[q].y * u.y;
+      pi[q] += a[q].x * u.y + a[q].y * u.x;
+    }
   }
-  part[(size_t)blockIdx.y * N + row] = make_double2(pr, pi);
+  for (; j < j1; ++j) {
+    const double2 a = A[(size_t)j * lda + row], u = us[j - j0];
+    pr[0] += a.x * u.x - a.y * u.y;
+    pi[0] += a.x * u.y + a.y * u.x;
+  }
+  part[(size_t)blockIdx.y * N + row] = make_double2(pr[0] + pr[1] + pr[2] + pr[3], pi[0] + pi[1] + pi[2] + pi[3]);
 }
 
 __global__ void __launch_bounds__(kHessThreads) hess_right_update_kernel(double2* A, long lda, int N, int k,
@@ -238,8 +251,6 @@ __global__ void hess_whq_kernel(const double2* __restrict__ P, long ldp, int N, 
 // T[<i, i] = -tau T (V^H u_i).  After the panel the trailing columns get A -= Y V^H (all rows) and
 // A[k+1.., ] -= V T^H (V^H A[k+1.., ]), three GEMMs.
 constexpr int kHbB = 32;           // panel width
-constexpr int kHbThreads = 256;    // the column kernel's CTA (32 complex partial sums per thread)
-constexpr int kHbMaxN = 12288;     // the column kernel keeps x (N complex) in shared memory
 
 // Sum over the CTA of per-thread partial sums part[0 .. n) (complex), n <= kHbB; the totals go to
 // out[0 .. n) (shared).  red: shared [warps][kHbB] complex.
@@ -267,78 +278,157 @@ __device__ void hb_multi_sum(double2 (&part)[kHbB], int n, double2* red, double2
   __syncthreads();
 }
 
-// Column c = k + i of the panel (one CTA of kHbThreads).  Y: N x kHbB (column-major, ldy), V: the
-// reflector store (ldv), T: kHbB x kHbB (column-major) of this panel, sv: kHbB (out: V^H u_i).
-// Dynamic shared memory: N complex (x).
-__global__ void __launch_bounds__(kHbThreads) hb_column_kernel(double2* A, long lda, int N, int k, int i,
-                                                               const double2* Y, long ldy, double2* V, long ldv,
-                                                               double2* T, double2* sv) {
-  extern __shared__ __align__(16) double2 x[];
-  __shared__ double2 red[(kHbThreads / 32) * kHbB];
-  __shared__ double2 w[kHbB], z[kHbB];
-  __shared__ double s_norm2, s_a0;
-  const int tid = threadIdx.x;
-  const int c = k + i;
-  // x = A[:, c] - Y[:, <i] conj(V[c, k + <i])
-  for (int r = tid; r < N; r += kHbThreads) {
-    double2 v = A[(size_t)c * lda + r];
-    for (int j = 0; j < i; ++j) {
+// The column step runs on all SMs: three row-parallel kernels (one row per thread, kHbRowT
+// threads a CTA, G = ceil(N / kHbRowT) CTAs) that hand sums over rows to the next kernel as one
+// partial per CTA (wpart, sspart, spart: [G][kHbB] or [G]), summed again by every CTA of the
+// next kernel in a fixed order.
+constexpr int kHbRowT = 128;
+
+// out[j] = sum over g < G of part[g * kHbB + j], j < n (shared out; all threads of the CTA).
+__device__ void hb_sum_partials(const double2* __restrict__ part, int G, int n, double2* red, double2* out) {
+  const int j = threadIdx.x & 31, q = threadIdx.x >> 5;
+  double re = 0.0, im = 0.0;
+  if (j < n)
+    for (int g = q; g < G; g += kHbRowT / 32) {
+      const double2 v = part[(size_t)g * kHbB + j];
+      re += v.x;
+      im += v.y;
+    }
+  red[q * kHbB + j] = make_double2(re, im);
+  __syncthreads();
+  if (threadIdx.x < n) {
+    double2 t = make_double2(0.0, 0.0);
+    for (int w = 0; w < kHbRowT / 32; ++w) {
+      t.x += red[w * kHbB + threadIdx.x].x;
+      t.y += red[w * kHbB + threadIdx.x].y;
+    }
+    out[threadIdx.x] = t;
+  }
+  __syncthreads();
+}
+
+// Sum over the CTA of one double per thread (all threads get it).
+__device__ double hb_block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < kHbRowT / 32; ++w) t += red[w];
+  __syncthreads();
+  return t;
+}
+
+// (a) iy >= 0: y of panel column iy, from the GEMV's chunk partial sums part[ch][r] (nchunk) and
+// s = V[:, <iy]^H u_iy (spart): Y[r, iy] = 2 (p_r - Y[r, <iy] s); CTA 0 also writes
+// T[<iy, iy] = -2 T[<iy, <iy] s.  (b) ix >= 0: column c = k + ix brought up to date on this row,
+// x_r = A[r, c] - Y[r, <ix] conj(V[c, k + <ix]), and this CTA's part of w = V[k+1.., <ix]^H x[k+1..]
+// into wpart.  Both touch only the thread's own row of Y and x, so (b) may follow (a) in one launch.
+__global__ void __launch_bounds__(kHbRowT) hb_yx_kernel(const double2* A, long lda, int N, int k, int iy, int ix,
+                                                        const double2* __restrict__ part, int nchunk,
+                                                        const double2* spart, double2* Y, long ldy, const double2* V,
+                                                        long ldv, double2* T, double2* x, double2* wpart) {
+  __shared__ double2 red[(kHbRowT / 32) * kHbB];
+  __shared__ double2 sv[kHbB];
+  const int G = gridDim.x;
+  const int r = blockIdx.x * kHbRowT + threadIdx.x;
+  if (iy >= 0) {
+    if (iy > 0) hb_sum_partials(spart, G, iy, red, sv);
+    if (r < N) {
+      double2 p = make_double2(0.0, 0.0);
+      for (int ch = 0; ch < nchunk; ++ch) {
+        const double2 q = part[(size_t)ch * N + r];
+        p.x += q.x;
+        p.y += q.y;
+      }
+      for (int j = 0; j < iy; ++j) cfms(p, Y[(size_t)j * ldy + r], sv[j]);
+      Y[(size_t)iy * ldy + r] = make_double2(2.0 * p.x, 2.0 * p.y);
+    }
+    if (blockIdx.x == 0 && threadIdx.x < iy) {
+      double2 t = make_double2(0.0, 0.0);
+      for (int m = threadIdx.x; m < iy; ++m) cfma(t, T[(size_t)m * kHbB + threadIdx.x], sv[m]);
+      T[(size_t)iy * kHbB + threadIdx.x] = make_double2(-2.0 * t.x, -2.0 * t.y);
+    }
+    __syncthreads();
+  }
+  if (ix < 0) return;
+  const int c = k + ix;
+  double2 v = make_double2(0.0, 0.0);
+  if (r < N) {
+    v = A[(size_t)c * lda + r];
+    for (int j = 0; j < ix; ++j) {
       const double2 vc = V[(size_t)(k + j) * ldv + c];
       cfms(v, Y[(size_t)j * ldy + r], make_double2(vc.x, -vc.y));
     }
     x[r] = v;
   }
-  __syncthreads();
-  if (i > 0) {
-    // w = V[k+1.., <i]^H x[k+1..]
-    double2 part[kHbB];
+  if (ix == 0) return;
+  double2 pp[kHbB];
 #pragma unroll
-    for (int j = 0; j < kHbB; ++j) part[j] = make_double2(0.0, 0.0);
-    for (int r = k + 1 + tid; r < N; r += kHbThreads) {
-      const double2 xr = x[r];
+  for (int j = 0; j < kHbB; ++j) pp[j] = make_double2(0.0, 0.0);
+  if (r < N && r >= k + 1) {
 #pragma unroll
-      for (int j = 0; j < kHbB; ++j) {
-        if (j >= i) break;
-        const double2 v = V[(size_t)(k + j) * ldv + r];
-        cfma(part[j], make_double2(v.x, -v.y), xr);
-      }
+    for (int j = 0; j < kHbB; ++j) {
+      if (j >= ix) break;
+      const double2 w = V[(size_t)(k + j) * ldv + r];
+      cfma(pp[j], make_double2(w.x, -w.y), v);
     }
-    hb_multi_sum(part, i, red, w);
-    // z = T^H w  (z_j = sum_{l <= j} conj(T[l, j]) w_l)
-    if (tid < i) {
+  }
+  hb_multi_sum(pp, ix, red, sv);
+  if (threadIdx.x < ix) wpart[(size_t)blockIdx.x * kHbB + threadIdx.x] = sv[threadIdx.x];
+}
+
+// Column c = k + i, second part: w from wpart, z = T^H w, x[k+1..] -= V[k+1.., <i] z; this CTA's
+// part of ||x[c+1..]||^2 into sspart.
+__global__ void __launch_bounds__(kHbRowT) hb_z_kernel(int N, int k, int i, const double2* V, long ldv,
+                                                       const double2* T, double2* x, const double2* wpart,
+                                                       double* sspart) {
+  __shared__ double2 red[(kHbRowT / 32) * kHbB];
+  __shared__ double2 w[kHbB], z[kHbB];
+  __shared__ double rd[kHbRowT / 32];
+  const int G = gridDim.x, c = k + i;
+  const int r = blockIdx.x * kHbRowT + threadIdx.x;
+  if (i > 0) {
+    hb_sum_partials(wpart, G, i, red, w);
+    // z_j = sum_{l <= j} conj(T[l, j]) w_l
+    if (threadIdx.x < i) {
       double2 acc = make_double2(0.0, 0.0);
-      for (int l = 0; l <= tid; ++l) {
-        const double2 t = T[(size_t)tid * kHbB + l];
+      for (int l = 0; l <= (int)threadIdx.x; ++l) {
+        const double2 t = T[(size_t)threadIdx.x * kHbB + l];
         cfma(acc, make_double2(t.x, -t.y), w[l]);
       }
-      z[tid] = acc;
+      z[threadIdx.x] = acc;
     }
     __syncthreads();
-    for (int r = k + 1 + tid; r < N; r += kHbThreads) {
-      double2 v = x[r];
+  }
+  double ss = 0.0;
+  if (r < N) {
+    double2 v = x[r];
+    if (i > 0 && r >= k + 1) {
       for (int j = 0; j < i; ++j) cfms(v, V[(size_t)(k + j) * ldv + r], z[j]);
       x[r] = v;
     }
-    __syncthreads();
+    if (r > c) ss = v.x * v.x + v.y * v.y;
   }
-  // reflector of x[c+1 ..]
-  {
-    double ss = 0.0;
-    for (int r = c + 1 + tid; r < N; r += kHbThreads) ss += x[r].x * x[r].x + x[r].y * x[r].y;
-    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
-    double* rd = reinterpret_cast<double*>(red);
-    if ((tid & 31) == 0) rd[tid >> 5] = ss;
-    __syncthreads();
-    if (tid == 0) {
-      double t = 0.0;
-      for (int q = 0; q < kHbThreads / 32; ++q) t += rd[q];
-      s_norm2 = t;
-      s_a0 = hypot(x[c + 1].x, x[c + 1].y);
-    }
-    __syncthreads();
-  }
-  const double ss = s_norm2, a0 = s_a0;
+  ss = hb_block_sum(ss, rd);
+  if (threadIdx.x == 0) sspart[blockIdx.x] = ss;
+}
+
+// Column c = k + i, third part: the reflector of x[c+1..] (||x[c+1..]||^2 from sspart): u into
+// V[:, c], the reduced column into A[:, c], this CTA's part of s = V[:, <i]^H u into spart; CTA 0
+// writes T[i.., i] (2, or 0 for an identity reflector, then zeros).
+__global__ void __launch_bounds__(kHbRowT) hb_u_kernel(double2* A, long lda, int N, int k, int i, double2* V,
+                                                       long ldv, double2* T, const double2* x, const double* sspart,
+                                                       double2* spart) {
+  __shared__ double2 red[(kHbRowT / 32) * kHbB];
+  __shared__ double2 sv[kHbB];
+  __shared__ double rd[kHbRowT / 32];
+  const int G = gridDim.x, c = k + i;
+  const int r = blockIdx.x * kHbRowT + threadIdx.x;
+  double t = 0.0;
+  for (int g = threadIdx.x; g < G; g += kHbRowT) t += sspart[g];
+  const double ss = hb_block_sum(t, rd);
   const double2 x0 = x[c + 1];
+  const double a0 = hypot(x0.x, x0.y);
   double2 gamma = x0;
   double winv = 0.0;
   if (ss > 0.0) {
@@ -347,10 +437,11 @@ __global__ void __launch_bounds__(kHbThreads) hb_column_kernel(double2* A, long 
     gamma = make_double2(-ph.x * nrm, -ph.y * nrm);
     winv = 1.0 / sqrt(2.0 * ss + 2.0 * nrm * a0);
   }
-  for (int r = tid; r < N; r += kHbThreads) {
-    double2 u = make_double2(0.0, 0.0);
+  double2 u = make_double2(0.0, 0.0);
+  if (r < N) {
+    const double2 xr = x[r];
     if (r > c && ss > 0.0) {
-      u = x[r];
+      u = xr;
       if (r == c + 1) {
         u.x -= gamma.x;
         u.y -= gamma.y;
@@ -359,52 +450,39 @@ __global__ void __launch_bounds__(kHbThreads) hb_column_kernel(double2* A, long 
       u.y *= winv;
     }
     V[(size_t)c * ldv + r] = u;
-    A[(size_t)c * lda + r] = r <= c ? x[r] : (r == c + 1 ? gamma : make_double2(0.0, 0.0));
+    A[(size_t)c * lda + r] = r <= c ? xr : (r == c + 1 ? gamma : make_double2(0.0, 0.0));
   }
-  __syncthreads();
-  // s = V[:, <i]^H u_i and the new column of T
-  double2 part[kHbB];
+  if (blockIdx.x == 0 && threadIdx.x >= i && threadIdx.x < kHbB)
+    T[(size_t)i * kHbB + threadIdx.x] = make_double2(threadIdx.x == i && ss > 0.0 ? 2.0 : 0.0, 0.0);
+  if (i == 0) return;
+  double2 pp[kHbB];
 #pragma unroll
-  for (int j = 0; j < kHbB; ++j) part[j] = make_double2(0.0, 0.0);
-  if (i > 0) {
-    for (int r = c + 1 + tid; r < N; r += kHbThreads) {
-      const double2 u = V[(size_t)c * ldv + r];
+  for (int j = 0; j < kHbB; ++j) pp[j] = make_double2(0.0, 0.0);
+  if (r < N && r > c) {
 #pragma unroll
-      for (int j = 0; j < kHbB; ++j) {
-        if (j >= i) break;
-        const double2 v = V[(size_t)(k + j) * ldv + r];
-        cfma(part[j], make_double2(v.x, -v.y), u);
-      }
+    for (int j = 0; j < kHbB; ++j) {
+      if (j >= i) break;
+      const double2 w = V[(size_t)(k + j) * ldv + r];
+      cfma(pp[j], make_double2(w.x, -w.y), u);
     }
   }
-  hb_multi_sum(part, i, red, w);
-  if (tid < kHbB) {
-    // T[:, i]: rows < i from -2 T[<i, <i] s, row i = 2 (or 0 for an identity reflector), rest 0
-    double2 t = make_double2(0.0, 0.0);
-    if (tid < i) {
-      for (int m = tid; m < i; ++m) cfma(t, T[(size_t)m * kHbB + tid], w[m]);
-      t = make_double2(-2.0 * t.x, -2.0 * t.y);
-    } else if (tid == i) {
-      t = make_double2(ss > 0.0 ? 2.0 : 0.0, 0.0);
-    }
-    T[(size_t)i * kHbB + tid] = t;
-    if (tid < i) sv[tid] = w[tid];
-  }
+  hb_multi_sum(pp, i, red, sv);
+  if (threadIdx.x < i) spart[(size_t)blockIdx.x * kHbB + threadIdx.x] = sv[threadIdx.x];
 }
 
-// y_i = 2 (A0[:, c+1 ..] u_i - Y[:, <i] s): the GEMV's chunk partial sums (hess_right_partial_kernel
-// with k = c) and s = V^H u_i from hb_column_kernel.  One thread per row.
-__global__ void hb_y_kernel(int N, int i, const double2* __restrict__ part, int nchunks, const double2* __restrict__ sv,
-                            double2* Y, long ldy, double uzero) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= N) return;
-  double2 p = make_double2(0.0, 0.0);
-  for (int ch = 0; ch < nchunks; ++ch) {
-    p.x += part[(size_t)ch * N + r].x;
-    p.y += part[(size_t)ch * N + r].y;
+// C (column-major, ldc, M x Nc) += sum of the split-K slices tmp[z] (same layout, slice stride
+// ldc * Nc): the partial products of a GEMM cut along K.
+__global__ void splitk_sum_kernel(double2* C, long ldc, int M, int Nc, const double2* __restrict__ tmp, int slices) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)M * Nc) return;
+  const int r = (int)(idx % M), col = (int)(idx / M);
+  const size_t off = (size_t)col * ldc + r, stride = (size_t)ldc * Nc;
+  double2 v = C[off];
+  for (int z = 0; z < slices; ++z) {
+    v.x += tmp[off + z * stride].x;
+    v.y += tmp[off + z * stride].y;
   }
-  for (int j = 0; j < i; ++j) cfms(p, Y[(size_t)j * ldy + r], sv[j]);
-  Y[(size_t)i * ldy + r] = make_double2(2.0 * p.x * uzero, 2.0 * p.y * uzero);
+  C[off] = v;
 }
 
 // Per panel (b columns at k): VH = V[:, k..k+b)^H (b x N, column-major, ld kHbB) and

@@ -199,7 +199,7 @@ struct hprmat_b200_ctx {
   int hess_fallback_last = 0;    // energies the last shifted scan sent to the LU path
   double hess_ms[6] = {};        // with profiling: reduce, solve, products, refine, U, fallback (ms)
   bool hess_blocked = true;      // blocked (panel + GEMM) Hessenberg reduction
-  DevBuf hbY, hbT, hbS, hbVH, hbVT, hbW, hUmat;
+  DevBuf hbY, hbT, hbX, hbPart, hbVH, hbVT, hbW, hbTmp, hUmat;
   // batched energy scans: worker contexts (own stream and buffers) and the blocks' potentials
   std::vector<hprmat_b200_ctx*> scan_workers;
   std::vector<std::unique_ptr<DevBuf>> scan_cpot;
@@ -2554,7 +2554,7 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_
 static int hess_reduce_blocked(hprmat_b200_ctx* c, double2* A, long ld, int N, double2* P);
 
 static int hess_reduce(hprmat_b200_ctx* c, double2* A, long ld, int N, double2* P) {
-  if (c->hess_blocked && N <= kHbMaxN && N > kHbB + 2) return hess_reduce_blocked(c, A, ld, N, P);
+  if (c->hess_blocked && N > kHbB + 2) return hess_reduce_blocked(c, A, ld, N, P);
   NvtxRange nv("hprmat.hess.reduce");
   TRY(c->hU.ensure((size_t)ld * N * sizeof(double2)));
   const int nchunk_max = (N + kHessChunk - 1) / kHessChunk;
@@ -2599,7 +2599,6 @@ static int hess_reduce_blocked(hprmat_b200_ctx* c, double2* A, long ld, int N, d
   TRY(c->hPart.ensure((size_t)nchunk_max * N * sizeof(double2)));
   TRY(c->hbY.ensure((size_t)N * kHbB * sizeof(double2)));
   TRY(c->hbT.ensure((size_t)np * kHbB * kHbB * sizeof(double2)));
-  TRY(c->hbS.ensure((size_t)kHbB * sizeof(double2)));
   TRY(c->hbVH.ensure((size_t)kHbB * N * sizeof(double2)));
   TRY(c->hbVT.ensure((size_t)N * kHbB * sizeof(double2)));
   TRY(c->hbW.ensure((size_t)kHbB * N * sizeof(double2)));
@@ -2608,8 +2607,14 @@ static int hess_reduce_blocked(hprmat_b200_ctx* c, double2* A, long ld, int N, d
   double2* VH = c->hbVH.as<double2>();
   double2* VT = c->hbVT.as<double2>();
   double2* W = c->hbW.as<double2>();
-  const size_t xsm = (size_t)N * sizeof(double2);
-  TRY(set_smem(hb_column_kernel, xsm));
+  const int G = cdiv_u(N, kHbRowT);
+  TRY(c->hbX.ensure((size_t)N * sizeof(double2)));
+  TRY(c->hbPart.ensure((size_t)G * (2 * kHbB * sizeof(double2) + sizeof(double))));
+  double2* xv = c->hbX.as<double2>();
+  double2* wpart = c->hbPart.as<double2>();
+  double2* spart = wpart + (size_t)G * kHbB;
+  double* sspart = reinterpret_cast<double*>(spart + (size_t)G * kHbB);
+  double2* part = c->hPart.as<double2>();
   auto gemm = [&](int M, int Nc, int K, const double2* Aop, long lda, const double2* Bop, long ldb, double2* Cop,
                   long ldc) -> int {
     if (zgemm_f64_update(M, Nc, K, Aop, lda, Bop, ldb, Cop, ldc, c->stream))
@@ -2617,19 +2622,44 @@ static int hess_reduce_blocked(hprmat_b200_ctx* c, double2* A, long ld, int N, d
     ++c->launches;
     return HPRMAT_B200_OK;
   };
+  // the short-wide products (M = panel width, K up to N) cut along K into slices that run side
+  // by side, then summed into C
+  auto gemm_splitk = [&](int M, int Nc, int K, const double2* Aop, long lda, const double2* Bop, long ldb,
+                         double2* Cop, long ldc) -> int {
+    const int S = std::max(1, std::min(16, K / 256));
+    if (S == 1) return gemm(M, Nc, K, Aop, lda, Bop, ldb, Cop, ldc);
+    const int Ks = K / S, tail = K - S * Ks;
+    const int slices = S + (tail > 0 ? 1 : 0);
+    const size_t slice = (size_t)ldc * Nc;
+    TRY(c->hbTmp.ensure((size_t)slices * slice * sizeof(double2)));
+    double2* tmp = c->hbTmp.as<double2>();
+    HPR_CUDA_TRY(cudaMemsetAsync(tmp, 0, (size_t)slices * slice * sizeof(double2), c->stream));
+    if (zgemm_f64_update_batched(M, Nc, Ks, Aop, lda, (long)Ks * lda, Bop, ldb, Ks, tmp, ldc, (long)slice, S,
+                                 c->stream))
+      return fail(HPRMAT_B200_ERR_CUDA, "%s", hprmat_b200_last_error());
+    if (tail > 0) TRY(gemm(M, Nc, tail, Aop + (size_t)S * Ks * lda, lda, Bop + (size_t)S * Ks, ldb, tmp + S * slice, ldc));
+    splitk_sum_kernel<<<cdiv_u((long)M * Nc, 256), 256, 0, c->stream>>>(Cop, ldc, M, Nc, tmp, slices);
+    LAUNCH_CHECK();
+    return HPRMAT_B200_OK;
+  };
   for (int p = 0; p < np; ++p) {
     const int k = p * kHbB, b = std::min(kHbB, ncols - k);
     double2* Tp = c->hbT.as<double2>() + (size_t)p * kHbB * kHbB;
+    // column i: x (with y of column i - 1), z and the norm, the reflector, the GEMV
+    hb_yx_kernel<<<G, kHbRowT, 0, c->stream>>>(A, ld, N, k, -1, 0, part, 0, spart, Y, N, V, ld, Tp, xv, wpart);
+    LAUNCH_CHECK();
     for (int i = 0; i < b; ++i) {
       const int col = k + i;
-      hb_column_kernel<<<1, kHbThreads, xsm, c->stream>>>(A, ld, N, k, i, Y, N, V, ld, Tp, c->hbS.as<double2>());
+      hb_z_kernel<<<G, kHbRowT, 0, c->stream>>>(N, k, i, V, ld, Tp, xv, wpart, sspart);
+      LAUNCH_CHECK();
+      hb_u_kernel<<<G, kHbRowT, 0, c->stream>>>(A, ld, N, k, i, V, ld, Tp, xv, sspart, spart);
       LAUNCH_CHECK();
       const int nchunk = (N - col - 1 + kHessChunk - 1) / kHessChunk;
       hess_right_partial_kernel<<<dim3(cdiv_u(N, kHessThreads), nchunk), kHessThreads, 0, c->stream>>>(
-          A, ld, N, col, V, ld, c->hPart.as<double2>());
+          A, ld, N, col, V, ld, part);
       LAUNCH_CHECK();
-      hb_y_kernel<<<cdiv_u(N, 256), 256, 0, c->stream>>>(N, i, c->hPart.as<double2>(), nchunk, c->hbS.as<double2>(), Y,
-                                                         N, 1.0);
+      hb_yx_kernel<<<G, kHbRowT, 0, c->stream>>>(A, ld, N, k, i, i + 1 < b ? i + 1 : -1, part, nchunk, spart, Y, N, V,
+                                                 ld, Tp, xv, wpart);
       LAUNCH_CHECK();
     }
     if (k + b < N) {
@@ -2640,7 +2670,8 @@ static int hess_reduce_blocked(hprmat_b200_ctx* c, double2* A, long ld, int N, d
       TRY(gemm(N, nt, b, Y, N, VH + (size_t)(k + b) * kHbB, kHbB, A + (size_t)(k + b) * ld, ld));
       // W = -V[k+1 .., ]^H A[k+1 .., k+b ..];  A[k+1 .., k+b ..] -= (-V T^H) W
       HPR_CUDA_TRY(cudaMemsetAsync(W, 0, (size_t)kHbB * nt * sizeof(double2), c->stream));
-      TRY(gemm(b, nt, N - k - 1, VH + (size_t)(k + 1) * kHbB, kHbB, A + (k + 1) + (size_t)(k + b) * ld, ld, W, kHbB));
+      TRY(gemm_splitk(b, nt, N - k - 1, VH + (size_t)(k + 1) * kHbB, kHbB, A + (k + 1) + (size_t)(k + b) * ld, ld, W,
+                      kHbB));
       TRY(gemm(N - k - 1, nt, b, VT + (k + 1), N, W, kHbB, A + (k + 1) + (size_t)(k + b) * ld, ld));
     }
   }
@@ -2654,7 +2685,7 @@ static int hess_reduce_blocked(hprmat_b200_ctx* c, double2* A, long ld, int N, d
     hb_prep_kernel<<<cdiv_u(N, 128), 128, 0, c->stream>>>(N, k, b, V, ld, Tp, VH, VT, false);
     LAUNCH_CHECK();
     HPR_CUDA_TRY(cudaMemsetAsync(W, 0, (size_t)kHbB * m * sizeof(double2), c->stream));
-    TRY(gemm(b, m, m, VH + (size_t)(k + 1) * kHbB, kHbB, P + (k + 1) + (size_t)(k + 1) * ld, ld, W, kHbB));
+    TRY(gemm_splitk(b, m, m, VH + (size_t)(k + 1) * kHbB, kHbB, P + (k + 1) + (size_t)(k + 1) * ld, ld, W, kHbB));
     TRY(gemm(m, m, b, VT + (k + 1), N, W, kHbB, P + (k + 1) + (size_t)(k + 1) * ld, ld));
   }
   return HPRMAT_B200_OK;
@@ -2793,7 +2824,8 @@ static int hess_scan_block(hprmat_b200_ctx* c, int bi, const hprmat_b200_scan_bl
   TRY(set_smem(hess_woodbury_kernel, hess_woodbury_smem(nch)));
   std::vector<unsigned char> hu((size_t)nb * ubp);
   std::vector<int> hinfo(3 * (size_t)nb);
-  std::vector<double> hchg(nb);
+  std::vector<double> hchg(nb), hprev(nb);
+  std::vector<char> hconv(nb);
   const double2* P = c->hP.as<double2>();
   const double2* PH = c->hPH.as<double2>();
   const double2* WH = c->hWH.as<double2>();
@@ -2911,8 +2943,18 @@ static int hess_scan_block(hprmat_b200_ctx* c, int bi, const hprmat_b200_scan_bl
       LAUNCH_CHECK();
       HPR_CUDA_TRY(cudaMemcpyAsync(hchg.data(), d_chg, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
       HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+      // Converged: the change is below surface_tol, or the error it leaves is predicted far below
+      // it.  The change of step s is the error of the iterate before it; every step multiplies the
+      // error by about the solver's relative accuracy, which is the first change itself (the same
+      // Hessenberg solve made the first iterate's error) and later the ratio of two changes.
       bool all = true;
-      for (int j = 0; j < m; ++j) all = all && hchg[j] < c->opts.surface_tol;
+      for (int j = 0; j < m; ++j) {
+        const double chg = hchg[j];
+        const double rate = steps == 0 ? chg : (hprev[j] > 0.0 ? chg / hprev[j] : 0.0);
+        hconv[j] = chg < c->opts.surface_tol || 1e3 * chg * std::max(rate, 1e-16) < c->opts.surface_tol;
+        hprev[j] = chg;
+        all = all && hconv[j];
+      }
       if (all || steps + 1 == max_steps) {
         ++steps;
         break;
@@ -2974,7 +3016,7 @@ static int hess_scan_block(hprmat_b200_ctx* c, int bi, const hprmat_b200_scan_bl
         continue;
       }
       int s = hinfo[2 * nb + j] != 0 ? HPRMAT_B200_SINGULAR : HPRMAT_B200_OK;
-      if (s == HPRMAT_B200_OK && !(hchg[j] < c->opts.surface_tol)) s = HPRMAT_B200_NOT_CONVERGED;
+      if (s == HPRMAT_B200_OK && !hconv[j]) s = HPRMAT_B200_NOT_CONVERGED;
       if (s == HPRMAT_B200_SINGULAR) set_last_error_msg("rmatrix_scan_shifted: singular Z_O in the collision-matrix step");
       if (s != HPRMAT_B200_SINGULAR) {
         HPR_CUDA_TRY(cudaMemcpyAsync(B.cu + (size_t)e * nn * 2, c->hCu.as<double2>() + (size_t)j * nn,

@@ -155,14 +155,29 @@ __global__ void __launch_bounds__(kThreads, 2)
       }
     }
     if ((int)(g % nchunks) == nchunks - 1) {
-      // the tile is complete: C -= acc, then start the next tile's accumulators at zero
+      // the tile is complete: C -= acc, then start the next tile's accumulators at zero.  The C
+      // loads of a row group of 8 go out before the previous group is written, so the loads'
+      // latency overlaps instead of stalling on every element.
       const long t = blockIdx.x + (g / nchunks) * (long)gridDim.x;
       const int z = (int)(t / ((long)mt * nt));
       const int r = (int)(t % ((long)mt * nt));
       const int m0 = (r % mt) * kBM, n0 = (r / mt) * kBN;
       double2* Cz = C + (size_t)z * sC;
+      double2 cv[2][4][2];
+      auto load_group = [&](int i, double2 (&dst)[4][2]) {
+        const int row = m0 + wm + 8 * i + fr;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int col = n0 + wn + 8 * j + 2 * fk + e;
+            dst[j][e] = (row < M && col < N) ? Cz[(size_t)row + (size_t)col * ldc] : make_double2(0.0, 0.0);
+          }
+      };
+      load_group(0, cv[0]);
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
+        if (i + 1 < 4) load_group(i + 1, cv[(i + 1) & 1]);
         const int row = m0 + wm + 8 * i + fr;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -170,11 +185,10 @@ __global__ void __launch_bounds__(kThreads, 2)
           for (int e = 0; e < 2; ++e) {
             const int col = n0 + wn + 8 * j + 2 * fk + e;
             if (row < M && col < N) {
-              double2* p = Cz + (size_t)row + (size_t)col * ldc;
-              double2 v = *p;
+              double2 v = cv[i & 1][j][e];
               v.x -= accr[i][j][e];
               v.y -= acci[i][j][e];
-              *p = v;
+              Cz[(size_t)row + (size_t)col * ldc] = v;
             }
             accr[i][j][e] = 0.0;
             acci[i][j][e] = 0.0;
