@@ -20,6 +20,7 @@
 // H x = gamma e1, and A <- H A H is a similarity.  After the steps k = 0 .. N-3,
 // C0 = P H_final P^H with P = H_0 H_1 ... H_{N-3}.
 #pragma once
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -129,18 +130,18 @@ __global__ void __launch_bounds__(kHessThreads) hess_right_partial_kernel(const 
   for (int j = j0 + threadIdx.x; j < j1; j += kHessThreads) us[j - j0] = ustore[(size_t)k * ldu + j];
   __syncthreads();
   if (row >= N) return;
-  // four independent sums, four loads in flight per thread
+  // four independent sums, eight loads in flight per thread
   double pr[4] = {0.0, 0.0, 0.0, 0.0}, pi[4] = {0.0, 0.0, 0.0, 0.0};
   int j = j0;
-  for (; j + 3 < j1; j += 4) {
-    double2 a[4];
+  for (; j + 7 < j1; j += 8) {
+    double2 a[8];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) a[q] = A[(size_t)(j + q) * lda + row];
+    for (int q = 0; q < 8; ++q) a[q] = A[(size_t)(j + q) * lda + row];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < 8; ++q) {
       const double2 u = us[j + q - j0];
-      pr[q] += a[q].x * u.x - a[q].y * u.y;
-      pi[q] += a[q].x * u.y + a[q].y * u.x;
+      pr[q & 3] += a[q].x * u.x - a[q].y * u.y;
+      pi[q & 3] += a[q].x * u.y + a[q].y * u.x;
     }
   }
   for (; j < j1; ++j) {
@@ -252,195 +253,244 @@ __global__ void hess_whq_kernel(const double2* __restrict__ P, long ldp, int N, 
 // A[k+1.., ] -= V T^H (V^H A[k+1.., ]), three GEMMs.
 constexpr int kHbB = 32;           // panel width
 
-// Sum over the CTA of per-thread partial sums part[0 .. n) (complex), n <= kHbB; the totals go to
-// out[0 .. n) (shared).  red: shared [warps][kHbB] complex.
-__device__ void hb_multi_sum(double2 (&part)[kHbB], int n, double2* red, double2* out) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+// The column step runs on one thread-block cluster (G = 8 or 16 CTAs of kHbCT threads, CTA q
+// holding rows [q rpc, (q + 1) rpc) of x in shared memory); its three sums over all rows are one
+// partial per CTA in shared memory, summed by every CTA through the cluster's distributed shared
+// memory after a hardware cluster barrier.  The GEMV that follows each column needs the
+// bandwidth of all SMs and is a launch of its own (hb_gemv_kernel).
+constexpr int kHbCT = 256;
+// The loops over the panel's earlier columns j < n (n runtime, at most kHbB) load in groups of 8
+// predicated loads (zero beyond n) issued together, so that their L2 latencies overlap.
+constexpr int kHbGrp = 8;
+
+// acc -= sum_{j < n} Y[j * ldy] * s[j]  (column stride ldy; s in shared memory)
+__device__ __forceinline__ void hb_sub_cols(double2& acc, const double2* Y, long ldy, const double2* s, int n) {
 #pragma unroll
-  for (int j = 0; j < kHbB; ++j) {
-    if (j >= n) break;
-    double re = part[j].x, im = part[j].y;
-    for (int o = 16; o > 0; o >>= 1) {
-      re += __shfl_xor_sync(0xffffffffu, re, o);
-      im += __shfl_xor_sync(0xffffffffu, im, o);
-    }
-    if (lane == 0) red[warp * kHbB + j] = make_double2(re, im);
+  for (int j0 = 0; j0 < kHbB; j0 += kHbGrp) {
+    if (j0 >= n) break;
+    double2 y[kHbGrp];
+#pragma unroll
+    for (int q = 0; q < kHbGrp; ++q) y[q] = j0 + q < n ? Y[(size_t)(j0 + q) * ldy] : make_double2(0.0, 0.0);
+#pragma unroll
+    for (int q = 0; q < kHbGrp; ++q)
+      if (j0 + q < n) cfms(acc, y[q], s[j0 + q]);
   }
-  __syncthreads();
-  if (threadIdx.x < n) {
-    double re = 0.0, im = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-      re += red[w * kHbB + threadIdx.x].x;
-      im += red[w * kHbB + threadIdx.x].y;
+}
+
+
+// acc1 -= sum_{j < n} Y[j * ldy] s1[j] and acc2 -= sum_{j < n} Y[j * ldy] s2[j], one load of each Y
+__device__ __forceinline__ void hb_sub_cols2(double2& acc1, const double2* s1, double2& acc2, const double2* s2,
+                                             const double2* Y, long ldy, int n) {
+#pragma unroll
+  for (int j0 = 0; j0 < kHbB; j0 += kHbGrp) {
+    if (j0 >= n) break;
+    double2 y[kHbGrp];
+#pragma unroll
+    for (int q = 0; q < kHbGrp; ++q) y[q] = j0 + q < n ? Y[(size_t)(j0 + q) * ldy] : make_double2(0.0, 0.0);
+#pragma unroll
+    for (int q = 0; q < kHbGrp; ++q)
+      if (j0 + q < n) {
+        cfms(acc1, y[q], s1[j0 + q]);
+        cfms(acc2, y[q], s2[j0 + q]);
+      }
+  }
+}
+
+namespace cgh = cooperative_groups;
+
+// out[j] = sum over rows r in [rlo, rhi) of conj(V[(k + j), r]) vec[r - r0], j < n (Vk = V + k ldv;
+// vec and out in shared memory): warp w takes j = 4w .. 4w + 3 over all the rows (lanes on
+// consecutive rows), then sums across its lanes.
+static_assert((kHbCT / 32) * 4 >= kHbB, "four columns per warp cover the panel");
+__device__ void hb_cta_dots(const double2* Vk, long ldv, const double2* vec, int rlo, int rhi, int r0, int n,
+                            double2* out) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, jb = warp * 4;
+  if (jb < n) {
+    double2 acc[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc[e] = make_double2(0.0, 0.0);
+#pragma unroll 4
+    for (int r = rlo + lane; r < rhi; r += 32) {
+      const double2 xr = vec[r - r0];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const double2 v = jb + e < n ? Vk[(size_t)(jb + e) * ldv + r] : make_double2(0.0, 0.0);
+        cfma(acc[e], make_double2(v.x, -v.y), xr);
+      }
     }
-    out[threadIdx.x] = make_double2(re, im);
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      for (int o = 16; o > 0; o >>= 1) {
+        acc[e].x += __shfl_xor_sync(0xffffffffu, acc[e].x, o);
+        acc[e].y += __shfl_xor_sync(0xffffffffu, acc[e].y, o);
+      }
+    if (lane == 0)
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (jb + e < n) out[jb + e] = acc[e];
   }
   __syncthreads();
 }
 
-// The column step runs on all SMs: three row-parallel kernels (one row per thread, kHbRowT
-// threads a CTA, G = ceil(N / kHbRowT) CTAs) that hand sums over rows to the next kernel as one
-// partial per CTA (wpart, sspart, spart: [G][kHbB] or [G]), summed again by every CTA of the
-// next kernel in a fixed order.
-constexpr int kHbRowT = 128;
-
-// out[j] = sum over g < G of part[g * kHbB + j], j < n (shared out; all threads of the CTA).
-__device__ void hb_sum_partials(const double2* __restrict__ part, int G, int n, double2* red, double2* out) {
-  const int j = threadIdx.x & 31, q = threadIdx.x >> 5;
-  double re = 0.0, im = 0.0;
+// tot[j] = sum over the cluster's ranks g < G of rank g's mine[j], j < n (tot shared; red: shared
+// [kHbCT / 32][32]).  Thread t reads ranks t / 32, t / 32 + 8, .. of j = t % 32: the remote loads of
+// all ranks are in flight together.
+__device__ void hb_cluster_sum(const cgh::cluster_group& cl, int G, double2* mine, int n, double2* red, double2* tot) {
+  const int j = threadIdx.x & 31, g0 = threadIdx.x >> 5;
+  double2 t = make_double2(0.0, 0.0);
   if (j < n)
-    for (int g = q; g < G; g += kHbRowT / 32) {
-      const double2 v = part[(size_t)g * kHbB + j];
-      re += v.x;
-      im += v.y;
+    for (int g = g0; g < G; g += kHbCT / 32) {
+      const double2 m = cl.map_shared_rank(mine, (unsigned)g)[j];
+      t.x += m.x;
+      t.y += m.y;
     }
-  red[q * kHbB + j] = make_double2(re, im);
+  red[g0 * 32 + j] = t;
   __syncthreads();
-  if (threadIdx.x < n) {
-    double2 t = make_double2(0.0, 0.0);
-    for (int w = 0; w < kHbRowT / 32; ++w) {
-      t.x += red[w * kHbB + threadIdx.x].x;
-      t.y += red[w * kHbB + threadIdx.x].y;
+  if ((int)threadIdx.x < n) {
+    double2 s = red[threadIdx.x];
+    for (int w = 1; w < kHbCT / 32; ++w) {
+      s.x += red[w * 32 + threadIdx.x].x;
+      s.y += red[w * 32 + threadIdx.x].y;
     }
-    out[threadIdx.x] = t;
+    tot[threadIdx.x] = s;
   }
   __syncthreads();
 }
 
-// Sum over the CTA of one double per thread (all threads get it).
-__device__ double hb_block_sum(double v, double* red) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-  __syncthreads();
-  double t = 0.0;
-  for (int w = 0; w < kHbRowT / 32; ++w) t += red[w];
-  __syncthreads();
-  return t;
-}
+struct HbColArgs {
+  double2* A;
+  long lda;
+  int N, k;
+  int iy, ix;            // y of panel column iy (if >= 0), then column ix (if >= 0)
+  int rpc;               // rows per CTA
+  const double2* part;   // GEMV chunk sums of column k + iy: part[ch * N + r]
+  int nchunk;
+  double2* Y;            // N x kHbB, column-major (ldy)
+  long ldy;
+  double2* V;            // reflector store (ldv)
+  long ldv;
+  double2* T;            // kHbB x kHbB of this panel
+  double2* s;            // kHbB: V[:, <i]^H u_i of the last column done (rank 0 writes it)
+};
 
-// (a) iy >= 0: y of panel column iy, from the GEMV's chunk partial sums part[ch][r] (nchunk) and
-// s = V[:, <iy]^H u_iy (spart): Y[r, iy] = 2 (p_r - Y[r, <iy] s); CTA 0 also writes
-// T[<iy, iy] = -2 T[<iy, <iy] s.  (b) ix >= 0: column c = k + ix brought up to date on this row,
-// x_r = A[r, c] - Y[r, <ix] conj(V[c, k + <ix]), and this CTA's part of w = V[k+1.., <ix]^H x[k+1..]
-// into wpart.  Both touch only the thread's own row of Y and x, so (b) may follow (a) in one launch.
-__global__ void __launch_bounds__(kHbRowT) hb_yx_kernel(const double2* A, long lda, int N, int k, int iy, int ix,
-                                                        const double2* __restrict__ part, int nchunk,
-                                                        const double2* spart, double2* Y, long ldy, const double2* V,
-                                                        long ldv, double2* T, double2* x, double2* wpart) {
-  __shared__ double2 red[(kHbRowT / 32) * kHbB];
-  __shared__ double2 sv[kHbB];
-  const int G = gridDim.x;
-  const int r = blockIdx.x * kHbRowT + threadIdx.x;
-  if (iy >= 0) {
-    if (iy > 0) hb_sum_partials(spart, G, iy, red, sv);
-    if (r < N) {
-      double2 p = make_double2(0.0, 0.0);
-      for (int ch = 0; ch < nchunk; ++ch) {
-        const double2 q = part[(size_t)ch * N + r];
-        p.x += q.x;
-        p.y += q.y;
+// (a) iy >= 0: Y[r, iy] = 2 (p_r - Y[r, <iy] s), p_r the GEMV chunk sums, s of column iy.
+// (b) ix >= 0, column c = k + ix: x_r = A[r, c] - Y[r, <ix] conj(V[c, k + <ix]); w = V[k+1.., <ix]^H x;
+// z = T^H w; x[k+1..] -= V z; the reflector of x[c+1..] into V[:, c] and A[:, c]; s = V[:, <ix]^H u
+// and T[:, ix] (rank 0).  With both, ix = iy + 1, and one pass over Y[r, <iy] serves (a) and (b).
+// Dynamic shared memory: rpc complex (x).
+__global__ void __launch_bounds__(kHbCT) hb_col_cluster_kernel(HbColArgs a) {
+  extern __shared__ __align__(16) double2 xs[];
+  __shared__ double2 mine[kHbB];  // this CTA's partial sums, read by the whole cluster
+  __shared__ double2 tot[kHbB], zv[kHbB], cv[kHbB], sv[kHbB];
+  __shared__ double2 Ts[kHbB * kHbB];  // T of the panel (columns < ix are final)
+  __shared__ double2 red[kHbCT];
+  __shared__ double mine_ss, rd[kHbCT / 32], sst_s;
+  __shared__ double2 mine_x0, x0_s;
+  cgh::cluster_group cl = cgh::this_cluster();
+  const int G = (int)cl.num_blocks(), q = (int)cl.block_rank();
+  const int tid = threadIdx.x, N = a.N, k = a.k;
+  const int r0 = q * a.rpc, r1 = min(N, r0 + a.rpc);
+  const int i = a.ix, c = k + i;
+  if (tid < a.iy) sv[tid] = a.s[tid];
+  if (tid < i) {
+    const double2 vc = a.V[(size_t)(k + tid) * a.ldv + c];
+    cv[tid] = make_double2(vc.x, -vc.y);
+  }
+  if (i > 0)
+    for (int e = tid; e < kHbB * i; e += kHbCT) Ts[e] = a.T[e];
+  __syncthreads();
+  for (int r = r0 + tid; r < r1; r += kHbCT) {
+    double2 xr = i >= 0 ? a.A[(size_t)c * a.lda + r] : make_double2(0.0, 0.0);
+    if (a.iy >= 0) {
+      double pr[4] = {0.0, 0.0, 0.0, 0.0}, pi[4] = {0.0, 0.0, 0.0, 0.0};
+      int ch = 0;
+      for (; ch + 3 < a.nchunk; ch += 4) {
+        double2 t[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) t[e] = a.part[(size_t)(ch + e) * N + r];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          pr[e] += t[e].x;
+          pi[e] += t[e].y;
+        }
       }
-      for (int j = 0; j < iy; ++j) cfms(p, Y[(size_t)j * ldy + r], sv[j]);
-      Y[(size_t)iy * ldy + r] = make_double2(2.0 * p.x, 2.0 * p.y);
+      for (; ch < a.nchunk; ++ch) {
+        const double2 t = a.part[(size_t)ch * N + r];
+        pr[0] += t.x;
+        pi[0] += t.y;
+      }
+      double2 p = make_double2(pr[0] + pr[1] + pr[2] + pr[3], pi[0] + pi[1] + pi[2] + pi[3]);
+      if (i >= 0)
+        hb_sub_cols2(p, sv, xr, cv, a.Y + r, a.ldy, a.iy);
+      else
+        hb_sub_cols(p, a.Y + r, a.ldy, sv, a.iy);
+      const double2 y = make_double2(2.0 * p.x, 2.0 * p.y);
+      a.Y[(size_t)a.iy * a.ldy + r] = y;
+      if (i >= 0) cfms(xr, y, cv[a.iy]);
     }
-    if (blockIdx.x == 0 && threadIdx.x < iy) {
-      double2 t = make_double2(0.0, 0.0);
-      for (int m = threadIdx.x; m < iy; ++m) cfma(t, T[(size_t)m * kHbB + threadIdx.x], sv[m]);
-      T[(size_t)iy * kHbB + threadIdx.x] = make_double2(-2.0 * t.x, -2.0 * t.y);
-    }
-    __syncthreads();
+    if (i >= 0) xs[r - r0] = xr;
   }
-  if (ix < 0) return;
-  const int c = k + ix;
-  double2 v = make_double2(0.0, 0.0);
-  if (r < N) {
-    v = A[(size_t)c * lda + r];
-    for (int j = 0; j < ix; ++j) {
-      const double2 vc = V[(size_t)(k + j) * ldv + c];
-      cfms(v, Y[(size_t)j * ldy + r], make_double2(vc.x, -vc.y));
-    }
-    x[r] = v;
-  }
-  if (ix == 0) return;
-  double2 pp[kHbB];
-#pragma unroll
-  for (int j = 0; j < kHbB; ++j) pp[j] = make_double2(0.0, 0.0);
-  if (r < N && r >= k + 1) {
-#pragma unroll
-    for (int j = 0; j < kHbB; ++j) {
-      if (j >= ix) break;
-      const double2 w = V[(size_t)(k + j) * ldv + r];
-      cfma(pp[j], make_double2(w.x, -w.y), v);
-    }
-  }
-  hb_multi_sum(pp, ix, red, sv);
-  if (threadIdx.x < ix) wpart[(size_t)blockIdx.x * kHbB + threadIdx.x] = sv[threadIdx.x];
-}
-
-// Column c = k + i, second part: w from wpart, z = T^H w, x[k+1..] -= V[k+1.., <i] z; this CTA's
-// part of ||x[c+1..]||^2 into sspart.
-__global__ void __launch_bounds__(kHbRowT) hb_z_kernel(int N, int k, int i, const double2* V, long ldv,
-                                                       const double2* T, double2* x, const double2* wpart,
-                                                       double* sspart) {
-  __shared__ double2 red[(kHbRowT / 32) * kHbB];
-  __shared__ double2 w[kHbB], z[kHbB];
-  __shared__ double rd[kHbRowT / 32];
-  const int G = gridDim.x, c = k + i;
-  const int r = blockIdx.x * kHbRowT + threadIdx.x;
+  if (i < 0) return;  // uniform: no CTA of the cluster reads another's shared memory
+  __syncthreads();
   if (i > 0) {
-    hb_sum_partials(wpart, G, i, red, w);
+    hb_cta_dots(a.V + (size_t)k * a.ldv, a.ldv, xs, max(r0, k + 1), r1, r0, i, mine);
+    cl.sync();
+    hb_cluster_sum(cl, G, mine, i, red, tot);
     // z_j = sum_{l <= j} conj(T[l, j]) w_l
-    if (threadIdx.x < i) {
+    if (tid < i) {
       double2 acc = make_double2(0.0, 0.0);
-      for (int l = 0; l <= (int)threadIdx.x; ++l) {
-        const double2 t = T[(size_t)threadIdx.x * kHbB + l];
-        cfma(acc, make_double2(t.x, -t.y), w[l]);
+      for (int l = 0; l <= tid; ++l) {
+        const double2 t = Ts[tid * kHbB + l];
+        cfma(acc, make_double2(t.x, -t.y), tot[l]);
       }
-      z[threadIdx.x] = acc;
+      zv[tid] = acc;
     }
     __syncthreads();
   }
   double ss = 0.0;
-  if (r < N) {
-    double2 v = x[r];
+  for (int r = r0 + tid; r < r1; r += kHbCT) {
+    double2 v = xs[r - r0];
     if (i > 0 && r >= k + 1) {
-      for (int j = 0; j < i; ++j) cfms(v, V[(size_t)(k + j) * ldv + r], z[j]);
-      x[r] = v;
+      hb_sub_cols(v, a.V + (size_t)k * a.ldv + r, a.ldv, zv, i);
+      xs[r - r0] = v;
     }
-    if (r > c) ss = v.x * v.x + v.y * v.y;
+    if (r > c) ss += v.x * v.x + v.y * v.y;
+    if (r == c + 1) mine_x0 = v;
   }
-  ss = hb_block_sum(ss, rd);
-  if (threadIdx.x == 0) sspart[blockIdx.x] = ss;
-}
-
-// Column c = k + i, third part: the reflector of x[c+1..] (||x[c+1..]||^2 from sspart): u into
-// V[:, c], the reduced column into A[:, c], this CTA's part of s = V[:, <i]^H u into spart; CTA 0
-// writes T[i.., i] (2, or 0 for an identity reflector, then zeros).
-__global__ void __launch_bounds__(kHbRowT) hb_u_kernel(double2* A, long lda, int N, int k, int i, double2* V,
-                                                       long ldv, double2* T, const double2* x, const double* sspart,
-                                                       double2* spart) {
-  __shared__ double2 red[(kHbRowT / 32) * kHbB];
-  __shared__ double2 sv[kHbB];
-  __shared__ double rd[kHbRowT / 32];
-  const int G = gridDim.x, c = k + i;
-  const int r = blockIdx.x * kHbRowT + threadIdx.x;
-  double t = 0.0;
-  for (int g = threadIdx.x; g < G; g += kHbRowT) t += sspart[g];
-  const double ss = hb_block_sum(t, rd);
-  const double2 x0 = x[c + 1];
+  for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+  if ((tid & 31) == 0) rd[tid >> 5] = ss;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kHbCT / 32; ++w) t += rd[w];
+    mine_ss = t;
+  }
+  cl.sync();  // also: every CTA has read the w partials
+  if (tid < 32) {
+    double v = tid < G ? *cl.map_shared_rank(&mine_ss, (unsigned)tid) : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (tid == 0) {
+      sst_s = v;
+      x0_s = *cl.map_shared_rank(&mine_x0, (unsigned)((c + 1) / a.rpc));
+    }
+  }
+  __syncthreads();
+  const double sst = sst_s;
+  const double2 x0 = x0_s;
   const double a0 = hypot(x0.x, x0.y);
   double2 gamma = x0;
   double winv = 0.0;
-  if (ss > 0.0) {
-    const double nrm = sqrt(ss);
+  if (sst > 0.0) {
+    const double nrm = sqrt(sst);
     const double2 ph = a0 > 0.0 ? make_double2(x0.x / a0, x0.y / a0) : make_double2(1.0, 0.0);
     gamma = make_double2(-ph.x * nrm, -ph.y * nrm);
-    winv = 1.0 / sqrt(2.0 * ss + 2.0 * nrm * a0);
+    winv = 1.0 / sqrt(2.0 * sst + 2.0 * nrm * a0);
   }
-  double2 u = make_double2(0.0, 0.0);
-  if (r < N) {
-    const double2 xr = x[r];
-    if (r > c && ss > 0.0) {
+  for (int r = r0 + tid; r < r1; r += kHbCT) {
+    const double2 xr = xs[r - r0];
+    double2 u = make_double2(0.0, 0.0);
+    if (r > c && sst > 0.0) {
       u = xr;
       if (r == c + 1) {
         u.x -= gamma.x;
@@ -449,25 +499,90 @@ __global__ void __launch_bounds__(kHbRowT) hb_u_kernel(double2* A, long lda, int
       u.x *= winv;
       u.y *= winv;
     }
-    V[(size_t)c * ldv + r] = u;
-    A[(size_t)c * lda + r] = r <= c ? xr : (r == c + 1 ? gamma : make_double2(0.0, 0.0));
+    a.V[(size_t)c * a.ldv + r] = u;
+    a.A[(size_t)c * a.lda + r] = r <= c ? xr : (r == c + 1 ? gamma : make_double2(0.0, 0.0));
+    xs[r - r0] = u;  // x is done with; u for the sums below
   }
-  if (blockIdx.x == 0 && threadIdx.x >= i && threadIdx.x < kHbB)
-    T[(size_t)i * kHbB + threadIdx.x] = make_double2(threadIdx.x == i && ss > 0.0 ? 2.0 : 0.0, 0.0);
-  if (i == 0) return;
-  double2 pp[kHbB];
-#pragma unroll
-  for (int j = 0; j < kHbB; ++j) pp[j] = make_double2(0.0, 0.0);
-  if (r < N && r > c) {
-#pragma unroll
-    for (int j = 0; j < kHbB; ++j) {
-      if (j >= i) break;
-      const double2 w = V[(size_t)(k + j) * ldv + r];
-      cfma(pp[j], make_double2(w.x, -w.y), u);
+  __syncthreads();
+  // the w partials in mine were read by every CTA before the barrier after the norm
+  if (i > 0) hb_cta_dots(a.V + (size_t)k * a.ldv, a.ldv, xs, max(r0, c + 1), r1, r0, i, mine);
+  cl.sync();
+  if (q == 0) {
+    hb_cluster_sum(cl, G, mine, i, red, tot);
+    if (tid < i) a.s[tid] = tot[tid];
+    // T[:, i]: rows < i from -2 T[<i, <i] s, row i = 2 (or 0 for an identity reflector), rest 0
+    if (tid < kHbB) {
+      double2 t = make_double2(0.0, 0.0);
+      if (tid < i) {
+        for (int m = tid; m < i; ++m) cfma(t, Ts[m * kHbB + tid], tot[m]);
+        t = make_double2(-2.0 * t.x, -2.0 * t.y);
+      } else if (tid == i) {
+        t = make_double2(sst > 0.0 ? 2.0 : 0.0, 0.0);
+      }
+      a.T[(size_t)i * kHbB + tid] = t;
     }
   }
-  hb_multi_sum(pp, i, red, sv);
-  if (threadIdx.x < i) spart[(size_t)blockIdx.x * kHbB + threadIdx.x] = sv[threadIdx.x];
+  cl.sync();  // no CTA leaves while rank 0 reads its partials
+}
+
+// The GEMV of column c: part[ch * N + r] = sum over the 256 columns j of chunk ch (from c + 1) of
+// A[r, j] u_j, u = V[:, c].  A CTA takes 32 rows and one chunk; warp w its 32 columns w * 32 ..,
+// 16 loads in flight per thread; the 8 warps' sums are added in shared memory.
+constexpr int kHbGemvCols = 256;
+__global__ void __launch_bounds__(256) hb_gemv_kernel(const double2* __restrict__ A, long lda, int N, int c,
+                                                      const double2* __restrict__ u, double2* part) {
+  __shared__ double2 us[kHbGemvCols];
+  __shared__ double2 red[8][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * 32 + lane;
+  const int j0 = c + 1 + blockIdx.y * kHbGemvCols;
+  const int j1 = min(j0 + kHbGemvCols, N);
+  us[threadIdx.x] = j0 + (int)threadIdx.x < j1 ? u[j0 + threadIdx.x] : make_double2(0.0, 0.0);
+  __syncthreads();
+  double pr[4] = {0.0, 0.0, 0.0, 0.0}, pi[4] = {0.0, 0.0, 0.0, 0.0};
+  const int jw = j0 + warp * 32;
+  if (row < N && jw + 32 <= j1) {
+    // all 32 columns in range: 16 unpredicated loads at a time
+    const double2* Ar = A + (size_t)jw * lda + row;
+#pragma unroll
+    for (int b = 0; b < 32; b += 16) {
+      double2 av[16];
+#pragma unroll
+      for (int e = 0; e < 16; ++e) av[e] = __ldg(Ar + (size_t)(b + e) * lda);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const double2 uu = us[warp * 32 + b + e];
+        pr[e & 3] += av[e].x * uu.x - av[e].y * uu.y;
+        pi[e & 3] += av[e].x * uu.y + av[e].y * uu.x;
+      }
+    }
+  } else if (row < N && jw < j1) {
+#pragma unroll
+    for (int b = 0; b < 32; b += 16) {
+      double2 av[16];
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const int j = jw + b + e;
+        av[e] = j < j1 ? A[(size_t)j * lda + row] : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const double2 uu = us[warp * 32 + b + e];
+        pr[e & 3] += av[e].x * uu.x - av[e].y * uu.y;
+        pi[e & 3] += av[e].x * uu.y + av[e].y * uu.x;
+      }
+    }
+  }
+  red[warp][lane] = make_double2(pr[0] + pr[1] + pr[2] + pr[3], pi[0] + pi[1] + pi[2] + pi[3]);
+  __syncthreads();
+  if (warp == 0 && row < N) {
+    double2 t = red[0][lane];
+    for (int w = 1; w < 8; ++w) {
+      t.x += red[w][lane].x;
+      t.y += red[w][lane].y;
+    }
+    part[(size_t)blockIdx.y * N + row] = t;
+  }
 }
 
 // C (column-major, ldc, M x Nc) += sum of the split-K slices tmp[z] (same layout, slice stride

@@ -199,7 +199,8 @@ struct hprmat_b200_ctx {
   int hess_fallback_last = 0;    // energies the last shifted scan sent to the LU path
   double hess_ms[6] = {};        // with profiling: reduce, solve, products, refine, U, fallback (ms)
   bool hess_blocked = true;      // blocked (panel + GEMM) Hessenberg reduction
-  DevBuf hbY, hbT, hbX, hbPart, hbVH, hbVT, hbW, hbTmp, hUmat;
+  DevBuf hbY, hbT, hbS, hbVH, hbVT, hbW, hbTmp, hUmat;
+  int hb_cluster = 0;  // CTAs of the Hessenberg column step's cluster (0: not chosen yet)
   // batched energy scans: worker contexts (own stream and buffers) and the blocks' potentials
   std::vector<hprmat_b200_ctx*> scan_workers;
   std::vector<std::unique_ptr<DevBuf>> scan_cpot;
@@ -2553,8 +2554,7 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* c, int nblocks, const hprmat_b200_
 // A = P H P^H, with P (ld) accumulated from the reflectors (kept in hU, column k: rows k+1 ..).
 static int hess_reduce_blocked(hprmat_b200_ctx* c, double2* A, long ld, int N, double2* P);
 
-static int hess_reduce(hprmat_b200_ctx* c, double2* A, long ld, int N, double2* P) {
-  if (c->hess_blocked && N > kHbB + 2) return hess_reduce_blocked(c, A, ld, N, P);
+static int hess_reduce_unblocked(hprmat_b200_ctx* c, double2* A, long ld, int N, double2* P) {
   NvtxRange nv("hprmat.hess.reduce");
   TRY(c->hU.ensure((size_t)ld * N * sizeof(double2)));
   const int nchunk_max = (N + kHessChunk - 1) / kHessChunk;
@@ -2586,10 +2586,15 @@ static int hess_reduce(hprmat_b200_ctx* c, double2* A, long ld, int N, double2* 
 }
 
 
+static int hess_reduce(hprmat_b200_ctx* c, double2* A, long ld, int N, double2* P) {
+  if (c->hess_blocked && N > kHbB + 2) return hess_reduce_blocked(c, A, ld, N, P);
+  return hess_reduce_unblocked(c, A, ld, N, P);
+}
+
 // The same reduction in panels of kHbB columns (hessenberg.cuh, "blocked reduction"): per column
-// one CTA brings the column up to date and forms its reflector, a GEMV of the trailing matrix
-// gives the column of Y; per panel three DMMA GEMMs update the trailing columns.  P is
-// accumulated backwards from the identity, panel by panel, by two GEMMs each.
+// one thread-block cluster brings the column up to date and forms its reflector, and a GEMV of
+// the trailing matrix gives the column of Y; per panel three DMMA GEMMs update the trailing
+// columns.  P is accumulated backwards from the identity, panel by panel, by two GEMMs each.
 static int hess_reduce_blocked(hprmat_b200_ctx* c, double2* A, long ld, int N, double2* P) {
   NvtxRange nv("hprmat.hess.reduce_blocked");
   const int ncols = N - 2;  // columns 0 .. N-3 get a reflector
@@ -2607,14 +2612,70 @@ static int hess_reduce_blocked(hprmat_b200_ctx* c, double2* A, long ld, int N, d
   double2* VH = c->hbVH.as<double2>();
   double2* VT = c->hbVT.as<double2>();
   double2* W = c->hbW.as<double2>();
-  const int G = cdiv_u(N, kHbRowT);
-  TRY(c->hbX.ensure((size_t)N * sizeof(double2)));
-  TRY(c->hbPart.ensure((size_t)G * (2 * kHbB * sizeof(double2) + sizeof(double))));
-  double2* xv = c->hbX.as<double2>();
-  double2* wpart = c->hbPart.as<double2>();
-  double2* spart = wpart + (size_t)G * kHbB;
-  double* sspart = reinterpret_cast<double*>(spart + (size_t)G * kHbB);
+  TRY(c->hbS.ensure((size_t)kHbB * sizeof(double2)));
   double2* part = c->hPart.as<double2>();
+  // the column step's cluster: 16 CTAs where the GPU holds such a cluster, else 8 (portable)
+  if (c->hb_cluster == 0) {
+    c->hb_cluster = 8;
+    if (cudaFuncSetAttribute((const void*)hb_col_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+            cudaSuccess &&
+        set_smem(hb_col_cluster_kernel, (size_t)cdiv_u(N, 16) * sizeof(double2)) == HPRMAT_B200_OK) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(16);
+      cfg.blockDim = dim3(kHbCT);
+      cfg.dynamicSmemBytes = (size_t)cdiv_u(N, 16) * sizeof(double2);
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = 16;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int n = 0;
+      if (cudaOccupancyMaxActiveClusters(&n, (const void*)hb_col_cluster_kernel, &cfg) == cudaSuccess && n >= 1)
+        c->hb_cluster = 16;
+    }
+    cudaGetLastError();
+  }
+  const int Gc = c->hb_cluster;
+  if (Gc > 8)
+    HPR_CUDA_TRY(cudaFuncSetAttribute((const void*)hb_col_cluster_kernel,
+                                      cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  const int rpc = cdiv_u(N, Gc);
+  const size_t xsm = (size_t)rpc * sizeof(double2);
+  if (xsm + 16384 > (size_t)c->smem_optin) return hess_reduce_unblocked(c, A, ld, N, P);
+  TRY(set_smem(hb_col_cluster_kernel, xsm));
+  HbColArgs ca{};
+  ca.A = A;
+  ca.lda = ld;
+  ca.N = N;
+  ca.rpc = rpc;
+  ca.part = part;
+  ca.Y = Y;
+  ca.ldy = N;
+  ca.V = V;
+  ca.ldv = ld;
+  ca.s = c->hbS.as<double2>();
+  auto column_step = [&]() -> int {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(Gc);
+    cfg.blockDim = dim3(kHbCT);
+    cfg.dynamicSmemBytes = xsm;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = Gc;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, hb_col_cluster_kernel, ca);
+    if (e != cudaSuccess)
+      return fail(HPRMAT_B200_ERR_CUDA, "Hessenberg column step (%d CTAs of %d rows): %s", Gc, rpc,
+                  cudaGetErrorString(e));
+    ++c->launches;
+    return HPRMAT_B200_OK;
+  };
   auto gemm = [&](int M, int Nc, int K, const double2* Aop, long lda, const double2* Bop, long ldb, double2* Cop,
                   long ldc) -> int {
     if (zgemm_f64_update(M, Nc, K, Aop, lda, Bop, ldb, Cop, ldc, c->stream))
@@ -2645,22 +2706,22 @@ static int hess_reduce_blocked(hprmat_b200_ctx* c, double2* A, long ld, int N, d
   for (int p = 0; p < np; ++p) {
     const int k = p * kHbB, b = std::min(kHbB, ncols - k);
     double2* Tp = c->hbT.as<double2>() + (size_t)p * kHbB * kHbB;
-    // column i: x (with y of column i - 1), z and the norm, the reflector, the GEMV
-    hb_yx_kernel<<<G, kHbRowT, 0, c->stream>>>(A, ld, N, k, -1, 0, part, 0, spart, Y, N, V, ld, Tp, xv, wpart);
-    LAUNCH_CHECK();
+    // per column: the column step (with y of the column before) on the cluster, then the GEMV
+    ca.k = k;
+    ca.T = Tp;
+    ca.iy = -1;
+    ca.ix = 0;
+    ca.nchunk = 0;
+    TRY(column_step());
     for (int i = 0; i < b; ++i) {
       const int col = k + i;
-      hb_z_kernel<<<G, kHbRowT, 0, c->stream>>>(N, k, i, V, ld, Tp, xv, wpart, sspart);
+      const int nchunk = cdiv_u(N - col - 1, kHbGemvCols);
+      hb_gemv_kernel<<<dim3(cdiv_u(N, 32), nchunk), 256, 0, c->stream>>>(A, ld, N, col, V + (size_t)col * ld, part);
       LAUNCH_CHECK();
-      hb_u_kernel<<<G, kHbRowT, 0, c->stream>>>(A, ld, N, k, i, V, ld, Tp, xv, sspart, spart);
-      LAUNCH_CHECK();
-      const int nchunk = (N - col - 1 + kHessChunk - 1) / kHessChunk;
-      hess_right_partial_kernel<<<dim3(cdiv_u(N, kHessThreads), nchunk), kHessThreads, 0, c->stream>>>(
-          A, ld, N, col, V, ld, part);
-      LAUNCH_CHECK();
-      hb_yx_kernel<<<G, kHbRowT, 0, c->stream>>>(A, ld, N, k, i, i + 1 < b ? i + 1 : -1, part, nchunk, spart, Y, N, V,
-                                                 ld, Tp, xv, wpart);
-      LAUNCH_CHECK();
+      ca.iy = i;
+      ca.ix = i + 1 < b ? i + 1 : -1;
+      ca.nchunk = nchunk;
+      TRY(column_step());
     }
     if (k + b < N) {
       const int nt = N - k - b;
@@ -3772,6 +3833,11 @@ int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* c, const char* key, int value) {
   }
   if (strcmp(key, "hess_blocked") == 0) {
     c->hess_blocked = value != 0;
+    return HPRMAT_B200_OK;
+  }
+  if (strcmp(key, "hess_cluster") == 0) {  // CTAs of the column step's cluster: 8 or 16 (0: choose)
+    if (value != 0 && value != 8 && value != 16) return fail(HPRMAT_B200_ERR_ARG, "hess_cluster must be 0, 8 or 16");
+    c->hb_cluster = value;
     return HPRMAT_B200_OK;
   }
   if (strcmp(key, "panel_rpc_min") == 0) {

@@ -125,6 +125,20 @@ __global__ void __launch_bounds__(kThreads, 2)
     // refill the slot consumed in the previous iteration (every warp has passed the barrier)
     if (g + kStages - 1 < nstream) load_chunk(g + kStages - 1);
     cp_async_commit();
+    if (g % nchunks == 0) {
+      // a new tile: its C lines (64 columns of 64 x 16 bytes) go to L2 now, so that the
+      // epilogue's loads of C meet them there
+      const long t = blockIdx.x + (g / nchunks) * (long)gridDim.x;
+      const int z = (int)(t / ((long)mt * nt));
+      const int r = (int)(t % ((long)mt * nt));
+      const int m0 = (r % mt) * kBM, n0 = (r / mt) * kBN;
+      const double2* Cz = C + (size_t)z * sC;
+#pragma unroll
+      for (int L = tid; L < kBN * 8; L += kThreads) {
+        const int col = n0 + (L >> 3), row = m0 + (L & 7) * 8;
+        if (row < M && col < N) asm volatile("prefetch.global.L2 [%0];" ::"l"(Cz + row + (size_t)col * ldc));
+      }
+    }
     const int stage = (int)(g % kStages);
     const double2* as = As + stage * kAStage;
     const double2* bs = Bs + stage * kBStage;
@@ -214,6 +228,12 @@ int zgemm_f64_update_batched(int M, int N, int K, const double2* A, long lda, lo
       sB < 0 || sC < 0) {
     set_last_error_msg("zgemm_f64_update: misaligned operand or leading dimension too small");
     return -1;
+  }
+  // a shared A with the problems' B and C blocks back to back (column-major) is one GEMM with
+  // batch x N columns: whole 64-wide tiles instead of one partial tile column per problem
+  if (batch > 1 && sA == 0 && sB == ldb * (long)N && sC == ldc * (long)N && (long)N * batch <= 0x7fffffffL) {
+    N *= batch;
+    batch = 1;
   }
   // per device and cheap next to a launch: set on every call (any thread, any device)
   HPR_CUDA_TRY(cudaFuncSetAttribute(zgemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes));

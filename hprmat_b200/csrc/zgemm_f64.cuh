@@ -14,7 +14,8 @@ int zgemm_f64_update(int M, int N, int K, const double2* A, long lda, const doub
                      long ldc, cudaStream_t s);
 
 // The same for `batch` independent problems in one launch: problem z uses A + z sA, B + z sB,
-// C + z sC (strides in complex elements; a stride 0 shares that operand).
+// C + z sC (strides in complex elements; a stride 0 shares that operand).  A shared A (sA = 0)
+// with sB = ldb N and sC = ldc N is computed as one problem of batch N columns.
 int zgemm_f64_update_batched(int M, int N, int K, const double2* A, long lda, long sA, const double2* B, long ldb,
                              long sB, double2* C, long ldc, long sC, int batch, cudaStream_t s);
 
