@@ -556,6 +556,7 @@ struct TrsmArgs {
   float* lup;        // optional LU planes: U12 rows k0.. (row-major, see PanelArgs)
   long lup_ld;
   long lup_plane;
+  int mode;          // 0: interchanges and solve; 1: interchanges only; 2: solve only (rows k0..)
 };
 
 template <typename T, int NB, int CW, int NT>
@@ -570,10 +571,11 @@ __global__ void __launch_bounds__(NT) trsm_lower_kernel(TrsmArgs<T> a) {
   const int ncw = min(CW, a.c_end - cb);
   if (ncw <= 0) return;
   const int ncols = a.ncols;
-  const int ne = *a.n_extra;
+  const bool swap = a.mode != 2, solve = a.mode != 1;
+  const int ne = swap ? *a.n_extra : 0;
   for (int idx = tid; idx < ncw * ncols; idx += NT) {
     int j = idx % ncols, cc = idx / ncols;
-    A[cc * NBP + j] = a.X[(size_t)a.top_src[j] + (size_t)(cb + cc) * a.ldx];
+    A[cc * NBP + j] = a.X[(size_t)(swap ? a.top_src[j] : a.k0 + j) + (size_t)(cb + cc) * a.ldx];
   }
   for (int idx = tid; idx < ncw * ne; idx += NT) {
     int e = idx % ne, cc = idx / ne;
@@ -584,7 +586,7 @@ __global__ void __launch_bounds__(NT) trsm_lower_kernel(TrsmArgs<T> a) {
     int e = idx % ne, cc = idx / ne;
     a.X[(size_t)a.extra_dst[e] + (size_t)(cb + cc) * a.ldx] = E[cc * NB + e];
   }
-  for (int j = 0; j < ncols - 1; ++j) {
+  for (int j = 0; j < (solve ? ncols - 1 : 0); ++j) {
     __syncthreads();
     const int nr = ncols - j - 1;
     const T* Lcol = a.W + (size_t)(a.k0 + j) * a.ld + a.k0;
@@ -604,7 +606,7 @@ __global__ void __launch_bounds__(NT) trsm_lower_kernel(TrsmArgs<T> a) {
     a.X[(size_t)(a.k0 + j) + (size_t)(cb + cc) * a.ldx] = v;
     gmax = fmax(gmax, cabs1(v));
   }
-  if (a.growth_bits) {
+  if (a.growth_bits && solve) {
     for (int o = 16; o > 0; o >>= 1) gmax = fmax(gmax, __shfl_down_sync(0xffffffffu, gmax, o));
     if ((tid & 31) == 0) atomicMax(a.growth_bits, mag_hi((double)gmax));
   }
@@ -637,6 +639,30 @@ __global__ void __launch_bounds__(NT) trsm_lower_kernel(TrsmArgs<T> a) {
       a.bop[2 * a.bop_plane + off] = hi_;
       a.bop[3 * a.bop_plane + off] = li;
     }
+  }
+}
+
+// dst[i + j ldd] = W[src(i) + (col0 + j) ld], i < nr, j < ncol, src(i) = rows[i] (or row0 + i
+// without a row list): a block of W, optionally with its rows gathered.
+template <typename T>
+__global__ void gather_block_kernel(const T* __restrict__ W, long ld, const int* __restrict__ rows, int row0, int nr,
+                                    int col0, int ncol, T* __restrict__ dst, long ldd) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nr) return;
+  const int src = rows ? rows[i] : row0 + i;
+  for (int j = blockIdx.y; j < ncol; j += gridDim.y) dst[(size_t)i + (size_t)j * ldd] = W[(size_t)src + (size_t)(col0 + j) * ld];
+}
+
+// The rows of a step's interchange list that move below the panel: dst[(extra_dst[e] - row0) +
+// j ldd] = W[extra_src[e] + (col0 + j) ld], e < *n_extra, j < ncol.
+template <typename T>
+__global__ void patch_rows_kernel(const T* __restrict__ W, long ld, const int* __restrict__ extra_dst,
+                                  const int* __restrict__ extra_src, const int* __restrict__ n_extra, int row0,
+                                  int col0, int ncol, T* __restrict__ dst, long ldd) {
+  const int ne = *n_extra;
+  for (int idx = threadIdx.x; idx < ne * ncol; idx += blockDim.x) {
+    const int e = idx % ne, j = idx / ne;
+    dst[(size_t)(extra_dst[e] - row0) + (size_t)j * ldd] = W[(size_t)extra_src[e] + (size_t)(col0 + j) * ld];
   }
 }
 

@@ -200,6 +200,8 @@ struct hprmat_b200_ctx {
   double hess_ms[6] = {};        // with profiling: reduce, solve, products, refine, U, fallback (ms)
   bool hess_blocked = true;      // blocked (panel + GEMM) Hessenberg reduction
   DevBuf hbY, hbT, hbS, hbVH, hbVT, hbW, hbTmp, hUmat;
+  bool f64_pair = true;  // plain FP64 LU: two block steps share one K = 128 trailing update
+  DevBuf f64_pair_buf;
   int hb_cluster = 0;  // CTAs of the Hessenberg column step's cluster (0: not chosen yet)
   // batched energy scans: worker contexts (own stream and buffers) and the blocks' potentials
   std::vector<hprmat_b200_ctx*> scan_workers;
@@ -698,6 +700,85 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
     }
     return HPRMAT_B200_OK;
   };
+
+  // Plain FP64 path, NB = 64: block steps s (even) and s + 1 share one K = 128 trailing update,
+  // so that the trailing matrix streams through memory once per two panels.  After panel s only
+  // the next panel's columns are brought up to date (interchanges, U12, a 64-column update);
+  // after panel s + 1, for the columns right of both panels: step s's interchanges and U12,
+  // step s + 1's interchanges, rows k1 .. k2 minus step s's product (its L21 rows in step s + 1's
+  // order), step s + 1's U12, and A22 -= [P L21(s) | L21(s+1)] [U12(s); U12(s+1)], the first
+  // half of the A operand gathered in step s + 1's row order.  The factors are stored as the
+  // single-step path stores them (L21 of a step in its own row order).
+  constexpr bool kPairable = std::is_same<T, double2>::value && NB == 64;
+  const bool pair = kPairable && !mixed && c->f64_pair && nsteps >= 3;
+  auto step_swaps = [&](int s) {
+    int* swb = c->swaps.as<int>() + (size_t)s * kSwapStride;
+    return StepSwaps{swb, swb + kMaxNB, swb + 2 * kMaxNB, swb + 3 * kMaxNB};
+  };
+  auto trsm = [&](int k0, int ncols, const StepSwaps& sw, int c_begin, int c_end, int mode) -> int {
+    if (c_end <= c_begin) return HPRMAT_B200_OK;
+    constexpr int CW = 32;
+    auto tk = trsm_lower_kernel<T, NB, CW, NT>;
+    const size_t tsm = (size_t)CW * (NB + 1) * sizeof(T) + (size_t)CW * NB * sizeof(T);
+    TRY(set_smem(tk, tsm));
+    TrsmArgs<T> ta{};
+    ta.W = W;
+    ta.ld = ld;
+    ta.k0 = k0;
+    ta.ncols = ncols;
+    ta.top_src = sw.top_src;
+    ta.extra_dst = sw.extra_dst;
+    ta.extra_src = sw.extra_src;
+    ta.n_extra = sw.n_extra;
+    ta.X = W;
+    ta.ldx = ld;
+    ta.c_begin = c_begin;
+    ta.c_end = c_end;
+    ta.growth_bits = growth;
+    ta.mode = mode;
+    tk<<<cdiv_u(c_end - c_begin, CW), NT, tsm, c->stream>>>(ta);
+    LAUNCH_CHECK();
+    return HPRMAT_B200_OK;
+  };
+  auto pair_first = [&](int s, int k0) -> int {  // after panel s: the next panel's columns
+    const int k1 = k0 + NB;
+    TRY(trsm(k0, NB, step_swaps(s), k1, k1 + NB, 0));
+    if constexpr (kPairable)
+      TRY(zgemm_update(c, N - k1, NB, NB, W + k1 + (size_t)k0 * ld, ld, W + k0 + (size_t)k1 * ld, ld,
+                       W + k1 + (size_t)k1 * ld, ld));
+    return HPRMAT_B200_OK;
+  };
+  auto pair_second = [&](int s, int k0) -> int {  // after panel s + 1: everything right of both
+    if constexpr (kPairable) {
+      const int k1 = k0 + NB, k2 = k1 + NB;
+      const int m2 = N - k2;
+      const StepSwaps s0 = step_swaps(s), s1 = step_swaps(s + 1);
+      TRY(trsm(k0, NB, s0, k2, N, 0));
+      TRY(trsm(k1, NB, s1, k2, N, 1));
+      // rows k1 .. k2 minus L21(s) (rows in step s + 1's order) U12(s)
+      TRY(c->f64_pair_buf.ensure(((size_t)NB * NB + (size_t)m2 * 2 * NB) * sizeof(T)));
+      T* F = c->f64_pair_buf.as<T>();
+      T* LL = F + (size_t)NB * NB;
+      gather_block_kernel<T><<<dim3(1, 16), NB, 0, c->stream>>>(W, ld, s1.top_src, 0, NB, k0, NB, F, NB);
+      LAUNCH_CHECK();
+      TRY(zgemm_update(c, NB, m2, NB, F, NB, W + k0 + (size_t)k2 * ld, ld, W + k1 + (size_t)k2 * ld, ld));
+      TRY(trsm(k1, NB, s1, k2, N, 2));
+      // A operand [P L21(s) | L21(s+1)], rows k2 .., and the K = 128 update
+      gather_block_kernel<T><<<dim3(cdiv_u(m2, 256), 32), 256, 0, c->stream>>>(W, ld, nullptr, k2, m2, k0, 2 * NB, LL,
+                                                                              m2);
+      LAUNCH_CHECK();
+      patch_rows_kernel<T><<<1, 256, 0, c->stream>>>(W, ld, s1.extra_dst, s1.extra_src, s1.n_extra, k2, k0, NB, LL, m2);
+      LAUNCH_CHECK();
+      TRY(zgemm_update(c, m2, m2, 2 * NB, LL, m2, W + k0 + (size_t)k2 * ld, ld, W + k2 + (size_t)k2 * ld, ld));
+    }
+    return HPRMAT_B200_OK;
+  };
+  // what follows the panel of step s
+  auto after_step = [&](int s, int k0, int ncols, const StepSwaps& sw) -> int {
+    if (pair && s + 2 < nsteps && (s & 1) == 0) return pair_first(s, k0);
+    if (pair && (s & 1) == 1 && s + 1 < nsteps) return pair_second(s - 1, k0 - NB);
+    return after_panel(s, k0, ncols, sw);
+  };
   auto pk = panel_kernel<T, NB, NT>;
   auto pkc = panel_cluster_kernel<T, NB, NT>;
   // the largest rows per CTA of a cluster panel (shared memory of the opt-in limit, less the
@@ -780,7 +861,7 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
                       Gc, rpcc, smc, cudaGetErrorString(e));
         ++c->launches;
         if (k0 + ncols >= N) break;
-        TRY(after_panel(s, k0, ncols, pa.sw));
+        TRY(after_step(s, k0, ncols, pa.sw));
         continue;
       }
     }
@@ -835,7 +916,7 @@ static int factor_impl(hprmat_b200_ctx* c, T* W, long ld, int N, bool mixed, LUS
     }
     ++c->launches;
     if (k0 + ncols >= N) break;
-    TRY(after_panel(s, k0, ncols, pa.sw));
+    TRY(after_step(s, k0, ncols, pa.sw));
   }
   // explicit inverses of the diagonal blocks for the solves
   {
@@ -3833,6 +3914,10 @@ int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* c, const char* key, int value) {
   }
   if (strcmp(key, "hess_blocked") == 0) {
     c->hess_blocked = value != 0;
+    return HPRMAT_B200_OK;
+  }
+  if (strcmp(key, "f64_pair") == 0) {
+    c->f64_pair = value != 0;
     return HPRMAT_B200_OK;
   }
   if (strcmp(key, "hess_cluster") == 0) {  // CTAs of the column step's cluster: 8 or 16 (0: choose)

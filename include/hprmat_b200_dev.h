@@ -67,7 +67,13 @@ int hprmat_b200_dev_counters(hprmat_b200_ctx* ctx, unsigned long long* launches,
      "inner_tol0_exp" first cycle runs until the residual fell 10^-value (7);
      "zero_start"     refinement from X = 0 instead of the FP32 solution (0);
      "reuse_max_inner" with opts.reuse_factors, factorise again once a solve on the held
-                      factors needed more FGMRES iterations than this (24). */
+                      factors needed more FGMRES iterations than this (24);
+     "f64_pair"       plain FP64 LU: two 64-column block steps share one K = 128 trailing
+                      update (1) or each step updates on its own (0);
+     "hess_blocked"   shifted scan: blocked Hessenberg reduction (1) or one reflector at a
+                      time (0);
+     "hess_cluster"   CTAs of the blocked reduction's column-step cluster: 8, 16, or 0 to
+                      take 16 where the GPU holds such a cluster. */
 int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* ctx, const char* key, int value);
 
 /* Failure-path check: one CTA waits, with a limit of `spins` polls (4096 .. 2^24), on a device
