@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--solves-only", action="store_true",
                     help="only the device-resident timed solves (for profiler launch lists)")
     ap.add_argument("--nch", type=int, default=128, help="channels of the production generator (N = 200 nch)")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed",
+                    help="production with --solves-only: the path of the timed solves (fp64: this library's plain "
+                         "FP64 LU with the DMMA GEMM, for profiler launch lists of its kernels)")
     ap.add_argument("--workload", choices=["production", "scan", "adjoint", "sweep"], default="production",
                     help="production: one N = 25600 solve per step (the headline); scan: the batched energy "
                          "scan, 12 J-pi blocks x 256 energies (3072 solves) per step; adjoint: loss and gradients "
@@ -525,7 +528,10 @@ def main():
 
     w = workloads.production(nch=args.nch)
     n_full = w.n
-    ctx = api.Context(device=local, precision="mixed", max_refine=3, tol=1e-12)
+    if args.precision != "mixed" and not args.solves_only:
+        print("bench: --precision fp64 is for --solves-only runs (the headline is the mixed path)", file=sys.stderr)
+        return 2
+    ctx = api.Context(device=local, precision=args.precision, max_refine=3, tol=1e-12)
     stream = torch.cuda.Stream(device=dev)
     ctx.set_stream(stream.cuda_stream)
     ctx.rmat_ini(w.nr, 1, w.rmax)
@@ -586,6 +592,7 @@ def main():
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                               "warmup": args.warmup, "ms_per_step": ms_per_step, "N": n_full, "u_rel_err": u_err,
+                              "precision": args.precision,
                               "gpu_launches": int(launches.value), "clocks": clk}))
         ctx.close()
         if world > 1:
