@@ -69,6 +69,9 @@ def parse():
                     help="scan: lu (every energy by its own mixed LU on concurrent worker streams) or shifted (one "
                          "Hessenberg reduction per J-pi block, O(N^2 nch) FP64 work per energy, "
                          "hprmat_b200_rmatrix_scan_shifted)")
+    ap.add_argument("--scan-blocks", type=int, default=0,
+                    help="scan: only the first K J-pi blocks (0: all 12; the first is the largest, N = 3180), for "
+                         "profiler runs of one block")
     ap.add_argument("--autotune", type=int, default=0,
                     help="scan: run the scan autotuner (hprmat_b200_scan_autotune) on the scan's blocks before "
                          "the warm-up, outside the timed region")
@@ -216,6 +219,8 @@ def run_scan(args):
     from oracle import rmatrix_oracle as orc
     from hprmat_b200.scan_shard import shard_units
     blocks = workloads.scan_blocks()
+    if args.scan_blocks > 0:
+        blocks = blocks[:args.scan_blocks]
     all_inputs = []
     for w, energies in blocks:
         ks = [workloads.channel_kinematics(e, w.thresholds, w.hm, w.params.z1z2) for e in energies]
@@ -310,7 +315,7 @@ def run_scan(args):
             "data": "synthetic (seeded scan generator, hprmat_b200/workloads.py)",
             "config": {"workload": "batched energy scan: 12 J-pi blocks, nch ~ U{4..64} x 60 points "
                                    "(N = 240..3840), 256 energies each, 3072 solves",
-                       "method": args.scan_method,
+                       "method": args.scan_method, "blocks": len(blocks),
                        "workers": args.workers, "reuse_factors": bool(args.reuse),
                        "autotune": bool(args.autotune)},
             "autotune": tune,
