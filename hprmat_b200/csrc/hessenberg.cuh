@@ -681,7 +681,10 @@ __device__ void hess_back_substitute(const double2* Ue, long ldh, int N, int nch
                                      double2* smem) {
   double2* us = smem;                       // [2][32][kHsUs]
   double2* ys = us + 2 * kHsUsTile;         // [2][32][kHsYs]
-  double2* acc_s = ys + 2 * kHsYsTile;      // [32][kHsMaxRhs]
+  // [32][kHsMaxRhs], used only after a block's chunk loop: over the Y chunk buffers, so that the
+  // kernel fits two CTAs per SM
+  double2* acc_s = ys;
+  static_assert(kHsRows * kHsMaxRhs <= 2 * kHsYsTile, "the block's right-hand sides fit the chunk buffers");
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wr = warp & 3, wc = warp >> 2;
   const int fr = lane >> 2, fk = lane & 3;
@@ -772,11 +775,15 @@ __device__ void hess_back_substitute(const double2* Ue, long ldh, int N, int nch
   }
 }
 
-constexpr size_t kHessSolveSmem =
-    (2 * (size_t)kHsUsTile + 2 * (size_t)kHsYsTile + (size_t)kHsRows * kHsMaxRhs) * sizeof(double2);
+constexpr size_t kHessSolveSmem = (2 * (size_t)kHsUsTile + 2 * (size_t)kHsYsTile) * sizeof(double2);
 
 // Factor and solve (W given) or re-solve with the stored factors (W == nullptr: the unit's Y
-// holds the right-hand sides).  Dynamic shared memory: max(kHessSolveSmem, N complex) bytes.
+// holds the right-hand sides).  PHASE 1: the elimination (factor, or the forward pass of a
+// re-solve) into Ue, lm, sw and Y; dynamic shared memory N complex with W, none without.
+// PHASE 2: the back substitution on Y; dynamic shared memory kHessSolveSmem.  The two run as
+// separate launches: the latency-bound eliminations of all units then share the SMs (several
+// CTAs each), and the DMMA-bound back substitutions follow.
+template <int PHASE>
 __global__ void __launch_bounds__(kHessThreads) hess_solve_kernel(HessSolveArgs a) {
   extern __shared__ __align__(16) double2 hsm[];
   const int unit = blockIdx.x;
@@ -785,6 +792,10 @@ __global__ void __launch_bounds__(kHessThreads) hess_solve_kernel(HessSolveArgs 
   double2* lm = a.lm + (size_t)unit * N;
   int* sw = a.sw + (size_t)unit * N;
   double2* Y = a.Y + (size_t)unit * a.sY;
+  if (PHASE == 2) {
+    hess_back_substitute(Ue, a.ldh, N, nch, Y, a.ldy, hsm);
+    return;
+  }
   if (a.W != nullptr) {
     // LU of Hs with the working row in shared memory; the right-hand sides follow row by row
     const double dl = a.delta[unit];
@@ -845,9 +856,29 @@ __global__ void __launch_bounds__(kHessThreads) hess_solve_kernel(HessSolveArgs 
   } else {
     // forward elimination of the unit's right-hand sides with the stored steps
     if (tid < nch) {
+      // step k reads y[k + 1] before step k + 1 writes it: the loads of 8 steps go out together
       double2* y = Y + (size_t)tid * a.ldy;
       double2 zc = y[0];
-      for (int k = 0; k < N - 1; ++k) {
+      int k = 0;
+      for (; k + 8 <= N - 1; k += 8) {
+        double2 zb[8], l[8];
+        int s[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          zb[e] = y[k + 1 + e];
+          l[e] = lm[k + e];
+          s[e] = sw[k + e];
+        }
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const double2 zp = s[e] ? zb[e] : zc, zo = s[e] ? zc : zb[e];
+          y[k + e] = zp;
+          double2 nz = zo;
+          cfms(nz, l[e], zp);
+          zc = nz;
+        }
+      }
+      for (; k < N - 1; ++k) {
         const double2 zb = y[k + 1];
         const bool swap = sw[k] != 0;
         const double2 zp = swap ? zb : zc, zo = swap ? zc : zb;
@@ -858,9 +889,7 @@ __global__ void __launch_bounds__(kHessThreads) hess_solve_kernel(HessSolveArgs 
       }
       y[N - 1] = zc;
     }
-    __syncthreads();
   }
-  hess_back_substitute(Ue, a.ldh, N, nch, Y, a.ldy, hsm);
 }
 
 // ---------------------------------------------------------------- per-unit Woodbury terms

@@ -2961,8 +2961,17 @@ static int hess_scan_block(hprmat_b200_ctx* c, int bi, const hprmat_b200_scan_bl
                                            (reinterpret_cast<uintptr_t>(d_uinfo + nb) & 7));
   std::vector<double> d_delta_host(nb);
   TRY(c->hChan.ensure((size_t)nb * sizeof(double) + 64));
-  const size_t smem_solve = std::max(kHessSolveSmem, (size_t)N * sizeof(double2));
-  TRY(set_smem(hess_solve_kernel, smem_solve));
+  const size_t smem_elim = (size_t)N * sizeof(double2);
+  TRY(set_smem(hess_solve_kernel<1>, smem_elim));
+  TRY(set_smem(hess_solve_kernel<2>, kHessSolveSmem));
+  // a solve: the eliminations of all units (several CTAs per SM), then the back substitutions
+  auto hess_solve = [&](const HessSolveArgs& args, int units) -> int {
+    hess_solve_kernel<1><<<units, kHessThreads, args.W ? smem_elim : 0, c->stream>>>(args);
+    LAUNCH_CHECK();
+    hess_solve_kernel<2><<<units, kHessThreads, kHessSolveSmem, c->stream>>>(args);
+    LAUNCH_CHECK();
+    return HPRMAT_B200_OK;
+  };
   TRY(set_smem(hess_woodbury_kernel, hess_woodbury_smem(nch)));
   std::vector<unsigned char> hu((size_t)nb * ubp);
   std::vector<int> hinfo(3 * (size_t)nb);
@@ -3020,8 +3029,7 @@ static int hess_scan_block(hprmat_b200_ctx* c, int bi, const hprmat_b200_scan_bl
     ha.info = d_info;
     {
       NvtxRange nv("hprmat.hess.solve");
-      hess_solve_kernel<<<m, kHessThreads, smem_solve, c->stream>>>(ha);
-      LAUNCH_CHECK();
+      TRY(hess_solve(ha, m));
     }
     TRY(phase(1));
     const long sN = ld * nch;
@@ -3072,8 +3080,7 @@ static int hess_scan_block(hprmat_b200_ctx* c, int bi, const hprmat_b200_scan_bl
       HessSolveArgs hr = ha;
       hr.W = nullptr;
       hr.Y = c->hYr.as<double2>();
-      hess_solve_kernel<<<m, kHessThreads, smem_solve, c->stream>>>(hr);
-      LAUNCH_CHECK();
+      TRY(hess_solve(hr, m));
       // G = W^H y_r; Delta = (I + S D)^-1 G; R += Delta
       HPR_CUDA_TRY(cudaMemsetAsync(c->hG.p, 0, (size_t)m * nn * sizeof(double2), c->stream));
       if (zgemm_f64_update_batched(nch, nch, N, WH, nch, 0, c->hYr.as<double2>(), ld, sN, c->hG.as<double2>(), nch,
