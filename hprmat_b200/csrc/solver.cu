@@ -199,6 +199,7 @@ struct hprmat_b200_ctx {
   int hess_fallback_last = 0;    // energies the last shifted scan sent to the LU path
   double hess_ms[6] = {};        // with profiling: reduce, solve, products, refine, U, fallback (ms)
   bool hess_blocked = true;      // blocked (panel + GEMM) Hessenberg reduction
+  int hess_workers = 3;          // shifted scan: blocks in flight at once (worker contexts)
   DevBuf hbY, hbT, hbS, hbVH, hbVT, hbW, hbTmp, hUmat;
   bool f64_pair = true;  // plain FP64 LU: two block steps share one K = 128 trailing update
   DevBuf f64_pair_buf;
@@ -2839,11 +2840,10 @@ static int hess_reduce_blocked(hprmat_b200_ctx* c, double2* A, long ld, int N, d
 // the shifted form (channels whose diagonal energy terms do not move together) or whose
 // Hessenberg or Woodbury pivots vanish are listed in `fallback` for the LU path.  COULFG
 // failures get their status as in rmatrix.
-static int hess_scan_block(hprmat_b200_ctx* c, int bi, const hprmat_b200_scan_block& B, double rmax, int nr,
-                           std::vector<int>& fallback, int* first_error, std::string* err_msg) {
+static int hess_scan_block(hprmat_b200_ctx* c, const double2* d_cpot, const hprmat_b200_scan_block& B, double rmax,
+                           int nr, std::vector<int>& fallback, int* first_error, std::string* err_msg) {
   const int nch = B.nch, N = nch * nr;
   const long ld = N;
-  const double2* d_cpot = c->scan_cpot[bi]->as<double2>();
   auto note = [&](int s) {
     if (s != HPRMAT_B200_OK && *first_error == HPRMAT_B200_OK) {
       *first_error = s;
@@ -3191,37 +3191,104 @@ int hprmat_b200_rmatrix_scan_shifted(hprmat_b200_ctx* c, int nblocks, const hprm
   int first_error = HPRMAT_B200_OK;
   std::string err_msg;
   c->hess_fallback_last = 0;
-  for (int b = 0; b < nblocks; ++b) {
+  // one block on context w: the shifted form, then the LU path for what it does not take
+  auto run_block = [&](hprmat_b200_ctx* w, int b, int* ferr, std::string* emsg) -> int {
     const hprmat_b200_scan_block& B = blocks[b];
+    const double2* d_cpot = c->scan_cpot[b]->as<double2>();
     std::vector<int> fallback;
     if (B.nch > kHsMaxRhs) {
       for (int e = 0; e < B.nenergies; ++e) fallback.push_back(e);
     } else {
-      TRY(hess_scan_block(c, b, B, rmax, nr, fallback, &first_error, &err_msg));
+      TRY(hess_scan_block(w, d_cpot, B, rmax, nr, fallback, ferr, emsg));
     }
-    // the LU path for what the shifted form does not take
-    c->hess_fallback_last += (int)fallback.size();
+    w->hess_fallback_last += (int)fallback.size();
     auto tfb = Clock::now();
     const size_t ubytes = (size_t)B.nch * B.nch * sizeof(double2);
     for (const int e : fallback) {
       int nopen = 0;
-      int s = c->cu.ensure(ubytes);
+      int s = w->cu.ensure(ubytes);
       if (s == HPRMAT_B200_OK)
-        s = rmatrix_core(c, B.nch, B.lval, B.qk + (size_t)e * B.nch, B.eta + (size_t)e * B.nch, rmax, nr, 1,
-                         c->scan_cpot[b]->as<double2>(), B.ncp1, B.nch, c->cu.as<double2>(), &nopen, nullptr);
+        s = rmatrix_core(w, B.nch, B.lval, B.qk + (size_t)e * B.nch, B.eta + (size_t)e * B.nch, rmax, nr, 1, d_cpot,
+                         B.ncp1, B.nch, w->cu.as<double2>(), &nopen, nullptr);
       if (s == HPRMAT_B200_OK || s == HPRMAT_B200_NOT_CONVERGED) {
-        HPR_CUDA_TRY(cudaMemcpyAsync(B.cu + (size_t)e * B.nch * B.nch * 2, c->cu.p, ubytes, cudaMemcpyDeviceToHost,
-                                     c->stream));
-        HPR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        HPR_CUDA_TRY(cudaMemcpyAsync(B.cu + (size_t)e * B.nch * B.nch * 2, w->cu.p, ubytes, cudaMemcpyDeviceToHost,
+                                     w->stream));
+        HPR_CUDA_TRY(cudaStreamSynchronize(w->stream));
       }
       B.nopen[e] = nopen;
       B.status[e] = s;
-      if (s != HPRMAT_B200_OK && first_error == HPRMAT_B200_OK) {
-        first_error = s;
-        err_msg = hprmat_b200_last_error();
+      if (s != HPRMAT_B200_OK && *ferr == HPRMAT_B200_OK) {
+        *ferr = s;
+        *emsg = hprmat_b200_last_error();
       }
     }
-    if (c->profile) c->hess_ms[5] += ms_since(tfb);
+    if (w->profile) w->hess_ms[5] += ms_since(tfb);
+    return HPRMAT_B200_OK;
+  };
+  const int nw = std::max(1, std::min(c->hess_workers, nblocks));
+  if (nw == 1) {
+    for (int b = 0; b < nblocks; ++b) TRY(run_block(c, b, &first_error, &err_msg));
+  } else {
+    // Several blocks in flight, one worker context (stream, buffers, host thread) each, so that
+    // one block's latency-bound reduction overlaps the others' GEMMs and solves.  Blocks go to
+    // the least loaded worker, largest first (cost ~ N^3 for the reduction plus
+    // nenergies N^2 nch for the energies); each worker gets its share of the batch budget.
+    TRY(scan_workers_ready(c, nw, nr, rmax));
+    c->hess_steps_last = 0;
+    std::vector<std::vector<int>> mine((size_t)nw);
+    {
+      std::vector<int> order(nblocks);
+      std::vector<double> cost(nblocks), load((size_t)nw, 0.0);
+      for (int b = 0; b < nblocks; ++b) {
+        order[b] = b;
+        const double n = (double)blocks[b].nch * nr;
+        cost[b] = n * n * n + (double)blocks[b].nenergies * n * n * blocks[b].nch;
+      }
+      std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+      for (const int b : order) {
+        const int i = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        mine[i].push_back(b);
+        load[i] += cost[b];
+      }
+    }
+    std::vector<int> status((size_t)nw, HPRMAT_B200_OK), ferr((size_t)nw, HPRMAT_B200_OK);
+    std::vector<std::string> fail_msg((size_t)nw), emsg((size_t)nw);
+    std::vector<std::thread> th;
+    for (int i = 0; i < nw; ++i) {
+      hprmat_b200_ctx* w = c->scan_workers[i];
+      w->hess_blocked = c->hess_blocked;
+      w->hb_cluster = c->hb_cluster;
+      w->hess_budget_gb = c->hess_budget_gb / nw;
+      w->profile = c->profile;
+      w->hess_fallback_last = 0;
+      for (double& v : w->hess_ms) v = 0.0;
+      th.emplace_back([&, i, w]() {
+        cudaSetDevice(w->device);
+        for (const int b : mine[i]) {
+          const int s = run_block(w, b, &ferr[i], &emsg[i]);
+          if (s != HPRMAT_B200_OK) {
+            status[i] = s;
+            fail_msg[i] = hprmat_b200_last_error();
+            break;
+          }
+        }
+        cudaStreamSynchronize(w->stream);
+      });
+    }
+    for (std::thread& t : th) t.join();
+    for (int i = 0; i < nw; ++i) {
+      hprmat_b200_ctx* w = c->scan_workers[i];
+      c->hess_fallback_last += w->hess_fallback_last;
+      c->hess_steps_last = std::max(c->hess_steps_last, w->hess_steps_last);
+      if (c->profile)
+        for (int k = 0; k < 6; ++k) c->hess_ms[k] += w->hess_ms[k];
+      if (ferr[i] != HPRMAT_B200_OK && first_error == HPRMAT_B200_OK) {
+        first_error = ferr[i];
+        err_msg = emsg[i];
+      }
+    }
+    for (int i = 0; i < nw; ++i)
+      if (status[i] != HPRMAT_B200_OK) return fail(status[i], "rmatrix_scan_shifted: %s", fail_msg[i].c_str());
   }
   if (seconds) *seconds = std::chrono::duration<double>(Clock::now() - t0).count();
   if (first_error != HPRMAT_B200_OK && first_error != HPRMAT_B200_NOT_CONVERGED)
@@ -3925,6 +3992,11 @@ int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* c, const char* key, int value) {
   }
   if (strcmp(key, "f64_pair") == 0) {
     c->f64_pair = value != 0;
+    return HPRMAT_B200_OK;
+  }
+  if (strcmp(key, "hess_workers") == 0) {  // shifted scan: blocks in flight at once, 1..8
+    if (value < 1 || value > 8) return fail(HPRMAT_B200_ERR_ARG, "hess_workers must be 1..8");
+    c->hess_workers = value;
     return HPRMAT_B200_OK;
   }
   if (strcmp(key, "hess_cluster") == 0) {  // CTAs of the column step's cluster: 8 or 16 (0: choose)
