@@ -65,7 +65,7 @@ def parse():
                     help="scan/adjoint: keep a block's factorisation across energies as the refinement's "
                          "preconditioner (opts.reuse_factors); default off (measured faster that way for "
                          "both workloads)")
-    ap.add_argument("--scan-method", choices=["lu", "shifted"], default="lu",
+    ap.add_argument("--scan-method", choices=["lu", "shifted"], default="shifted",
                     help="scan: lu (every energy by its own mixed LU on concurrent worker streams) or shifted (one "
                          "Hessenberg reduction per J-pi block, O(N^2 nch) FP64 work per energy, "
                          "hprmat_b200_rmatrix_scan_shifted)")

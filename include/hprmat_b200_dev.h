@@ -73,7 +73,9 @@ int hprmat_b200_dev_counters(hprmat_b200_ctx* ctx, unsigned long long* launches,
      "hess_blocked"   shifted scan: blocked Hessenberg reduction (1) or one reflector at a
                       time (0);
      "hess_cluster"   CTAs of the blocked reduction's column-step cluster: 8, 16, or 0 to
-                      take 16 where the GPU holds such a cluster. */
+                      take 16 where the GPU holds such a cluster;
+     "hess_workers"   shifted scan: J-pi blocks in flight at once, each on a worker context
+                      of its own, 1..8 (3). */
 int hprmat_b200_dev_set_tuning(hprmat_b200_ctx* ctx, const char* key, int value);
 
 /* Failure-path check: one CTA waits, with a limit of `spins` polls (4096 .. 2^24), on a device
