@@ -477,7 +477,7 @@ def run_sweep(args):
         # the FP64 LU of the same C(E), with its 1-norm condition estimate (Hager-Higham on the
         # FP64 factors; reported separately from the timed mixed solves)
         ctx.set_precision("fp64")
-        # a small FP64 solve first, so that the timed one does not include creating the ZGEMM handle
+        # a small FP64 solve first, so that the timed one does not include the FP64 path's first-use setup
         a_w = np.eye(300, dtype=np.complex128) * 4.0 + 0.01
         ctx.solve_linear(a_w, np.ones((300, 1), np.complex128))
         ctx.set_estimate_condition(True)
@@ -486,13 +486,20 @@ def run_sweep(args):
         kappa1 = ctx.last_stats["cond_estimate"]
         condest_ms = ctx.last_stats["ms_condest"]
         diff = float(np.linalg.norm(cu_m[:nopen, :nopen] - cu_d[:nopen, :nopen]) / np.linalg.norm(cu_d[:nopen, :nopen]))
+        # against the oracle's U (FP64 zgesv) where the committed fixture exists (N = 10000 .. 25600)
+        fx = os.path.join(ROOT, "tests", "golden", f"sweep_u_nch{nch}.npz")
+        err_fx = None
+        if os.path.exists(fx):
+            ref = np.load(fx)["u"]
+            err_fx = float(np.linalg.norm(cu_m[:nopen, :nopen] - ref) / np.linalg.norm(ref))
         n = w.n
         rows.append({"N": n, "nch": nch, "nopen": nopen, "ms_per_solve": best, "solves_per_s": 1e3 / best,
                      "complex_tflops": 8.0 * n ** 3 / 3.0 / (best * 1e-3) / 1e12, "nb": st["nb"],
                      "refine_steps": st["refine_steps"], "inner_iterations": st["inner_iterations"],
                      "rel_residual": st["rel_residual"], "residual_floor": st["residual_floor"],
                      "pivot_growth": st["pivot_growth"], "fp64_fallback": st["fp64_fallback"],
-                     "u_rel_diff_vs_device_fp64": diff, "device_fp64_ms": fp64_ms,
+                     "u_rel_diff_vs_device_fp64": diff, "u_rel_err_vs_oracle_fixture": err_fx,
+                     "device_fp64_ms": fp64_ms,
                      "mixed_over_fp64": fp64_ms / best, "cond1_estimate": kappa1, "cond1_estimate_ms": condest_ms,
                      "tc_update_tflops": tc_flops.value / max(tc_ms.value, 1e-9) / 1e9,
                      "tc_update_share": tc_ms.value / best})
