@@ -185,6 +185,15 @@ struct KineticTile {
   const double2* X;
   long ldx;
   int with_b;
+  long sx = 0, sch = 0;  // per-unit strides of X and of the channel data (batched launches)
+  __device__ KineticTile at(int u) const {
+    KineticTile t = *this;
+    t.X += (size_t)u * sx;
+    t.ch.fac += (size_t)u * sch;
+    t.ch.kk += (size_t)u * sch;
+    t.ch.bloch += (size_t)u * sch;
+    return t;
+  }
   __device__ double a(int c, int i, int j) const {
     const int nr = mesh.nr;
     double k = mesh.tc[i + (size_t)j * nr] - ch.bloch[c] * mesh.blo0[i + (size_t)j * nr];
@@ -206,6 +215,12 @@ struct CouplingTile {
   const double2* X;
   long ldx;
   int nr, nch;
+  long sx = 0;  // per-unit stride of X (batched launches)
+  __device__ CouplingTile at(int u) const {
+    CouplingTile t = *this;
+    t.X += (size_t)u * sx;
+    return t;
+  }
   __device__ double2 a(int i, int c, int cp) const { return vt[((size_t)i * nch + cp) * nch + c]; }
   __device__ double2 b(int i, int cp, int col) const { return X[(size_t)cp * nr + i + (size_t)col * ldx]; }
   __device__ size_t o(int i, int c, int col, long ldo) const { return (size_t)c * nr + i + (size_t)col * ldo; }
@@ -294,15 +309,21 @@ __global__ void __launch_bounds__(256, 2) resid_tile_kernel(Op op, int M, int Nc
 //   kAbs2:   coupling, out += |V| |X| (real part).
 enum ResidTileMode { kComp1 = 0, kComp2 = 1, kAbs1 = 2, kAbs2 = 3 };
 
+// Batched over units (energies): blockIdx.y = column tile + ytiles * unit; unit u works on
+// op.at(u) and on out, lo + u * so.
 template <class Op, bool REAL_A, int MODE>
-__global__ void __launch_bounds__(256) resid_tile2_kernel(Op op, int M, int Ncol, int K, double2* out, long ldo,
-                                                          double2* lo) {
+__global__ void __launch_bounds__(256) resid_tile2_kernel(Op op_all, int M, int Ncol, int K, double2* out, long ldo,
+                                                          double2* lo, int ytiles, long so) {
   constexpr int BM = 32, BN = 64, BK = 16;
   using AT = typename std::conditional<REAL_A, double, double2>::type;
   __shared__ AT As[BK][BM];
   __shared__ double2 Bs[BK][BN + 1];
   const int z = blockIdx.z;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int unit = blockIdx.y / ytiles;
+  const Op op = op_all.at(unit);
+  out += (size_t)unit * so;
+  if (lo) lo += (size_t)unit * so;
+  const int m0 = blockIdx.x * BM, n0 = (blockIdx.y - unit * ytiles) * BN;
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;
   Acc2 sr[2][4], si[2][4];

@@ -1152,17 +1152,18 @@ static int apply_residual(hprmat_b200_ctx* c, const Operator& op, const double2*
     }
     KineticTile kt{op.mesh, op.ch, X, ldx, with_b ? 1 : 0};
     CouplingTile ct{op.vt, X, ldx, nr, op.nch};
-    const dim3 gk(cdiv_u(nr, 32), cdiv_u(ncol, 64), op.nch), gc(cdiv_u(op.nch, 32), cdiv_u(ncol, 64), nr);
+    const int yt = (int)cdiv_u(ncol, 64);
+    const dim3 gk(cdiv_u(nr, 32), yt, op.nch), gc(cdiv_u(op.nch, 32), yt, nr);
     if (absmode) {
-      resid_tile2_kernel<KineticTile, true, kAbs1><<<gk, 256, 0, c->stream>>>(kt, nr, ncol, nr, out, ldo, lo);
+      resid_tile2_kernel<KineticTile, true, kAbs1><<<gk, 256, 0, c->stream>>>(kt, nr, ncol, nr, out, ldo, lo, yt, 0);
       LAUNCH_CHECK();
       resid_tile2_kernel<CouplingTile, false, kAbs2><<<gc, 256, 0, c->stream>>>(ct, op.nch, ncol, op.nch, out, ldo,
-                                                                               lo);
+                                                                               lo, yt, 0);
     } else {
-      resid_tile2_kernel<KineticTile, true, kComp1><<<gk, 256, 0, c->stream>>>(kt, nr, ncol, nr, out, ldo, lo);
+      resid_tile2_kernel<KineticTile, true, kComp1><<<gk, 256, 0, c->stream>>>(kt, nr, ncol, nr, out, ldo, lo, yt, 0);
       LAUNCH_CHECK();
       resid_tile2_kernel<CouplingTile, false, kComp2><<<gc, 256, 0, c->stream>>>(ct, op.nch, ncol, op.nch, out,
-                                                                                ldo, lo);
+                                                                                ldo, lo, yt, 0);
     }
     LAUNCH_CHECK();
     return HPRMAT_B200_OK;
@@ -1178,6 +1179,30 @@ static int apply_residual(hprmat_b200_ctx* c, const Operator& op, const double2*
     // dense operator (solve_linear, non-local potentials): a plain FP64 GEMM (zgemm_f64.cu)
     TRY(zgemm_update(c, N, ncol, N, op.A, op.lda, X, ldx, out, ldo));
   }
+  return HPRMAT_B200_OK;
+}
+
+// The outer (compensated) residual out_u = B - C_u X_u of `units` structured operators that
+// differ only in their channel data (unit u: X + u sx, out + u so, channel data + u sch
+// doubles), two launches for all of them.  op holds unit 0's channel data.
+static int apply_residual_units(hprmat_b200_ctx* c, const Operator& op, const double2* X, long ldx, long sx, int ncol,
+                                double2* out, long ldo, long so, long sch, int units) {
+  const int nr = op.mesh.nr;
+  if (so < ldo * (long)ncol) return fail(HPRMAT_B200_ERR_ARG, "apply_residual_units: unit stride below one block");
+  TRY(c->rlo.ensure((size_t)so * units * sizeof(double2)));
+  double2* lo = c->rlo.as<double2>();
+  KineticTile kt{op.mesh, op.ch, X, ldx, 1};
+  kt.sx = sx;
+  kt.sch = sch;
+  CouplingTile ct{op.vt, X, ldx, nr, op.nch};
+  ct.sx = sx;
+  const int yt = (int)cdiv_u(ncol, 64);
+  const dim3 gk(cdiv_u(nr, 32), yt * units, op.nch), gc(cdiv_u(op.nch, 32), yt * units, nr);
+  resid_tile2_kernel<KineticTile, true, kComp1><<<gk, 256, 0, c->stream>>>(kt, nr, ncol, nr, out, ldo, lo, yt, so);
+  LAUNCH_CHECK();
+  resid_tile2_kernel<CouplingTile, false, kComp2><<<gc, 256, 0, c->stream>>>(ct, op.nch, ncol, op.nch, out, ldo, lo,
+                                                                            yt, so);
+  LAUNCH_CHECK();
   return HPRMAT_B200_OK;
 }
 
@@ -3057,8 +3082,9 @@ static int hess_scan_block(hprmat_b200_ctx* c, const double2* d_cpot, const hprm
     const int max_steps = std::max(1, c->opts.max_refine);
     for (; steps < max_steps; ++steps) {
       NvtxRange nv("hprmat.hess.refine");
-      for (int j = 0; j < m; ++j) {
-        const double* ud_ = unit_d(j);
+      {
+        // r = Q - C(E) X of every unit of the batch in two launches (unit blocks ubp bytes apart)
+        const double* ud_ = unit_d(0);
         Operator op;
         op.structured = true;
         op.mesh = md;
@@ -3069,8 +3095,7 @@ static int hess_scan_block(hprmat_b200_ctx* c, const double2* d_cpot, const hprm
         op.q2 = md.q2;
         op.q1 = md.q1;
         op.nr = nr;
-        TRY(apply_residual(c, op, c->hX.as<double2>() + (size_t)j * sN, ld, nch, c->hR.as<double2>() + (size_t)j * sN,
-                           ld, true));
+        TRY(apply_residual_units(c, op, c->hX.as<double2>(), ld, sN, nch, c->hR.as<double2>(), ld, sN, ldD, m));
       }
       // -y_r = -(H + delta I)^-1 P^H r
       HPR_CUDA_TRY(cudaMemsetAsync(c->hYr.p, 0, (size_t)m * sN * sizeof(double2), c->stream));
