@@ -611,19 +611,22 @@ __global__ void hb_prep_kernel(int N, int k, int b, const double2* __restrict__ 
   for (int j = 0; j < kHbB; ++j) v[j] = j < b ? V[(size_t)(k + j) * ldv + r] : make_double2(0.0, 0.0);
 #pragma unroll
   for (int j = 0; j < kHbB; ++j) VH[(size_t)r * kHbB + j] = make_double2(v[j].x, -v[j].y);
+  // (V T^H)[r, j] = sum_{l >= j} V[r, l] conj(T[j, l]);  (V T)[r, j] = sum_{l <= j} V[r, l] T[l, j].
+  // Both loops fully unrolled (v stays in registers); V is zero in the columns l >= b.
+#pragma unroll
   for (int j = 0; j < kHbB; ++j) {
     double2 acc = make_double2(0.0, 0.0);
-    if (j < b) {
-      // (V T^H)[r, j] = sum_{l >= j} V[r, l] conj(T[j, l]);  (V T)[r, j] = sum_{l <= j} V[r, l] T[l, j]
-      if (conj_t) {
-        for (int l = j; l < b; ++l) {
-          const double2 t = T[(size_t)l * kHbB + j];
-          cfma(acc, v[l], make_double2(t.x, -t.y));
-        }
-      } else {
-        for (int l = 0; l <= j; ++l) cfma(acc, v[l], T[(size_t)j * kHbB + l]);
+    if (conj_t) {
+#pragma unroll
+      for (int l = j; l < kHbB; ++l) {
+        const double2 t = l < b ? T[(size_t)l * kHbB + j] : make_double2(0.0, 0.0);
+        cfma(acc, v[l], make_double2(t.x, -t.y));
       }
+    } else {
+#pragma unroll
+      for (int l = 0; l <= j; ++l) cfma(acc, v[l], T[(size_t)j * kHbB + l]);
     }
+    if (j >= b) acc = make_double2(0.0, 0.0);
     VT[(size_t)j * N + r] = make_double2(-acc.x, -acc.y);
   }
 }
