@@ -314,9 +314,13 @@ def run_scan(args):
                       else "c64 via 3xTF32 tensor cores + c128 refinement"),
             "data": "synthetic (seeded scan generator, hprmat_b200/workloads.py)",
             "config": {"workload": "batched energy scan: 12 J-pi blocks, nch ~ U{4..64} x 60 points "
-                                   "(N = 240..3840), 256 energies each, 3072 solves",
+                                   "(N = 240..3840), 256 energies each, 3072 solves"
+                                   + (f" (first {len(blocks)} block(s) only)" if len(blocks) < 12 else ""),
                        "method": args.scan_method, "blocks": len(blocks),
-                       "workers": args.workers, "reuse_factors": bool(args.reuse),
+                       # the LU scan's worker streams; the shifted scan keeps the library's
+                       # default of 3 blocks in flight
+                       "workers": args.workers if args.scan_method == "lu" else 3,
+                       "reuse_factors": bool(args.reuse),
                        "autotune": bool(args.autotune)},
             "autotune": tune,
             "lu_equivalent_complex_tflops": float(tot_flops.item()) * args.steps / wall / 1e12,
