@@ -215,6 +215,26 @@ def test_shifted_scan_matches_oracle_per_unit():
     ctx.close()
 
 
+def test_shifted_scan_workers_give_identical_results():
+    """Blocks dealt to concurrent worker contexts (hess_workers) go through the same kernels as
+    one block at a time; every energy's arithmetic is independent of the batch and the stream it
+    runs in, so U, nopen and status are bitwise the same for 1 and 3 workers."""
+    from hprmat_b200 import _native as nat
+    lib = nat.load()
+    blocks = _blocks()
+    args = [(w.lval, w.cpot, qk, eta) for w, qk, eta in blocks]
+    ctx = api.Context(precision="mixed")
+    out = {}
+    for nw in (1, 3):
+        nat.check(lib.hprmat_b200_dev_set_tuning(ctx._h, b"hess_workers", nw))
+        out[nw] = ctx.rmatrix_scan(args, 20.0, 60, method="shifted")
+    for (cu1, no1, st1), (cu3, no3, st3) in zip(out[1], out[3]):
+        assert np.array_equal(st1, st3) and np.array_equal(no1, no3)
+        assert np.array_equal(cu1, cu3)
+    assert lib.hprmat_b200_dev_set_tuning(ctx._h, b"hess_workers", 0) == nat.ERR_ARG
+    ctx.close()
+
+
 def test_shifted_scan_on_a_config3_sample():
     """A sample of the energy-scan configuration (blocks of 4..64 channels x 60 points, energies
     in 1-30 MeV): the shifted scan against the oracle on every fourth energy of three blocks,
