@@ -189,8 +189,12 @@ int hprmat_b200_rmatrix_scan(hprmat_b200_ctx* ctx, int nblocks, const hprmat_b20
    every energy then costs O(N^2 nch) -- an LU of H + delta I with row-pair pivoting, the
    back substitution for P^H Q, and the Woodbury identity for the Bloch terms on an nch x nch
    system -- followed by FP64 refinement steps against the structured C(E) (at most
-   opts.max_refine; converged when a step changes R by less than opts.surface_tol).  Energies
-   are solved in batches of independent units per launch.  Units the shifted form cannot take
+   opts.max_refine; converged when a step changes R by less than opts.surface_tol, or when the
+   error that step leaves is predicted a thousand times below it).  Energies are solved in
+   batches of independent units per launch.  Up to three blocks are in flight at once, each on a
+   worker context (stream, working buffers, host thread) that the context creates on the first
+   scan and keeps, as hprmat_b200_rmatrix_scan's workers; the results do not depend on how the
+   blocks are dealt.  Units the shifted form cannot take
    (blocks with more than 64 channels, channels whose energy terms do not move together, a zero
    Hessenberg or Woodbury pivot) run the LU path of hprmat_b200_rmatrix.  Outputs, statuses and
    return value as hprmat_b200_rmatrix_scan; precision is FP64 throughout. */
