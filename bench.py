@@ -522,6 +522,10 @@ def run_sweep(args):
 # ------------------------------------------------------------------ our arm
 def main():
     args = parse()
+    if args.precision != "mixed" and (not args.solves_only or args.workload != "production"):
+        print("bench: --precision fp64 is for --solves-only runs of the production workload (the headline is the "
+              "mixed path)", file=sys.stderr)
+        return 2
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "scan":
@@ -544,9 +548,6 @@ def main():
 
     w = workloads.production(nch=args.nch)
     n_full = w.n
-    if args.precision != "mixed" and not args.solves_only:
-        print("bench: --precision fp64 is for --solves-only runs (the headline is the mixed path)", file=sys.stderr)
-        return 2
     ctx = api.Context(device=local, precision=args.precision, max_refine=3, tol=1e-12)
     stream = torch.cuda.Stream(device=dev)
     ctx.set_stream(stream.cuda_stream)
