@@ -226,7 +226,8 @@ def run_scan(args):
         ks = [workloads.channel_kinematics(e, w.thresholds, w.hm, w.params.z1z2) for e in energies]
         all_inputs.append((w.lval, w.cpot, np.array([k[0] for k in ks]), np.array([k[1] for k in ks])))
     # this rank's runs of 32 energies (one run per block when alone), sharded by cost
-    units, inputs = shard_units(all_inputs, 60, rank, world, chunk=None if world == 1 else 32)
+    units, inputs = shard_units(all_inputs, 60, rank, world, chunk=None if world == 1 else 32,
+                                method=args.scan_method)
     mine = [(blocks[b][0], np.asarray(blocks[b][1])[idx]) for b, idx in units]
     flops = sum(len(e) * 8.0 * float(w.n) ** 3 / 3.0 for w, e in mine)
     nunits = sum(len(e) for _, e in mine)

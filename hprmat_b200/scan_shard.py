@@ -14,7 +14,19 @@ from typing import Callable, Sequence
 
 import numpy as np
 
-__all__ = ["block_costs", "lpt_shards", "scan_units", "shard_units", "run_sharded_scan"]
+__all__ = ["block_costs", "unit_cost", "lpt_shards", "scan_units", "shard_units", "run_sharded_scan"]
+
+
+def unit_cost(nch: int, nr: int, nenergies: int, method: str = "lu") -> float:
+    """Cost of solving nenergies energies of one block of nch channels: nenergies N^3 for the LU
+    method (one factorisation each, N = nch nr); N^3 + nenergies N^2 nch for the shifted method
+    (one Hessenberg reduction for the unit, then O(N^2 nch) per energy)."""
+    n = float(nch * nr)
+    if method == "shifted":
+        return n ** 3 + nenergies * n * n * nch
+    if method == "lu":
+        return nenergies * n ** 3
+    raise ValueError(f"unknown scan method {method!r}")
 
 
 def block_costs(blocks: Sequence, nr: int) -> list[float]:
@@ -49,10 +61,15 @@ def scan_units(blocks: Sequence, chunk: int | None) -> list[tuple[int, np.ndarra
     return units
 
 
-def shard_units(blocks: Sequence, nr: int, rank: int, world: int, chunk: int | None = 32):
-    """This rank's units and the sub-blocks (lval, cpot, qk[idx], eta[idx]) that solve them."""
+def shard_units(blocks: Sequence, nr: int, rank: int, world: int, chunk: int | None = 32, method: str = "lu"):
+    """This rank's units and the sub-blocks (lval, cpot, qk[idx], eta[idx]) that solve them, with
+    the units' costs by ``method`` (unit_cost).  The shifted method reduces every unit's block
+    once, so it is sharded in whole blocks (``chunk`` ignored): a block split over ranks would
+    repeat its reduction on each."""
+    if method == "shifted":
+        chunk = None
     units = scan_units(blocks, chunk)
-    costs = [len(idx) * float(len(blocks[b][0]) * nr) ** 3 for b, idx in units]
+    costs = [unit_cost(len(blocks[b][0]), nr, len(idx), method) for b, idx in units]
     mine = [units[i] for i in lpt_shards(costs, world)[rank]]
     subs = [(blocks[b][0], blocks[b][1], np.asarray(blocks[b][2])[idx], np.asarray(blocks[b][3])[idx])
             for b, idx in mine]

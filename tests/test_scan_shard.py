@@ -11,7 +11,7 @@ import torch.distributed as dist
 import torch.multiprocessing as mp
 
 from hprmat_b200 import workloads
-from hprmat_b200.scan_shard import block_costs, lpt_shards, run_sharded_scan, scan_units, shard_units
+from hprmat_b200.scan_shard import block_costs, lpt_shards, run_sharded_scan, scan_units, shard_units, unit_cost
 from oracle import rmatrix_oracle as orc
 
 NR, RMAX = 16, 12.0
@@ -82,6 +82,27 @@ def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         return s.getsockname()[1]
+
+
+def test_shifted_method_shards_whole_blocks():
+    """The shifted scan reduces each unit's block once, so its shards hold whole blocks: over any
+    number of ranks every block is on exactly one rank with all its energies, and the costs are
+    one reduction plus the energies' O(N^2 nch) work."""
+    b = _blocks()
+    n1 = 5 * NR
+    assert unit_cost(5, NR, 1, "shifted") == n1 ** 3 + n1 * n1 * 5
+    assert unit_cost(5, NR, 1, "lu") == n1 ** 3
+    for world in (1, 2, 3, 6):
+        held = []
+        for rank in range(world):
+            mine, subs = shard_units(b, NR, rank, world, chunk=1, method="shifted")
+            for (blk, idx), sub in zip(mine, subs):
+                assert list(idx) == list(range(np.asarray(b[blk][2]).shape[0]))
+                assert np.array_equal(sub[2], b[blk][2])
+                held.append(blk)
+        assert sorted(held) == list(range(len(b)))
+    with pytest.raises(ValueError):
+        unit_cost(2, NR, 1, "other")
 
 
 def test_two_rank_gloo_sharded_scan_matches_single_process():
