@@ -250,9 +250,12 @@ def run_scan(args):
                 import torch as _t
                 with open(args.tune_cache, "w") as f:
                     json.dump({"device": _t.cuda.get_device_name(local), "workers": args.workers, "table": table}, f)
+    # warm-up: the LU method's first block already runs on every worker; the shifted method
+    # puts up to three blocks in flight, so its warm-up takes all of them (worker contexts and
+    # their buffers are created outside the timed steps)
     for _ in range(args.warmup):
-        ctx.rmatrix_scan(inputs[:1], 20.0, 60, nworkers=args.workers, allow_unconverged=True,
-                         raise_on_unit_error=False, method=args.scan_method)
+        ctx.rmatrix_scan(inputs if args.scan_method == "shifted" else inputs[:1], 20.0, 60, nworkers=args.workers,
+                         allow_unconverged=True, raise_on_unit_error=False, method=args.scan_method)
     lib.hprmat_b200_dev_factorizations(ctx._h, 1)
     secs = []
     res = None
