@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--scan-blocks", type=int, default=0,
                     help="scan: only the first K J-pi blocks (0: all 12; the first is the largest, N = 3180), for "
                          "profiler runs of one block")
+    ap.add_argument("--scan-energies", type=int, default=0,
+                    help="scan: only the first K energies of each block (0: all 256), for profiler runs that must "
+                         "hold little device memory")
     ap.add_argument("--autotune", type=int, default=0,
                     help="scan: run the scan autotuner (hprmat_b200_scan_autotune) on the scan's blocks before "
                          "the warm-up, outside the timed region")
@@ -221,6 +224,8 @@ def run_scan(args):
     blocks = workloads.scan_blocks()
     if args.scan_blocks > 0:
         blocks = blocks[:args.scan_blocks]
+    if args.scan_energies > 0:
+        blocks = [(w, np.asarray(e)[:args.scan_energies]) for w, e in blocks]
     all_inputs = []
     for w, energies in blocks:
         ks = [workloads.channel_kinematics(e, w.thresholds, w.hm, w.params.z1z2) for e in energies]
@@ -319,8 +324,11 @@ def run_scan(args):
             "data": "synthetic (seeded scan generator, hprmat_b200/workloads.py)",
             "config": {"workload": "batched energy scan: 12 J-pi blocks, nch ~ U{4..64} x 60 points "
                                    "(N = 240..3840), 256 energies each, 3072 solves"
-                                   + (f" (first {len(blocks)} block(s) only)" if len(blocks) < 12 else ""),
+                                   + (f" (first {len(blocks)} block(s) only)" if len(blocks) < 12 else "")
+                                   + (f" (first {args.scan_energies} energies of each)" if args.scan_energies > 0
+                                      else ""),
                        "method": args.scan_method, "blocks": len(blocks),
+                       "energies_per_block": args.scan_energies or None,
                        # the LU scan's worker streams; the shifted scan keeps the library's
                        # default of 3 blocks in flight
                        "workers": args.workers if args.scan_method == "lu" else 3,

@@ -17,7 +17,7 @@ def test_help_lists_the_options():
     r = _run("--help")
     assert r.returncode == 0
     for opt in ("--gpus", "--steps", "--warmup", "--impl", "--workload", "--scan-method", "--scan-blocks",
-                "--precision", "--solves-only", "--ref-budget-s"):
+                "--precision", "--solves-only", "--ref-budget-s", "--scan-energies"):
         assert opt in r.stdout, opt
 
 
