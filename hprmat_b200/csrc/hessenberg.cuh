@@ -813,40 +813,101 @@ __global__ void __launch_bounds__(kHessThreads) hess_solve_kernel(HessSolveArgs 
     double2 zc = tid < nch ? a.W[(size_t)tid * a.ldw] : make_double2(0.0, 0.0);
     if (tid == 0) s_info = 0;
     __syncthreads();
-    for (int k = 0; k < N - 1; ++k) {
-      const double2* hn = a.Hr + (size_t)(k + 1) * a.ldh;  // row k + 1 of H (columns k ..)
-      double2 bk = hn[k];
-      const double2 ak = cur[k];
-      const bool swap = (fabs(bk.x) + fabs(bk.y)) > (fabs(ak.x) + fabs(ak.y));
-      const double2 piv = swap ? bk : ak, oth = swap ? ak : bk;
-      const bool zero = piv.x == 0.0 && piv.y == 0.0;
-      const double2 l = zero ? make_double2(0.0, 0.0) : cdiv(oth, piv);
-      if (zero && tid == 0 && s_info == 0) s_info = k + 1;
-      for (int j = k + tid; j < N; j += kHessThreads) {
-        double2 b = hn[j];
-        if (j == k + 1) b.x += dl;
-        const double2 c = cur[j];
-        const double2 p = swap ? b : c, o = swap ? c : b;
-        Ue[(size_t)k * a.ldh + j] = p;
-        if (j > k) {
-          double2 nv = o;
-          cfms(nv, l, p);
-          cur[j] = nv;
+    constexpr int kEV = 16;  // row values per thread held in registers (N <= kEV kHessThreads)
+    if (N <= kEV * kHessThreads) {
+      // Row k + 1 of H (columns k + tid + i kHessThreads), its subdiagonal entry and the
+      // right-hand sides' entries are loaded one step ahead, all in flight together, so that a
+      // step costs one barrier and no dependent load.
+      double2 hv[kEV];
+      auto load_row = [&](int k) {
+        const double2* hn = a.Hr + (size_t)(k + 1) * a.ldh;
+#pragma unroll
+        for (int i = 0; i < kEV; ++i) {
+          const int j = k + tid + i * kHessThreads;
+          hv[i] = j < N ? hn[j] : make_double2(0.0, 0.0);
         }
+      };
+      load_row(0);
+      double2 bk = a.Hr[(size_t)a.ldh];
+      double2 zb = tid < nch ? a.W[(size_t)tid * a.ldw + 1] : make_double2(0.0, 0.0);
+      for (int k = 0; k < N - 1; ++k) {
+        const double2 ak = cur[k];
+        const bool swap = (fabs(bk.x) + fabs(bk.y)) > (fabs(ak.x) + fabs(ak.y));
+        const double2 piv = swap ? bk : ak, oth = swap ? ak : bk;
+        const bool zero = piv.x == 0.0 && piv.y == 0.0;
+        const double2 l = zero ? make_double2(0.0, 0.0) : cdiv(oth, piv);
+        if (zero && tid == 0 && s_info == 0) s_info = k + 1;
+#pragma unroll
+        for (int i = 0; i < kEV; ++i) {
+          const int j = k + tid + i * kHessThreads;
+          if (j < N) {
+            double2 b = hv[i];
+            if (j == k + 1) b.x += dl;
+            const double2 c = cur[j];
+            const double2 p = swap ? b : c, o = swap ? c : b;
+            Ue[(size_t)k * a.ldh + j] = p;
+            if (j > k) {
+              double2 nv = o;
+              cfms(nv, l, p);
+              cur[j] = nv;
+            }
+          }
+        }
+        if (tid == 0) {
+          lm[k] = l;
+          sw[k] = swap ? 1 : 0;
+        }
+        const double2 zk = zb;
+        if (k + 2 < N) {
+          load_row(k + 1);
+          bk = a.Hr[(size_t)(k + 2) * a.ldh + k + 1];
+          if (tid < nch) zb = a.W[(size_t)tid * a.ldw + k + 2];
+        }
+        if (tid < nch) {
+          const double2 zp = swap ? zk : zc, zo = swap ? zc : zk;
+          Y[(size_t)tid * a.ldy + k] = zp;
+          double2 nz = zo;
+          cfms(nz, l, zp);
+          zc = nz;
+        }
+        __syncthreads();
       }
-      if (tid == 0) {
-        lm[k] = l;
-        sw[k] = swap ? 1 : 0;
+    } else {
+      for (int k = 0; k < N - 1; ++k) {
+        const double2* hn = a.Hr + (size_t)(k + 1) * a.ldh;  // row k + 1 of H (columns k ..)
+        double2 bk = hn[k];
+        const double2 ak = cur[k];
+        const bool swap = (fabs(bk.x) + fabs(bk.y)) > (fabs(ak.x) + fabs(ak.y));
+        const double2 piv = swap ? bk : ak, oth = swap ? ak : bk;
+        const bool zero = piv.x == 0.0 && piv.y == 0.0;
+        const double2 l = zero ? make_double2(0.0, 0.0) : cdiv(oth, piv);
+        if (zero && tid == 0 && s_info == 0) s_info = k + 1;
+        for (int j = k + tid; j < N; j += kHessThreads) {
+          double2 b = hn[j];
+          if (j == k + 1) b.x += dl;
+          const double2 c = cur[j];
+          const double2 p = swap ? b : c, o = swap ? c : b;
+          Ue[(size_t)k * a.ldh + j] = p;
+          if (j > k) {
+            double2 nv = o;
+            cfms(nv, l, p);
+            cur[j] = nv;
+          }
+        }
+        if (tid == 0) {
+          lm[k] = l;
+          sw[k] = swap ? 1 : 0;
+        }
+        if (tid < nch) {
+          const double2 zb = a.W[(size_t)tid * a.ldw + k + 1];
+          const double2 zp = swap ? zb : zc, zo = swap ? zc : zb;
+          Y[(size_t)tid * a.ldy + k] = zp;
+          double2 nz = zo;
+          cfms(nz, l, zp);
+          zc = nz;
+        }
+        __syncthreads();
       }
-      if (tid < nch) {
-        const double2 zb = a.W[(size_t)tid * a.ldw + k + 1];
-        const double2 zp = swap ? zb : zc, zo = swap ? zc : zb;
-        Y[(size_t)tid * a.ldy + k] = zp;
-        double2 nz = zo;
-        cfms(nz, l, zp);
-        zc = nz;
-      }
-      __syncthreads();
     }
     if (tid == 0) {
       const double2 d = cur[N - 1];
