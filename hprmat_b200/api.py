@@ -178,7 +178,7 @@ class Context:
         by its own LU on concurrent worker streams, hprmat_b200_rmatrix_scan) or "shifted" (one
         Hessenberg reduction per block and O(N^2 nch) per energy, hprmat_b200_rmatrix_scan_shifted;
         up to three blocks in flight on worker contexts; ``nworkers`` is not used).  For blocks of
-        at most 64 channels the shifted method is the faster one: 1.66-1.69 s against 6.5-7.1 s on
+        at most 64 channels the shifted method is the faster one: 1.61-1.63 s against 6.5-7.1 s on
         the 12-block, 3072-energy scan."""
         keep, arr, out = self._scan_blocks(blocks)
         self._ensure_mesh(nr, 1, rmax)
