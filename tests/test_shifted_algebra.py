@@ -20,6 +20,53 @@ from oracle import rmatrix_oracle as orc
 NR, RMAX = 30, 20.0
 
 
+def _hess_solve(H, delta, Z):
+    """(H + delta I)^-1 Z as hess_solve_kernel computes it: elimination down the rows with a
+    working row, pivoting between the working row and the next row of H (the larger |re| + |im|,
+    the working row on ties), the right-hand sides following row by row; the steps' multipliers
+    and swaps (lm, sw) are kept for re-solves; then back substitution with the upper factor."""
+    n = H.shape[0]
+    U = np.zeros_like(H)
+    lm = np.zeros(n, complex)
+    sw = np.zeros(n, bool)
+    cur = H[0].copy()
+    cur[0] += delta
+    zc = Z[0].copy()
+    Y = np.zeros_like(Z)
+    for k in range(n - 1):
+        nxt = H[k + 1].copy()
+        nxt[k + 1] += delta
+        ak, bk = cur[k], nxt[k]
+        swap = abs(bk.real) + abs(bk.imag) > abs(ak.real) + abs(ak.imag)
+        piv, oth = (bk, ak) if swap else (ak, bk)
+        l = oth / piv
+        p_row, o_row = (nxt, cur) if swap else (cur, nxt)
+        U[k, k:] = p_row[k:]
+        cur = o_row - l * p_row
+        lm[k], sw[k] = l, swap
+        zp, zo = (Z[k + 1], zc) if swap else (zc, Z[k + 1])
+        Y[k] = zp
+        zc = zo - l * zp
+    U[n - 1, n - 1] = cur[n - 1]
+    Y[n - 1] = zc
+    return np.linalg.solve(np.triu(U), Y), (U, lm, sw)
+
+
+def _hess_resolve(factors, Z):
+    """A re-solve with the kept steps: the forward pass over the right-hand sides, then back."""
+    U, lm, sw = factors
+    n = U.shape[0]
+    y = Z.copy()
+    zc = y[0].copy()
+    for k in range(n - 1):
+        zb = y[k + 1].copy()
+        zp, zo = (zb, zc) if sw[k] else (zc, zb)
+        y[k] = zp
+        zc = zo - lm[k] * zp
+    y[n - 1] = zc
+    return np.linalg.solve(np.triu(U), y)
+
+
 def _kk(qk):
     """The diagonal energy term of each channel in the assembly: -k^2 open, +k^2 closed."""
     return np.where(qk > 0, -qk * qk, qk * qk)
@@ -52,7 +99,12 @@ def test_shifted_form_reproduces_the_oracle():
         D = np.diag(np.where(qk < 0, -bnd.xc[:, 0] / RMAX, 0.0))
         assert np.allclose(C, C0 + delta * np.eye(n) + Q @ D @ Q.T, rtol=0, atol=1e-12 * np.abs(C).max())
 
-        Y = np.linalg.solve(H + delta * np.eye(n), W)
+        Y, factors = _hess_solve(H, delta, W)
+        Yl = np.linalg.solve(H + delta * np.eye(n), W)
+        assert np.linalg.norm(Y - Yl) <= 1e-11 * np.linalg.norm(Yl)
+        Z = np.random.default_rng(3).standard_normal((n, 2)) + 0j
+        assert np.linalg.norm(_hess_resolve(factors, Z) - np.linalg.solve(H + delta * np.eye(n), Z)) <= \
+            1e-11 * np.linalg.norm(np.linalg.solve(H + delta * np.eye(n), Z))
         S = Q.T @ P @ Y
         T = np.eye(nch) - D @ np.linalg.solve(np.eye(nch) + S @ D, S)
         R = S @ T
